@@ -1,0 +1,173 @@
+"""Loader for the in-tree CUDA library ``bounce_b200/libb3g.so`` (include/b3g.h).
+
+The product path has no CPU fallback: if the library is missing or a call
+fails, an exception is raised.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libb3g.so")
+
+B3G_OK = 0
+B3G_E_INVALID = -1
+B3G_E_CAPACITY = -2
+B3G_E_CUDA = -3
+B3G_E_TIMEOUT = -4
+B3G_E_STATE = -5
+
+SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_TRIANGLE, SHAPE_HULL, SHAPE_MESH = 0, 1, 2, 3, 4
+BODY_STATIC, BODY_KINEMATIC, BODY_DYNAMIC = 0, 1, 2
+FLAG_WARM_STARTING = 1
+FLAG_CONVEX_CACHE = 2
+FIXTURE_SENSOR = 1
+
+
+class B3GError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"b3g error {code}: {msg}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("max_proxies", ctypes.c_uint32),
+        ("max_contacts", ctypes.c_uint32),
+        ("max_hull_data", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class Counts(ctypes.Structure):
+    _fields_ = [
+        ("contacts", ctypes.c_uint32),
+        ("begun", ctypes.c_uint32),
+        ("ended", ctypes.c_uint32),
+        ("touching", ctypes.c_uint32),
+        ("manifolds", ctypes.c_uint32),
+        ("points", ctypes.c_uint32),
+        ("moved", ctypes.c_uint32),
+        ("status", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# b3ManifoldPoint / b3Manifold (include/bounce/collision/collision.h:97-128), 72 / 320 bytes.
+POINT_DTYPE = np.dtype(
+    [
+        ("n", "<f4", 3),
+        ("p1", "<f4", 3),
+        ("p2", "<f4", 3),
+        ("normalImpulse", "<f4"),
+        ("triangleKey", "<u4"),
+        ("pad0", "<u4"),
+        ("key", "<u4", 4),
+        ("persisting", "u1"),
+        ("edgeContact", "u1"),
+        ("pad1", "u1", 6),
+    ]
+)
+MANIFOLD_DTYPE = np.dtype(
+    [
+        ("points", POINT_DTYPE, 4),
+        ("pointCount", "<u4"),
+        ("tangentImpulse", "<f4", 2),
+        ("motorImpulse", "<f4"),
+        ("motorSpeed", "<f4"),
+        ("tangentSpeed1", "<f4"),
+        ("tangentSpeed2", "<f4"),
+        ("pad", "<u4"),
+    ]
+)
+assert POINT_DTYPE.itemsize == 72 and MANIFOLD_DTYPE.itemsize == 320
+
+EXPORTED = [
+    "b3g_create",
+    "b3g_destroy",
+    "b3g_last_error",
+    "b3g_set_hulls",
+    "b3g_set_bodies",
+    "b3g_set_fixtures",
+    "b3g_set_awake",
+    "b3g_collide",
+    "b3g_get_counts",
+    "b3g_fetch_contacts",
+    "b3g_fetch_manifolds",
+    "b3g_fetch_touching",
+    "b3g_fetch_ended",
+    "b3g_fetch_caches",
+    "b3g_fetch_fat_aabbs",
+    "b3g_load_impulses",
+    "b3g_device_results",
+    "b3g_collide_pairs",
+    "b3g_hull_from_points",
+    "b3g_hull_box",
+]
+
+_lib = None
+
+
+def _p(t):
+    return ctypes.POINTER(t)
+
+
+def load():
+    """Load libb3g.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+            "(make -C bounce_b200/csrc); there is no CPU fallback"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    u32p, f32p, u8p, vp = _p(ctypes.c_uint32), _p(ctypes.c_float), _p(ctypes.c_uint8), ctypes.c_void_p
+    ctx = ctypes.c_void_p
+    sig = {
+        "b3g_create": ([_p(Config), _p(ctypes.c_void_p)], ctypes.c_int),
+        "b3g_destroy": ([ctx], None),
+        "b3g_last_error": ([ctx], ctypes.c_char_p),
+        "b3g_set_hulls": ([ctx, ctypes.c_uint32, u32p, f32p, u32p, u32p, f32p, f32p], ctypes.c_int),
+        "b3g_set_bodies": ([ctx, ctypes.c_uint32, u32p, u32p, u8p], ctypes.c_int),
+        "b3g_set_fixtures": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, u32p], ctypes.c_int),
+        "b3g_set_awake": ([ctx, u8p], ctypes.c_int),
+        "b3g_collide": ([ctx, vp, ctypes.c_int, vp], ctypes.c_int),
+        "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
+        "b3g_fetch_contacts": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_ended": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_caches": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_fat_aabbs": ([ctx, f32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_load_impulses": ([ctx, f32p, f32p, f32p], ctypes.c_int),
+        "b3g_device_results": ([ctx, _p(ctypes.c_void_p), _p(ctypes.c_void_p)], ctypes.c_int),
+        "b3g_collide_pairs": (
+            [ctx, ctypes.c_uint32, u32p, u32p, f32p, f32p, f32p, f32p, u32p, vp],
+            ctypes.c_int,
+        ),
+        "b3g_hull_from_points": ([f32p, ctypes.c_uint32, f32p, u32p, u32p, f32p, f32p, u32p], ctypes.c_int),
+        "b3g_hull_box": (
+            [ctypes.c_float, ctypes.c_float, ctypes.c_float, f32p, u32p, u32p, f32p, f32p, u32p],
+            ctypes.c_int,
+        ),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def ptr(a, t):
+    """ctypes pointer into a C-contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(ctypes.POINTER(t))

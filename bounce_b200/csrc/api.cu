@@ -1,0 +1,865 @@
+// C ABI of the pipeline (include/b3g.h): context lifetime, scene upload, the
+// pass sequence and result transfers. Device memory is allocated once in
+// b3g_create for the configured capacities.
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "collide_common.cuh"
+
+void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
+void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	cudaStream_t s);
+void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s);
+
+namespace {
+
+int fail(b3g_ctx* c, int code, const char* fmt, ...)
+{
+	if (c)
+	{
+		char buf[512];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		c->err = buf;
+	}
+	return code;
+}
+
+#define CK(call)                                                                                 \
+	do                                                                                           \
+	{                                                                                            \
+		cudaError_t e_ = (call);                                                                 \
+		if (e_ != cudaSuccess)                                                                   \
+			return fail(c, B3G_E_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));         \
+	} while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t count)
+{
+	if (count == 0)
+		count = 1;
+	return cudaMalloc((void**)p, sizeof(T) * count);
+}
+
+template <class T>
+void dfree(T*& p)
+{
+	if (p)
+		cudaFree((void*)p);
+	p = nullptr;
+}
+
+uint32_t pow2_at_least(uint32_t v)
+{
+	uint32_t p = 1;
+	while (p < v)
+		p <<= 1;
+	return p;
+}
+
+__global__ void k_pass_begin(uint32_t* counters, int havePass, uint32_t cap)
+{
+	uint32_t i = threadIdx.x;
+	if (i >= CTR_COUNT)
+		return;
+	uint32_t pairs = counters[CTR_PAIRS];
+	__syncthreads();
+	if (i == CTR_PREV_PAIRS)
+		counters[i] = havePass ? min(pairs, cap) : 0u;
+	else
+		counters[i] = 0;
+}
+
+__global__ void k_touch_flags(const DevManifold* man, const uint32_t* cstate, uint32_t n, uint32_t* flags)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n)
+		return;
+	flags[c] = (((cstate[c] >> 8) & 0xFFu) && man[c].pointCount > 0) ? 1u : 0u;
+}
+
+__global__ void k_touch_scatter(const DevManifold* man, const uint32_t* flagsIn, const uint32_t* offsets,
+	uint32_t n, uint32_t* index, DevManifold* out)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n || !flagsIn[c])
+		return;
+	uint32_t o = offsets[c];
+	index[o] = c;
+	out[o] = man[c];
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+
+extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
+{
+	if (!cfg || !out)
+		return B3G_E_INVALID;
+	*out = nullptr;
+	b3g_ctx* c = new b3g_ctx();
+	std::memset(&c->scene, 0, sizeof(c->scene));
+	std::memset(&c->buf, 0, sizeof(c->buf));
+	c->cfg = *cfg;
+	c->device = cfg->device;
+	c->stream = nullptr;
+	c->nHulls = c->nBodies = c->nFixtures = 0;
+	c->nWorlds = 1;
+	c->hullVerts = c->hullEdges = c->hullFaces = 0;
+	c->maxUniqueEdges = 0;
+	c->cur = 0;
+	c->creationPass = true;
+	c->havePass = false;
+	c->impulsesLoaded = false;
+	c->dHulls = nullptr;
+	c->dHverts = nullptr;
+	c->dHedges = nullptr;
+	c->dHfaces = nullptr;
+	c->dHplanes = nullptr;
+	c->dBodyWorld = c->dBodyType = nullptr;
+	c->dBodyAwake = nullptr;
+	c->dBodyState = nullptr;
+	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = nullptr;
+	c->dFixParams = nullptr;
+	c->hCounters = nullptr;
+	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
+	{
+		delete c;
+		return B3G_E_INVALID;
+	}
+	int rc = B3G_OK;
+	auto step = [&](cudaError_t e, const char* what) {
+		if (rc == B3G_OK && e != cudaSuccess)
+			rc = fail(c, B3G_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+	};
+	step(cudaSetDevice(cfg->device), "cudaSetDevice");
+	step(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+	const uint32_t P = cfg->max_proxies, C = cfg->max_contacts;
+	Buffers& B = c->buf;
+	step(dalloc(&B.fatLo, P), "alloc");
+	step(dalloc(&B.fatHi, P), "alloc");
+	step(dalloc(&B.moved, P), "alloc");
+	step(dalloc(&B.keysA, P), "alloc");
+	step(dalloc(&B.keysB, P), "alloc");
+	step(dalloc(&B.valsA, P), "alloc");
+	step(dalloc(&B.valsB, P), "alloc");
+	step(dalloc(&B.sortHist, 256 * ((P + 4095) / 4096 + 1)), "alloc");
+	step(dalloc(&B.sceneBounds, 8), "alloc");
+	step(dalloc(&B.nodeLo, 2 * P), "alloc");
+	step(dalloc(&B.nodeHi, 2 * P), "alloc");
+	step(dalloc(&B.nodeLeft, 2 * P), "alloc");
+	step(dalloc(&B.nodeRight, 2 * P), "alloc");
+	step(dalloc(&B.nodeRope, 2 * P), "alloc");
+	step(dalloc(&B.nodeFirst, 2 * P), "alloc");
+	step(dalloc(&B.nodeParent, 2 * P), "alloc");
+	step(dalloc(&B.nodeEnd, P), "alloc");
+	step(dalloc(&B.splitRight, P), "alloc");
+	step(dalloc(&B.refitFlag, P), "alloc");
+	step(dalloc(&B.worldEnd, P), "alloc");
+	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
+	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
+	for (int k = 0; k < 2; ++k)
+	{
+		step(dalloc(&B.pairA[k], C), "alloc");
+		step(dalloc(&B.pairB[k], C), "alloc");
+		step(dalloc(&B.cstate[k], C), "alloc");
+		step(dalloc(&B.cache[k], C), "alloc");
+		step(dalloc(&B.man[k], C), "alloc");
+	}
+	B.hashCap = pow2_at_least(2 * C);
+	for (int k = 0; k < 2; ++k)
+	{
+		step(dalloc(&B.hashKeys[k], B.hashCap), "alloc");
+		step(dalloc(&B.hashVals[k], B.hashCap), "alloc");
+	}
+	step(dalloc(&B.prevIndex, C), "alloc");
+	step(dalloc(&B.prevFound, C), "alloc");
+	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
+	step(dalloc(&B.counters, CTR_COUNT), "alloc");
+	step(dalloc(&B.endedList, 3 * (size_t)C), "alloc");
+	step(dalloc(&B.touchIndex, C), "alloc");
+	step(dalloc(&B.touchMan, C), "alloc");
+	step(dalloc(&B.contactOut, 3 * (size_t)C), "alloc");
+	step(dalloc(&B.impulseNormal, 4 * (size_t)C), "alloc");
+	step(dalloc(&B.impulseTangent, 2 * (size_t)C), "alloc");
+	step(dalloc(&B.impulseMotor, C), "alloc");
+	step(cudaMallocHost((void**)&c->hCounters, sizeof(uint32_t) * CTR_COUNT), "cudaMallocHost");
+	if (rc == B3G_OK)
+	{
+		step(cudaMemsetAsync(B.counters, 0, sizeof(uint32_t) * CTR_COUNT, c->stream), "memset");
+		step(cudaMemsetAsync(B.cstate[0], 0, sizeof(uint32_t) * C, c->stream), "memset");
+		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
+		step(cudaMemsetAsync(B.hashKeys[0], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
+		step(cudaMemsetAsync(B.hashKeys[1], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
+		step(cudaStreamSynchronize(c->stream), "sync");
+	}
+	if (rc != B3G_OK)
+	{
+		std::string msg = c->err;
+		b3g_destroy(c);
+		fprintf(stderr, "b3g_create: %s\n", msg.c_str());
+		return rc;
+	}
+	*out = c;
+	return B3G_OK;
+}
+
+extern "C" void b3g_destroy(b3g_ctx* c)
+{
+	if (!c)
+		return;
+	cudaSetDevice(c->device);
+	if (c->stream)
+		cudaStreamSynchronize(c->stream);
+	Buffers& B = c->buf;
+	dfree(B.fatLo);
+	dfree(B.fatHi);
+	dfree(B.moved);
+	dfree(B.keysA);
+	dfree(B.keysB);
+	dfree(B.valsA);
+	dfree(B.valsB);
+	dfree(B.sortHist);
+	dfree(B.sceneBounds);
+	dfree(B.nodeLo);
+	dfree(B.nodeHi);
+	dfree(B.nodeLeft);
+	dfree(B.nodeRight);
+	dfree(B.nodeRope);
+	dfree(B.nodeFirst);
+	dfree(B.nodeParent);
+	dfree(B.nodeEnd);
+	dfree(B.splitRight);
+	dfree(B.refitFlag);
+	dfree(B.worldEnd);
+	dfree(B.leafCount);
+	dfree(B.scanAux);
+	for (int k = 0; k < 2; ++k)
+	{
+		dfree(B.pairA[k]);
+		dfree(B.pairB[k]);
+		dfree(B.cstate[k]);
+		dfree(B.cache[k]);
+		dfree(B.man[k]);
+		dfree(B.hashKeys[k]);
+		dfree(B.hashVals[k]);
+	}
+	dfree(B.prevIndex);
+	dfree(B.prevFound);
+	dfree(B.bucketList);
+	dfree(B.counters);
+	dfree(B.endedList);
+	dfree(B.touchIndex);
+	dfree(B.touchMan);
+	dfree(B.contactOut);
+	dfree(B.impulseNormal);
+	dfree(B.impulseTangent);
+	dfree(B.impulseMotor);
+	dfree(c->dHulls);
+	dfree(c->dHverts);
+	dfree(c->dHedges);
+	dfree(c->dHfaces);
+	dfree(c->dHplanes);
+	dfree(c->dBodyWorld);
+	dfree(c->dBodyType);
+	dfree(c->dBodyAwake);
+	dfree(c->dBodyState);
+	dfree(c->dFixBody);
+	dfree(c->dFixType);
+	dfree(c->dFixHull);
+	dfree(c->dFixFlags);
+	dfree(c->dFixKey);
+	dfree(c->dFixParams);
+	if (c->hCounters)
+		cudaFreeHost(c->hCounters);
+	if (c->stream)
+		cudaStreamDestroy(c->stream);
+	delete c;
+}
+
+extern "C" const char* b3g_last_error(const b3g_ctx* c)
+{
+	return c ? c->err.c_str() : "null context";
+}
+
+extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, const float* verts,
+	const uint32_t* edges, const uint32_t* faces, const float* planes, const float* centroids)
+{
+	if (!c || (nh && (!desc || !verts || !edges || !faces || !planes || !centroids)))
+		return fail(c, B3G_E_INVALID, "b3g_set_hulls: null argument");
+	CK(cudaSetDevice(c->device));
+	uint32_t nv = 0, ne = 0, nf = 0, maxUE = 0;
+	std::vector<HullDesc> hd(nh);
+	for (uint32_t h = 0; h < nh; ++h)
+	{
+		const uint32_t* d = desc + 6 * h;
+		if (d[1] < 1 || d[3] < 2 || (d[3] & 1u) || d[5] < 1)
+			return fail(c, B3G_E_INVALID, "hull %u: bad counts", h);
+		for (uint32_t e = 0; e < d[3]; ++e)
+		{
+			const uint32_t* E = edges + 5 * (size_t)(d[2] + e);
+			if (E[1] != (e ^ 1u))
+				return fail(c, B3G_E_INVALID, "hull %u: twin of half-edge %u is not %u", h, e, e ^ 1u);
+			if (E[0] >= d[1] || E[2] >= d[5] || E[3] >= d[3] || E[4] >= d[3])
+				return fail(c, B3G_E_INVALID, "hull %u: half-edge %u out of range", h, e);
+		}
+		for (uint32_t f = 0; f < d[5]; ++f)
+			if (faces[d[4] + f] >= d[3])
+				return fail(c, B3G_E_INVALID, "hull %u: face %u edge out of range", h, f);
+		hd[h] = HullDesc{d[0], d[1], d[2], d[3], d[4], d[5], centroids[3 * h], centroids[3 * h + 1],
+			centroids[3 * h + 2], {0, 0, 0}};
+		nv = std::max(nv, d[0] + d[1]);
+		ne = std::max(ne, d[2] + d[3]);
+		nf = std::max(nf, d[4] + d[5]);
+		maxUE = std::max(maxUE, d[3] / 2);
+	}
+	if (c->cfg.max_hull_data && (size_t)nv + ne + nf > c->cfg.max_hull_data)
+		return fail(c, B3G_E_CAPACITY, "hull data %zu exceeds max_hull_data %u", (size_t)nv + ne + nf,
+			c->cfg.max_hull_data);
+	std::vector<float4> v4(nv), p4(nf);
+	std::vector<uint4> e4(ne);
+	for (uint32_t i = 0; i < nv; ++i)
+		v4[i] = make_float4(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2], 0.0f);
+	for (uint32_t i = 0; i < nf; ++i)
+		p4[i] = make_float4(planes[4 * i], planes[4 * i + 1], planes[4 * i + 2], planes[4 * i + 3]);
+	for (uint32_t i = 0; i < ne; ++i)
+		e4[i] = make_uint4(edges[5 * i + 0], edges[5 * i + 2], edges[5 * i + 3], edges[5 * i + 4]);
+	dfree(c->dHulls);
+	dfree(c->dHverts);
+	dfree(c->dHedges);
+	dfree(c->dHfaces);
+	dfree(c->dHplanes);
+	CK(dalloc(&c->dHulls, nh));
+	CK(dalloc(&c->dHverts, nv));
+	CK(dalloc(&c->dHedges, ne));
+	CK(dalloc(&c->dHfaces, nf));
+	CK(dalloc(&c->dHplanes, nf));
+	if (nh)
+	{
+		CK(cudaMemcpy(c->dHulls, hd.data(), sizeof(HullDesc) * nh, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dHverts, v4.data(), sizeof(float4) * nv, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dHedges, e4.data(), sizeof(uint4) * ne, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dHfaces, faces, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dHplanes, p4.data(), sizeof(float4) * nf, cudaMemcpyHostToDevice));
+	}
+	c->nHulls = nh;
+	c->hullVerts = nv;
+	c->hullEdges = ne;
+	c->hullFaces = nf;
+	c->maxUniqueEdges = maxUE;
+	c->scene.hulls = c->dHulls;
+	c->scene.hverts = c->dHverts;
+	c->scene.hedges = c->dHedges;
+	c->scene.hfaces = c->dHfaces;
+	c->scene.hplanes = c->dHplanes;
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, const uint32_t* type,
+	const uint8_t* awake)
+{
+	if (!c || (nb && (!world || !type || !awake)))
+		return fail(c, B3G_E_INVALID, "b3g_set_bodies: null argument");
+	CK(cudaSetDevice(c->device));
+	uint32_t nw = 1;
+	for (uint32_t i = 0; i < nb; ++i)
+	{
+		if (type[i] > B3G_BODY_DYNAMIC)
+			return fail(c, B3G_E_INVALID, "body %u: bad type %u", i, type[i]);
+		nw = std::max(nw, world[i] + 1);
+	}
+	if (nw > c->cfg.max_proxies)
+		return fail(c, B3G_E_CAPACITY, "too many worlds");
+	dfree(c->dBodyWorld);
+	dfree(c->dBodyType);
+	dfree(c->dBodyAwake);
+	dfree(c->dBodyState);
+	CK(dalloc(&c->dBodyWorld, nb));
+	CK(dalloc(&c->dBodyType, nb));
+	CK(dalloc(&c->dBodyAwake, nb));
+	CK(dalloc(&c->dBodyState, 17 * (size_t)nb));
+	if (nb)
+	{
+		CK(cudaMemcpy(c->dBodyWorld, world, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dBodyType, type, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dBodyAwake, awake, nb, cudaMemcpyHostToDevice));
+	}
+	c->nBodies = nb;
+	c->nWorlds = nw;
+	c->scene.bodyWorld = c->dBodyWorld;
+	c->scene.bodyType = c->dBodyType;
+	c->scene.bodyAwake = c->dBodyAwake;
+	c->scene.bodyState = c->dBodyState;
+	c->creationPass = true;
+	c->havePass = false;
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, const uint32_t* shapeType,
+	const uint32_t* hull, const float* params, const uint32_t* flags, const uint32_t* proxyKey)
+{
+	if (!c || (nf && (!body || !shapeType || !hull || !params || !flags)))
+		return fail(c, B3G_E_INVALID, "b3g_set_fixtures: null argument");
+	if (nf > c->cfg.max_proxies)
+		return fail(c, B3G_E_CAPACITY, "%u fixtures exceed max_proxies %u", nf, c->cfg.max_proxies);
+	CK(cudaSetDevice(c->device));
+	std::vector<uint32_t> key(nf);
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		if (body[i] >= c->nBodies)
+			return fail(c, B3G_E_INVALID, "fixture %u: body %u out of range", i, body[i]);
+		if (shapeType[i] > B3G_SHAPE_HULL)
+			return fail(c, B3G_E_INVALID, "fixture %u: shape type %u not supported", i, shapeType[i]);
+		if (shapeType[i] == B3G_SHAPE_HULL && hull[i] >= c->nHulls)
+			return fail(c, B3G_E_INVALID, "fixture %u: hull %u out of range", i, hull[i]);
+		key[i] = proxyKey ? proxyKey[i] : i;
+	}
+	std::vector<float4> p4(3 * (size_t)nf);
+	for (size_t i = 0; i < 3 * (size_t)nf; ++i)
+		p4[i] = make_float4(params[4 * i], params[4 * i + 1], params[4 * i + 2], params[4 * i + 3]);
+	dfree(c->dFixBody);
+	dfree(c->dFixType);
+	dfree(c->dFixHull);
+	dfree(c->dFixFlags);
+	dfree(c->dFixKey);
+	dfree(c->dFixParams);
+	CK(dalloc(&c->dFixBody, nf));
+	CK(dalloc(&c->dFixType, nf));
+	CK(dalloc(&c->dFixHull, nf));
+	CK(dalloc(&c->dFixFlags, nf));
+	CK(dalloc(&c->dFixKey, nf));
+	CK(dalloc(&c->dFixParams, 3 * (size_t)nf));
+	if (nf)
+	{
+		CK(cudaMemcpy(c->dFixBody, body, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixType, shapeType, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixHull, hull, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixFlags, flags, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixKey, key.data(), sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixParams, p4.data(), sizeof(float4) * 3 * nf, cudaMemcpyHostToDevice));
+	}
+	c->hFixType.assign(shapeType, shapeType + nf);
+	c->nFixtures = nf;
+	c->scene.fixBody = c->dFixBody;
+	c->scene.fixType = c->dFixType;
+	c->scene.fixHull = c->dFixHull;
+	c->scene.fixFlags = c->dFixFlags;
+	c->scene.fixKey = c->dFixKey;
+	c->scene.fixParams = c->dFixParams;
+	c->creationPass = true;
+	c->havePass = false;
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_awake(b3g_ctx* c, const uint8_t* awake)
+{
+	if (!c || !awake)
+		return fail(c, B3G_E_INVALID, "b3g_set_awake: null argument");
+	CK(cudaSetDevice(c->device));
+	if (c->nBodies)
+		CK(cudaMemcpyAsync(c->dBodyAwake, awake, c->nBodies, cudaMemcpyHostToDevice, c->stream));
+	return B3G_OK;
+}
+
+extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* stream)
+{
+	if (!c || !state)
+		return fail(c, B3G_E_INVALID, "b3g_collide: null argument");
+	if (c->nBodies == 0 || c->nFixtures == 0)
+		return fail(c, B3G_E_STATE, "b3g_collide: no scene");
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
+	if (onDevice)
+		CK(cudaMemcpyAsync(c->dBodyState, state, bytes, cudaMemcpyDeviceToDevice, s));
+	else
+		CK(cudaMemcpyAsync(c->dBodyState, state, bytes, cudaMemcpyHostToDevice, s));
+	if (c->havePass)
+		c->cur ^= 1u;
+	k_pass_begin<<<1, CTR_COUNT, 0, s>>>(c->buf.counters, c->havePass ? 1 : 0, c->cfg.max_contacts);
+	launch_sync(c, s);
+	launch_broadphase(c, s);
+	launch_pairs_diff(c, s);
+	launch_narrowphase(c, s);
+	launch_finalize(c, s);
+	CK(cudaGetLastError());
+	c->creationPass = false;
+	c->havePass = true;
+	c->impulsesLoaded = false;
+	return B3G_OK;
+}
+
+static int sync_counts(b3g_ctx* c)
+{
+	CK(cudaSetDevice(c->device));
+	CK(cudaMemcpyAsync(c->hCounters, c->buf.counters, sizeof(uint32_t) * CTR_COUNT, cudaMemcpyDeviceToHost,
+		c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	CK(cudaDeviceSynchronize());
+	return B3G_OK;
+}
+
+static uint32_t status_code(uint32_t st)
+{
+	if (st & (B3G_ST_PAIR_OVERFLOW | B3G_ST_HASH_OVERFLOW | B3G_ST_POLY_OVERFLOW))
+		return (uint32_t)(-B3G_E_CAPACITY);
+	if (st & B3G_ST_WAIT_TIMEOUT)
+		return (uint32_t)(-B3G_E_TIMEOUT);
+	return 0;
+}
+
+extern "C" int b3g_get_counts(b3g_ctx* c, b3g_counts* out)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "b3g_get_counts: null argument");
+	int rc = sync_counts(c);
+	if (rc)
+		return rc;
+	const uint32_t* h = c->hCounters;
+	out->contacts = std::min(h[CTR_PAIRS], c->cfg.max_contacts);
+	out->begun = h[CTR_BEGUN];
+	out->ended = h[CTR_ENDED];
+	out->touching = h[CTR_TOUCHING];
+	out->manifolds = h[CTR_MANIFOLDS];
+	out->points = h[CTR_POINTS];
+	out->moved = h[CTR_MOVED];
+	out->status = status_code(h[CTR_STATUS]);
+	if (out->status)
+		return fail(c, -(int)out->status, "pass status 0x%x (pairs %u, capacity %u)", h[CTR_STATUS],
+			h[CTR_PAIRS], c->cfg.max_contacts);
+	return B3G_OK;
+}
+
+static int contacts_now(b3g_ctx* c, uint32_t& n)
+{
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "no pass yet");
+	int rc = sync_counts(c);
+	if (rc)
+		return rc;
+	n = std::min(c->hCounters[CTR_PAIRS], c->cfg.max_contacts);
+	return B3G_OK;
+}
+
+extern "C" int b3g_fetch_contacts(b3g_ctx* c, uint32_t* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	n = std::min(n, capacity);
+	if (n)
+		CK(cudaMemcpy(out, c->buf.contactOut, sizeof(uint32_t) * 3 * n, cudaMemcpyDeviceToHost));
+	return (int)n;
+}
+
+extern "C" int b3g_fetch_manifolds(b3g_ctx* c, void* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	n = std::min(n, capacity);
+	if (n)
+		CK(cudaMemcpy(out, c->buf.man[c->cur], sizeof(DevManifold) * n, cudaMemcpyDeviceToHost));
+	return (int)n;
+}
+
+extern "C" int b3g_fetch_touching(b3g_ctx* c, uint32_t* index, void* manifolds, uint32_t capacity)
+{
+	if (!c || !index || !manifolds)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	Buffers& B = c->buf;
+	if (n == 0)
+		return 0;
+	uint32_t* flags = B.leafCount; // sized max(P, C)
+	k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], B.cstate[c->cur], n, flags);
+	CK(cudaMemcpyAsync(B.prevIndex, flags, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+	scan_exclusive(flags, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
+	k_touch_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], (const uint32_t*)B.prevIndex, flags,
+		n, B.touchIndex, B.touchMan);
+	uint32_t total = 0;
+	CK(cudaMemcpyAsync(&total, B.counters + CTR_TOUCH_OUT, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	uint32_t m = std::min(total, capacity);
+	if (m)
+	{
+		CK(cudaMemcpy(index, B.touchIndex, sizeof(uint32_t) * m, cudaMemcpyDeviceToHost));
+		CK(cudaMemcpy(manifolds, B.touchMan, sizeof(DevManifold) * m, cudaMemcpyDeviceToHost));
+	}
+	return (int)m;
+}
+
+extern "C" int b3g_fetch_ended(b3g_ctx* c, uint32_t* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	uint32_t m = std::min(c->hCounters[CTR_ENDED], capacity);
+	if (m)
+		CK(cudaMemcpy(out, c->buf.endedList, sizeof(uint32_t) * 3 * m, cudaMemcpyDeviceToHost));
+	return (int)m;
+}
+
+extern "C" int b3g_fetch_caches(b3g_ctx* c, uint32_t* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	n = std::min(n, capacity);
+	if (n)
+		CK(cudaMemcpy(out, c->buf.cache[c->cur], sizeof(uint4) * n, cudaMemcpyDeviceToHost));
+	return (int)n;
+}
+
+extern "C" int b3g_fetch_fat_aabbs(b3g_ctx* c, float* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "no pass yet");
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	uint32_t n = std::min(c->nFixtures, capacity);
+	std::vector<float4> lo(n), hi(n);
+	if (n)
+	{
+		CK(cudaMemcpy(lo.data(), c->buf.fatLo, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+		CK(cudaMemcpy(hi.data(), c->buf.fatHi, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+	}
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		out[6 * i + 0] = lo[i].x;
+		out[6 * i + 1] = lo[i].y;
+		out[6 * i + 2] = lo[i].z;
+		out[6 * i + 3] = hi[i].x;
+		out[6 * i + 4] = hi[i].y;
+		out[6 * i + 5] = hi[i].z;
+	}
+	return (int)n;
+}
+
+extern "C" int b3g_load_impulses(b3g_ctx* c, const float* normal, const float* tangent, const float* motor)
+{
+	if (!c || !normal || !tangent || !motor)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	if (n)
+	{
+		CK(cudaMemcpy(c->buf.impulseNormal, normal, sizeof(float) * 4 * n, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->buf.impulseTangent, tangent, sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->buf.impulseMotor, motor, sizeof(float) * n, cudaMemcpyHostToDevice));
+	}
+	c->impulsesLoaded = true;
+	return B3G_OK;
+}
+
+extern "C" int b3g_device_results(b3g_ctx* c, const void** contacts, const void** manifolds)
+{
+	if (!c || !contacts || !manifolds)
+		return fail(c, B3G_E_INVALID, "null argument");
+	*contacts = c->buf.contactOut;
+	*manifolds = c->buf.man[c->cur];
+	return B3G_OK;
+}
+
+// Stand-alone narrowphase over a caller's pair list (see include/b3g.h).
+extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, const uint32_t* fixB,
+	const float* xfA, const float* xfB, const float* xf0A, const float* xf0B, uint32_t* cache4, void* manifolds)
+{
+	if (!c || (n && (!fixA || !fixB || !xfA || !xfB || !manifolds)))
+		return fail(c, B3G_E_INVALID, "b3g_collide_pairs: null argument");
+	if (n == 0)
+		return B3G_OK;
+	CK(cudaSetDevice(c->device));
+	std::vector<std::vector<uint32_t>> lists(BK_COUNT);
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		if (fixA[i] >= c->nFixtures || fixB[i] >= c->nFixtures)
+			return fail(c, B3G_E_INVALID, "pair %u: fixture out of range", i);
+		uint32_t ta = c->hFixType[fixA[i]], tb = c->hFixType[fixB[i]];
+		uint32_t bk = BK_COUNT;
+		if (ta == B3G_SHAPE_SPHERE && tb == B3G_SHAPE_SPHERE)
+			bk = BK_SPHERES;
+		else if (ta == B3G_SHAPE_CAPSULE && tb == B3G_SHAPE_SPHERE)
+			bk = BK_CAPSULE_SPHERE;
+		else if (ta == B3G_SHAPE_CAPSULE && tb == B3G_SHAPE_CAPSULE)
+			bk = BK_CAPSULES;
+		else if (ta == B3G_SHAPE_HULL && tb == B3G_SHAPE_SPHERE)
+			bk = BK_HULL_SPHERE;
+		else if (ta == B3G_SHAPE_HULL && tb == B3G_SHAPE_CAPSULE)
+			bk = BK_HULL_CAPSULE;
+		else if (ta == B3G_SHAPE_HULL && tb == B3G_SHAPE_HULL)
+			bk = BK_HULLS;
+		if (bk == BK_COUNT)
+			return fail(c, B3G_E_INVALID, "pair %u: shape pair (%u, %u) not supported here", i, ta, tb);
+		lists[bk].push_back(i);
+	}
+	uint32_t *dA = nullptr, *dB = nullptr, *dState = nullptr, *dList = nullptr, *dCount = nullptr, *dPrevState = nullptr;
+	uint32_t* dStatus = nullptr;
+	int32_t* dPrev = nullptr;
+	uint4 *dCache = nullptr, *dCacheIn = nullptr;
+	float *dXA = nullptr, *dXB = nullptr, *dX0A = nullptr, *dX0B = nullptr;
+	DevManifold *dMan = nullptr, *dPrevMan = nullptr;
+	int rc = B3G_OK;
+	auto step = [&](cudaError_t e) {
+		if (rc == B3G_OK && e != cudaSuccess)
+			rc = fail(c, B3G_E_CUDA, "b3g_collide_pairs: %s", cudaGetErrorString(e));
+	};
+	step(dalloc(&dA, n));
+	step(dalloc(&dB, n));
+	step(dalloc(&dState, n));
+	step(dalloc(&dPrevState, n));
+	step(dalloc(&dList, n));
+	step(dalloc(&dCount, BK_COUNT));
+	step(dalloc(&dStatus, 1));
+	step(dalloc(&dPrev, n));
+	step(dalloc(&dCache, n));
+	step(dalloc(&dCacheIn, n));
+	step(dalloc(&dXA, 7 * (size_t)n));
+	step(dalloc(&dXB, 7 * (size_t)n));
+	step(dalloc(&dX0A, 7 * (size_t)n));
+	step(dalloc(&dX0B, 7 * (size_t)n));
+	step(dalloc(&dMan, n));
+	step(dalloc(&dPrevMan, 1));
+	if (rc == B3G_OK)
+	{
+		std::vector<int32_t> prev(n);
+		std::vector<uint4> cin(n);
+		for (uint32_t i = 0; i < n; ++i)
+		{
+			prev[i] = (int32_t)i;
+			cin[i] = cache4 ? make_uint4(cache4[4 * i], cache4[4 * i + 1], cache4[4 * i + 2], cache4[4 * i + 3])
+							: make_uint4(0, 1, 0, 0);
+		}
+		step(cudaMemcpy(dA, fixA, 4 * n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dB, fixB, 4 * n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dXA, xfA, 28 * (size_t)n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dXB, xfB, 28 * (size_t)n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dX0A, xf0A ? xf0A : xfA, 28 * (size_t)n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dX0B, xf0B ? xf0B : xfB, 28 * (size_t)n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dPrev, prev.data(), 4 * n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dCacheIn, cin.data(), 16 * (size_t)n, cudaMemcpyHostToDevice));
+		step(cudaMemset(dPrevState, 0, 4 * n));
+		step(cudaMemset(dStatus, 0, 4));
+	}
+	if (rc == B3G_OK)
+	{
+		NPArgs a;
+		a.S = c->scene;
+		a.pairA = dA;
+		a.pairB = dB;
+		a.cstate = dState;
+		a.cache = dCache;
+		a.man = dMan;
+		a.prevState = dPrevState; // manifold count 0: no warm start
+		a.prevCache = dCacheIn;
+		a.prevMan = dPrevMan;
+		a.prevIndex = dPrev;
+		a.status = dStatus;
+		a.warmStarting = 0;
+		a.convexCache = (c->cfg.flags & B3G_FLAG_CONVEX_CACHE) ? 1 : 0;
+		a.impN = a.impT = a.impM = nullptr;
+		a.exA = dXA;
+		a.exB = dXB;
+		a.ex0A = dX0A;
+		a.ex0B = dX0B;
+		std::vector<uint32_t> flat(n), counts(BK_COUNT, 0);
+		std::vector<uint32_t> offs(BK_COUNT, 0);
+		uint32_t o = 0;
+		for (int b = 0; b < BK_COUNT; ++b)
+		{
+			offs[b] = o;
+			counts[b] = (uint32_t)lists[b].size();
+			for (uint32_t v : lists[b])
+				flat[o++] = v;
+		}
+		step(cudaMemcpy(dList, flat.data(), 4 * n, cudaMemcpyHostToDevice));
+		step(cudaMemcpy(dCount, counts.data(), 4 * BK_COUNT, cudaMemcpyHostToDevice));
+		if (rc == B3G_OK)
+		{
+			// One launch per bucket with the list offset by the bucket start.
+			for (int b = 0; b < BK_COUNT; ++b)
+			{
+				if (!counts[b])
+					continue;
+				if (b == BK_HULLS)
+				{
+					launch_hulls(a, dList + offs[b], dCount + b, c->maxUniqueEdges, c->stream);
+				}
+				else
+				{
+					// launch_convex_buckets indexes lists by bucket * cap; give it a
+					// view where only bucket b is non-empty.
+					std::vector<uint32_t> one(BK_COUNT, 0);
+					one[b] = counts[b];
+					uint32_t* dOne = nullptr;
+					step(dalloc(&dOne, BK_COUNT));
+					step(cudaMemcpy(dOne, one.data(), 4 * BK_COUNT, cudaMemcpyHostToDevice));
+					launch_convex_buckets(a, dList + offs[b] - (size_t)b * n, dOne, n, c->stream);
+					step(cudaStreamSynchronize(c->stream));
+					dfree(dOne);
+				}
+			}
+			step(cudaStreamSynchronize(c->stream));
+			step(cudaGetLastError());
+		}
+		if (rc == B3G_OK)
+		{
+			step(cudaMemcpy(manifolds, dMan, sizeof(DevManifold) * n, cudaMemcpyDeviceToHost));
+			if (cache4)
+			{
+				std::vector<uint4> cout(n);
+				step(cudaMemcpy(cout.data(), dCache, 16 * (size_t)n, cudaMemcpyDeviceToHost));
+				for (uint32_t i = 0; i < n; ++i)
+				{
+					cache4[4 * i + 0] = cout[i].x;
+					cache4[4 * i + 1] = cout[i].y;
+					cache4[4 * i + 2] = cout[i].z;
+					cache4[4 * i + 3] = cout[i].w;
+				}
+			}
+		}
+	}
+	dfree(dA);
+	dfree(dB);
+	dfree(dState);
+	dfree(dPrevState);
+	dfree(dList);
+	dfree(dCount);
+	dfree(dStatus);
+	dfree(dPrev);
+	dfree(dCache);
+	dfree(dCacheIn);
+	dfree(dXA);
+	dfree(dXB);
+	dfree(dX0A);
+	dfree(dX0B);
+	dfree(dMan);
+	dfree(dPrevMan);
+	return rc;
+}

@@ -1,0 +1,216 @@
+// Internal state of a b3g context and the launchers shared by the .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/b3g.h"
+#include "b3g_math.cuh"
+
+// Device-side status bits (b3g_counts::status).
+#define B3G_ST_PAIR_OVERFLOW 1u
+#define B3G_ST_HASH_OVERFLOW 2u
+#define B3G_ST_POLY_OVERFLOW 4u
+#define B3G_ST_WAIT_TIMEOUT 8u
+
+// Narrowphase buckets: one per b3Contact subclass (contact.cpp:256-267).
+enum Bucket : uint32_t
+{
+	BK_SPHERES = 0,      // b3SphereContact
+	BK_CAPSULE_SPHERE,   // b3CapsuleAndSphereContact
+	BK_CAPSULES,         // b3CapsuleContact
+	BK_TRIANGLE_SPHERE,  // b3TriangleAndSphereContact
+	BK_TRIANGLE_CAPSULE, // b3TriangleAndCapsuleContact
+	BK_HULL_SPHERE,      // b3HullAndSphereContact
+	BK_HULL_CAPSULE,     // b3HullAndCapsuleContact
+	BK_HULL_TRIANGLE,    // b3HullAndTriangleContact
+	BK_HULLS,            // b3HullContact
+	BK_SENSOR,           // any pair with a sensor: b3Contact::TestOverlap path
+	BK_INACTIVE,         // both bodies asleep or static: state carried over
+	BK_COUNT
+};
+
+// b3Manifold / b3ManifoldPoint, byte-identical to the reference layout
+// (collision.h:66-128; 72 and 320 bytes).
+struct alignas(8) DevPoint
+{
+	float n[3];
+	float p1[3];
+	float p2[3];
+	float normalImpulse;
+	uint32_t triangleKey;
+	uint32_t pad0;
+	uint32_t key[4];
+	uint8_t persisting;
+	uint8_t edgeContact;
+	uint8_t pad1[6];
+};
+static_assert(sizeof(DevPoint) == 72, "b3ManifoldPoint layout");
+
+struct alignas(8) DevManifold
+{
+	DevPoint points[4];
+	uint32_t pointCount;
+	float tangentImpulse[2];
+	float motorImpulse;
+	float motorSpeed;
+	float tangentSpeed1;
+	float tangentSpeed2;
+	uint32_t pad;
+};
+static_assert(sizeof(DevManifold) == 320, "b3Manifold layout");
+
+struct HullDesc
+{
+	uint32_t vOff, vCnt, eOff, eCnt, fOff, fCnt;
+	float cx, cy, cz;
+	uint32_t pad[3];
+};
+static_assert(sizeof(HullDesc) == 48, "HullDesc");
+
+// Scene and per-pass device buffers.
+struct DevScene
+{
+	// hulls
+	const HullDesc* hulls;
+	const float4* hverts;  // xyz
+	const uint4* hedges;   // origin, face, prev, next (twin = i ^ 1)
+	const uint32_t* hfaces;
+	const float4* hplanes; // normal, offset
+
+	// bodies
+	const uint32_t* bodyWorld;
+	const uint32_t* bodyType;
+	const uint8_t* bodyAwake;
+	const float* bodyState; // 17 floats per body
+
+	// fixtures
+	const uint32_t* fixBody;
+	const uint32_t* fixType;
+	const uint32_t* fixHull;
+	const float4* fixParams; // 3 float4 per fixture
+	const uint32_t* fixFlags;
+	const uint32_t* fixKey;
+};
+
+struct Buffers
+{
+	// broadphase, per proxy
+	float4* fatLo;
+	float4* fatHi;
+	uint8_t* moved;
+	unsigned long long* keysA;
+	unsigned long long* keysB;
+	uint32_t* valsA;
+	uint32_t* valsB;
+	uint32_t* sortHist;
+	float* sceneBounds; // 6 floats (ordered-int encoded during reduction)
+	// LBVH: internal nodes [0, n-1), leaves [n-1, 2n-1)
+	float4* nodeLo;
+	float4* nodeHi;
+	uint32_t* nodeLeft;   // internal: left child node; leaf: proxy index
+	uint32_t* nodeRight;  // internal: right child node
+	uint32_t* nodeRope;
+	uint32_t* nodeFirst;  // first sorted leaf of the node's range
+	uint32_t* nodeParent;
+	uint32_t* nodeEnd;    // internal: last sorted leaf of the range
+	uint32_t* splitRight; // right child of the internal node whose split is i
+	uint32_t* refitFlag;
+	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
+	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
+	uint32_t* scanAux;
+
+	// contacts, double-buffered [cur], [prev]
+	uint32_t* pairA[2];
+	uint32_t* pairB[2];
+	uint32_t* cstate[2]; // bit0 touching, bits 8-15 manifold count, bit 16 begun
+	uint4* cache[2];
+	DevManifold* man[2];
+	int32_t* prevIndex; // per current contact
+	uint32_t* prevFound; // per previous contact
+	unsigned long long* hashKeys[2];
+	uint32_t* hashVals[2];
+	uint32_t hashCap;
+
+	// narrowphase work lists
+	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
+	uint32_t* counters;   // device counters (see CTR_*)
+	uint32_t* endedList;  // 3 u32 per ended contact
+	uint32_t* touchIndex;
+	DevManifold* touchMan;
+	uint32_t* contactOut; // 3 u32 per contact: A, B, flags
+
+	// warm start from the host solver
+	float* impulseNormal;
+	float* impulseTangent;
+	float* impulseMotor;
+};
+
+// Counter slots in Buffers::counters.
+enum
+{
+	CTR_PAIRS = 0,      // contacts this pass
+	CTR_PREV_PAIRS,     // contacts of the previous pass
+	CTR_BEGUN,
+	CTR_ENDED,
+	CTR_TOUCHING,
+	CTR_MANIFOLDS,
+	CTR_POINTS,
+	CTR_MOVED,
+	CTR_STATUS,
+	CTR_TOUCH_OUT,
+	CTR_BUCKET0 = 16,   // BK_COUNT bucket sizes
+	CTR_COUNT = 32
+};
+
+struct b3g_ctx
+{
+	b3g_config cfg;
+	int device;
+	cudaStream_t stream;
+	std::string err;
+
+	uint32_t nHulls, nBodies, nFixtures, nWorlds;
+	uint32_t hullVerts, hullEdges, hullFaces;
+	uint32_t maxUniqueEdges; // unique edges (half-edge pairs) of the largest hull
+	uint32_t cur; // index of the current contact buffer
+	bool creationPass;
+	bool havePass;
+	bool impulsesLoaded;
+
+	DevScene scene;
+	Buffers buf;
+
+	// owned scene allocations
+	HullDesc* dHulls;
+	float4* dHverts;
+	uint4* dHedges;
+	uint32_t* dHfaces;
+	float4* dHplanes;
+	uint32_t *dBodyWorld, *dBodyType;
+	uint8_t* dBodyAwake;
+	float* dBodyState;
+	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey;
+	float4* dFixParams;
+
+	// pinned host staging
+	uint32_t* hCounters;
+
+	// host copies of fixture types (for the stand-alone narrowphase)
+	std::vector<uint32_t> hFixType;
+};
+
+// Launchers (defined in the .cu files).
+void launch_sync(b3g_ctx* c, cudaStream_t s);
+void launch_broadphase(b3g_ctx* c, cudaStream_t s);
+void launch_pairs_diff(b3g_ctx* c, cudaStream_t s);
+void launch_narrowphase(b3g_ctx* c, cudaStream_t s);
+void launch_finalize(b3g_ctx* c, cudaStream_t s);
+void launch_collide_pairs(b3g_ctx* c, cudaStream_t s, uint32_t n, const uint32_t* fixA,
+	const uint32_t* fixB, const float* xfA, const float* xfB, const float* xf0A,
+	const float* xf0B, uint4* cache, DevManifold* out);
+
+// Grid size for grid-stride loops over device-side counts.
+inline int persistent_blocks(int perSM = 8) { return 148 * perSM; }

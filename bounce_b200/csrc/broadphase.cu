@@ -1,0 +1,726 @@
+// Fat-AABB update and broadphase of one collision pass.
+//
+//  k_sync        per proxy: swept AABB of the fixture over [xf0, xf1] and the
+//                b3DynamicTree::MoveProxy keep-or-reinsert rule
+//                (fixture.cpp:120-132, dynamic_tree.cpp:139-207), or the
+//                CreateProxy fattening on a creation pass (dynamic_tree.cpp:108-128)
+//  k_bounds / k_morton / radix sort
+//                world-major 64-bit keys: world index << 32 | 30-bit Morton code
+//                of the fat-AABB centre, sorted by an LSD radix sort
+//  k_build       Karras (2012) radix tree over the sorted keys, with ropes
+//                (the next node in depth-first order after a subtree)
+//  k_refit       bottom-up node AABBs
+//  k_traverse    stackless rope traversal from each leaf's own rope, which
+//                visits exactly the leaves after it in sorted order, so each
+//                overlapping pair is met once; the AddPair filters
+//                (contact_manager.cpp:98-160) and the b3Contact::Create A/B
+//                order (contact.cpp:290-322) are applied per pair
+//
+// The overlap set found this way equals the reference's contact set after
+// FindNewContacts: a contact exists iff its fat AABBs overlap (pairs are
+// created when either proxy moves and destroyed by UpdateContacts once the
+// fat AABBs separate, contact_manager.cpp:270-281).
+
+#include "b3g_internal.cuh"
+
+namespace {
+
+constexpr uint32_t SENT = 0xFFFFFFFFu;
+
+__device__ __forceinline__ XF load_xf(const float* s)
+{
+	XF x;
+	x.p = V3{s[0], s[1], s[2]};
+	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	return x;
+}
+
+// b3Shape::ComputeAABB for one transform (hull_shape.cpp:160-164,
+// sphere_shape.cpp:51-57, capsule_shape.cpp:124-131, triangle_shape.cpp:59-67).
+// Two transforms are handled in one vertex loop for hulls.
+__device__ void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb,
+	bool two, AABB& a, AABB& b)
+{
+	uint32_t type = S.fixType[fix];
+	float4 p0 = S.fixParams[3 * fix + 0];
+	float4 p1 = S.fixParams[3 * fix + 1];
+	float4 p2 = S.fixParams[3 * fix + 2];
+	if (type == B3G_SHAPE_SPHERE)
+	{
+		V3 c = V3{p0.x, p0.y, p0.z};
+		float r = p0.w;
+		V3 rv = V3{r, r, r};
+		V3 ca = xmul(xa, c);
+		a.lo = ca - rv;
+		a.hi = ca + rv;
+		if (two)
+		{
+			V3 cb = xmul(xb, c);
+			b.lo = cb - rv;
+			b.hi = cb + rv;
+		}
+	}
+	else if (type == B3G_SHAPE_CAPSULE)
+	{
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		float r = p1.z;
+		V3 rv = V3{r, r, r};
+		V3 c1 = xmul(xa, v1), c2 = xmul(xa, v2);
+		a.lo = vmin(c1, c2) - rv;
+		a.hi = vmax(c1, c2) + rv;
+		if (two)
+		{
+			c1 = xmul(xb, v1);
+			c2 = xmul(xb, v2);
+			b.lo = vmin(c1, c2) - rv;
+			b.hi = vmax(c1, c2) + rv;
+		}
+	}
+	else if (type == B3G_SHAPE_TRIANGLE)
+	{
+		// The reference ignores the transform here (triangle_shape.cpp:59-67).
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		V3 v3_ = V3{p1.z, p1.w, p2.x};
+		float r = p2.y;
+		V3 rv = V3{r, r, r};
+		a.lo = vmin(v1, vmin(v2, v3_)) - rv;
+		a.hi = vmax(v1, vmax(v2, v3_)) + rv;
+		b = a;
+	}
+	else // hull
+	{
+		const HullDesc h = S.hulls[S.fixHull[fix]];
+		const float4* hv = S.hverts + h.vOff;
+		float4 w = hv[0];
+		V3 v = V3{w.x, w.y, w.z};
+		V3 ta = xmul(xa, v);
+		a.lo = ta;
+		a.hi = ta;
+		V3 tb;
+		if (two)
+		{
+			tb = xmul(xb, v);
+			b.lo = tb;
+			b.hi = tb;
+		}
+		for (uint32_t i = 1; i < h.vCnt; ++i)
+		{
+			w = hv[i];
+			v = V3{w.x, w.y, w.z};
+			ta = xmul(xa, v);
+			a.lo = vmin(a.lo, ta);
+			a.hi = vmax(a.hi, ta);
+			if (two)
+			{
+				tb = xmul(xb, v);
+				b.lo = vmin(b.lo, tb);
+				b.hi = vmax(b.hi, tb);
+			}
+		}
+		float r = p0.x;
+		aabb_extend(a, r);
+		if (two)
+			aabb_extend(b, r);
+	}
+}
+
+__global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= nf)
+		return;
+	uint32_t body = S.fixBody[i];
+	const float* st = S.bodyState + 17 * (size_t)body;
+	XF xf1 = load_xf(st);
+	if (creation)
+	{
+		// b3DynamicTree::CreateProxy (dynamic_tree.cpp:108-128).
+		AABB a, unused;
+		compute_aabbs(S, i, xf1, xf1, false, a, unused);
+		V3 r = V3{B3G_AABB_EXTENSION, B3G_AABB_EXTENSION, B3G_AABB_EXTENSION};
+		V3 lo = a.lo - r, hi = a.hi + r;
+		B.fatLo[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+		B.fatHi[i] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+		B.moved[i] = 1;
+		return;
+	}
+	uint32_t btype = S.bodyType[body];
+	if (btype == B3G_BODY_STATIC || S.bodyAwake[body] == 0)
+	{
+		// Not in an island: not synchronised (world.cpp:427-442).
+		B.moved[i] = 0;
+		return;
+	}
+	// b3Body::SynchronizeFixtures (body.cpp:216-229): xf0 from the sweep start.
+	XF xf0;
+	xf0.q = Q4{V3{st[10], st[11], st[12]}, st[13]};
+	V3 c0 = V3{st[7], st[8], st[9]};
+	V3 lc = V3{st[14], st[15], st[16]};
+	xf0.p = c0 - rot(xf0.q, lc);
+
+	// b3Fixture::Synchronize (fixture.cpp:120-132).
+	AABB a1, a2;
+	compute_aabbs(S, i, xf0, xf1, true, a1, a2);
+	AABB aabb;
+	aabb.lo = vmin(a1.lo, a2.lo);
+	aabb.hi = vmax(a1.hi, a2.hi);
+	V3 disp = aabb_center(a2) - aabb_center(a1);
+
+	// b3DynamicTree::MoveProxy (dynamic_tree.cpp:139-207).
+	AABB fat = aabb;
+	aabb_extend(fat, B3G_AABB_EXTENSION);
+	V3 d = B3G_AABB_MULTIPLIER * disp;
+	if (d.x < 0.0f)
+		fat.lo.x += d.x;
+	else
+		fat.hi.x += d.x;
+	if (d.y < 0.0f)
+		fat.lo.y += d.y;
+	else
+		fat.hi.y += d.y;
+	if (d.z < 0.0f)
+		fat.lo.z += d.z;
+	else
+		fat.hi.z += d.z;
+
+	float4 tl = B.fatLo[i], th = B.fatHi[i];
+	AABB tree;
+	tree.lo = V3{tl.x, tl.y, tl.z};
+	tree.hi = V3{th.x, th.y, th.z};
+	if (aabb_contains(tree, aabb))
+	{
+		AABB huge = fat;
+		aabb_extend(huge, 4.0f * B3G_AABB_EXTENSION);
+		if (aabb_contains(huge, tree))
+		{
+			B.moved[i] = 0;
+			return;
+		}
+	}
+	B.fatLo[i] = make_float4(fat.lo.x, fat.lo.y, fat.lo.z, 0.0f);
+	B.fatHi[i] = make_float4(fat.hi.x, fat.hi.y, fat.hi.z, 0.0f);
+	B.moved[i] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// Scene bounds of the fat-AABB centres (for Morton quantisation).
+
+__device__ __forceinline__ int f2o(float f)
+{
+	int i = __float_as_int(f);
+	return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float o2f(int i)
+{
+	return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF);
+}
+
+__global__ void k_bounds_init(int* bnd)
+{
+	if (threadIdx.x < 3)
+		bnd[threadIdx.x] = 0x7FFFFFFF;
+	else if (threadIdx.x < 6)
+		bnd[threadIdx.x] = (int)0x80000000;
+}
+
+__global__ void k_bounds(Buffers B, uint32_t n, int* bnd)
+{
+	__shared__ int s[6][8];
+	float mn[3] = {B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR};
+	float mx[3] = {-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR};
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		float4 lo = B.fatLo[i], hi = B.fatHi[i];
+		float c[3] = {0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z)};
+		for (int k = 0; k < 3; ++k)
+		{
+			mn[k] = fminf(mn[k], c[k]);
+			mx[k] = fmaxf(mx[k], c[k]);
+		}
+	}
+	for (int k = 0; k < 3; ++k)
+	{
+		for (int o = 16; o > 0; o >>= 1)
+		{
+			mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+			mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+		}
+	}
+	int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
+	{
+		for (int k = 0; k < 3; ++k)
+		{
+			s[k][warp] = f2o(mn[k]);
+			s[3 + k][warp] = f2o(mx[k]);
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x < 6)
+	{
+		int nw = blockDim.x >> 5;
+		int v = s[threadIdx.x][0];
+		for (int w = 1; w < nw; ++w)
+			v = threadIdx.x < 3 ? min(v, s[threadIdx.x][w]) : max(v, s[threadIdx.x][w]);
+		if (threadIdx.x < 3)
+			atomicMin(bnd + threadIdx.x, v);
+		else
+			atomicMax(bnd + threadIdx.x, v);
+	}
+}
+
+__device__ __forceinline__ uint32_t expand10(uint32_t v)
+{
+	v = (v * 0x00010001u) & 0xFF0000FFu;
+	v = (v * 0x00000101u) & 0x0F00F00Fu;
+	v = (v * 0x00000011u) & 0xC30C30C3u;
+	v = (v * 0x00000005u) & 0x49249249u;
+	return v;
+}
+
+__global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	float lo[3] = {o2f(bnd[0]), o2f(bnd[1]), o2f(bnd[2])};
+	float hi[3] = {o2f(bnd[3]), o2f(bnd[4]), o2f(bnd[5])};
+	float4 a = B.fatLo[i], b = B.fatHi[i];
+	float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+	uint32_t q[3];
+	for (int k = 0; k < 3; ++k)
+	{
+		float ext = hi[k] - lo[k];
+		float t = ext > 0.0f ? (c[k] - lo[k]) / ext : 0.0f;
+		t = fminf(fmaxf(t, 0.0f), 1.0f);
+		q[k] = min((uint32_t)(t * 1024.0f), 1023u);
+	}
+	uint32_t code = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+	uint32_t world = S.bodyWorld[S.fixBody[i]];
+	B.keysA[i] = ((unsigned long long)world << 32) | code;
+	B.valsA[i] = i;
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort of (u64 key, u32 value), 8-bit digits, stable.
+// Tiles of 4096 elements (256 threads x 16). Per pass: per-tile digit
+// histograms, one exclusive scan in digit-major order, and a stable scatter
+// that ranks equal digits within a warp with __match_any_sync and across the
+// warps of a round through shared-memory prefix sums.
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+
+__global__ void k_rs_hist(const unsigned long long* keys, uint32_t n, int shift, uint32_t* hist,
+	uint32_t numTiles)
+{
+	__shared__ uint32_t h[256];
+	h[threadIdx.x] = 0;
+	__syncthreads();
+	uint32_t base = blockIdx.x * RS_TILE;
+	for (int k = 0; k < RS_ITEMS; ++k)
+	{
+		uint32_t idx = base + k * RS_THREADS + threadIdx.x;
+		if (idx < n)
+			atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 0xFFu], 1u);
+	}
+	__syncthreads();
+	hist[threadIdx.x * numTiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Single-block exclusive scan of m entries (m <= 1024 * per-thread chunk).
+__global__ void k_scan_single(uint32_t* data, uint32_t m, uint32_t* total)
+{
+	__shared__ uint32_t s[1024];
+	uint32_t per = (m + blockDim.x - 1) / blockDim.x;
+	uint32_t beg = threadIdx.x * per;
+	uint32_t end = min(beg + per, m);
+	uint32_t sum = 0;
+	for (uint32_t i = beg; i < end; ++i)
+		sum += data[i];
+	s[threadIdx.x] = sum;
+	__syncthreads();
+	for (uint32_t off = 1; off < blockDim.x; off <<= 1)
+	{
+		uint32_t v = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+		__syncthreads();
+		s[threadIdx.x] += v;
+		__syncthreads();
+	}
+	uint32_t run = s[threadIdx.x] - sum;
+	for (uint32_t i = beg; i < end; ++i)
+	{
+		uint32_t v = data[i];
+		data[i] = run;
+		run += v;
+	}
+	if (total && threadIdx.x == blockDim.x - 1)
+		*total = s[threadIdx.x];
+}
+
+__global__ void k_rs_scatter(const unsigned long long* kin, const uint32_t* vin,
+	unsigned long long* kout, uint32_t* vout, uint32_t n, int shift, const uint32_t* hist,
+	uint32_t numTiles)
+{
+	__shared__ uint32_t base[256];
+	__shared__ uint32_t run[256];
+	__shared__ uint32_t wc[RS_THREADS / 32][256];
+	const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+	base[t] = hist[t * numTiles + blockIdx.x];
+	run[t] = 0;
+	for (int w = 0; w < RS_THREADS / 32; ++w)
+		wc[w][t] = 0;
+	__syncthreads();
+	const uint32_t lt = (1u << lane) - 1u;
+	uint32_t tile = blockIdx.x * RS_TILE;
+	for (int r = 0; r < RS_ITEMS; ++r)
+	{
+		uint32_t idx = tile + r * RS_THREADS + t;
+		bool valid = idx < n;
+		unsigned long long key = valid ? kin[idx] : 0ull;
+		uint32_t val = valid ? vin[idx] : 0u;
+		uint32_t d = valid ? ((uint32_t)(key >> shift) & 0xFFu) : 0x100u;
+		uint32_t peers = __match_any_sync(0xffffffffu, d);
+		uint32_t rank = __popc(peers & lt);
+		if (valid && rank == 0)
+			wc[warp][d] = __popc(peers);
+		__syncthreads();
+		{
+			uint32_t sum = run[t];
+			for (int w = 0; w < RS_THREADS / 32; ++w)
+			{
+				uint32_t c = wc[w][t];
+				wc[w][t] = sum;
+				sum += c;
+			}
+			run[t] = sum;
+		}
+		__syncthreads();
+		if (valid)
+		{
+			uint32_t pos = base[d] + wc[warp][d] + rank;
+			kout[pos] = key;
+			vout[pos] = val;
+		}
+		__syncthreads();
+		for (int w = 0; w < RS_THREADS / 32; ++w)
+			wc[w][t] = 0;
+		__syncthreads();
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Karras radix tree.
+
+__device__ __forceinline__ int delta(const unsigned long long* k, int n, int i, int j)
+{
+	if (j < 0 || j >= n)
+		return -1;
+	unsigned long long a = k[i], b = k[j];
+	if (a == b)
+		return 64 + __clz((uint32_t)i ^ (uint32_t)j);
+	return __clzll(a ^ b);
+}
+
+__global__ void k_build(Buffers B, int n)
+{
+	int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n - 1)
+		return;
+	const unsigned long long* k = B.keysA;
+	int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+	int dmin = delta(k, n, i, i - d);
+	int lmax = 2;
+	while (delta(k, n, i, i + lmax * d) > dmin)
+		lmax <<= 1;
+	int l = 0;
+	for (int t = lmax >> 1; t >= 1; t >>= 1)
+		if (delta(k, n, i, i + (l + t) * d) > dmin)
+			l += t;
+	int j = i + l * d;
+	int dnode = delta(k, n, i, j);
+	int s = 0;
+	int t = l;
+	do
+	{
+		t = (t + 1) >> 1;
+		if (delta(k, n, i, i + (s + t) * d) > dnode)
+			s += t;
+	} while (t > 1);
+	int gamma = i + s * d + min(d, 0);
+	int first = min(i, j), last = max(i, j);
+	uint32_t left = (first == gamma) ? (uint32_t)(n - 1 + gamma) : (uint32_t)gamma;
+	uint32_t right = (last == gamma + 1) ? (uint32_t)(n - 1 + gamma + 1) : (uint32_t)(gamma + 1);
+	B.nodeLeft[i] = left;
+	B.nodeRight[i] = right;
+	B.nodeParent[left] = i;
+	B.nodeParent[right] = i;
+	B.nodeFirst[i] = first;
+	B.nodeEnd[i] = last;
+	B.splitRight[gamma] = right;
+}
+
+__global__ void k_leaves(DevScene S, Buffers B, int n)
+{
+	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n)
+		return;
+	uint32_t node = n - 1 + j;
+	uint32_t proxy = B.valsA[j];
+	B.nodeLeft[node] = proxy;
+	B.nodeFirst[node] = j;
+	B.nodeLo[node] = B.fatLo[proxy];
+	B.nodeHi[node] = B.fatHi[proxy];
+	B.nodeRope[node] = (j == n - 1) ? SENT : B.splitRight[j];
+	if (j < n - 1)
+	{
+		B.nodeRope[j] = (B.nodeEnd[j] == (uint32_t)(n - 1)) ? SENT : B.splitRight[B.nodeEnd[j]];
+		B.refitFlag[j] = 0;
+	}
+	// Last sorted leaf of each world.
+	uint32_t w = S.bodyWorld[S.fixBody[proxy]];
+	if (j == n - 1 || S.bodyWorld[S.fixBody[B.valsA[j + 1]]] != w)
+		B.worldEnd[w] = j;
+}
+
+__global__ void k_refit(Buffers B, int n)
+{
+	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n || n < 2)
+		return;
+	uint32_t node = n - 1 + j;
+	uint32_t p = B.nodeParent[node];
+	while (true)
+	{
+		__threadfence();
+		uint32_t old = atomicAdd(&B.refitFlag[p], 1u);
+		if (old == 0)
+			return;
+		__threadfence();
+		uint32_t l = B.nodeLeft[p], r = B.nodeRight[p];
+		float4 al = __ldcg(&B.nodeLo[l]), ah = __ldcg(&B.nodeHi[l]);
+		float4 bl = __ldcg(&B.nodeLo[r]), bh = __ldcg(&B.nodeHi[r]);
+		B.nodeLo[p] = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
+		B.nodeHi[p] = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+		if (p == 0)
+			return;
+		p = B.nodeParent[p];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Pair search.
+
+// b3Contact::s_registers (contact.cpp:253-288): registered type pairs, and
+// whether (t1, t2) is the primary order (fixture A keeps type t1).
+__device__ __forceinline__ bool registered(uint32_t a, uint32_t b)
+{
+	// bit (a * 5 + b)
+	const uint32_t mask =
+		(1u << (0 * 5 + 0)) | (1u << (1 * 5 + 0)) | (1u << (0 * 5 + 1)) | (1u << (1 * 5 + 1)) |
+		(1u << (2 * 5 + 0)) | (1u << (0 * 5 + 2)) | (1u << (2 * 5 + 1)) | (1u << (1 * 5 + 2)) |
+		(1u << (3 * 5 + 0)) | (1u << (0 * 5 + 3)) | (1u << (3 * 5 + 1)) | (1u << (1 * 5 + 3)) |
+		(1u << (3 * 5 + 2)) | (1u << (2 * 5 + 3)) | (1u << (3 * 5 + 3)) |
+		(1u << (3 * 5 + 4)) | (1u << (4 * 5 + 3)) | (1u << (4 * 5 + 0)) | (1u << (0 * 5 + 4)) |
+		(1u << (4 * 5 + 1)) | (1u << (1 * 5 + 4));
+	return (mask >> (a * 5 + b)) & 1u;
+}
+__device__ __forceinline__ bool primary(uint32_t a, uint32_t b)
+{
+	const uint32_t mask = (1u << (0 * 5 + 0)) | (1u << (1 * 5 + 0)) | (1u << (1 * 5 + 1)) |
+		(1u << (2 * 5 + 0)) | (1u << (2 * 5 + 1)) | (1u << (3 * 5 + 0)) | (1u << (3 * 5 + 1)) |
+		(1u << (3 * 5 + 2)) | (1u << (3 * 5 + 3)) | (1u << (3 * 5 + 4)) | (1u << (4 * 5 + 0)) |
+		(1u << (4 * 5 + 1));
+	return (mask >> (a * 5 + b)) & 1u;
+}
+
+// AddPair filters: same body (contact_manager.cpp:104-108), b3Body::ShouldCollide
+// (at least one dynamic body, body.cpp:240-246) and a registered shape pair
+// (b3Contact::Create returns nullptr otherwise, contact.cpp:318-321).
+__device__ __forceinline__ bool pair_filter(const DevScene& S, uint32_t pa, uint32_t pb)
+{
+	uint32_t ba = S.fixBody[pa], bb = S.fixBody[pb];
+	if (ba == bb)
+		return false;
+	if (S.bodyType[ba] != B3G_BODY_DYNAMIC && S.bodyType[bb] != B3G_BODY_DYNAMIC)
+		return false;
+	return registered(S.fixType[pa], S.fixType[pb]);
+}
+
+template <bool WRITE>
+__global__ void k_traverse(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
+{
+	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n)
+		return;
+	uint32_t leaf = n - 1 + j;
+	uint32_t pa = B.nodeLeft[leaf];
+	float4 ql = B.nodeLo[leaf], qh = B.nodeHi[leaf];
+	AABB q;
+	q.lo = V3{ql.x, ql.y, ql.z};
+	q.hi = V3{qh.x, qh.y, qh.z};
+	uint32_t wend = B.worldEnd[S.bodyWorld[S.fixBody[pa]]];
+	uint32_t count = 0;
+	uint32_t base = WRITE ? B.leafCount[j] : 0;
+	uint32_t node = B.nodeRope[leaf];
+	uint32_t keyA = S.fixKey[pa];
+	while (node != SENT)
+	{
+		if (B.nodeFirst[node] > wend)
+			break;
+		float4 lo = B.nodeLo[node], hi = B.nodeHi[node];
+		AABB nb;
+		nb.lo = V3{lo.x, lo.y, lo.z};
+		nb.hi = V3{hi.x, hi.y, hi.z};
+		if (aabb_overlap(nb, q))
+		{
+			if (node >= (uint32_t)(n - 1))
+			{
+				uint32_t pb = B.nodeLeft[node];
+				if (pair_filter(S, pa, pb))
+				{
+					if (WRITE)
+					{
+						uint32_t slot = base + count;
+						if (slot < cap)
+						{
+							// Broadphase order (min, max) of proxy ids, then the
+							// factory's primary-type swap.
+							uint32_t keyB = S.fixKey[pb];
+							uint32_t f1 = keyA < keyB ? pa : pb;
+							uint32_t f2 = keyA < keyB ? pb : pa;
+							uint32_t A = f1, Bf = f2;
+							if (!primary(S.fixType[f1], S.fixType[f2]))
+							{
+								A = f2;
+								Bf = f1;
+							}
+							B.pairA[cur][slot] = A;
+							B.pairB[cur][slot] = Bf;
+						}
+					}
+					++count;
+				}
+				node = B.nodeRope[node];
+			}
+			else
+			{
+				node = B.nodeLeft[node];
+			}
+		}
+		else
+		{
+			node = B.nodeRope[node];
+		}
+	}
+	if (!WRITE)
+		B.leafCount[j] = count;
+}
+
+// Multi-block exclusive scan of u32 (in place) with the total written to *total.
+constexpr int SCAN_BLOCK = 1024;
+
+__global__ void k_scan_blocks(uint32_t* data, uint32_t n, uint32_t* blockSums)
+{
+	__shared__ uint32_t s[SCAN_BLOCK];
+	uint32_t i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+	uint32_t v = i < n ? data[i] : 0;
+	s[threadIdx.x] = v;
+	__syncthreads();
+	for (uint32_t off = 1; off < SCAN_BLOCK; off <<= 1)
+	{
+		uint32_t a = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+		__syncthreads();
+		s[threadIdx.x] += a;
+		__syncthreads();
+	}
+	if (i < n)
+		data[i] = s[threadIdx.x] - v;
+	if (threadIdx.x == SCAN_BLOCK - 1)
+		blockSums[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void k_scan_add(uint32_t* data, uint32_t n, const uint32_t* blockSums)
+{
+	uint32_t i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+	if (i < n)
+		data[i] += blockSums[blockIdx.x];
+}
+
+} // namespace
+
+void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s)
+{
+	uint32_t blocks = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+	if (blocks == 0)
+	{
+		cudaMemsetAsync(total, 0, sizeof(uint32_t), s);
+		return;
+	}
+	k_scan_blocks<<<blocks, SCAN_BLOCK, 0, s>>>(data, n, aux);
+	k_scan_single<<<1, 1024, 0, s>>>(aux, blocks, total);
+	k_scan_add<<<blocks, SCAN_BLOCK, 0, s>>>(data, n, aux);
+}
+
+void launch_sync(b3g_ctx* c, cudaStream_t s)
+{
+	uint32_t n = c->nFixtures;
+	if (n == 0)
+		return;
+	k_sync<<<(n + 127) / 128, 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
+}
+
+void launch_broadphase(b3g_ctx* c, cudaStream_t s)
+{
+	Buffers& B = c->buf;
+	int n = (int)c->nFixtures;
+	uint32_t cur = c->cur;
+	if (n == 0)
+	{
+		cudaMemsetAsync(B.counters + CTR_PAIRS, 0, sizeof(uint32_t), s);
+		return;
+	}
+	int* bnd = (int*)B.sceneBounds;
+	k_bounds_init<<<1, 32, 0, s>>>(bnd);
+	k_bounds<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(B, (uint32_t)n, bnd);
+	k_morton<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
+
+	// Radix sort over the Morton bits and, for several worlds, the world bits.
+	uint32_t numTiles = (n + RS_TILE - 1) / RS_TILE;
+	int shifts[8];
+	int ns = 0;
+	for (int sft = 0; sft < 32; sft += 8)
+		shifts[ns++] = sft;
+	uint32_t wb = 0;
+	while ((1u << wb) < c->nWorlds)
+		++wb;
+	for (uint32_t sft = 0; sft < wb; sft += 8)
+		shifts[ns++] = 32 + (int)sft;
+	unsigned long long *kin = B.keysA, *kout = B.keysB;
+	uint32_t *vin = B.valsA, *vout = B.valsB;
+	for (int p = 0; p < ns; ++p)
+	{
+		k_rs_hist<<<numTiles, RS_THREADS, 0, s>>>(kin, n, shifts[p], B.sortHist, numTiles);
+		k_scan_single<<<1, 1024, 0, s>>>(B.sortHist, 256 * numTiles, nullptr);
+		k_rs_scatter<<<numTiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shifts[p], B.sortHist, numTiles);
+		std::swap(kin, kout);
+		std::swap(vin, vout);
+	}
+	if (kin != B.keysA)
+	{
+		cudaMemcpyAsync(B.keysA, kin, sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, s);
+		cudaMemcpyAsync(B.valsA, vin, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s);
+	}
+
+	if (n > 1)
+		k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(B, n);
+	k_leaves<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, n);
+	k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
+
+	k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_PAIRS, s);
+	k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+}

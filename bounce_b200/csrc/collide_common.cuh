@@ -1,0 +1,617 @@
+// Shared narrowphase pieces: hull accessors, clipping (clip.cpp), manifold
+// initialisation and warm-start matching (collision.cpp:23-61, contact.cpp:399-501).
+#pragma once
+
+#include "b3g_internal.cuh"
+#include "gjk.cuh"
+
+#define B3G_NULL_EDGE 0xFFFFFFFFu
+#define B3G_NULL_TRIANGLE 0xFFFFFFFFu
+#define B3G_MAX_POLY 64 // b3StackArray<b3ClipVertex, 32> grows; 64 bounds every hull here
+
+struct HullRef
+{
+	const float4* v;
+	const uint4* e; // origin, face, prev, next; twin = i ^ 1
+	const uint32_t* f;
+	const float4* p;
+	uint32_t vCnt, eCnt, fCnt;
+	V3 centroid;
+};
+
+__device__ __forceinline__ HullRef hull_ref(const DevScene& S, uint32_t h)
+{
+	HullDesc d = S.hulls[h];
+	HullRef r;
+	r.v = S.hverts + d.vOff;
+	r.e = S.hedges + d.eOff;
+	r.f = S.hfaces + d.fOff;
+	r.p = S.hplanes + d.fOff;
+	r.vCnt = d.vCnt;
+	r.eCnt = d.eCnt;
+	r.fCnt = d.fCnt;
+	r.centroid = V3{d.cx, d.cy, d.cz};
+	return r;
+}
+
+__device__ __forceinline__ V3 hv(const HullRef& h, uint32_t i)
+{
+	float4 w = h.v[i];
+	return V3{w.x, w.y, w.z};
+}
+__device__ __forceinline__ PL hp(const HullRef& h, uint32_t i)
+{
+	float4 w = h.p[i];
+	return PL{V3{w.x, w.y, w.z}, w.w};
+}
+__device__ __forceinline__ uint32_t he_origin(const HullRef& h, uint32_t i) { return h.e[i].x; }
+__device__ __forceinline__ uint32_t he_face(const HullRef& h, uint32_t i) { return h.e[i].y; }
+__device__ __forceinline__ uint32_t he_prev(const HullRef& h, uint32_t i) { return h.e[i].z; }
+__device__ __forceinline__ uint32_t he_next(const HullRef& h, uint32_t i) { return h.e[i].w; }
+
+// b3Hull::GetSupportVertex (hull.h:105-119): first maximum.
+__device__ __forceinline__ uint32_t hull_support_vertex(const HullRef& h, V3 d)
+{
+	uint32_t maxIndex = 0;
+	float maxProj = dot(d, hv(h, 0));
+	for (uint32_t i = 1; i < h.vCnt; ++i)
+	{
+		float proj = dot(d, hv(h, i));
+		if (proj > maxProj)
+		{
+			maxIndex = i;
+			maxProj = proj;
+		}
+	}
+	return maxIndex;
+}
+
+// b3Hull::GetSupportFace (hull.h:121-135).
+__device__ __forceinline__ uint32_t hull_support_face(const HullRef& h, V3 d)
+{
+	uint32_t maxIndex = 0;
+	float maxProj = dot(d, hp(h, 0).n);
+	for (uint32_t i = 1; i < h.fCnt; ++i)
+	{
+		float proj = dot(d, hp(h, i).n);
+		if (proj > maxProj)
+		{
+			maxIndex = i;
+			maxProj = proj;
+		}
+	}
+	return maxIndex;
+}
+
+// b3Hull::GetEdgeSidePlane (hull.h:137-152).
+__device__ __forceinline__ PL hull_edge_side_plane(const HullRef& h, uint32_t index)
+{
+	uint4 e = h.e[index];
+	uint32_t twinOrigin = h.e[index ^ 1u].x;
+	PL face = hp(h, e.y);
+	V3 P = hv(h, e.x);
+	V3 Q = hv(h, twinOrigin);
+	V3 E = Q - P;
+	V3 D = cross(E, face.n);
+	PL pl;
+	pl.n = normalized(D);
+	pl.d = dot(pl.n, P);
+	return pl;
+}
+
+// ---------------------------------------------------------------------------
+// Clipping (clip.cpp).
+
+struct FPair
+{
+	uint32_t inEdge1, outEdge1, inEdge2, outEdge2;
+};
+
+struct ClipV
+{
+	V3 pos;
+	FPair pair;
+};
+
+__device__ __forceinline__ FPair mkpair(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+	return FPair{a, b, c, d};
+}
+
+// b3ClipSegmentToPlane (clip.cpp:62-98).
+__device__ __forceinline__ uint32_t clip_segment_to_plane(ClipV vOut[2], const ClipV vIn[2], PL plane,
+	uint32_t edge)
+{
+	uint32_t numOut = 0;
+	float d1 = pdist(vIn[0].pos, plane);
+	float d2 = pdist(vIn[1].pos, plane);
+	if (d1 <= 0.0f)
+		vOut[numOut++] = vIn[0];
+	if (d2 <= 0.0f)
+		vOut[numOut++] = vIn[1];
+	if (d1 <= 0.0f && d2 > 0.0f)
+	{
+		float fraction = d1 / (d1 - d2);
+		vOut[numOut].pos = vIn[0].pos + fraction * (vIn[1].pos - vIn[0].pos);
+		vOut[numOut].pair = mkpair(edge, B3G_NULL_EDGE, vIn[0].pair.outEdge2, B3G_NULL_EDGE);
+		++numOut;
+	}
+	else if (d1 > 0.0f && d2 <= 0.0f)
+	{
+		float fraction = d1 / (d1 - d2);
+		vOut[numOut].pos = vIn[0].pos + fraction * (vIn[1].pos - vIn[0].pos);
+		vOut[numOut].pair = mkpair(B3G_NULL_EDGE, edge, B3G_NULL_EDGE, vIn[1].pair.inEdge2);
+		++numOut;
+	}
+	return numOut;
+}
+
+// b3BuildSegment (clip.cpp:24-30).
+__device__ __forceinline__ void build_segment(ClipV v[2], V3 a, V3 b)
+{
+	v[0].pos = a;
+	v[0].pair = mkpair(B3G_NULL_EDGE, B3G_NULL_EDGE, 0, 0);
+	v[1].pos = b;
+	v[1].pair = mkpair(B3G_NULL_EDGE, B3G_NULL_EDGE, 1, 0);
+}
+
+// b3ClipSegmentToSegmentSidePlanes (clip.cpp:153-199).
+__device__ __forceinline__ uint32_t clip_segment_to_segment_side_planes(ClipV vOut[2], const ClipV vIn[2],
+	V3 P1, V3 Q1)
+{
+	vOut[0] = vIn[0];
+	vOut[1] = vIn[1];
+	V3 E1 = Q1 - P1;
+	PL plane1;
+	plane1.n = normalized(E1);
+	plane1.d = dot(plane1.n, Q1);
+	ClipV c1[2] = {vOut[0], vOut[1]};
+	uint32_t numOut = clip_segment_to_plane(c1, vOut, plane1, 0);
+	vOut[0] = c1[0];
+	vOut[1] = c1[1];
+	if (numOut < 2)
+		return numOut;
+	PL plane2;
+	plane2.n = -plane1.n;
+	plane2.d = dot(plane2.n, P1);
+	ClipV c2[2] = {vOut[0], vOut[1]};
+	numOut = clip_segment_to_plane(c2, vOut, plane2, 1);
+	vOut[0] = c2[0];
+	vOut[1] = c2[1];
+	return numOut;
+}
+
+// b3ClipSegmentToFaceSidePlanes (clip.cpp:202-241).
+__device__ __forceinline__ uint32_t clip_segment_to_face_side_planes(ClipV vOut[2], const ClipV vIn[2],
+	const XF& xf, float r, uint32_t index, const HullRef& h)
+{
+	vOut[0] = vIn[0];
+	vOut[1] = vIn[1];
+	uint32_t numOut = 0;
+	uint32_t begin = h.f[index];
+	uint32_t edge = begin;
+	do
+	{
+		uint32_t edgeId = edge; // twin of the twin
+		PL plane = hull_edge_side_plane(h, edgeId);
+		plane.d += r;
+		PL cp = pmul(xf, plane);
+		ClipV cs[2] = {vOut[0], vOut[1]};
+		numOut = clip_segment_to_plane(cs, vOut, cp, edgeId);
+		vOut[0] = cs[0];
+		vOut[1] = cs[1];
+		if (numOut == 0)
+			return 0;
+		edge = he_next(h, edge);
+	} while (edge != begin);
+	return numOut;
+}
+
+struct Poly
+{
+	ClipV v[B3G_MAX_POLY];
+	uint32_t n;
+};
+
+// b3BuildPolygon (clip.cpp:33-58).
+__device__ __forceinline__ bool build_polygon(Poly& out, const XF& xf, uint32_t index, const HullRef& h)
+{
+	out.n = 0;
+	uint32_t begin = h.f[index];
+	uint32_t edge = begin;
+	do
+	{
+		if (out.n >= B3G_MAX_POLY)
+			return false;
+		uint32_t inEdge = he_prev(h, edge);
+		uint32_t outEdge = edge;
+		ClipV& cv = out.v[out.n++];
+		cv.pos = xmul(xf, hv(h, he_origin(h, edge)));
+		cv.pair = mkpair(B3G_NULL_EDGE, B3G_NULL_EDGE, inEdge, outEdge);
+		edge = he_next(h, edge);
+	} while (edge != begin);
+	return true;
+}
+
+// b3ClipPolygonToPlane (clip.cpp:101-150).
+__device__ __forceinline__ bool clip_polygon_to_plane(Poly& out, const Poly& in, PL plane, uint32_t edge)
+{
+	out.n = 0;
+	ClipV v1 = in.v[in.n - 1];
+	float d1 = pdist(v1.pos, plane);
+	for (uint32_t i = 0; i < in.n; ++i)
+	{
+		ClipV v2 = in.v[i];
+		float d2 = pdist(v2.pos, plane);
+		if (d1 <= 0.0f && d2 <= 0.0f)
+		{
+			if (out.n >= B3G_MAX_POLY)
+				return false;
+			out.v[out.n++] = v2;
+		}
+		else if (d1 <= 0.0f && d2 > 0.0f)
+		{
+			if (out.n >= B3G_MAX_POLY)
+				return false;
+			float fraction = d1 / (d1 - d2);
+			ClipV& vx = out.v[out.n++];
+			vx.pos = v1.pos + fraction * (v2.pos - v1.pos);
+			vx.pair = mkpair(edge, B3G_NULL_EDGE, v1.pair.outEdge2, B3G_NULL_EDGE);
+		}
+		else if (d1 > 0.0f && d2 <= 0.0f)
+		{
+			if (out.n + 2 > B3G_MAX_POLY)
+				return false;
+			float fraction = d1 / (d1 - d2);
+			ClipV& vx = out.v[out.n++];
+			vx.pos = v1.pos + fraction * (v2.pos - v1.pos);
+			vx.pair = mkpair(B3G_NULL_EDGE, edge, B3G_NULL_EDGE, v2.pair.inEdge2);
+			out.v[out.n++] = v2;
+		}
+		v1 = v2;
+		d1 = d2;
+	}
+	return true;
+}
+
+// b3ClipPolygonToFaceSidePlanes (clip.cpp:244-281). Ping-pongs between two
+// polygons; returns a pointer to the one holding the result.
+__device__ __forceinline__ Poly* clip_polygon_to_face_side_planes(Poly& a, Poly& b, const XF& xf, float r,
+	uint32_t index, const HullRef& h, bool& ok)
+{
+	Poly* in = &a;
+	Poly* out = &b;
+	uint32_t begin = h.f[index];
+	uint32_t edge = begin;
+	ok = true;
+	do
+	{
+		uint32_t edgeId = edge;
+		PL plane = hull_edge_side_plane(h, edgeId);
+		plane.d += r;
+		PL cp = pmul(xf, plane);
+		if (!clip_polygon_to_plane(*out, *in, cp, edgeId))
+		{
+			ok = false;
+			return out;
+		}
+		Poly* t = in;
+		in = out;
+		out = t;
+		if (in->n == 0)
+			return in;
+		edge = he_next(h, edge);
+	} while (edge != begin);
+	return in;
+}
+
+// ---------------------------------------------------------------------------
+// Polygon reduction (cluster.cpp:24-200).
+
+struct CV
+{
+	V3 pos;
+	uint32_t clipIndex;
+};
+
+__device__ __forceinline__ bool is_ccw(V3 A, V3 B, V3 C, V3 N)
+{
+	V3 n = cross(B - A, C - A);
+	return dot(n, N) > 0.0f;
+}
+
+// b3SortPolygon (cluster.cpp:34-57). B is read once per i, before the swaps.
+__device__ __forceinline__ void sort_polygon(CV* p, uint32_t n, V3 N)
+{
+	V3 A = p[0].pos;
+	for (uint32_t i = 1; i < n; ++i)
+	{
+		V3 B = p[i].pos;
+		for (uint32_t j = i + 1; j < n; ++j)
+		{
+			V3 C = p[j].pos;
+			if (!is_ccw(A, B, C, N))
+			{
+				CV t = p[i];
+				p[i] = p[j];
+				p[j] = t;
+			}
+		}
+	}
+}
+
+// b3ReducePolygon (cluster.cpp:59-200). out holds at most 4 vertices.
+__device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint32_t n, V3 N, uint32_t initialPoint)
+{
+	if (n <= 4)
+	{
+		for (uint32_t i = 0; i < n; ++i)
+			out[i] = in[i];
+		sort_polygon(out, n, N);
+		return n;
+	}
+	uint64_t chosen = 0; // n <= B3G_MAX_POLY
+	uint32_t cnt = 0;
+	out[cnt++] = in[initialPoint];
+	chosen |= 1ull << initialPoint;
+	{
+		V3 A = out[0].pos;
+		uint32_t index = 0;
+		float mx = -B3G_MAX_SCALAR;
+		for (uint32_t i = 0; i < n; ++i)
+		{
+			if (chosen >> i & 1ull)
+				continue;
+			V3 d = in[i].pos - A;
+			float dd = dot(d, d);
+			if (dd > mx)
+			{
+				mx = dd;
+				index = i;
+			}
+		}
+		if (mx < B3G_EPSILON * B3G_EPSILON)
+			return cnt;
+		out[cnt++] = in[index];
+		chosen |= 1ull << index;
+	}
+	{
+		V3 A = out[0].pos;
+		V3 B = out[1].pos;
+		uint32_t index = 0;
+		float mx = -B3G_MAX_SCALAR;
+		for (uint32_t i = 0; i < n; ++i)
+		{
+			if (chosen >> i & 1ull)
+				continue;
+			V3 C = in[i].pos;
+			V3 Nn = cross(B - A, C - A);
+			float sa2 = dot(Nn, N);
+			float a2 = fabsr(sa2);
+			if (a2 > mx)
+			{
+				mx = a2;
+				index = i;
+			}
+		}
+		const float kAreaTol = 0.01f;
+		if (mx < 2.0f * kAreaTol)
+			return cnt;
+		V3 C = in[index].pos;
+		if (!is_ccw(A, B, C, N))
+		{
+			CV t = out[0];
+			out[0] = out[1];
+			out[1] = t;
+		}
+		out[cnt++] = in[index];
+		chosen |= 1ull << index;
+	}
+	{
+		V3 A = out[0].pos;
+		V3 B = out[1].pos;
+		uint32_t index = 0;
+		float mn = B3G_MAX_SCALAR;
+		for (uint32_t i = 0; i < n; ++i)
+		{
+			if (chosen >> i & 1ull)
+				continue;
+			V3 D = in[i].pos;
+			V3 Nn = cross(B - A, D - A);
+			float sa2 = dot(Nn, N);
+			if (sa2 < mn)
+			{
+				mn = sa2;
+				index = i;
+			}
+		}
+		const float kAreaTol = 0.01f;
+		if (fabsr(mn) < 2.0f * kAreaTol)
+			return cnt;
+		out[cnt++] = in[index];
+		chosen |= 1ull << index;
+	}
+	sort_polygon(out, cnt, N);
+	return cnt;
+}
+
+// ---------------------------------------------------------------------------
+// Manifolds.
+
+// b3Manifold::Initialize() (collision.cpp:23-38) plus cleared geometry.
+__device__ __forceinline__ void man_clear(DevManifold& m)
+{
+	m.pointCount = 0;
+	m.tangentImpulse[0] = 0.0f;
+	m.tangentImpulse[1] = 0.0f;
+	m.motorImpulse = 0.0f;
+	m.motorSpeed = 0.0f;
+	m.tangentSpeed1 = 0.0f;
+	m.tangentSpeed2 = 0.0f;
+	m.pad = 0;
+	for (int i = 0; i < 4; ++i)
+	{
+		DevPoint& p = m.points[i];
+		for (int k = 0; k < 3; ++k)
+		{
+			p.n[k] = 0.0f;
+			p.p1[k] = 0.0f;
+			p.p2[k] = 0.0f;
+		}
+		p.normalImpulse = 0.0f;
+		p.triangleKey = 0;
+		p.pad0 = 0;
+		p.key[0] = p.key[1] = p.key[2] = p.key[3] = 0;
+		p.persisting = 0;
+		p.edgeContact = 0;
+		for (int k = 0; k < 6; ++k)
+			p.pad1[k] = 0;
+	}
+}
+
+__device__ __forceinline__ void set_point(DevPoint& p, V3 n, V3 p1, V3 p2)
+{
+	p.n[0] = n.x;
+	p.n[1] = n.y;
+	p.n[2] = n.z;
+	p.p1[0] = p1.x;
+	p.p1[1] = p1.y;
+	p.p1[2] = p1.z;
+	p.p2[0] = p2.x;
+	p.p2[1] = p2.y;
+	p.p2[2] = p2.z;
+}
+
+// b3MakeID(key1, key2) with key1 = key2 = 0, and b3MakeID(pair) (collision.h:80-95).
+__device__ __forceinline__ void set_id0(DevPoint& p)
+{
+	p.triangleKey = B3G_NULL_TRIANGLE;
+	p.key[0] = p.key[1] = p.key[2] = p.key[3] = 0;
+}
+__device__ __forceinline__ void set_id(DevPoint& p, FPair f)
+{
+	p.triangleKey = B3G_NULL_TRIANGLE;
+	p.key[0] = f.inEdge1;
+	p.key[1] = f.outEdge1;
+	p.key[2] = f.inEdge2;
+	p.key[3] = f.outEdge2;
+}
+
+__device__ __forceinline__ bool id_equal(const DevPoint& a, const DevPoint& b)
+{
+	return a.triangleKey == b.triangleKey && a.key[0] == b.key[0] && a.key[1] == b.key[1] &&
+		a.key[2] == b.key[2] && a.key[3] == b.key[3];
+}
+
+// b3Manifold::Initialize(old) (collision.cpp:40-61).
+__device__ __forceinline__ void man_warm_start(DevManifold& m, const DevManifold& old)
+{
+	m.tangentImpulse[0] = old.tangentImpulse[0];
+	m.tangentImpulse[1] = old.tangentImpulse[1];
+	m.motorImpulse = old.motorImpulse;
+	for (uint32_t i = 0; i < m.pointCount; ++i)
+	{
+		DevPoint& p1 = m.points[i];
+		for (uint32_t j = 0; j < old.pointCount; ++j)
+		{
+			const DevPoint& p2 = old.points[j];
+			if (id_equal(p2, p1))
+			{
+				p1.normalImpulse = p2.normalImpulse;
+				p1.persisting = 1;
+				break;
+			}
+		}
+	}
+}
+
+// Per-pass context passed to the narrowphase kernels.
+struct NPArgs
+{
+	DevScene S;
+	uint32_t* pairA;
+	uint32_t* pairB;
+	uint32_t* cstate;
+	uint4* cache;
+	DevManifold* man;
+	const uint32_t* prevState;
+	const uint4* prevCache;
+	const DevManifold* prevMan;
+	const int32_t* prevIndex;
+	const uint32_t* list;
+	const uint32_t* listCount;
+	uint32_t* status;
+	int warmStarting;
+	int convexCache;
+	// warm-start overrides from the host solver (indexed by previous contact)
+	const float* impN;
+	const float* impT;
+	const float* impM;
+	// explicit transforms per contact (7 floats), used instead of the body
+	// state when set (stand-alone narrowphase)
+	const float* exA;
+	const float* exB;
+	const float* ex0A;
+	const float* ex0B;
+};
+
+__device__ __forceinline__ XF load_xf7(const float* s)
+{
+	XF x;
+	x.p = V3{s[0], s[1], s[2]};
+	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	return x;
+}
+
+// The tail of b3Contact::Update for a convex contact (contact.cpp:424-465):
+// warm start from the previous manifold, touching flag, manifold count 1.
+__device__ __forceinline__ void finish_convex(const NPArgs& a, uint32_t c, DevManifold& m)
+{
+	int32_t prev = a.prevIndex[c];
+	uint32_t oldCount = prev >= 0 ? ((a.prevState[prev] >> 8) & 0xFFu) : 0u;
+	if (a.warmStarting && oldCount > 0)
+	{
+		DevManifold old = a.prevMan[prev];
+		if (a.impN)
+		{
+			for (int k = 0; k < 4; ++k)
+				old.points[k].normalImpulse = a.impN[4 * prev + k];
+			old.tangentImpulse[0] = a.impT[2 * prev + 0];
+			old.tangentImpulse[1] = a.impT[2 * prev + 1];
+			old.motorImpulse = a.impM[prev];
+		}
+		man_warm_start(m, old);
+	}
+	uint32_t touching = m.pointCount > 0 ? 1u : 0u;
+	uint32_t begun = prev < 0 ? 1u : 0u;
+	a.cstate[c] = touching | (1u << 8) | (begun << 16);
+	a.man[c] = m;
+}
+
+__device__ __forceinline__ XF body_xf(const DevScene& S, uint32_t body)
+{
+	const float* s = S.bodyState + 17 * (size_t)body;
+	XF x;
+	x.p = V3{s[0], s[1], s[2]};
+	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	return x;
+}
+
+// b3Sweep::GetTransform(0) (sweep.h:43-63) from the stored sweep start.
+__device__ __forceinline__ XF body_xf0(const DevScene& S, uint32_t body)
+{
+	const float* s = S.bodyState + 17 * (size_t)body;
+	Q4 q1 = Q4{V3{s[10], s[11], s[12]}, s[13]};
+	Q4 q2 = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	V3 c0 = V3{s[7], s[8], s[9]};
+	V3 lc = V3{s[14], s[15], s[16]};
+	if (qdot(q1, q2) < 0.0f)
+		q1 = qneg(q1);
+	// (1 - 0) * c0 + 0 * c and (1 - 0) * q1 + 0 * q2 reduce to c0 and q1.
+	Q4 q = q1;
+	qnormalize_inplace(q);
+	XF x;
+	x.p = c0 - rot(q, lc);
+	x.q = q;
+	return x;
+}

@@ -1,0 +1,532 @@
+// Thread-per-pair narrowphase for the rounded convex pairs:
+//   b3CollideSpheres          collide_spheres.cpp:22-52
+//   b3CollideCapsuleAndSphere collide_capsule_sphere.cpp:23-120
+//   b3CollideCapsules         collide_capsules.cpp:25-123
+//   b3CollideHullAndSphere    collide_hull_sphere.cpp:26-97
+//   b3CollideHullAndCapsule   collide_hull_capsule.cpp:29-190, sat_hull_edge.cpp:29-146
+// and the sensor path b3TestOverlap (collision.cpp:104-113). Each routine
+// evaluates the reference's operations in the reference's order.
+
+#include "collide_common.cuh"
+
+namespace {
+
+__device__ __forceinline__ V3 f3(float4 a) { return V3{a.x, a.y, a.z}; }
+
+struct ShapeP
+{
+	uint32_t type;
+	float4 p0, p1, p2;
+	uint32_t hull;
+};
+
+__device__ __forceinline__ ShapeP load_shape(const DevScene& S, uint32_t fix)
+{
+	ShapeP s;
+	s.type = S.fixType[fix];
+	s.p0 = S.fixParams[3 * fix + 0];
+	s.p1 = S.fixParams[3 * fix + 1];
+	s.p2 = S.fixParams[3 * fix + 2];
+	s.hull = S.fixHull[fix];
+	return s;
+}
+
+__device__ __forceinline__ V3 sph_center(const ShapeP& s) { return V3{s.p0.x, s.p0.y, s.p0.z}; }
+__device__ __forceinline__ float sph_radius(const ShapeP& s) { return s.p0.w; }
+__device__ __forceinline__ V3 cap_v1(const ShapeP& s) { return V3{s.p0.x, s.p0.y, s.p0.z}; }
+__device__ __forceinline__ V3 cap_v2(const ShapeP& s) { return V3{s.p0.w, s.p1.x, s.p1.y}; }
+__device__ __forceinline__ float cap_radius(const ShapeP& s) { return s.p1.z; }
+__device__ __forceinline__ float hull_radius(const ShapeP& s) { return s.p0.x; }
+
+__device__ void collide_spheres(DevManifold& m, const XF& xf1, const ShapeP& s1, const XF& xf2, const ShapeP& s2)
+{
+	V3 c1 = xmul(xf1, sph_center(s1));
+	float r1 = sph_radius(s1);
+	V3 c2 = xmul(xf2, sph_center(s2));
+	float r2 = sph_radius(s2);
+	V3 d = c2 - c1;
+	float dd = dot(d, d);
+	float totalRadius = r1 + r2;
+	if (dd > totalRadius * totalRadius)
+		return;
+	float distance = len(d);
+	V3 normal = V3{0.0f, 1.0f, 0.0f};
+	if (distance > B3G_EPSILON)
+		normal = d / distance;
+	m.pointCount = 1;
+	set_point(m.points[0], rotc(xf1.q, normal), sph_center(s1), sph_center(s2));
+	set_id0(m.points[0]);
+}
+
+__device__ void collide_capsule_sphere(DevManifold& m, const XF& xf1, const ShapeP& c1, const XF& xf2,
+	const ShapeP& s2)
+{
+	V3 Q = xmult(xf1, xmul(xf2, sph_center(s2)));
+	V3 A = cap_v1(c1), B = cap_v2(c1);
+	V3 AB = B - A;
+	float u = dot(B - Q, AB);
+	float v = dot(Q - A, AB);
+	float radius = cap_radius(c1) + sph_radius(s2);
+	if (v <= 0.0f || u <= 0.0f)
+	{
+		V3 P = v <= 0.0f ? A : B;
+		V3 d = Q - P;
+		float dd = dot(d, d);
+		if (dd > radius * radius)
+			return;
+		V3 n = V3{0.0f, 1.0f, 0.0f};
+		float l = len(d);
+		if (l > B3G_EPSILON)
+			n = d / l;
+		m.pointCount = 1;
+		set_point(m.points[0], n, P, sph_center(s2));
+		set_id0(m.points[0]);
+		return;
+	}
+	float s = dot(AB, AB);
+	V3 P = (u * A + v * B) / s;
+	V3 d = Q - P;
+	float dd = dot(d, d);
+	if (dd > radius * radius)
+		return;
+	V3 AQ = Q - A;
+	V3 AB_x_AQ = cross(AB, AQ);
+	V3 n = cross(AB_x_AQ, AB);
+	if (dot(n, AQ) < 0.0f)
+		n = -n;
+	normalize_inplace(n);
+	m.pointCount = 1;
+	set_point(m.points[0], n, P, sph_center(s2));
+	set_id0(m.points[0]);
+}
+
+// b3AreParalell (collide_capsules.cpp:25-45).
+__device__ __forceinline__ bool are_parallel(V3 a1, V3 a2, V3 b1, V3 b2)
+{
+	V3 E1 = a2 - a1;
+	float L1 = len(E1);
+	if (L1 < B3G_LINEAR_SLOP)
+		return false;
+	V3 E2 = b2 - b1;
+	float L2 = len(E2);
+	if (L2 < B3G_LINEAR_SLOP)
+		return false;
+	const float kTol = 0.005f;
+	V3 N = cross(E1, E2);
+	return len(N) < (kTol * L1) * L2;
+}
+
+__device__ void collide_capsules(DevManifold& m, const XF& xf1, const ShapeP& k1, const XF& xf2, const ShapeP& k2)
+{
+	V3 s1a = xmul(xf1, cap_v1(k1)), s1b = xmul(xf1, cap_v2(k1));
+	V3 s2a = xmul(xf2, cap_v1(k2)), s2b = xmul(xf2, cap_v2(k2));
+	V3 point1, point2;
+	closest_on_segments(point1, point2, s1a, s1b, s2a, s2b);
+	float distance = len(point1 - point2);
+	float r1 = cap_radius(k1), r2 = cap_radius(k2);
+	float totalRadius = r1 + r2;
+	if (distance > totalRadius)
+		return;
+	if (distance > 0.0f && are_parallel(s1a, s1b, s2a, s2b))
+	{
+		ClipV in1[2];
+		build_segment(in1, s1a, s1b);
+		ClipV clip1[2];
+		uint32_t clipCount = clip_segment_to_segment_side_planes(clip1, in1, s2a, s2b);
+		if (clipCount == 2)
+		{
+			V3 cp1 = closest_on_segment(clip1[0].pos, s2a, s2b);
+			V3 cp2 = closest_on_segment(clip1[1].pos, s2a, s2b);
+			float d1 = len(clip1[0].pos - cp1);
+			float d2 = len(clip1[1].pos - cp2);
+			if (d1 > B3G_EPSILON && d1 <= totalRadius && d2 > B3G_EPSILON && d2 <= totalRadius)
+			{
+				V3 n1 = (cp1 - clip1[0].pos) / d1;
+				V3 n2 = (cp2 - clip1[1].pos) / d2;
+				m.pointCount = 2;
+				set_point(m.points[0], rotc(xf1.q, n1), xmult(xf1, clip1[0].pos), xmult(xf2, cp1));
+				set_id(m.points[0], clip1[0].pair);
+				set_point(m.points[1], rotc(xf1.q, n2), xmult(xf1, clip1[1].pos), xmult(xf2, cp2));
+				set_id(m.points[1], clip1[1].pair);
+				return;
+			}
+		}
+	}
+	if (distance > 0.0f)
+	{
+		V3 normal = (point2 - point1) / distance;
+		m.pointCount = 1;
+		set_point(m.points[0], rotc(xf1.q, normal), xmult(xf1, point1), xmult(xf2, point2));
+		set_id0(m.points[0]);
+	}
+}
+
+__device__ __forceinline__ GProxy hull_proxy(const HullRef& h, float r)
+{
+	GProxy p;
+	p.gv = h.v;
+	p.count = h.vCnt;
+	p.radius = r;
+	return p;
+}
+
+__device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
+	const XF& xf2, const ShapeP& s2)
+{
+	float radius = hull_radius(hs) + sph_radius(s2);
+	HullRef h1 = hull_ref(S, hs.hull);
+	V3 cLocal = xmult(xf1, xmul(xf2, sph_center(s2)));
+	uint32_t faceIndex = 0;
+	float separation = -B3G_MAX_SCALAR;
+	for (uint32_t i = 0; i < h1.fCnt; ++i)
+	{
+		PL plane = hp(h1, i);
+		float s = pdist(cLocal, plane);
+		if (s > radius)
+			return;
+		if (s > separation)
+		{
+			faceIndex = i;
+			separation = s;
+		}
+	}
+	if (separation < 0.0f)
+	{
+		PL lp = hp(h1, faceIndex);
+		V3 c1 = pclosest(cLocal, lp);
+		m.pointCount = 1;
+		set_point(m.points[0], lp.n, c1, sph_center(s2));
+		set_id0(m.points[0]);
+		return;
+	}
+	GProxy p1 = hull_proxy(h1, hull_radius(hs));
+	GProxy p2;
+	p2.gv = nullptr;
+	p2.lv[0] = sph_center(s2);
+	p2.count = 1;
+	p2.radius = sph_radius(s2);
+	GJKOut q = gjk(xf1, p1, xf2, p2, false);
+	if (q.distance > radius)
+		return;
+	if (q.distance > 0.0f)
+	{
+		V3 normal = (q.point2 - q.point1) / q.distance;
+		m.pointCount = 1;
+		set_point(m.points[0], rotc(xf1.q, normal), xmult(xf1, q.point1), sph_center(s2));
+		set_id0(m.points[0]);
+	}
+}
+
+// b3QueryFaceSeparation(hull, capsule) (sat_hull_edge.cpp:29-59).
+__device__ void query_face_hull_capsule(const HullRef& h1, V3 lv1, V3 lv2, uint32_t& index, float& sep)
+{
+	uint32_t maxIndex = 0;
+	float maxSep = -B3G_MAX_SCALAR;
+	for (uint32_t i = 0; i < h1.fCnt; ++i)
+	{
+		PL plane = hp(h1, i);
+		V3 d = -plane.n;
+		V3 support = dot(d, lv1) > dot(d, lv2) ? lv1 : lv2; // b3Capsule::GetSupportVertex
+		float s = pdist(support, plane);
+		if (s > maxSep)
+		{
+			maxIndex = i;
+			maxSep = s;
+		}
+	}
+	index = maxIndex;
+	sep = maxSep;
+}
+
+// b3ProjectEdge (sat_hull_edge.cpp:68-100).
+__device__ __forceinline__ float project_edge_capsule(V3 P1, V3 E1, V3 C1, V3 P2, V3 E2)
+{
+	float L1 = len(E1);
+	if (L1 < B3G_LINEAR_SLOP)
+		return -B3G_MAX_SCALAR;
+	float L2 = len(E2);
+	if (L2 < B3G_LINEAR_SLOP)
+		return -B3G_MAX_SCALAR;
+	const float kTol = 0.005f;
+	V3 E1_x_E2 = cross(E1, E2);
+	float L = len(E1_x_E2);
+	if (L < (kTol * L1) * L2)
+		return -B3G_MAX_SCALAR;
+	V3 N = (1.0f / L) * E1_x_E2;
+	if (dot(N, P1 - C1) < 0.0f)
+		N = -N;
+	return dot(N, P2 - P1);
+}
+
+// b3QueryEdgeSeparation(hull, capsule) (sat_hull_edge.cpp:102-146).
+__device__ void query_edge_hull_capsule(const HullRef& h1, V3 P2, V3 Q2, uint32_t& index, float& sep)
+{
+	uint32_t maxIndex = 0;
+	float maxSep = -B3G_MAX_SCALAR;
+	V3 C1 = h1.centroid;
+	V3 E2 = Q2 - P2;
+	for (uint32_t i = 0; i < h1.eCnt; i += 2)
+	{
+		uint4 e1 = h1.e[i], t1 = h1.e[i + 1];
+		V3 P1 = hv(h1, e1.x);
+		V3 Q1 = hv(h1, t1.x);
+		V3 E1 = Q1 - P1;
+		V3 U1 = hp(h1, e1.y).n;
+		V3 V1 = hp(h1, t1.y).n;
+		// b3IsMinkowskiFace(E2, U1, V1)
+		if (dot(E2, U1) * dot(E2, V1) < 0.0f)
+		{
+			float s = project_edge_capsule(P1, E1, C1, P2, E2);
+			if (s > maxSep)
+			{
+				maxSep = s;
+				maxIndex = i;
+			}
+		}
+	}
+	index = maxIndex;
+	sep = maxSep;
+}
+
+__device__ void hull_capsule_edge_contact(DevManifold& m, const XF& xf1, const HullRef& h1, uint32_t index1,
+	const XF& xf2, V3 v1, V3 v2)
+{
+	uint4 e1 = h1.e[index1], t1 = h1.e[index1 + 1];
+	V3 C1 = xmul(xf1, h1.centroid);
+	V3 P1 = xmul(xf1, hv(h1, e1.x));
+	V3 Q1 = xmul(xf1, hv(h1, t1.x));
+	V3 E1 = Q1 - P1;
+	V3 P2 = xmul(xf2, v1);
+	V3 Q2 = xmul(xf2, v2);
+	V3 E2 = Q2 - P2;
+	V3 N = cross(E1, E2);
+	normalize_inplace(N);
+	if (dot(N, P1 - C1) < 0.0f)
+		N = -N;
+	V3 point1, point2;
+	closest_on_segments(point1, point2, P1, Q1, P2, Q2);
+	m.pointCount = 1;
+	set_point(m.points[0], rotc(xf1.q, N), xmult(xf1, point1), xmult(xf2, point2));
+	set_id(m.points[0], mkpair(index1, index1 + 1, 0, 1));
+}
+
+__device__ void hull_capsule_face_contact(DevManifold& m, const XF& xf1, const HullRef& h1, uint32_t index1,
+	float r1, const XF& xf2, V3 v1, V3 v2, float r2)
+{
+	ClipV seg[2];
+	build_segment(seg, xmul(xf2, v1), xmul(xf2, v2));
+	ClipV clip2[2];
+	uint32_t clipCount = clip_segment_to_face_side_planes(clip2, seg, xf1, r1, index1, h1);
+	PL localPlane1 = hp(h1, index1);
+	PL plane1 = pmul(xf1, localPlane1);
+	float totalRadius = r1 + r2;
+	uint32_t pointCount = 0;
+	for (uint32_t i = 0; i < clipCount; ++i)
+	{
+		V3 c2 = clip2[i].pos;
+		float s = pdist(c2, plane1);
+		if (s <= totalRadius)
+		{
+			V3 c1 = pclosest(c2, plane1);
+			DevPoint& mp = m.points[pointCount];
+			set_point(mp, localPlane1.n, xmult(xf1, c1), xmult(xf2, c2));
+			set_id(mp, clip2[i].pair);
+			++pointCount;
+		}
+	}
+	m.pointCount = pointCount;
+}
+
+__device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
+	const XF& xf2, const ShapeP& k2)
+{
+	float r1 = hull_radius(hs), r2 = cap_radius(k2);
+	float totalRadius = r1 + r2;
+	HullRef h1 = hull_ref(S, hs.hull);
+	GProxy p1 = hull_proxy(h1, r1);
+	GProxy p2;
+	p2.gv = nullptr;
+	p2.lv[0] = cap_v1(k2);
+	p2.lv[1] = cap_v2(k2);
+	p2.count = 2;
+	p2.radius = r2;
+	GJKOut q = gjk(xf1, p1, xf2, p2, false);
+	if (q.distance > totalRadius)
+		return;
+	V3 v1 = cap_v1(k2), v2 = cap_v2(k2);
+	if (q.distance > 0.0f)
+	{
+		V3 c1 = q.point1, c2 = q.point2;
+		float d = q.distance;
+		V3 N1 = (c2 - c1) / d;
+		V3 localN1 = rotc(xf1.q, N1);
+		uint32_t index1 = hull_support_face(h1, localN1);
+		V3 localFaceN1 = hp(h1, index1).n;
+		const float kTol = 0.005f;
+		V3 N = cross(localN1, localFaceN1);
+		float L = dot(N, N);
+		if (L < kTol * kTol)
+		{
+			hull_capsule_face_contact(m, xf1, h1, index1, r1, xf2, v1, v2, r2);
+			if (m.pointCount == 2)
+				return;
+		}
+		m.pointCount = 1;
+		set_point(m.points[0], localN1, xmult(xf1, c1), xmult(xf2, c2));
+		set_id0(m.points[0]);
+		return;
+	}
+	// Deep overlap: SAT on the hull against the capsule segment.
+	XF xf = xmult(xf1, xf2);
+	V3 lv1 = xmul(xf, v1), lv2 = xmul(xf, v2);
+	uint32_t faceIndex;
+	float faceSep;
+	query_face_hull_capsule(h1, lv1, lv2, faceIndex, faceSep);
+	if (faceSep > totalRadius)
+		return;
+	uint32_t edgeIndex;
+	float edgeSep;
+	query_edge_hull_capsule(h1, lv1, lv2, edgeIndex, edgeSep);
+	if (edgeSep > totalRadius)
+		return;
+	const float kRelEdgeTol = 0.90f;
+	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
+	if (edgeSep > kRelEdgeTol * faceSep + kAbsTol)
+		hull_capsule_edge_contact(m, xf1, h1, edgeIndex, xf2, v1, v2);
+	else
+		hull_capsule_face_contact(m, xf1, h1, faceIndex, r1, xf2, v1, v2, r2);
+}
+
+__device__ GProxy shape_proxy(const DevScene& S, const ShapeP& s)
+{
+	GProxy p;
+	p.gv = nullptr;
+	switch (s.type)
+	{
+	case B3G_SHAPE_SPHERE:
+		p.lv[0] = sph_center(s);
+		p.count = 1;
+		p.radius = sph_radius(s);
+		break;
+	case B3G_SHAPE_CAPSULE:
+		p.lv[0] = cap_v1(s);
+		p.lv[1] = cap_v2(s);
+		p.count = 2;
+		p.radius = cap_radius(s);
+		break;
+	case B3G_SHAPE_TRIANGLE:
+		p.lv[0] = V3{s.p0.x, s.p0.y, s.p0.z};
+		p.lv[1] = V3{s.p0.w, s.p1.x, s.p1.y};
+		p.lv[2] = V3{s.p1.z, s.p1.w, s.p2.x};
+		p.count = 3;
+		p.radius = s.p2.y;
+		break;
+	default:
+	{
+		HullRef h = hull_ref(S, s.hull);
+		p = hull_proxy(h, hull_radius(s));
+		break;
+	}
+	}
+	return p;
+}
+
+// Contacts listed in one bucket, one thread each.
+template <int BUCKET>
+__global__ void k_convex(NPArgs a)
+{
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.list[t];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+		XF xfA = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
+		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
+		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
+		DevManifold m;
+		man_clear(m);
+		if (BUCKET == BK_SPHERES)
+			collide_spheres(m, xfA, sa, xfB, sb);
+		else if (BUCKET == BK_CAPSULE_SPHERE)
+			collide_capsule_sphere(m, xfA, sa, xfB, sb);
+		else if (BUCKET == BK_CAPSULES)
+			collide_capsules(m, xfA, sa, xfB, sb);
+		else if (BUCKET == BK_HULL_SPHERE)
+			collide_hull_sphere(m, a.S, xfA, sa, xfB, sb);
+		else if (BUCKET == BK_HULL_CAPSULE)
+			collide_hull_capsule(m, a.S, xfA, sa, xfB, sb);
+		finish_convex(a, c, m);
+		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+	}
+}
+
+// Sensor contacts: touching = b3TestOverlap (collision.cpp:104-113), no manifolds.
+__global__ void k_sensor(NPArgs a)
+{
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.list[t];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		XF xfA = body_xf(a.S, a.S.fixBody[fa]), xfB = body_xf(a.S, a.S.fixBody[fb]);
+		GProxy pa = shape_proxy(a.S, load_shape(a.S, fa));
+		GProxy pb = shape_proxy(a.S, load_shape(a.S, fb));
+		GJKOut q = gjk(xfA, pa, xfB, pb, true);
+		const float kTol = 10.0f * B3G_EPSILON;
+		uint32_t touching = q.distance <= kTol ? 1u : 0u;
+		int32_t prev = a.prevIndex[c];
+		uint32_t begun = prev < 0 ? 1u : 0u;
+		a.cstate[c] = touching | (begun << 16);
+		DevManifold m;
+		man_clear(m);
+		a.man[c] = m;
+		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+	}
+}
+
+// Contacts whose bodies are both inactive keep their state (contact_manager.cpp:262-268).
+__global__ void k_inactive(NPArgs a)
+{
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.list[t];
+		int32_t prev = a.prevIndex[c];
+		if (prev >= 0)
+		{
+			a.cstate[c] = a.prevState[prev] & ~(1u << 16);
+			a.cache[c] = a.prevCache[prev];
+			a.man[c] = a.prevMan[prev];
+		}
+		else
+		{
+			a.cstate[c] = 1u << 16;
+			a.cache[c] = make_uint4(0, B3G_NULL, B3G_NULL, B3G_NULL);
+			DevManifold m;
+			man_clear(m);
+			a.man[c] = m;
+		}
+	}
+}
+
+} // namespace
+
+void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	cudaStream_t s)
+{
+	const int blocks = persistent_blocks(4);
+	NPArgs a = base;
+#define B3G_LAUNCH(BK, KERNEL)                     \
+	a.list = lists + (size_t)(BK)*cap;             \
+	a.listCount = counts + (BK);                   \
+	KERNEL<<<blocks, 128, 0, s>>>(a);
+	B3G_LAUNCH(BK_SPHERES, k_convex<BK_SPHERES>);
+	B3G_LAUNCH(BK_CAPSULE_SPHERE, k_convex<BK_CAPSULE_SPHERE>);
+	B3G_LAUNCH(BK_CAPSULES, k_convex<BK_CAPSULES>);
+	B3G_LAUNCH(BK_HULL_SPHERE, k_convex<BK_HULL_SPHERE>);
+	B3G_LAUNCH(BK_HULL_CAPSULE, k_convex<BK_HULL_CAPSULE>);
+	B3G_LAUNCH(BK_SENSOR, k_sensor);
+	B3G_LAUNCH(BK_INACTIVE, k_inactive);
+#undef B3G_LAUNCH
+}

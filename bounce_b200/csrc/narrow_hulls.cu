@@ -1,0 +1,645 @@
+// Warp-per-pair hull-hull narrowphase: b3CollideHulls with the feature cache
+// (collide_hulls.cpp:355-534) and without it (collide_hulls.cpp:189-264).
+//
+// The 32 lanes of a warp share one contact. The separating-axis queries are
+// spread over the lanes: face queries (sat.cpp:33-58) put faces on lanes and
+// loop over the other hull's vertices for the support point; the edge query
+// (sat.cpp:111-174) flattens the (edge1, edge2) double loop onto lanes after
+// the per-edge data (both endpoints, edge vector and length, the two adjacent
+// face normals of the Gauss map) is precomputed into shared memory. Every
+// argmax is reduced with warp shuffles on (value, flattened index), keeping
+// the larger value and, on equal values, the lower index - which is exactly
+// the first maximum the reference's sequential "if (s > max)" loops select.
+// The serial remainder (incident face clipping, polygon reduction, the cache
+// decision tree) runs on lane 0.
+
+#include "collide_common.cuh"
+
+namespace {
+
+constexpr int HW_WARPS = 4; // warps per block
+
+struct EdgeRec
+{
+	float4 P; // xyz endpoint, w = |E|
+	float4 E; // xyz edge vector
+	float4 U; // xyz normal of the edge's face
+	float4 V; // xyz normal of the twin's face
+};
+
+__device__ __forceinline__ V3 f3(float4 a) { return V3{a.x, a.y, a.z}; }
+
+// First-maximum reduction across the warp on (value, index).
+__device__ __forceinline__ void warp_argmax(float& v, uint32_t& idx)
+{
+	for (int o = 16; o > 0; o >>= 1)
+	{
+		float ov = __shfl_xor_sync(0xffffffffu, v, o);
+		uint32_t oi = __shfl_xor_sync(0xffffffffu, idx, o);
+		if (ov > v || (ov == v && oi < idx))
+		{
+			v = ov;
+			idx = oi;
+		}
+	}
+}
+
+// b3Project(hull, plane) (sat.cpp:26-30) with the support vertex
+// (hull.h:105-119) searched over the lanes. Uniform result on all lanes.
+__device__ float warp_project(const HullRef& h, PL plane, uint32_t lane)
+{
+	V3 d = -plane.n;
+	float best = 0.0f;
+	uint32_t bi = 0xFFFFFFFFu;
+	for (uint32_t i = lane; i < h.vCnt; i += 32)
+	{
+		float proj = dot(d, hv(h, i));
+		if (bi == 0xFFFFFFFFu || proj > best)
+		{
+			best = proj;
+			bi = i;
+		}
+	}
+	if (bi == 0xFFFFFFFFu)
+		best = -INFINITY;
+	warp_argmax(best, bi);
+	return pdist(hv(h, bi), plane);
+}
+
+// b3QueryFaceSeparation(hull, hull) (sat.cpp:33-58).
+__device__ void warp_query_faces(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2,
+	uint32_t lane, uint32_t& index, float& sep)
+{
+	XF xf = xmult(xf2, xf1);
+	float best = -B3G_MAX_SCALAR;
+	uint32_t bi = 0xFFFFFFFFu;
+	for (uint32_t i = lane; i < h1.fCnt; i += 32)
+	{
+		PL plane = pmul(xf, hp(h1, i));
+		V3 d = -plane.n;
+		uint32_t si = 0;
+		float sp = dot(d, hv(h2, 0));
+		for (uint32_t k = 1; k < h2.vCnt; ++k)
+		{
+			float proj = dot(d, hv(h2, k));
+			if (proj > sp)
+			{
+				si = k;
+				sp = proj;
+			}
+		}
+		float s = pdist(hv(h2, si), plane);
+		if (s > best)
+		{
+			best = s;
+			bi = i;
+		}
+	}
+	warp_argmax(best, bi);
+	index = bi == 0xFFFFFFFFu ? 0u : bi;
+	sep = best;
+}
+
+// b3IsMinkowskiFace (sat.cpp:60-71).
+__device__ __forceinline__ bool is_minkowski_face(V3 A, V3 B, V3 BxA, V3 C, V3 D, V3 DxC)
+{
+	float ADC = dot(A, DxC);
+	float BDC = dot(B, DxC);
+	float CBA = dot(C, BxA);
+	float DBA = dot(D, BxA);
+	return CBA * DBA < 0.0f && ADC * BDC < 0.0f && CBA * BDC > 0.0f;
+}
+
+// b3Project(P1, Q1, E1, P2, E2, C1) (sat.cpp:73-109); L1 = |E1|, L2 = |E2|.
+__device__ __forceinline__ float project_edges(V3 P1, V3 E1, float L1, V3 P2, V3 E2, float L2, V3 C1)
+{
+	if (L1 < B3G_LINEAR_SLOP)
+		return -B3G_MAX_SCALAR;
+	if (L2 < B3G_LINEAR_SLOP)
+		return -B3G_MAX_SCALAR;
+	const float kTol = 0.005f;
+	V3 E1_x_E2 = cross(E1, E2);
+	float L = len(E1_x_E2);
+	if (L < (kTol * L1) * L2)
+		return -B3G_MAX_SCALAR;
+	V3 N = (1.0f / L) * E1_x_E2;
+	if (dot(N, P1 - C1) < 0.0f)
+		N = -N;
+	return dot(N, P2 - P1);
+}
+
+__device__ __forceinline__ void edge_rec_1(EdgeRec& r, const XF& xf, const HullRef& h1, uint32_t i)
+{
+	uint4 e1 = h1.e[i], t1 = h1.e[i + 1];
+	V3 P1 = xmul(xf, hv(h1, e1.x));
+	V3 Q1 = xmul(xf, hv(h1, t1.x));
+	V3 E1 = Q1 - P1;
+	V3 U1 = rot(xf.q, hp(h1, e1.y).n);
+	V3 V1 = rot(xf.q, hp(h1, t1.y).n);
+	r.P = make_float4(P1.x, P1.y, P1.z, len(E1));
+	r.E = make_float4(E1.x, E1.y, E1.z, 0.0f);
+	r.U = make_float4(U1.x, U1.y, U1.z, 0.0f);
+	r.V = make_float4(V1.x, V1.y, V1.z, 0.0f);
+}
+
+__device__ __forceinline__ void edge_rec_2(EdgeRec& r, const HullRef& h2, uint32_t j)
+{
+	uint4 e2 = h2.e[j], t2 = h2.e[j + 1];
+	V3 P2 = hv(h2, e2.x);
+	V3 Q2 = hv(h2, t2.x);
+	V3 E2 = Q2 - P2;
+	V3 U2 = hp(h2, e2.y).n;
+	V3 V2 = hp(h2, t2.y).n;
+	r.P = make_float4(P2.x, P2.y, P2.z, len(E2));
+	r.E = make_float4(E2.x, E2.y, E2.z, 0.0f);
+	r.U = make_float4(U2.x, U2.y, U2.z, 0.0f);
+	r.V = make_float4(V2.x, V2.y, V2.z, 0.0f);
+}
+
+__device__ __forceinline__ float edge_pair_sep(const EdgeRec& a, const EdgeRec& b, V3 C1)
+{
+	V3 U1 = f3(a.U), V1 = f3(a.V), E1 = f3(a.E);
+	V3 U2 = f3(b.U), V2 = f3(b.V), E2 = f3(b.E);
+	if (!is_minkowski_face(U1, V1, -E1, -U2, -V2, -E2))
+		return -INFINITY; // not a Minkowski face: never a candidate
+	return project_edges(f3(a.P), E1, a.P.w, f3(b.P), E2, b.P.w, C1);
+}
+
+// b3QueryEdgeSeparation(hull, hull) (sat.cpp:111-174). recs holds room for
+// the unique edges of both hulls (maxUE each).
+__device__ void warp_query_edges(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2,
+	uint32_t lane, EdgeRec* recs, uint32_t maxUE, uint32_t& index1, uint32_t& index2, float& sep)
+{
+	XF xf = xmult(xf2, xf1);
+	V3 C1 = xmul(xf, h1.centroid);
+	uint32_t n1 = h1.eCnt / 2, n2 = h2.eCnt / 2;
+	EdgeRec* r1 = recs;
+	EdgeRec* r2 = recs + maxUE;
+	bool staged = n1 <= maxUE && n2 <= maxUE;
+	if (staged)
+	{
+		for (uint32_t i = lane; i < n1; i += 32)
+			edge_rec_1(r1[i], xf, h1, 2 * i);
+		for (uint32_t j = lane; j < n2; j += 32)
+			edge_rec_2(r2[j], h2, 2 * j);
+		__syncwarp();
+	}
+	float best = -B3G_MAX_SCALAR;
+	uint32_t bk = 0xFFFFFFFFu;
+	uint32_t total = n1 * n2;
+	for (uint32_t k = lane; k < total; k += 32)
+	{
+		uint32_t i = k / n2, j = k - i * n2;
+		float s;
+		if (staged)
+		{
+			s = edge_pair_sep(r1[i], r2[j], C1);
+		}
+		else
+		{
+			EdgeRec a, b;
+			edge_rec_1(a, xf, h1, 2 * i);
+			edge_rec_2(b, h2, 2 * j);
+			s = edge_pair_sep(a, b, C1);
+		}
+		if (s > best)
+		{
+			best = s;
+			bk = k;
+		}
+	}
+	warp_argmax(best, bk);
+	if (bk == 0xFFFFFFFFu)
+	{
+		index1 = 0;
+		index2 = 0;
+	}
+	else
+	{
+		index1 = 2 * (bk / n2);
+		index2 = 2 * (bk % n2);
+	}
+	sep = best;
+	__syncwarp();
+}
+
+// b3BuildEdgeContact (collide_hulls.cpp:30-73).
+__device__ void build_edge_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1,
+	const XF& xf2, uint32_t index2, const HullRef& h2)
+{
+	uint4 e1 = h1.e[index1], t1 = h1.e[index1 + 1];
+	V3 C1 = xmul(xf1, h1.centroid);
+	V3 P1 = xmul(xf1, hv(h1, e1.x));
+	V3 Q1 = xmul(xf1, hv(h1, t1.x));
+	V3 E1 = Q1 - P1;
+	uint4 e2 = h2.e[index2], t2 = h2.e[index2 + 1];
+	V3 P2 = xmul(xf2, hv(h2, e2.x));
+	V3 Q2 = xmul(xf2, hv(h2, t2.x));
+	V3 E2 = Q2 - P2;
+	V3 N = cross(E1, E2);
+	normalize_inplace(N);
+	if (dot(N, P1 - C1) < 0.0f)
+		N = -N;
+	V3 point1, point2;
+	closest_on_segments(point1, point2, P1, Q1, P2, Q2);
+	m.pointCount = 1;
+	set_point(m.points[0], rotc(xf1.q, N), xmult(xf1, point1), xmult(xf2, point2));
+	set_id(m.points[0], mkpair(index1, index1 + 1, index2, index2 + 1));
+	m.points[0].edgeContact = 1;
+}
+
+// b3BuildFaceContact (collide_hulls.cpp:75-187). Runs on one lane.
+__device__ void build_face_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1, float r1,
+	const XF& xf2, const HullRef& h2, float r2, bool flipNormal, uint32_t* status)
+{
+	float totalRadius = r1 + r2;
+	PL localPlane1 = hp(h1, index1);
+	PL plane1 = pmul(xf1, localPlane1);
+	V3 normal1 = rotc(xf2.q, plane1.n);
+	uint32_t index2 = hull_support_face(h2, -normal1);
+	Poly pa, pb;
+	if (!build_polygon(pa, xf2, index2, h2))
+	{
+		atomicOr(status, B3G_ST_POLY_OVERFLOW);
+		return;
+	}
+	bool ok;
+	Poly* clip = clip_polygon_to_face_side_planes(pa, pb, xf1, totalRadius, index1, h1, ok);
+	if (!ok)
+	{
+		atomicOr(status, B3G_ST_POLY_OVERFLOW);
+		return;
+	}
+	if (clip->n == 0)
+		return;
+	CV poly1[B3G_MAX_POLY];
+	uint32_t n1 = 0;
+	uint32_t minIndex = 0;
+	float minSep = B3G_MAX_SCALAR;
+	for (uint32_t i = 0; i < clip->n; ++i)
+	{
+		V3 p = clip->v[i].pos;
+		float s = pdist(p, plane1);
+		if (s <= totalRadius)
+		{
+			if (s < minSep)
+			{
+				minIndex = n1;
+				minSep = s;
+			}
+			poly1[n1].pos = pclosest(p, plane1);
+			poly1[n1].clipIndex = i;
+			++n1;
+		}
+	}
+	if (n1 == 0)
+		return;
+	V3 normal = plane1.n;
+	V3 oriented = flipNormal ? -normal : normal;
+	CV red[4];
+	uint32_t cnt = reduce_polygon(red, poly1, n1, oriented, minIndex);
+	for (uint32_t i = 0; i < cnt; ++i)
+	{
+		const ClipV& v2 = clip->v[red[i].clipIndex];
+		V3 v1 = pclosest(v2.pos, plane1);
+		DevPoint& mp = m.points[i];
+		if (flipNormal)
+		{
+			set_point(mp, rotc(xf2.q, oriented), xmult(xf2, v2.pos), xmult(xf1, v1));
+			set_id(mp, mkpair(v2.pair.inEdge2, v2.pair.outEdge2, v2.pair.inEdge1, v2.pair.outEdge1));
+		}
+		else
+		{
+			set_point(mp, rotc(xf1.q, oriented), xmult(xf1, v1), xmult(xf2, v2.pos));
+			set_id(mp, v2.pair);
+		}
+		mp.edgeContact = 0;
+	}
+	m.pointCount = cnt;
+}
+
+// b3RebuildEdgeContact (collide_hulls.cpp:266-321).
+__device__ void rebuild_edge_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1,
+	const XF& xf2, uint32_t index2, const HullRef& h2)
+{
+	uint4 e1 = h1.e[index1], t1 = h1.e[index1 + 1];
+	V3 C1 = xmul(xf1, h1.centroid);
+	V3 P1 = xmul(xf1, hv(h1, e1.x));
+	V3 Q1 = xmul(xf1, hv(h1, t1.x));
+	V3 E1 = Q1 - P1;
+	uint4 e2 = h2.e[index2], t2 = h2.e[index2 + 1];
+	V3 P2 = xmul(xf2, hv(h2, e2.x));
+	V3 Q2 = xmul(xf2, hv(h2, t2.x));
+	V3 E2 = Q2 - P2;
+	V3 point1, point2;
+	closest_on_segments(point1, point2, P1, Q1, P2, Q2);
+	float w1[3], w2[3];
+	barycentric_segment(w1, P2, Q2, point1);
+	barycentric_segment(w2, P1, Q1, point2);
+	if (w1[1] > 0.0f && w1[1] <= w1[2] && w2[1] > 0.0f && w2[1] <= w2[2])
+	{
+		V3 N = cross(E1, E2);
+		normalize_inplace(N);
+		if (dot(N, P1 - C1) < 0.0f)
+			N = -N;
+		m.pointCount = 1;
+		set_point(m.points[0], rotc(xf1.q, N), xmult(xf1, point1), xmult(xf2, point2));
+		set_id(m.points[0], mkpair(index1, index1 + 1, index2, index2 + 1));
+		m.points[0].edgeContact = 1;
+	}
+}
+
+// b3RebuildFaceContact (collide_hulls.cpp:323-353).
+__device__ void rebuild_face_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1, float r1,
+	const XF& xf2, const HullRef& h2, float r2, bool flipNormal, const XF& xf01, const XF& xf02,
+	uint32_t* status)
+{
+	Q4 q01 = xf01.q, q1 = xf1.q;
+	Q4 q02 = xf02.q, q2 = xf2.q;
+	Q4 dq0 = qmul(conj(q01), q02);
+	Q4 dq = qmul(conj(q1), q2);
+	Q4 q = qmul(conj(dq0), dq);
+	const float kCosTol = 0.995f;
+	if (fabsr(q.s) > kCosTol)
+		build_face_contact(m, xf1, index1, h1, r1, xf2, h2, r2, flipNormal, status);
+}
+
+enum
+{
+	CT_EMPTY = 0,
+	CT_SEPARATION = 1,
+	CT_OVERLAP = 2
+};
+enum
+{
+	FT_EDGES = 0,
+	FT_FACE1 = 1,
+	FT_FACE2 = 2
+};
+
+// b3FeatureCache::ReadFace (sat.cpp:209-224).
+__device__ uint32_t read_face(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2, uint32_t index1,
+	float totalRadius, uint32_t lane)
+{
+	XF xf = xmult(xf2, xf1);
+	PL plane = pmul(xf, hp(h1, index1));
+	float s = warp_project(h2, plane, lane);
+	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
+}
+
+// b3FeatureCache::ReadEdges (sat.cpp:226-281).
+__device__ uint32_t read_edges(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2, uint32_t i,
+	uint32_t j, float totalRadius)
+{
+	XF xf = xmult(xf2, xf1);
+	V3 C1 = xmul(xf, h1.centroid);
+	EdgeRec a, b;
+	edge_rec_1(a, xf, h1, i);
+	edge_rec_2(b, h2, j);
+	V3 U1 = f3(a.U), V1 = f3(a.V), E1 = f3(a.E);
+	V3 U2 = f3(b.U), V2 = f3(b.V), E2 = f3(b.E);
+	if (is_minkowski_face(U1, V1, -E1, -U2, -V2, -E2))
+	{
+		float s = project_edges(f3(a.P), E1, a.P.w, f3(b.P), E2, b.P.w, C1);
+		return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
+	}
+	return CT_EMPTY;
+}
+
+struct HullCtx
+{
+	XF xf1, xf2, xf01, xf02;
+	HullRef h1, h2;
+	float r1, r2;
+	EdgeRec* recs;
+	uint32_t maxUE;
+	uint32_t* status;
+};
+
+// Lane 0 builds, the warp learns the point count.
+__device__ uint32_t face_contact_all(DevManifold& m, const HullCtx& H, bool flip, uint32_t index, uint32_t lane)
+{
+	if (lane == 0)
+	{
+		if (flip)
+			build_face_contact(m, H.xf2, index, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status);
+		else
+			build_face_contact(m, H.xf1, index, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status);
+	}
+	return __shfl_sync(0xffffffffu, m.pointCount, 0);
+}
+
+// b3CollideHulls without cache (collide_hulls.cpp:189-264).
+__device__ void collide_hulls_nocache(DevManifold& m, const HullCtx& H, uint32_t lane)
+{
+	float totalRadius = H.r1 + H.r2;
+	uint32_t fi1, fi2, ei1, ei2;
+	float fs1, fs2, es;
+	warp_query_faces(H.xf1, H.h1, H.xf2, H.h2, lane, fi1, fs1);
+	if (fs1 > totalRadius)
+		return;
+	warp_query_faces(H.xf2, H.h2, H.xf1, H.h1, lane, fi2, fs2);
+	if (fs2 > totalRadius)
+		return;
+	warp_query_edges(H.xf1, H.h1, H.xf2, H.h2, lane, H.recs, H.maxUE, ei1, ei2, es);
+	if (es > totalRadius)
+		return;
+	const float kRelEdgeTol = 0.90f;
+	const float kRelFaceTol = 0.98f;
+	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
+	uint32_t pc;
+	if (es > kRelEdgeTol * fmaxr(fs1, fs2) + kAbsTol)
+	{
+		if (lane == 0)
+			build_edge_contact(m, H.xf1, ei1, H.h1, H.xf2, ei2, H.h2);
+		pc = 1;
+	}
+	else if (fs2 > kRelFaceTol * fs1 + kAbsTol)
+		pc = face_contact_all(m, H, true, fi2, lane);
+	else
+		pc = face_contact_all(m, H, false, fi1, lane);
+	if (pc > 0)
+		return;
+	if (es > fmaxr(fs1, fs2))
+	{
+		if (lane == 0)
+			build_edge_contact(m, H.xf1, ei1, H.h1, H.xf2, ei2, H.h2);
+	}
+	else if (fs2 > fs1)
+		face_contact_all(m, H, true, fi2, lane);
+	else
+		face_contact_all(m, H, false, fi1, lane);
+}
+
+// b3CollideHullsCache (collide_hulls.cpp:355-515). cache is uniform across
+// the warp; m is meaningful on lane 0.
+__device__ void collide_hulls_cache(DevManifold& m, const HullCtx& H, uint4& cache, uint32_t lane)
+{
+	float totalRadius = H.r1 + H.r2;
+	uint32_t state0 = cache.x;
+	// b3FeatureCache::ReadState (sat.cpp:178-207).
+	if (cache.x == CT_EMPTY)
+	{
+		cache.x = CT_SEPARATION;
+		cache.y = FT_FACE1;
+		cache.z = 0;
+		cache.w = 0;
+	}
+	uint32_t state1;
+	if (cache.y == FT_EDGES)
+		state1 = read_edges(H.xf1, H.h1, H.xf2, H.h2, cache.z, cache.w, totalRadius);
+	else if (cache.y == FT_FACE1)
+		state1 = read_face(H.xf1, H.h1, H.xf2, H.h2, cache.z, totalRadius, lane);
+	else if (cache.y == FT_FACE2)
+		state1 = read_face(H.xf2, H.h2, H.xf1, H.h1, cache.z, totalRadius, lane);
+	else
+		state1 = CT_EMPTY;
+
+	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
+		return; // separation cache hit
+	if (state0 == CT_OVERLAP && state1 == CT_OVERLAP)
+	{
+		if (lane == 0)
+		{
+			if (cache.y == FT_EDGES)
+				rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
+			else if (cache.y == FT_FACE1)
+				rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02,
+					H.status);
+			else if (cache.y == FT_FACE2)
+				rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01,
+					H.status);
+		}
+		uint32_t pc = __shfl_sync(0xffffffffu, m.pointCount, 0);
+		if (pc > 0)
+			return; // overlap cache hit
+	}
+	// Miss: flush and rerun the SAT.
+	cache.x = CT_EMPTY;
+	uint32_t fi1, fi2, ei1, ei2;
+	float fs1, fs2, es;
+	warp_query_faces(H.xf1, H.h1, H.xf2, H.h2, lane, fi1, fs1);
+	if (fs1 > totalRadius)
+	{
+		cache = make_uint4(CT_SEPARATION, FT_FACE1, fi1, fi1);
+		return;
+	}
+	warp_query_faces(H.xf2, H.h2, H.xf1, H.h1, lane, fi2, fs2);
+	if (fs2 > totalRadius)
+	{
+		cache = make_uint4(CT_SEPARATION, FT_FACE2, fi2, fi2);
+		return;
+	}
+	warp_query_edges(H.xf1, H.h1, H.xf2, H.h2, lane, H.recs, H.maxUE, ei1, ei2, es);
+	if (es > totalRadius)
+	{
+		cache = make_uint4(CT_SEPARATION, FT_EDGES, ei1, ei2);
+		return;
+	}
+	const float kRelEdgeTol = 0.90f;
+	const float kRelFaceTol = 0.98f;
+	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
+	if (es > kRelEdgeTol * fmaxr(fs1, fs2) + kAbsTol)
+	{
+		if (lane == 0)
+			build_edge_contact(m, H.xf1, ei1, H.h1, H.xf2, ei2, H.h2);
+		cache = make_uint4(CT_OVERLAP, FT_EDGES, ei1, ei2);
+		return;
+	}
+	if (fs2 > kRelFaceTol * fs1 + kAbsTol)
+	{
+		if (face_contact_all(m, H, true, fi2, lane) > 0)
+		{
+			cache = make_uint4(CT_OVERLAP, FT_FACE2, fi2, fi2);
+			return;
+		}
+	}
+	else
+	{
+		if (face_contact_all(m, H, false, fi1, lane) > 0)
+		{
+			cache = make_uint4(CT_OVERLAP, FT_FACE1, fi1, fi1);
+			return;
+		}
+	}
+	// Heuristic failed. Fallback.
+	if (es > fmaxr(fs1, fs2))
+	{
+		if (lane == 0)
+			build_edge_contact(m, H.xf1, ei1, H.h1, H.xf2, ei2, H.h2);
+		cache = make_uint4(CT_OVERLAP, FT_EDGES, ei1, ei2);
+		return;
+	}
+	if (fs2 > fs1)
+	{
+		if (face_contact_all(m, H, true, fi2, lane) > 0)
+			cache = make_uint4(CT_OVERLAP, FT_FACE2, fi2, fi2);
+	}
+	else
+	{
+		if (face_contact_all(m, H, false, fi1, lane) > 0)
+			cache = make_uint4(CT_OVERLAP, FT_FACE1, fi1, fi1);
+	}
+}
+
+__global__ void __launch_bounds__(HW_WARPS * 32) k_hulls(NPArgs a, uint32_t maxUE)
+{
+	extern __shared__ float4 smem[];
+	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	uint32_t n = *a.listCount;
+	uint32_t gw = blockIdx.x * HW_WARPS + warp;
+	uint32_t nw = gridDim.x * HW_WARPS;
+	for (uint32_t t = gw; t < n; t += nw)
+	{
+		uint32_t c = a.list[t];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+		HullCtx H;
+		H.xf1 = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
+		H.xf2 = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
+		H.xf01 = a.ex0A ? load_xf7(a.ex0A + 7 * (size_t)c) : body_xf0(a.S, ba);
+		H.xf02 = a.ex0B ? load_xf7(a.ex0B + 7 * (size_t)c) : body_xf0(a.S, bb);
+		H.h1 = hull_ref(a.S, a.S.fixHull[fa]);
+		H.h2 = hull_ref(a.S, a.S.fixHull[fb]);
+		H.r1 = a.S.fixParams[3 * fa].x;
+		H.r2 = a.S.fixParams[3 * fb].x;
+		H.recs = recs;
+		H.maxUE = maxUE;
+		H.status = a.status;
+		int32_t prev = a.prevIndex[c];
+		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
+		DevManifold m;
+		if (lane == 0)
+			man_clear(m);
+		else
+			m.pointCount = 0;
+		if (a.convexCache)
+			collide_hulls_cache(m, H, cache, lane);
+		else
+			collide_hulls_nocache(m, H, lane);
+		if (lane == 0)
+		{
+			finish_convex(a, c, m);
+			a.cache[c] = cache;
+		}
+		__syncwarp();
+	}
+}
+
+} // namespace
+
+void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s)
+{
+	NPArgs a = base;
+	a.list = list;
+	a.listCount = count;
+	size_t smem = (size_t)HW_WARPS * 2 * maxUE * sizeof(EdgeRec);
+	static size_t configured = 0;
+	if (smem > 48 * 1024 && smem > configured)
+	{
+		cudaFuncSetAttribute(k_hulls, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		configured = smem;
+	}
+	k_hulls<<<persistent_blocks(2), HW_WARPS * 32, smem, s>>>(a, maxUE);
+}

@@ -1,0 +1,168 @@
+"""Python host mirror of the pipeline's C ABI (include/b3g.h).
+
+``CollisionPipeline`` plays the role of Bounce's b3ContactManager +
+b3BroadPhase for one context: ``collide()`` is one collision pass (the fixture
+sync and FindNewContacts of the "Find New Pairs" block, world.cpp:424-449,
+then UpdateContacts, contact_manager.cpp:225-287), and the fetch methods read
+the contact list, the b3Manifold records and the destroyed contacts back.
+Errors raise ``B3GError`` with the library's message; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+u32, f32 = ctypes.c_uint32, ctypes.c_float
+
+
+class CollisionPipeline:
+    def __init__(self, scene, max_contacts=None, warm_starting=True, convex_cache=True, device=0):
+        self.lib = N.load()
+        self.scene = scene
+        nf = scene.n_fixtures
+        if max_contacts is None:
+            max_contacts = max(1024, 32 * nf)
+        ha = scene.hull_arrays
+        cfg = N.Config(
+            max_proxies=max(nf, 1),
+            max_contacts=int(max_contacts),
+            max_hull_data=0,
+            flags=(N.FLAG_WARM_STARTING if warm_starting else 0) | (N.FLAG_CONVEX_CACHE if convex_cache else 0),
+            device=device,
+        )
+        h = ctypes.c_void_p()
+        rc = self.lib.b3g_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise N.B3GError(rc, "b3g_create failed")
+        self.ctx = h
+        self.max_contacts = int(max_contacts)
+        nh = len(scene.hulls)
+        self._check(
+            self.lib.b3g_set_hulls(
+                self.ctx, nh, N.ptr(ha["desc"], u32), N.ptr(ha["verts"], f32), N.ptr(ha["edges"], u32),
+                N.ptr(ha["faces"], u32), N.ptr(ha["planes"], f32), N.ptr(ha["centroids"], f32),
+            )
+        )
+        awake = np.ones(scene.n_bodies, np.uint8)
+        self._check(
+            self.lib.b3g_set_bodies(
+                self.ctx, scene.n_bodies, N.ptr(scene.body_world, u32), N.ptr(scene.body_type, u32),
+                N.ptr(awake, ctypes.c_uint8),
+            )
+        )
+        self._check(
+            self.lib.b3g_set_fixtures(
+                self.ctx, nf, N.ptr(scene.fix_body, u32), N.ptr(scene.fix_type, u32), N.ptr(scene.fix_hull, u32),
+                N.ptr(scene.fix_params, f32), N.ptr(scene.fix_flags, u32), None,
+            )
+        )
+
+    def _check(self, rc):
+        if rc < 0:
+            msg = self.lib.b3g_last_error(self.ctx)
+            raise N.B3GError(rc, msg.decode() if msg else "")
+        return rc
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.b3g_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- pass -------------------------------------------------------------
+
+    def set_awake(self, awake):
+        a = np.ascontiguousarray(awake, np.uint8)
+        self._check(self.lib.b3g_set_awake(self.ctx, N.ptr(a, ctypes.c_uint8)))
+
+    def collide(self, state17, on_device=False, stream=None):
+        """One collision pass. state17: host float32 array (17 per body) or,
+        with on_device=True, a device pointer (int) to the same layout."""
+        if on_device:
+            p = ctypes.c_void_p(int(state17))
+        else:
+            assert state17.dtype == np.float32 and state17.flags["C_CONTIGUOUS"]
+            p = ctypes.c_void_p(state17.ctypes.data)
+        self._check(self.lib.b3g_collide(self.ctx, p, 1 if on_device else 0, ctypes.c_void_p(stream or 0)))
+
+    def counts(self):
+        c = N.Counts()
+        self._check(self.lib.b3g_get_counts(self.ctx, ctypes.byref(c)))
+        return c.as_dict()
+
+    # -- results ----------------------------------------------------------
+
+    def contacts(self):
+        n = self.counts()["contacts"]
+        out = np.zeros((max(n, 1), 3), np.uint32)
+        m = self._check(self.lib.b3g_fetch_contacts(self.ctx, N.ptr(out, u32), n))
+        return out[:m]
+
+    def manifolds(self):
+        n = self.counts()["contacts"]
+        out = np.zeros(max(n, 1), N.MANIFOLD_DTYPE)
+        m = self._check(self.lib.b3g_fetch_manifolds(self.ctx, ctypes.c_void_p(out.ctypes.data), n))
+        return out[:m]
+
+    def touching(self):
+        n = self.counts()["contacts"]
+        idx = np.zeros(max(n, 1), np.uint32)
+        man = np.zeros(max(n, 1), N.MANIFOLD_DTYPE)
+        m = self._check(self.lib.b3g_fetch_touching(self.ctx, N.ptr(idx, u32), ctypes.c_void_p(man.ctypes.data), n))
+        return idx[:m], man[:m]
+
+    def ended(self):
+        c = self.counts()
+        out = np.zeros((max(c["ended"], 1), 3), np.uint32)
+        m = self._check(self.lib.b3g_fetch_ended(self.ctx, N.ptr(out, u32), c["ended"]))
+        return out[:m]
+
+    def caches(self):
+        n = self.counts()["contacts"]
+        out = np.zeros((max(n, 1), 4), np.uint32)
+        m = self._check(self.lib.b3g_fetch_caches(self.ctx, N.ptr(out, u32), n))
+        return out[:m]
+
+    def fat_aabbs(self):
+        nf = self.scene.n_fixtures
+        out = np.zeros((nf, 6), np.float32)
+        self._check(self.lib.b3g_fetch_fat_aabbs(self.ctx, N.ptr(out, f32), nf))
+        return out
+
+    def load_impulses(self, normal, tangent, motor):
+        n = np.ascontiguousarray(normal, np.float32)
+        t = np.ascontiguousarray(tangent, np.float32)
+        m = np.ascontiguousarray(motor, np.float32)
+        self._check(self.lib.b3g_load_impulses(self.ctx, N.ptr(n, f32), N.ptr(t, f32), N.ptr(m, f32)))
+
+    def device_results(self):
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        self._check(self.lib.b3g_device_results(self.ctx, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def collide_pairs(self, fixA, fixB, xfA, xfB, xf0A=None, xf0B=None, cache=None):
+        """Stand-alone narrowphase on explicit pairs and transforms (7 floats each)."""
+        n = len(fixA)
+        fa = np.ascontiguousarray(fixA, np.uint32)
+        fb = np.ascontiguousarray(fixB, np.uint32)
+        xa = np.ascontiguousarray(xfA, np.float32).reshape(-1)
+        xb = np.ascontiguousarray(xfB, np.float32).reshape(-1)
+        x0a = None if xf0A is None else np.ascontiguousarray(xf0A, np.float32).reshape(-1)
+        x0b = None if xf0B is None else np.ascontiguousarray(xf0B, np.float32).reshape(-1)
+        cc = None if cache is None else np.ascontiguousarray(cache, np.uint32).reshape(-1)
+        out = np.zeros(max(n, 1), N.MANIFOLD_DTYPE)
+        self._check(
+            self.lib.b3g_collide_pairs(
+                self.ctx, n, N.ptr(fa, u32), N.ptr(fb, u32), N.ptr(xa, f32), N.ptr(xb, f32), N.ptr(x0a, f32),
+                N.ptr(x0b, f32), N.ptr(cc, u32), ctypes.c_void_p(out.ctypes.data),
+            )
+        )
+        if cache is not None:
+            cache[...] = cc.reshape(cache.shape)
+        return out[:n]

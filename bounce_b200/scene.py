@@ -1,0 +1,383 @@
+"""Seeded synthetic scenes for the collision pipeline and the kinematic driver
+that moves their bodies between passes.
+
+Scenes follow the workloads the pipeline is measured on:
+
+* ``plain_scene``   1,000 unit boxes (half extent 0.5 m) + 1,000 spheres
+  (r = 0.5 m), positions uniform in a 20 m cube above a static 100 x 1 x 100 m
+  ground box, uniform random orientations.
+* ``mixed_scene``   N mixed bodies: 40 % spheres r ~ U[0.2, 1], 30 % capsules
+  r ~ U[0.1, 0.5], half-height ~ U[0.2, 1] (segment along local y), 30 % convex
+  hulls of 8-32 points on ellipsoids with semi-axes ~ U[0.3, 1.2]; positions
+  uniform in a cube of side L, linear velocities N(0, 1) m/s, angular N(0, 1) rad/s.
+* ``batched_scene`` many independent worlds whose body counts are log-uniform
+  in [16, 4096], each with the plain-scene shape mix.
+
+All arithmetic that feeds the pipeline's inputs is float32 with the same
+operation order as the reference's inline math (include/bounce/common/math/
+quat.h:270-274, transform.h:66-69, body.h SynchronizeTransform), so transforms
+computed here equal the ones b3Body would hold, bit for bit.
+"""
+import numpy as np
+
+from . import _native as N
+
+F = np.float32
+
+# ---------------------------------------------------------------------------
+# float32 vector helpers with the reference's operation order.
+
+
+def _cross(a, b):
+    return np.stack(
+        [
+            a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+            a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+            a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0],
+        ],
+        axis=-1,
+    ).astype(F)
+
+
+def quat_rotate(q, v):
+    """b3Mul(quat, vec): v + s * t + qv x t with t = 2 (qv x v)."""
+    qv = q[..., :3]
+    s = q[..., 3:4]
+    t = F(2) * _cross(qv, v)
+    return ((v + s * t) + _cross(qv, t)).astype(F)
+
+
+def xf_apply(p, q, v):
+    """b3Mul(transform, vec)."""
+    return (quat_rotate(q, v) + p).astype(F)
+
+
+def quat_normalize(q):
+    """b3Quat::Normalize: v scaled by 1/len, s divided by len."""
+    v = q[..., :3]
+    s = q[..., 3]
+    l = np.sqrt(((v[..., 0] * v[..., 0] + v[..., 1] * v[..., 1]) + v[..., 2] * v[..., 2]) + s * s).astype(F)
+    ok = l > F(1.1920928955078125e-07)
+    inv = np.where(ok, F(1) / np.where(ok, l, F(1)), F(1)).astype(F)
+    out = q.copy()
+    out[..., 0] = np.where(ok, v[..., 0] * inv, v[..., 0])
+    out[..., 1] = np.where(ok, v[..., 1] * inv, v[..., 1])
+    out[..., 2] = np.where(ok, v[..., 2] * inv, v[..., 2])
+    out[..., 3] = np.where(ok, s / np.where(ok, l, F(1)), s)
+    return out.astype(F)
+
+
+def random_quats(rng, n):
+    """Uniform random unit quaternions (Shoemake), x y z w."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1 - u1), np.sqrt(u1)
+    q = np.stack(
+        [a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2), b * np.sin(2 * np.pi * u3), b * np.cos(2 * np.pi * u3)],
+        axis=-1,
+    )
+    return q.astype(F)
+
+
+# ---------------------------------------------------------------------------
+# Hull pool.
+
+
+class HullPool:
+    """Packed b3Hull arrays (include/b3g.h b3g_set_hulls layout)."""
+
+    def __init__(self):
+        self.desc, self.verts, self.edges, self.faces, self.planes, self.centroids = [], [], [], [], [], []
+        self._nv = self._ne = self._nf = 0
+
+    def _add(self, v, e, f, p, c, counts):
+        nv, ne, nf = (int(x) for x in counts)
+        self.desc.append([self._nv, nv, self._ne, ne, self._nf, nf])
+        self.verts.append(v[: 3 * nv])
+        self.edges.append(e[: 5 * ne])
+        self.faces.append(f[:nf])
+        self.planes.append(p[: 4 * nf])
+        self.centroids.append(c)
+        self._nv += nv
+        self._ne += ne
+        self._nf += nf
+        return len(self.desc) - 1
+
+    def add_points(self, pts):
+        lib = N.load()
+        pts = np.ascontiguousarray(pts, dtype=F)
+        n = len(pts)
+        v = np.zeros(3 * n, F)
+        e = np.zeros(5 * (6 * n), np.uint32)
+        f = np.zeros(2 * n, np.uint32)
+        p = np.zeros(4 * 2 * n, F)
+        c = np.zeros(3, F)
+        counts = np.zeros(3, np.uint32)
+        rc = lib.b3g_hull_from_points(
+            N.ptr(pts, N.ctypes.c_float), n, N.ptr(v, N.ctypes.c_float), N.ptr(e, N.ctypes.c_uint32),
+            N.ptr(f, N.ctypes.c_uint32), N.ptr(p, N.ctypes.c_float), N.ptr(c, N.ctypes.c_float),
+            N.ptr(counts, N.ctypes.c_uint32),
+        )
+        if rc != 0:
+            raise ValueError("degenerate hull point set")
+        return self._add(v, e, f, p, c, counts)
+
+    def add_box(self, ex, ey, ez):
+        lib = N.load()
+        v = np.zeros(24, F)
+        e = np.zeros(5 * 24, np.uint32)
+        f = np.zeros(6, np.uint32)
+        p = np.zeros(24, F)
+        c = np.zeros(3, F)
+        counts = np.zeros(3, np.uint32)
+        lib.b3g_hull_box(
+            F(ex), F(ey), F(ez), N.ptr(v, N.ctypes.c_float), N.ptr(e, N.ctypes.c_uint32), N.ptr(f, N.ctypes.c_uint32),
+            N.ptr(p, N.ctypes.c_float), N.ptr(c, N.ctypes.c_float), N.ptr(counts, N.ctypes.c_uint32),
+        )
+        return self._add(v, e, f, p, c, counts)
+
+    def arrays(self):
+        cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0, dt), dtype=dt)
+        return dict(
+            desc=np.ascontiguousarray(np.array(self.desc, np.uint32).reshape(-1)),
+            verts=cat(self.verts, F),
+            edges=cat(self.edges, np.uint32),
+            faces=cat(self.faces, np.uint32),
+            planes=cat(self.planes, F),
+            centroids=np.ascontiguousarray(np.array(self.centroids, F).reshape(-1)),
+        )
+
+    def __len__(self):
+        return len(self.desc)
+
+
+# ---------------------------------------------------------------------------
+# Scenes.
+
+
+class Scene:
+    """Bodies (one fixture each here, the API allows several), fixtures and hulls."""
+
+    def __init__(self):
+        self.hulls = HullPool()
+        self.body_world, self.body_type, self.body_pos, self.body_quat = [], [], [], []
+        self.body_lin, self.body_ang = [], []
+        self.fix_body, self.fix_type, self.fix_hull, self.fix_params, self.fix_flags = [], [], [], [], []
+        self.hull_centroid_of = {}
+
+    def add_body(self, world, btype, pos, quat, lin=(0, 0, 0), ang=(0, 0, 0)):
+        self.body_world.append(world)
+        self.body_type.append(btype)
+        self.body_pos.append(pos)
+        self.body_quat.append(quat)
+        self.body_lin.append(lin)
+        self.body_ang.append(ang)
+        return len(self.body_world) - 1
+
+    def add_fixture(self, body, stype, params, hull=0, flags=0):
+        p = np.zeros(12, F)
+        p[: len(params)] = params
+        self.fix_body.append(body)
+        self.fix_type.append(stype)
+        self.fix_hull.append(hull)
+        self.fix_params.append(p)
+        self.fix_flags.append(flags)
+        return len(self.fix_body) - 1
+
+    def finalize(self):
+        self.hull_arrays = self.hulls.arrays()
+        self.body_world = np.ascontiguousarray(self.body_world, np.uint32)
+        self.body_type = np.ascontiguousarray(self.body_type, np.uint32)
+        self.body_pos = np.ascontiguousarray(np.array(self.body_pos, F).reshape(-1, 3))
+        self.body_quat = np.ascontiguousarray(np.array(self.body_quat, F).reshape(-1, 4))
+        self.body_lin = np.ascontiguousarray(np.array(self.body_lin, F).reshape(-1, 3))
+        self.body_ang = np.ascontiguousarray(np.array(self.body_ang, F).reshape(-1, 3))
+        self.fix_body = np.ascontiguousarray(self.fix_body, np.uint32)
+        self.fix_type = np.ascontiguousarray(self.fix_type, np.uint32)
+        self.fix_hull = np.ascontiguousarray(self.fix_hull, np.uint32)
+        self.fix_params = np.ascontiguousarray(np.array(self.fix_params, F).reshape(-1))
+        self.fix_flags = np.ascontiguousarray(self.fix_flags, np.uint32)
+        self.body_pose = np.ascontiguousarray(np.concatenate([self.body_pos, self.body_quat], axis=1))
+        self.local_center = self._local_centers()
+        return self
+
+    @property
+    def n_bodies(self):
+        return len(self.body_world)
+
+    @property
+    def n_fixtures(self):
+        return len(self.fix_body)
+
+    @property
+    def n_worlds(self):
+        return int(self.body_world.max()) + 1 if self.n_bodies else 0
+
+    def _local_centers(self):
+        """Body centre of mass in body frame for single-fixture dynamic bodies:
+        the shape's centroid (sphere centre, capsule midpoint, hull volume
+        centroid); zero for static and kinematic bodies (body.cpp:265-281)."""
+        lc = np.zeros((self.n_bodies, 3), F)
+        params = self.fix_params.reshape(-1, 12)
+        cents = self.hull_arrays["centroids"].reshape(-1, 3)
+        for f in range(self.n_fixtures):
+            b = self.fix_body[f]
+            if self.body_type[b] != N.BODY_DYNAMIC:
+                continue
+            t = self.fix_type[f]
+            if t == N.SHAPE_SPHERE:
+                lc[b] = params[f, 0:3]
+            elif t == N.SHAPE_CAPSULE:
+                lc[b] = F(0.5) * (params[f, 0:3] + params[f, 3:6])
+            elif t == N.SHAPE_HULL:
+                lc[b] = cents[self.fix_hull[f]]
+        return lc
+
+    def set_local_centers(self, lc):
+        self.local_center = np.ascontiguousarray(lc, F).reshape(-1, 3)
+
+
+def plain_scene(seed=1, n_boxes=1000, n_spheres=1000, cube=20.0, world=0, scene=None, box_hull=None):
+    """Boxes and spheres above a static ground box."""
+    rng = np.random.default_rng(seed)
+    s = scene if scene is not None else Scene()
+    if box_hull is None:
+        box_hull = s.hulls.add_box(0.5, 0.5, 0.5)
+    ground_hull = s.hulls.add_box(50.0, 0.5, 50.0)
+    g = s.add_body(world, N.BODY_STATIC, (0, -0.5, 0), (0, 0, 0, 1))
+    s.add_fixture(g, N.SHAPE_HULL, [0.0], hull=ground_hull)
+    n = n_boxes + n_spheres
+    half = cube / 2
+    pos = np.stack(
+        [rng.uniform(-half, half, n), rng.uniform(0.5, 0.5 + cube, n), rng.uniform(-half, half, n)], axis=-1
+    ).astype(F)
+    quat = random_quats(rng, n)
+    lin = rng.normal(0, 1, (n, 3)).astype(F)
+    ang = rng.normal(0, 1, (n, 3)).astype(F)
+    for i in range(n):
+        b = s.add_body(world, N.BODY_DYNAMIC, pos[i], quat[i], lin[i], ang[i])
+        if i < n_boxes:
+            s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=box_hull)
+        else:
+            s.add_fixture(b, N.SHAPE_SPHERE, [0, 0, 0, 0.5])
+    return s
+
+
+def ellipsoid_points(rng, n, axes):
+    d = rng.normal(0, 1, (n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return (d * axes).astype(F)
+
+
+def mixed_scene(seed=2, n=65536, side=49.0, hull_pts=(8, 32), hull_axes=(0.3, 1.2), world=0, scene=None):
+    """Mixed spheres / capsules / hulls in a cube, all dynamic."""
+    rng = np.random.default_rng(seed)
+    s = scene if scene is not None else Scene()
+    kind = rng.random(n)
+    pos = rng.uniform(-side / 2, side / 2, (n, 3)).astype(F)
+    quat = random_quats(rng, n)
+    lin = rng.normal(0, 1, (n, 3)).astype(F)
+    ang = rng.normal(0, 1, (n, 3)).astype(F)
+    for i in range(n):
+        b = s.add_body(world, N.BODY_DYNAMIC, pos[i], quat[i], lin[i], ang[i])
+        k = kind[i]
+        if k < 0.4:
+            s.add_fixture(b, N.SHAPE_SPHERE, [0, 0, 0, rng.uniform(0.2, 1.0)])
+        elif k < 0.7:
+            r = rng.uniform(0.1, 0.5)
+            h = rng.uniform(0.2, 1.0)
+            s.add_fixture(b, N.SHAPE_CAPSULE, [0, -h, 0, 0, h, 0, r])
+        else:
+            while True:
+                m = int(rng.integers(hull_pts[0], hull_pts[1] + 1))
+                axes = rng.uniform(hull_axes[0], hull_axes[1], 3)
+                try:
+                    h = s.hulls.add_points(ellipsoid_points(rng, m, axes))
+                    break
+                except ValueError:
+                    continue
+            s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=h)
+    return s
+
+
+def batched_scene(seed=3, n_worlds=1024, lo=16, hi=4096, cube=20.0):
+    """Independent worlds, body counts log-uniform in [lo, hi], plain-scene mix
+    (boxes and spheres in equal numbers above a ground box per world)."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    box = s.hulls.add_box(0.5, 0.5, 0.5)
+    counts = np.round(np.exp(rng.uniform(np.log(lo), np.log(hi), n_worlds))).astype(int)
+    for w in range(n_worlds):
+        nb = int(counts[w])
+        # Keep the body density of the plain scene: cube volume scales with nb.
+        side = cube * (nb / 2000.0) ** (1.0 / 3.0)
+        plain_scene(seed=int(rng.integers(1 << 31)), n_boxes=nb // 2, n_spheres=nb - nb // 2, cube=max(side, 4.0),
+                    world=w, scene=s, box_hull=box)
+    return s, counts
+
+
+# ---------------------------------------------------------------------------
+# Kinematic driver.
+
+
+class KinematicDriver:
+    """Moves bodies with constant velocities between passes and produces the
+    per-pass body state (include/b3g.h b3g_collide layout, 17 floats per body)
+    and the sweep input of the reference driver (14 floats per body).
+
+    Per pass k the sweep start is the previous pose and the sweep end the new
+    one: c_k = c_{k-1} + dt v, q_k = normalize(q_{k-1} + dt/2 (w, 0) q_{k-1})."""
+
+    def __init__(self, scene, dt=1.0 / 60.0):
+        self.s = scene
+        self.dt = F(dt)
+        self.lc = scene.local_center
+        p, q = scene.body_pos, scene.body_quat
+        # b3Body::ResetMass: worldCenter = xf * localCenter (body.cpp).
+        self.c = xf_apply(p, q, self.lc)
+        self.q = q.copy()
+        self.c0 = self.c.copy()
+        self.q0 = self.q.copy()
+        self.p = p.copy()
+        self.moving = scene.body_type != N.BODY_STATIC
+        self.step_index = 0
+
+    def advance(self):
+        """Move one step (static bodies stay)."""
+        dt = self.dt
+        m = self.moving
+        c1 = (self.c + dt * self.s.body_lin).astype(F)
+        w = self.s.body_ang
+        q = self.q
+        # qdot = 0.5 * (w, 0) * q  (quat.h b3Derivative / b3Integrate)
+        wv = w
+        qv, qs = q[:, :3], q[:, 3:4]
+        dv = (_cross(wv, qv) + qs * wv).astype(F)  # w x qv + qs w (0 * qv term vanishes)
+        ds = (-(wv * qv).sum(axis=1, keepdims=True)).astype(F)
+        qd = np.concatenate([F(0.5) * dv, F(0.5) * ds], axis=1).astype(F)
+        q1 = quat_normalize((q + dt * qd).astype(F))
+        self.c0 = np.where(m[:, None], self.c, self.c0).astype(F)
+        self.q0 = np.where(m[:, None], self.q, self.q0).astype(F)
+        self.c = np.where(m[:, None], c1, self.c).astype(F)
+        self.q = np.where(m[:, None], q1, self.q).astype(F)
+        # b3Body::SynchronizeTransform: xf.p = worldCenter - R(q) localCenter.
+        self.p = np.where(m[:, None], (self.c - quat_rotate(self.q, self.lc)).astype(F), self.p).astype(F)
+        self.step_index += 1
+
+    def state17(self):
+        """Per-body pipeline input: xf (p, q), sweep worldCenter0, orientation0, localCenter."""
+        out = np.empty((self.s.n_bodies, 17), F)
+        out[:, 0:3] = self.p
+        out[:, 3:7] = self.q
+        out[:, 7:10] = self.c0
+        out[:, 10:14] = self.q0
+        out[:, 14:17] = self.lc
+        return np.ascontiguousarray(out.reshape(-1))
+
+    def sweeps14(self):
+        """Reference driver input: worldCenter0, orientation0, worldCenter, orientation."""
+        out = np.empty((self.s.n_bodies, 14), F)
+        out[:, 0:3] = self.c0
+        out[:, 3:7] = self.q0
+        out[:, 7:10] = self.c
+        out[:, 10:14] = self.q
+        return np.ascontiguousarray(out.reshape(-1))

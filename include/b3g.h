@@ -1,0 +1,214 @@
+/*
+ * b3g.h - C ABI of the B200 collision pipeline for the Bounce physics engine.
+ *
+ * One call of b3g_collide() is one collision pass of Bounce's b3World::Step:
+ * the per-fixture fat-AABB update of the "Find New Pairs" block
+ * (src/bounce/dynamics/world.cpp:424-449), the broadphase pair search and
+ * contact creation of b3ContactManager::FindNewContacts / AddPair
+ * (src/bounce/dynamics/contact_manager.cpp:98-223) and the narrowphase of
+ * b3ContactManager::UpdateContacts (contact_manager.cpp:225-287), all on the
+ * GPU. The reference's solver, islands, sleep and TOI stay host code and
+ * consume the manifolds this library writes in the reference's own
+ * b3Manifold layout (include/bounce/collision/collision.h:110-128, 320 bytes).
+ *
+ * Conventions
+ *  - Every entry point returns B3G_OK (0) or a negative status; the message of
+ *    the last failure is available from b3g_last_error(). The reference has
+ *    no error returns (it asserts and grows buffers); capacity overflows here
+ *    are reported as B3G_E_CAPACITY and leave the previous state intact.
+ *  - Host buffers are owned by the caller. Device memory is owned by the
+ *    context and allocated in b3g_create (fixed capacities).
+ *  - Calls on one context are serialised by the caller; a context runs on one
+ *    CUDA stream. Different contexts are independent.
+ *  - Indices of fixtures/bodies/hulls are the positions in the arrays given to
+ *    b3g_set_*; a "world" groups bodies whose fixtures may collide.
+ */
+#ifndef B3G_H
+#define B3G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; the entry points below are
+ * the only exported symbols. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define B3G_OK 0
+#define B3G_E_INVALID (-1)   /* bad argument or call order */
+#define B3G_E_CAPACITY (-2)  /* a fixed device capacity was exceeded */
+#define B3G_E_CUDA (-3)      /* a CUDA runtime call failed */
+#define B3G_E_TIMEOUT (-4)   /* a bounded device wait gave up */
+#define B3G_E_STATE (-5)     /* the context holds no scene yet */
+
+/* b3Shape::Type (include/bounce/collision/shapes/shape.h:45-53) */
+#define B3G_SHAPE_SPHERE 0
+#define B3G_SHAPE_CAPSULE 1
+#define B3G_SHAPE_TRIANGLE 2
+#define B3G_SHAPE_HULL 3
+#define B3G_SHAPE_MESH 4
+
+/* b3BodyType (include/bounce/dynamics/body.h:39-44) */
+#define B3G_BODY_STATIC 0
+#define B3G_BODY_KINEMATIC 1
+#define B3G_BODY_DYNAMIC 2
+
+/* Context flags. */
+#define B3G_FLAG_WARM_STARTING 1u /* b3World::SetWarmStarting (world.h:95) */
+#define B3G_FLAG_CONVEX_CACHE 2u  /* b3_convexCache (collide_hulls.cpp:27, forced on by b3World()) */
+
+/* Fixture flags. */
+#define B3G_FIXTURE_SENSOR 1u     /* b3FixtureDef::isSensor (fixture.h:60) */
+
+typedef struct b3g_ctx b3g_ctx;
+
+typedef struct b3g_config
+{
+	uint32_t max_proxies;   /* fixtures (broadphase proxies) over all worlds */
+	uint32_t max_contacts;  /* contacts (overlapping fat-AABB pairs) over all worlds */
+	uint32_t max_hull_data; /* total hull vertices + half-edges + faces */
+	uint32_t flags;         /* B3G_FLAG_* */
+	int32_t device;         /* CUDA device ordinal */
+} b3g_config;
+
+/* Counters of the last pass. */
+typedef struct b3g_counts
+{
+	uint32_t contacts;     /* contacts after the pass (b3ContactManager::m_contactCount) */
+	uint32_t begun;        /* contacts created by this pass (AddPair) */
+	uint32_t ended;        /* contacts destroyed by this pass (Destroy) */
+	uint32_t touching;     /* contacts with the touching flag */
+	uint32_t manifolds;    /* manifolds with at least one point */
+	uint32_t points;       /* manifold points */
+	uint32_t moved;        /* proxies whose fat AABB was re-inserted (BufferMove) */
+	uint32_t status;       /* 0 or the B3G_E_* of a device-side failure (positive) */
+} b3g_counts;
+
+/* Lifetime -------------------------------------------------------------- */
+
+/* Replaces: b3World::b3World / b3ContactManager::b3ContactManager
+ * (world.cpp:26-75, contact_manager.cpp:26-34). */
+int b3g_create(const b3g_config* config, b3g_ctx** out);
+void b3g_destroy(b3g_ctx* ctx);
+const char* b3g_last_error(const b3g_ctx* ctx);
+
+/* Scene ----------------------------------------------------------------- */
+
+/* Shared convex hull geometry, the b3Hull half-edge layout
+ * (include/bounce/collision/geometry/hull.h:24-72): per hull desc[6] =
+ * {vertexOffset, vertexCount, edgeOffset, edgeCount, faceOffset, faceCount};
+ * verts 3 floats, edges 5 u32 (origin, twin, face, prev, next; hull-local,
+ * twin of edge i is i^1 as b3QueryEdgeSeparation asserts, sat.cpp:131),
+ * faces 1 u32 (first half-edge), planes 4 floats (normal, offset), centroid
+ * 3 floats. Replaces the b3HullShape::m_hull pointer (hull_shape.h:42). */
+int b3g_set_hulls(b3g_ctx* ctx, uint32_t hull_count, const uint32_t* desc,
+	const float* verts, const uint32_t* edges, const uint32_t* faces,
+	const float* planes, const float* centroids);
+
+/* Bodies: world index, b3BodyType, awake flag (b3Body::IsAwake, body.h:585).
+ * Replaces: b3World::CreateBody (world.cpp:98-126). */
+int b3g_set_bodies(b3g_ctx* ctx, uint32_t body_count, const uint32_t* world,
+	const uint32_t* type, const uint8_t* awake);
+
+/* Fixtures (one broadphase proxy each). params: 12 floats per fixture:
+ *   sphere   p[0..2] center, p[3] radius           (sphere_shape.h)
+ *   capsule  p[0..2] vertex1, p[3..5] vertex2, p[6] radius (capsule_shape.h)
+ *   triangle p[0..8] vertices, p[9] radius         (triangle_shape.h)
+ *   hull     p[0] radius (B3_HULL_RADIUS = 0)       (hull_shape.cpp:28)
+ * proxy_key orders the two fixtures of a pair exactly as the reference's
+ * proxy ids do (b3BroadPhase::Report keeps (min, max), broad_phase.cpp:341-342);
+ * NULL uses the fixture index, which equals the reference's proxy order for
+ * fixtures created in index order and never destroyed.
+ * Replaces: b3Body::CreateFixture + b3BroadPhase::CreateProxy (body.cpp:105-136,
+ * broad_phase.cpp:291-297). The next pass is a creation pass (fat AABB = AABB
+ * +/- B3_AABB_EXTENSION, every proxy buffered as moved, dynamic_tree.cpp:108-128). */
+int b3g_set_fixtures(b3g_ctx* ctx, uint32_t fixture_count, const uint32_t* body,
+	const uint32_t* shape_type, const uint32_t* hull, const float* params,
+	const uint32_t* flags, const uint32_t* proxy_key);
+
+/* Awake flags per body. Replaces: b3Body::SetAwake (body.h:588-603). */
+int b3g_set_awake(b3g_ctx* ctx, const uint8_t* awake);
+
+/* Pass ------------------------------------------------------------------ */
+
+/* One collision pass. body_state holds 17 floats per body:
+ *   m_xf.translation (3), m_xf.rotation (x, y, z, s), m_sweep.worldCenter0 (3),
+ *   m_sweep.orientation0 (x, y, z, s), m_sweep.localCenter (3)
+ * (body.h; sweep.h:28-36). If state_on_device is non-zero the pointer is a
+ * device pointer, otherwise host memory that is copied in on the context's
+ * stream. stream is a cudaStream_t or NULL for the context's own stream.
+ * Replaces, in this order: b3Body::SynchronizeFixtures + b3Fixture::Synchronize
+ * + b3BroadPhase::MoveProxy (body.cpp:216-238, fixture.cpp:120-132,
+ * dynamic_tree.cpp:139-207), b3ContactManager::FindNewContacts
+ * (contact_manager.cpp:213-223), b3ContactManager::UpdateContacts
+ * (contact_manager.cpp:225-287). The call is asynchronous. */
+int b3g_collide(b3g_ctx* ctx, const float* body_state, int state_on_device, void* stream);
+
+/* Waits for the last pass and returns its counters. */
+int b3g_get_counts(b3g_ctx* ctx, b3g_counts* out);
+
+/* Results ---------------------------------------------------------------- */
+
+/* Contacts of the last pass, 3 u32 each: fixtureA, fixtureB (after the
+ * b3Contact::Create A/B swap, contact.cpp:306-317), flags (bit0 touching,
+ * bit1 begun this pass, bits 8-15 manifold count). Up to capacity records;
+ * returns the number written or a negative status. */
+int b3g_fetch_contacts(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
+
+/* Manifolds of the last pass in contact order, each in the reference's
+ * b3Manifold layout (320 bytes, collision.h:110-128). */
+int b3g_fetch_manifolds(b3g_ctx* ctx, void* out, uint32_t capacity);
+
+/* Compact output: contact index (u32) and b3Manifold (320 bytes) of every
+ * contact whose manifold has points, in contact order. Returns the count. */
+int b3g_fetch_touching(b3g_ctx* ctx, uint32_t* index, void* manifolds, uint32_t capacity);
+
+/* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above
+ * (flags of the destroyed contact). Replaces the Destroy calls of
+ * UpdateContacts (contact_manager.cpp:270-281). */
+int b3g_fetch_ended(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
+
+/* Hull feature caches (b3FeatureCache, sat.h:65-86) in contact order:
+ * cacheType, featureType, index1, index2; 0xFFFFFFFF for non hull-hull. */
+int b3g_fetch_caches(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
+
+/* Fat AABBs of all proxies (6 floats: lower, upper), b3BroadPhase::GetFatAABB. */
+int b3g_fetch_fat_aabbs(b3g_ctx* ctx, float* out, uint32_t capacity);
+
+/* Warm-start state written by the host solver after a pass, in contact order
+ * of that pass: 4 normal impulses per contact and per-manifold tangent (2) and
+ * motor (1) impulses. The next pass matches points by b3ContactID exactly as
+ * b3Manifold::Initialize(old) does (collision.cpp:40-61). */
+int b3g_load_impulses(b3g_ctx* ctx, const float* normal_impulse, const float* tangent_impulse,
+	const float* motor_impulse);
+
+/* Device pointers of the last pass's results for zero-copy consumers:
+ * contacts (3 u32 each) and manifolds (320 bytes each). */
+int b3g_device_results(b3g_ctx* ctx, const void** contacts, const void** manifolds);
+
+/* Stand-alone narrowphase ------------------------------------------------ */
+
+/* Runs the b3Collide* routine of each pair (collision.h:152-202) on the GPU:
+ * for pair i, fixtures fixA[i] / fixB[i] of the current scene, transforms
+ * xfA/xfB (7 floats each) and, for hull pairs, previous transforms xf0A/xf0B
+ * and the feature cache cache4 (read and written back). Writes one b3Manifold
+ * (320 bytes) per pair. Hosts use it to call the narrowphase on their own
+ * pair lists, e.g. for unit checks against the reference's collide functions. */
+int b3g_collide_pairs(b3g_ctx* ctx, uint32_t n, const uint32_t* fixA, const uint32_t* fixB,
+	const float* xfA, const float* xfB, const float* xf0A, const float* xf0B,
+	uint32_t* cache4, void* manifolds);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B3G_H */

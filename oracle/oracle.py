@@ -1,0 +1,246 @@
+"""ctypes driver for the reference build in oracle/_ref (see Makefile and
+ref_harness.cpp).
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's CPU-baseline leg; never by the product.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REFERENCE_SRC = "/root/reference"
+
+# Harness dump records (ref_harness.cpp DumpPoint / DumpManifold / DumpContact).
+DPOINT = np.dtype(
+    [
+        ("n", "<f8", 3),
+        ("p1", "<f8", 3),
+        ("p2", "<f8", 3),
+        ("normalImpulse", "<f8"),
+        ("triangleKey", "<u4"),
+        ("key", "<u4", 4),
+        ("persisting", "<u4"),
+        ("edgeContact", "<u4"),
+        ("pad", "<u4"),
+    ]
+)
+DMANIFOLD = np.dtype(
+    [("pointCount", "<u4"), ("pad", "<u4"), ("tangentImpulse", "<f8", 2), ("motorImpulse", "<f8"), ("points", DPOINT, 4)]
+)
+DCONTACT = np.dtype(
+    [
+        ("fixtureA", "<u4"),
+        ("fixtureB", "<u4"),
+        ("flags", "<u4"),
+        ("manifoldCount", "<u4"),
+        ("cache", "<u4", 4),
+        ("manifolds", DMANIFOLD, 3),
+    ]
+)
+
+
+def build(quiet=True):
+    """Compile oracle/_ref from the reference sources (needs /root/reference)."""
+    if not os.path.isdir(REFERENCE_SRC):
+        return False
+    cmd = ["make", "-C", HERE, "-j8", f"REF={REFERENCE_SRC}"]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
+    return True
+
+
+def available(precision=32):
+    return os.path.exists(os.path.join(REF_DIR, f"libb3ref{precision}.so"))
+
+
+_libs = {}
+
+
+def lib(precision=32):
+    if precision in _libs:
+        return _libs[precision]
+    path = os.path.join(REF_DIR, f"libb3ref{precision}.so")
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} missing: build the oracle with make -C oracle")
+    L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+    vp, u32p, f32p, f64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "refh_create": ([ctypes.c_uint32, u32p, f32p, u32p, u32p, f32p, f32p], vp),
+        "refh_destroy": ([vp], None),
+        "refw_create": (
+            [vp, ctypes.c_uint32, u32p, f32p, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, ctypes.c_uint32],
+            vp,
+        ),
+        "refw_destroy": ([vp], None),
+        "refw_get_bodies": ([vp, f32p], None),
+        "refw_set_sweeps": ([vp, f32p], None),
+        "refw_set_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
+        "refw_set_convex_cache": ([ctypes.c_uint32], None),
+        "refw_first_pass": ([vp, f64p], None),
+        "refw_pass": ([vp, f64p], None),
+        "refw_contact_count": ([vp], ctypes.c_uint32),
+        "refw_touching_count": ([vp, u32p, u32p], ctypes.c_uint32),
+        "refw_fat_aabbs": ([vp, f32p], None),
+        "refw_proxy_ids": ([vp, u32p], None),
+        "refw_dump_pairs": ([vp, u32p], ctypes.c_uint32),
+        "refw_dump_contacts": ([vp, ctypes.c_uint32, ctypes.c_uint32, vp], ctypes.c_uint32),
+        "refw_load_impulses": ([vp, vp], None),
+        "ref_sizeof_dump_contact": ([], ctypes.c_uint32),
+        "ref_sizeof_scalar": ([], ctypes.c_uint32),
+        "ref_collide": (
+            [vp, ctypes.c_uint32, f32p, ctypes.c_uint32, ctypes.c_uint32, f32p, ctypes.c_uint32, f32p, f32p, f32p, f32p,
+             u32p, vp],
+            ctypes.c_int,
+        ),
+        "ref_sweep_xf0": ([f32p, f32p, f32p, f32p, f32p], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    assert L.ref_sizeof_dump_contact() == DCONTACT.itemsize, "dump layout mismatch"
+    _libs[precision] = L
+    return L
+
+
+def _p(a, t):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+class RefHulls:
+    def __init__(self, hull_arrays, precision=32):
+        self.L = lib(precision)
+        h = hull_arrays
+        self._keep = h
+        nh = len(h["desc"]) // 6
+        self.h = self.L.refh_create(
+            nh, _p(h["desc"], ctypes.c_uint32), _p(h["verts"], ctypes.c_float), _p(h["edges"], ctypes.c_uint32),
+            _p(h["faces"], ctypes.c_uint32), _p(h["planes"], ctypes.c_float), _p(h["centroids"], ctypes.c_float),
+        )
+
+    def __del__(self):
+        try:
+            self.L.refh_destroy(self.h)
+        except Exception:
+            pass
+
+
+class RefWorld:
+    """One reference b3World built from a bounce_b200.scene.Scene."""
+
+    def __init__(self, scene, precision=32, warm_starting=True, hulls=None):
+        self.L = lib(precision)
+        self.precision = precision
+        self.scene = scene
+        self.hulls = hulls or RefHulls(scene.hull_arrays, precision)
+        s = scene
+        self.w = self.L.refw_create(
+            self.hulls.h, s.n_bodies, _p(s.body_type, ctypes.c_uint32), _p(s.body_pose, ctypes.c_float),
+            s.n_fixtures, _p(s.fix_body, ctypes.c_uint32), _p(s.fix_type, ctypes.c_uint32),
+            _p(s.fix_hull, ctypes.c_uint32), _p(s.fix_params, ctypes.c_float), _p(s.fix_flags, ctypes.c_uint32),
+            1 if warm_starting else 0,
+        )
+        self.times = np.zeros(2)
+
+    def close(self):
+        if self.w:
+            self.L.refw_destroy(self.w)
+            self.w = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bodies17(self):
+        out = np.zeros(17 * self.scene.n_bodies, np.float32)
+        self.L.refw_get_bodies(self.w, _p(out, ctypes.c_float))
+        return out
+
+    def local_centers(self):
+        return self.bodies17().reshape(-1, 17)[:, 14:17].copy()
+
+    def set_sweeps(self, sweeps14):
+        a = np.ascontiguousarray(sweeps14, np.float32)
+        self.L.refw_set_sweeps(self.w, _p(a, ctypes.c_float))
+
+    def set_awake(self, awake):
+        a = np.ascontiguousarray(awake, np.uint8)
+        self.L.refw_set_awake(self.w, _p(a, ctypes.c_uint8))
+
+    def first_pass(self):
+        t = np.zeros(2)
+        self.L.refw_first_pass(self.w, _p(t, ctypes.c_double))
+        self.times = t
+        return t
+
+    def step_pass(self):
+        t = np.zeros(2)
+        self.L.refw_pass(self.w, _p(t, ctypes.c_double))
+        self.times = t
+        return t
+
+    def contact_count(self):
+        return self.L.refw_contact_count(self.w)
+
+    def touching(self):
+        m, p = ctypes.c_uint32(), ctypes.c_uint32()
+        t = self.L.refw_touching_count(self.w, ctypes.byref(m), ctypes.byref(p))
+        return t, m.value, p.value
+
+    def pairs(self):
+        n = self.contact_count()
+        out = np.zeros((max(n, 1), 3), np.uint32)
+        self.L.refw_dump_pairs(self.w, _p(out, ctypes.c_uint32))
+        return out[:n]
+
+    def contacts(self, start=0, count=None):
+        n = self.contact_count()
+        if count is None:
+            count = n - start
+        out = np.zeros(max(count, 1), DCONTACT)
+        m = self.L.refw_dump_contacts(self.w, start, count, ctypes.c_void_p(out.ctypes.data))
+        return out[:m]
+
+    def fat_aabbs(self):
+        out = np.zeros((self.scene.n_fixtures, 6), np.float32)
+        self.L.refw_fat_aabbs(self.w, _p(out, ctypes.c_float))
+        return out
+
+    def proxy_ids(self):
+        out = np.zeros(self.scene.n_fixtures, np.uint32)
+        self.L.refw_proxy_ids(self.w, _p(out, ctypes.c_uint32))
+        return out
+
+
+def set_convex_cache(on, precision=32):
+    lib(precision).refw_set_convex_cache(1 if on else 0)
+
+
+def collide(hulls, typeA, pA, hullA, typeB, pB, hullB, xfA, xfB, xf0A=None, xf0B=None, cache=None, precision=32):
+    """One b3Collide* call of the reference (ref_collide in ref_harness.cpp)."""
+    L = lib(precision)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    pa, pb = f(np.pad(np.asarray(pA, np.float32), (0, 12 - len(pA)))), f(np.pad(np.asarray(pB, np.float32), (0, 12 - len(pB))))
+    xa, xb = f(xfA), f(xfB)
+    x0a = f(xf0A if xf0A is not None else xfA)
+    x0b = f(xf0B if xf0B is not None else xfB)
+    c = np.ascontiguousarray(cache if cache is not None else np.array([0, 1, 0, 0]), np.uint32)
+    out = np.zeros(1, DMANIFOLD)
+    rc = L.ref_collide(
+        hulls.h, typeA, _p(pa, ctypes.c_float), hullA, typeB, _p(pb, ctypes.c_float), hullB, _p(xa, ctypes.c_float),
+        _p(xb, ctypes.c_float), _p(x0a, ctypes.c_float), _p(x0b, ctypes.c_float), _p(c, ctypes.c_uint32),
+        ctypes.c_void_p(out.ctypes.data),
+    )
+    if rc != 0:
+        raise ValueError("unsupported shape pair")
+    if cache is not None:
+        cache[...] = c
+    return out[0]

@@ -1,0 +1,604 @@
+// Headless driver around the unmodified reference (Bounce) library.
+//
+// TEST INFRASTRUCTURE ONLY: this file is compiled together with the
+// reference's own sources into oracle/_ref/libb3ref{32,64}.so. It is loaded by
+// tests/, by __graft_entry__.smoke() as the checker and by bench.py's CPU
+// baseline leg; the product never links or calls it.
+//
+// It builds a b3World from flat arrays (the same arrays the product's C ABI
+// takes), drives the collision pass exactly as b3World::Step and the tail of
+// b3World::Solve do, and dumps the contact list, manifolds and hull feature
+// caches in a fixed record layout that tests compare against.
+//
+// Reference call sites mirrored here:
+//   first pass   = b3World::Step with dt = 0  (src/bounce/dynamics/world.cpp:201-225)
+//   later passes = "Find New Pairs" block     (world.cpp:424-449) followed by
+//                  b3ContactManager::UpdateContacts (contact_manager.cpp:225-287)
+// Bodies are moved kinematically between passes: the driver writes the sweep
+// (worldCenter0/orientation0 = previous, worldCenter/orientation = current)
+// and lets b3Body::SynchronizeTransform (body.h) derive m_xf, which is what
+// b3Island::Solve leaves behind after integrating positions.
+
+#include <algorithm>
+#include <assert.h>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <float.h>
+#include <new>
+#include <stdarg.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <vector>
+
+// The harness needs the engine's private state (sweeps, the contact manager,
+// the per-body fixture sync). Access specifiers do not change layout.
+#define private public
+#define protected public
+#include <bounce/bounce.h>
+#include <bounce/dynamics/contacts/hull_contact.h>
+#include <bounce/dynamics/contacts/mesh_contact.h>
+#include <bounce/collision/sat/sat.h>
+#undef private
+#undef protected
+
+#define REF_API extern "C" __attribute__((visibility("default")))
+
+// Runtime switch of the hull feature cache (collide_hulls.cpp:27).
+extern bool b3_convexCache;
+
+// ---------------------------------------------------------------------------
+// Fixed dump records (doubles so the FP32 and FP64 builds share one layout).
+
+struct DumpPoint
+{
+	double localNormal1[3];
+	double localPoint1[3];
+	double localPoint2[3];
+	double normalImpulse;
+	uint32_t triangleKey;
+	uint32_t key[4];
+	uint32_t persisting;
+	uint32_t edgeContact;
+	uint32_t pad;
+};
+
+struct DumpManifold
+{
+	uint32_t pointCount;
+	uint32_t pad;
+	double tangentImpulse[2];
+	double motorImpulse;
+	DumpPoint points[4];
+};
+
+struct DumpContact
+{
+	uint32_t fixtureA;
+	uint32_t fixtureB;
+	uint32_t flags;          // bit0 touching
+	uint32_t manifoldCount;
+	uint32_t cache[4];       // hull-hull feature cache: cacheType, featureType, index1, index2
+	DumpManifold manifolds[3];
+};
+
+static void DumpM(DumpManifold* out, const b3Manifold& m)
+{
+	memset(out, 0, sizeof(DumpManifold));
+	out->pointCount = m.pointCount;
+	out->tangentImpulse[0] = m.tangentImpulse.x;
+	out->tangentImpulse[1] = m.tangentImpulse.y;
+	out->motorImpulse = m.motorImpulse;
+	for (uint32 i = 0; i < m.pointCount && i < 4; ++i)
+	{
+		const b3ManifoldPoint& p = m.points[i];
+		DumpPoint* q = out->points + i;
+		for (int k = 0; k < 3; ++k)
+		{
+			q->localNormal1[k] = p.localNormal1[k];
+			q->localPoint1[k] = p.localPoint1[k];
+			q->localPoint2[k] = p.localPoint2[k];
+		}
+		q->normalImpulse = p.normalImpulse;
+		q->triangleKey = p.id.triangleKey;
+		q->key[0] = p.id.key.pair.inEdge1;
+		q->key[1] = p.id.key.pair.outEdge1;
+		q->key[2] = p.id.key.pair.inEdge2;
+		q->key[3] = p.id.key.pair.outEdge2;
+		q->persisting = p.persisting ? 1 : 0;
+		q->edgeContact = p.edgeContact ? 1 : 0;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Hull pool: b3Hull views over flat arrays.
+//   desc[6*h] = vertexOffset, vertexCount, edgeOffset, edgeCount, faceOffset, faceCount
+//   edges: 5 u32 per half-edge (origin, twin, face, prev, next), hull-local
+//   planes: 4 floats per face (normal xyz, offset)
+
+struct HullPool
+{
+	std::vector<b3Hull> hulls;
+	std::vector<b3Vec3> verts;
+	std::vector<b3HalfEdge> edges;
+	std::vector<b3Face> faces;
+	std::vector<b3Plane> planes;
+};
+
+REF_API void* refh_create(uint32_t nh, const uint32_t* desc, const float* hv, const uint32_t* he,
+	const uint32_t* hf, const float* hp, const float* hc)
+{
+	HullPool* pool = new HullPool;
+	uint32_t nv = 0, ne = 0, nf = 0;
+	for (uint32_t h = 0; h < nh; ++h)
+	{
+		nv = std::max(nv, desc[6 * h + 0] + desc[6 * h + 1]);
+		ne = std::max(ne, desc[6 * h + 2] + desc[6 * h + 3]);
+		nf = std::max(nf, desc[6 * h + 4] + desc[6 * h + 5]);
+	}
+	pool->verts.resize(nv);
+	pool->edges.resize(ne);
+	pool->faces.resize(nf);
+	pool->planes.resize(nf);
+	for (uint32_t i = 0; i < nv; ++i)
+		pool->verts[i].Set(hv[3 * i + 0], hv[3 * i + 1], hv[3 * i + 2]);
+	for (uint32_t i = 0; i < ne; ++i)
+		pool->edges[i] = b3MakeEdge(he[5 * i + 0], he[5 * i + 1], he[5 * i + 2], he[5 * i + 3], he[5 * i + 4]);
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		pool->faces[i].edge = hf[i];
+		pool->planes[i].normal.Set(hp[4 * i + 0], hp[4 * i + 1], hp[4 * i + 2]);
+		pool->planes[i].offset = hp[4 * i + 3];
+	}
+	pool->hulls.resize(nh);
+	for (uint32_t h = 0; h < nh; ++h)
+	{
+		b3Hull& H = pool->hulls[h];
+		H.centroid.Set(hc[3 * h + 0], hc[3 * h + 1], hc[3 * h + 2]);
+		H.vertexCount = desc[6 * h + 1];
+		H.vertices = pool->verts.data() + desc[6 * h + 0];
+		H.edgeCount = desc[6 * h + 3];
+		H.edges = pool->edges.data() + desc[6 * h + 2];
+		H.faceCount = desc[6 * h + 5];
+		H.faces = pool->faces.data() + desc[6 * h + 4];
+		H.planes = pool->planes.data() + desc[6 * h + 4];
+	}
+	return pool;
+}
+
+REF_API void refh_destroy(void* p)
+{
+	delete (HullPool*)p;
+}
+
+// ---------------------------------------------------------------------------
+// Shapes from fixture parameters.
+//   type 0 sphere:   p[0..2] center, p[3] radius
+//   type 1 capsule:  p[0..2] vertex1, p[3..5] vertex2, p[6] radius
+//   type 2 triangle: p[0..8] vertices, p[9] radius
+//   type 3 hull:     p[0] radius (B3_HULL_RADIUS when the shape keeps its default)
+
+struct ShapeStore
+{
+	b3SphereShape sphere;
+	b3CapsuleShape capsule;
+	b3TriangleShape triangle;
+	b3HullShape hull;
+};
+
+static const b3Shape* MakeShape(ShapeStore& s, uint32_t type, const float* p, uint32_t hullIndex, const HullPool* pool)
+{
+	switch (type)
+	{
+	case 0:
+		s.sphere.m_center.Set(p[0], p[1], p[2]);
+		s.sphere.m_radius = p[3];
+		return &s.sphere;
+	case 1:
+		s.capsule.m_vertex1.Set(p[0], p[1], p[2]);
+		s.capsule.m_vertex2.Set(p[3], p[4], p[5]);
+		s.capsule.m_radius = p[6];
+		return &s.capsule;
+	case 2:
+		s.triangle.Set(b3Vec3(p[0], p[1], p[2]), b3Vec3(p[3], p[4], p[5]), b3Vec3(p[6], p[7], p[8]));
+		s.triangle.m_radius = p[9];
+		return &s.triangle;
+	case 3:
+		s.hull.m_hull = &pool->hulls[hullIndex];
+		s.hull.m_radius = p[0];
+		return &s.hull;
+	default:
+		return nullptr;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// World.
+
+struct RefWorld
+{
+	b3World* world;
+	std::vector<b3Body*> bodies;
+	std::vector<b3Fixture*> fixtures;
+	const HullPool* pool;
+	double tFind;
+	double tUpdate;
+};
+
+static inline double Now()
+{
+	return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// body_pose: 7 floats per body (position xyz, quaternion xyzw)
+// fix_flags: bit0 sensor
+REF_API void* refw_create(void* hullPool, uint32_t nb, const uint32_t* bodyType, const float* bodyPose,
+	uint32_t nf, const uint32_t* fixBody, const uint32_t* fixType, const uint32_t* fixHull,
+	const float* fixParams, const uint32_t* fixFlags, uint32_t warmStarting)
+{
+	RefWorld* w = new RefWorld;
+	w->pool = (const HullPool*)hullPool;
+	w->world = new b3World();
+	w->world->SetGravity(b3Vec3(0, 0, 0));
+	w->world->SetSleeping(false);
+	w->world->SetWarmStarting(warmStarting != 0);
+	w->tFind = 0;
+	w->tUpdate = 0;
+	for (uint32_t i = 0; i < nb; ++i)
+	{
+		b3BodyDef bd;
+		bd.type = (b3BodyType)bodyType[i];
+		bd.position.Set(bodyPose[7 * i + 0], bodyPose[7 * i + 1], bodyPose[7 * i + 2]);
+		bd.orientation.v.Set(bodyPose[7 * i + 3], bodyPose[7 * i + 4], bodyPose[7 * i + 5]);
+		bd.orientation.s = bodyPose[7 * i + 6];
+		bd.allowSleep = false;
+		bd.awake = true;
+		w->bodies.push_back(w->world->CreateBody(bd));
+	}
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		ShapeStore store;
+		const b3Shape* shape = MakeShape(store, fixType[i], fixParams + 12 * i, fixHull[i], w->pool);
+		b3FixtureDef fd;
+		fd.shape = shape;
+		fd.density = bodyType[fixBody[i]] == e_dynamicBody ? scalar(1) : scalar(0);
+		fd.isSensor = (fixFlags[i] & 1) != 0;
+		fd.userData = (void*)(uintptr_t)i;
+		w->fixtures.push_back(w->bodies[fixBody[i]]->CreateFixture(fd));
+	}
+	return w;
+}
+
+REF_API void refw_destroy(void* p)
+{
+	RefWorld* w = (RefWorld*)p;
+	delete w->world;
+	delete w;
+}
+
+// 17 floats per body: xf.translation(3), xf.rotation(xyzw 4), sweep.worldCenter0(3),
+// sweep.orientation0(4), sweep.localCenter(3)
+REF_API void refw_get_bodies(void* p, float* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		const b3Body* b = w->bodies[i];
+		float* o = out + 17 * i;
+		o[0] = (float)b->m_xf.translation.x; o[1] = (float)b->m_xf.translation.y; o[2] = (float)b->m_xf.translation.z;
+		o[3] = (float)b->m_xf.rotation.v.x; o[4] = (float)b->m_xf.rotation.v.y; o[5] = (float)b->m_xf.rotation.v.z;
+		o[6] = (float)b->m_xf.rotation.s;
+		o[7] = (float)b->m_sweep.worldCenter0.x; o[8] = (float)b->m_sweep.worldCenter0.y; o[9] = (float)b->m_sweep.worldCenter0.z;
+		o[10] = (float)b->m_sweep.orientation0.v.x; o[11] = (float)b->m_sweep.orientation0.v.y;
+		o[12] = (float)b->m_sweep.orientation0.v.z; o[13] = (float)b->m_sweep.orientation0.s;
+		o[14] = (float)b->m_sweep.localCenter.x; o[15] = (float)b->m_sweep.localCenter.y; o[16] = (float)b->m_sweep.localCenter.z;
+	}
+}
+
+// 14 floats per body: worldCenter0(3), orientation0(4), worldCenter(3), orientation(4).
+// Static bodies are skipped (their sweep never changes in the reference).
+REF_API void refw_set_sweeps(void* p, const float* in)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		b3Body* b = w->bodies[i];
+		if (b->m_type == e_staticBody)
+			continue;
+		const float* s = in + 14 * i;
+		b->m_sweep.worldCenter0.Set(s[0], s[1], s[2]);
+		b->m_sweep.orientation0.v.Set(s[3], s[4], s[5]);
+		b->m_sweep.orientation0.s = s[6];
+		b->m_sweep.worldCenter.Set(s[7], s[8], s[9]);
+		b->m_sweep.orientation.v.Set(s[10], s[11], s[12]);
+		b->m_sweep.orientation.s = s[13];
+		b->SynchronizeTransform();
+	}
+}
+
+// Awake flags per body (1 awake, 0 asleep).
+REF_API void refw_set_awake(void* p, const uint8_t* awake)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		b3Body* b = w->bodies[i];
+		if (awake[i])
+			b->m_flags |= b3Body::e_awakeFlag;
+		else
+			b->m_flags &= ~b3Body::e_awakeFlag;
+	}
+}
+
+REF_API void refw_set_convex_cache(uint32_t on)
+{
+	b3_convexCache = on != 0;
+}
+
+// The first collision pass of a fresh world: b3World::Step(0, ...) runs
+// FindNewContacts (m_newContacts is set by CreateFixture) then UpdateContacts.
+REF_API void refw_first_pass(void* p, double* times)
+{
+	RefWorld* w = (RefWorld*)p;
+	double t0 = Now();
+	if (w->world->m_newContacts)
+	{
+		w->world->m_contactManager.FindNewContacts();
+		w->world->m_newContacts = false;
+	}
+	double t1 = Now();
+	w->world->m_contactManager.UpdateContacts();
+	double t2 = Now();
+	times[0] = t1 - t0;
+	times[1] = t2 - t1;
+}
+
+// One later collision pass after the driver has moved the bodies: the
+// "Find New Pairs" block of b3World::Solve, then the next step's UpdateContacts.
+REF_API void refw_pass(void* p, double* times)
+{
+	RefWorld* w = (RefWorld*)p;
+	b3World* world = w->world;
+	double t0 = Now();
+	for (b3Body* b = world->m_bodyList; b; b = b->m_next)
+	{
+		if (b->GetType() == e_staticBody)
+			continue;
+		if (!b->IsAwake())
+			continue;
+		b->SynchronizeFixtures();
+	}
+	world->m_contactManager.SynchronizeFixtures();
+	world->m_contactManager.FindNewContacts();
+	double t1 = Now();
+	world->m_contactManager.UpdateContacts();
+	double t2 = Now();
+	times[0] = t1 - t0;
+	times[1] = t2 - t1;
+}
+
+REF_API uint32_t refw_contact_count(void* p)
+{
+	return ((RefWorld*)p)->world->m_contactManager.m_contactCount;
+}
+
+REF_API uint32_t refw_touching_count(void* p, uint32_t* manifolds, uint32_t* points)
+{
+	RefWorld* w = (RefWorld*)p;
+	uint32_t touching = 0, nm = 0, np = 0;
+	for (b3Contact* c = w->world->m_contactManager.m_contactList; c; c = c->m_next)
+	{
+		if (c->IsTouching())
+			++touching;
+		for (uint32 i = 0; i < c->m_manifoldCount; ++i)
+		{
+			if (c->m_manifolds[i].pointCount > 0)
+			{
+				++nm;
+				np += c->m_manifolds[i].pointCount;
+			}
+		}
+	}
+	if (manifolds) *manifolds = nm;
+	if (points) *points = np;
+	return touching;
+}
+
+// Fat AABBs of every fixture proxy, 6 floats each (lower xyz, upper xyz).
+REF_API void refw_fat_aabbs(void* p, float* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	const b3BroadPhase& bp = w->world->m_contactManager.m_broadPhase;
+	for (size_t i = 0; i < w->fixtures.size(); ++i)
+	{
+		const b3AABB& a = bp.GetFatAABB(w->fixtures[i]->m_proxyId);
+		out[6 * i + 0] = (float)a.lowerBound.x; out[6 * i + 1] = (float)a.lowerBound.y; out[6 * i + 2] = (float)a.lowerBound.z;
+		out[6 * i + 3] = (float)a.upperBound.x; out[6 * i + 4] = (float)a.upperBound.y; out[6 * i + 5] = (float)a.upperBound.z;
+	}
+}
+
+REF_API void refw_proxy_ids(void* p, uint32_t* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->fixtures.size(); ++i)
+		out[i] = w->fixtures[i]->m_proxyId;
+}
+
+static void DumpOne(DumpContact* d, const b3Contact* c)
+{
+	memset(d, 0, sizeof(DumpContact));
+	d->fixtureA = (uint32_t)(uintptr_t)c->m_fixtureA->m_userData;
+	d->fixtureB = (uint32_t)(uintptr_t)c->m_fixtureB->m_userData;
+	d->flags = c->IsTouching() ? 1 : 0;
+	d->manifoldCount = c->m_manifoldCount;
+	d->cache[0] = d->cache[1] = d->cache[2] = d->cache[3] = 0xFFFFFFFFu;
+	if (c->m_fixtureA->GetType() == b3Shape::e_hull && c->m_fixtureB->GetType() == b3Shape::e_hull)
+	{
+		const b3HullContact* hc = (const b3HullContact*)c;
+		d->cache[0] = (uint32_t)hc->m_cache.cacheType;
+		d->cache[1] = (uint32_t)hc->m_cache.featureType;
+		d->cache[2] = hc->m_cache.index1;
+		d->cache[3] = hc->m_cache.index2;
+	}
+	for (uint32 i = 0; i < c->m_manifoldCount && i < 3; ++i)
+		DumpM(d->manifolds + i, c->m_manifolds[i]);
+}
+
+// Pairs in contact-list order: 3 u32 per contact (fixtureA, fixtureB, flags | manifoldCount << 8).
+REF_API uint32_t refw_dump_pairs(void* p, uint32_t* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	uint32_t n = 0;
+	for (b3Contact* c = w->world->m_contactManager.m_contactList; c; c = c->m_next, ++n)
+	{
+		out[3 * n + 0] = (uint32_t)(uintptr_t)c->m_fixtureA->m_userData;
+		out[3 * n + 1] = (uint32_t)(uintptr_t)c->m_fixtureB->m_userData;
+		out[3 * n + 2] = (c->IsTouching() ? 1u : 0u) | (c->m_manifoldCount << 8);
+	}
+	return n;
+}
+
+// Full records for contacts [start, start + count) of the contact list.
+REF_API uint32_t refw_dump_contacts(void* p, uint32_t start, uint32_t count, void* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	uint32_t i = 0, n = 0;
+	for (b3Contact* c = w->world->m_contactManager.m_contactList; c && n < count; c = c->m_next, ++i)
+	{
+		if (i < start)
+			continue;
+		DumpOne((DumpContact*)out + n, c);
+		++n;
+	}
+	return n;
+}
+
+// Overwrite the warm-start state of every contact's manifolds (as the solver
+// would leave it): per contact in list order, per manifold point, the normal
+// impulse; per manifold the tangent and motor impulses. Records as dumped.
+REF_API void refw_load_impulses(void* p, const void* in)
+{
+	RefWorld* w = (RefWorld*)p;
+	const DumpContact* d = (const DumpContact*)in;
+	for (b3Contact* c = w->world->m_contactManager.m_contactList; c; c = c->m_next, ++d)
+	{
+		for (uint32 i = 0; i < c->m_manifoldCount && i < 3; ++i)
+		{
+			b3Manifold& m = c->m_manifolds[i];
+			m.tangentImpulse.x = (scalar)d->manifolds[i].tangentImpulse[0];
+			m.tangentImpulse.y = (scalar)d->manifolds[i].tangentImpulse[1];
+			m.motorImpulse = (scalar)d->manifolds[i].motorImpulse;
+			for (uint32 k = 0; k < m.pointCount && k < 4; ++k)
+				m.points[k].normalImpulse = (scalar)d->manifolds[i].points[k].normalImpulse;
+		}
+	}
+}
+
+// Layout of b3ManifoldPoint / b3Manifold (collision.h:97-128) for checking the
+// device records: sizes and field offsets.
+REF_API void ref_manifold_layout(uint32_t* out)
+{
+	out[0] = (uint32_t)sizeof(b3ManifoldPoint);
+	out[1] = (uint32_t)offsetof(b3ManifoldPoint, localNormal1);
+	out[2] = (uint32_t)offsetof(b3ManifoldPoint, localPoint1);
+	out[3] = (uint32_t)offsetof(b3ManifoldPoint, localPoint2);
+	out[4] = (uint32_t)offsetof(b3ManifoldPoint, normalImpulse);
+	out[5] = (uint32_t)offsetof(b3ManifoldPoint, id);
+	out[6] = (uint32_t)(offsetof(b3ManifoldPoint, id) + offsetof(b3ContactID, key));
+	out[7] = (uint32_t)offsetof(b3ManifoldPoint, persisting);
+	out[8] = (uint32_t)offsetof(b3ManifoldPoint, edgeContact);
+	out[9] = (uint32_t)sizeof(b3Manifold);
+	out[10] = (uint32_t)offsetof(b3Manifold, pointCount);
+	out[11] = (uint32_t)offsetof(b3Manifold, tangentImpulse);
+	out[12] = (uint32_t)offsetof(b3Manifold, motorImpulse);
+	out[13] = (uint32_t)offsetof(b3Manifold, motorSpeed);
+	out[14] = (uint32_t)offsetof(b3Manifold, tangentSpeed1);
+	out[15] = (uint32_t)offsetof(b3Manifold, tangentSpeed2);
+}
+
+REF_API uint32_t ref_sizeof_dump_contact() { return (uint32_t)sizeof(DumpContact); }
+REF_API uint32_t ref_sizeof_scalar() { return (uint32_t)sizeof(scalar); }
+
+// ---------------------------------------------------------------------------
+// Direct calls of the b3Collide* routines (collision.h:152-202) for unit-level
+// checks. xf: 7 floats (translation xyz, rotation xyzw). cache4 (hull-hull
+// only) is read and written back. xf0 is the previous-step transform used by
+// the hull feature cache (hull_contact.cpp:43-44).
+
+static b3Transform MakeXf(const float* x)
+{
+	b3Transform xf;
+	xf.translation.Set(x[0], x[1], x[2]);
+	xf.rotation.v.Set(x[3], x[4], x[5]);
+	xf.rotation.s = x[6];
+	return xf;
+}
+
+REF_API int ref_collide(void* hullPool, uint32_t typeA, const float* pA, uint32_t hullA,
+	uint32_t typeB, const float* pB, uint32_t hullB, const float* xfA, const float* xfB,
+	const float* xf0A, const float* xf0B, uint32_t* cache4, void* out)
+{
+	const HullPool* pool = (const HullPool*)hullPool;
+	ShapeStore sa, sb;
+	const b3Shape* A = MakeShape(sa, typeA, pA, hullA, pool);
+	const b3Shape* B = MakeShape(sb, typeB, pB, hullB, pool);
+	b3Transform XA = MakeXf(xfA), XB = MakeXf(xfB);
+	b3Manifold m;
+	m.Initialize();
+	int rc = 0;
+	if (typeA == 0 && typeB == 0)
+		b3CollideSpheres(m, XA, (const b3SphereShape*)A, XB, (const b3SphereShape*)B);
+	else if (typeA == 1 && typeB == 0)
+		b3CollideCapsuleAndSphere(m, XA, (const b3CapsuleShape*)A, XB, (const b3SphereShape*)B);
+	else if (typeA == 1 && typeB == 1)
+		b3CollideCapsules(m, XA, (const b3CapsuleShape*)A, XB, (const b3CapsuleShape*)B);
+	else if (typeA == 2 && typeB == 0)
+		b3CollideTriangleAndSphere(m, XA, (const b3TriangleShape*)A, XB, (const b3SphereShape*)B);
+	else if (typeA == 2 && typeB == 1)
+		b3CollideTriangleAndCapsule(m, XA, (const b3TriangleShape*)A, XB, (const b3CapsuleShape*)B);
+	else if (typeA == 3 && typeB == 0)
+		b3CollideHullAndSphere(m, XA, (const b3HullShape*)A, XB, (const b3SphereShape*)B);
+	else if (typeA == 3 && typeB == 1)
+		b3CollideHullAndCapsule(m, XA, (const b3HullShape*)A, XB, (const b3CapsuleShape*)B);
+	else if (typeA == 3 && typeB == 2)
+		b3CollideHullAndTriangle(m, XA, (const b3HullShape*)A, XB, (const b3TriangleShape*)B);
+	else if (typeA == 3 && typeB == 3)
+	{
+		b3FeatureCache cache;
+		cache.cacheType = (b3CacheType)cache4[0];
+		cache.featureType = (b3FeatureType)cache4[1];
+		cache.index1 = cache4[2];
+		cache.index2 = cache4[3];
+		b3CollideHulls(m, XA, (const b3HullShape*)A, XB, (const b3HullShape*)B, cache, MakeXf(xf0A), MakeXf(xf0B));
+		cache4[0] = (uint32_t)cache.cacheType;
+		cache4[1] = (uint32_t)cache.featureType;
+		cache4[2] = cache.index1;
+		cache4[3] = cache.index2;
+	}
+	else
+		rc = -1;
+	DumpM((DumpManifold*)out, m);
+	return rc;
+}
+
+// b3Sweep::GetTransform(0) (sweep.h:43-63) for checking the device's xf0.
+REF_API void ref_sweep_xf0(const float* c0, const float* q0, const float* q, const float* lc, float* out)
+{
+	b3Sweep s;
+	s.worldCenter0.Set(c0[0], c0[1], c0[2]);
+	s.orientation0.v.Set(q0[0], q0[1], q0[2]);
+	s.orientation0.s = q0[3];
+	s.worldCenter = s.worldCenter0;
+	s.orientation.v.Set(q[0], q[1], q[2]);
+	s.orientation.s = q[3];
+	s.localCenter.Set(lc[0], lc[1], lc[2]);
+	s.t0 = 0;
+	b3Transform xf = s.GetTransform(scalar(0));
+	out[0] = (float)xf.translation.x; out[1] = (float)xf.translation.y; out[2] = (float)xf.translation.z;
+	out[3] = (float)xf.rotation.v.x; out[4] = (float)xf.rotation.v.y; out[5] = (float)xf.rotation.v.z;
+	out[6] = (float)xf.rotation.s;
+}

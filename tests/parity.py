@@ -1,0 +1,69 @@
+"""Comparison helpers: pipeline results vs reference dumps (test infrastructure)."""
+import numpy as np
+
+
+def keys(a, b):
+    return (np.asarray(a, np.uint64) << np.uint64(32)) | np.asarray(b, np.uint64)
+
+
+def compare_contacts(pipe, rw, label="", check_cache=True):
+    """Contact set, touching flags, manifolds and hull feature caches must be
+    identical (bit for bit) between the pipeline and the FP32 reference."""
+    g = pipe.contacts()
+    r = rw.pairs()
+    gk, rk = keys(g[:, 0], g[:, 1]), keys(r[:, 0], r[:, 1])
+    gs, rs = np.sort(gk), np.sort(rk)
+    if not np.array_equal(gs, rs):
+        only_g = np.setdiff1d(gs, rs)
+        only_r = np.setdiff1d(rs, gs)
+        raise AssertionError(
+            f"{label}: contact sets differ: gpu {len(gs)} ref {len(rs)}; "
+            f"gpu-only {[(int(k >> 32), int(k & 0xFFFFFFFF)) for k in only_g[:5]]} "
+            f"ref-only {[(int(k >> 32), int(k & 0xFFFFFFFF)) for k in only_r[:5]]}"
+        )
+    gi = np.argsort(gk)
+    rc = rw.contacts()
+    ri = np.argsort(keys(rc["fixtureA"], rc["fixtureB"]))
+    gt = g[gi, 2] & 1
+    rt = rc["flags"][ri] & 1
+    bad = np.nonzero(gt != rt)[0]
+    assert len(bad) == 0, f"{label}: touching flags differ at {len(bad)} contacts, e.g. {gk[gi][bad[:3]]}"
+    gm = pipe.manifolds()[gi]
+    rm = rc["manifolds"][ri, 0]
+    rcount = rc["manifoldCount"][ri]
+    gcount = (g[gi, 2] >> 8) & 0xFF
+    assert np.array_equal(gcount, rcount), f"{label}: manifold counts differ"
+    gpc = np.where(gcount > 0, gm["pointCount"], 0)
+    rpc = np.where(rcount > 0, rm["pointCount"], 0)
+    badpc = np.nonzero(gpc != rpc)[0]
+    assert len(badpc) == 0, (
+        f"{label}: point counts differ at {len(badpc)} of {len(gpc)} contacts; first "
+        f"{[(int(gk[gi][i] >> 32), int(gk[gi][i] & 0xFFFFFFFF), int(gpc[i]), int(rpc[i])) for i in badpc[:5]]}"
+    )
+    mask = np.arange(4)[None, :] < gpc[:, None]
+    for f in ("n", "p1", "p2"):
+        a = gm["points"][f][mask]
+        b = rm["points"][f][mask].astype(np.float32)
+        bad = np.nonzero(~np.all(a == b, axis=-1))[0]
+        assert len(bad) == 0, f"{label}: manifold field {f} differs at {len(bad)} points; e.g. {a[bad[:2]]} vs {b[bad[:2]]}"
+    assert np.array_equal(gm["points"]["key"][mask], rm["points"]["key"][mask]), f"{label}: feature ids differ"
+    assert np.array_equal(gm["points"]["triangleKey"][mask], rm["points"]["triangleKey"][mask])
+    assert np.array_equal(gm["points"]["edgeContact"][mask], rm["points"]["edgeContact"][mask].astype(np.uint8))
+    assert np.array_equal(gm["points"]["persisting"][mask], rm["points"]["persisting"][mask].astype(np.uint8)), (
+        f"{label}: persisting flags differ"
+    )
+    assert np.array_equal(gm["points"]["normalImpulse"][mask], rm["points"]["normalImpulse"][mask].astype(np.float32))
+    if check_cache:
+        gc = pipe.caches()[gi]
+        rcache = rc["cache"][ri]
+        hh = rcache[:, 0] != 0xFFFFFFFF
+        bad = np.nonzero(~np.all(gc[hh] == rcache[hh], axis=1))[0]
+        assert len(bad) == 0, f"{label}: feature caches differ at {len(bad)}: {gc[hh][bad[:3]]} vs {rcache[hh][bad[:3]]}"
+    return dict(contacts=len(gs), touching=int(gt.sum()), points=int(gpc.sum()))
+
+
+def compare_fat_aabbs(pipe, rw, label=""):
+    a = pipe.fat_aabbs()
+    b = rw.fat_aabbs()
+    bad = np.nonzero(~np.all(a == b, axis=1))[0]
+    assert len(bad) == 0, f"{label}: fat AABBs differ at {len(bad)} proxies, e.g. {a[bad[:2]]} vs {b[bad[:2]]}"
