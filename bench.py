@@ -1,0 +1,375 @@
+"""Benchmark: one collision pass per step of the 65,536-body mixed world.
+
+Workload: one world of 65,536 bodies (40 % spheres r ~ U[0.2, 1] m, 30 %
+capsules r ~ U[0.1, 0.5] m, half-height ~ U[0.2, 1] m, 30 % quickhull-style
+hulls of 8-32 points on ellipsoids with semi-axes ~ U[0.3, 1.2] m) in a 49 m
+cube, linear velocities N(0, 1) m/s, angular N(0, 1) rad/s, seeded; bodies
+move kinematically between passes (dt = 1/60 s). A step is one collision pass:
+fat-AABB update, broadphase, contact begin/end, narrowphase manifolds (the
+"Find New Pairs" block and UpdateContacts of b3World::Step).
+
+Metric: manifolds/s = manifolds with at least one point produced per second.
+`value` times passes with the body state already in HBM; `e2e` times the same
+through the C ABI with host buffers (host->device state copy, device->host
+contact list and touching manifolds every step). The reference arm
+(--impl reference) runs the reference's own CPU pipeline (oracle/_ref, the
+unmodified Bounce sources) on the same scene and body motion.
+
+Multi-GPU: replicas only (independent worlds per GPU, no collective); value is
+the sum over ranks divided by the max time over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BODIES = 65536
+SIDE = 49.0
+SEED = 2
+WORKLOAD = "one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% hull 8-32 pts), 49 m cube, kinematic motion"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--bodies", type=int, default=N_BODIES)
+    ap.add_argument("--e2e-steps", type=int, default=60)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-stages", action="store_true", default=True)
+    return ap.parse_args()
+
+
+def dist_init(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    return rank, world, local, dist
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(mx)) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def build_scene(n, seed):
+    from bounce_b200 import scene as S
+
+    return S.mixed_scene(seed=seed, n=n, side=SIDE * (n / N_BODIES) ** (1.0 / 3.0)).finalize()
+
+
+def config_dict(args, extra=None):
+    d = {"workload": WORKLOAD, "bodies": args.bodies, "proxies": args.bodies, "dt": 1.0 / 60.0,
+         "passes_timed": args.steps, "warmup_passes": args.warmup,
+         "l2": "inputs larger than L2: per-pass contact state (two 320 B manifolds per contact) exceeds 126 MB",
+         "parallelism": f"replicas x{args.gpus}"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU pipeline (oracle/_ref): the CPU baseline leg and --impl reference.
+
+
+def reference_run(scene, passes, seconds_cap=None, warmup=0):
+    """Runs the reference's collision pass on the CPU: creation pass, `warmup`
+    untimed passes, then up to `passes` timed passes (stopping early once
+    seconds_cap of measured time is spent). Returns (manifolds, seconds, passes)."""
+    from bounce_b200 import scene as S
+    from oracle import oracle as O
+
+    if not O.available(32):
+        raise RuntimeError("oracle/_ref/libb3ref32.so not built")
+    rw = O.RefWorld(scene)
+    scene.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(scene)
+    rw.first_pass()
+    for _ in range(warmup):
+        drv.advance()
+        rw.set_sweeps(drv.sweeps14())
+        rw.step_pass()
+    total_m, total_t, done = 0, 0.0, 0
+    for _ in range(passes):
+        drv.advance()
+        rw.set_sweeps(drv.sweeps14())
+        t = rw.step_pass()
+        total_t += float(t[0] + t[1])
+        total_m += rw.touching()[1]
+        done += 1
+        if seconds_cap is not None and total_t >= seconds_cap:
+            break
+    rw.close()
+    return total_m, total_t, done
+
+
+def run_reference_arm(args, rank, world, dist):
+    if rank != 0:
+        return
+    scene = build_scene(args.bodies, SEED)
+    m, t, done = reference_run(scene, args.steps, warmup=args.warmup)
+    v = m / t if t > 0 else 0.0
+    line = {
+        "metric": "manifolds/s", "value": v, "unit": "manifolds/s", "n_gpus": args.gpus, "steps": done,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t / max(done, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_dict(args), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "manifolds/s", "cores": 1, "kind": "reference",
+                         "sample": f"{done} passes of the full workload on 1 host core (the reference is single-threaded)"},
+        "e2e": {"value": v, "unit": "manifolds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+
+
+def algorithmic_bytes(scene, counts):
+    """Algorithmic HBM bytes of one pass's broadphase front end (the sync
+    stage): per proxy the body state (68 B), fixture record (60 B), old and new
+    fat AABB (2 x 32 B) and moved flag, plus each hull's local vertices once
+    (16 B each, float4)."""
+    ha = scene.hull_arrays
+    desc = ha["desc"].reshape(-1, 6)
+    hull_fix = scene.fix_type == 3
+    hv = desc[scene.fix_hull[hull_fix], 1].sum() * 16
+    return int(scene.n_fixtures * (68 + 60 + 64 + 1) + hv)
+
+
+def run_ours(args, rank, world, local, dist):
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+    from bounce_b200 import scene as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene = build_scene(args.bodies, SEED + rank)
+    drv = S.KinematicDriver(scene)
+    total = 1 + args.warmup + args.steps + args.e2e_steps
+    nb = scene.n_bodies
+    states = np.empty((total, 17 * nb), np.float32)
+    states[0] = drv.state17()
+    for k in range(1, total):
+        drv.advance()
+        states[k] = drv.state17()
+    d_states = torch.from_numpy(states[: 1 + args.warmup + args.steps]).to(dev)
+    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    row = 17 * nb * 4
+    base = d_states.data_ptr()
+
+    # creation pass + warm-up
+    with torch.cuda.stream(stream):
+        for k in range(0, 1 + args.warmup):
+            pipe.collide(base + k * row, on_device=True, stream=sptr)
+    stream.synchronize()
+    c = pipe.counts()
+    assert c["status"] == 0, c
+    pipe.totals(reset=True)
+    if args.profile_stages:
+        pipe.set_profiling(True)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(1 + args.warmup, 1 + args.warmup + args.steps):
+        pipe.collide(base + k * row, on_device=True, stream=sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    tot = pipe.totals()
+    prof = pipe.profile() if args.profile_stages else {}
+    pipe.set_profiling(False)
+    c = pipe.counts()
+    assert c["status"] == 0, c
+
+    ms_max = ms
+    manifolds_all = tot["manifolds"]
+    if dist is not None:
+        t = torch.tensor([ms, float(tot["manifolds"])], device=dev, dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms_max = float(tmax[0])
+        manifolds_all = float(tsum[1])
+    value = manifolds_all / (ms_max / 1000.0)
+
+    # e2e through the C ABI with host buffers (pinned), continuing the motion.
+    nmax = pipe.max_contacts
+    h_contacts = torch.empty((nmax, 3), dtype=torch.int32, pin_memory=True)
+    h_index = torch.empty(nmax, dtype=torch.int32, pin_memory=True)
+    h_man = torch.empty((nmax, 80), dtype=torch.int32, pin_memory=True)
+    h_state = torch.empty(17 * nb, dtype=torch.float32, pin_memory=True)
+    import ctypes
+
+    lib = pipe.lib
+    e2e_m, e2e_h2d, e2e_d2h = 0, 0, 0
+    k0 = 1 + args.warmup + args.steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(k0, k0 + args.e2e_steps):
+        h_state.numpy()[:] = states[k]
+        pipe.collide(h_state.numpy())
+        nc = pipe._check(lib.b3g_fetch_contacts(pipe.ctx, ctypes.cast(h_contacts.data_ptr(), ctypes.POINTER(ctypes.c_uint32)), nmax))
+        nt = pipe._check(lib.b3g_fetch_touching(pipe.ctx, ctypes.cast(h_index.data_ptr(), ctypes.POINTER(ctypes.c_uint32)),
+                                                ctypes.c_void_p(h_man.data_ptr()), nmax))
+        e2e_m += nt
+        e2e_h2d += 17 * 4 * nb
+        e2e_d2h += nc * 12 + nt * (4 + 320)
+    t1 = time.perf_counter()
+    e2e_s = t1 - t0
+    e2e_value = e2e_m / e2e_s
+    if dist is not None:
+        t = torch.tensor([e2e_s, float(e2e_m)], device=dev, dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        e2e_value = float(tsum[1]) / float(tmax[0])
+
+    # Roofline of the dominant stage.
+    roof = None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    stage_ms = {k: v[0] / max(v[1], 1) for k, v in prof.items()}
+    if stage_ms:
+        sync_ms = stage_ms.get("sync", 0.0)
+        sb = algorithmic_bytes(scene, c)
+        achieved = sb / (sync_ms / 1000.0) / 1e9 if sync_ms > 0 else 0.0
+        roof = {"kernel": "k_sync (fat-AABB update)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "algorithmic_bytes_per_launch": sb,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_scene = build_scene(args.bodies, SEED)
+            m, t, done = reference_run(ref_scene, 50, seconds_cap=args.cpu_seconds)
+            cpu = {"value": m / t, "unit": "manifolds/s", "cores": 1, "kind": "reference",
+                   "sample": f"{done} passes of the same workload (creation pass excluded) on 1 host core; "
+                             "the reference is single-threaded"}
+        except Exception as e:  # the GPU number stands on its own
+            cpu = {"value": None, "unit": "manifolds/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "manifolds/s", "value": value, "unit": "manifolds/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": config_dict(args, {"contacts_last_pass": c["contacts"], "touching_last_pass": c["touching"],
+                                          "points_last_pass": c["points"]}),
+            "e2e": {"value": e2e_value, "unit": "manifolds/s", "h2d_bytes_per_step": e2e_h2d // max(args.e2e_steps, 1),
+                    "d2h_bytes_per_step": e2e_d2h // max(args.e2e_steps, 1), "steps": args.e2e_steps},
+            "gpu_launches": tot["launches"],
+            "pairs_per_s": tot["contacts"] / (ms / 1000.0),
+            "points_per_s": tot["points"] / (ms / 1000.0),
+            "stage_ms": stage_ms,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    pipe.close()
+
+
+def main():
+    args = parse()
+    rank, world, local, dist = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, rank, world, dist)
+        else:
+            run_ours(args, rank, world, local, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

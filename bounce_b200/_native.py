@@ -104,6 +104,10 @@ EXPORTED = [
     "b3g_fetch_fat_aabbs",
     "b3g_load_impulses",
     "b3g_device_results",
+    "b3g_get_totals",
+    "b3g_set_profiling",
+    "b3g_get_profile",
+    "b3g_stage_name",
     "b3g_collide_pairs",
     "b3g_hull_from_points",
     "b3g_hull_box",
@@ -147,6 +151,10 @@ def load():
         "b3g_fetch_fat_aabbs": ([ctx, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_load_impulses": ([ctx, f32p, f32p, f32p], ctypes.c_int),
         "b3g_device_results": ([ctx, _p(ctypes.c_void_p), _p(ctypes.c_void_p)], ctypes.c_int),
+        "b3g_get_totals": ([ctx, _p(ctypes.c_uint64), ctypes.c_int], ctypes.c_int),
+        "b3g_set_profiling": ([ctx, ctypes.c_int], ctypes.c_int),
+        "b3g_get_profile": ([ctx, _p(ctypes.c_double), u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_stage_name": ([ctypes.c_uint32], ctypes.c_char_p),
         "b3g_collide_pairs": (
             [ctx, ctypes.c_uint32, u32p, u32p, f32p, f32p, f32p, f32p, u32p, vp],
             ctypes.c_int,

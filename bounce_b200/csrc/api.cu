@@ -98,6 +98,116 @@ __global__ void k_touch_scatter(const DevManifold* man, const uint32_t* flagsIn,
 } // namespace
 
 // ---------------------------------------------------------------------------
+// Stage profiling.
+
+static const char* kStageNames[PROF_STAGES] = {
+	"upload",        // body state copy + counter reset
+	"sync",          // fat-AABB update (MoveProxy rule)
+	"sort",          // bounds, Morton keys, radix sort
+	"build",         // Karras tree, leaves, ropes, refit
+	"traverse",      // pair count, scan, pair write
+	"diff",          // persistent-pair hash, ended contacts
+	"narrow_convex", // buckets + sphere/capsule/hull-sphere/hull-capsule/sensor
+	"narrow_hulls",  // hull-hull SAT
+	"finalize",      // counters, contact records
+};
+
+void prof_mark(b3g_ctx* c, int mark, cudaStream_t s)
+{
+	if (!c->profiling)
+		return;
+	size_t slot = (size_t)(c->profPass % PROF_RING);
+	cudaEventRecord(c->profEvents[slot * PROF_MARKS + mark], s);
+}
+
+static void prof_harvest_one(b3g_ctx* c)
+{
+	size_t slot = (size_t)(c->profHarvest % PROF_RING);
+	cudaEvent_t* ev = c->profEvents + slot * PROF_MARKS;
+	cudaEventSynchronize(ev[PROF_MARKS - 1]);
+	for (int k = 0; k < PROF_STAGES; ++k)
+	{
+		float ms = 0.0f;
+		if (cudaEventElapsedTime(&ms, ev[k], ev[k + 1]) == cudaSuccess)
+		{
+			c->profMs[k] += ms;
+			c->profCount[k] += 1;
+		}
+	}
+	++c->profHarvest;
+}
+
+static int prof_begin_pass(b3g_ctx* c)
+{
+	// Reuse a ring slot only after its events were read.
+	while (c->profPass - c->profHarvest >= (uint64_t)PROF_RING)
+		prof_harvest_one(c);
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_profiling(b3g_ctx* c, int enable)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	CK(cudaSetDevice(c->device));
+	if (enable && !c->profEvents)
+	{
+		c->profEvents = new cudaEvent_t[PROF_RING * PROF_MARKS];
+		for (int i = 0; i < PROF_RING * PROF_MARKS; ++i)
+			CK(cudaEventCreate(&c->profEvents[i]));
+	}
+	c->profiling = enable != 0;
+	c->profPass = c->profHarvest = 0;
+	for (int k = 0; k < 16; ++k)
+	{
+		c->profMs[k] = 0.0;
+		c->profCount[k] = 0;
+	}
+	return B3G_OK;
+}
+
+extern "C" int b3g_get_profile(b3g_ctx* c, double* ms, uint32_t* passes, uint32_t capacity)
+{
+	if (!c || !ms || !passes)
+		return fail(c, B3G_E_INVALID, "null argument");
+	CK(cudaSetDevice(c->device));
+	while (c->profHarvest < c->profPass)
+		prof_harvest_one(c);
+	uint32_t n = std::min<uint32_t>(capacity, PROF_STAGES);
+	for (uint32_t k = 0; k < n; ++k)
+	{
+		ms[k] = c->profMs[k];
+		passes[k] = c->profCount[k];
+	}
+	return (int)n;
+}
+
+extern "C" const char* b3g_stage_name(uint32_t stage)
+{
+	return stage < PROF_STAGES ? kStageNames[stage] : nullptr;
+}
+
+extern "C" int b3g_get_totals(b3g_ctx* c, uint64_t* out, int reset)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "null argument");
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	CK(cudaDeviceSynchronize());
+	unsigned long long t[8];
+	CK(cudaMemcpy(t, c->buf.totals, sizeof(t), cudaMemcpyDeviceToHost));
+	for (int k = 0; k < 6; ++k)
+		out[k] = t[k];
+	out[6] = c->launches;
+	if (reset)
+	{
+		CK(cudaMemset(c->buf.totals, 0, sizeof(t)));
+		c->launches = 0;
+	}
+	return B3G_OK;
+}
+
+// ---------------------------------------------------------------------------
 
 extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 {
@@ -129,6 +239,10 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = nullptr;
 	c->dFixParams = nullptr;
 	c->hCounters = nullptr;
+	c->profiling = false;
+	c->launches = 0;
+	c->profPass = c->profHarvest = 0;
+	c->profEvents = nullptr;
 	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
 	{
 		delete c;
@@ -183,6 +297,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.prevFound, C), "alloc");
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
+	step(dalloc(&B.totals, 8), "alloc");
 	step(dalloc(&B.endedList, 3 * (size_t)C), "alloc");
 	step(dalloc(&B.touchIndex, C), "alloc");
 	step(dalloc(&B.touchMan, C), "alloc");
@@ -194,6 +309,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	if (rc == B3G_OK)
 	{
 		step(cudaMemsetAsync(B.counters, 0, sizeof(uint32_t) * CTR_COUNT, c->stream), "memset");
+		step(cudaMemsetAsync(B.totals, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[0], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.hashKeys[0], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
@@ -255,6 +371,13 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.prevFound);
 	dfree(B.bucketList);
 	dfree(B.counters);
+	dfree(B.totals);
+	if (c->profEvents)
+	{
+		for (int i = 0; i < PROF_RING * PROF_MARKS; ++i)
+			cudaEventDestroy(c->profEvents[i]);
+		delete[] c->profEvents;
+	}
 	dfree(B.endedList);
 	dfree(B.touchIndex);
 	dfree(B.touchMan);
@@ -311,8 +434,21 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 				return fail(c, B3G_E_INVALID, "hull %u: half-edge %u out of range", h, e);
 		}
 		for (uint32_t f = 0; f < d[5]; ++f)
-			if (faces[d[4] + f] >= d[3])
+		{
+			uint32_t begin = faces[d[4] + f];
+			if (begin >= d[3])
 				return fail(c, B3G_E_INVALID, "hull %u: face %u edge out of range", h, f);
+			// Every face loop must close within the hull's half-edge count and
+			// stay on its face (b3Hull::Validate, hull.cpp:21-78).
+			uint32_t e = begin, steps = 0;
+			do
+			{
+				const uint32_t* E = edges + 5 * (size_t)(d[2] + e);
+				if (E[2] != f || ++steps > d[3])
+					return fail(c, B3G_E_INVALID, "hull %u: face %u loop is broken", h, f);
+				e = E[4];
+			} while (e != begin);
+		}
 		hd[h] = HullDesc{d[0], d[1], d[2], d[3], d[4], d[5], centroids[3 * h], centroids[3 * h + 1],
 			centroids[3 * h + 2], {0, 0, 0}};
 		nv = std::max(nv, d[0] + d[1]);
@@ -477,6 +613,13 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	CK(cudaSetDevice(c->device));
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
+	if (c->profiling)
+	{
+		int rc = prof_begin_pass(c);
+		if (rc)
+			return rc;
+	}
+	prof_mark(c, PM_BEGIN, s);
 	if (onDevice)
 		CK(cudaMemcpyAsync(c->dBodyState, state, bytes, cudaMemcpyDeviceToDevice, s));
 	else
@@ -484,11 +627,19 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	if (c->havePass)
 		c->cur ^= 1u;
 	k_pass_begin<<<1, CTR_COUNT, 0, s>>>(c->buf.counters, c->havePass ? 1 : 0, c->cfg.max_contacts);
+	prof_mark(c, PM_UPLOADED, s);
 	launch_sync(c, s);
+	prof_mark(c, PM_SYNCED, s);
 	launch_broadphase(c, s);
 	launch_pairs_diff(c, s);
+	prof_mark(c, PM_DIFFED, s);
 	launch_narrowphase(c, s);
 	launch_finalize(c, s);
+	prof_mark(c, PM_FINAL, s);
+	if (c->profiling)
+		++c->profPass;
+	// pass_begin, sync, broadphase, diff (+ ended), bucket + 7 convex + hulls, finalize + pass_end
+	c->launches += 1 + 1 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 9 + 2;
 	CK(cudaGetLastError());
 	c->creationPass = false;
 	c->havePass = true;

@@ -137,6 +137,7 @@ struct Buffers
 	// narrowphase work lists
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
 	uint32_t* counters;   // device counters (see CTR_*)
+	unsigned long long* totals; // cumulative: passes, contacts, manifolds, points, begun, ended
 	uint32_t* endedList;  // 3 u32 per ended contact
 	uint32_t* touchIndex;
 	DevManifold* touchMan;
@@ -200,7 +201,40 @@ struct b3g_ctx
 
 	// host copies of fixture types (for the stand-alone narrowphase)
 	std::vector<uint32_t> hFixType;
+
+	// kernels launched by passes (host count)
+	uint64_t launches;
+
+	// stage profiling: a ring of per-pass event sets
+	bool profiling;
+	uint64_t profPass;     // passes recorded since enabling
+	uint64_t profHarvest;  // passes already accumulated
+	cudaEvent_t* profEvents; // PROF_RING * PROF_MARKS
+	double profMs[16];
+	uint32_t profCount[16];
 };
+
+// Stage boundaries of one pass (see b3g_stage_name).
+enum
+{
+	PM_BEGIN = 0,
+	PM_UPLOADED,
+	PM_SYNCED,
+	PM_SORTED,
+	PM_BUILT,
+	PM_TRAVERSED,
+	PM_DIFFED,
+	PM_CONVEX,
+	PM_HULLS,
+	PM_FINAL,
+	PROF_MARKS
+};
+constexpr int PROF_STAGES = PROF_MARKS - 1;
+constexpr int PROF_RING = 64;
+
+// Records boundary `mark` of the current pass when profiling is on.
+void prof_mark(b3g_ctx* c, int mark, cudaStream_t s);
+uint32_t broadphase_launches(const b3g_ctx* c);
 
 // Launchers (defined in the .cu files).
 void launch_sync(b3g_ctx* c, cudaStream_t s);

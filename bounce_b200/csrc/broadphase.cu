@@ -567,8 +567,16 @@ __global__ void k_traverse(DevScene S, Buffers B, int n, uint32_t cur, uint32_t 
 	uint32_t base = WRITE ? B.leafCount[j] : 0;
 	uint32_t node = B.nodeRope[leaf];
 	uint32_t keyA = S.fixKey[pa];
+	// A depth-first walk visits each of the 2n - 1 nodes at most once.
+	uint32_t steps = 0;
+	const uint32_t maxSteps = 2u * (uint32_t)n + 1u;
 	while (node != SENT)
 	{
+		if (++steps > maxSteps || node >= 2u * (uint32_t)n - 1u)
+		{
+			atomicOr(&B.counters[CTR_STATUS], B3G_ST_WAIT_TIMEOUT);
+			break;
+		}
 		if (B.nodeFirst[node] > wend)
 			break;
 		float4 lo = B.nodeLo[node], hi = B.nodeHi[node];
@@ -673,6 +681,20 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 	k_sync<<<(n + 127) / 128, 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
 }
 
+// Kernels launched by launch_broadphase for the current scene (kept next to
+// the launcher so the count follows its structure).
+uint32_t broadphase_launches(const b3g_ctx* c)
+{
+	uint32_t n = c->nFixtures;
+	if (n == 0)
+		return 0;
+	uint32_t wb = 0;
+	while ((1u << wb) < c->nWorlds)
+		++wb;
+	uint32_t passes = 4 + (wb + 7) / 8;
+	return 3 + 3 * passes + (n > 1 ? 1 : 0) + 2 + 2 + 3;
+}
+
 void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
@@ -714,13 +736,16 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 		cudaMemcpyAsync(B.keysA, kin, sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, s);
 		cudaMemcpyAsync(B.valsA, vin, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s);
 	}
+	prof_mark(c, PM_SORTED, s);
 
 	if (n > 1)
 		k_build<<<(n - 1 + 255) / 256, 256, 0, s>>>(B, n);
 	k_leaves<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, n);
 	k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
+	prof_mark(c, PM_BUILT, s);
 
 	k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_PAIRS, s);
 	k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	prof_mark(c, PM_TRAVERSED, s);
 }

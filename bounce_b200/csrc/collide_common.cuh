@@ -190,8 +190,11 @@ __device__ __forceinline__ uint32_t clip_segment_to_face_side_planes(ClipV vOut[
 	uint32_t numOut = 0;
 	uint32_t begin = h.f[index];
 	uint32_t edge = begin;
+	uint32_t guard = 0;
 	do
 	{
+		if (++guard > h.eCnt)
+			return 0; // face loops are validated on upload; never loop forever
 		uint32_t edgeId = edge; // twin of the twin
 		PL plane = hull_edge_side_plane(h, edgeId);
 		plane.d += r;
@@ -284,8 +287,14 @@ __device__ __forceinline__ Poly* clip_polygon_to_face_side_planes(Poly& a, Poly&
 	uint32_t begin = h.f[index];
 	uint32_t edge = begin;
 	ok = true;
+	uint32_t guard = 0;
 	do
 	{
+		if (++guard > h.eCnt)
+		{
+			ok = false;
+			return in;
+		}
 		uint32_t edgeId = edge;
 		PL plane = hull_edge_side_plane(h, edgeId);
 		plane.d += r;

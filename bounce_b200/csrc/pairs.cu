@@ -187,6 +187,21 @@ __global__ void k_finalize(Buffers B, uint32_t cur, uint32_t cap)
 			atomicAdd(&B.counters[CTR_MANIFOLDS], manifolds);
 		if (points)
 			atomicAdd(&B.counters[CTR_POINTS], points);
+		if (manifolds)
+			atomicAdd(&B.totals[2], (unsigned long long)manifolds);
+		if (points)
+			atomicAdd(&B.totals[3], (unsigned long long)points);
+	}
+}
+
+__global__ void k_pass_end(Buffers B, uint32_t cap)
+{
+	if (threadIdx.x == 0)
+	{
+		B.totals[0] += 1;
+		B.totals[1] += min(B.counters[CTR_PAIRS], cap);
+		B.totals[4] += B.counters[CTR_BEGUN];
+		B.totals[5] += B.counters[CTR_ENDED];
 	}
 }
 
@@ -250,11 +265,14 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	a.impM = c->impulsesLoaded ? B.impulseMotor : nullptr;
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, s);
+	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
 		c->maxUniqueEdges, s);
+	prof_mark(c, PM_HULLS, s);
 }
 
 void launch_finalize(b3g_ctx* c, cudaStream_t s)
 {
 	k_finalize<<<persistent_blocks(4), 256, 0, s>>>(c->buf, c->cur, c->cfg.max_contacts);
+	k_pass_end<<<1, 32, 0, s>>>(c->buf, c->cfg.max_contacts);
 }

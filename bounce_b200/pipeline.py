@@ -141,6 +141,23 @@ class CollisionPipeline:
         m = np.ascontiguousarray(motor, np.float32)
         self._check(self.lib.b3g_load_impulses(self.ctx, N.ptr(n, f32), N.ptr(t, f32), N.ptr(m, f32)))
 
+    def totals(self, reset=False):
+        """Cumulative device counters: passes, contacts, manifolds, points, begun, ended."""
+        out = np.zeros(7, np.uint64)
+        self._check(self.lib.b3g_get_totals(self.ctx, N.ptr(out, ctypes.c_uint64), 1 if reset else 0))
+        names = ("passes", "contacts", "manifolds", "points", "begun", "ended", "launches")
+        return dict(zip(names, (int(x) for x in out)))
+
+    def set_profiling(self, on=True):
+        self._check(self.lib.b3g_set_profiling(self.ctx, 1 if on else 0))
+
+    def profile(self):
+        """Per-stage summed milliseconds and pass counts (CUDA events on the pass stream)."""
+        ms = np.zeros(16, np.float64)
+        cnt = np.zeros(16, np.uint32)
+        n = self._check(self.lib.b3g_get_profile(self.ctx, N.ptr(ms, ctypes.c_double), N.ptr(cnt, u32), 16))
+        return {self.lib.b3g_stage_name(k).decode(): (float(ms[k]), int(cnt[k])) for k in range(n)}
+
     def device_results(self):
         a, b = ctypes.c_void_p(), ctypes.c_void_p()
         self._check(self.lib.b3g_device_results(self.ctx, ctypes.byref(a), ctypes.byref(b)))

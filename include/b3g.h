@@ -187,6 +187,23 @@ int b3g_fetch_fat_aabbs(b3g_ctx* ctx, float* out, uint32_t capacity);
 int b3g_load_impulses(b3g_ctx* ctx, const float* normal_impulse, const float* tangent_impulse,
 	const float* motor_impulse);
 
+/* Cumulative counters since creation or the last reset: out[0] passes,
+ * out[1] contacts, out[2] manifolds with points, out[3] manifold points,
+ * out[4] contacts created, out[5] contacts destroyed, out[6] CUDA kernels the
+ * passes launched (counted on the host; 7 entries). Kept on the device and
+ * summed without host synchronisation inside the passes. Replaces the
+ * reference's per-step statistics (b3_convexCalls etc., world.cpp:191-199). */
+int b3g_get_totals(b3g_ctx* ctx, uint64_t* out, int reset);
+
+/* Stage timing with CUDA events on the pass's stream, the device-side
+ * counterpart of b3Profiler scopes (include/bounce/common/profiler.h:96-161).
+ * enable != 0 starts (and clears) accumulation. b3g_get_profile waits for the
+ * recorded passes and returns per stage the summed milliseconds and the
+ * number of passes, in the order of b3g_stage_name(0 .. count-1). */
+int b3g_set_profiling(b3g_ctx* ctx, int enable);
+int b3g_get_profile(b3g_ctx* ctx, double* ms, uint32_t* passes, uint32_t capacity);
+const char* b3g_stage_name(uint32_t stage);
+
 /* Device pointers of the last pass's results for zero-copy consumers:
  * contacts (3 u32 each) and manifolds (320 bytes each). */
 int b3g_device_results(b3g_ctx* ctx, const void** contacts, const void** manifolds);
