@@ -34,7 +34,7 @@ sys.path.insert(0, ROOT)
 N_BODIES = 65536
 SIDE = 49.0
 SEED = 2
-WORKLOAD = "one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% hull 8-32 pts), 49 m cube, kinematic motion"
+WORKLOAD = "one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% hull 8-32 pts), 49 m cube, kinematic motion reflected at the cube faces"
 
 
 def parse():
@@ -120,6 +120,12 @@ class ClockSampler:
         }
 
 
+def scene_half(scene):
+    """Half-size of the cube the bodies start in; the driver reflects centres of
+    mass off its faces so the contact density stays constant over long runs."""
+    return float(np.abs(scene.body_pos).max())
+
+
 def build_scene(n, seed):
     from bounce_b200 import scene as S
 
@@ -151,7 +157,7 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0):
         raise RuntimeError("oracle/_ref/libb3ref32.so not built")
     rw = O.RefWorld(scene)
     scene.set_local_centers(rw.local_centers())
-    drv = S.KinematicDriver(scene)
+    drv = S.KinematicDriver(scene, walls=scene_half(scene))
     rw.first_pass()
     for _ in range(warmup):
         drv.advance()
@@ -214,7 +220,7 @@ def run_ours(args, rank, world, local, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     scene = build_scene(args.bodies, SEED + rank)
-    drv = S.KinematicDriver(scene)
+    drv = S.KinematicDriver(scene, walls=scene_half(scene))
     total = 1 + args.warmup + args.steps + args.e2e_steps
     nb = scene.n_bodies
     states = np.empty((total, 17 * nb), np.float32)

@@ -327,9 +327,14 @@ class KinematicDriver:
     Per pass k the sweep start is the previous pose and the sweep end the new
     one: c_k = c_{k-1} + dt v, q_k = normalize(q_{k-1} + dt/2 (w, 0) q_{k-1})."""
 
-    def __init__(self, scene, dt=1.0 / 60.0):
+    def __init__(self, scene, dt=1.0 / 60.0, walls=None):
+        """walls: half-size of an axis-aligned box whose faces reflect the
+        centre-of-mass velocity, keeping the body density constant over long
+        runs (None: free motion)."""
         self.s = scene
         self.dt = F(dt)
+        self.walls = None if walls is None else F(walls)
+        self.lin = scene.body_lin.copy()
         self.lc = scene.local_center
         p, q = scene.body_pos, scene.body_quat
         # b3Body::ResetMass: worldCenter = xf * localCenter (body.cpp).
@@ -345,7 +350,11 @@ class KinematicDriver:
         """Move one step (static bodies stay)."""
         dt = self.dt
         m = self.moving
-        c1 = (self.c + dt * self.s.body_lin).astype(F)
+        if self.walls is not None:
+            out_hi = (self.c > self.walls) & (self.lin > 0)
+            out_lo = (self.c < -self.walls) & (self.lin < 0)
+            self.lin = np.where(out_hi | out_lo, -self.lin, self.lin).astype(F)
+        c1 = (self.c + dt * self.lin).astype(F)
         w = self.s.body_ang
         q = self.q
         # qdot = 0.5 * (w, 0) * q  (quat.h b3Derivative / b3Integrate)
