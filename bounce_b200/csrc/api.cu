@@ -278,6 +278,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.refitFlag, P), "alloc");
 	step(dalloc(&B.worldEnd, P), "alloc");
 	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
+	step(dalloc(&B.pairScratch, 16 * (size_t)P), "alloc");
 	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
 	for (int k = 0; k < 2; ++k)
 	{
@@ -296,6 +297,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.prevIndex, C), "alloc");
 	step(dalloc(&B.prevFound, C), "alloc");
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
+	step(dalloc(&B.missList, C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
 	step(dalloc(&B.totals, 8), "alloc");
 	step(dalloc(&B.endedList, 3 * (size_t)C), "alloc");
@@ -356,6 +358,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.refitFlag);
 	dfree(B.worldEnd);
 	dfree(B.leafCount);
+	dfree(B.pairScratch);
 	dfree(B.scanAux);
 	for (int k = 0; k < 2; ++k)
 	{
@@ -370,6 +373,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.prevIndex);
 	dfree(B.prevFound);
 	dfree(B.bucketList);
+	dfree(B.missList);
 	dfree(B.counters);
 	dfree(B.totals);
 	if (c->profEvents)
@@ -638,8 +642,8 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	prof_mark(c, PM_FINAL, s);
 	if (c->profiling)
 		++c->profPass;
-	// pass_begin, sync, broadphase, diff (+ ended), bucket + 7 convex + hulls, finalize + pass_end
-	c->launches += 1 + 1 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 9 + 2;
+	// pass_begin, sync, broadphase, diff (+ ended), bucket + 7 convex + 2 hull, finalize + pass_end
+	c->launches += 1 + 1 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 10 + 2;
 	CK(cudaGetLastError());
 	c->creationPass = false;
 	c->havePass = true;
@@ -872,6 +876,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	}
 	uint32_t *dA = nullptr, *dB = nullptr, *dState = nullptr, *dList = nullptr, *dCount = nullptr, *dPrevState = nullptr;
 	uint32_t* dStatus = nullptr;
+	uint32_t *dMiss = nullptr, *dMissCount = nullptr;
 	int32_t* dPrev = nullptr;
 	uint4 *dCache = nullptr, *dCacheIn = nullptr;
 	float *dXA = nullptr, *dXB = nullptr, *dX0A = nullptr, *dX0B = nullptr;
@@ -897,6 +902,8 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	step(dalloc(&dX0B, 7 * (size_t)n));
 	step(dalloc(&dMan, n));
 	step(dalloc(&dPrevMan, 1));
+	step(dalloc(&dMiss, n));
+	step(dalloc(&dMissCount, 1));
 	if (rc == B3G_OK)
 	{
 		std::vector<int32_t> prev(n);
@@ -917,6 +924,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 		step(cudaMemcpy(dCacheIn, cin.data(), 16 * (size_t)n, cudaMemcpyHostToDevice));
 		step(cudaMemset(dPrevState, 0, 4 * n));
 		step(cudaMemset(dStatus, 0, 4));
+		step(cudaMemset(dMissCount, 0, 4));
 	}
 	if (rc == B3G_OK)
 	{
@@ -939,6 +947,8 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 		a.exB = dXB;
 		a.ex0A = dX0A;
 		a.ex0B = dX0B;
+		a.missList = dMiss;
+		a.missCount = dMissCount;
 		std::vector<uint32_t> flat(n), counts(BK_COUNT, 0);
 		std::vector<uint32_t> offs(BK_COUNT, 0);
 		uint32_t o = 0;
@@ -1012,5 +1022,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	dfree(dX0B);
 	dfree(dMan);
 	dfree(dPrevMan);
+	dfree(dMiss);
+	dfree(dMissCount);
 	return rc;
 }

@@ -120,6 +120,7 @@ struct Buffers
 	uint32_t* refitFlag;
 	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
+	uint32_t* pairScratch; // first partners found per leaf, slot-major (16 x n)
 	uint32_t* scanAux;
 
 	// contacts, double-buffered [cur], [prev]
@@ -136,6 +137,7 @@ struct Buffers
 
 	// narrowphase work lists
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
+	uint32_t* missList;   // hull-hull contacts for the SAT kernel
 	uint32_t* counters;   // device counters (see CTR_*)
 	unsigned long long* totals; // cumulative: passes, contacts, manifolds, points, begun, ended
 	uint32_t* endedList;  // 3 u32 per ended contact
@@ -162,6 +164,7 @@ enum
 	CTR_MOVED,
 	CTR_STATUS,
 	CTR_TOUCH_OUT,
+	CTR_HULL_MISS,      // hull-hull contacts the feature cache did not resolve
 	CTR_BUCKET0 = 16,   // BK_COUNT bucket sizes
 	CTR_COUNT = 32
 };

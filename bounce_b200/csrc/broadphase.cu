@@ -470,11 +470,15 @@ __global__ void k_leaves(DevScene S, Buffers B, int n)
 		return;
 	uint32_t node = n - 1 + j;
 	uint32_t proxy = B.valsA[j];
+	uint32_t rope = (j == n - 1) ? SENT : B.splitRight[j];
 	B.nodeLeft[node] = proxy;
 	B.nodeFirst[node] = j;
-	B.nodeLo[node] = B.fatLo[proxy];
-	B.nodeHi[node] = B.fatHi[proxy];
-	B.nodeRope[node] = (j == n - 1) ? SENT : B.splitRight[j];
+	// Traversal reads a node as two float4: (lower, left child or proxy) and
+	// (upper, rope).
+	float4 lo = B.fatLo[proxy], hi = B.fatHi[proxy];
+	B.nodeLo[node] = make_float4(lo.x, lo.y, lo.z, __uint_as_float(proxy));
+	B.nodeHi[node] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(rope));
+	B.nodeRope[node] = rope;
 	if (j < n - 1)
 	{
 		B.nodeRope[j] = (B.nodeEnd[j] == (uint32_t)(n - 1)) ? SENT : B.splitRight[B.nodeEnd[j]];
@@ -503,8 +507,9 @@ __global__ void k_refit(Buffers B, int n)
 		uint32_t l = B.nodeLeft[p], r = B.nodeRight[p];
 		float4 al = __ldcg(&B.nodeLo[l]), ah = __ldcg(&B.nodeHi[l]);
 		float4 bl = __ldcg(&B.nodeLo[r]), bh = __ldcg(&B.nodeHi[r]);
-		B.nodeLo[p] = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
-		B.nodeHi[p] = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+		B.nodeLo[p] = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), __uint_as_float(l));
+		B.nodeHi[p] = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z),
+			__uint_as_float(B.nodeRope[p]));
 		if (p == 0)
 			return;
 		p = B.nodeParent[p];
@@ -550,82 +555,124 @@ __device__ __forceinline__ bool pair_filter(const DevScene& S, uint32_t pa, uint
 	return registered(S.fixType[pa], S.fixType[pb]);
 }
 
-template <bool WRITE>
-__global__ void k_traverse(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
+// Writes contact slot `slot` for the overlapping proxies pa, pb in the
+// broadphase order (min, max) of proxy ids (b3BroadPhase::Report,
+// broad_phase.cpp:341-342) followed by the factory's primary-type swap
+// (b3Contact::Create, contact.cpp:306-317).
+__device__ __forceinline__ void write_pair(const DevScene& S, Buffers& B, uint32_t cur, uint32_t slot, uint32_t pa,
+	uint32_t pb)
 {
-	int j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= n)
-		return;
+	uint32_t keyA = S.fixKey[pa], keyB = S.fixKey[pb];
+	uint32_t f1 = keyA < keyB ? pa : pb;
+	uint32_t f2 = keyA < keyB ? pb : pa;
+	uint32_t A = f1, Bf = f2;
+	if (!primary(S.fixType[f1], S.fixType[f2]))
+	{
+		A = f2;
+		Bf = f1;
+	}
+	B.pairA[cur][slot] = A;
+	B.pairB[cur][slot] = Bf;
+}
+
+// Rope walk from leaf j's own rope. A node is read as two float4:
+// (lower, left child | proxy) and (upper, rope). MODE 0 counts the filtered
+// overlaps and keeps the first TRAV_SLOTS partners in the leaf's scratch
+// slots; MODE 1 writes every pair from `base` (leaves whose partners did not
+// fit). MW: several worlds share the tree, so the walk stops at the first
+// node past the query's world (worlds are contiguous in depth-first order).
+constexpr uint32_t TRAV_SLOTS = 16;
+
+template <int MODE, bool MW>
+__device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cur, uint32_t cap,
+	uint32_t base)
+{
 	uint32_t leaf = n - 1 + j;
-	uint32_t pa = B.nodeLeft[leaf];
 	float4 ql = B.nodeLo[leaf], qh = B.nodeHi[leaf];
-	AABB q;
-	q.lo = V3{ql.x, ql.y, ql.z};
-	q.hi = V3{qh.x, qh.y, qh.z};
-	uint32_t wend = B.worldEnd[S.bodyWorld[S.fixBody[pa]]];
+	uint32_t pa = __float_as_uint(ql.w);
+	uint32_t wend = MW ? B.worldEnd[S.bodyWorld[S.fixBody[pa]]] : 0xFFFFFFFFu;
 	uint32_t count = 0;
-	uint32_t base = WRITE ? B.leafCount[j] : 0;
-	uint32_t node = B.nodeRope[leaf];
-	uint32_t keyA = S.fixKey[pa];
+	uint32_t node = __float_as_uint(qh.w);
 	// A depth-first walk visits each of the 2n - 1 nodes at most once.
 	uint32_t steps = 0;
 	const uint32_t maxSteps = 2u * (uint32_t)n + 1u;
+	const uint32_t nodes = 2u * (uint32_t)n - 1u;
 	while (node != SENT)
 	{
-		if (++steps > maxSteps || node >= 2u * (uint32_t)n - 1u)
+		if (++steps > maxSteps || node >= nodes)
 		{
 			atomicOr(&B.counters[CTR_STATUS], B3G_ST_WAIT_TIMEOUT);
 			break;
 		}
-		if (B.nodeFirst[node] > wend)
+		if (MW && B.nodeFirst[node] > wend)
 			break;
 		float4 lo = B.nodeLo[node], hi = B.nodeHi[node];
-		AABB nb;
-		nb.lo = V3{lo.x, lo.y, lo.z};
-		nb.hi = V3{hi.x, hi.y, hi.z};
-		if (aabb_overlap(nb, q))
+		bool overlap = !(hi.x < ql.x || lo.x > qh.x || hi.y < ql.y || lo.y > qh.y || hi.z < ql.z || lo.z > qh.z);
+		if (overlap && node < (uint32_t)(n - 1))
 		{
-			if (node >= (uint32_t)(n - 1))
+			node = __float_as_uint(lo.w); // descend
+			continue;
+		}
+		if (overlap)
+		{
+			uint32_t pb = __float_as_uint(lo.w);
+			if (pair_filter(S, pa, pb))
 			{
-				uint32_t pb = B.nodeLeft[node];
-				if (pair_filter(S, pa, pb))
+				if (MODE == 0)
 				{
-					if (WRITE)
-					{
-						uint32_t slot = base + count;
-						if (slot < cap)
-						{
-							// Broadphase order (min, max) of proxy ids, then the
-							// factory's primary-type swap.
-							uint32_t keyB = S.fixKey[pb];
-							uint32_t f1 = keyA < keyB ? pa : pb;
-							uint32_t f2 = keyA < keyB ? pb : pa;
-							uint32_t A = f1, Bf = f2;
-							if (!primary(S.fixType[f1], S.fixType[f2]))
-							{
-								A = f2;
-								Bf = f1;
-							}
-							B.pairA[cur][slot] = A;
-							B.pairB[cur][slot] = Bf;
-						}
-					}
-					++count;
+					if (count < TRAV_SLOTS)
+						B.pairScratch[(size_t)count * n + j] = pb;
 				}
-				node = B.nodeRope[node];
-			}
-			else
-			{
-				node = B.nodeLeft[node];
+				else
+				{
+					uint32_t slot = base + count;
+					if (slot < cap)
+						write_pair(S, B, cur, slot, pa, pb);
+				}
+				++count;
 			}
 		}
-		else
+		node = __float_as_uint(hi.w);
+	}
+	return count;
+}
+
+template <bool MW>
+__global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
+{
+	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n)
+		return;
+	B.leafCount[j] = walk<0, MW>(S, B, n, j, cur, cap, 0);
+}
+
+// After the exclusive scan leafCount holds offsets; a leaf's count is the
+// difference to the next offset (the last one to the total).
+template <bool MW>
+__global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
+{
+	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n)
+		return;
+	uint32_t base = B.leafCount[j];
+	uint32_t end = (j == n - 1) ? B.counters[CTR_PAIRS] : B.leafCount[j + 1];
+	uint32_t count = end - base;
+	if (count == 0)
+		return;
+	if (count <= TRAV_SLOTS)
+	{
+		uint32_t pa = __float_as_uint(B.nodeLo[n - 1 + j].w);
+		for (uint32_t k = 0; k < count; ++k)
 		{
-			node = B.nodeRope[node];
+			uint32_t slot = base + k;
+			if (slot < cap)
+				write_pair(S, B, cur, slot, pa, B.pairScratch[(size_t)k * n + j]);
 		}
 	}
-	if (!WRITE)
-		B.leafCount[j] = count;
+	else
+	{
+		walk<1, MW>(S, B, n, j, cur, cap, base);
+	}
 }
 
 // Multi-block exclusive scan of u32 (in place) with the total written to *total.
@@ -744,8 +791,14 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
 	prof_mark(c, PM_BUILT, s);
 
-	k_traverse<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	if (c->nWorlds > 1)
+		k_traverse_count<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	else
+		k_traverse_count<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_PAIRS, s);
-	k_traverse<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	if (c->nWorlds > 1)
+		k_traverse_emit<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	else
+		k_traverse_emit<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	prof_mark(c, PM_TRAVERSED, s);
 }

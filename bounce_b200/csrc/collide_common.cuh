@@ -447,35 +447,15 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 // ---------------------------------------------------------------------------
 // Manifolds.
 
-// b3Manifold::Initialize() (collision.cpp:23-38) plus cleared geometry.
+// b3Manifold::Initialize() (collision.cpp:23-38) plus cleared geometry: the
+// whole 320-byte record is zeroed with 16-byte stores (records are 16-byte
+// aligned in the contact arrays), then the header fields that are not zero.
 __device__ __forceinline__ void man_clear(DevManifold& m)
 {
-	m.pointCount = 0;
-	m.tangentImpulse[0] = 0.0f;
-	m.tangentImpulse[1] = 0.0f;
-	m.motorImpulse = 0.0f;
-	m.motorSpeed = 0.0f;
-	m.tangentSpeed1 = 0.0f;
-	m.tangentSpeed2 = 0.0f;
-	m.pad = 0;
-	for (int i = 0; i < 4; ++i)
-	{
-		DevPoint& p = m.points[i];
-		for (int k = 0; k < 3; ++k)
-		{
-			p.n[k] = 0.0f;
-			p.p1[k] = 0.0f;
-			p.p2[k] = 0.0f;
-		}
-		p.normalImpulse = 0.0f;
-		p.triangleKey = 0;
-		p.pad0 = 0;
-		p.key[0] = p.key[1] = p.key[2] = p.key[3] = 0;
-		p.persisting = 0;
-		p.edgeContact = 0;
-		for (int k = 0; k < 6; ++k)
-			p.pad1[k] = 0;
-	}
+	uint4* w = reinterpret_cast<uint4*>(&m);
+#pragma unroll
+	for (int i = 0; i < (int)(sizeof(DevManifold) / 16); ++i)
+		w[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 
 __device__ __forceinline__ void set_point(DevPoint& p, V3 n, V3 p1, V3 p2)
@@ -512,28 +492,6 @@ __device__ __forceinline__ bool id_equal(const DevPoint& a, const DevPoint& b)
 		a.key[2] == b.key[2] && a.key[3] == b.key[3];
 }
 
-// b3Manifold::Initialize(old) (collision.cpp:40-61).
-__device__ __forceinline__ void man_warm_start(DevManifold& m, const DevManifold& old)
-{
-	m.tangentImpulse[0] = old.tangentImpulse[0];
-	m.tangentImpulse[1] = old.tangentImpulse[1];
-	m.motorImpulse = old.motorImpulse;
-	for (uint32_t i = 0; i < m.pointCount; ++i)
-	{
-		DevPoint& p1 = m.points[i];
-		for (uint32_t j = 0; j < old.pointCount; ++j)
-		{
-			const DevPoint& p2 = old.points[j];
-			if (id_equal(p2, p1))
-			{
-				p1.normalImpulse = p2.normalImpulse;
-				p1.persisting = 1;
-				break;
-			}
-		}
-	}
-}
-
 // Per-pass context passed to the narrowphase kernels.
 struct NPArgs
 {
@@ -562,6 +520,9 @@ struct NPArgs
 	const float* exB;
 	const float* ex0A;
 	const float* ex0B;
+	// hull-hull pairs the feature cache could not resolve
+	uint32_t* missList;
+	uint32_t* missCount;
 };
 
 __device__ __forceinline__ XF load_xf7(const float* s)
@@ -573,28 +534,51 @@ __device__ __forceinline__ XF load_xf7(const float* s)
 }
 
 // The tail of b3Contact::Update for a convex contact (contact.cpp:424-465):
-// warm start from the previous manifold, touching flag, manifold count 1.
+// warm start from the previous manifold as b3Manifold::Initialize(old) does
+// (collision.cpp:40-61: tangent and motor impulses copied, normal impulses
+// copied to points whose b3ContactID matches), touching flag, manifold count 1.
+// m is the contact's output record (device memory); the previous record is
+// read field by field.
 __device__ __forceinline__ void finish_convex(const NPArgs& a, uint32_t c, DevManifold& m)
 {
 	int32_t prev = a.prevIndex[c];
 	uint32_t oldCount = prev >= 0 ? ((a.prevState[prev] >> 8) & 0xFFu) : 0u;
+	uint32_t pc = m.pointCount;
 	if (a.warmStarting && oldCount > 0)
 	{
-		DevManifold old = a.prevMan[prev];
+		const DevManifold& old = a.prevMan[prev];
 		if (a.impN)
 		{
-			for (int k = 0; k < 4; ++k)
-				old.points[k].normalImpulse = a.impN[4 * prev + k];
-			old.tangentImpulse[0] = a.impT[2 * prev + 0];
-			old.tangentImpulse[1] = a.impT[2 * prev + 1];
-			old.motorImpulse = a.impM[prev];
+			m.tangentImpulse[0] = a.impT[2 * prev + 0];
+			m.tangentImpulse[1] = a.impT[2 * prev + 1];
+			m.motorImpulse = a.impM[prev];
 		}
-		man_warm_start(m, old);
+		else
+		{
+			m.tangentImpulse[0] = old.tangentImpulse[0];
+			m.tangentImpulse[1] = old.tangentImpulse[1];
+			m.motorImpulse = old.motorImpulse;
+		}
+		uint32_t opc = old.pointCount;
+		for (uint32_t i = 0; i < pc; ++i)
+		{
+			DevPoint& p1 = m.points[i];
+			for (uint32_t j = 0; j < opc; ++j)
+			{
+				const DevPoint& p2 = old.points[j];
+				if (p2.triangleKey == p1.triangleKey && p2.key[0] == p1.key[0] && p2.key[1] == p1.key[1] &&
+					p2.key[2] == p1.key[2] && p2.key[3] == p1.key[3])
+				{
+					p1.normalImpulse = a.impN ? a.impN[4 * prev + j] : p2.normalImpulse;
+					p1.persisting = 1;
+					break;
+				}
+			}
+		}
 	}
-	uint32_t touching = m.pointCount > 0 ? 1u : 0u;
+	uint32_t touching = pc > 0 ? 1u : 0u;
 	uint32_t begun = prev < 0 ? 1u : 0u;
 	a.cstate[c] = touching | (1u << 8) | (begun << 16);
-	a.man[c] = m;
 }
 
 __device__ __forceinline__ XF body_xf(const DevScene& S, uint32_t body)

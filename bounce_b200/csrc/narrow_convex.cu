@@ -444,7 +444,7 @@ __global__ void k_convex(NPArgs a)
 		XF xfA = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
 		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
 		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
-		DevManifold m;
+		DevManifold& m = a.man[c];
 		man_clear(m);
 		if (BUCKET == BK_SPHERES)
 			collide_spheres(m, xfA, sa, xfB, sb);
@@ -478,9 +478,7 @@ __global__ void k_sensor(NPArgs a)
 		int32_t prev = a.prevIndex[c];
 		uint32_t begun = prev < 0 ? 1u : 0u;
 		a.cstate[c] = touching | (begun << 16);
-		DevManifold m;
-		man_clear(m);
-		a.man[c] = m;
+		man_clear(a.man[c]);
 		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
 }
@@ -503,9 +501,7 @@ __global__ void k_inactive(NPArgs a)
 		{
 			a.cstate[c] = 1u << 16;
 			a.cache[c] = make_uint4(0, B3G_NULL, B3G_NULL, B3G_NULL);
-			DevManifold m;
-			man_clear(m);
-			a.man[c] = m;
+			man_clear(a.man[c]);
 		}
 	}
 }

@@ -471,13 +471,27 @@ __device__ void collide_hulls_nocache(DevManifold& m, const HullCtx& H, uint32_t
 		face_contact_all(m, H, false, fi1, lane);
 }
 
-// b3CollideHullsCache (collide_hulls.cpp:355-515). cache is uniform across
-// the warp; m is meaningful on lane 0.
-__device__ void collide_hulls_cache(DevManifold& m, const HullCtx& H, uint4& cache, uint32_t lane)
+// Thread-level b3FeatureCache::ReadFace (sat.cpp:209-224).
+__device__ uint32_t read_face_thread(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2,
+	uint32_t index1, float totalRadius)
+{
+	XF xf = xmult(xf2, xf1);
+	PL plane = pmul(xf, hp(h1, index1));
+	uint32_t si = hull_support_vertex(h2, -plane.n);
+	float s = pdist(hv(h2, si), plane);
+	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
+}
+
+// The cache half of b3CollideHullsCache (collide_hulls.cpp:367-415), one
+// thread per contact: b3FeatureCache::ReadState (sat.cpp:178-207), then the
+// separation hit, or the overlap hit that rebuilds the cached edge or face
+// contact. Returns true when the contact is finished; otherwise the cache is
+// flushed (cacheType = empty, the feature fields as ReadState left them) and
+// the contact needs the SAT.
+__device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 {
 	float totalRadius = H.r1 + H.r2;
 	uint32_t state0 = cache.x;
-	// b3FeatureCache::ReadState (sat.cpp:178-207).
 	if (cache.x == CT_EMPTY)
 	{
 		cache.x = CT_SEPARATION;
@@ -489,33 +503,33 @@ __device__ void collide_hulls_cache(DevManifold& m, const HullCtx& H, uint4& cac
 	if (cache.y == FT_EDGES)
 		state1 = read_edges(H.xf1, H.h1, H.xf2, H.h2, cache.z, cache.w, totalRadius);
 	else if (cache.y == FT_FACE1)
-		state1 = read_face(H.xf1, H.h1, H.xf2, H.h2, cache.z, totalRadius, lane);
+		state1 = read_face_thread(H.xf1, H.h1, H.xf2, H.h2, cache.z, totalRadius);
 	else if (cache.y == FT_FACE2)
-		state1 = read_face(H.xf2, H.h2, H.xf1, H.h1, cache.z, totalRadius, lane);
+		state1 = read_face_thread(H.xf2, H.h2, H.xf1, H.h1, cache.z, totalRadius);
 	else
 		state1 = CT_EMPTY;
-
 	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
-		return; // separation cache hit
+		return true; // separation cache hit
 	if (state0 == CT_OVERLAP && state1 == CT_OVERLAP)
 	{
-		if (lane == 0)
-		{
-			if (cache.y == FT_EDGES)
-				rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
-			else if (cache.y == FT_FACE1)
-				rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02,
-					H.status);
-			else if (cache.y == FT_FACE2)
-				rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01,
-					H.status);
-		}
-		uint32_t pc = __shfl_sync(0xffffffffu, m.pointCount, 0);
-		if (pc > 0)
-			return; // overlap cache hit
+		if (cache.y == FT_EDGES)
+			rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
+		else if (cache.y == FT_FACE1)
+			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
+		else if (cache.y == FT_FACE2)
+			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
+		if (m.pointCount > 0)
+			return true; // overlap cache hit
 	}
-	// Miss: flush and rerun the SAT.
 	cache.x = CT_EMPTY;
+	return false;
+}
+
+// The SAT half of b3CollideHullsCache (collide_hulls.cpp:417-515), one warp
+// per contact. cache is uniform across the warp; m is written by lane 0.
+__device__ void sat_after_miss(DevManifold& m, const HullCtx& H, uint4& cache, uint32_t lane)
+{
+	float totalRadius = H.r1 + H.r2;
 	uint32_t fi1, fi2, ei1, ei2;
 	float fs1, fs2, es;
 	warp_query_faces(H.xf1, H.h1, H.xf2, H.h2, lane, fi1, fs1);
@@ -582,42 +596,84 @@ __device__ void collide_hulls_cache(DevManifold& m, const HullCtx& H, uint4& cac
 	}
 }
 
-__global__ void __launch_bounds__(HW_WARPS * 32) k_hulls(NPArgs a, uint32_t maxUE)
+__device__ __forceinline__ void load_hull_ctx(const NPArgs& a, uint32_t c, HullCtx& H)
+{
+	uint32_t fa = a.pairA[c], fb = a.pairB[c];
+	uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+	H.xf1 = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
+	H.xf2 = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
+	H.xf01 = a.ex0A ? load_xf7(a.ex0A + 7 * (size_t)c) : body_xf0(a.S, ba);
+	H.xf02 = a.ex0B ? load_xf7(a.ex0B + 7 * (size_t)c) : body_xf0(a.S, bb);
+	H.h1 = hull_ref(a.S, a.S.fixHull[fa]);
+	H.h2 = hull_ref(a.S, a.S.fixHull[fb]);
+	H.r1 = a.S.fixParams[3 * fa].x;
+	H.r2 = a.S.fixParams[3 * fb].x;
+	H.status = a.status;
+	H.recs = nullptr;
+	H.maxUE = 0;
+}
+
+// Pass 1: one thread per hull-hull contact reads its feature cache.
+__global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
+{
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.list[t];
+		int32_t prev = a.prevIndex[c];
+		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
+		DevManifold& m = a.man[c];
+		man_clear(m);
+		bool done = false;
+		if (a.convexCache)
+		{
+			HullCtx H;
+			load_hull_ctx(a, c, H);
+			done = probe_cache(m, H, cache);
+		}
+		a.cache[c] = cache;
+		if (done)
+		{
+			finish_convex(a, c, m);
+		}
+		else
+		{
+			// Warp-aggregated append to the SAT list.
+			uint32_t mask = __activemask();
+			uint32_t lane = threadIdx.x & 31;
+			uint32_t leader = __ffs(mask) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(a.missCount, (uint32_t)__popc(mask));
+			base = __shfl_sync(mask, base, leader);
+			a.missList[base + __popc(mask & ((1u << lane) - 1u))] = c;
+		}
+	}
+}
+
+// Pass 2: one warp per contact the cache did not resolve.
+__global__ void __launch_bounds__(HW_WARPS * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
-	uint32_t n = *a.listCount;
+	uint32_t n = *a.missCount;
 	uint32_t gw = blockIdx.x * HW_WARPS + warp;
 	uint32_t nw = gridDim.x * HW_WARPS;
 	for (uint32_t t = gw; t < n; t += nw)
 	{
-		uint32_t c = a.list[t];
-		uint32_t fa = a.pairA[c], fb = a.pairB[c];
-		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+		uint32_t c = a.missList[t];
 		HullCtx H;
-		H.xf1 = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
-		H.xf2 = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
-		H.xf01 = a.ex0A ? load_xf7(a.ex0A + 7 * (size_t)c) : body_xf0(a.S, ba);
-		H.xf02 = a.ex0B ? load_xf7(a.ex0B + 7 * (size_t)c) : body_xf0(a.S, bb);
-		H.h1 = hull_ref(a.S, a.S.fixHull[fa]);
-		H.h2 = hull_ref(a.S, a.S.fixHull[fb]);
-		H.r1 = a.S.fixParams[3 * fa].x;
-		H.r2 = a.S.fixParams[3 * fb].x;
+		load_hull_ctx(a, c, H);
 		H.recs = recs;
 		H.maxUE = maxUE;
-		H.status = a.status;
-		int32_t prev = a.prevIndex[c];
-		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
-		DevManifold m;
-		if (lane == 0)
-			man_clear(m);
-		else
-			m.pointCount = 0;
+		uint4 cache = a.cache[c];
+		DevManifold& m = a.man[c];
 		if (a.convexCache)
-			collide_hulls_cache(m, H, cache, lane);
+			sat_after_miss(m, H, cache, lane);
 		else
 			collide_hulls_nocache(m, H, lane);
+		__syncwarp();
 		if (lane == 0)
 		{
 			finish_convex(a, c, m);
@@ -634,12 +690,13 @@ void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* coun
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
+	k_hulls_probe<<<persistent_blocks(4), 128, 0, s>>>(a);
 	size_t smem = (size_t)HW_WARPS * 2 * maxUE * sizeof(EdgeRec);
 	static size_t configured = 0;
 	if (smem > 48 * 1024 && smem > configured)
 	{
-		cudaFuncSetAttribute(k_hulls, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		cudaFuncSetAttribute(k_hulls_sat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 		configured = smem;
 	}
-	k_hulls<<<persistent_blocks(2), HW_WARPS * 32, smem, s>>>(a, maxUE);
+	k_hulls_sat<<<persistent_blocks(2), HW_WARPS * 32, smem, s>>>(a, maxUE);
 }

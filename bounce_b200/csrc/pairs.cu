@@ -264,6 +264,8 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	a.impT = c->impulsesLoaded ? B.impulseTangent : nullptr;
 	a.impM = c->impulsesLoaded ? B.impulseMotor : nullptr;
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
+	a.missList = B.missList;
+	a.missCount = B.counters + CTR_HULL_MISS;
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, s);
 	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
