@@ -238,6 +238,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dBodyState = nullptr;
 	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = nullptr;
 	c->dFixParams = nullptr;
+	c->dFixBound = nullptr;
 	c->hCounters = nullptr;
 	c->profiling = false;
 	c->launches = 0;
@@ -278,7 +279,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.refitFlag, P), "alloc");
 	step(dalloc(&B.worldEnd, P), "alloc");
 	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
-	step(dalloc(&B.pairScratch, 16 * (size_t)P), "alloc");
+	step(dalloc(&B.pairScratch, 2 * 16 * (size_t)P), "alloc"); // 16 uint2 records per leaf
 	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
 	for (int k = 0; k < 2; ++k)
 	{
@@ -398,12 +399,15 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dBodyType);
 	dfree(c->dBodyAwake);
 	dfree(c->dBodyState);
+	dfree(c->scene.bodyXf);
+	dfree(c->scene.bodyXf0);
 	dfree(c->dFixBody);
 	dfree(c->dFixType);
 	dfree(c->dFixHull);
 	dfree(c->dFixFlags);
 	dfree(c->dFixKey);
 	dfree(c->dFixParams);
+	dfree(c->dFixBound);
 	if (c->hCounters)
 		cudaFreeHost(c->hCounters);
 	if (c->stream)
@@ -489,6 +493,8 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 		CK(cudaMemcpy(c->dHfaces, faces, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(c->dHplanes, p4.data(), sizeof(float4) * nf, cudaMemcpyHostToDevice));
 	}
+	c->hHullDesc.assign(desc, desc + 6 * (size_t)nh);
+	c->hHullVerts.assign(verts, verts + 3 * (size_t)nv);
 	c->nHulls = nh;
 	c->hullVerts = nv;
 	c->hullEdges = ne;
@@ -521,10 +527,14 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 	dfree(c->dBodyType);
 	dfree(c->dBodyAwake);
 	dfree(c->dBodyState);
+	dfree(c->scene.bodyXf);
+	dfree(c->scene.bodyXf0);
 	CK(dalloc(&c->dBodyWorld, nb));
 	CK(dalloc(&c->dBodyType, nb));
 	CK(dalloc(&c->dBodyAwake, nb));
 	CK(dalloc(&c->dBodyState, 17 * (size_t)nb));
+	CK(dalloc(&c->scene.bodyXf, 2 * (size_t)nb));
+	CK(dalloc(&c->scene.bodyXf0, 2 * (size_t)nb));
 	if (nb)
 	{
 		CK(cudaMemcpy(c->dBodyWorld, world, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
@@ -564,6 +574,64 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	std::vector<float4> p4(3 * (size_t)nf);
 	for (size_t i = 0; i < 3 * (size_t)nf; ++i)
 		p4[i] = make_float4(params[4 * i], params[4 * i + 1], params[4 * i + 2], params[4 * i + 3]);
+	// Bounding spheres in the body frame: a float centre and a radius computed
+	// in double from that centre and rounded up, so the sphere contains the
+	// shape (with its skin radius) exactly.
+	std::vector<float4> bound(nf);
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		const float* p = params + 12 * (size_t)i;
+		std::vector<double> pts;
+		double skin = 0.0;
+		switch (shapeType[i])
+		{
+		case B3G_SHAPE_SPHERE:
+			pts = {p[0], p[1], p[2]};
+			skin = p[3];
+			break;
+		case B3G_SHAPE_CAPSULE:
+			pts = {p[0], p[1], p[2], p[3], p[4], p[5]};
+			skin = p[6];
+			break;
+		case B3G_SHAPE_TRIANGLE:
+			pts = {p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8]};
+			skin = p[9];
+			break;
+		default:
+		{
+			const uint32_t* d = c->hHullDesc.data() + 6 * (size_t)hull[i];
+			for (uint32_t v = 0; v < d[1]; ++v)
+				for (int k = 0; k < 3; ++k)
+					pts.push_back(c->hHullVerts[3 * (size_t)(d[0] + v) + k]);
+			skin = p[0];
+			break;
+		}
+		}
+		size_t np = pts.size() / 3;
+		double cx = 0, cy = 0, cz = 0;
+		for (size_t v = 0; v < np; ++v)
+		{
+			cx += pts[3 * v];
+			cy += pts[3 * v + 1];
+			cz += pts[3 * v + 2];
+		}
+		float fx = (float)(cx / np), fy = (float)(cy / np), fz = (float)(cz / np);
+		double r = 0;
+		for (size_t v = 0; v < np; ++v)
+		{
+			double dx = pts[3 * v] - fx, dy = pts[3 * v + 1] - fy, dz = pts[3 * v + 2] - fz;
+			r = std::max(r, std::sqrt(dx * dx + dy * dy + dz * dz));
+		}
+		r += std::fabs(skin);
+		float fr = (float)r;
+		fr = std::nextafter(std::nextafter(fr, INFINITY), INFINITY);
+		bound[i] = make_float4(fx, fy, fz, fr);
+	}
+	dfree(c->dFixBound);
+	CK(dalloc(&c->dFixBound, nf));
+	if (nf)
+		CK(cudaMemcpy(c->dFixBound, bound.data(), sizeof(float4) * nf, cudaMemcpyHostToDevice));
+	c->scene.fixBound = c->dFixBound;
 	dfree(c->dFixBody);
 	dfree(c->dFixType);
 	dfree(c->dFixHull);
@@ -643,7 +711,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	if (c->profiling)
 		++c->profPass;
 	// pass_begin, sync, broadphase, diff (+ ended), bucket + 7 convex + 2 hull, finalize + pass_end
-	c->launches += 1 + 1 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 10 + 2;
+	c->launches += 1 + 2 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 10 + 2;
 	CK(cudaGetLastError());
 	c->creationPass = false;
 	c->havePass = true;

@@ -85,12 +85,15 @@ struct DevScene
 	const uint32_t* bodyType;
 	const uint8_t* bodyAwake;
 	const float* bodyState; // 17 floats per body
+	float4* bodyXf;         // per pass: m_xf, 2 float4 per body
+	float4* bodyXf0;        // per pass: b3Sweep::GetTransform(0), 2 float4 per body
 
 	// fixtures
 	const uint32_t* fixBody;
 	const uint32_t* fixType;
 	const uint32_t* fixHull;
 	const float4* fixParams; // 3 float4 per fixture
+	const float4* fixBound;  // bounding sphere per fixture: body-frame centre, radius
 	const uint32_t* fixFlags;
 	const uint32_t* fixKey;
 };
@@ -120,7 +123,7 @@ struct Buffers
 	uint32_t* refitFlag;
 	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
-	uint32_t* pairScratch; // first partners found per leaf, slot-major (16 x n)
+	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (16 x n uint2)
 	uint32_t* scanAux;
 
 	// contacts, double-buffered [cur], [prev]
@@ -198,6 +201,11 @@ struct b3g_ctx
 	float* dBodyState;
 	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey;
 	float4* dFixParams;
+	float4* dFixBound;
+
+	// host copies of the hull arrays (bounding spheres at fixture upload)
+	std::vector<uint32_t> hHullDesc;
+	std::vector<float> hHullVerts;
 
 	// pinned host staging
 	uint32_t* hCounters;

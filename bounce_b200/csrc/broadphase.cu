@@ -21,7 +21,7 @@
 // created when either proxy moves and destroyed by UpdateContacts once the
 // fat AABBs separate, contact_manager.cpp:270-281).
 
-#include "b3g_internal.cuh"
+#include "collide_common.cuh"
 
 namespace {
 
@@ -202,6 +202,17 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	B.fatLo[i] = make_float4(fat.lo.x, fat.lo.y, fat.lo.z, 0.0f);
 	B.fatHi[i] = make_float4(fat.hi.x, fat.hi.y, fat.hi.z, 0.0f);
 	B.moved[i] = 1;
+}
+
+// Per-body transforms used by the narrowphase, computed once per pass:
+// m_xf and b3Sweep::GetTransform(0) (sweep.h:43-63).
+__global__ void k_body_prep(DevScene S, uint32_t nb)
+{
+	uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+	if (b >= nb)
+		return;
+	pack_xf(S.bodyXf, b, load_xf(S.bodyState + 17 * (size_t)b));
+	pack_xf(S.bodyXf0, b, sweep_xf0(S, b));
 }
 
 // ---------------------------------------------------------------------------
@@ -555,32 +566,27 @@ __device__ __forceinline__ bool pair_filter(const DevScene& S, uint32_t pa, uint
 	return registered(S.fixType[pa], S.fixType[pb]);
 }
 
-// Writes contact slot `slot` for the overlapping proxies pa, pb in the
-// broadphase order (min, max) of proxy ids (b3BroadPhase::Report,
-// broad_phase.cpp:341-342) followed by the factory's primary-type swap
-// (b3Contact::Create, contact.cpp:306-317).
-__device__ __forceinline__ void write_pair(const DevScene& S, Buffers& B, uint32_t cur, uint32_t slot, uint32_t pa,
-	uint32_t pb)
+// The contact record of overlapping proxies pa, pb: the broadphase order
+// (min, max) of proxy ids (b3BroadPhase::Report, broad_phase.cpp:341-342)
+// followed by the factory's primary-type swap (b3Contact::Create,
+// contact.cpp:306-317). x = fixture A, y = fixture B.
+__device__ __forceinline__ uint2 canon_pair(const DevScene& S, uint32_t pa, uint32_t pb)
 {
 	uint32_t keyA = S.fixKey[pa], keyB = S.fixKey[pb];
 	uint32_t f1 = keyA < keyB ? pa : pb;
 	uint32_t f2 = keyA < keyB ? pb : pa;
-	uint32_t A = f1, Bf = f2;
 	if (!primary(S.fixType[f1], S.fixType[f2]))
-	{
-		A = f2;
-		Bf = f1;
-	}
-	B.pairA[cur][slot] = A;
-	B.pairB[cur][slot] = Bf;
+		return make_uint2(f2, f1);
+	return make_uint2(f1, f2);
 }
 
 // Rope walk from leaf j's own rope. A node is read as two float4:
 // (lower, left child | proxy) and (upper, rope). MODE 0 counts the filtered
-// overlaps and keeps the first TRAV_SLOTS partners in the leaf's scratch
-// slots; MODE 1 writes every pair from `base` (leaves whose partners did not
-// fit). MW: several worlds share the tree, so the walk stops at the first
-// node past the query's world (worlds are contiguous in depth-first order).
+// overlaps and keeps the first TRAV_SLOTS contact records in the leaf's
+// scratch slots (slot-major); MODE 1 writes the records past the first
+// TRAV_SLOTS from `base` (leaves whose partners did not fit). MW: several
+// worlds share the tree, so the walk stops at the first node past the query's
+// world (worlds are contiguous in depth-first order).
 constexpr uint32_t TRAV_SLOTS = 16;
 
 template <int MODE, bool MW>
@@ -593,6 +599,7 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 	uint32_t wend = MW ? B.worldEnd[S.bodyWorld[S.fixBody[pa]]] : 0xFFFFFFFFu;
 	uint32_t count = 0;
 	uint32_t node = __float_as_uint(qh.w);
+	uint2* scratch = reinterpret_cast<uint2*>(B.pairScratch);
 	// A depth-first walk visits each of the 2n - 1 nodes at most once.
 	uint32_t steps = 0;
 	const uint32_t maxSteps = 2u * (uint32_t)n + 1u;
@@ -621,13 +628,17 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 				if (MODE == 0)
 				{
 					if (count < TRAV_SLOTS)
-						B.pairScratch[(size_t)count * n + j] = pb;
+						scratch[(size_t)count * n + j] = canon_pair(S, pa, pb);
 				}
-				else
+				else if (count >= TRAV_SLOTS)
 				{
 					uint32_t slot = base + count;
 					if (slot < cap)
-						write_pair(S, B, cur, slot, pa, pb);
+					{
+						uint2 p = canon_pair(S, pa, pb);
+						B.pairA[cur][slot] = p.x;
+						B.pairB[cur][slot] = p.y;
+					}
 				}
 				++count;
 			}
@@ -646,33 +657,33 @@ __global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uin
 	B.leafCount[j] = walk<0, MW>(S, B, n, j, cur, cap, 0);
 }
 
-// After the exclusive scan leafCount holds offsets; a leaf's count is the
-// difference to the next offset (the last one to the total).
+// One thread per (slot, leaf), slot-major: copies the scratch records to the
+// contact arrays. After the exclusive scan leafCount holds offsets; a leaf's
+// count is the difference to the next offset (the last one to the total).
+// Slot-0 threads of leaves with more than TRAV_SLOTS partners walk again for
+// the rest.
 template <bool MW>
 __global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
 {
-	int j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= n)
+	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= (uint32_t)n * TRAV_SLOTS)
 		return;
+	uint32_t k = t / (uint32_t)n, j = t - k * (uint32_t)n;
 	uint32_t base = B.leafCount[j];
-	uint32_t end = (j == n - 1) ? B.counters[CTR_PAIRS] : B.leafCount[j + 1];
+	uint32_t end = (j == (uint32_t)n - 1) ? B.counters[CTR_PAIRS] : B.leafCount[j + 1];
 	uint32_t count = end - base;
-	if (count == 0)
-		return;
-	if (count <= TRAV_SLOTS)
+	if (k < count && k < TRAV_SLOTS)
 	{
-		uint32_t pa = __float_as_uint(B.nodeLo[n - 1 + j].w);
-		for (uint32_t k = 0; k < count; ++k)
+		uint32_t slot = base + k;
+		if (slot < cap)
 		{
-			uint32_t slot = base + k;
-			if (slot < cap)
-				write_pair(S, B, cur, slot, pa, B.pairScratch[(size_t)k * n + j]);
+			uint2 p = reinterpret_cast<const uint2*>(B.pairScratch)[(size_t)k * n + j];
+			B.pairA[cur][slot] = p.x;
+			B.pairB[cur][slot] = p.y;
 		}
 	}
-	else
-	{
-		walk<1, MW>(S, B, n, j, cur, cap, base);
-	}
+	if (k == 0 && count > TRAV_SLOTS)
+		walk<1, MW>(S, B, n, (int)j, cur, cap, base);
 }
 
 // Multi-block exclusive scan of u32 (in place) with the total written to *total.
@@ -725,6 +736,7 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 	uint32_t n = c->nFixtures;
 	if (n == 0)
 		return;
+	k_body_prep<<<(c->nBodies + 255) / 256, 256, 0, s>>>(c->scene, c->nBodies);
 	k_sync<<<(n + 127) / 128, 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
 }
 
@@ -797,8 +809,8 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 		k_traverse_count<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_PAIRS, s);
 	if (c->nWorlds > 1)
-		k_traverse_emit<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
-		k_traverse_emit<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_emit<false><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	prof_mark(c, PM_TRAVERSED, s);
 }

@@ -447,19 +447,28 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 // ---------------------------------------------------------------------------
 // Manifolds.
 
-// b3Manifold::Initialize() (collision.cpp:23-38) plus cleared geometry: the
-// whole 320-byte record is zeroed with 16-byte stores (records are 16-byte
-// aligned in the contact arrays), then the header fields that are not zero.
+// b3Manifold::Initialize() (collision.cpp:23-38): the 32-byte header
+// (pointCount, impulses, speeds) is zeroed with two 16-byte stores; every
+// point a collide routine produces is written whole by set_point. As in the
+// reference, which reuses the manifold memory of a contact from step to step,
+// points at or beyond pointCount keep unspecified older contents.
 __device__ __forceinline__ void man_clear(DevManifold& m)
 {
-	uint4* w = reinterpret_cast<uint4*>(&m);
-#pragma unroll
-	for (int i = 0; i < (int)(sizeof(DevManifold) / 16); ++i)
-		w[i] = make_uint4(0u, 0u, 0u, 0u);
+	uint4* w = reinterpret_cast<uint4*>(&m.pointCount);
+	w[0] = make_uint4(0u, 0u, 0u, 0u);
+	w[1] = make_uint4(0u, 0u, 0u, 0u);
 }
 
+// Writes a produced point: geometry here, the id by set_id / set_id0;
+// normalImpulse, persisting and edgeContact start cleared (Initialize()).
 __device__ __forceinline__ void set_point(DevPoint& p, V3 n, V3 p1, V3 p2)
 {
+	p.normalImpulse = 0.0f;
+	p.pad0 = 0;
+	p.persisting = 0;
+	p.edgeContact = 0;
+	for (int k = 0; k < 6; ++k)
+		p.pad1[k] = 0;
 	p.n[0] = n.x;
 	p.n[1] = n.y;
 	p.n[2] = n.z;
@@ -581,17 +590,30 @@ __device__ __forceinline__ void finish_convex(const NPArgs& a, uint32_t c, DevMa
 	a.cstate[c] = touching | (1u << 8) | (begun << 16);
 }
 
-__device__ __forceinline__ XF body_xf(const DevScene& S, uint32_t body)
+// Per-body transforms prepared once per pass by k_body_prep (two float4 each:
+// translation + rotation.x, rotation.yzw).
+__device__ __forceinline__ XF unpack_xf(const float4* t, uint32_t body)
 {
-	const float* s = S.bodyState + 17 * (size_t)body;
+	float4 a = t[2 * (size_t)body], b = t[2 * (size_t)body + 1];
 	XF x;
-	x.p = V3{s[0], s[1], s[2]};
-	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	x.p = V3{a.x, a.y, a.z};
+	x.q = Q4{V3{a.w, b.x, b.y}, b.z};
 	return x;
 }
+__device__ __forceinline__ void pack_xf(float4* t, uint32_t body, const XF& x)
+{
+	t[2 * (size_t)body] = make_float4(x.p.x, x.p.y, x.p.z, x.q.v.x);
+	t[2 * (size_t)body + 1] = make_float4(x.q.v.y, x.q.v.z, x.q.s, 0.0f);
+}
+
+// b3Body::m_xf.
+__device__ __forceinline__ XF body_xf(const DevScene& S, uint32_t body) { return unpack_xf(S.bodyXf, body); }
+
+// b3Sweep::GetTransform(0), as b3HullContact::Evaluate uses it (hull_contact.cpp:43-44).
+__device__ __forceinline__ XF body_xf0(const DevScene& S, uint32_t body) { return unpack_xf(S.bodyXf0, body); }
 
 // b3Sweep::GetTransform(0) (sweep.h:43-63) from the stored sweep start.
-__device__ __forceinline__ XF body_xf0(const DevScene& S, uint32_t body)
+__device__ __forceinline__ XF sweep_xf0(const DevScene& S, uint32_t body)
 {
 	const float* s = S.bodyState + 17 * (size_t)body;
 	Q4 q1 = Q4{V3{s[10], s[11], s[12]}, s[13]};

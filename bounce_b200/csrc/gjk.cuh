@@ -403,6 +403,10 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 		v.index2 = 0;
 		sx.count = 1;
 	}
+	// The simplex is indexed with constants only (unrolled loops, explicit
+	// slot selection) so it stays in registers.
+	for (int i = 1; i < 4; ++i)
+		sx.v[i] = sx.v[0];
 	uint32_t save1[4], save2[4];
 	uint32_t saveCount = 0;
 	const uint32_t kMaxIters = 20;
@@ -410,7 +414,8 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 	while (iter < kMaxIters)
 	{
 		saveCount = sx.count;
-		for (uint32_t i = 0; i < saveCount; ++i)
+#pragma unroll
+		for (int i = 0; i < 4; ++i)
 		{
 			save1[i] = sx.v[i].index1;
 			save2[i] = sx.v[i].index2;
@@ -426,24 +431,27 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 		V3 d = sx.search_dir();
 		if (dot(d, d) < B3G_EPSILON * B3G_EPSILON)
 			break;
-		SVert& vx = sx.v[sx.count];
+		SVert vx;
 		vx.index1 = gp_support(p1, rotc(xf1.q, -d));
 		vx.point1 = xmul(xf1, gp_vertex(p1, vx.index1));
 		vx.index2 = gp_support(p2, rotc(xf2.q, d));
 		vx.point2 = xmul(xf2, gp_vertex(p2, vx.index2));
 		vx.point = vx.point2 - vx.point1;
+		vx.weight = 0.0f;
 		++iter;
 		bool duplicate = false;
-		for (uint32_t i = 0; i < saveCount; ++i)
-		{
-			if (vx.index1 == save1[i] && vx.index2 == save2[i])
-			{
+#pragma unroll
+		for (int i = 0; i < 4; ++i)
+			if ((uint32_t)i < saveCount && vx.index1 == save1[i] && vx.index2 == save2[i])
 				duplicate = true;
-				break;
-			}
-		}
 		if (duplicate)
 			break;
+		if (sx.count == 1)
+			sx.v[1] = vx;
+		else if (sx.count == 2)
+			sx.v[2] = vx;
+		else
+			sx.v[3] = vx;
 		++sx.count;
 	}
 	GJKOut out;

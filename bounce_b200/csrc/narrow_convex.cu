@@ -432,8 +432,30 @@ __device__ GProxy shape_proxy(const DevScene& S, const ShapeP& s)
 }
 
 // Contacts listed in one bucket, one thread each.
+// Exact cull, not in the reference: every routine of this file returns no
+// point when the shapes are farther apart than their radii sum (the sphere
+// and capsule routines compare closest-point distances with the radii; the
+// hull routines' face loop or GJK, whose witness points lie on the shapes,
+// then report a distance above the radii). Bounding spheres (fixture-local
+// centre, conservative radius from b3g_set_fixtures) separated by more than
+// the radii plus a margin that dominates the FP32 rounding of those
+// distances (1e-3 m + 1e-5 of the coordinate magnitude) therefore mean an
+// empty manifold, and the routine can be skipped without changing the output.
+__device__ __forceinline__ bool spheres_apart(const DevScene& S, uint32_t fa, const XF& xfA, uint32_t fb,
+	const XF& xfB)
+{
+	float4 ba = S.fixBound[fa], bb = S.fixBound[fb];
+	V3 ca = xmul(xfA, V3{ba.x, ba.y, ba.z});
+	V3 cb = xmul(xfB, V3{bb.x, bb.y, bb.z});
+	V3 d = cb - ca;
+	float mag = fmaxf(fmaxf(fmaxf(fabsf(ca.x), fabsf(ca.y)), fabsf(ca.z)),
+		fmaxf(fmaxf(fabsf(cb.x), fabsf(cb.y)), fabsf(cb.z)));
+	float reach = (ba.w + bb.w) + (1e-3f + 1e-5f * mag);
+	return dot(d, d) > reach * reach;
+}
+
 template <int BUCKET>
-__global__ void k_convex(NPArgs a)
+__global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 {
 	uint32_t n = *a.listCount;
 	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
@@ -443,9 +465,15 @@ __global__ void k_convex(NPArgs a)
 		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
 		XF xfA = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
 		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
-		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
 		DevManifold& m = a.man[c];
 		man_clear(m);
+		if (spheres_apart(a.S, fa, xfA, fb, xfB))
+		{
+			finish_convex(a, c, m);
+			a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+			continue;
+		}
+		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
 		if (BUCKET == BK_SPHERES)
 			collide_spheres(m, xfA, sa, xfB, sb);
 		else if (BUCKET == BK_CAPSULE_SPHERE)
