@@ -109,6 +109,7 @@ EXPORTED = [
     "b3g_get_profile",
     "b3g_stage_name",
     "b3g_collide_pairs",
+    "b3g_find_pairs_static",
     "b3g_hull_from_points",
     "b3g_hull_box",
 ]
@@ -159,6 +160,7 @@ def load():
             [ctx, ctypes.c_uint32, u32p, u32p, f32p, f32p, f32p, f32p, u32p, vp],
             ctypes.c_int,
         ),
+        "b3g_find_pairs_static": ([vp, ctypes.c_uint32, vp, ctypes.c_uint32, vp, vp], ctypes.c_int),
         "b3g_hull_from_points": ([f32p, ctypes.c_uint32, f32p, u32p, u32p, f32p, f32p, u32p], ctypes.c_int),
         "b3g_hull_box": (
             [ctypes.c_float, ctypes.c_float, ctypes.c_float, f32p, u32p, u32p, f32p, f32p, u32p],

@@ -220,6 +220,33 @@ int b3g_collide_pairs(b3g_ctx* ctx, uint32_t n, const uint32_t* fixA, const uint
 	const float* xfA, const float* xfB, const float* xf0A, const float* xf0B,
 	uint32_t* cache4, void* manifolds);
 
+/* Pair search without device allocation ------------------------------------
+ *
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: an engine that owns all GPU memory through its own arena, code that
+ * runs while a CUDA graph is being captured (cudaMalloc cannot be captured),
+ * or a thread that must not wait on the allocator. It allocates nothing (no
+ * cudaMalloc, cudaFree or allocating library call); its scratch is one
+ * file-scope device array sized for B3G_STATIC_MAX_PROXIES proxies (about
+ * 200 KB on every GPU that loads the library, held until exit).
+ *
+ * aabbs: n fat AABBs in device memory, 6 floats each (lower, upper), as
+ * b3g_fetch_fat_aabbs returns them. Writes every overlapping pair (closed
+ * test, b3TestOverlap) as (min index, max index) into pairs (device memory,
+ * 2 u32 each, up to capacity pairs, unspecified order) and the number of
+ * overlapping pairs into *count (device memory; may exceed capacity).
+ * Asynchronous on stream (a cudaStream_t, NULL for the legacy stream), on
+ * the current device. Returns B3G_E_CAPACITY when n > B3G_STATIC_MAX_PROXIES.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array: the counters that must start at
+ * zero are cleared by each call, and calls that overlap on the GPU (e.g. on
+ * two unordered streams) race. */
+#define B3G_STATIC_MAX_PROXIES 16384u
+int b3g_find_pairs_static(const float* aabbs, uint32_t n, uint32_t* pairs, uint32_t capacity,
+	uint32_t* count, void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
