@@ -37,7 +37,7 @@ class CollisionPipeline:
             raise N.B3GError(rc, "b3g_create failed")
         self.ctx = h
         self.max_contacts = int(max_contacts)
-        nh = len(scene.hulls)
+        nh = len(ha["desc"]) // 6
         self._check(
             self.lib.b3g_set_hulls(
                 self.ctx, nh, N.ptr(ha["desc"], u32), N.ptr(ha["verts"], f32), N.ptr(ha["edges"], u32),

@@ -183,8 +183,10 @@ class Scene:
         self.fix_flags.append(flags)
         return len(self.fix_body) - 1
 
-    def finalize(self):
-        self.hull_arrays = self.hulls.arrays()
+    def finalize(self, hull_arrays=None):
+        """Pack the lists into arrays. hull_arrays: prebuilt b3g_set_hulls
+        arrays to use instead of this scene's HullPool."""
+        self.hull_arrays = hull_arrays if hull_arrays is not None else self.hulls.arrays()
         self.body_world = np.ascontiguousarray(self.body_world, np.uint32)
         self.body_type = np.ascontiguousarray(self.body_type, np.uint32)
         self.body_pos = np.ascontiguousarray(np.array(self.body_pos, F).reshape(-1, 3))

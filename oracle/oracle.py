@@ -220,6 +220,55 @@ class RefWorld:
         return out
 
 
+_restate = None
+
+
+def restate():
+    """The C restatement of the broadphase front end (restate.c)."""
+    global _restate
+    if _restate is None:
+        path = os.path.join(REF_DIR, "librestate.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: build the oracle with make -C oracle")
+        L = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        L.rs_sync.argtypes = [ctypes.c_int, ctypes.c_uint32] + [vp] * 11
+        L.rs_sync.restype = None
+        L.rs_pairs.argtypes = [ctypes.c_uint32, vp, vp, vp, vp, vp, vp, ctypes.c_uint32]
+        L.rs_pairs.restype = ctypes.c_uint32
+        _restate = L
+    return _restate
+
+
+def restate_sync(scene, state17, fat, awake=None, creation=False):
+    """Fat-AABB update of every fixture (in place on fat, 6 floats each); returns moved flags."""
+    L = restate()
+    nf = scene.n_fixtures
+    aw = np.ascontiguousarray(np.ones(scene.n_bodies, np.uint8) if awake is None else awake, np.uint8)
+    moved = np.zeros(nf, np.uint8)
+    st = np.ascontiguousarray(state17, np.float32)
+    ha = scene.hull_arrays
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    L.rs_sync(1 if creation else 0, nf, p(scene.fix_body), p(scene.fix_type), p(scene.fix_hull), p(scene.fix_params),
+              p(scene.body_type), p(aw), p(st), p(ha["desc"]), p(ha["verts"]), p(fat), p(moved))
+    return moved
+
+
+def restate_pairs(scene, fat, keys=None):
+    """Contact set (fixture A, fixture B) of the fat AABBs, sorted by pair."""
+    L = restate()
+    nf = scene.n_fixtures
+    k = np.ascontiguousarray(np.arange(nf, dtype=np.uint32) if keys is None else keys, np.uint32)
+    p = lambda a: ctypes.c_void_p(a.ctypes.data)
+    cap = 64 * nf + 1024
+    out = np.zeros((cap, 2), np.uint32)
+    n = L.rs_pairs(nf, p(fat), p(scene.fix_body), p(scene.body_type), p(scene.fix_type), p(k), p(out), cap)
+    assert n <= cap
+    out = out[:n]
+    order = np.argsort((out[:, 0].astype(np.uint64) << 32) | out[:, 1])
+    return out[order]
+
+
 def set_convex_cache(on, precision=32):
     lib(precision).refw_set_convex_cache(1 if on else 0)
 

@@ -1,0 +1,87 @@
+"""CPU checks that pin the oracle: the scene generator and hull builder
+reproduce the golden inputs, the reference build reproduces the golden
+outputs it was used to make, and the C restatement of the broadphase front
+end (oracle/restate.c) reproduces the reference's fat AABBs and contact sets."""
+import numpy as np
+import pytest
+
+from bounce_b200 import scene as S
+from tests import golden_util as G
+
+
+@pytest.mark.parametrize("name", G.SCENES)
+def test_generator_reproduces_golden_inputs(name):
+    d = G.load(name)
+    builders = {
+        "plain_small": lambda: S.plain_scene(seed=31, n_boxes=120, n_spheres=120, cube=6.0),
+        "mixed_small": lambda: S.mixed_scene(seed=32, n=400, side=9.0),
+    }
+    sc = builders[name]().finalize()
+    for k in ("desc", "verts", "edges", "faces", "planes"):
+        assert np.array_equal(sc.hull_arrays[k], d[f"hull_{k}"]), k
+    for k in ("body_type", "body_pose", "fix_body", "fix_type", "fix_hull", "fix_params"):
+        assert np.array_equal(getattr(sc, k), d[k]), k
+
+
+@pytest.mark.parametrize("name", G.SCENES)
+def test_reference_reproduces_golden_outputs(name, oracle_mod):
+    O = oracle_mod
+    d = G.load(name)
+    sc = G.scene_from(d)
+    rw = O.RefWorld(sc, 32)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    for p in range(G.PASSES):
+        if p == 0:
+            rw.first_pass()
+        else:
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass()
+        assert np.array_equal(rw.bodies17(), d[f"p{p}_state"])
+        pairs = rw.pairs()
+        order = np.argsort(G.contact_keys(pairs))
+        assert np.array_equal(pairs[order][:, :2], d[f"p{p}_r32_pairs"][:, :2])
+        assert np.array_equal(rw.fat_aabbs(), d[f"p{p}_r32_fat"])
+
+
+@pytest.mark.parametrize("name", G.SCENES)
+def test_restatement_matches_reference_golden(name, oracle_mod):
+    """restate.c: fat AABBs bit-exact and contact sets identical to the
+    reference's, pass after pass (creation pass, then MoveProxy passes)."""
+    O = oracle_mod
+    d = G.load(name)
+    sc = G.scene_from(d)
+    fat = np.zeros((sc.n_fixtures, 6), np.float32)
+    for p in range(G.PASSES):
+        O.restate_sync(sc, d[f"p{p}_state"], fat, creation=(p == 0))
+        assert np.array_equal(fat, d[f"p{p}_r32_fat"]), f"pass {p}: fat AABBs differ"
+        pairs = O.restate_pairs(sc, fat)
+        assert np.array_equal(pairs, d[f"p{p}_r32_pairs"][:, :2]), f"pass {p}: contact sets differ"
+
+
+def test_fp64_rerun_agrees_with_fp32_within_tolerance():
+    """The FP32 reference stated against its FP64 rerun: same contact sets on
+    these scenes, and manifold points within the pipeline's tolerance
+    (1e-4 m) wherever both produce the same point count (SAT ties are counted)."""
+    for name in G.SCENES:
+        d = G.load(name)
+        for p in range(G.PASSES):
+            a, b = d[f"p{p}_r32_pairs"], d[f"p{p}_r64_pairs"]
+            assert np.array_equal(a[:, :2], b[:, :2])
+            pa, pb = d[f"p{p}_r32_point_count"], d[f"p{p}_r64_point_count"]
+            same = np.nonzero(pa == pb)[0]
+            assert len(same) >= 0.97 * len(pa)
+            ta = {int(i): k for k, i in enumerate(d[f"p{p}_r32_touch_index"])}
+            tb = {int(i): k for k, i in enumerate(d[f"p{p}_r64_touch_index"])}
+            worst = 0.0
+            for i in same:
+                if pa[i] == 0:
+                    continue
+                ka, kb = ta[int(i)], tb[int(i)]
+                for j in range(pa[i]):
+                    if not np.array_equal(d[f"p{p}_r32_key"][ka, j], d[f"p{p}_r64_key"][kb, j]):
+                        continue  # feature choice differs: a tie, counted by the GPU tests
+                    e = np.abs(d[f"p{p}_r32_p1"][ka, j] - d[f"p{p}_r64_p1"][kb, j]).max()
+                    worst = max(worst, float(e))
+            assert worst <= 1e-4, (name, p, worst)
