@@ -100,6 +100,7 @@ EXPORTED = [
     "b3g_fetch_manifolds",
     "b3g_fetch_touching",
     "b3g_fetch_ended",
+    "b3g_fetch_awake",
     "b3g_fetch_caches",
     "b3g_fetch_fat_aabbs",
     "b3g_load_impulses",
@@ -148,6 +149,7 @@ def load():
         "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_ended": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_awake": ([ctx, u8p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_caches": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_fat_aabbs": ([ctx, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_load_impulses": ([ctx, f32p, f32p, f32p], ctypes.c_int),

@@ -10,11 +10,6 @@
 
 #include "collide_common.cuh"
 
-void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
-void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
-	cudaStream_t s);
-void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s);
-
 namespace {
 
 int fail(b3g_ctx* c, int code, const char* fmt, ...)
@@ -29,6 +24,15 @@ int fail(b3g_ctx* c, int code, const char* fmt, ...)
 		c->err = buf;
 	}
 	return code;
+}
+
+// Non-static bodies with a cleared awake flag.
+uint32_t count_asleep(const b3g_ctx* c, const uint8_t* awake)
+{
+	uint32_t n = 0;
+	for (size_t i = 0; i < c->hBodyType.size(); ++i)
+		n += (awake[i] == 0 && c->hBodyType[i] != B3G_BODY_STATIC) ? 1u : 0u;
+	return n;
 }
 
 #define CK(call)                                                                                 \
@@ -236,7 +240,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dBodyWorld = c->dBodyType = nullptr;
 	c->dBodyAwake = nullptr;
 	c->dBodyState = nullptr;
-	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = nullptr;
+	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = c->dFixRank = nullptr;
+	c->asleep = 0;
 	c->dFixParams = nullptr;
 	c->dFixBound = nullptr;
 	c->hCounters = nullptr;
@@ -297,6 +302,19 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	}
 	step(dalloc(&B.prevIndex, C), "alloc");
 	step(dalloc(&B.prevFound, C), "alloc");
+	step(dalloc(&B.rawA, C), "alloc");
+	step(dalloc(&B.rawB, C), "alloc");
+	step(dalloc(&B.newList, C), "alloc");
+	step(dalloc(&B.newOff, (size_t)P + 1), "alloc");
+	step(dalloc(&B.newFill, (size_t)P + 1), "alloc");
+	step(dalloc(&B.newTmp, C), "alloc");
+	step(dalloc(&B.newTmpMax, C), "alloc");
+	step(dalloc(&B.keptScan, C), "alloc");
+	step(dalloc(&B.posKey, C), "alloc");
+	step(dalloc(&B.wakeList, C), "alloc");
+	step(dalloc(&B.inactiveSave, C), "alloc");
+	step(dalloc(&B.activated, C), "alloc");
+	step(dalloc(&B.lateDestroyed, C), "alloc");
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
 	step(dalloc(&B.missList, C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
@@ -373,6 +391,20 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	}
 	dfree(B.prevIndex);
 	dfree(B.prevFound);
+	dfree(B.rawA);
+	dfree(B.rawB);
+	dfree(B.newList);
+	dfree(B.newOff);
+	dfree(B.newFill);
+	dfree(B.newTmp);
+	dfree(B.newTmpMax);
+	dfree(B.keptScan);
+	dfree(B.posKey);
+	dfree(B.wakeList);
+	dfree(B.inactiveSave);
+	dfree(B.activated);
+	dfree(B.lateDestroyed);
+	dfree(B.tWake);
 	dfree(B.bucketList);
 	dfree(B.missList);
 	dfree(B.counters);
@@ -406,6 +438,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dFixHull);
 	dfree(c->dFixFlags);
 	dfree(c->dFixKey);
+	dfree(c->dFixRank);
 	dfree(c->dFixParams);
 	dfree(c->dFixBound);
 	if (c->hCounters)
@@ -529,12 +562,14 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 	dfree(c->dBodyState);
 	dfree(c->scene.bodyXf);
 	dfree(c->scene.bodyXf0);
+	dfree(c->buf.tWake);
 	CK(dalloc(&c->dBodyWorld, nb));
 	CK(dalloc(&c->dBodyType, nb));
 	CK(dalloc(&c->dBodyAwake, nb));
 	CK(dalloc(&c->dBodyState, 17 * (size_t)nb));
 	CK(dalloc(&c->scene.bodyXf, 2 * (size_t)nb));
 	CK(dalloc(&c->scene.bodyXf0, 2 * (size_t)nb));
+	CK(dalloc(&c->buf.tWake, nb));
 	if (nb)
 	{
 		CK(cudaMemcpy(c->dBodyWorld, world, sizeof(uint32_t) * nb, cudaMemcpyHostToDevice));
@@ -543,6 +578,8 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 	}
 	c->nBodies = nb;
 	c->nWorlds = nw;
+	c->hBodyType.assign(type, type + nb);
+	c->asleep = count_asleep(c, awake);
 	c->scene.bodyWorld = c->dBodyWorld;
 	c->scene.bodyType = c->dBodyType;
 	c->scene.bodyAwake = c->dBodyAwake;
@@ -570,6 +607,21 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 		if (shapeType[i] == B3G_SHAPE_HULL && hull[i] >= c->nHulls)
 			return fail(c, B3G_E_INVALID, "fixture %u: hull %u out of range", i, hull[i]);
 		key[i] = proxyKey ? proxyKey[i] : i;
+	}
+	// Rank of each proxy key: pairs are ordered by (smaller key, larger key).
+	std::vector<uint32_t> rank(nf);
+	{
+		std::vector<uint32_t> order(nf);
+		for (uint32_t i = 0; i < nf; ++i)
+			order[i] = i;
+		std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+		for (uint32_t r = 0; r < nf; ++r)
+		{
+			if (r > 0 && key[order[r]] == key[order[r - 1]])
+				return fail(c, B3G_E_INVALID, "fixtures %u and %u share proxy key %u", order[r - 1], order[r],
+					key[order[r]]);
+			rank[order[r]] = r;
+		}
 	}
 	std::vector<float4> p4(3 * (size_t)nf);
 	for (size_t i = 0; i < 3 * (size_t)nf; ++i)
@@ -637,12 +689,14 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	dfree(c->dFixHull);
 	dfree(c->dFixFlags);
 	dfree(c->dFixKey);
+	dfree(c->dFixRank);
 	dfree(c->dFixParams);
 	CK(dalloc(&c->dFixBody, nf));
 	CK(dalloc(&c->dFixType, nf));
 	CK(dalloc(&c->dFixHull, nf));
 	CK(dalloc(&c->dFixFlags, nf));
 	CK(dalloc(&c->dFixKey, nf));
+	CK(dalloc(&c->dFixRank, nf));
 	CK(dalloc(&c->dFixParams, 3 * (size_t)nf));
 	if (nf)
 	{
@@ -651,6 +705,7 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 		CK(cudaMemcpy(c->dFixHull, hull, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(c->dFixFlags, flags, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(c->dFixKey, key.data(), sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
+		CK(cudaMemcpy(c->dFixRank, rank.data(), sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
 		CK(cudaMemcpy(c->dFixParams, p4.data(), sizeof(float4) * 3 * nf, cudaMemcpyHostToDevice));
 	}
 	c->hFixType.assign(shapeType, shapeType + nf);
@@ -660,6 +715,7 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	c->scene.fixHull = c->dFixHull;
 	c->scene.fixFlags = c->dFixFlags;
 	c->scene.fixKey = c->dFixKey;
+	c->scene.fixRank = c->dFixRank;
 	c->scene.fixParams = c->dFixParams;
 	c->creationPass = true;
 	c->havePass = false;
@@ -672,8 +728,24 @@ extern "C" int b3g_set_awake(b3g_ctx* c, const uint8_t* awake)
 		return fail(c, B3G_E_INVALID, "b3g_set_awake: null argument");
 	CK(cudaSetDevice(c->device));
 	if (c->nBodies)
+	{
 		CK(cudaMemcpyAsync(c->dBodyAwake, awake, c->nBodies, cudaMemcpyHostToDevice, c->stream));
+		CK(cudaStreamSynchronize(c->stream));
+	}
+	c->asleep = count_asleep(c, awake);
 	return B3G_OK;
+}
+
+extern "C" int b3g_fetch_awake(b3g_ctx* c, uint8_t* out, uint32_t capacity)
+{
+	if (!c || (!out && capacity))
+		return fail(c, B3G_E_INVALID, "b3g_fetch_awake: null argument");
+	CK(cudaSetDevice(c->device));
+	CK(cudaDeviceSynchronize());
+	uint32_t n = std::min(c->nBodies, capacity);
+	if (n)
+		CK(cudaMemcpy(out, c->dBodyAwake, n, cudaMemcpyDeviceToHost));
+	return (int)c->nBodies;
 }
 
 extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* stream)
@@ -706,12 +778,18 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	launch_pairs_diff(c, s);
 	prof_mark(c, PM_DIFFED, s);
 	launch_narrowphase(c, s);
+	if (c->asleep > 0)
+	{
+		int rc = resolve_wakeups(c, s);
+		if (rc)
+			return fail(c, rc, "b3g_collide: wake-up rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
+	}
 	launch_finalize(c, s);
 	prof_mark(c, PM_FINAL, s);
 	if (c->profiling)
 		++c->profPass;
-	// pass_begin, sync, broadphase, diff (+ ended), bucket + 7 convex + 2 hull, finalize + pass_end
-	c->launches += 1 + 2 + broadphase_launches(c) + 3 + (c->havePass ? 1 : 0) + 10 + 2;
+	// pass_begin, sync, broadphase, diff + list order, bucket + 7 convex + 2 hull, finalize + pass_end
+	c->launches += 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 2;
 	CK(cudaGetLastError());
 	c->creationPass = false;
 	c->havePass = true;

@@ -96,6 +96,7 @@ struct DevScene
 	const float4* fixBound;  // bounding sphere per fixture: body-frame centre, radius
 	const uint32_t* fixFlags;
 	const uint32_t* fixKey;
+	const uint32_t* fixRank; // rank of the fixture's proxy key among all keys
 };
 
 struct Buffers
@@ -125,6 +126,17 @@ struct Buffers
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
 	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (16 x n uint2)
 	uint32_t* scanAux;
+	uint32_t* rawA;       // overlapping pairs in traversal order (this pass)
+	uint32_t* rawB;
+
+	// contact-list order: new contacts, then the kept previous ones
+	uint32_t* newList;    // raw indices of pairs without a previous contact
+	uint32_t* newOff;     // per smaller-key rank (reversed): offsets, nFixtures + 1
+	uint32_t* newFill;
+	uint32_t* newTmp;     // raw index per new-contact slot, grouped by smaller key
+	uint32_t* newTmpMax;  // larger key rank per slot
+	uint32_t* keptScan;   // per previous contact: kept flag, then exclusive offsets
+	uint32_t* posKey;     // per contact: position in the list UpdateContacts walks
 
 	// contacts, double-buffered [cur], [prev]
 	uint32_t* pairA[2];
@@ -133,7 +145,7 @@ struct Buffers
 	uint4* cache[2];
 	DevManifold* man[2];
 	int32_t* prevIndex; // per current contact
-	uint32_t* prevFound; // per previous contact
+	uint32_t* prevFound; // per previous contact: its pair overlaps again this pass
 	unsigned long long* hashKeys[2];
 	uint32_t* hashVals[2];
 	uint32_t hashCap;
@@ -147,6 +159,13 @@ struct Buffers
 	uint32_t* touchIndex;
 	DevManifold* touchMan;
 	uint32_t* contactOut; // 3 u32 per contact: A, B, flags
+
+	// wake-ups of UpdateContacts (only when some body is asleep)
+	uint32_t* tWake;        // per body: earliest list position that woke it
+	uint32_t* wakeList;     // contacts activated this round
+	uint32_t* inactiveSave; // contacts skipped as inactive in the first round
+	uint32_t* activated;    // per inactiveSave entry
+	uint32_t* lateDestroyed; // per contact
 
 	// warm start from the host solver
 	float* impulseNormal;
@@ -168,7 +187,14 @@ enum
 	CTR_STATUS,
 	CTR_TOUCH_OUT,
 	CTR_HULL_MISS,      // hull-hull contacts the feature cache did not resolve
+	CTR_RAW,            // overlapping pairs found by the traversal
+	CTR_KEPT,           // previous contacts kept
+	CTR_WAKE_EVENTS,
+	CTR_WAKE_ACTIVATED,
+	CTR_LATE_DESTROYED,
 	CTR_BUCKET0 = 16,   // BK_COUNT bucket sizes
+	CTR_ASLEEP = 27,    // non-static bodies still asleep after the wake-ups
+	CTR_SCRATCH = 28,
 	CTR_COUNT = 32
 };
 
@@ -199,7 +225,7 @@ struct b3g_ctx
 	uint32_t *dBodyWorld, *dBodyType;
 	uint8_t* dBodyAwake;
 	float* dBodyState;
-	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey;
+	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey, *dFixRank;
 	float4* dFixParams;
 	float4* dFixBound;
 
@@ -212,6 +238,11 @@ struct b3g_ctx
 
 	// host copies of fixture types (for the stand-alone narrowphase)
 	std::vector<uint32_t> hFixType;
+
+	// host copy of body types; non-static bodies asleep at the start of the
+	// next pass
+	std::vector<uint32_t> hBodyType;
+	uint32_t asleep;
 
 	// kernels launched by passes (host count)
 	uint64_t launches;
@@ -253,6 +284,8 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s);
 void launch_pairs_diff(b3g_ctx* c, cudaStream_t s);
 void launch_narrowphase(b3g_ctx* c, cudaStream_t s);
 void launch_finalize(b3g_ctx* c, cudaStream_t s);
+uint32_t pairs_diff_launches(const b3g_ctx* c);
+int resolve_wakeups(b3g_ctx* c, cudaStream_t s);
 void launch_collide_pairs(b3g_ctx* c, cudaStream_t s, uint32_t n, const uint32_t* fixA,
 	const uint32_t* fixB, const float* xfA, const float* xfB, const float* xf0A,
 	const float* xf0B, uint4* cache, DevManifold* out);

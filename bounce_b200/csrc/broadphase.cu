@@ -16,10 +16,10 @@
 //                (contact_manager.cpp:98-160) and the b3Contact::Create A/B
 //                order (contact.cpp:290-322) are applied per pair
 //
-// The overlap set found this way equals the reference's contact set after
-// FindNewContacts: a contact exists iff its fat AABBs overlap (pairs are
-// created when either proxy moves and destroyed by UpdateContacts once the
-// fat AABBs separate, contact_manager.cpp:270-281).
+// The overlap set found this way is the set of pairs the reference has a
+// contact for after FindNewContacts (pairs are created when either proxy
+// moves); order.cu turns it into the contact list, which also keeps the
+// contacts UpdateContacts skips because neither body is active.
 
 #include "collide_common.cuh"
 
@@ -146,10 +146,15 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 		B.moved[i] = 1;
 		return;
 	}
+	// Every non-static body is synchronised, whatever its awake flag:
+	// b3World::Solve synchronises each body of a solved island
+	// (world.cpp:424-449), including those the island put to sleep in that
+	// step (island.cpp:297-305). A body asleep since its last move keeps its
+	// sweep, so synchronising it again finds its AABB inside the fat AABB it
+	// got then and moves nothing: the result is the reference's, which skips it.
 	uint32_t btype = S.bodyType[body];
-	if (btype == B3G_BODY_STATIC || S.bodyAwake[body] == 0)
+	if (btype == B3G_BODY_STATIC)
 	{
-		// Not in an island: not synchronised (world.cpp:427-442).
 		B.moved[i] = 0;
 		return;
 	}
@@ -636,8 +641,8 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 					if (slot < cap)
 					{
 						uint2 p = canon_pair(S, pa, pb);
-						B.pairA[cur][slot] = p.x;
-						B.pairB[cur][slot] = p.y;
+						B.rawA[slot] = p.x;
+						B.rawB[slot] = p.y;
 					}
 				}
 				++count;
@@ -670,7 +675,7 @@ __global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint
 		return;
 	uint32_t k = t / (uint32_t)n, j = t - k * (uint32_t)n;
 	uint32_t base = B.leafCount[j];
-	uint32_t end = (j == (uint32_t)n - 1) ? B.counters[CTR_PAIRS] : B.leafCount[j + 1];
+	uint32_t end = (j == (uint32_t)n - 1) ? B.counters[CTR_RAW] : B.leafCount[j + 1];
 	uint32_t count = end - base;
 	if (k < count && k < TRAV_SLOTS)
 	{
@@ -678,8 +683,8 @@ __global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint
 		if (slot < cap)
 		{
 			uint2 p = reinterpret_cast<const uint2*>(B.pairScratch)[(size_t)k * n + j];
-			B.pairA[cur][slot] = p.x;
-			B.pairB[cur][slot] = p.y;
+			B.rawA[slot] = p.x;
+			B.rawB[slot] = p.y;
 		}
 	}
 	if (k == 0 && count > TRAV_SLOTS)
@@ -761,7 +766,7 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	uint32_t cur = c->cur;
 	if (n == 0)
 	{
-		cudaMemsetAsync(B.counters + CTR_PAIRS, 0, sizeof(uint32_t), s);
+		cudaMemsetAsync(B.counters + CTR_RAW, 0, sizeof(uint32_t), s);
 		return;
 	}
 	int* bnd = (int*)B.sceneBounds;
@@ -807,7 +812,7 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 		k_traverse_count<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
 		k_traverse_count<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
-	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_PAIRS, s);
+	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, s);
 	if (c->nWorlds > 1)
 		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else

@@ -534,6 +534,93 @@ struct NPArgs
 	uint32_t* missCount;
 };
 
+// ---------------------------------------------------------------------------
+// Pair hash tables (one per pass): open addressing, fixture pair -> contact.
+
+constexpr unsigned long long B3G_EMPTY_KEY = 0xFFFFFFFFFFFFFFFFull;
+
+__device__ __forceinline__ unsigned long long pair_key(uint32_t a, uint32_t b)
+{
+	return ((unsigned long long)a << 32) | b;
+}
+
+__device__ __forceinline__ uint32_t pair_hash(unsigned long long k)
+{
+	k ^= k >> 33;
+	k *= 0xff51afd7ed558ccdull;
+	k ^= k >> 33;
+	k *= 0xc4ceb9fe1a85ec53ull;
+	k ^= k >> 33;
+	return (uint32_t)k;
+}
+
+// Contact index of `key`, or -1.
+__device__ __forceinline__ int32_t pair_hash_find(const unsigned long long* keys, const uint32_t* vals,
+	uint32_t capPow2, unsigned long long key)
+{
+	uint32_t mask = capPow2 - 1u;
+	uint32_t h = pair_hash(key) & mask;
+	for (uint32_t probe = 0; probe <= mask; ++probe)
+	{
+		unsigned long long k = keys[h];
+		if (k == key)
+			return (int32_t)vals[h];
+		if (k == B3G_EMPTY_KEY)
+			return -1;
+		h = (h + 1) & mask;
+	}
+	return -1;
+}
+
+// False when the table is full.
+__device__ __forceinline__ bool pair_hash_insert(unsigned long long* keys, uint32_t* vals, uint32_t capPow2,
+	unsigned long long key, uint32_t value)
+{
+	uint32_t mask = capPow2 - 1u;
+	uint32_t h = pair_hash(key) & mask;
+	for (uint32_t probe = 0; probe <= mask; ++probe)
+	{
+		unsigned long long old = atomicCAS(&keys[h], B3G_EMPTY_KEY, key);
+		if (old == B3G_EMPTY_KEY || old == key)
+		{
+			vals[h] = value;
+			return true;
+		}
+		h = (h + 1) & mask;
+	}
+	return false;
+}
+
+// Shape-type pair -> narrowphase bucket (A carries the primary type;
+// contact.cpp:60-68).
+__device__ __forceinline__ uint32_t bucket_of(uint32_t ta, uint32_t tb)
+{
+	if (ta == B3G_SHAPE_SPHERE)
+		return BK_SPHERES;
+	if (ta == B3G_SHAPE_CAPSULE)
+		return tb == B3G_SHAPE_SPHERE ? BK_CAPSULE_SPHERE : BK_CAPSULES;
+	if (ta == B3G_SHAPE_TRIANGLE)
+		return tb == B3G_SHAPE_SPHERE ? BK_TRIANGLE_SPHERE : BK_TRIANGLE_CAPSULE;
+	if (ta == B3G_SHAPE_HULL)
+	{
+		if (tb == B3G_SHAPE_SPHERE)
+			return BK_HULL_SPHERE;
+		if (tb == B3G_SHAPE_CAPSULE)
+			return BK_HULL_CAPSULE;
+		if (tb == B3G_SHAPE_TRIANGLE)
+			return BK_HULL_TRIANGLE;
+		return BK_HULLS;
+	}
+	return BK_COUNT; // mesh pairs: not handled by these buckets
+}
+
+// Narrowphase arguments of the current pass (contact arrays of c->cur).
+NPArgs make_np_args(b3g_ctx* c);
+void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	cudaStream_t s);
+void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s);
+void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
+
 __device__ __forceinline__ XF load_xf7(const float* s)
 {
 	XF x;

@@ -507,7 +507,10 @@ __global__ void k_sensor(NPArgs a)
 		uint32_t begun = prev < 0 ? 1u : 0u;
 		a.cstate[c] = touching | (begun << 16);
 		man_clear(a.man[c]);
-		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+		// A hull-hull sensor contact keeps the b3FeatureCache it was built
+		// with: e_empty (sat.h:69), the other fields unset.
+		bool hulls = a.S.fixType[fa] == B3G_SHAPE_HULL && a.S.fixType[fb] == B3G_SHAPE_HULL;
+		a.cache[c] = make_uint4(hulls ? 0u : B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
 }
 

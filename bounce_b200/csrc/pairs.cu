@@ -1,129 +1,54 @@
 // Persistent-pair bookkeeping of one pass and the narrowphase dispatch.
 //
 //  k_diff      looks each overlapping pair up in the previous pass's hash
-//              table (pair key -> contact index) and inserts it into this
-//              pass's table: found = the contact persists (its manifold and
-//              feature cache are carried over), missing = a new contact
-//              (b3ContactManager::AddPair, contact_manager.cpp:98-201)
-//  k_ended     previous contacts whose pair was not found again are the ones
-//              UpdateContacts destroys because their fat AABBs stopped
-//              overlapping (contact_manager.cpp:270-281)
+//              table (pair key -> contact index): found = the contact persists
+//              (its manifold and feature cache are carried over), missing = a
+//              new contact (b3ContactManager::AddPair, contact_manager.cpp:63-140);
+//              new pairs are listed and counted per smaller proxy key for the
+//              list-order layout (order.cu), which also lists the contacts
+//              UpdateContacts destroys (contact_manager.cpp:263-276)
 //  k_bucket    one work list per b3Contact subclass (contact.cpp:253-288)
 //  k_finalize  touching counts and the host-facing contact records
 
 #include "collide_common.cuh"
 
-void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
-	cudaStream_t s);
-void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s);
-void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
+void launch_order(b3g_ctx* c, cudaStream_t s);
+uint32_t order_launches(const b3g_ctx* c);
 
 namespace {
 
-constexpr unsigned long long EMPTY_KEY = 0xFFFFFFFFFFFFFFFFull;
-
-__device__ __forceinline__ uint32_t hash64(unsigned long long k)
+__global__ void k_diff(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32_t nf, int havePrev)
 {
-	k ^= k >> 33;
-	k *= 0xff51afd7ed558ccdull;
-	k ^= k >> 33;
-	k *= 0xc4ceb9fe1a85ec53ull;
-	k ^= k >> 33;
-	return (uint32_t)k;
-}
-
-__global__ void k_diff(Buffers B, uint32_t cur, uint32_t cap, int havePrev)
-{
-	uint32_t n = min(B.counters[CTR_PAIRS], cap);
+	uint32_t n = min(B.counters[CTR_RAW], cap);
 	uint32_t prevBuf = cur ^ 1u;
-	uint32_t mask = B.hashCap - 1u;
-	const unsigned long long* pk = B.hashKeys[prevBuf];
-	const uint32_t* pv = B.hashVals[prevBuf];
-	unsigned long long* ck = B.hashKeys[cur];
-	uint32_t* cv = B.hashVals[cur];
-	uint32_t begun = 0;
-	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+	const uint32_t lane = threadIdx.x & 31;
+	for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
 	{
-		unsigned long long key = ((unsigned long long)B.pairA[cur][c] << 32) | B.pairB[cur][c];
-		uint32_t h = hash64(key) & mask;
-		int32_t prev = -1;
-		if (havePrev)
+		uint32_t c = base + threadIdx.x;
+		bool isNew = false;
+		if (c < n)
 		{
-			for (uint32_t probe = 0; probe <= mask; ++probe)
+			uint32_t a = B.rawA[c], b = B.rawB[c];
+			int32_t prev = havePrev ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf], B.hashCap,
+											pair_key(a, b))
+									: -1;
+			if (prev >= 0)
+				B.prevFound[prev] = 1;
+			else
 			{
-				unsigned long long k = pk[h];
-				if (k == key)
-				{
-					prev = (int32_t)pv[h];
-					break;
-				}
-				if (k == EMPTY_KEY)
-					break;
-				h = (h + 1) & mask;
+				isNew = true;
+				atomicAdd(&B.newOff[nf - 1u - min(S.fixRank[a], S.fixRank[b])], 1u);
 			}
 		}
-		B.prevIndex[c] = prev;
-		if (prev >= 0)
-			B.prevFound[prev] = 1;
-		else
-			++begun;
-		h = hash64(key) & mask;
-		bool done = false;
-		for (uint32_t probe = 0; probe <= mask; ++probe)
-		{
-			unsigned long long old = atomicCAS(&ck[h], EMPTY_KEY, key);
-			if (old == EMPTY_KEY || old == key)
-			{
-				cv[h] = c;
-				done = true;
-				break;
-			}
-			h = (h + 1) & mask;
-		}
-		if (!done)
-			atomicOr(&B.counters[CTR_STATUS], B3G_ST_HASH_OVERFLOW);
+		// Warp-aggregated append to the new-pair list.
+		uint32_t ballot = __ballot_sync(0xffffffffu, isNew);
+		uint32_t slot = 0;
+		if (lane == 0 && ballot)
+			slot = atomicAdd(&B.counters[CTR_BEGUN], (uint32_t)__popc(ballot));
+		slot = __shfl_sync(0xffffffffu, slot, 0);
+		if (isNew)
+			B.newList[slot + __popc(ballot & ((1u << lane) - 1u))] = c;
 	}
-	for (int o = 16; o > 0; o >>= 1)
-		begun += __shfl_xor_sync(0xffffffffu, begun, o);
-	if ((threadIdx.x & 31) == 0 && begun)
-		atomicAdd(&B.counters[CTR_BEGUN], begun);
-}
-
-__global__ void k_ended(Buffers B, uint32_t cur, uint32_t cap)
-{
-	uint32_t prevBuf = cur ^ 1u;
-	uint32_t n = min(B.counters[CTR_PREV_PAIRS], cap);
-	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-	{
-		if (B.prevFound[p])
-			continue;
-		uint32_t slot = atomicAdd(&B.counters[CTR_ENDED], 1u);
-		B.endedList[3 * slot + 0] = B.pairA[prevBuf][p];
-		B.endedList[3 * slot + 1] = B.pairB[prevBuf][p];
-		B.endedList[3 * slot + 2] = B.cstate[prevBuf][p];
-	}
-}
-
-// Shape-type pair -> bucket (A carries the primary type).
-__device__ __forceinline__ uint32_t bucket_of(uint32_t ta, uint32_t tb)
-{
-	if (ta == B3G_SHAPE_SPHERE)
-		return BK_SPHERES;
-	if (ta == B3G_SHAPE_CAPSULE)
-		return tb == B3G_SHAPE_SPHERE ? BK_CAPSULE_SPHERE : BK_CAPSULES;
-	if (ta == B3G_SHAPE_TRIANGLE)
-		return tb == B3G_SHAPE_SPHERE ? BK_TRIANGLE_SPHERE : BK_TRIANGLE_CAPSULE;
-	if (ta == B3G_SHAPE_HULL)
-	{
-		if (tb == B3G_SHAPE_SPHERE)
-			return BK_HULL_SPHERE;
-		if (tb == B3G_SHAPE_CAPSULE)
-			return BK_HULL_CAPSULE;
-		if (tb == B3G_SHAPE_TRIANGLE)
-			return BK_HULL_TRIANGLE;
-		return BK_HULLS;
-	}
-	return BK_COUNT; // mesh pairs: not handled by these buckets
 }
 
 __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
@@ -218,7 +143,7 @@ __global__ void k_count_moved(Buffers B, uint32_t n)
 
 __global__ void k_overflow_check(Buffers B, uint32_t cap)
 {
-	if (B.counters[CTR_PAIRS] > cap)
+	if (B.counters[CTR_RAW] > cap)
 		atomicOr(&B.counters[CTR_STATUS], B3G_ST_PAIR_OVERFLOW);
 }
 
@@ -229,21 +154,26 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 	Buffers& B = c->buf;
 	uint32_t cap = c->cfg.max_contacts;
 	uint32_t cur = c->cur;
+	uint32_t nf = c->nFixtures;
 	cudaMemsetAsync(B.hashKeys[cur], 0xFF, sizeof(unsigned long long) * B.hashCap, s);
 	cudaMemsetAsync(B.prevFound, 0, sizeof(uint32_t) * cap, s);
+	cudaMemsetAsync(B.newOff, 0, sizeof(uint32_t) * (nf + 1), s);
+	cudaMemsetAsync(B.newFill, 0, sizeof(uint32_t) * (nf + 1), s);
 	k_overflow_check<<<1, 1, 0, s>>>(B, cap);
-	k_diff<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, c->havePass ? 1 : 0);
-	if (c->havePass)
-		k_ended<<<persistent_blocks(4), 256, 0, s>>>(B, cur, cap);
+	k_diff<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, cur, cap, nf, c->havePass ? 1 : 0);
+	launch_order(c, s);
 	k_count_moved<<<persistent_blocks(2), 256, 0, s>>>(B, c->nFixtures);
 }
 
-void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
+uint32_t pairs_diff_launches(const b3g_ctx* c)
+{
+	return 2 + order_launches(c) + 1;
+}
+
+NPArgs make_np_args(b3g_ctx* c)
 {
 	Buffers& B = c->buf;
-	uint32_t cap = c->cfg.max_contacts;
 	uint32_t cur = c->cur, prev = cur ^ 1u;
-	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, cur, cap);
 	NPArgs a;
 	a.S = c->scene;
 	a.pairA = B.pairA[cur];
@@ -266,6 +196,15 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
 	a.missList = B.missList;
 	a.missCount = B.counters + CTR_HULL_MISS;
+	return a;
+}
+
+void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
+{
+	Buffers& B = c->buf;
+	uint32_t cap = c->cfg.max_contacts;
+	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
+	NPArgs a = make_np_args(c);
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, s);
 	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,

@@ -37,6 +37,7 @@ class CollisionPipeline:
             raise N.B3GError(rc, "b3g_create failed")
         self.ctx = h
         self.max_contacts = int(max_contacts)
+        self.n_bodies = int(scene.n_bodies)
         nh = len(ha["desc"]) // 6
         self._check(
             self.lib.b3g_set_hulls(
@@ -122,6 +123,12 @@ class CollisionPipeline:
         out = np.zeros((max(c["ended"], 1), 3), np.uint32)
         m = self._check(self.lib.b3g_fetch_ended(self.ctx, N.ptr(out, u32), c["ended"]))
         return out[:m]
+
+    def awake(self):
+        """Awake flag per body after the last pass (its wake-ups applied)."""
+        out = np.zeros(max(self.n_bodies, 1), np.uint8)
+        self._check(self.lib.b3g_fetch_awake(self.ctx, N.ptr(out, ctypes.c_uint8), self.n_bodies))
+        return out[: self.n_bodies]
 
     def caches(self):
         n = self.counts()["contacts"]

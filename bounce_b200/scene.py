@@ -270,10 +270,15 @@ def ellipsoid_points(rng, n, axes):
     return (d * axes).astype(F)
 
 
-def mixed_scene(seed=2, n=65536, side=49.0, hull_pts=(8, 32), hull_axes=(0.3, 1.2), world=0, scene=None):
-    """Mixed spheres / capsules / hulls in a cube, all dynamic."""
+def mixed_scene(seed=2, n=65536, side=49.0, hull_pts=(8, 32), hull_axes=(0.3, 1.2), world=0, scene=None,
+                static_frac=0.0, sensor_frac=0.0):
+    """Mixed spheres / capsules / hulls in a cube, all dynamic unless
+    static_frac / sensor_frac turn that fraction of the bodies static / of the
+    fixtures into sensors (drawn from a second generator, so the other draws
+    do not change)."""
     rng = np.random.default_rng(seed)
     s = scene if scene is not None else Scene()
+    b0, f0 = len(s.body_type), len(s.fix_type)
     kind = rng.random(n)
     pos = rng.uniform(-side / 2, side / 2, (n, 3)).astype(F)
     quat = random_quats(rng, n)
@@ -298,6 +303,14 @@ def mixed_scene(seed=2, n=65536, side=49.0, hull_pts=(8, 32), hull_axes=(0.3, 1.
                 except ValueError:
                     continue
             s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=h)
+    if static_frac > 0 or sensor_frac > 0:
+        rng2 = np.random.default_rng(seed + 0x5EED)
+        for i in np.nonzero(rng2.random(n) < static_frac)[0]:
+            s.body_type[b0 + i] = N.BODY_STATIC
+            s.body_lin[b0 + i] = np.zeros(3, F)
+            s.body_ang[b0 + i] = np.zeros(3, F)
+        for i in np.nonzero(rng2.random(n) < sensor_frac)[0]:
+            s.fix_flags[f0 + i] = N.FIXTURE_SENSOR
     return s
 
 
@@ -348,10 +361,11 @@ class KinematicDriver:
         self.moving = scene.body_type != N.BODY_STATIC
         self.step_index = 0
 
-    def advance(self):
-        """Move one step (static bodies stay)."""
+    def advance(self, mask=None):
+        """Move one step (static bodies stay; with a mask, only the bodies it
+        flags move, the others keep their sweep as a sleeping body does)."""
         dt = self.dt
-        m = self.moving
+        m = self.moving if mask is None else (self.moving & (np.asarray(mask) != 0))
         if self.walls is not None:
             out_hi = (self.c > self.walls) & (self.lin > 0)
             out_lo = (self.c < -self.walls) & (self.lin < 0)

@@ -131,7 +131,9 @@ int b3g_set_fixtures(b3g_ctx* ctx, uint32_t fixture_count, const uint32_t* body,
 	const uint32_t* shape_type, const uint32_t* hull, const float* params,
 	const uint32_t* flags, const uint32_t* proxy_key);
 
-/* Awake flags per body. Replaces: b3Body::SetAwake (body.h:588-603). */
+/* Awake flags per body. Replaces: b3Body::SetAwake (body.h:588-603). A pass
+ * applies its own wake-ups to these flags (see b3g_fetch_awake), so the host
+ * only needs to call this when its solver puts bodies to sleep or wakes them. */
 int b3g_set_awake(b3g_ctx* ctx, const uint8_t* awake);
 
 /* Pass ------------------------------------------------------------------ */
@@ -157,7 +159,15 @@ int b3g_get_counts(b3g_ctx* ctx, b3g_counts* out);
 /* Contacts of the last pass, 3 u32 each: fixtureA, fixtureB (after the
  * b3Contact::Create A/B swap, contact.cpp:306-317), flags (bit0 touching,
  * bit1 begun this pass, bits 8-15 manifold count). Up to capacity records;
- * returns the number written or a negative status. */
+ * returns the number written or a negative status.
+ * Every per-contact output is in the order of the reference's contact list
+ * (b3ContactManager::m_contactList) after UpdateContacts: the contacts this
+ * pass created, in descending (smaller proxy key, larger proxy key) order
+ * (AddPair prepends the pairs FindPairs reports in ascending order,
+ * broad_phase.h:181-206, contact_manager.cpp:105-111), then the older contacts
+ * in their previous order. A contact whose fat AABBs no longer overlap is kept
+ * (state unchanged) while neither body is active, as UpdateContacts skips it
+ * (contact_manager.cpp:253-259). */
 int b3g_fetch_contacts(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
 
 /* Manifolds of the last pass in contact order, each in the reference's
@@ -169,9 +179,17 @@ int b3g_fetch_manifolds(b3g_ctx* ctx, void* out, uint32_t capacity);
 int b3g_fetch_touching(b3g_ctx* ctx, uint32_t* index, void* manifolds, uint32_t capacity);
 
 /* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above
- * (flags of the destroyed contact). Replaces the Destroy calls of
- * UpdateContacts (contact_manager.cpp:270-281). */
+ * (flags of the destroyed contact), in the order UpdateContacts destroys them.
+ * Replaces the Destroy calls of UpdateContacts (contact_manager.cpp:270-281). */
 int b3g_fetch_ended(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
+
+/* Awake flag per body after the last pass: the flags the pass started with
+ * plus the wake-ups of UpdateContacts, resolved in contact-list order (a
+ * contact that starts or stops touching wakes both bodies, contact.cpp:249-254;
+ * a destroyed contact with points wakes both, contact.cpp:108-126; contacts
+ * later in the list see those bodies awake). Writes min(body count, capacity)
+ * bytes and returns the body count. */
+int b3g_fetch_awake(b3g_ctx* ctx, uint8_t* out, uint32_t capacity);
 
 /* Hull feature caches (b3FeatureCache, sat.h:65-86) in contact order:
  * cacheType, featureType, index1, index2; 0xFFFFFFFF for non hull-hull. */

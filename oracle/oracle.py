@@ -78,6 +78,8 @@ def lib(precision=32):
         "refw_get_bodies": ([vp, f32p], None),
         "refw_set_sweeps": ([vp, f32p], None),
         "refw_set_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
+        "refw_get_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
+        "refw_pass_sleep": ([vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint8), f64p], None),
         "refw_set_convex_cache": ([ctypes.c_uint32], None),
         "refw_first_pass": ([vp, f64p], None),
         "refw_pass": ([vp, f64p], None),
@@ -186,6 +188,21 @@ class RefWorld:
         self.L.refw_pass(self.w, _p(t, ctypes.c_double))
         self.times = t
         return t
+
+    def step_pass_sleep(self, moved, awake):
+        """A pass whose synchronised bodies are `moved` and whose
+        UpdateContacts starts with the awake flags `awake`."""
+        t = np.zeros(2)
+        m = np.ascontiguousarray(moved, np.uint8)
+        a = np.ascontiguousarray(awake, np.uint8)
+        self.L.refw_pass_sleep(self.w, _p(m, ctypes.c_uint8), _p(a, ctypes.c_uint8), _p(t, ctypes.c_double))
+        self.times = t
+        return t
+
+    def awake(self):
+        out = np.zeros(len(self.bodies17()) // 17, np.uint8)
+        self.L.refw_get_awake(self.w, _p(out, ctypes.c_uint8))
+        return out
 
     def contact_count(self):
         return self.L.refw_contact_count(self.w)

@@ -381,6 +381,41 @@ REF_API void refw_pass(void* p, double* times)
 	times[1] = t2 - t1;
 }
 
+// A pass in which some bodies fall asleep at the end of the solve that moved
+// them (b3Island::Solve puts an island to sleep after integrating it,
+// island.cpp:297-305, and b3World::Solve still synchronises its fixtures,
+// world.cpp:424-449): the bodies flagged in `moved`
+// are synchronised, pairs are found, then the awake flags become `awake` and
+// UpdateContacts runs.
+REF_API void refw_pass_sleep(void* p, const uint8_t* moved, const uint8_t* awake, double* times)
+{
+	RefWorld* w = (RefWorld*)p;
+	b3World* world = w->world;
+	double t0 = Now();
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		b3Body* b = w->bodies[i];
+		if (b->GetType() != e_staticBody && moved[i])
+			b->SynchronizeFixtures();
+	}
+	world->m_contactManager.SynchronizeFixtures();
+	world->m_contactManager.FindNewContacts();
+	refw_set_awake(p, awake);
+	double t1 = Now();
+	world->m_contactManager.UpdateContacts();
+	double t2 = Now();
+	times[0] = t1 - t0;
+	times[1] = t2 - t1;
+}
+
+// Awake flags per body (1 awake, 0 asleep).
+REF_API void refw_get_awake(void* p, uint8_t* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+		out[i] = w->bodies[i]->IsAwake() ? 1 : 0;
+}
+
 REF_API uint32_t refw_contact_count(void* p)
 {
 	return ((RefWorld*)p)->world->m_contactManager.m_contactCount;

@@ -58,15 +58,98 @@ def test_mixed_passes(oracle_mod):
     assert st[-1]["touching"] > 100
 
 
-@pytest.mark.xfail(strict=True, reason="wake-ups inside UpdateContacts follow the reference's contact-list "
-                   "order (contact.cpp:455-460, contact.cpp:227-237); the pass does not propagate them yet")
+def compare_order(pipe, rw, label):
+    """The contact arrays follow the reference's contact list exactly:
+    fixtures, touching flag and manifold count per position."""
+    g = pipe.contacts()
+    r = rw.pairs()
+    assert len(g) == len(r), f"{label}: {len(g)} contacts vs {len(r)}"
+    bad = np.nonzero(np.any(g[:, :2] != r[:, :2], axis=1))[0]
+    assert len(bad) == 0, f"{label}: list order differs at {len(bad)} positions, first {bad[:5]}: {g[bad[:3]]} vs {r[bad[:3]]}"
+    assert np.array_equal(g[:, 2] & 0xFF01, r[:, 2] & 0xFF01), f"{label}: flags differ in list order"
+
+
+def test_list_order(oracle_mod):
+    """New contacts first in descending proxy-pair order, then the older ones
+    in their previous order (broad_phase.h:181-206, contact_manager.cpp:105-111),
+    and the destroyed ones listed in list order."""
+    sc = S.mixed_scene(seed=11, n=2000, side=16.0).finalize()
+    rw = oracle_mod.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    prev = None
+    for k in range(6):
+        if k:
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass()
+        else:
+            rw.first_pass()
+        pipe.collide(drv.state17())
+        assert pipe.counts()["status"] == 0
+        compare_order(pipe, rw, f"order pass {k}")
+        cur = rw.pairs()
+        if prev is not None:
+            ck = set(map(tuple, cur[:, :2].tolist()))
+            want = np.array([r for r in prev.tolist() if (r[0], r[1]) not in ck], np.uint32).reshape(-1, 3)
+            got = pipe.ended()
+            assert np.array_equal(got[:, :2], want[:, :2]), f"pass {k}: ended list"
+            assert np.array_equal(got[:, 2] & 1, want[:, 2] & 1), f"pass {k}: ended touching flags"
+        prev = cur
+    pipe.close()
+
+
+def run_sleeping(O, sc, passes, label, seed, sleep_frac):
+    """Sleep as the reference's solver produces it: the bodies awake after a
+    pass (wake-ups included) move in the next one, a random part of them falls
+    asleep right after moving (synchronised, then asleep for UpdateContacts),
+    and a sleeping body keeps its sweep."""
+    rw = O.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    rng = np.random.default_rng(seed)
+    dynamic = sc.body_type != 0
+    moved = np.ones(sc.n_bodies, np.uint8)
+    woken_total = 0
+    for k in range(passes):
+        if k:
+            drv.advance(moved)
+            awake = moved & (rng.random(sc.n_bodies) > sleep_frac).astype(np.uint8)
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass_sleep(moved, awake)
+            pipe.set_awake(awake)
+        else:
+            awake = moved
+            rw.first_pass()
+        pipe.collide(drv.state17())
+        c = pipe.counts()
+        assert c["status"] == 0, c
+        compare_fat_aabbs(pipe, rw, f"{label} pass {k}")
+        compare_contacts(pipe, rw, f"{label} pass {k}")
+        compare_order(pipe, rw, f"{label} pass {k}")
+        ga, ra = pipe.awake(), rw.awake()
+        bad = np.nonzero(ga != ra)[0]
+        assert len(bad) == 0, f"{label} pass {k}: awake flags differ at {len(bad)} bodies, first {bad[:5]}"
+        woken_total += int(np.count_nonzero(dynamic & (ga != 0) & (awake == 0)))
+        moved = ga.copy()
+    pipe.close()
+    return woken_total
+
+
 def test_mixed_sleeping(oracle_mod):
     """Asleep bodies are neither synchronised nor collided (world.cpp:427-442,
-    contact_manager.cpp:262-268)."""
-    sc = S.mixed_scene(seed=9, n=1500, side=14.0).finalize()
+    contact_manager.cpp:253-259); contacts that start or stop touching, and
+    destroyed contacts with points, wake bodies for the contacts after them in
+    the list (contact.cpp:249-254, contact.cpp:108-126)."""
+    sc = S.mixed_scene(seed=9, n=1500, side=14.0, static_frac=0.1, sensor_frac=0.05).finalize()
+    woken = run_sleeping(oracle_mod, sc, 8, "sleep", seed=100, sleep_frac=0.3)
+    assert woken > 0
 
-    def awake(k, n):
-        rng = np.random.default_rng(100 + k)
-        return (rng.random(n) > 0.3).astype(np.uint8)
 
-    run_parity(oracle_mod, sc, 5, "sleep", awake_fn=awake)
+def test_mostly_sleeping(oracle_mod):
+    """Most bodies asleep: long wake-up chains through the list."""
+    sc = S.mixed_scene(seed=13, n=2500, side=15.0, static_frac=0.05, sensor_frac=0.03).finalize()
+    woken = run_sleeping(oracle_mod, sc, 8, "mostly-asleep", seed=7, sleep_frac=0.8)
+    assert woken > 0
