@@ -47,8 +47,20 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=60)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-stages", action="store_true", default=True)
-    return ap.parse_args()
+    ap.add_argument("--profile-steps", type=int, default=30,
+                    help="passes after the timed ones, with per-stage CUDA events (not part of value)")
+    ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "batched"])
+    ap.add_argument("--worlds", type=int, default=1024)
+    ap.add_argument("--autotune", action="store_true", default=True)
+    args = ap.parse_args()
+    if args.workload == "batched":
+        # 30 steps.
+        if "--steps" not in sys.argv:
+            args.steps = 30
+        if "--warmup" not in sys.argv:
+            args.warmup = 3
+    return args
 
 
 def dist_init(args):
@@ -221,30 +233,38 @@ def run_ours(args, rank, world, local, dist):
     dev = torch.device("cuda", local)
     scene = build_scene(args.bodies, SEED + rank)
     drv = S.KinematicDriver(scene, walls=scene_half(scene))
-    total = 1 + args.warmup + args.steps + args.e2e_steps
+    # states: creation + warm-up, 2 passes that capture the tuned graphs, timed, profiled
+    t0_k = 1 + args.warmup + 2
+    n_dev = t0_k + args.steps + args.profile_steps
+    total = n_dev + args.e2e_steps
     nb = scene.n_bodies
     states = np.empty((total, 17 * nb), np.float32)
     states[0] = drv.state17()
     for k in range(1, total):
         drv.advance()
         states[k] = drv.state17()
-    d_states = torch.from_numpy(states[: 1 + args.warmup + args.steps]).to(dev)
-    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local)
+    d_states = torch.from_numpy(states[:n_dev]).to(dev)
+    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local, graph=not args.no_graph)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     row = 17 * nb * 4
     base = d_states.data_ptr()
 
-    # creation pass + warm-up
+    # creation pass + warm-up (the first steady-state passes capture the graphs)
     with torch.cuda.stream(stream):
         for k in range(0, 1 + args.warmup):
             pipe.collide(base + k * row, on_device=True, stream=sptr)
     stream.synchronize()
     c = pipe.counts()
     assert c["status"] == 0, c
+    tuning = pipe.autotune(reps=5, stream=sptr).tolist() if args.autotune else pipe.tuning().tolist()
+    # Two passes (one per contact-buffer parity) capture the graphs with the
+    # tuned launch shapes before the timed region.
+    with torch.cuda.stream(stream):
+        for k in range(1 + args.warmup, t0_k):
+            pipe.collide(base + k * row, on_device=True, stream=sptr)
+    stream.synchronize()
     pipe.totals(reset=True)
-    if args.profile_stages:
-        pipe.set_profiling(True)
 
     sampler = ClockSampler(local)
     sampler.start()
@@ -255,7 +275,7 @@ def run_ours(args, rank, world, local, dist):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for k in range(1 + args.warmup, 1 + args.warmup + args.steps):
+    for k in range(t0_k, t0_k + args.steps):
         pipe.collide(base + k * row, on_device=True, stream=sptr)
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -264,10 +284,20 @@ def run_ours(args, rank, world, local, dist):
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     tot = pipe.totals()
-    prof = pipe.profile() if args.profile_stages else {}
-    pipe.set_profiling(False)
     c = pipe.counts()
     assert c["status"] == 0, c
+
+    # Stage times: further passes with CUDA events between the stages
+    # (launched kernel by kernel; not part of the timed value).
+    prof = {}
+    if args.profile_steps > 0:
+        pipe.set_profiling(True)
+        k0 = t0_k + args.steps
+        for k in range(k0, k0 + args.profile_steps):
+            pipe.collide(base + k * row, on_device=True, stream=sptr)
+        prof = pipe.profile()
+        pipe.set_profiling(False)
+        assert pipe.counts()["status"] == 0
 
     ms_max = ms
     manifolds_all = tot["manifolds"]
@@ -291,7 +321,7 @@ def run_ours(args, rank, world, local, dist):
 
     lib = pipe.lib
     e2e_m, e2e_h2d, e2e_d2h = 0, 0, 0
-    k0 = 1 + args.warmup + args.steps
+    k0 = n_dev
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k in range(k0, k0 + args.e2e_steps):
@@ -353,6 +383,8 @@ def run_ours(args, rank, world, local, dist):
             "e2e": {"value": e2e_value, "unit": "manifolds/s", "h2d_bytes_per_step": e2e_h2d // max(args.e2e_steps, 1),
                     "d2h_bytes_per_step": e2e_d2h // max(args.e2e_steps, 1), "steps": args.e2e_steps},
             "gpu_launches": tot["launches"],
+            "graph_passes": tot["graph_passes"],
+            "launch_shapes": tuning,
             "pairs_per_s": tot["contacts"] / (ms / 1000.0),
             "points_per_s": tot["points"] / (ms / 1000.0),
             "stage_ms": stage_ms,
@@ -364,12 +396,199 @@ def run_ours(args, rank, world, local, dist):
     pipe.close()
 
 
+# ---------------------------------------------------------------------------
+# Batched worlds (config 3): one context for all worlds against one context
+# per world, run world by world.
+
+BATCHED_WORKLOAD = ("1,024 independent worlds, body count per world log-uniform in [16, 4096], "
+                    "unit boxes (b3Hull half-extent 0.5 m) and spheres r = 0.5 m in equal numbers over a "
+                    "static ground box per world, positions in a cube scaled to keep the plain-scene density, "
+                    "kinematic motion")
+
+
+def batched_cpu_worker(job):
+    """One host process: the reference's pass on a share of the worlds
+    (creation pass + `passes` timed passes each) until `budget` seconds of
+    measured pass time are spent. Returns (manifolds, seconds, worlds, passes)."""
+    scenes, passes, budget = job
+    sys.path.insert(0, ROOT)
+    from bounce_b200 import scene as S
+    from oracle import oracle as O
+
+    m, t, nw, npass = 0, 0.0, 0, 0
+    for sub in scenes:
+        rw = O.RefWorld(sub)
+        sub.set_local_centers(rw.local_centers())
+        drv = S.KinematicDriver(sub)
+        rw.first_pass()
+        for _ in range(passes):
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            tt = rw.step_pass()
+            t += float(tt[0] + tt[1])
+            m += rw.touching()[1]
+            npass += 1
+        rw.close()
+        nw += 1
+        if t >= budget:
+            break
+    return m, t, nw, npass
+
+
+def batched_cpu_baseline(sc, n_worlds, seconds):
+    """The reference's CPU pass on all host cores, one process per core, each
+    on its own share of the worlds (a bounded sample: each process stops after
+    about `seconds` of pass time)."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    shares = [[] for _ in range(cores)]
+    for w in range(n_worlds):
+        shares[w % cores].append(sc.world_subset(w)[0])
+    jobs = [(sh, 5, seconds) for sh in shares if sh]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(len(jobs)) as pool:
+        res = pool.map(batched_cpu_worker, jobs)
+    wall = time.perf_counter() - t0
+    m = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    worlds = sum(r[2] for r in res)
+    passes = sum(r[3] for r in res)
+    return {"value": m / busy if busy > 0 else None, "unit": "manifolds/s", "cores": len(jobs), "kind": "reference",
+            "sample": f"{worlds} of the {n_worlds} worlds, 5 passes each after the creation pass, one reference "
+                      f"process per host core ({passes} passes in all; throughput = manifolds / the longest "
+                      f"process's pass time; wall {wall:.1f} s including process start)"}
+
+
+def run_batched(args, rank, world, local, dist):
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+    from bounce_b200 import scene as S
+
+    sc, counts = S.batched_scene(seed=3 + rank, n_worlds=args.worlds, lo=16, hi=4096, cube=20.0)
+    sc.finalize()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # Host processes first (spawned before this process touches the GPU).
+        try:
+            cpu = batched_cpu_baseline(sc, args.worlds, args.cpu_seconds)
+        except Exception as e:
+            cpu = {"value": None, "unit": "manifolds/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    drv = S.KinematicDriver(sc)
+    nb = sc.n_bodies
+    t0_k = 1 + args.warmup + 2
+    n_states = t0_k + args.steps
+    states = np.empty((n_states, 17 * nb), np.float32)
+    states[0] = drv.state17()
+    for k in range(1, n_states):
+        drv.advance()
+        states[k] = drv.state17()
+    d_states = torch.from_numpy(states).to(dev)
+    base = d_states.data_ptr()
+    row = 17 * nb * 4
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+
+    # Batched: one context, all worlds, graph replay, autotuned shapes.
+    pipe = CollisionPipeline(sc, device=local, graph=not args.no_graph)
+    for k in range(0, 1 + args.warmup):
+        pipe.collide(base + k * row, on_device=True, stream=sptr)
+    stream.synchronize()
+    assert pipe.counts()["status"] == 0
+    tuning = pipe.autotune(reps=5, stream=sptr).tolist() if args.autotune else pipe.tuning().tolist()
+    for k in range(1 + args.warmup, t0_k):
+        pipe.collide(base + k * row, on_device=True, stream=sptr)
+    stream.synchronize()
+    pipe.totals(reset=True)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(t0_k, t0_k + args.steps):
+        pipe.collide(base + k * row, on_device=True, stream=sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    tot = pipe.totals()
+    cb = pipe.counts()
+    assert cb["status"] == 0, cb
+    pipe.close()
+
+    # World by world: one context per world, the plain pass launched kernel by
+    # kernel for each world in turn, on the same states (a world's bodies are
+    # contiguous, so its state is a slice of the batched state).
+    # First body of each world (worlds were built one after the other).
+    starts = np.searchsorted(sc.body_world, np.arange(args.worlds))
+    pipes = [CollisionPipeline(sc.world_subset(w)[0], device=local) for w in range(args.worlds)]
+    for k in range(0, t0_k):
+        for w, p in enumerate(pipes):
+            p.collide(base + k * row + int(starts[w]) * 68, on_device=True, stream=sptr)
+    stream.synchronize()
+    for p in pipes:
+        p.totals(reset=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for k in range(t0_k, t0_k + args.steps):
+        for w, p in enumerate(pipes):
+            p.collide(base + k * row + int(starts[w]) * 68, on_device=True, stream=sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms_wbw = ev0.elapsed_time(ev1)
+    m_wbw = sum(p.totals()["manifolds"] for p in pipes)
+    c_wbw = sum(p.counts()["contacts"] for p in pipes)
+    for p in pipes:
+        p.close()
+
+    ms_max, m_all = ms, float(tot["manifolds"])
+    if dist is not None:
+        t = torch.tensor([ms, m_all], device=dev, dtype=torch.float64)
+        tmax, tsum = t.clone(), t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms_max, m_all = float(tmax[0]), float(tsum[1])
+    value = m_all / (ms_max / 1000.0)
+    v_wbw = m_wbw / (ms_wbw / 1000.0)
+    if rank == 0:
+        line = {
+            "metric": "manifolds/s", "value": value, "unit": "manifolds/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": BATCHED_WORKLOAD, "worlds": args.worlds, "bodies": int(nb),
+                       "proxies": int(sc.n_fixtures), "passes_timed": args.steps,
+                       "l2": "inputs larger than L2 (contact state of ~0.75 M bodies)",
+                       "parallelism": f"replicas x{world}", "graph": not args.no_graph},
+            "gpu_launches": tot["launches"], "graph_passes": tot["graph_passes"], "launch_shapes": tuning,
+            "world_by_world": {"value": v_wbw, "unit": "manifolds/s", "ms_per_step": ms_wbw / args.steps,
+                               "contacts_last_pass": c_wbw},
+            "speedup_vs_world_by_world": value / v_wbw if v_wbw > 0 else None,
+            "same_contact_count": c_wbw == cb["contacts"],
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_init(args)
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world, dist)
+        elif args.workload == "batched":
+            run_batched(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

@@ -22,6 +22,8 @@ SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_TRIANGLE, SHAPE_HULL, SHAPE_MESH = 0, 1, 2, 3
 BODY_STATIC, BODY_KINEMATIC, BODY_DYNAMIC = 0, 1, 2
 FLAG_WARM_STARTING = 1
 FLAG_CONVEX_CACHE = 2
+FLAG_GRAPH = 4
+TUNE_CONVEX, TUNE_PROBE, TUNE_SAT_WARPS, TUNE_SAT_BLOCKS, TUNE_TRAVERSE, TUNE_COUNT = 0, 7, 8, 9, 10, 11
 FIXTURE_SENSOR = 1
 
 
@@ -111,6 +113,9 @@ EXPORTED = [
     "b3g_stage_name",
     "b3g_collide_pairs",
     "b3g_find_pairs_static",
+    "b3g_autotune",
+    "b3g_set_tuning",
+    "b3g_get_tuning",
     "b3g_hull_from_points",
     "b3g_hull_box",
 ]
@@ -163,6 +168,9 @@ def load():
             ctypes.c_int,
         ),
         "b3g_find_pairs_static": ([vp, ctypes.c_uint32, vp, ctypes.c_uint32, vp, vp], ctypes.c_int),
+        "b3g_autotune": ([ctx, ctypes.c_uint32, vp, u32p], ctypes.c_int),
+        "b3g_set_tuning": ([ctx, u32p], ctypes.c_int),
+        "b3g_get_tuning": ([ctx, u32p], ctypes.c_int),
         "b3g_hull_from_points": ([f32p, ctypes.c_uint32, f32p, u32p, u32p, f32p, f32p, u32p], ctypes.c_int),
         "b3g_hull_box": (
             [ctypes.c_float, ctypes.c_float, ctypes.c_float, f32p, u32p, u32p, f32p, f32p, u32p],

@@ -59,6 +59,31 @@ void dfree(T*& p)
 	p = nullptr;
 }
 
+// Captured passes become invalid when the scene or a launch shape changes.
+void destroy_graphs(b3g_ctx* c)
+{
+	for (int i = 0; i < 2; ++i)
+		for (int j = 0; j < 2; ++j)
+		{
+			if (c->graphs[i][j].exec)
+				cudaGraphExecDestroy(c->graphs[i][j].exec);
+			if (c->graphs[i][j].graph)
+				cudaGraphDestroy(c->graphs[i][j].graph);
+			c->graphs[i][j] = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+		}
+}
+
+// Launch shapes before any tuning.
+void default_tuning(Tune& t)
+{
+	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
+		t.v[B3G_TUNE_CONVEX + k] = 4;
+	t.v[B3G_TUNE_PROBE] = 4;
+	t.v[B3G_TUNE_SAT_WARPS] = 4;
+	t.v[B3G_TUNE_SAT_BLOCKS] = 2;
+	t.v[B3G_TUNE_TRAVERSE] = 128;
+}
+
 uint32_t pow2_at_least(uint32_t v)
 {
 	uint32_t p = 1;
@@ -203,10 +228,12 @@ extern "C" int b3g_get_totals(b3g_ctx* c, uint64_t* out, int reset)
 	for (int k = 0; k < 6; ++k)
 		out[k] = t[k];
 	out[6] = c->launches;
+	out[7] = c->graphLaunches;
 	if (reset)
 	{
 		CK(cudaMemset(c->buf.totals, 0, sizeof(t)));
 		c->launches = 0;
+		c->graphLaunches = 0;
 	}
 	return B3G_OK;
 }
@@ -242,6 +269,12 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dBodyState = nullptr;
 	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = c->dFixRank = nullptr;
 	c->asleep = 0;
+	c->graphLaunches = 0;
+	c->lastPassImpulses = false;
+	for (int i = 0; i < 2; ++i)
+		for (int j = 0; j < 2; ++j)
+			c->graphs[i][j] = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+	default_tuning(c->tune);
 	c->dFixParams = nullptr;
 	c->dFixBound = nullptr;
 	c->hCounters = nullptr;
@@ -355,6 +388,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	cudaSetDevice(c->device);
 	if (c->stream)
 		cudaStreamSynchronize(c->stream);
+	destroy_graphs(c);
 	Buffers& B = c->buf;
 	dfree(B.fatLo);
 	dfree(B.fatHi);
@@ -459,6 +493,8 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 	if (!c || (nh && (!desc || !verts || !edges || !faces || !planes || !centroids)))
 		return fail(c, B3G_E_INVALID, "b3g_set_hulls: null argument");
 	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	destroy_graphs(c);
 	uint32_t nv = 0, ne = 0, nf = 0, maxUE = 0;
 	std::vector<HullDesc> hd(nh);
 	for (uint32_t h = 0; h < nh; ++h)
@@ -547,6 +583,8 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 	if (!c || (nb && (!world || !type || !awake)))
 		return fail(c, B3G_E_INVALID, "b3g_set_bodies: null argument");
 	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	destroy_graphs(c);
 	uint32_t nw = 1;
 	for (uint32_t i = 0; i < nb; ++i)
 	{
@@ -597,6 +635,8 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	if (nf > c->cfg.max_proxies)
 		return fail(c, B3G_E_CAPACITY, "%u fixtures exceed max_proxies %u", nf, c->cfg.max_proxies);
 	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	destroy_graphs(c);
 	std::vector<uint32_t> key(nf);
 	for (uint32_t i = 0; i < nf; ++i)
 	{
@@ -748,6 +788,32 @@ extern "C" int b3g_fetch_awake(b3g_ctx* c, uint8_t* out, uint32_t capacity)
 	return (int)c->nBodies;
 }
 
+// Kernels of one pass up to the narrowphase, on s (profiling marks when on).
+// While s is being captured, *copyNode receives the state copy's graph node.
+static void issue_pass(b3g_ctx* c, cudaStream_t s, const float* state, size_t bytes, cudaMemcpyKind kind,
+	cudaGraphNode_t* copyNode = nullptr)
+{
+	prof_mark(c, PM_BEGIN, s);
+	cudaMemcpyAsync(c->dBodyState, state, bytes, kind, s);
+	if (copyNode)
+	{
+		cudaStreamCaptureStatus st;
+		const cudaGraphNode_t* deps = nullptr;
+		size_t nd = 0;
+		*copyNode = nullptr;
+		if (cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &deps, &nd) == cudaSuccess && nd == 1)
+			*copyNode = deps[0];
+	}
+	k_pass_begin<<<1, CTR_COUNT, 0, s>>>(c->buf.counters, c->havePass ? 1 : 0, c->cfg.max_contacts);
+	prof_mark(c, PM_UPLOADED, s);
+	launch_sync(c, s);
+	prof_mark(c, PM_SYNCED, s);
+	launch_broadphase(c, s);
+	launch_pairs_diff(c, s);
+	prof_mark(c, PM_DIFFED, s);
+	launch_narrowphase(c, s);
+}
+
 extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* stream)
 {
 	if (!c || !state)
@@ -757,39 +823,79 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	CK(cudaSetDevice(c->device));
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
-	if (c->profiling)
-	{
-		int rc = prof_begin_pass(c);
-		if (rc)
-			return rc;
-	}
-	prof_mark(c, PM_BEGIN, s);
-	if (onDevice)
-		CK(cudaMemcpyAsync(c->dBodyState, state, bytes, cudaMemcpyDeviceToDevice, s));
-	else
-		CK(cudaMemcpyAsync(c->dBodyState, state, bytes, cudaMemcpyHostToDevice, s));
-	if (c->havePass)
-		c->cur ^= 1u;
-	k_pass_begin<<<1, CTR_COUNT, 0, s>>>(c->buf.counters, c->havePass ? 1 : 0, c->cfg.max_contacts);
-	prof_mark(c, PM_UPLOADED, s);
-	launch_sync(c, s);
-	prof_mark(c, PM_SYNCED, s);
-	launch_broadphase(c, s);
-	launch_pairs_diff(c, s);
-	prof_mark(c, PM_DIFFED, s);
-	launch_narrowphase(c, s);
-	if (c->asleep > 0)
-	{
-		int rc = resolve_wakeups(c, s);
-		if (rc)
-			return fail(c, rc, "b3g_collide: wake-up rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
-	}
-	launch_finalize(c, s);
-	prof_mark(c, PM_FINAL, s);
-	if (c->profiling)
-		++c->profPass;
+	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
 	// pass_begin, sync, broadphase, diff + list order, bucket + 7 convex + 2 hull, finalize + pass_end
-	c->launches += 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 2;
+	const uint32_t passLaunches = 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 2;
+	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
+		c->havePass && !c->creationPass && s != nullptr;
+	c->lastPassImpulses = c->impulsesLoaded;
+	if (graph)
+	{
+		c->cur ^= 1u;
+		PassGraph& g = c->graphs[c->cur][c->impulsesLoaded ? 1 : 0];
+		if (g.exec && g.stream == s && g.state != state)
+		{
+			// Same pass, state at another address: re-point the copy node.
+			if (g.copyNode && cudaGraphExecMemcpyNodeSetParams1D(g.exec, g.copyNode, c->dBodyState, state, bytes,
+								   kind) == cudaSuccess)
+				g.state = state;
+			else
+				cudaGetLastError();
+		}
+		if (!g.exec || g.state != state || g.stream != s)
+		{
+			if (g.exec)
+				cudaGraphExecDestroy(g.exec);
+			if (g.graph)
+				cudaGraphDestroy(g.graph);
+			g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+			// The captured kernels use the contact buffers of this parity and
+			// the host-side pass state every later pass of this parity has.
+			CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+			issue_pass(c, s, state, bytes, kind, &g.copyNode);
+			launch_finalize(c, s);
+			cudaError_t e = cudaStreamEndCapture(s, &g.graph);
+			if (e != cudaSuccess)
+			{
+				g.graph = nullptr;
+				return fail(c, B3G_E_CUDA, "b3g_collide: pass capture failed: %s", cudaGetErrorString(e));
+			}
+			e = cudaGraphInstantiate(&g.exec, g.graph, 0);
+			if (e != cudaSuccess)
+			{
+				cudaGraphDestroy(g.graph);
+				g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+				return fail(c, B3G_E_CUDA, "b3g_collide: graph instantiation failed: %s", cudaGetErrorString(e));
+			}
+			g.state = state;
+			g.stream = s;
+		}
+		CK(cudaGraphLaunch(g.exec, s));
+		++c->graphLaunches;
+	}
+	else
+	{
+		if (c->profiling)
+		{
+			int rc = prof_begin_pass(c);
+			if (rc)
+				return rc;
+		}
+		if (c->havePass)
+			c->cur ^= 1u;
+		issue_pass(c, s, state, bytes, kind);
+		if (c->asleep > 0)
+		{
+			int rc = resolve_wakeups(c, s);
+			if (rc)
+				return fail(c, rc, "b3g_collide: wake-up rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
+		}
+		launch_finalize(c, s);
+		prof_mark(c, PM_FINAL, s);
+		if (c->profiling)
+			++c->profPass;
+	}
+	c->launches += passLaunches;
 	CK(cudaGetLastError());
 	c->creationPass = false;
 	c->havePass = true;
@@ -1116,7 +1222,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 					continue;
 				if (b == BK_HULLS)
 				{
-					launch_hulls(a, dList + offs[b], dCount + b, c->maxUniqueEdges, c->stream);
+					launch_hulls(a, dList + offs[b], dCount + b, c->maxUniqueEdges, c->tune, c->stream);
 				}
 				else
 				{
@@ -1127,7 +1233,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 					uint32_t* dOne = nullptr;
 					step(dalloc(&dOne, BK_COUNT));
 					step(cudaMemcpy(dOne, one.data(), 4 * BK_COUNT, cudaMemcpyHostToDevice));
-					launch_convex_buckets(a, dList + offs[b] - (size_t)b * n, dOne, n, c->stream);
+					launch_convex_buckets(a, dList + offs[b] - (size_t)b * n, dOne, n, c->tune, c->stream);
 					step(cudaStreamSynchronize(c->stream));
 					dfree(dOne);
 				}
@@ -1171,4 +1277,168 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	dfree(dMiss);
 	dfree(dMissCount);
 	return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Launch shapes and the autotuner.
+
+size_t hull_sat_smem(int warps, uint32_t maxUE);
+
+namespace {
+
+const uint32_t kBlocksPerSM[] = {1, 2, 4, 8, 16};
+const uint32_t kSatWarps[] = {2, 4, 8};
+const uint32_t kSatBlocks[] = {1, 2, 4, 8};
+const uint32_t kTraverse[] = {64, 128, 256};
+
+template <size_t N>
+bool one_of(const uint32_t (&set)[N], uint32_t v)
+{
+	for (size_t i = 0; i < N; ++i)
+		if (set[i] == v)
+			return true;
+	return false;
+}
+
+bool sat_fits(const b3g_ctx* c, uint32_t warps)
+{
+	int optin = 0;
+	cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+	return hull_sat_smem((int)warps, c->maxUniqueEdges) <= (size_t)optin;
+}
+
+} // namespace
+
+extern "C" int b3g_set_tuning(b3g_ctx* c, const uint32_t* t)
+{
+	if (!c || !t)
+		return fail(c, B3G_E_INVALID, "b3g_set_tuning: null argument");
+	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
+		if (!one_of(kBlocksPerSM, t[B3G_TUNE_CONVEX + k]))
+			return fail(c, B3G_E_INVALID, "tuning[%d] = %u: not a candidate", B3G_TUNE_CONVEX + k, t[k]);
+	if (!one_of(kBlocksPerSM, t[B3G_TUNE_PROBE]) || !one_of(kSatWarps, t[B3G_TUNE_SAT_WARPS]) ||
+		!one_of(kSatBlocks, t[B3G_TUNE_SAT_BLOCKS]) || !one_of(kTraverse, t[B3G_TUNE_TRAVERSE]))
+		return fail(c, B3G_E_INVALID, "b3g_set_tuning: value outside the candidate sets");
+	CK(cudaSetDevice(c->device));
+	if (!sat_fits(c, t[B3G_TUNE_SAT_WARPS]))
+		return fail(c, B3G_E_INVALID, "b3g_set_tuning: %u SAT warps need more shared memory than a block has",
+			t[B3G_TUNE_SAT_WARPS]);
+	CK(cudaDeviceSynchronize());
+	destroy_graphs(c);
+	for (int k = 0; k < B3G_TUNE_COUNT; ++k)
+		c->tune.v[k] = t[k];
+	return B3G_OK;
+}
+
+extern "C" int b3g_get_tuning(b3g_ctx* c, uint32_t* t)
+{
+	if (!c || !t)
+		return fail(c, B3G_E_INVALID, "b3g_get_tuning: null argument");
+	for (int k = 0; k < B3G_TUNE_COUNT; ++k)
+		t[k] = c->tune.v[k];
+	return B3G_OK;
+}
+
+// Coordinate search over the launch shapes, each kernel timed alone on the
+// last pass's data. A candidate replaces the current shape only when it is at
+// least 3 % faster, so timing noise does not flip between equal shapes.
+extern "C" int b3g_autotune(b3g_ctx* c, uint32_t reps, void* stream, uint32_t* out)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "b3g_autotune: needs a pass first");
+	if (reps == 0)
+		reps = 10;
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	CK(cudaDeviceSynchronize());
+	uint32_t h[CTR_COUNT];
+	CK(cudaMemcpy(h, c->buf.counters, sizeof(h), cudaMemcpyDeviceToHost));
+	Buffers& B = c->buf;
+	const uint32_t cap = c->cfg.max_contacts;
+	// The narrowphase re-runs see exactly what the pass saw.
+	const bool loaded = c->impulsesLoaded;
+	c->impulsesLoaded = c->lastPassImpulses;
+	NPArgs a = make_np_args(c);
+	c->impulsesLoaded = loaded;
+	cudaEvent_t e0, e1;
+	CK(cudaEventCreate(&e0));
+	CK(cudaEventCreate(&e1));
+	int rc = B3G_OK;
+	auto timeit = [&](auto&& body) -> float {
+		body(); // warm-up
+		cudaEventRecord(e0, s);
+		for (uint32_t r = 0; r < reps; ++r)
+			body();
+		cudaEventRecord(e1, s);
+		float ms = 0.0f;
+		if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+			rc = B3G_E_CUDA;
+		return ms;
+	};
+	auto pick = [&](uint32_t& slot, const uint32_t* cands, size_t nc, auto&& run) {
+		float best = timeit(run);
+		uint32_t bestV = slot;
+		const uint32_t start = slot;
+		for (size_t i = 0; i < nc && rc == B3G_OK; ++i)
+		{
+			if (cands[i] == start)
+				continue;
+			slot = cands[i];
+			float ms = timeit(run);
+			if (ms < 0.97f * best)
+			{
+				best = ms;
+				bestV = cands[i];
+			}
+		}
+		slot = bestV;
+	};
+	static const uint32_t convexBucket[B3G_CONVEX_KERNELS] = {BK_SPHERES, BK_CAPSULE_SPHERE, BK_CAPSULES,
+		BK_HULL_SPHERE, BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
+	for (int k = 0; k < B3G_CONVEX_KERNELS && rc == B3G_OK; ++k)
+	{
+		if (h[CTR_BUCKET0 + convexBucket[k]] == 0)
+			continue;
+		pick(c->tune.v[B3G_TUNE_CONVEX + k], kBlocksPerSM, 5,
+			[&] { launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s); });
+	}
+	const uint32_t* hullList = B.bucketList + (size_t)BK_HULLS * cap;
+	const uint32_t* hullCount = B.counters + CTR_BUCKET0 + BK_HULLS;
+	auto probe = [&] {
+		cudaMemsetAsync(B.counters + CTR_HULL_MISS, 0, sizeof(uint32_t), s);
+		launch_hulls_probe(a, hullList, hullCount, c->tune, s);
+	};
+	if (h[CTR_BUCKET0 + BK_HULLS] && rc == B3G_OK)
+	{
+		pick(c->tune.v[B3G_TUNE_PROBE], kBlocksPerSM, 5, probe);
+		// The SAT kernel rewrites the caches the probe reads back: each run
+		// is probe + SAT, so every run starts from the pass's inputs.
+		uint32_t warps[3];
+		size_t nw = 0;
+		for (uint32_t w : kSatWarps)
+			if (sat_fits(c, w))
+				warps[nw++] = w;
+		auto probeSat = [&] {
+			probe();
+			launch_hulls_sat(a, c->maxUniqueEdges, c->tune, s);
+		};
+		pick(c->tune.v[B3G_TUNE_SAT_WARPS], warps, nw, probeSat);
+		pick(c->tune.v[B3G_TUNE_SAT_BLOCKS], kSatBlocks, 4, probeSat);
+		probeSat();
+	}
+	if (rc == B3G_OK)
+		pick(c->tune.v[B3G_TUNE_TRAVERSE], kTraverse, 3, [&] { launch_traverse(c, s); });
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	CK(cudaStreamSynchronize(s));
+	CK(cudaGetLastError());
+	if (rc != B3G_OK)
+		return fail(c, rc, "b3g_autotune: timing failed");
+	destroy_graphs(c);
+	if (out)
+		for (int k = 0; k < B3G_TUNE_COUNT; ++k)
+			out[k] = c->tune.v[k];
+	return B3G_OK;
 }

@@ -198,6 +198,25 @@ enum
 	CTR_COUNT = 32
 };
 
+// Launch shapes of the tunable kernels (include/b3g.h, B3G_TUNE_*).
+#define B3G_CONVEX_KERNELS 7
+struct Tune
+{
+	uint32_t v[B3G_TUNE_COUNT];
+};
+
+// A captured steady-state pass (one per contact-buffer parity and warm-start
+// source), valid for the stream it was captured on; the state copy node is
+// re-pointed when a pass brings its state from another address.
+struct PassGraph
+{
+	cudaGraph_t graph;
+	cudaGraphExec_t exec;
+	cudaGraphNode_t copyNode;
+	const float* state;
+	cudaStream_t stream;
+};
+
 struct b3g_ctx
 {
 	b3g_config cfg;
@@ -247,6 +266,12 @@ struct b3g_ctx
 	// kernels launched by passes (host count)
 	uint64_t launches;
 
+	// launch shapes and captured passes
+	Tune tune;
+	PassGraph graphs[2][2]; // [contact buffer][warm start from host impulses]
+	uint64_t graphLaunches;
+	bool lastPassImpulses;  // the last pass warm-started from host impulses
+
 	// stage profiling: a ring of per-pass event sets
 	bool profiling;
 	uint64_t profPass;     // passes recorded since enabling
@@ -281,6 +306,7 @@ uint32_t broadphase_launches(const b3g_ctx* c);
 // Launchers (defined in the .cu files).
 void launch_sync(b3g_ctx* c, cudaStream_t s);
 void launch_broadphase(b3g_ctx* c, cudaStream_t s);
+void launch_traverse(b3g_ctx* c, cudaStream_t s);
 void launch_pairs_diff(b3g_ctx* c, cudaStream_t s);
 void launch_narrowphase(b3g_ctx* c, cudaStream_t s);
 void launch_finalize(b3g_ctx* c, cudaStream_t s);

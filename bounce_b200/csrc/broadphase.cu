@@ -808,14 +808,28 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
 	prof_mark(c, PM_BUILT, s);
 
+	launch_traverse(c, s);
+	prof_mark(c, PM_TRAVERSED, s);
+}
+
+// LBVH traversal (count, offsets, emit) of the tree built by this pass; the
+// count kernel runs with the tuned block size. Re-running it on the same tree
+// writes the same pairs.
+void launch_traverse(b3g_ctx* c, cudaStream_t s)
+{
+	Buffers& B = c->buf;
+	int n = (int)c->nFixtures;
+	uint32_t cur = c->cur;
+	if (n == 0)
+		return;
+	const int tb = (int)c->tune.v[B3G_TUNE_TRAVERSE];
 	if (c->nWorlds > 1)
-		k_traverse_count<true><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
-		k_traverse_count<false><<<(n + 127) / 128, 128, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, s);
 	if (c->nWorlds > 1)
 		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
 		k_traverse_emit<false><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
-	prof_mark(c, PM_TRAVERSED, s);
 }

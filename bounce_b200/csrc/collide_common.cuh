@@ -617,8 +617,14 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t ta, uint32_t tb)
 // Narrowphase arguments of the current pass (contact arrays of c->cur).
 NPArgs make_np_args(b3g_ctx* c);
 void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	const Tune& tune, cudaStream_t s);
+void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	const Tune& tune, cudaStream_t s);
+void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, const Tune& tune,
 	cudaStream_t s);
-void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s);
+void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t* count, const Tune& tune,
+	cudaStream_t s);
+void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s);
 void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
 
 __device__ __forceinline__ XF load_xf7(const float* s)

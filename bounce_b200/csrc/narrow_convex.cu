@@ -539,21 +539,46 @@ __global__ void k_inactive(NPArgs a)
 
 } // namespace
 
-void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
-	cudaStream_t s)
+// Bucket kernel k of launch_convex_buckets (the order of B3G_TUNE_CONVEX).
+void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	const Tune& tune, cudaStream_t s)
 {
-	const int blocks = persistent_blocks(4);
+	static const uint32_t buckets[B3G_CONVEX_KERNELS] = {BK_SPHERES, BK_CAPSULE_SPHERE, BK_CAPSULES, BK_HULL_SPHERE,
+		BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
+	const uint32_t bk = buckets[k];
 	NPArgs a = base;
-#define B3G_LAUNCH(BK, KERNEL)                     \
-	a.list = lists + (size_t)(BK)*cap;             \
-	a.listCount = counts + (BK);                   \
-	KERNEL<<<blocks, 128, 0, s>>>(a);
-	B3G_LAUNCH(BK_SPHERES, k_convex<BK_SPHERES>);
-	B3G_LAUNCH(BK_CAPSULE_SPHERE, k_convex<BK_CAPSULE_SPHERE>);
-	B3G_LAUNCH(BK_CAPSULES, k_convex<BK_CAPSULES>);
-	B3G_LAUNCH(BK_HULL_SPHERE, k_convex<BK_HULL_SPHERE>);
-	B3G_LAUNCH(BK_HULL_CAPSULE, k_convex<BK_HULL_CAPSULE>);
-	B3G_LAUNCH(BK_SENSOR, k_sensor);
-	B3G_LAUNCH(BK_INACTIVE, k_inactive);
-#undef B3G_LAUNCH
+	a.list = lists + (size_t)bk * cap;
+	a.listCount = counts + bk;
+	const int blocks = persistent_blocks((int)tune.v[B3G_TUNE_CONVEX + k]);
+	switch (k)
+	{
+	case 0:
+		k_convex<BK_SPHERES><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 1:
+		k_convex<BK_CAPSULE_SPHERE><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 2:
+		k_convex<BK_CAPSULES><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 3:
+		k_convex<BK_HULL_SPHERE><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 4:
+		k_convex<BK_HULL_CAPSULE><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 5:
+		k_sensor<<<blocks, 128, 0, s>>>(a);
+		break;
+	default:
+		k_inactive<<<blocks, 128, 0, s>>>(a);
+		break;
+	}
+}
+
+void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
+	const Tune& tune, cudaStream_t s)
+{
+	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
+		launch_convex_one(k, base, lists, counts, cap, tune, s);
 }

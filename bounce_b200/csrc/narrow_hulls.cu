@@ -17,7 +17,6 @@
 
 namespace {
 
-constexpr int HW_WARPS = 4; // warps per block
 
 struct EdgeRec
 {
@@ -651,15 +650,16 @@ __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 	}
 }
 
-// Pass 2: one warp per contact the cache did not resolve.
-__global__ void __launch_bounds__(HW_WARPS * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
+// Pass 2: one warp per contact the cache did not resolve (W warps per block).
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
 	uint32_t n = *a.missCount;
-	uint32_t gw = blockIdx.x * HW_WARPS + warp;
-	uint32_t nw = gridDim.x * HW_WARPS;
+	uint32_t gw = blockIdx.x * W + warp;
+	uint32_t nw = gridDim.x * W;
 	for (uint32_t t = gw; t < n; t += nw)
 	{
 		uint32_t c = a.missList[t];
@@ -685,18 +685,59 @@ __global__ void __launch_bounds__(HW_WARPS * 32) k_hulls_sat(NPArgs a, uint32_t 
 
 } // namespace
 
-void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, cudaStream_t s)
+void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s);
+
+template <int W>
+void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
+{
+	size_t smem = (size_t)W * 2 * maxUE * sizeof(EdgeRec);
+	static size_t configured = 0;
+	if (smem > 48 * 1024 && smem > configured)
+	{
+		cudaFuncSetAttribute(k_hulls_sat<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		configured = smem;
+	}
+	k_hulls_sat<W><<<persistent_blocks(blocksPerSM), W * 32, smem, s>>>(a, maxUE);
+}
+
+void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, const Tune& tune,
+	cudaStream_t s)
 {
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	k_hulls_probe<<<persistent_blocks(4), 128, 0, s>>>(a);
-	size_t smem = (size_t)HW_WARPS * 2 * maxUE * sizeof(EdgeRec);
-	static size_t configured = 0;
-	if (smem > 48 * 1024 && smem > configured)
+	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
+	launch_hulls_sat(a, maxUE, tune, s);
+}
+
+void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s)
+{
+	const int bps = (int)tune.v[B3G_TUNE_SAT_BLOCKS];
+	switch (tune.v[B3G_TUNE_SAT_WARPS])
 	{
-		cudaFuncSetAttribute(k_hulls_sat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		configured = smem;
+	case 2:
+		launch_sat<2>(a, maxUE, bps, s);
+		break;
+	case 8:
+		launch_sat<8>(a, maxUE, bps, s);
+		break;
+	default:
+		launch_sat<4>(a, maxUE, bps, s);
+		break;
 	}
-	k_hulls_sat<<<persistent_blocks(2), HW_WARPS * 32, smem, s>>>(a, maxUE);
+}
+
+void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t* count, const Tune& tune,
+	cudaStream_t s)
+{
+	NPArgs a = base;
+	a.list = list;
+	a.listCount = count;
+	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
+}
+
+// Dynamic shared memory of the SAT kernel with `warps` warps per block.
+size_t hull_sat_smem(int warps, uint32_t maxUE)
+{
+	return (size_t)warps * 2 * maxUE * sizeof(EdgeRec);
 }

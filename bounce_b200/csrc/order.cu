@@ -486,9 +486,9 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 				break;
 			if (act)
 			{
-				launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, s);
+				launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 				launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
-					c->maxUniqueEdges, s);
+					c->maxUniqueEdges, c->tune, s);
 				k_wake_events<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, cap, B.wakeList,
 					B.counters + CTR_WAKE_ACTIVATED, 0);
 				launches += 7 + 2 + 1;

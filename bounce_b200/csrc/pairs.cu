@@ -205,10 +205,10 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	uint32_t cap = c->cfg.max_contacts;
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
 	NPArgs a = make_np_args(c);
-	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, s);
+	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
-		c->maxUniqueEdges, s);
+		c->maxUniqueEdges, c->tune, s);
 	prof_mark(c, PM_HULLS, s);
 }
 

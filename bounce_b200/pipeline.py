@@ -17,7 +17,7 @@ u32, f32 = ctypes.c_uint32, ctypes.c_float
 
 
 class CollisionPipeline:
-    def __init__(self, scene, max_contacts=None, warm_starting=True, convex_cache=True, device=0):
+    def __init__(self, scene, max_contacts=None, warm_starting=True, convex_cache=True, device=0, graph=False):
         self.lib = N.load()
         self.scene = scene
         nf = scene.n_fixtures
@@ -28,7 +28,8 @@ class CollisionPipeline:
             max_proxies=max(nf, 1),
             max_contacts=int(max_contacts),
             max_hull_data=0,
-            flags=(N.FLAG_WARM_STARTING if warm_starting else 0) | (N.FLAG_CONVEX_CACHE if convex_cache else 0),
+            flags=(N.FLAG_WARM_STARTING if warm_starting else 0) | (N.FLAG_CONVEX_CACHE if convex_cache else 0)
+            | (N.FLAG_GRAPH if graph else 0),
             device=device,
         )
         h = ctypes.c_void_p()
@@ -150,10 +151,28 @@ class CollisionPipeline:
 
     def totals(self, reset=False):
         """Cumulative device counters: passes, contacts, manifolds, points, begun, ended."""
-        out = np.zeros(7, np.uint64)
+        out = np.zeros(8, np.uint64)
         self._check(self.lib.b3g_get_totals(self.ctx, N.ptr(out, ctypes.c_uint64), 1 if reset else 0))
-        names = ("passes", "contacts", "manifolds", "points", "begun", "ended", "launches")
+        names = ("passes", "contacts", "manifolds", "points", "begun", "ended", "launches", "graph_passes")
         return dict(zip(names, (int(x) for x in out)))
+
+    def autotune(self, reps=10, stream=None):
+        """Times the tunable kernels on the last pass's data and keeps the
+        fastest launch shapes; returns the tuning table."""
+        out = np.zeros(N.TUNE_COUNT, np.uint32)
+        s = ctypes.c_void_p(int(stream)) if stream else None
+        self._check(self.lib.b3g_autotune(self.ctx, int(reps), s, N.ptr(out, u32)))
+        return out
+
+    def tuning(self):
+        out = np.zeros(N.TUNE_COUNT, np.uint32)
+        self._check(self.lib.b3g_get_tuning(self.ctx, N.ptr(out, u32)))
+        return out
+
+    def set_tuning(self, table):
+        t = np.ascontiguousarray(table, np.uint32)
+        assert t.size == N.TUNE_COUNT
+        self._check(self.lib.b3g_set_tuning(self.ctx, N.ptr(t, u32)))
 
     def set_profiling(self, on=True):
         self._check(self.lib.b3g_set_profiling(self.ctx, 1 if on else 0))

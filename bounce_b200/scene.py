@@ -237,6 +237,31 @@ class Scene:
     def set_local_centers(self, lc):
         self.local_center = np.ascontiguousarray(lc, F).reshape(-1, 3)
 
+    def world_subset(self, w):
+        """The bodies and fixtures of world w as a one-world scene (world 0,
+        same hull arrays), with the indices they had here: returns
+        (scene, body indices, fixture indices)."""
+        bodies = np.nonzero(self.body_world == w)[0]
+        fixtures = np.nonzero(self.body_world[self.fix_body] == w)[0]
+        remap = np.full(self.n_bodies, -1, np.int64)
+        remap[bodies] = np.arange(len(bodies))
+        s = Scene()
+        s.hull_arrays = self.hull_arrays
+        s.body_world = np.zeros(len(bodies), np.uint32)
+        s.body_type = np.ascontiguousarray(self.body_type[bodies])
+        s.body_pos = np.ascontiguousarray(self.body_pos[bodies])
+        s.body_quat = np.ascontiguousarray(self.body_quat[bodies])
+        s.body_lin = np.ascontiguousarray(self.body_lin[bodies])
+        s.body_ang = np.ascontiguousarray(self.body_ang[bodies])
+        s.body_pose = np.ascontiguousarray(self.body_pose[bodies])
+        s.fix_body = np.ascontiguousarray(remap[self.fix_body[fixtures]].astype(np.uint32))
+        s.fix_type = np.ascontiguousarray(self.fix_type[fixtures])
+        s.fix_hull = np.ascontiguousarray(self.fix_hull[fixtures])
+        s.fix_params = np.ascontiguousarray(self.fix_params.reshape(-1, 12)[fixtures].reshape(-1))
+        s.fix_flags = np.ascontiguousarray(self.fix_flags[fixtures])
+        s.local_center = np.ascontiguousarray(self.local_center[bodies])
+        return s, bodies, fixtures
+
 
 def plain_scene(seed=1, n_boxes=1000, n_spheres=1000, cube=20.0, world=0, scene=None, box_hull=None):
     """Boxes and spheres above a static ground box."""

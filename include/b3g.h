@@ -61,6 +61,8 @@ extern "C" {
 /* Context flags. */
 #define B3G_FLAG_WARM_STARTING 1u /* b3World::SetWarmStarting (world.h:95) */
 #define B3G_FLAG_CONVEX_CACHE 2u  /* b3_convexCache (collide_hulls.cpp:27, forced on by b3World()) */
+/* Replay each steady-state pass from a captured CUDA graph (see b3g_collide). */
+#define B3G_FLAG_GRAPH 4u
 
 /* Fixture flags. */
 #define B3G_FIXTURE_SENSOR 1u     /* b3FixtureDef::isSensor (fixture.h:60) */
@@ -148,7 +150,14 @@ int b3g_set_awake(b3g_ctx* ctx, const uint8_t* awake);
  * + b3BroadPhase::MoveProxy (body.cpp:216-238, fixture.cpp:120-132,
  * dynamic_tree.cpp:139-207), b3ContactManager::FindNewContacts
  * (contact_manager.cpp:213-223), b3ContactManager::UpdateContacts
- * (contact_manager.cpp:225-287). The call is asynchronous. */
+ * (contact_manager.cpp:225-287). The call is asynchronous.
+ * With B3G_FLAG_GRAPH, a pass whose state is on the device, that follows an
+ * earlier pass of the same scene, with profiling off and no body asleep, is
+ * captured once into a CUDA graph per contact-buffer parity (and state
+ * pointer, stream and warm-start source) and replayed afterwards: one graph
+ * launch per pass, same kernels, same results. Other passes launch their
+ * kernels one by one. stream must not be the legacy NULL stream for capture;
+ * NULL selects the context's own stream. */
 int b3g_collide(b3g_ctx* ctx, const float* body_state, int state_on_device, void* stream);
 
 /* Waits for the last pass and returns its counters. */
@@ -208,7 +217,8 @@ int b3g_load_impulses(b3g_ctx* ctx, const float* normal_impulse, const float* ta
 /* Cumulative counters since creation or the last reset: out[0] passes,
  * out[1] contacts, out[2] manifolds with points, out[3] manifold points,
  * out[4] contacts created, out[5] contacts destroyed, out[6] CUDA kernels the
- * passes launched (counted on the host; 7 entries). Kept on the device and
+ * passes launched (counted on the host, graph replays included), out[7]
+ * passes replayed from a captured graph (8 entries). Kept on the device and
  * summed without host synchronisation inside the passes. Replaces the
  * reference's per-step statistics (b3_convexCalls etc., world.cpp:191-199). */
 int b3g_get_totals(b3g_ctx* ctx, uint64_t* out, int reset);
@@ -221,6 +231,36 @@ int b3g_get_totals(b3g_ctx* ctx, uint64_t* out, int reset);
 int b3g_set_profiling(b3g_ctx* ctx, int enable);
 int b3g_get_profile(b3g_ctx* ctx, double* ms, uint32_t* passes, uint32_t capacity);
 const char* b3g_stage_name(uint32_t stage);
+
+/* Launch shapes ------------------------------------------------------------
+ *
+ * No counterpart in the reference (its loops are sequential). The bucket,
+ * hull and traversal kernels are grid-stride loops whose results do not
+ * depend on their launch shape; the shape only changes their speed. The
+ * tuning table holds B3G_TUNE_COUNT entries:
+ *   [B3G_TUNE_CONVEX + k]  blocks per SM of the thread-per-pair kernel of
+ *                          bucket k: spheres, capsule-sphere, capsules,
+ *                          hull-sphere, hull-capsule, sensor, inactive
+ *                          (128 threads per block)
+ *   [B3G_TUNE_PROBE]       blocks per SM of the hull feature-cache probe
+ *   [B3G_TUNE_SAT_WARPS]   warps per block of the hull-hull SAT kernel (2, 4, 8)
+ *   [B3G_TUNE_SAT_BLOCKS]  blocks per SM of the hull-hull SAT kernel
+ *   [B3G_TUNE_TRAVERSE]    threads per block of the LBVH traversal (64, 128, 256)
+ * b3g_autotune picks each entry by timing the kernel it drives on the last
+ * pass's data (the kernels re-run on the same inputs write the same outputs,
+ * so the pass's results are unchanged), reps launches per candidate; it
+ * needs a pass first and writes the chosen table to out (may be NULL).
+ * b3g_set_tuning / b3g_get_tuning set and read the table directly;
+ * set_tuning rejects values outside the candidate sets with B3G_E_INVALID. */
+#define B3G_TUNE_CONVEX 0
+#define B3G_TUNE_PROBE 7
+#define B3G_TUNE_SAT_WARPS 8
+#define B3G_TUNE_SAT_BLOCKS 9
+#define B3G_TUNE_TRAVERSE 10
+#define B3G_TUNE_COUNT 11
+int b3g_autotune(b3g_ctx* ctx, uint32_t reps, void* stream, uint32_t* out);
+int b3g_set_tuning(b3g_ctx* ctx, const uint32_t* table);
+int b3g_get_tuning(b3g_ctx* ctx, uint32_t* table);
 
 /* Device pointers of the last pass's results for zero-copy consumers:
  * contacts (3 u32 each) and manifolds (320 bytes each). */
