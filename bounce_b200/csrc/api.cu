@@ -268,6 +268,13 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dBodyAwake = nullptr;
 	c->dBodyState = nullptr;
 	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = c->dFixRank = nullptr;
+	c->dFixLife = nullptr;
+	c->capBodies = c->capFixtures = 0;
+	c->keysAreIndex = true;
+	for (int i = 0; i < B3G_STAGE_RING; ++i)
+		c->stage[i] = StageSlot{nullptr, nullptr, 0, nullptr};
+	c->stageNext = 0;
+	c->dWorldCounts = nullptr;
 	c->asleep = 0;
 	c->graphLaunches = 0;
 	c->lastPassImpulses = false;
@@ -473,8 +480,19 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dFixFlags);
 	dfree(c->dFixKey);
 	dfree(c->dFixRank);
+	dfree(c->dFixLife);
 	dfree(c->dFixParams);
 	dfree(c->dFixBound);
+	for (int i = 0; i < B3G_STAGE_RING; ++i)
+	{
+		if (c->stage[i].done)
+			cudaEventDestroy(c->stage[i].done);
+		if (c->stage[i].host)
+			cudaFreeHost(c->stage[i].host);
+		if (c->stage[i].dev)
+			cudaFree(c->stage[i].dev);
+	}
+	dfree(c->dWorldCounts);
 	if (c->hCounters)
 		cudaFreeHost(c->hCounters);
 	if (c->stream)
@@ -615,8 +633,10 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 		CK(cudaMemcpy(c->dBodyAwake, awake, nb, cudaMemcpyHostToDevice));
 	}
 	c->nBodies = nb;
+	c->capBodies = nb;
 	c->nWorlds = nw;
 	c->hBodyType.assign(type, type + nb);
+	c->hAwake.assign(awake, awake + nb);
 	c->asleep = count_asleep(c, awake);
 	c->scene.bodyWorld = c->dBodyWorld;
 	c->scene.bodyType = c->dBodyType;
@@ -730,6 +750,7 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	dfree(c->dFixFlags);
 	dfree(c->dFixKey);
 	dfree(c->dFixRank);
+	dfree(c->dFixLife);
 	dfree(c->dFixParams);
 	CK(dalloc(&c->dFixBody, nf));
 	CK(dalloc(&c->dFixType, nf));
@@ -737,6 +758,8 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	CK(dalloc(&c->dFixFlags, nf));
 	CK(dalloc(&c->dFixKey, nf));
 	CK(dalloc(&c->dFixRank, nf));
+	CK(dalloc(&c->dFixLife, nf));
+	CK(cudaMemset(c->dFixLife, FIX_LIVE, nf ? nf : 1));
 	CK(dalloc(&c->dFixParams, 3 * (size_t)nf));
 	if (nf)
 	{
@@ -750,15 +773,299 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	}
 	c->hFixType.assign(shapeType, shapeType + nf);
 	c->nFixtures = nf;
+	c->capFixtures = nf;
+	c->keysAreIndex = true;
+	if (proxyKey)
+		for (uint32_t i = 0; i < nf && c->keysAreIndex; ++i)
+			c->keysAreIndex = proxyKey[i] == i;
 	c->scene.fixBody = c->dFixBody;
 	c->scene.fixType = c->dFixType;
 	c->scene.fixHull = c->dFixHull;
 	c->scene.fixFlags = c->dFixFlags;
 	c->scene.fixKey = c->dFixKey;
 	c->scene.fixRank = c->dFixRank;
+	c->scene.fixLife = c->dFixLife;
 	c->scene.fixParams = c->dFixParams;
 	c->creationPass = true;
 	c->havePass = false;
+	return B3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scene updates between passes (serving).
+
+namespace {
+
+// The bounding sphere b3g_set_fixtures computes on the host, computed the
+// same way on the device (double sums in the same order, the radius rounded
+// up twice).
+__device__ float4 fixture_bound(const DevScene& S, uint32_t type, uint32_t hull, const float* p)
+{
+	double pts[9];
+	uint32_t np = 0;
+	double skin = 0.0;
+	const float4* hv = nullptr;
+	if (type == B3G_SHAPE_SPHERE)
+	{
+		pts[0] = p[0], pts[1] = p[1], pts[2] = p[2];
+		np = 1;
+		skin = p[3];
+	}
+	else if (type == B3G_SHAPE_CAPSULE)
+	{
+		for (int k = 0; k < 6; ++k)
+			pts[k] = p[k];
+		np = 2;
+		skin = p[6];
+	}
+	else if (type == B3G_SHAPE_TRIANGLE)
+	{
+		for (int k = 0; k < 9; ++k)
+			pts[k] = p[k];
+		np = 3;
+		skin = p[9];
+	}
+	else
+	{
+		HullDesc d = S.hulls[hull];
+		hv = S.hverts + d.vOff;
+		np = d.vCnt;
+		skin = p[0];
+	}
+	auto at = [&](uint32_t v, int k) -> double {
+		if (hv)
+		{
+			float4 w = hv[v];
+			return k == 0 ? w.x : (k == 1 ? w.y : w.z);
+		}
+		return pts[3 * v + k];
+	};
+	double cx = 0, cy = 0, cz = 0;
+	for (uint32_t v = 0; v < np; ++v)
+	{
+		cx += at(v, 0);
+		cy += at(v, 1);
+		cz += at(v, 2);
+	}
+	float fx = (float)(cx / np), fy = (float)(cy / np), fz = (float)(cz / np);
+	double r = 0;
+	for (uint32_t v = 0; v < np; ++v)
+	{
+		double dx = at(v, 0) - fx, dy = at(v, 1) - fy, dz = at(v, 2) - fz;
+		r = fmax(r, sqrt(dx * dx + dy * dy + dz * dz));
+	}
+	r += fabs(skin);
+	float fr = (float)r;
+	fr = nextafterf(nextafterf(fr, INFINITY), INFINITY);
+	return make_float4(fx, fy, fz, fr);
+}
+
+struct UpdateArgs
+{
+	uint32_t nb, nf, nr;
+	const uint32_t* bIdx;
+	const uint32_t* bWorld;
+	const uint32_t* bType;
+	const uint8_t* bAwake;
+	const uint32_t* fIdx;
+	const uint32_t* fBody;
+	const uint32_t* fType;
+	const uint32_t* fHull;
+	const uint32_t* fFlags;
+	const float* fParams;
+	const uint32_t* rIdx;
+};
+
+__global__ void k_retire(DevScene S, UpdateArgs u)
+{
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < u.nr; t += gridDim.x * blockDim.x)
+		S.fixLife[u.rIdx[t]] = FIX_DEAD;
+}
+
+__global__ void k_scatter(DevScene S, UpdateArgs u, uint32_t* world, uint32_t* btype, uint8_t* awake,
+	uint32_t* fbody, uint32_t* ftype, uint32_t* fhull, uint32_t* fflags, float4* fparams, float4* fbound)
+{
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < u.nb + u.nf; t += gridDim.x * blockDim.x)
+	{
+		if (t < u.nb)
+		{
+			uint32_t b = u.bIdx[t];
+			world[b] = u.bWorld[t];
+			btype[b] = u.bType[t];
+			awake[b] = u.bAwake[t];
+			continue;
+		}
+		uint32_t j = t - u.nb;
+		uint32_t f = u.fIdx[j];
+		const float* p = u.fParams + 12 * (size_t)j;
+		fbody[f] = u.fBody[j];
+		ftype[f] = u.fType[j];
+		fhull[f] = u.fHull[j];
+		fflags[f] = u.fFlags[j];
+		for (int k = 0; k < 3; ++k)
+			fparams[3 * (size_t)f + k] = make_float4(p[4 * k], p[4 * k + 1], p[4 * k + 2], p[4 * k + 3]);
+		fbound[f] = fixture_bound(S, u.fType[j], u.fHull[j], p);
+		S.fixLife[f] = FIX_FRESH;
+	}
+}
+
+__global__ void k_world_counts(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32_t worlds, uint32_t* out)
+{
+	uint32_t n = min(B.counters[CTR_PAIRS], cap);
+	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+	{
+		uint32_t w = S.bodyWorld[S.fixBody[B.pairA[cur][c]]];
+		if (w >= worlds)
+			continue;
+		uint32_t st = B.cstate[cur][c];
+		uint32_t pc = ((st >> 8) & 0xFFu) ? B.man[cur][c].pointCount : 0u;
+		if (st & 1u)
+			atomicAdd(&out[3 * w + 0], 1u);
+		if (pc)
+		{
+			atomicAdd(&out[3 * w + 1], 1u);
+			atomicAdd(&out[3 * w + 2], pc);
+		}
+	}
+}
+
+} // namespace
+
+extern "C" int b3g_update_scene(b3g_ctx* c, uint32_t nb, const uint32_t* bodyIndex, const uint32_t* world,
+	const uint32_t* type, const uint8_t* awake, uint32_t nf, const uint32_t* fixIndex, const uint32_t* body,
+	const uint32_t* shapeType, const uint32_t* hull, const float* params, const uint32_t* flags, uint32_t nr,
+	const uint32_t* retireIndex, void* stream)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if ((nb && (!bodyIndex || !world || !type || !awake)) ||
+		(nf && (!fixIndex || !body || !shapeType || !hull || !params || !flags)) || (nr && !retireIndex))
+		return fail(c, B3G_E_INVALID, "b3g_update_scene: null argument");
+	if (c->capFixtures == 0 || c->capBodies == 0)
+		return fail(c, B3G_E_STATE, "b3g_update_scene: no scene");
+	if (!c->keysAreIndex)
+		return fail(c, B3G_E_STATE, "b3g_update_scene: needs proxy keys equal to fixture indices");
+	for (uint32_t i = 0; i < nb; ++i)
+		if (bodyIndex[i] >= c->capBodies || world[i] >= c->nWorlds || type[i] > B3G_BODY_DYNAMIC)
+			return fail(c, B3G_E_INVALID, "b3g_update_scene: body record %u invalid", i);
+	for (uint32_t i = 0; i < nf; ++i)
+		if (fixIndex[i] >= c->capFixtures || body[i] >= c->capBodies ||
+			!(shapeType[i] == B3G_SHAPE_SPHERE || shapeType[i] == B3G_SHAPE_CAPSULE ||
+				shapeType[i] == B3G_SHAPE_HULL) ||
+			(shapeType[i] == B3G_SHAPE_HULL && hull[i] >= c->nHulls))
+			return fail(c, B3G_E_INVALID, "b3g_update_scene: fixture record %u invalid", i);
+	for (uint32_t i = 0; i < nr; ++i)
+		if (retireIndex[i] >= c->capFixtures)
+			return fail(c, B3G_E_INVALID, "b3g_update_scene: retire index %u out of range", i);
+	if (nb + nf + nr == 0)
+		return B3G_OK;
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	// One host staging block per call, copied in one transfer. The staging
+	// buffers form a ring; a slot is reused once its previous copy finished.
+	size_t words = 4 * (size_t)nb + (size_t)(nb + 3) / 4 + 17 * (size_t)nf + nr;
+	size_t bytes = words * 4 + 64;
+	StageSlot& slot = c->stage[c->stageNext];
+	c->stageNext = (c->stageNext + 1) % B3G_STAGE_RING;
+	if (slot.done)
+		CK(cudaEventSynchronize(slot.done));
+	if (slot.bytes < bytes)
+	{
+		CK(cudaStreamSynchronize(s));
+		if (slot.host)
+			cudaFreeHost(slot.host);
+		if (slot.dev)
+			cudaFree(slot.dev);
+		slot.host = nullptr;
+		slot.dev = nullptr;
+		slot.bytes = 0;
+		size_t grow = std::max(bytes, (size_t)1 << 20);
+		CK(cudaMallocHost(&slot.host, grow));
+		CK(cudaMalloc(&slot.dev, grow));
+		slot.bytes = grow;
+	}
+	if (!slot.done)
+		CK(cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming));
+	uint32_t* h = (uint32_t*)slot.host;
+	uint32_t* d = (uint32_t*)slot.dev;
+	size_t o = 0;
+	UpdateArgs u;
+	u.nb = nb;
+	u.nf = nf;
+	u.nr = nr;
+	auto put = [&](const void* src, size_t n32) -> const uint32_t* {
+		std::memcpy(h + o, src, n32 * 4);
+		const uint32_t* dp = d + o;
+		o += n32;
+		return dp;
+	};
+	u.bIdx = put(bodyIndex, nb);
+	u.bWorld = put(world, nb);
+	u.bType = put(type, nb);
+	std::memcpy(h + o, awake, nb);
+	u.bAwake = (const uint8_t*)(d + o);
+	o += (nb + 3) / 4;
+	u.fIdx = put(fixIndex, nf);
+	u.fBody = put(body, nf);
+	u.fType = put(shapeType, nf);
+	u.fHull = put(hull, nf);
+	u.fFlags = put(flags, nf);
+	u.fParams = (const float*)put(params, 12 * (size_t)nf);
+	u.rIdx = put(retireIndex, nr);
+	CK(cudaMemcpyAsync(slot.dev, slot.host, o * 4, cudaMemcpyHostToDevice, s));
+	CK(cudaEventRecord(slot.done, s));
+	const int blocks = persistent_blocks(2);
+	if (nr)
+		k_retire<<<blocks, 256, 0, s>>>(c->scene, u);
+	if (nb + nf)
+		k_scatter<<<blocks, 256, 0, s>>>(c->scene, u, c->dBodyWorld, c->dBodyType, c->dBodyAwake, c->dFixBody,
+			c->dFixType, c->dFixHull, c->dFixFlags, c->dFixParams, c->dFixBound);
+	CK(cudaGetLastError());
+	// Host shadows: fixture types (stand-alone narrowphase) and sleep count.
+	for (uint32_t i = 0; i < nf; ++i)
+		c->hFixType[fixIndex[i]] = shapeType[i];
+	for (uint32_t i = 0; i < nb; ++i)
+	{
+		uint32_t b = bodyIndex[i];
+		bool was = c->hAwake[b] == 0 && c->hBodyType[b] != B3G_BODY_STATIC;
+		bool now = awake[i] == 0 && type[i] != B3G_BODY_STATIC;
+		c->hBodyType[b] = type[i];
+		c->hAwake[b] = awake[i];
+		c->asleep = c->asleep - (was ? 1u : 0u) + (now ? 1u : 0u);
+	}
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_active(b3g_ctx* c, uint32_t bodies, uint32_t fixtures)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if (bodies > c->capBodies || fixtures > c->capFixtures || fixtures == 0 || bodies == 0)
+		return fail(c, B3G_E_INVALID, "b3g_set_active: %u bodies / %u fixtures outside 1..(%u, %u)", bodies,
+			fixtures, c->capBodies, c->capFixtures);
+	if (bodies == c->nBodies && fixtures == c->nFixtures)
+		return B3G_OK;
+	CK(cudaSetDevice(c->device));
+	CK(cudaDeviceSynchronize());
+	destroy_graphs(c);
+	c->nBodies = bodies;
+	c->nFixtures = fixtures;
+	return B3G_OK;
+}
+
+extern "C" int b3g_world_counts(b3g_ctx* c, uint32_t worlds, uint32_t* out, void* stream)
+{
+	if (!c || (!out && worlds))
+		return fail(c, B3G_E_INVALID, "b3g_world_counts: null argument");
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "b3g_world_counts: no pass yet");
+	if (worlds == 0)
+		return B3G_OK;
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	CK(cudaMemsetAsync(out, 0, sizeof(uint32_t) * 3 * (size_t)worlds, s));
+	k_world_counts<<<persistent_blocks(4), 256, 0, s>>>(c->scene, c->buf, c->cur, c->cfg.max_contacts, worlds, out);
+	CK(cudaGetLastError());
 	return B3G_OK;
 }
 
@@ -773,6 +1080,7 @@ extern "C" int b3g_set_awake(b3g_ctx* c, const uint8_t* awake)
 		CK(cudaStreamSynchronize(c->stream));
 	}
 	c->asleep = count_asleep(c, awake);
+	c->hAwake.assign(awake, awake + c->capBodies);
 	return B3G_OK;
 }
 
@@ -824,8 +1132,8 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-	// pass_begin, sync, broadphase, diff + list order, bucket + 7 convex + 2 hull, finalize + pass_end
-	const uint32_t passLaunches = 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 2;
+	// pass_begin, sync, broadphase, diff + list order, bucket + 7 convex + 2 hull, finalize + pass_end + settle
+	const uint32_t passLaunches = 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 3;
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
 		c->havePass && !c->creationPass && s != nullptr;
 	c->lastPassImpulses = c->impulsesLoaded;

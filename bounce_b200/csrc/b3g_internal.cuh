@@ -97,6 +97,19 @@ struct DevScene
 	const uint32_t* fixFlags;
 	const uint32_t* fixKey;
 	const uint32_t* fixRank; // rank of the fixture's proxy key among all keys
+	uint8_t* fixLife;        // FIX_LIVE / FIX_FRESH / FIX_DEAD (scene updates between passes)
+};
+
+// Fixture life states. A fresh fixture was written by a scene update since the
+// last pass: the pass creates its proxy (CreateProxy fattening) and none of
+// its pairs continues a contact of the fixture that held the slot before. A
+// dead fixture has no proxy: it sorts after every live one, never pairs, and
+// the contacts it had are destroyed.
+enum : uint8_t
+{
+	FIX_LIVE = 0,
+	FIX_FRESH = 1,
+	FIX_DEAD = 2
 };
 
 struct Buffers
@@ -217,6 +230,16 @@ struct PassGraph
 	cudaStream_t stream;
 };
 
+// One staging block of b3g_update_scene.
+#define B3G_STAGE_RING 4
+struct StageSlot
+{
+	void* host;
+	void* dev;
+	size_t bytes;
+	cudaEvent_t done; // the block's last copy to the device finished
+};
+
 struct b3g_ctx
 {
 	b3g_config cfg;
@@ -245,6 +268,14 @@ struct b3g_ctx
 	uint8_t* dBodyAwake;
 	float* dBodyState;
 	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey, *dFixRank;
+	uint8_t* dFixLife;
+	uint32_t capBodies, capFixtures; // uploaded counts; nBodies / nFixtures are the processed prefixes
+	bool keysAreIndex;               // proxy keys = fixture indices (scene updates need it)
+	// staging of b3g_update_scene: a ring of pinned host / device blocks
+	StageSlot stage[B3G_STAGE_RING];
+	uint32_t stageNext;
+	uint32_t* dWorldCounts;
+	std::vector<uint8_t> hAwake; // host copy of the awake flags (sleep count)
 	float4* dFixParams;
 	float4* dFixBound;
 

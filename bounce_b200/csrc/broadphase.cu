@@ -131,10 +131,19 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= nf)
 		return;
+	const uint8_t life = S.fixLife[i];
+	if (life == FIX_DEAD)
+	{
+		// No proxy: an empty box (lower > upper) that overlaps nothing.
+		B.fatLo[i] = make_float4(B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR, 0.0f);
+		B.fatHi[i] = make_float4(-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR, 0.0f);
+		B.moved[i] = 0;
+		return;
+	}
 	uint32_t body = S.fixBody[i];
 	const float* st = S.bodyState + 17 * (size_t)body;
 	XF xf1 = load_xf(st);
-	if (creation)
+	if (creation || life == FIX_FRESH)
 	{
 		// b3DynamicTree::CreateProxy (dynamic_tree.cpp:108-128).
 		AABB a, unused;
@@ -241,13 +250,15 @@ __global__ void k_bounds_init(int* bnd)
 		bnd[threadIdx.x] = (int)0x80000000;
 }
 
-__global__ void k_bounds(Buffers B, uint32_t n, int* bnd)
+__global__ void k_bounds(DevScene S, Buffers B, uint32_t n, int* bnd)
 {
 	__shared__ int s[6][8];
 	float mn[3] = {B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR};
 	float mx[3] = {-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR};
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
 	{
+		if (S.fixLife[i] == FIX_DEAD)
+			continue;
 		float4 lo = B.fatLo[i], hi = B.fatHi[i];
 		float c[3] = {0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z)};
 		for (int k = 0; k < 3; ++k)
@@ -315,7 +326,8 @@ __global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
 	}
 	uint32_t code = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
 	uint32_t world = S.bodyWorld[S.fixBody[i]];
-	B.keysA[i] = ((unsigned long long)world << 32) | code;
+	// Dead proxies sort after every live one.
+	B.keysA[i] = S.fixLife[i] == FIX_DEAD ? ~0ull : ((unsigned long long)world << 32) | code;
 	B.valsA[i] = i;
 }
 
@@ -500,10 +512,14 @@ __global__ void k_leaves(DevScene S, Buffers B, int n)
 		B.nodeRope[j] = (B.nodeEnd[j] == (uint32_t)(n - 1)) ? SENT : B.splitRight[B.nodeEnd[j]];
 		B.refitFlag[j] = 0;
 	}
-	// Last sorted leaf of each world.
-	uint32_t w = S.bodyWorld[S.fixBody[proxy]];
-	if (j == n - 1 || S.bodyWorld[S.fixBody[B.valsA[j + 1]]] != w)
-		B.worldEnd[w] = j;
+	// Last sorted leaf of each world (dead proxies, sorted last, belong to none).
+	if (S.fixLife[proxy] != FIX_DEAD)
+	{
+		uint32_t w = S.bodyWorld[S.fixBody[proxy]];
+		uint32_t nx = j == n - 1 ? SENT : B.valsA[j + 1];
+		if (nx == SENT || S.fixLife[nx] == FIX_DEAD || S.bodyWorld[S.fixBody[nx]] != w)
+			B.worldEnd[w] = j;
+	}
 }
 
 __global__ void k_refit(Buffers B, int n)
@@ -659,6 +675,11 @@ __global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uin
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= n)
 		return;
+	if (S.fixLife[B.valsA[j]] == FIX_DEAD)
+	{
+		B.leafCount[j] = 0;
+		return;
+	}
 	B.leafCount[j] = walk<0, MW>(S, B, n, j, cur, cap, 0);
 }
 
@@ -771,7 +792,7 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	}
 	int* bnd = (int*)B.sceneBounds;
 	k_bounds_init<<<1, 32, 0, s>>>(bnd);
-	k_bounds<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(B, (uint32_t)n, bnd);
+	k_bounds<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
 	k_morton<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
 
 	// Radix sort over the Morton bits and, for several worlds, the world bits.

@@ -159,9 +159,12 @@ __global__ void k_kept(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
 	{
 		uint32_t kept = 1;
-		if (!B.prevFound[p])
+		uint32_t fa = B.pairA[prevBuf][p], fb = B.pairB[prevBuf][p];
+		if (S.fixLife[fa] != FIX_LIVE || S.fixLife[fb] != FIX_LIVE)
+			kept = 0; // a fixture was replaced or removed by a scene update
+		else if (!B.prevFound[p])
 		{
-			uint32_t ba = S.fixBody[B.pairA[prevBuf][p]], bb = S.fixBody[B.pairB[prevBuf][p]];
+			uint32_t ba = S.fixBody[fa], bb = S.fixBody[fb];
 			kept = (body_active(S, ba) || body_active(S, bb)) ? 0u : 1u;
 		}
 		B.keptScan[p] = kept;
@@ -535,6 +538,13 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 	if (!fetch())
 		return B3G_E_CUDA;
 	c->asleep = h[CTR_ASLEEP];
+	// Bodies past the processed prefix keep their flags.
+	if (c->hAwake.size() >= c->nBodies &&
+		cudaMemcpy(c->hAwake.data(), c->dBodyAwake, c->nBodies, cudaMemcpyDeviceToHost) != cudaSuccess)
+		return B3G_E_CUDA;
+	for (uint32_t b = c->nBodies; b < c->hAwake.size(); ++b)
+		if (c->hAwake[b] == 0 && c->hBodyType[b] != B3G_BODY_STATIC)
+			++c->asleep;
 	c->launches += launches;
 	return cudaGetLastError() == cudaSuccess ? B3G_OK : B3G_E_CUDA;
 }

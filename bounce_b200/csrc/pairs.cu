@@ -29,9 +29,11 @@ __global__ void k_diff(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32
 		if (c < n)
 		{
 			uint32_t a = B.rawA[c], b = B.rawB[c];
-			int32_t prev = havePrev ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf], B.hashCap,
-											pair_key(a, b))
-									: -1;
+			// A fresh fixture continues no contact of its slot's previous holder.
+			bool fresh = S.fixLife[a] == FIX_FRESH || S.fixLife[b] == FIX_FRESH;
+			int32_t prev = havePrev && !fresh ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf],
+													B.hashCap, pair_key(a, b))
+											  : -1;
 			if (prev >= 0)
 				B.prevFound[prev] = 1;
 			else
@@ -141,6 +143,14 @@ __global__ void k_count_moved(Buffers B, uint32_t n)
 		atomicAdd(&B.counters[CTR_MOVED], m);
 }
 
+// After the pass, fresh fixtures are ordinary live ones.
+__global__ void k_settle(DevScene S, uint32_t nf)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < nf && S.fixLife[i] == FIX_FRESH)
+		S.fixLife[i] = FIX_LIVE;
+}
+
 __global__ void k_overflow_check(Buffers B, uint32_t cap)
 {
 	if (B.counters[CTR_RAW] > cap)
@@ -216,4 +226,5 @@ void launch_finalize(b3g_ctx* c, cudaStream_t s)
 {
 	k_finalize<<<persistent_blocks(4), 256, 0, s>>>(c->buf, c->cur, c->cfg.max_contacts);
 	k_pass_end<<<1, 32, 0, s>>>(c->buf, c->cfg.max_contacts);
+	k_settle<<<(c->nFixtures + 255) / 256, 256, 0, s>>>(c->scene, c->nFixtures);
 }

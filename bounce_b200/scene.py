@@ -263,13 +263,15 @@ class Scene:
         return s, bodies, fixtures
 
 
-def plain_scene(seed=1, n_boxes=1000, n_spheres=1000, cube=20.0, world=0, scene=None, box_hull=None):
+def plain_scene(seed=1, n_boxes=1000, n_spheres=1000, cube=20.0, world=0, scene=None, box_hull=None,
+                ground_hull=None):
     """Boxes and spheres above a static ground box."""
     rng = np.random.default_rng(seed)
     s = scene if scene is not None else Scene()
     if box_hull is None:
         box_hull = s.hulls.add_box(0.5, 0.5, 0.5)
-    ground_hull = s.hulls.add_box(50.0, 0.5, 50.0)
+    if ground_hull is None:
+        ground_hull = s.hulls.add_box(50.0, 0.5, 50.0)
     g = s.add_body(world, N.BODY_STATIC, (0, -0.5, 0), (0, 0, 0, 1))
     s.add_fixture(g, N.SHAPE_HULL, [0.0], hull=ground_hull)
     n = n_boxes + n_spheres

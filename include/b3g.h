@@ -138,6 +138,53 @@ int b3g_set_fixtures(b3g_ctx* ctx, uint32_t fixture_count, const uint32_t* body,
  * only needs to call this when its solver puts bodies to sleep or wakes them. */
 int b3g_set_awake(b3g_ctx* ctx, const uint8_t* awake);
 
+/* Scene updates between passes --------------------------------------------
+ *
+ * For a host that keeps many worlds resident in one context and replaces
+ * some of them between passes (admitting new worlds, retiring finished ones)
+ * without disturbing the others; the reference has no counterpart (a new
+ * b3World per request). Needs a scene set with proxy keys equal to the
+ * fixture indices (NULL keys).
+ *
+ * b3g_update_scene overwrites body_count bodies (body_index[i]: world, type,
+ * awake, as b3g_set_bodies) and fixture_count fixtures (fixture_index[j]:
+ * body, shape type, hull, 12 params, flags, as b3g_set_fixtures; spheres,
+ * capsules and hulls), and retires retire_count fixtures (retire_index[k]).
+ * Retiring applies first, so an index may be retired and rewritten in one
+ * call. The next pass creates the proxy of every written fixture
+ * (b3DynamicTree::CreateProxy, dynamic_tree.cpp:108-128), treats each of its
+ * pairs as a new contact (AddPair) and destroys the contacts the slot's
+ * previous fixture had; a retired fixture has no proxy and its contacts are
+ * destroyed. Other fixtures keep their proxies, contacts and manifolds.
+ * World indices stay below the count set by b3g_set_bodies. Asynchronous on
+ * stream (NULL: the context's stream); the host arrays may be reused when
+ * the call returns.
+ *
+ * b3g_set_active limits the passes to bodies [0, bodies) and fixtures
+ * [0, fixtures) of the uploaded scene; everything past them must be retired
+ * (or unused). Captured passes are dropped when the limits change.
+ *
+ * b3g_world_counts writes, for worlds [0, worlds) of the last pass, 3 u32
+ * each into out (device memory): contacts touching, manifolds with points,
+ * manifold points. Asynchronous on stream. */
+int b3g_update_scene(b3g_ctx* ctx, uint32_t body_count, const uint32_t* body_index,
+	const uint32_t* world, const uint32_t* type, const uint8_t* awake,
+	uint32_t fixture_count, const uint32_t* fixture_index, const uint32_t* body,
+	const uint32_t* shape_type, const uint32_t* hull, const float* params, const uint32_t* flags,
+	uint32_t retire_count, const uint32_t* retire_index, void* stream);
+int b3g_set_active(b3g_ctx* ctx, uint32_t bodies, uint32_t fixtures);
+int b3g_world_counts(b3g_ctx* ctx, uint32_t worlds, uint32_t* out, void* stream);
+
+/* Kinematic motion on the device, for hosts whose body state lives in device
+ * memory (the serving loop): advances bodies [0, n) by dt. state: 17 floats
+ * per body (the b3g_collide layout); motion: 17 floats per body (centre 3,
+ * orientation x y z s, local centre 3, linear velocity 3, angular velocity 3,
+ * moving flag: 0 keeps the body where it is). The sweep start becomes the
+ * current pose, c += dt v, q = normalize(q + dt/2 (w, 0) q), and the
+ * transform follows (b3Body::SynchronizeTransform). Not part of the
+ * reference's collision pass (its solver moves bodies). Asynchronous. */
+int b3g_kinematic_step(float* state, float* motion, uint32_t n, float dt, void* stream);
+
 /* Pass ------------------------------------------------------------------ */
 
 /* One collision pass. body_state holds 17 floats per body:
