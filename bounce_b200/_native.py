@@ -115,6 +115,7 @@ EXPORTED = [
     "b3g_find_pairs_static",
     "b3g_autotune",
     "b3g_update_scene",
+    "b3g_update_scene_device",
     "b3g_set_active",
     "b3g_world_counts",
     "b3g_kinematic_step",
@@ -175,6 +176,8 @@ def load():
         "b3g_autotune": ([ctx, ctypes.c_uint32, vp, u32p], ctypes.c_int),
         "b3g_update_scene": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, u8p, ctypes.c_uint32, u32p, u32p, u32p, u32p,
                               f32p, u32p, ctypes.c_uint32, u32p, vp], ctypes.c_int),
+        "b3g_update_scene_device": ([ctx, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp,
+                                     ctypes.c_uint32, vp, vp], ctypes.c_int),
         "b3g_set_active": ([ctx, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_int),
         "b3g_world_counts": ([ctx, ctypes.c_uint32, vp, vp], ctypes.c_int),
         "b3g_kinematic_step": ([vp, vp, ctypes.c_uint32, ctypes.c_float, vp], ctypes.c_int),

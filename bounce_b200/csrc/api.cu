@@ -275,6 +275,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 		c->stage[i] = StageSlot{nullptr, nullptr, 0, nullptr};
 	c->stageNext = 0;
 	c->dWorldCounts = nullptr;
+	c->dUpdateBad = nullptr;
+	c->fixTypeStale = false;
 	c->asleep = 0;
 	c->graphLaunches = 0;
 	c->lastPassImpulses = false;
@@ -358,6 +360,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
 	step(dalloc(&B.missList, C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
+	step(dalloc(&c->dUpdateBad, 1), "alloc");
 	step(dalloc(&B.totals, 8), "alloc");
 	step(dalloc(&B.endedList, 3 * (size_t)C), "alloc");
 	step(dalloc(&B.touchIndex, C), "alloc");
@@ -370,6 +373,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	if (rc == B3G_OK)
 	{
 		step(cudaMemsetAsync(B.counters, 0, sizeof(uint32_t) * CTR_COUNT, c->stream), "memset");
+		step(cudaMemsetAsync(c->dUpdateBad, 0, sizeof(uint32_t), c->stream), "memset");
 		step(cudaMemsetAsync(B.totals, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[0], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
@@ -493,6 +497,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 			cudaFree(c->stage[i].dev);
 	}
 	dfree(c->dWorldCounts);
+	dfree(c->dUpdateBad);
 	if (c->hCounters)
 		cudaFreeHost(c->hCounters);
 	if (c->stream)
@@ -876,27 +881,57 @@ struct UpdateArgs
 	const uint32_t* rIdx;
 };
 
-__global__ void k_retire(DevScene S, UpdateArgs u)
+// Limits the records are checked against on the device (records from device
+// memory are not seen by the host): an invalid record is skipped and flagged.
+struct UpdateLimits
+{
+	uint32_t bodies, fixtures, worlds, hulls;
+	uint32_t* bad;
+};
+
+__global__ void k_retire(DevScene S, UpdateArgs u, UpdateLimits lim)
 {
 	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < u.nr; t += gridDim.x * blockDim.x)
-		S.fixLife[u.rIdx[t]] = FIX_DEAD;
+	{
+		uint32_t f = u.rIdx[t];
+		if (f >= lim.fixtures)
+		{
+			atomicOr(lim.bad, 1u);
+			continue;
+		}
+		S.fixLife[f] = FIX_DEAD;
+	}
 }
 
-__global__ void k_scatter(DevScene S, UpdateArgs u, uint32_t* world, uint32_t* btype, uint8_t* awake,
-	uint32_t* fbody, uint32_t* ftype, uint32_t* fhull, uint32_t* fflags, float4* fparams, float4* fbound)
+__global__ void k_scatter(DevScene S, UpdateArgs u, UpdateLimits lim, uint32_t* world, uint32_t* btype,
+	uint8_t* awake, uint32_t* fbody, uint32_t* ftype, uint32_t* fhull, uint32_t* fflags, float4* fparams,
+	float4* fbound)
 {
 	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < u.nb + u.nf; t += gridDim.x * blockDim.x)
 	{
 		if (t < u.nb)
 		{
 			uint32_t b = u.bIdx[t];
+			if (b >= lim.bodies || u.bWorld[t] >= lim.worlds || u.bType[t] > B3G_BODY_DYNAMIC)
+			{
+				atomicOr(lim.bad, 1u);
+				continue;
+			}
 			world[b] = u.bWorld[t];
 			btype[b] = u.bType[t];
-			awake[b] = u.bAwake[t];
+			awake[b] = u.bAwake ? u.bAwake[t] : 1;
 			continue;
 		}
 		uint32_t j = t - u.nb;
 		uint32_t f = u.fIdx[j];
+		uint32_t ty = u.fType[j];
+		if (f >= lim.fixtures || u.fBody[j] >= lim.bodies ||
+			!(ty == B3G_SHAPE_SPHERE || ty == B3G_SHAPE_CAPSULE || ty == B3G_SHAPE_HULL) ||
+			(ty == B3G_SHAPE_HULL && u.fHull[j] >= lim.hulls))
+		{
+			atomicOr(lim.bad, 1u);
+			continue;
+		}
 		const float* p = u.fParams + 12 * (size_t)j;
 		fbody[f] = u.fBody[j];
 		ftype[f] = u.fType[j];
@@ -930,6 +965,60 @@ __global__ void k_world_counts(DevScene S, Buffers B, uint32_t cur, uint32_t cap
 }
 
 } // namespace
+
+static void launch_update(b3g_ctx* c, const UpdateArgs& u, cudaStream_t s)
+{
+	UpdateLimits lim{c->capBodies, c->capFixtures, c->nWorlds, c->nHulls, c->dUpdateBad};
+	const int blocks = persistent_blocks(2);
+	if (u.nr)
+		k_retire<<<blocks, 256, 0, s>>>(c->scene, u, lim);
+	if (u.nb + u.nf)
+		k_scatter<<<blocks, 256, 0, s>>>(c->scene, u, lim, c->dBodyWorld, c->dBodyType, c->dBodyAwake,
+			c->dFixBody, c->dFixType, c->dFixHull, c->dFixFlags, c->dFixParams, c->dFixBound);
+}
+
+extern "C" int b3g_update_scene_device(b3g_ctx* c, uint32_t nb, const uint32_t* bodyIndex, const uint32_t* world,
+	const uint32_t* type, uint32_t nf, const uint32_t* fixIndex, const uint32_t* body, const uint32_t* shapeType,
+	const uint32_t* hull, const float* params, const uint32_t* flags, uint32_t nr, const uint32_t* retireIndex,
+	void* stream)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if ((nb && (!bodyIndex || !world || !type)) ||
+		(nf && (!fixIndex || !body || !shapeType || !hull || !params || !flags)) || (nr && !retireIndex))
+		return fail(c, B3G_E_INVALID, "b3g_update_scene_device: null argument");
+	if (c->capFixtures == 0 || c->capBodies == 0)
+		return fail(c, B3G_E_STATE, "b3g_update_scene_device: no scene");
+	if (!c->keysAreIndex)
+		return fail(c, B3G_E_STATE, "b3g_update_scene_device: needs proxy keys equal to fixture indices");
+	if (nb + nf + nr == 0)
+		return B3G_OK;
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	UpdateArgs u;
+	u.nb = nb;
+	u.nf = nf;
+	u.nr = nr;
+	u.bIdx = bodyIndex;
+	u.bWorld = world;
+	u.bType = type;
+	u.bAwake = nullptr; // written bodies are awake
+	u.fIdx = fixIndex;
+	u.fBody = body;
+	u.fType = shapeType;
+	u.fHull = hull;
+	u.fFlags = flags;
+	u.fParams = params;
+	u.rIdx = retireIndex;
+	launch_update(c, u, s);
+	CK(cudaGetLastError());
+	// The host copy of fixture types is refreshed when the stand-alone
+	// narrowphase next needs it; written bodies are awake, so the sleep count
+	// can only have dropped (it stays an upper bound until the next wake-up
+	// replay recounts it).
+	c->fixTypeStale = true;
+	return B3G_OK;
+}
 
 extern "C" int b3g_update_scene(b3g_ctx* c, uint32_t nb, const uint32_t* bodyIndex, const uint32_t* world,
 	const uint32_t* type, const uint8_t* awake, uint32_t nf, const uint32_t* fixIndex, const uint32_t* body,
@@ -1014,12 +1103,7 @@ extern "C" int b3g_update_scene(b3g_ctx* c, uint32_t nb, const uint32_t* bodyInd
 	u.rIdx = put(retireIndex, nr);
 	CK(cudaMemcpyAsync(slot.dev, slot.host, o * 4, cudaMemcpyHostToDevice, s));
 	CK(cudaEventRecord(slot.done, s));
-	const int blocks = persistent_blocks(2);
-	if (nr)
-		k_retire<<<blocks, 256, 0, s>>>(c->scene, u);
-	if (nb + nf)
-		k_scatter<<<blocks, 256, 0, s>>>(c->scene, u, c->dBodyWorld, c->dBodyType, c->dBodyAwake, c->dFixBody,
-			c->dFixType, c->dFixHull, c->dFixFlags, c->dFixParams, c->dFixBound);
+	launch_update(c, u, s);
 	CK(cudaGetLastError());
 	// Host shadows: fixture types (stand-alone narrowphase) and sleep count.
 	for (uint32_t i = 0; i < nf; ++i)
@@ -1245,6 +1329,16 @@ extern "C" int b3g_get_counts(b3g_ctx* c, b3g_counts* out)
 	out->manifolds = h[CTR_MANIFOLDS];
 	out->points = h[CTR_POINTS];
 	out->moved = h[CTR_MOVED];
+	uint32_t bad = 0;
+	if (c->dUpdateBad)
+	{
+		CK(cudaMemcpy(&bad, c->dUpdateBad, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+		if (bad)
+		{
+			CK(cudaMemset(c->dUpdateBad, 0, sizeof(uint32_t)));
+			return fail(c, B3G_E_INVALID, "a device-side scene update held invalid records (skipped)");
+		}
+	}
 	out->status = status_code(h[CTR_STATUS]);
 	if (out->status)
 		return fail(c, -(int)out->status, "pass status 0x%x (pairs %u, capacity %u)", h[CTR_STATUS],
@@ -1411,6 +1505,12 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	if (n == 0)
 		return B3G_OK;
 	CK(cudaSetDevice(c->device));
+	if (c->fixTypeStale)
+	{
+		CK(cudaDeviceSynchronize());
+		CK(cudaMemcpy(c->hFixType.data(), c->dFixType, sizeof(uint32_t) * c->hFixType.size(), cudaMemcpyDeviceToHost));
+		c->fixTypeStale = false;
+	}
 	std::vector<std::vector<uint32_t>> lists(BK_COUNT);
 	for (uint32_t i = 0; i < n; ++i)
 	{

@@ -98,6 +98,11 @@ struct DevScene
 	const uint32_t* fixKey;
 	const uint32_t* fixRank; // rank of the fixture's proxy key among all keys
 	uint8_t* fixLife;        // FIX_LIVE / FIX_FRESH / FIX_DEAD (scene updates between passes)
+	// triangle fixtures: b3TriangleHull per fixture (vertices 0-2, planes 3-4,
+	// centroid 5; 6 float4) and the edge wings (3 float4: wing vertex, w = 1
+	// when the edge has one)
+	const float4* fixTri;
+	const float4* fixWing;
 };
 
 // Fixture life states. A fresh fixture was written by a scene update since the
@@ -269,12 +274,16 @@ struct b3g_ctx
 	float* dBodyState;
 	uint32_t *dFixBody, *dFixType, *dFixHull, *dFixFlags, *dFixKey, *dFixRank;
 	uint8_t* dFixLife;
+	float4* dFixTri;
+	float4* dFixWing;
 	uint32_t capBodies, capFixtures; // uploaded counts; nBodies / nFixtures are the processed prefixes
 	bool keysAreIndex;               // proxy keys = fixture indices (scene updates need it)
 	// staging of b3g_update_scene: a ring of pinned host / device blocks
 	StageSlot stage[B3G_STAGE_RING];
 	uint32_t stageNext;
 	uint32_t* dWorldCounts;
+	uint32_t* dUpdateBad;        // a device-side scene update skipped invalid records
+	bool fixTypeStale;           // hFixType lags device-side scene updates
 	std::vector<uint8_t> hAwake; // host copy of the awake flags (sleep count)
 	float4* dFixParams;
 	float4* dFixBound;

@@ -34,6 +34,30 @@ __device__ __forceinline__ HullRef hull_ref(const DevScene& S, uint32_t h)
 	return r;
 }
 
+// b3TriangleHull (triangle_hull.h:26-70): every triangle hull has the same
+// topology, two faces of three half-edges each (twin = i ^ 1; origin, face,
+// prev, next), so only its vertices, planes and centroid are stored per
+// fixture.
+__device__ const uint4 kTriEdges[6] = {
+	{0, 0, 4, 2}, {1, 1, 3, 5}, {1, 0, 0, 4}, {2, 1, 5, 1}, {2, 0, 2, 0}, {0, 1, 1, 3}};
+__device__ const uint32_t kTriFaces[2] = {0, 1};
+
+__device__ __forceinline__ HullRef tri_ref(const DevScene& S, uint32_t fix)
+{
+	const float4* t = S.fixTri + 6 * (size_t)fix;
+	HullRef r;
+	r.v = t;
+	r.e = kTriEdges;
+	r.f = kTriFaces;
+	r.p = t + 3;
+	r.vCnt = 3;
+	r.eCnt = 6;
+	r.fCnt = 2;
+	float4 c = t[5];
+	r.centroid = V3{c.x, c.y, c.z};
+	return r;
+}
+
 __device__ __forceinline__ V3 hv(const HullRef& h, uint32_t i)
 {
 	float4 w = h.v[i];

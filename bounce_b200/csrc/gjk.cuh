@@ -58,6 +58,13 @@ struct GJKOut
 	uint32_t iterations;
 };
 
+// The final simplex's support indices (b3Simplex::WriteCache, gjk.cpp:870-878).
+struct GJKSimplexOut
+{
+	uint32_t count;
+	uint32_t index1[4], index2[4];
+};
+
 // b3Barycentric (gjk.cpp:99-113): divisor = u + v.
 __device__ __forceinline__ void bary2(float out[3], V3 A, V3 B, V3 Q)
 {
@@ -389,7 +396,8 @@ struct Simplex
 };
 
 // b3GJK with an empty simplex cache (gjk.cpp:654-812 via :1104-1110).
-__device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, bool applyRadius)
+__device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, bool applyRadius,
+	GJKSimplexOut* simplexOut = nullptr)
 {
 	Simplex sx;
 	{
@@ -453,6 +461,16 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 		else
 			sx.v[3] = vx;
 		++sx.count;
+	}
+	if (simplexOut)
+	{
+		simplexOut->count = sx.count;
+#pragma unroll
+		for (int i = 0; i < 4; ++i)
+		{
+			simplexOut->index1[i] = sx.v[i].index1;
+			simplexOut->index2[i] = sx.v[i].index2;
+		}
 	}
 	GJKOut out;
 	sx.closest_points(out.point1, out.point2);

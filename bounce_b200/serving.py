@@ -159,12 +159,10 @@ class ServingEngine:
         self.state[:, 13] = 1.0
         self.motion = torch.zeros((capacity, 17), dtype=f32, device=self.dev)
         self.motion[:, 6] = 1.0
-        self.up_host = torch.zeros((capacity, 34), dtype=f32, pin_memory=True)
-        self.up_idx_host = torch.zeros(capacity, dtype=torch.int64, pin_memory=True)
         self.counts_dev = torch.zeros((ring, max_worlds, 3), dtype=torch.int32, device=self.dev)
         self.counts_host = torch.zeros((ring, max_worlds, 3), dtype=torch.int32, pin_memory=True)
         self.ring = ring
-        self.up_ready = None
+        self._keep = None
         self.events = collections.deque()  # (step, ring slot, event, finished requests)
         self.stream = torch.cuda.Stream(device=self.dev)
         self.sptr = self.stream.cuda_stream
@@ -227,68 +225,87 @@ class ServingEngine:
         self.pending_admit.append(req)
         return True
 
+    def load_templates(self, templates):
+        """Stages the worlds requests may ask for in device memory (a request's
+        payload is uploaded once; admission copies it into its slot on the
+        device)."""
+        torch = self.torch
+        off = 0
+        rows = []
+        for t in templates:
+            t.offset = off
+            off += t.n
+            center = S.xf_apply(t.pos, t.quat, t.lc).astype(F)
+            st = np.concatenate([t.pos, t.quat, center, t.quat, t.lc], axis=1)
+            mo = np.concatenate([center, t.quat, t.lc, t.lin, t.ang,
+                                 (t.body_type == N.BODY_DYNAMIC).astype(F)[:, None]], axis=1)
+            rows.append((t, st, mo))
+        cat = lambda xs, dt: torch.from_numpy(np.ascontiguousarray(np.concatenate(xs), dt)).to(self.dev)
+        self.st_btype = cat([t.body_type for t, _, _ in rows], np.int32)
+        self.st_fbody = cat([t.fix_body for t, _, _ in rows], np.int32)
+        self.st_ftype = cat([t.fix_type for t, _, _ in rows], np.int32)
+        self.st_fhull = cat([t.fix_hull for t, _, _ in rows], np.int32)
+        self.st_fflags = cat([t.fix_flags for t, _, _ in rows], np.int32)
+        self.st_params = cat([t.fix_params for t, _, _ in rows], F)
+        self.st_state = cat([st for _, st, _ in rows], F)
+        self.st_motion = cat([mo for _, _, mo in rows], F)
+        return templates
+
+    def _expand(self, starts, counts, offsets=None):
+        """Device index vectors of the ranges (start_i, count_i): for each
+        element its destination, its source (offset_i + local) and its range."""
+        torch = self.torch
+        total = int(sum(counts))
+        c = torch.tensor(counts, dtype=torch.int64).to(self.dev, non_blocking=True)
+        st = torch.tensor(starts, dtype=torch.int64).to(self.dev, non_blocking=True)
+        rep = torch.repeat_interleave(torch.arange(len(counts), device=self.dev), c, output_size=total)
+        base = torch.cumsum(c, 0) - c
+        local = torch.arange(total, device=self.dev) - base[rep]
+        dst = st[rep] + local
+        src = None
+        if offsets is not None:
+            src = torch.tensor(offsets, dtype=torch.int64).to(self.dev, non_blocking=True)[rep] + local
+        return dst, src, rep, st
+
     def _flush_updates(self):
         torch = self.torch
         adm = self.pending_admit
-        if adm and self.up_ready is not None:
-            self.up_ready.synchronize()
         ret = self.pending_retire
         if not adm and not ret:
             return
-        if adm:
-            bidx = np.concatenate([r.start + np.arange(r.tmpl.n, dtype=np.uint32) for r in adm]).astype(np.uint32)
-            world = np.concatenate([np.full(r.tmpl.n, r.world, np.uint32) for r in adm])
-            btype = np.concatenate([r.tmpl.body_type for r in adm]).astype(np.uint32)
-            awake = np.ones(len(bidx), np.uint8)
-            fbody = np.concatenate([r.start + r.tmpl.fix_body for r in adm]).astype(np.uint32)
-            ftype = np.concatenate([r.tmpl.fix_type for r in adm]).astype(np.uint32)
-            fhull = np.concatenate([r.tmpl.fix_hull for r in adm]).astype(np.uint32)
-            fparams = np.ascontiguousarray(np.concatenate([r.tmpl.fix_params for r in adm]), F)
-            fflags = np.concatenate([r.tmpl.fix_flags for r in adm]).astype(np.uint32)
-            fidx = bidx  # one fixture per body, fixture i on body i
-            # initial pass input and motion record of the admitted bodies
-            pos = np.concatenate([r.tmpl.pos for r in adm])
-            quat = np.concatenate([r.tmpl.quat for r in adm])
-            lcs = np.concatenate([r.tmpl.lc for r in adm])
-            center = S.xf_apply(pos, quat, lcs).astype(F)
-            nb = len(bidx)
-            up = self.up_host.numpy()[:nb]
-            up[:, 0:3] = pos
-            up[:, 3:7] = quat
-            up[:, 7:10] = center
-            up[:, 10:14] = quat
-            up[:, 14:17] = lcs
-            up[:, 17:20] = center
-            up[:, 20:24] = quat
-            up[:, 24:27] = lcs
-            up[:, 27:30] = np.concatenate([r.tmpl.lin for r in adm])
-            up[:, 30:33] = np.concatenate([r.tmpl.ang for r in adm])
-            up[:, 33] = np.concatenate([r.tmpl.body_type == N.BODY_DYNAMIC for r in adm])
-            self.up_idx_host.numpy()[:nb] = bidx
-        else:
-            bidx = world = btype = fbody = ftype = fhull = fflags = fidx = np.zeros(0, np.uint32)
-            awake = np.zeros(0, np.uint8)
-            fparams = np.zeros((0, 12), F)
-        rix = np.concatenate([np.arange(s, s + n, dtype=np.uint32) for s, n in ret]) if ret else np.zeros(0, np.uint32)
         with torch.cuda.stream(self.stream):
-            self._check(self.lib.b3g_update_scene(
-                self.ctx, len(bidx), N.ptr(bidx, u32), N.ptr(world, u32), N.ptr(btype, u32),
-                N.ptr(awake, ctypes.c_uint8), len(fidx), N.ptr(fidx, u32), N.ptr(fbody, u32), N.ptr(ftype, u32),
-                N.ptr(fhull, u32), N.ptr(fparams, ctypes.c_float), N.ptr(fflags, u32), len(rix), N.ptr(rix, u32),
-                ctypes.c_void_p(self.sptr)))
+            keep = []
+            nb = nr = 0
+            z = self.st_btype[:0]
+            bidx = world = btype = fbody = ftype = fhull = fflags = rix = z
+            params = self.st_params[:0]
             if adm:
+                dst, src, rep, st = self._expand([r.start for r in adm], [r.tmpl.n for r in adm],
+                                                 [r.tmpl.offset for r in adm])
+                wids = torch.tensor([r.world for r in adm], dtype=torch.int32).to(self.dev, non_blocking=True)
+                bidx = dst.to(torch.int32)
+                world = wids[rep]
+                btype = self.st_btype[src]
+                fbody = (st[rep] + self.st_fbody[src]).to(torch.int32)
+                ftype = self.st_ftype[src]
+                fhull = self.st_fhull[src]
+                fflags = self.st_fflags[src]
+                params = self.st_params[src].contiguous()
+                self.state.index_copy_(0, dst, self.st_state[src])
+                self.motion.index_copy_(0, dst, self.st_motion[src])
                 nb = len(bidx)
-                idx = self.up_idx_host[:nb].to(self.dev, non_blocking=True)
-                up = self.up_host[:nb].to(self.dev, non_blocking=True)
-                self.state.index_copy_(0, idx, up[:, :17])
-                self.motion.index_copy_(0, idx, up[:, 17:])
-                # the pinned staging is rewritten by the next admission
-                self.up_ready = torch.cuda.Event()
-                self.up_ready.record(self.stream)
+            if ret:
+                rdst, _, _, _ = self._expand([a for a, _ in ret], [n for _, n in ret])
+                rix = rdst.to(torch.int32)
+                nr = len(rix)
+            keep = [bidx, world, btype, fbody, ftype, fhull, fflags, params, rix]
+            p = lambda t: ctypes.c_void_p(t.data_ptr()) if t.numel() else None
+            self._check(self.lib.b3g_update_scene_device(
+                self.ctx, nb, p(bidx), p(world), p(btype), nb, p(bidx), p(fbody), p(ftype), p(fhull), p(params),
+                p(fflags), nr, p(rix), ctypes.c_void_p(self.sptr)))
+            self._keep = keep  # alive until the next update (stream order covers their use)
         self.pending_admit = []
         self.pending_retire = []
-
-    # -- one step --------------------------------------------------------------
 
     def _integrate(self, n):
         """One kinematic step of body slots [0, n) (b3g_kinematic_step)."""
@@ -391,7 +408,7 @@ def make_templates(engine, n_templates, seed, lo=32, hi=8192):
         n = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
         out.append(WorldTemplate(int(rng.integers(1 << 31)), n, engine.box_hull, engine.ground_hull,
                                  engine.hull_arrays))
-    return out
+    return engine.load_templates(out)
 
 
 def run_stream(engine, templates, rate, duration, seed, max_in_flight=2, kmax=16, drain=5.0):

@@ -172,6 +172,15 @@ int b3g_update_scene(b3g_ctx* ctx, uint32_t body_count, const uint32_t* body_ind
 	uint32_t fixture_count, const uint32_t* fixture_index, const uint32_t* body,
 	const uint32_t* shape_type, const uint32_t* hull, const float* params, const uint32_t* flags,
 	uint32_t retire_count, const uint32_t* retire_index, void* stream);
+/* The same update from device memory (every array a device pointer, bodies
+ * written awake): the host never sees the records, so they are checked on
+ * the device; invalid ones are skipped and the next b3g_get_counts returns
+ * B3G_E_INVALID. */
+int b3g_update_scene_device(b3g_ctx* ctx, uint32_t body_count, const uint32_t* body_index,
+	const uint32_t* world, const uint32_t* type,
+	uint32_t fixture_count, const uint32_t* fixture_index, const uint32_t* body,
+	const uint32_t* shape_type, const uint32_t* hull, const float* params, const uint32_t* flags,
+	uint32_t retire_count, const uint32_t* retire_index, void* stream);
 int b3g_set_active(b3g_ctx* ctx, uint32_t bodies, uint32_t fixtures);
 int b3g_world_counts(b3g_ctx* ctx, uint32_t worlds, uint32_t* out, void* stream);
 

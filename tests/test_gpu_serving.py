@@ -57,6 +57,7 @@ def test_world_alone_equals_in_mix():
     mix.close()
 
     alone = SV.ServingEngine(capacity=1 << 16, max_worlds=64, active_quantum=4096)
+    alone.load_templates(tmpls)
     a = SV.Request(0, target, 6, 0.0)
     assert alone.admit(a) and a.start == 0
     ref = None
