@@ -23,7 +23,7 @@ BODY_STATIC, BODY_KINEMATIC, BODY_DYNAMIC = 0, 1, 2
 FLAG_WARM_STARTING = 1
 FLAG_CONVEX_CACHE = 2
 FLAG_GRAPH = 4
-TUNE_CONVEX, TUNE_PROBE, TUNE_SAT_WARPS, TUNE_SAT_BLOCKS, TUNE_TRAVERSE, TUNE_COUNT = 0, 7, 8, 9, 10, 11
+TUNE_CONVEX, TUNE_PROBE, TUNE_SAT_WARPS, TUNE_SAT_BLOCKS, TUNE_TRAVERSE, TUNE_COUNT = 0, 9, 10, 11, 12, 13
 FIXTURE_SENSOR = 1
 
 
@@ -96,6 +96,7 @@ EXPORTED = [
     "b3g_set_bodies",
     "b3g_set_fixtures",
     "b3g_set_awake",
+    "b3g_set_triangle_wings",
     "b3g_collide",
     "b3g_get_counts",
     "b3g_fetch_contacts",
@@ -153,6 +154,7 @@ def load():
         "b3g_set_bodies": ([ctx, ctypes.c_uint32, u32p, u32p, u8p], ctypes.c_int),
         "b3g_set_fixtures": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, u32p], ctypes.c_int),
         "b3g_set_awake": ([ctx, u8p], ctypes.c_int),
+        "b3g_set_triangle_wings": ([ctx, ctypes.c_uint32, u32p, f32p], ctypes.c_int),
         "b3g_collide": ([ctx, vp, ctypes.c_int, vp], ctypes.c_int),
         "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
         "b3g_fetch_contacts": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),

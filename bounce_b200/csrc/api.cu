@@ -105,6 +105,28 @@ __global__ void k_pass_begin(uint32_t* counters, int havePass, uint32_t cap)
 		counters[i] = 0;
 }
 
+// b3TriangleHull::Set (triangle_hull.h:36-69) for every triangle fixture:
+// vertices, the two face planes (normal from (B - A) x (C - A), through the
+// centroid) and the centroid.
+__global__ void k_triangle_hulls(DevScene S, uint32_t nf, float4* tri)
+{
+	uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+	if (f >= nf || S.fixType[f] != B3G_SHAPE_TRIANGLE)
+		return;
+	float4 p0 = S.fixParams[3 * f], p1 = S.fixParams[3 * f + 1], p2 = S.fixParams[3 * f + 2];
+	V3 A = V3{p0.x, p0.y, p0.z}, B = V3{p0.w, p1.x, p1.y}, C = V3{p1.z, p1.w, p2.x};
+	V3 centroid = ((A + B) + C) / 3.0f;
+	V3 N = normalized(cross(B - A, C - A));
+	float4* t = tri + 6 * (size_t)f;
+	t[0] = make_float4(A.x, A.y, A.z, 0.0f);
+	t[1] = make_float4(B.x, B.y, B.z, 0.0f);
+	t[2] = make_float4(C.x, C.y, C.z, 0.0f);
+	t[3] = make_float4(N.x, N.y, N.z, dot(N, centroid));
+	V3 M = -N;
+	t[4] = make_float4(M.x, M.y, M.z, dot(M, centroid));
+	t[5] = make_float4(centroid.x, centroid.y, centroid.z, 0.0f);
+}
+
 __global__ void k_touch_flags(const DevManifold* man, const uint32_t* cstate, uint32_t n, uint32_t* flags)
 {
 	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -269,6 +291,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dBodyState = nullptr;
 	c->dFixBody = c->dFixType = c->dFixHull = c->dFixFlags = c->dFixKey = c->dFixRank = nullptr;
 	c->dFixLife = nullptr;
+	c->dFixTri = nullptr;
+	c->dFixWing = nullptr;
+	c->triSlots = 0;
 	c->capBodies = c->capFixtures = 0;
 	c->keysAreIndex = true;
 	for (int i = 0; i < B3G_STAGE_RING; ++i)
@@ -485,6 +510,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dFixKey);
 	dfree(c->dFixRank);
 	dfree(c->dFixLife);
+	dfree(c->dFixTri);
+	dfree(c->dFixWing);
 	dfree(c->dFixParams);
 	dfree(c->dFixBound);
 	for (int i = 0; i < B3G_STAGE_RING; ++i)
@@ -663,12 +690,15 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	CK(cudaStreamSynchronize(c->stream));
 	destroy_graphs(c);
 	std::vector<uint32_t> key(nf);
+	bool hasTriangles = false;
 	for (uint32_t i = 0; i < nf; ++i)
 	{
 		if (body[i] >= c->nBodies)
 			return fail(c, B3G_E_INVALID, "fixture %u: body %u out of range", i, body[i]);
 		if (shapeType[i] > B3G_SHAPE_HULL)
 			return fail(c, B3G_E_INVALID, "fixture %u: shape type %u not supported", i, shapeType[i]);
+		if (shapeType[i] == B3G_SHAPE_TRIANGLE)
+			hasTriangles = true;
 		if (shapeType[i] == B3G_SHAPE_HULL && hull[i] >= c->nHulls)
 			return fail(c, B3G_E_INVALID, "fixture %u: hull %u out of range", i, hull[i]);
 		key[i] = proxyKey ? proxyKey[i] : i;
@@ -791,6 +821,24 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	c->scene.fixRank = c->dFixRank;
 	c->scene.fixLife = c->dFixLife;
 	c->scene.fixParams = c->dFixParams;
+	// Triangle fixtures (after every scene pointer above is current): their b3TriangleHull, built on the device with the
+	// pass's arithmetic, and wings (none until b3g_set_triangle_wings).
+	dfree(c->dFixTri);
+	dfree(c->dFixWing);
+	const size_t triSlots = hasTriangles ? nf : 1;
+	CK(dalloc(&c->dFixTri, 6 * triSlots));
+	CK(dalloc(&c->dFixWing, 3 * triSlots));
+	CK(cudaMemset(c->dFixTri, 0, sizeof(float4) * 6 * triSlots));
+	CK(cudaMemset(c->dFixWing, 0, sizeof(float4) * 3 * triSlots));
+	c->scene.fixTri = c->dFixTri;
+	c->scene.fixWing = c->dFixWing;
+	c->triSlots = (uint32_t)triSlots;
+	if (hasTriangles)
+	{
+		k_triangle_hulls<<<(nf + 255) / 256, 256>>>(c->scene, nf, c->dFixTri);
+		CK(cudaGetLastError());
+		CK(cudaDeviceSynchronize());
+	}
 	c->creationPass = true;
 	c->havePass = false;
 	return B3G_OK;
@@ -1168,6 +1216,30 @@ extern "C" int b3g_set_awake(b3g_ctx* c, const uint8_t* awake)
 	return B3G_OK;
 }
 
+extern "C" int b3g_set_triangle_wings(b3g_ctx* c, uint32_t n, const uint32_t* fixture, const float* wings)
+{
+	if (!c || (n && (!fixture || !wings)))
+		return fail(c, B3G_E_INVALID, "b3g_set_triangle_wings: null argument");
+	if (c->nFixtures == 0)
+		return fail(c, B3G_E_STATE, "b3g_set_triangle_wings: no fixtures");
+	std::vector<float4> w(3 * (size_t)n);
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		if (fixture[i] >= c->capFixtures || c->hFixType[fixture[i]] != B3G_SHAPE_TRIANGLE ||
+			fixture[i] >= c->triSlots)
+			return fail(c, B3G_E_INVALID, "b3g_set_triangle_wings: fixture %u is not a triangle", fixture[i]);
+		const float* x = wings + 12 * (size_t)i;
+		for (int k = 0; k < 3; ++k)
+			w[3 * i + k] = make_float4(x[3 * k], x[3 * k + 1], x[3 * k + 2], x[9 + k] != 0.0f ? 1.0f : 0.0f);
+	}
+	CK(cudaSetDevice(c->device));
+	CK(cudaDeviceSynchronize());
+	for (uint32_t i = 0; i < n; ++i)
+		CK(cudaMemcpy(c->dFixWing + 3 * (size_t)fixture[i], &w[3 * i], sizeof(float4) * 3, cudaMemcpyHostToDevice));
+	destroy_graphs(c);
+	return B3G_OK;
+}
+
 extern "C" int b3g_fetch_awake(b3g_ctx* c, uint8_t* out, uint32_t capacity)
 {
 	if (!c || (!out && capacity))
@@ -1216,8 +1288,10 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-	// pass_begin, sync, broadphase, diff + list order, bucket + 7 convex + 2 hull, finalize + pass_end + settle
-	const uint32_t passLaunches = 1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 10 + 3;
+	// pass_begin, sync, broadphase, diff + list order, bucket + convex kernels + 2 hull + hull-triangle,
+	// finalize + pass_end + settle
+	const uint32_t passLaunches =
+		1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 1 + B3G_CONVEX_KERNELS + 2 + 1 + 3;
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
 		c->havePass && !c->creationPass && s != nullptr;
 	c->lastPassImpulses = c->impulsesLoaded;
@@ -1530,6 +1604,12 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 			bk = BK_HULL_CAPSULE;
 		else if (ta == B3G_SHAPE_HULL && tb == B3G_SHAPE_HULL)
 			bk = BK_HULLS;
+		else if (ta == B3G_SHAPE_TRIANGLE && tb == B3G_SHAPE_SPHERE)
+			bk = BK_TRIANGLE_SPHERE;
+		else if (ta == B3G_SHAPE_TRIANGLE && tb == B3G_SHAPE_CAPSULE)
+			bk = BK_TRIANGLE_CAPSULE;
+		else if (ta == B3G_SHAPE_HULL && tb == B3G_SHAPE_TRIANGLE)
+			bk = BK_HULL_TRIANGLE;
 		if (bk == BK_COUNT)
 			return fail(c, B3G_E_INVALID, "pair %u: shape pair (%u, %u) not supported here", i, ta, tb);
 		lists[bk].push_back(i);
@@ -1631,6 +1711,10 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 				if (b == BK_HULLS)
 				{
 					launch_hulls(a, dList + offs[b], dCount + b, c->maxUniqueEdges, c->tune, c->stream);
+				}
+				else if (b == BK_HULL_TRIANGLE)
+				{
+					launch_hull_triangles(a, dList + offs[b], dCount + b, c->maxUniqueEdges, c->tune, c->stream);
 				}
 				else
 				{
@@ -1804,7 +1888,7 @@ extern "C" int b3g_autotune(b3g_ctx* c, uint32_t reps, void* stream, uint32_t* o
 		slot = bestV;
 	};
 	static const uint32_t convexBucket[B3G_CONVEX_KERNELS] = {BK_SPHERES, BK_CAPSULE_SPHERE, BK_CAPSULES,
-		BK_HULL_SPHERE, BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
+		BK_TRIANGLE_SPHERE, BK_TRIANGLE_CAPSULE, BK_HULL_SPHERE, BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
 	for (int k = 0; k < B3G_CONVEX_KERNELS && rc == B3G_OK; ++k)
 	{
 		if (h[CTR_BUCKET0 + convexBucket[k]] == 0)

@@ -217,7 +217,7 @@ enum
 };
 
 // Launch shapes of the tunable kernels (include/b3g.h, B3G_TUNE_*).
-#define B3G_CONVEX_KERNELS 7
+#define B3G_CONVEX_KERNELS 9
 struct Tune
 {
 	uint32_t v[B3G_TUNE_COUNT];
@@ -276,6 +276,7 @@ struct b3g_ctx
 	uint8_t* dFixLife;
 	float4* dFixTri;
 	float4* dFixWing;
+	uint32_t triSlots; // fixtures with triangle storage (all, or 1 when there are no triangles)
 	uint32_t capBodies, capFixtures; // uploaded counts; nBodies / nFixtures are the processed prefixes
 	bool keysAreIndex;               // proxy keys = fixture indices (scene updates need it)
 	// staging of b3g_update_scene: a ring of pinned host / device blocks

@@ -263,6 +263,25 @@ B3G_HD void barycentric_segment(float out[3], V3 A, V3 B, V3 Q)
 	out[2] = divisor;
 }
 
+// b3BarycentricCoordinates for a triangle (geometry.h:45-68): u, v, w and
+// the divisor.
+B3G_HD void barycentric_triangle(float out[4], V3 A, V3 B, V3 C, V3 Q)
+{
+	V3 AB = B - A;
+	V3 AC = C - A;
+	V3 QA = A - Q;
+	V3 QB = B - Q;
+	V3 QC = C - Q;
+	V3 QB_x_QC = cross(QB, QC);
+	V3 QC_x_QA = cross(QC, QA);
+	V3 QA_x_QB = cross(QA, QB);
+	V3 AB_x_AC = cross(AB, AC);
+	out[0] = dot(QB_x_QC, AB_x_AC);
+	out[1] = dot(QC_x_QA, AB_x_AC);
+	out[2] = dot(QA_x_QB, AB_x_AC);
+	out[3] = dot(AB_x_AC, AB_x_AC);
+}
+
 // b3Perp (vec3.h:247-262).
 B3G_HD V3 perp(V3 v)
 {

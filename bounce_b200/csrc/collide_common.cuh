@@ -649,6 +649,8 @@ void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* coun
 void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t* count, const Tune& tune,
 	cudaStream_t s);
 void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s);
+void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE,
+	const Tune& tune, cudaStream_t s);
 void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
 
 __device__ __forceinline__ XF load_xf7(const float* s)

@@ -397,6 +397,285 @@ __device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF
 		hull_capsule_face_contact(m, xf1, h1, faceIndex, r1, xf2, v1, v2, r2);
 }
 
+// ---------------------------------------------------------------------------
+// Triangles (with optional edge wings for smooth edges).
+
+struct TriWings
+{
+	V3 e[3];
+	bool has[3];
+};
+
+__device__ __forceinline__ TriWings load_wings(const DevScene& S, uint32_t fix)
+{
+	TriWings w;
+	for (int k = 0; k < 3; ++k)
+	{
+		float4 x = S.fixWing[3 * (size_t)fix + k];
+		w.e[k] = V3{x.x, x.y, x.z};
+		w.has[k] = x.w != 0.0f;
+	}
+	return w;
+}
+
+__device__ __forceinline__ V3 tri_v1(const ShapeP& s) { return V3{s.p0.x, s.p0.y, s.p0.z}; }
+__device__ __forceinline__ V3 tri_v2(const ShapeP& s) { return V3{s.p0.w, s.p1.x, s.p1.y}; }
+__device__ __forceinline__ V3 tri_v3(const ShapeP& s) { return V3{s.p1.z, s.p1.w, s.p2.x}; }
+__device__ __forceinline__ float tri_radius(const ShapeP& s) { return s.p2.y; }
+
+// One point from P on the triangle to the sphere centre (every region of
+// b3CollideTriangleAndSphere ends this way).
+__device__ __forceinline__ bool tri_sphere_point(DevManifold& m, V3 P, V3 Q, float radius, V3 center2)
+{
+	V3 d = Q - P;
+	float dd = dot(d, d);
+	if (dd > radius * radius)
+		return false;
+	V3 n = V3{0.0f, 1.0f, 0.0f};
+	float l = len(d);
+	if (l > B3G_EPSILON)
+		n = d / l;
+	m.pointCount = 1;
+	set_point(m.points[0], n, P, center2);
+	set_id0(m.points[0]);
+	return true;
+}
+
+// Is Q in the face region of the wing triangle (A1, B1, C1)?
+__device__ __forceinline__ bool in_wing_face(V3 A1, V3 B1, V3 C1, V3 Q)
+{
+	float w[4];
+	barycentric_triangle(w, A1, B1, C1, Q);
+	return w[0] > 0.0f && w[1] > 0.0f && w[2] > 0.0f;
+}
+
+// b3CollideTriangleAndSphere (collide_triangle_sphere.cpp:24-296): Voronoi
+// regions of the triangle, edge regions suppressed when the sphere lies in
+// the face region of the triangle across a winged edge.
+__device__ void collide_triangle_sphere(DevManifold& m, const XF& xf1, const ShapeP& t1, const TriWings& wg,
+	const XF& xf2, const ShapeP& s2)
+{
+	V3 center2 = sph_center(s2);
+	V3 Q = xmult(xf1, xmul(xf2, center2));
+	V3 A = tri_v1(t1), B = tri_v2(t1), C = tri_v3(t1);
+	float radius = tri_radius(t1) + sph_radius(s2);
+	float wAB[3], wBC[3], wCA[3];
+	barycentric_segment(wAB, A, B, Q);
+	barycentric_segment(wBC, B, C, Q);
+	barycentric_segment(wCA, C, A, Q);
+	// vertex regions
+	if (wAB[1] <= 0.0f && wCA[0] <= 0.0f)
+	{
+		tri_sphere_point(m, A, Q, radius, center2);
+		return;
+	}
+	if (wAB[0] <= 0.0f && wBC[1] <= 0.0f)
+	{
+		tri_sphere_point(m, B, Q, radius, center2);
+		return;
+	}
+	if (wBC[0] <= 0.0f && wCA[1] <= 0.0f)
+	{
+		tri_sphere_point(m, C, Q, radius, center2);
+		return;
+	}
+	float wABC[4];
+	barycentric_triangle(wABC, A, B, C, Q);
+	// edge regions
+	if (wAB[0] > 0.0f && wAB[1] > 0.0f && wABC[3] * wABC[2] <= 0.0f)
+	{
+		float den = 1.0f / wAB[2];
+		V3 P = den * (wAB[0] * A + wAB[1] * B);
+		V3 d = Q - P;
+		if (dot(d, d) > radius * radius)
+			return;
+		if (wg.has[0] && in_wing_face(wg.e[0], B, A, Q))
+			return;
+		tri_sphere_point(m, P, Q, radius, center2);
+		return;
+	}
+	if (wBC[0] > 0.0f && wBC[1] > 0.0f && wABC[3] * wABC[0] <= 0.0f)
+	{
+		float den = 1.0f / wBC[2];
+		V3 P = den * (wBC[0] * B + wBC[1] * C);
+		V3 d = Q - P;
+		if (dot(d, d) > radius * radius)
+			return;
+		if (wg.has[1] && in_wing_face(wg.e[1], C, B, Q))
+			return;
+		tri_sphere_point(m, P, Q, radius, center2);
+		return;
+	}
+	if (wCA[0] > 0.0f && wCA[1] > 0.0f && wABC[3] * wABC[1] <= 0.0f)
+	{
+		float den = 1.0f / wCA[2];
+		V3 P = den * (wCA[0] * C + wCA[1] * A);
+		V3 d = Q - P;
+		if (dot(d, d) > radius * radius)
+			return;
+		if (wg.has[2] && in_wing_face(wg.e[2], A, C, Q))
+			return;
+		tri_sphere_point(m, P, Q, radius, center2);
+		return;
+	}
+	// face region
+	if (wABC[3] == 0.0f)
+		return;
+	float den = 1.0f / wABC[3];
+	V3 P = den * ((wABC[0] * A + wABC[1] * B) + wABC[2] * C);
+	tri_sphere_point(m, P, Q, radius, center2);
+}
+
+// b3UniqueCount (gjk_feature_pair.cpp): distinct values among the first n.
+__device__ __forceinline__ uint32_t unique_count(const uint32_t* v, uint32_t n)
+{
+	uint32_t u = 0;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		bool seen = false;
+		for (uint32_t j = 0; j < i; ++j)
+			seen = seen || v[j] == v[i];
+		u += seen ? 0u : 1u;
+	}
+	return u;
+}
+
+// The shape-1 edge of b3GetFeaturePair (gjk_feature_pair.cpp:20-236) when its
+// count1 is 2: false otherwise.
+__device__ bool feature_edge1(const GJKSimplexOut& sx, uint32_t& v1, uint32_t& v2)
+{
+	uint32_t n = sx.count;
+	if (n != 2 && n != 3)
+		return false;
+	uint32_t u1 = unique_count(sx.index1, n), u2 = unique_count(sx.index2, n);
+	if (n == 2)
+	{
+		// EE, then VE (count1 1), then EV
+		if ((u1 == 2 && u2 == 2) || (u1 != 1 && u2 == 1))
+		{
+			v1 = sx.index1[0];
+			v2 = sx.index1[1];
+			return true;
+		}
+		return false;
+	}
+	// EE and EF: the two distinct shape-1 indices
+	if (u1 == 2 && (u2 == 2 || u2 == 3))
+	{
+		v1 = sx.index1[0];
+		v2 = sx.index1[0] == sx.index1[1] ? sx.index1[2] : sx.index1[1];
+		return true;
+	}
+	return false;
+}
+
+// b3CollideTriangleAndCapsule (collide_triangle_capsule.cpp:104-278).
+__device__ void collide_triangle_capsule(DevManifold& m, const DevScene& S, uint32_t fix1, const XF& xf1,
+	const ShapeP& t1, const TriWings& wg, const XF& xf2, const ShapeP& k2)
+{
+	float r1 = tri_radius(t1), r2 = cap_radius(k2);
+	float totalRadius = r1 + r2;
+	GProxy p1;
+	p1.gv = nullptr;
+	p1.lv[0] = tri_v1(t1);
+	p1.lv[1] = tri_v2(t1);
+	p1.lv[2] = tri_v3(t1);
+	p1.count = 3;
+	p1.radius = r1;
+	GProxy p2;
+	p2.gv = nullptr;
+	p2.lv[0] = cap_v1(k2);
+	p2.lv[1] = cap_v2(k2);
+	p2.count = 2;
+	p2.radius = r2;
+	GJKSimplexOut sx;
+	GJKOut q = gjk(xf1, p1, xf2, p2, false, &sx);
+	if (q.distance > totalRadius)
+		return;
+	HullRef h1 = tri_ref(S, fix1);
+	V3 v1 = cap_v1(k2), v2 = cap_v2(k2);
+	if (q.distance > 0.0f)
+	{
+		V3 c1 = q.point1, c2 = q.point2;
+		float d = q.distance;
+		V3 N1 = (c2 - c1) / d;
+		V3 localN1 = rotc(xf1.q, N1);
+		uint32_t index1 = hull_support_face(h1, localN1);
+		V3 localFaceN1 = hp(h1, index1).n;
+		const float kTol = 0.005f;
+		V3 N = cross(localN1, localFaceN1);
+		float L = dot(N, N);
+		if (L < kTol * kTol)
+		{
+			hull_capsule_face_contact(m, xf1, h1, index1, r1, xf2, v1, v2, r2);
+			if (m.pointCount == 2)
+				return;
+		}
+		uint32_t e1, e2;
+		if ((wg.has[0] || wg.has[1] || wg.has[2]) && feature_edge1(sx, e1, e2))
+		{
+			V3 vtx[3] = {tri_v1(t1), tri_v2(t1), tri_v3(t1)};
+			int edgeIndex = -1;
+			for (uint32_t i = 0; i < 3 && edgeIndex < 0; ++i)
+			{
+				uint32_t j = i + 1 < 3 ? i + 1 : 0;
+				if ((e1 == i && e2 == j) || (e2 == i && e1 == j))
+					edgeIndex = (int)i;
+			}
+			if (edgeIndex >= 0 && wg.has[edgeIndex])
+			{
+				uint32_t ev1 = (uint32_t)edgeIndex;
+				uint32_t ev2 = ev1 + 1 < 3 ? ev1 + 1 : 0;
+				V3 Q = xmult(xf1, c2);
+				V3 A = wg.e[edgeIndex];
+				V3 B = vtx[ev2];
+				V3 C = vtx[ev1];
+				float w[4];
+				barycentric_triangle(w, A, B, C, Q);
+				// In the adjacent face's region: no edge point (the manifold
+				// keeps what the face-contact attempt left in it).
+				if (w[0] > 0.0f && w[1] > 0.0f && w[2] > 0.0f)
+					return;
+				V3 center = ((A + B) + C) / 3.0f;
+				PL plane = hp(h1, 0);
+				float distance = pdist(center, plane);
+				const float kCoplanarTol = 0.005f;
+				if (distance > -kCoplanarTol && distance < kCoplanarTol)
+				{
+					V3 n = plane.n;
+					if (dot(n, localN1) < 0.0f)
+						n = -n;
+					V3 nc2 = c1 + d * rot(xf1.q, n);
+					localN1 = n;
+					c2 = nc2;
+				}
+			}
+		}
+		m.pointCount = 1;
+		set_point(m.points[0], localN1, xmult(xf1, c1), xmult(xf2, c2));
+		set_id0(m.points[0]);
+		return;
+	}
+	XF xf = xmult(xf1, xf2);
+	V3 lv1 = xmul(xf, v1), lv2 = xmul(xf, v2);
+	uint32_t faceIndex;
+	float faceSep;
+	query_face_hull_capsule(h1, lv1, lv2, faceIndex, faceSep);
+	if (faceSep > totalRadius)
+		return;
+	uint32_t edgeIndex;
+	float edgeSep;
+	query_edge_hull_capsule(h1, lv1, lv2, edgeIndex, edgeSep);
+	if (edgeSep > totalRadius)
+		return;
+	const float kRelEdgeTol = 0.90f;
+	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
+	if (edgeSep > kRelEdgeTol * faceSep + kAbsTol)
+		hull_capsule_edge_contact(m, xf1, h1, edgeIndex, xf2, v1, v2);
+	else
+		hull_capsule_face_contact(m, xf1, h1, faceIndex, r1, xf2, v1, v2, r2);
+}
+
 __device__ GProxy shape_proxy(const DevScene& S, const ShapeP& s)
 {
 	GProxy p;
@@ -484,6 +763,10 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 			collide_hull_sphere(m, a.S, xfA, sa, xfB, sb);
 		else if (BUCKET == BK_HULL_CAPSULE)
 			collide_hull_capsule(m, a.S, xfA, sa, xfB, sb);
+		else if (BUCKET == BK_TRIANGLE_SPHERE)
+			collide_triangle_sphere(m, xfA, sa, load_wings(a.S, fa), xfB, sb);
+		else if (BUCKET == BK_TRIANGLE_CAPSULE)
+			collide_triangle_capsule(m, a.S, fa, xfA, sa, load_wings(a.S, fa), xfB, sb);
 		finish_convex(a, c, m);
 		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
@@ -543,8 +826,8 @@ __global__ void k_inactive(NPArgs a)
 void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
 	const Tune& tune, cudaStream_t s)
 {
-	static const uint32_t buckets[B3G_CONVEX_KERNELS] = {BK_SPHERES, BK_CAPSULE_SPHERE, BK_CAPSULES, BK_HULL_SPHERE,
-		BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
+	static const uint32_t buckets[B3G_CONVEX_KERNELS] = {BK_SPHERES, BK_CAPSULE_SPHERE, BK_CAPSULES,
+		BK_TRIANGLE_SPHERE, BK_TRIANGLE_CAPSULE, BK_HULL_SPHERE, BK_HULL_CAPSULE, BK_SENSOR, BK_INACTIVE};
 	const uint32_t bk = buckets[k];
 	NPArgs a = base;
 	a.list = lists + (size_t)bk * cap;
@@ -562,12 +845,18 @@ void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const u
 		k_convex<BK_CAPSULES><<<blocks, 128, 0, s>>>(a);
 		break;
 	case 3:
-		k_convex<BK_HULL_SPHERE><<<blocks, 128, 0, s>>>(a);
+		k_convex<BK_TRIANGLE_SPHERE><<<blocks, 128, 0, s>>>(a);
 		break;
 	case 4:
-		k_convex<BK_HULL_CAPSULE><<<blocks, 128, 0, s>>>(a);
+		k_convex<BK_TRIANGLE_CAPSULE><<<blocks, 128, 0, s>>>(a);
 		break;
 	case 5:
+		k_convex<BK_HULL_SPHERE><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 6:
+		k_convex<BK_HULL_CAPSULE><<<blocks, 128, 0, s>>>(a);
+		break;
+	case 7:
 		k_sensor<<<blocks, 128, 0, s>>>(a);
 		break;
 	default:

@@ -683,9 +683,142 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 	}
 }
 
+// b3CollideHullAndTriangle (collide_hull_triangle.cpp:24-124) after the
+// hull-hull SAT: points on a triangle edge that has a coplanar wing take the
+// triangle's face normal (oriented from the hull to the triangle) so bodies
+// slide over mesh edges. Lane 0 only.
+__device__ void triangle_wing_normals(DevManifold& m, const DevScene& S, uint32_t fixT, const XF& xf1,
+	const HullRef& h1, const XF& xf2, const HullRef& h2)
+{
+	float4 w4[3];
+	for (int k = 0; k < 3; ++k)
+		w4[k] = S.fixWing[3 * (size_t)fixT + k];
+	PL plane2 = pmul(xf2, hp(h2, 0));
+	V3 centroid1 = xmul(xf1, h1.centroid);
+	V3 centroid2 = xmul(xf2, h2.centroid);
+	for (uint32_t i = 0; i < m.pointCount; ++i)
+	{
+		DevPoint& mp = m.points[i];
+		uint32_t inEdge2 = mp.key[2], outEdge2 = mp.key[3];
+		uint32_t e2;
+		if (mp.edgeContact)
+			e2 = inEdge2;
+		else
+		{
+			e2 = inEdge2 == B3G_NULL_EDGE ? outEdge2 : inEdge2;
+			if (e2 == B3G_NULL_EDGE)
+				continue;
+		}
+		uint32_t edgeIndex = e2 >> 1; // half-edges 2k, 2k + 1 lie on triangle edge k
+		if (edgeIndex > 2 || w4[edgeIndex].w == 0.0f)
+			continue;
+		uint32_t ev1 = edgeIndex;
+		uint32_t ev2 = edgeIndex + 1 < 3 ? edgeIndex + 1 : 0;
+		V3 A = V3{w4[edgeIndex].x, w4[edgeIndex].y, w4[edgeIndex].z};
+		V3 B = hv(h2, ev2);
+		V3 C = hv(h2, ev1);
+		V3 center = ((A + B) + C) / 3.0f;
+		float distance = pdist(center, hp(h2, 0));
+		const float kCoplanarTol = 0.005f;
+		if (distance > -kCoplanarTol && distance < kCoplanarTol)
+		{
+			V3 localN1 = V3{mp.n[0], mp.n[1], mp.n[2]};
+			V3 localC1 = V3{mp.p1[0], mp.p1[1], mp.p1[2]};
+			V3 localC2 = V3{mp.p2[0], mp.p2[1], mp.p2[2]};
+			V3 n1 = rot(xf1.q, localN1);
+			V3 c1 = xmul(xf1, localC1);
+			V3 c2 = xmul(xf2, localC2);
+			float sep = dot(c2 - c1, n1);
+			V3 n = plane2.n;
+			if (dot(n, centroid2 - centroid1) < 0.0f)
+				n = -n;
+			V3 nc1 = c2 - sep * n;
+			V3 ln = rotc(xf1.q, n);
+			V3 lp = xmult(xf1, nc1);
+			mp.n[0] = ln.x, mp.n[1] = ln.y, mp.n[2] = ln.z;
+			mp.p1[0] = lp.x, mp.p1[1] = lp.y, mp.p1[2] = lp.z;
+		}
+	}
+}
+
+// Hull (A) against triangle (B): one warp per contact, the full SAT of
+// b3CollideHulls without a feature cache (b3HullAndTriangleContact keeps
+// none), on the triangle's two-faced hull.
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_hull_triangle(NPArgs a, uint32_t maxUE)
+{
+	extern __shared__ float4 smem[];
+	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * W + warp; t < n; t += gridDim.x * W)
+	{
+		uint32_t c = a.list[t];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		HullCtx H;
+		H.xf1 = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, a.S.fixBody[fa]);
+		H.xf2 = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, a.S.fixBody[fb]);
+		H.h1 = hull_ref(a.S, a.S.fixHull[fa]);
+		H.h2 = tri_ref(a.S, fb);
+		H.r1 = a.S.fixParams[3 * fa].x;
+		H.r2 = a.S.fixParams[3 * fb + 2].y;
+		H.status = a.status;
+		H.recs = recs;
+		H.maxUE = maxUE;
+		DevManifold& m = a.man[c];
+		if (lane == 0)
+			man_clear(m);
+		__syncwarp();
+		collide_hulls_nocache(m, H, lane);
+		__syncwarp();
+		if (lane == 0)
+		{
+			triangle_wing_normals(m, a.S, fb, H.xf1, H.h1, H.xf2, H.h2);
+			finish_convex(a, c, m);
+			a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+		}
+		__syncwarp();
+	}
+}
+
 } // namespace
 
 void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s);
+size_t hull_sat_smem(int warps, uint32_t maxUE);
+
+// Hull-triangle contacts (bucket BK_HULL_TRIANGLE), with the SAT kernel's
+// warps per block.
+void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE,
+	const Tune& tune, cudaStream_t s)
+{
+	NPArgs a = base;
+	a.list = list;
+	a.listCount = count;
+	uint32_t ue = maxUE > 3 ? maxUE : 3;
+	const int bps = (int)tune.v[B3G_TUNE_SAT_BLOCKS];
+	size_t smem;
+	switch (tune.v[B3G_TUNE_SAT_WARPS])
+	{
+	case 2:
+		smem = hull_sat_smem(2, ue);
+		if (smem > 48 * 1024)
+			cudaFuncSetAttribute(k_hull_triangle<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		k_hull_triangle<2><<<persistent_blocks(bps), 64, smem, s>>>(a, ue);
+		break;
+	case 8:
+		smem = hull_sat_smem(8, ue);
+		if (smem > 48 * 1024)
+			cudaFuncSetAttribute(k_hull_triangle<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		k_hull_triangle<8><<<persistent_blocks(bps), 256, smem, s>>>(a, ue);
+		break;
+	default:
+		smem = hull_sat_smem(4, ue);
+		if (smem > 48 * 1024)
+			cudaFuncSetAttribute(k_hull_triangle<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		k_hull_triangle<4><<<persistent_blocks(bps), 128, smem, s>>>(a, ue);
+		break;
+	}
+}
 
 template <int W>
 void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)

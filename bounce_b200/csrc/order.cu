@@ -492,9 +492,11 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 				launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 				launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
 					c->maxUniqueEdges, c->tune, s);
+				launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap,
+					B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE, c->maxUniqueEdges, c->tune, s);
 				k_wake_events<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, cap, B.wakeList,
 					B.counters + CTR_WAKE_ACTIVATED, 0);
-				launches += 7 + 2 + 1;
+				launches += B3G_CONVEX_KERNELS + 2 + 1 + 1;
 			}
 		}
 		cudaMemsetAsync(B.counters + CTR_BUCKET0, 0, sizeof(uint32_t) * BK_COUNT, s);

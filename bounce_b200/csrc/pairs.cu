@@ -219,6 +219,8 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
 		c->maxUniqueEdges, c->tune, s);
+	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
+		c->maxUniqueEdges, c->tune, s);
 	prof_mark(c, PM_HULLS, s);
 }
 

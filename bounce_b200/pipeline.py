@@ -59,6 +59,11 @@ class CollisionPipeline:
                 N.ptr(scene.fix_params, f32), N.ptr(scene.fix_flags, u32), None,
             )
         )
+        wings = getattr(scene, "tri_wings", None)
+        if wings is not None and len(wings):
+            fx = np.ascontiguousarray(scene.tri_fixtures, np.uint32)
+            w = np.ascontiguousarray(wings, np.float32).reshape(-1)
+            self._check(self.lib.b3g_set_triangle_wings(self.ctx, len(fx), N.ptr(fx, u32), N.ptr(w, f32)))
 
     def _check(self, rc):
         if rc < 0:

@@ -433,3 +433,81 @@ class KinematicDriver:
         out[:, 7:10] = self.c
         out[:, 10:14] = self.q
         return np.ascontiguousarray(out.reshape(-1))
+
+
+def terrain_triangles(nx, nz, spacing, seed, amplitude=0.5):
+    """Triangles of a height-field grid of nx x nz vertices (two per cell) and
+    the edge wings of each (the third vertex of the triangle across each
+    edge, as b3Mesh adjacency gives them): returns (params (n, 12), wings (n, 12))."""
+    rng = np.random.default_rng(seed)
+    xs = (np.arange(nx) - (nx - 1) / 2.0) * spacing
+    zs = (np.arange(nz) - (nz - 1) / 2.0) * spacing
+    ph = rng.uniform(0, 2 * np.pi, 4)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    Y = amplitude * (np.sin(0.7 * X + ph[0]) * np.sin(0.5 * Z + ph[1]) + 0.5 * np.sin(1.3 * X + ph[2]) * np.sin(0.9 * Z + ph[3]))
+    V = np.stack([X, Y, Z], axis=-1).astype(F).reshape(-1, 3)
+    idx = lambda i, j: i * nz + j
+    tris = []
+    for i in range(nx - 1):
+        for j in range(nz - 1):
+            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
+            # counter-clockwise seen from +y
+            tris.append((a, d, c))
+            tris.append((a, c, b))
+    tris = np.array(tris, np.int64)
+    edge_owner = {}
+    for t, (a, b, c) in enumerate(tris):
+        for k, (u, v) in enumerate(((a, b), (b, c), (c, a))):
+            edge_owner.setdefault((min(u, v), max(u, v)), []).append((t, k))
+    params = np.zeros((len(tris), 12), F)
+    wings = np.zeros((len(tris), 12), F)
+    for t, (a, b, c) in enumerate(tris):
+        params[t, 0:3], params[t, 3:6], params[t, 6:9] = V[a], V[b], V[c]
+        for k, (u, v) in enumerate(((a, b), (b, c), (c, a))):
+            for (t2, _) in edge_owner[(min(u, v), max(u, v))]:
+                if t2 != t:
+                    third = [x for x in tris[t2] if x != u and x != v][0]
+                    wings[t, 3 * k:3 * k + 3] = V[third]
+                    wings[t, 9 + k] = 1.0
+    return params, wings
+
+
+def terrain_scene(seed=3, n=800, grid=12, spacing=1.5, height=4.0, static_frac=0.0):
+    """Mixed moving bodies (spheres, capsules, hulls) above a static terrain of
+    triangle fixtures with edge wings (scene.tri_wings: fixture -> 12 floats)."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    g = s.add_body(0, N.BODY_STATIC, (0, 0, 0), (0, 0, 0, 1))
+    params, wings = terrain_triangles(grid, grid, spacing, seed)
+    first = len(s.fix_type)
+    for p in params:
+        s.add_fixture(g, N.SHAPE_TRIANGLE, list(p[:9]) + [0.0])
+    half = 0.5 * spacing * (grid - 1)
+    pos = np.stack([rng.uniform(-half, half, n), rng.uniform(-0.5, height, n), rng.uniform(-half, half, n)],
+                   axis=-1).astype(F)
+    quat = random_quats(rng, n)
+    lin = rng.normal(0, 1, (n, 3)).astype(F)
+    lin[:, 1] -= 1.0
+    ang = rng.normal(0, 1, (n, 3)).astype(F)
+    for i in range(n):
+        b = s.add_body(0, N.BODY_DYNAMIC, pos[i], quat[i], lin[i], ang[i])
+        k = rng.random()
+        if k < 0.35:
+            s.add_fixture(b, N.SHAPE_SPHERE, [0, 0, 0, rng.uniform(0.2, 0.6)])
+        elif k < 0.65:
+            r = rng.uniform(0.1, 0.4)
+            h = rng.uniform(0.2, 0.7)
+            s.add_fixture(b, N.SHAPE_CAPSULE, [0, -h, 0, 0, h, 0, r])
+        else:
+            while True:
+                m = int(rng.integers(8, 20))
+                axes = rng.uniform(0.3, 0.8, 3)
+                try:
+                    hh = s.hulls.add_points(ellipsoid_points(rng, m, axes))
+                    break
+                except ValueError:
+                    continue
+            s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=hh)
+    s.tri_fixtures = np.arange(first, first + len(params), dtype=np.uint32)
+    s.tri_wings = wings
+    return s

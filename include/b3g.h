@@ -120,7 +120,8 @@ int b3g_set_bodies(b3g_ctx* ctx, uint32_t body_count, const uint32_t* world,
 /* Fixtures (one broadphase proxy each). params: 12 floats per fixture:
  *   sphere   p[0..2] center, p[3] radius           (sphere_shape.h)
  *   capsule  p[0..2] vertex1, p[3..5] vertex2, p[6] radius (capsule_shape.h)
- *   triangle p[0..8] vertices, p[9] radius         (triangle_shape.h)
+ *   triangle p[0..8] vertices, p[9] radius         (triangle_shape.h; wings:
+ *            b3g_set_triangle_wings)
  *   hull     p[0] radius (B3_HULL_RADIUS = 0)       (hull_shape.cpp:28)
  * proxy_key orders the two fixtures of a pair exactly as the reference's
  * proxy ids do (b3BroadPhase::Report keeps (min, max), broad_phase.cpp:341-342);
@@ -132,6 +133,14 @@ int b3g_set_bodies(b3g_ctx* ctx, uint32_t body_count, const uint32_t* world,
 int b3g_set_fixtures(b3g_ctx* ctx, uint32_t fixture_count, const uint32_t* body,
 	const uint32_t* shape_type, const uint32_t* hull, const float* params,
 	const uint32_t* flags, const uint32_t* proxy_key);
+
+/* Edge wings of triangle fixtures (b3TriangleShape::m_e1Vertex..m_e3Vertex and
+ * m_hasE1Vertex..m_hasE3Vertex, triangle_shape.h:45-48): for fixture
+ * fixture[i], 12 floats: the wing vertices of edges 1-2, 2-3 and 3-1 (3 each,
+ * shape frame) and three flags (non-zero: the edge has a wing). Fixtures
+ * without a call have no wings. Needs b3g_set_fixtures first; a later
+ * b3g_set_fixtures clears them. */
+int b3g_set_triangle_wings(b3g_ctx* ctx, uint32_t count, const uint32_t* fixture, const float* wings);
 
 /* Awake flags per body. Replaces: b3Body::SetAwake (body.h:588-603). A pass
  * applies its own wake-ups to these flags (see b3g_fetch_awake), so the host
@@ -296,11 +305,12 @@ const char* b3g_stage_name(uint32_t stage);
  * tuning table holds B3G_TUNE_COUNT entries:
  *   [B3G_TUNE_CONVEX + k]  blocks per SM of the thread-per-pair kernel of
  *                          bucket k: spheres, capsule-sphere, capsules,
- *                          hull-sphere, hull-capsule, sensor, inactive
- *                          (128 threads per block)
+ *                          triangle-sphere, triangle-capsule, hull-sphere,
+ *                          hull-capsule, sensor, inactive (128 threads per block)
  *   [B3G_TUNE_PROBE]       blocks per SM of the hull feature-cache probe
- *   [B3G_TUNE_SAT_WARPS]   warps per block of the hull-hull SAT kernel (2, 4, 8)
- *   [B3G_TUNE_SAT_BLOCKS]  blocks per SM of the hull-hull SAT kernel
+ *   [B3G_TUNE_SAT_WARPS]   warps per block of the hull-hull and hull-triangle
+ *                          SAT kernels (2, 4, 8)
+ *   [B3G_TUNE_SAT_BLOCKS]  blocks per SM of those kernels
  *   [B3G_TUNE_TRAVERSE]    threads per block of the LBVH traversal (64, 128, 256)
  * b3g_autotune picks each entry by timing the kernel it drives on the last
  * pass's data (the kernels re-run on the same inputs write the same outputs,
@@ -309,11 +319,11 @@ const char* b3g_stage_name(uint32_t stage);
  * b3g_set_tuning / b3g_get_tuning set and read the table directly;
  * set_tuning rejects values outside the candidate sets with B3G_E_INVALID. */
 #define B3G_TUNE_CONVEX 0
-#define B3G_TUNE_PROBE 7
-#define B3G_TUNE_SAT_WARPS 8
-#define B3G_TUNE_SAT_BLOCKS 9
-#define B3G_TUNE_TRAVERSE 10
-#define B3G_TUNE_COUNT 11
+#define B3G_TUNE_PROBE 9
+#define B3G_TUNE_SAT_WARPS 10
+#define B3G_TUNE_SAT_BLOCKS 11
+#define B3G_TUNE_TRAVERSE 12
+#define B3G_TUNE_COUNT 13
 int b3g_autotune(b3g_ctx* ctx, uint32_t reps, void* stream, uint32_t* out);
 int b3g_set_tuning(b3g_ctx* ctx, const uint32_t* table);
 int b3g_get_tuning(b3g_ctx* ctx, uint32_t* table);

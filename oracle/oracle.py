@@ -79,6 +79,7 @@ def lib(precision=32):
         "refw_set_sweeps": ([vp, f32p], None),
         "refw_set_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
         "refw_get_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
+        "refw_set_triangle_wings": ([vp, ctypes.c_uint32, u32p, f32p], None),
         "refw_pass_sleep": ([vp, ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint8), f64p], None),
         "refw_set_convex_cache": ([ctypes.c_uint32], None),
         "refw_first_pass": ([vp, f64p], None),
@@ -95,6 +96,11 @@ def lib(precision=32):
         "ref_collide": (
             [vp, ctypes.c_uint32, f32p, ctypes.c_uint32, ctypes.c_uint32, f32p, ctypes.c_uint32, f32p, f32p, f32p, f32p,
              u32p, vp],
+            ctypes.c_int,
+        ),
+        "ref_collide_wings": (
+            [vp, ctypes.c_uint32, f32p, ctypes.c_uint32, ctypes.c_uint32, f32p, ctypes.c_uint32, f32p, f32p, f32p, f32p,
+             u32p, vp, f32p, f32p],
             ctypes.c_int,
         ),
         "ref_sweep_xf0": ([f32p, f32p, f32p, f32p, f32p], None),
@@ -149,6 +155,9 @@ class RefWorld:
             1 if warm_starting else 0,
         )
         self.times = np.zeros(2)
+        wings = getattr(scene, "tri_wings", None)
+        if wings is not None and len(wings):
+            self.set_triangle_wings(scene.tri_fixtures, wings)
 
     def close(self):
         if self.w:
@@ -198,6 +207,11 @@ class RefWorld:
         self.L.refw_pass_sleep(self.w, _p(m, ctypes.c_uint8), _p(a, ctypes.c_uint8), _p(t, ctypes.c_double))
         self.times = t
         return t
+
+    def set_triangle_wings(self, fixtures, wings):
+        f = np.ascontiguousarray(fixtures, np.uint32)
+        w = np.ascontiguousarray(wings, np.float32).reshape(-1)
+        self.L.refw_set_triangle_wings(self.w, len(f), _p(f, ctypes.c_uint32), _p(w, ctypes.c_float))
 
     def awake(self):
         out = np.zeros(len(self.bodies17()) // 17, np.uint8)
@@ -290,8 +304,10 @@ def set_convex_cache(on, precision=32):
     lib(precision).refw_set_convex_cache(1 if on else 0)
 
 
-def collide(hulls, typeA, pA, hullA, typeB, pB, hullB, xfA, xfB, xf0A=None, xf0B=None, cache=None, precision=32):
-    """One b3Collide* call of the reference (ref_collide in ref_harness.cpp)."""
+def collide(hulls, typeA, pA, hullA, typeB, pB, hullB, xfA, xfB, xf0A=None, xf0B=None, cache=None, precision=32,
+            wingsA=None, wingsB=None):
+    """One b3Collide* call of the reference (ref_collide in ref_harness.cpp);
+    wingsA / wingsB: 12 floats of triangle edge wings."""
     L = lib(precision)
     f = lambda a: np.ascontiguousarray(a, np.float32)
     pa, pb = f(np.pad(np.asarray(pA, np.float32), (0, 12 - len(pA)))), f(np.pad(np.asarray(pB, np.float32), (0, 12 - len(pB))))
@@ -300,10 +316,13 @@ def collide(hulls, typeA, pA, hullA, typeB, pB, hullB, xfA, xfB, xf0A=None, xf0B
     x0b = f(xf0B if xf0B is not None else xfB)
     c = np.ascontiguousarray(cache if cache is not None else np.array([0, 1, 0, 0]), np.uint32)
     out = np.zeros(1, DMANIFOLD)
-    rc = L.ref_collide(
+    wa = None if wingsA is None else f(wingsA)
+    wb = None if wingsB is None else f(wingsB)
+    rc = L.ref_collide_wings(
         hulls.h, typeA, _p(pa, ctypes.c_float), hullA, typeB, _p(pb, ctypes.c_float), hullB, _p(xa, ctypes.c_float),
         _p(xb, ctypes.c_float), _p(x0a, ctypes.c_float), _p(x0b, ctypes.c_float), _p(c, ctypes.c_uint32),
-        ctypes.c_void_p(out.ctypes.data),
+        ctypes.c_void_p(out.ctypes.data), None if wa is None else _p(wa, ctypes.c_float),
+        None if wb is None else _p(wb, ctypes.c_float),
     )
     if rc != 0:
         raise ValueError("unsupported shape pair")

@@ -190,6 +190,17 @@ struct ShapeStore
 	b3HullShape hull;
 };
 
+// Wings of a triangle shape: 12 floats (e1, e2, e3 vertices, three flags).
+static void SetWings(b3TriangleShape& t, const float* w)
+{
+	t.m_e1Vertex.Set(w[0], w[1], w[2]);
+	t.m_e2Vertex.Set(w[3], w[4], w[5]);
+	t.m_e3Vertex.Set(w[6], w[7], w[8]);
+	t.m_hasE1Vertex = w[9] != 0.0f;
+	t.m_hasE2Vertex = w[10] != 0.0f;
+	t.m_hasE3Vertex = w[11] != 0.0f;
+}
+
 static const b3Shape* MakeShape(ShapeStore& s, uint32_t type, const float* p, uint32_t hullIndex, const HullPool* pool)
 {
 	switch (type)
@@ -408,6 +419,18 @@ REF_API void refw_pass_sleep(void* p, const uint8_t* moved, const uint8_t* awake
 	times[1] = t2 - t1;
 }
 
+// Edge wings of triangle fixtures (12 floats per listed fixture).
+REF_API void refw_set_triangle_wings(void* p, uint32_t n, const uint32_t* fixture, const float* wings)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		b3Fixture* f = w->fixtures[fixture[i]];
+		if (f->GetType() == b3Shape::e_triangle)
+			SetWings(*(b3TriangleShape*)f->GetShape(), wings + 12 * (size_t)i);
+	}
+}
+
 // Awake flags per body (1 awake, 0 asleep).
 REF_API void refw_get_awake(void* p, uint8_t* out)
 {
@@ -573,14 +596,31 @@ static b3Transform MakeXf(const float* x)
 	return xf;
 }
 
+// As ref_collide, with edge wings for triangle shapes (12 floats each, or NULL).
+REF_API int ref_collide_wings(void* hullPool, uint32_t typeA, const float* pA, uint32_t hullA,
+	uint32_t typeB, const float* pB, uint32_t hullB, const float* xfA, const float* xfB,
+	const float* xf0A, const float* xf0B, uint32_t* cache4, void* out, const float* wingsA, const float* wingsB);
+
 REF_API int ref_collide(void* hullPool, uint32_t typeA, const float* pA, uint32_t hullA,
 	uint32_t typeB, const float* pB, uint32_t hullB, const float* xfA, const float* xfB,
 	const float* xf0A, const float* xf0B, uint32_t* cache4, void* out)
+{
+	return ref_collide_wings(hullPool, typeA, pA, hullA, typeB, pB, hullB, xfA, xfB, xf0A, xf0B, cache4, out,
+		nullptr, nullptr);
+}
+
+REF_API int ref_collide_wings(void* hullPool, uint32_t typeA, const float* pA, uint32_t hullA,
+	uint32_t typeB, const float* pB, uint32_t hullB, const float* xfA, const float* xfB,
+	const float* xf0A, const float* xf0B, uint32_t* cache4, void* out, const float* wingsA, const float* wingsB)
 {
 	const HullPool* pool = (const HullPool*)hullPool;
 	ShapeStore sa, sb;
 	const b3Shape* A = MakeShape(sa, typeA, pA, hullA, pool);
 	const b3Shape* B = MakeShape(sb, typeB, pB, hullB, pool);
+	if (typeA == 2 && wingsA)
+		SetWings(sa.triangle, wingsA);
+	if (typeB == 2 && wingsB)
+		SetWings(sb.triangle, wingsB);
 	b3Transform XA = MakeXf(xfA), XB = MakeXf(xfB);
 	b3Manifold m;
 	m.Initialize();

@@ -183,8 +183,91 @@ def collide_poses():
     print(path, os.path.getsize(path))
 
 
+def triangle_poses():
+    """Direct b3Collide* calls of the triangle pairs (triangle-sphere,
+    triangle-capsule, hull-triangle) on seeded poses around one triangle,
+    without wings, with coplanar wings on every edge, and with one coplanar,
+    one bent and one missing wing."""
+    sc = S.Scene()
+    rng = np.random.default_rng(41)
+    small = sc.hulls.add_box(0.4, 0.4, 0.4)
+    ell = sc.hulls.add_points(S.ellipsoid_points(rng, 16, np.array([0.6, 0.35, 0.45])))
+    ha = sc.hulls.arrays()
+    hulls = O.RefHulls(ha, 32)
+    tri = [-1.5, 0, 1, 1.5, 0, 1, 0, 0, -1.6, 0.0]
+    shapes = {
+        "triangle": (2, tri, 0),
+        "sphere": (0, [0, 0, 0, 0.5], 0),
+        "capsule": (1, [0, -0.6, 0, 0, 0.6, 0, 0.3], 0),
+        "box": (3, [0.0], small),
+        "ellipsoid": (3, [0.0], ell),
+    }
+    z = [0.0] * 3
+    wing_sets = [
+        np.zeros(12, np.float32),
+        np.array([0, 0, 3.5, 2.5, 0, -1.5, -2.5, 0, -1.5, 1, 1, 1], np.float32),
+        np.array([0, 0, 3.5, 2.5, -0.7, -1.5] + z + [1, 1, 0], np.float32),
+    ]
+    kinds = [("triangle", "sphere"), ("triangle", "capsule"), ("box", "triangle"), ("ellipsoid", "triangle")]
+    recs = []
+    for a, b in kinds:
+        for w, wings in enumerate(wing_sets):
+            verts = np.array(tri[:9], np.float32).reshape(3, 3)
+            for i in range(60):
+                qa, qb = S.random_quats(rng, 2)
+                pa = rng.uniform(-0.3, 0.3, 3).astype(np.float32)
+                if i % 2:
+                    # near an edge: a point on it pushed out a little
+                    e = int(rng.integers(3))
+                    t = rng.uniform(0.1, 0.9)
+                    on = verts[e] + t * (verts[(e + 1) % 3] - verts[e])
+                    out = on - verts.mean(axis=0)
+                    local = on + rng.uniform(0.0, 0.5) * out / np.linalg.norm(out)
+                    local[1] = rng.uniform(-0.3, 0.55)
+                else:
+                    local = np.array([rng.uniform(-1.8, 1.8), rng.uniform(-0.4, 0.6), rng.uniform(-1.8, 1.4)])
+                local = local.astype(np.float32)
+                pb = (pa + S.quat_rotate(qa[None], local[None])[0]).astype(np.float32)
+                recs.append((a, b, np.concatenate([pa, qa]), np.concatenate([pb, qb]), wings))
+    out = {f"hull_{k}": v for k, v in ha.items()}
+    ta, tb, xa, xb, wa, wb, dumps = [], [], [], [], [], [], []
+    for a, b, xfa, xfb, wings in recs:
+        A, B = shapes[a], shapes[b]
+        m = O.collide(hulls, A[0], A[1], A[2], B[0], B[1], B[2], xfa, xfb, xfa, xfb, None, 32,
+                      wingsA=wings if A[0] == 2 else None, wingsB=wings if B[0] == 2 else None)
+        ta.append([A[0], A[2]])
+        tb.append([B[0], B[2]])
+        xa.append(xfa)
+        xb.append(xfb)
+        wa.append(wings if A[0] == 2 else np.zeros(12, np.float32))
+        wb.append(wings if B[0] == 2 else np.zeros(12, np.float32))
+        dumps.append(m)
+    pad = lambda v: v + [0] * (12 - len(v))
+    out["shape_a"] = np.array([pad(shapes[r[0]][1]) for r in recs], np.float32)
+    out["shape_b"] = np.array([pad(shapes[r[1]][1]) for r in recs], np.float32)
+    out["type_a"] = np.array(ta, np.uint32)
+    out["type_b"] = np.array(tb, np.uint32)
+    out["xf_a"] = np.array(xa, np.float32)
+    out["xf_b"] = np.array(xb, np.float32)
+    out["wings_a"] = np.array(wa, np.float32)
+    out["wings_b"] = np.array(wb, np.float32)
+    d = np.array(dumps)
+    out["point_count"] = d["pointCount"].astype(np.uint32)
+    out["n"] = d["points"]["n"]
+    out["p1"] = d["points"]["p1"]
+    out["p2"] = d["points"]["p2"]
+    out["key"] = d["points"]["key"].astype(np.uint32)
+    path = os.path.join(HERE, "triangle_poses.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "points", int(out["point_count"].sum()))
+
+
 if __name__ == "__main__":
     assert O.available(32) and O.available(64), "build the oracle first: make -C oracle"
-    for name, build in SCENES.items():
-        make(name, build)
-    collide_poses()
+    only = sys.argv[1:]
+    if not only:
+        for name, build in SCENES.items():
+            make(name, build)
+        collide_poses()
+    if not only or "triangle_poses" in only:
+        triangle_poses()

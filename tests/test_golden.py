@@ -85,3 +85,23 @@ def test_fp64_rerun_agrees_with_fp32_within_tolerance():
                     e = np.abs(d[f"p{p}_r32_p1"][ka, j] - d[f"p{p}_r64_p1"][kb, j]).max()
                     worst = max(worst, float(e))
             assert worst <= 1e-4, (name, p, worst)
+
+
+def test_reference_reproduces_triangle_poses(oracle_mod):
+    """The committed triangle-pair fixture (tests/golden/make_golden.py
+    triangle_poses) is what the reference computes: the pin for the GPU
+    triangle tests."""
+    O = oracle_mod
+    d = G.load("triangle_poses")
+    ha = {k: np.ascontiguousarray(d[f"hull_{k}"]) for k in ("desc", "verts", "edges", "faces", "planes", "centroids")}
+    hulls = O.RefHulls(ha, 32)
+    for i in range(len(d["point_count"])):
+        ta, tb = d["type_a"][i], d["type_b"][i]
+        m = O.collide(hulls, int(ta[0]), d["shape_a"][i], int(ta[1]), int(tb[0]), d["shape_b"][i], int(tb[1]),
+                      d["xf_a"][i], d["xf_b"][i], None, None, None, 32,
+                      wingsA=d["wings_a"][i] if ta[0] == 2 else None, wingsB=d["wings_b"][i] if tb[0] == 2 else None)
+        pc = int(m["pointCount"])
+        assert pc == d["point_count"][i], i
+        for f in ("n", "p1", "p2"):
+            assert np.array_equal(m["points"][f][:pc].astype(np.float32), d[f][i][:pc]), (i, f)
+        assert np.array_equal(m["points"]["key"][:pc], d["key"][i][:pc]), i

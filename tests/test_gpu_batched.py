@@ -71,14 +71,14 @@ def test_launch_shapes_do_not_change_results():
     high = CollisionPipeline(sc)
     tuned = CollisionPipeline(sc)
     t = base.tuning()
-    assert list(t) == [4] * 7 + [4, 4, 2, 128]
-    lo = np.array([1] * 7 + [1, 2, 1, 64], np.uint32)
-    hi = np.array([16] * 7 + [16, 8, 8, 256], np.uint32)
+    assert list(t) == [4] * 9 + [4, 4, 2, 128]
+    lo = np.array([1] * 9 + [1, 2, 1, 64], np.uint32)
+    hi = np.array([16] * 9 + [16, 8, 8, 256], np.uint32)
     low.set_tuning(lo)
     high.set_tuning(hi)
     assert np.array_equal(high.tuning(), hi)
     with pytest.raises(N.B3GError):
-        low.set_tuning(np.array([3] * 11, np.uint32))
+        low.set_tuning(np.array([3] * 13, np.uint32))
     chosen = None
     for k in range(6):
         if k:
