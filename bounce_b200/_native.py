@@ -97,6 +97,8 @@ EXPORTED = [
     "b3g_set_fixtures",
     "b3g_set_awake",
     "b3g_set_triangle_wings",
+    "b3g_set_meshes",
+    "b3g_mesh_wings",
     "b3g_collide",
     "b3g_get_counts",
     "b3g_fetch_contacts",
@@ -155,6 +157,8 @@ def load():
         "b3g_set_fixtures": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, u32p], ctypes.c_int),
         "b3g_set_awake": ([ctx, u8p], ctypes.c_int),
         "b3g_set_triangle_wings": ([ctx, ctypes.c_uint32, u32p, f32p], ctypes.c_int),
+        "b3g_set_meshes": ([ctx, ctypes.c_uint32, u32p, f32p, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_mesh_wings": ([ctx, ctypes.c_uint32, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_collide": ([ctx, vp, ctypes.c_int, vp], ctypes.c_int),
         "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
         "b3g_fetch_contacts": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),

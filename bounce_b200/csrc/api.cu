@@ -127,23 +127,41 @@ __global__ void k_triangle_hulls(DevScene S, uint32_t nf, float4* tri)
 	t[5] = make_float4(centroid.x, centroid.y, centroid.z, 0.0f);
 }
 
-__global__ void k_touch_flags(const DevManifold* man, const uint32_t* cstate, uint32_t n, uint32_t* flags)
+// Manifolds with points per contact: the first, and for a mesh contact its
+// other cluster manifolds.
+__global__ void k_touch_flags(const DevManifold* man, const DevManifold* extra, const uint32_t* cstate, uint32_t n,
+	uint32_t* flags)
 {
 	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
 	if (c >= n)
 		return;
-	flags[c] = (((cstate[c] >> 8) & 0xFFu) && man[c].pointCount > 0) ? 1u : 0u;
+	uint32_t mc = (cstate[c] >> 8) & 0xFFu;
+	uint32_t k = 0;
+	for (uint32_t j = 0; j < mc && j < 3; ++j)
+	{
+		const DevManifold& m = j == 0 ? man[c] : extra[2 * (size_t)c + j - 1];
+		k += m.pointCount > 0 ? 1u : 0u;
+	}
+	flags[c] = k;
 }
 
-__global__ void k_touch_scatter(const DevManifold* man, const uint32_t* flagsIn, const uint32_t* offsets,
-	uint32_t n, uint32_t* index, DevManifold* out)
+__global__ void k_touch_scatter(const DevManifold* man, const DevManifold* extra, const uint32_t* cstate,
+	const uint32_t* offsets, uint32_t n, uint32_t* index, DevManifold* out)
 {
 	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-	if (c >= n || !flagsIn[c])
+	if (c >= n)
 		return;
+	uint32_t mc = (cstate[c] >> 8) & 0xFFu;
 	uint32_t o = offsets[c];
-	index[o] = c;
-	out[o] = man[c];
+	for (uint32_t j = 0; j < mc && j < 3; ++j)
+	{
+		const DevManifold& m = j == 0 ? man[c] : extra[2 * (size_t)c + j - 1];
+		if (m.pointCount == 0)
+			continue;
+		index[o] = c;
+		out[o] = m;
+		++o;
+	}
 }
 
 } // namespace
@@ -294,6 +312,14 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->dFixTri = nullptr;
 	c->dFixWing = nullptr;
 	c->triSlots = 0;
+	c->nMeshes = 0;
+	c->dMeshes = nullptr;
+	c->dMeshVerts = nullptr;
+	c->dMeshTris = nullptr;
+	c->dMeshWings = nullptr;
+	c->dMeshNodes = nullptr;
+	c->dMeshFix = nullptr;
+	c->nMeshFix = 0;
 	c->capBodies = c->capFixtures = 0;
 	c->keysAreIndex = true;
 	for (int i = 0; i < B3G_STAGE_RING; ++i)
@@ -514,6 +540,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dFixWing);
 	dfree(c->dFixParams);
 	dfree(c->dFixBound);
+	dfree(c->dMeshFix);
+	free_mesh(c);
 	for (int i = 0; i < B3G_STAGE_RING; ++i)
 	{
 		if (c->stage[i].done)
@@ -690,15 +718,27 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	CK(cudaStreamSynchronize(c->stream));
 	destroy_graphs(c);
 	std::vector<uint32_t> key(nf);
+	std::vector<uint32_t> meshFix;
 	bool hasTriangles = false;
 	for (uint32_t i = 0; i < nf; ++i)
 	{
 		if (body[i] >= c->nBodies)
 			return fail(c, B3G_E_INVALID, "fixture %u: body %u out of range", i, body[i]);
-		if (shapeType[i] > B3G_SHAPE_HULL)
+		if (shapeType[i] > B3G_SHAPE_MESH)
 			return fail(c, B3G_E_INVALID, "fixture %u: shape type %u not supported", i, shapeType[i]);
 		if (shapeType[i] == B3G_SHAPE_TRIANGLE)
 			hasTriangles = true;
+		if (shapeType[i] == B3G_SHAPE_MESH)
+		{
+			if (hull[i] >= c->nMeshes)
+				return fail(c, B3G_E_INVALID, "fixture %u: mesh %u out of range", i, hull[i]);
+			if (c->hBodyType[body[i]] != B3G_BODY_STATIC)
+				return fail(c, B3G_E_INVALID, "fixture %u: a mesh needs a static body", i);
+			const float* p = params + 12 * (size_t)i;
+			if (p[0] == 0.0f || p[1] == 0.0f || p[2] == 0.0f)
+				return fail(c, B3G_E_INVALID, "fixture %u: zero mesh scale", i);
+			meshFix.push_back(i);
+		}
 		if (shapeType[i] == B3G_SHAPE_HULL && hull[i] >= c->nHulls)
 			return fail(c, B3G_E_INVALID, "fixture %u: hull %u out of range", i, hull[i]);
 		key[i] = proxyKey ? proxyKey[i] : i;
@@ -728,6 +768,11 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	for (uint32_t i = 0; i < nf; ++i)
 	{
 		const float* p = params + 12 * (size_t)i;
+		if (shapeType[i] == B3G_SHAPE_MESH)
+		{
+			bound[i] = make_float4(0.0f, 0.0f, 0.0f, INFINITY);
+			continue;
+		}
 		std::vector<double> pts;
 		double skin = 0.0;
 		switch (shapeType[i])
@@ -839,6 +884,12 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 		CK(cudaGetLastError());
 		CK(cudaDeviceSynchronize());
 	}
+	// Mesh fixtures (their proxies are built by k_mesh_fat).
+	dfree(c->dMeshFix);
+	c->nMeshFix = (uint32_t)meshFix.size();
+	CK(dalloc(&c->dMeshFix, meshFix.size()));
+	if (!meshFix.empty())
+		CK(cudaMemcpy(c->dMeshFix, meshFix.data(), sizeof(uint32_t) * meshFix.size(), cudaMemcpyHostToDevice));
 	c->creationPass = true;
 	c->havePass = false;
 	return B3G_OK;
@@ -1290,8 +1341,8 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
 	// pass_begin, sync, broadphase, diff + list order, bucket + convex kernels + 2 hull + hull-triangle,
 	// finalize + pass_end + settle
-	const uint32_t passLaunches =
-		1 + 2 + broadphase_launches(c) + pairs_diff_launches(c) + 1 + B3G_CONVEX_KERNELS + 2 + 1 + 3;
+	const uint32_t passLaunches = 1 + 2 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
+		pairs_diff_launches(c) + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
 		c->havePass && !c->creationPass && s != nullptr;
 	c->lastPassImpulses = c->impulsesLoaded;
@@ -1470,14 +1521,17 @@ extern "C" int b3g_fetch_touching(b3g_ctx* c, uint32_t* index, void* manifolds, 
 	Buffers& B = c->buf;
 	if (n == 0)
 		return 0;
-	uint32_t* flags = B.leafCount; // sized max(P, C)
-	k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], B.cstate[c->cur], n, flags);
-	CK(cudaMemcpyAsync(B.prevIndex, flags, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
-	scan_exclusive(flags, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
-	k_touch_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], (const uint32_t*)B.prevIndex, flags,
-		n, B.touchIndex, B.touchMan);
+	uint32_t* offsets = B.leafCount; // sized max(P, C)
+	const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
+	k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, offsets);
+	scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
 	uint32_t total = 0;
 	CK(cudaMemcpyAsync(&total, B.counters + CTR_TOUCH_OUT, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	if (total > c->cfg.max_contacts)
+		return fail(c, B3G_E_CAPACITY, "b3g_fetch_touching: %u manifolds exceed the output buffer", total);
+	k_touch_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], offsets, n,
+		B.touchIndex, B.touchMan);
 	CK(cudaStreamSynchronize(c->stream));
 	uint32_t m = std::min(total, capacity);
 	if (m)

@@ -27,7 +27,8 @@ enum Bucket : uint32_t
 	BK_HULL_CAPSULE,     // b3HullAndCapsuleContact
 	BK_HULL_TRIANGLE,    // b3HullAndTriangleContact
 	BK_HULLS,            // b3HullContact
-	BK_SENSOR,           // any pair with a sensor: b3Contact::TestOverlap path
+	BK_MESH,             // b3MeshContact subclasses (mesh-sphere, mesh-capsule, hull-mesh), sensors included
+	BK_SENSOR,           // any other pair with a sensor: b3Contact::TestOverlap path
 	BK_INACTIVE,         // both bodies asleep or static: state carried over
 	BK_COUNT
 };
@@ -70,6 +71,19 @@ struct HullDesc
 };
 static_assert(sizeof(HullDesc) == 48, "HullDesc");
 
+// A triangle mesh (b3Mesh, mesh.h:40-60): vertices, triangles with their
+// edge wings (b3Mesh::BuildAdjacency) and the static AABB tree
+// (b3StaticTree, built on the host exactly as b3Mesh::BuildTree does).
+struct MeshDesc
+{
+	uint32_t vOff, vCnt;   // vertices (float4)
+	uint32_t tOff, tCnt;   // triangles (uint4 vertex indices) and wings (uint4)
+	uint32_t nOff, nCnt;   // tree nodes (2 float4 each)
+	uint32_t root, pad;
+};
+static_assert(sizeof(MeshDesc) == 32, "MeshDesc");
+#define B3G_NULL_NODE 0xFFFFFFFFu
+
 // Scene and per-pass device buffers.
 struct DevScene
 {
@@ -103,6 +117,14 @@ struct DevScene
 	// when the edge has one)
 	const float4* fixTri;
 	const float4* fixWing;
+
+	// triangle meshes: fixtures of type mesh keep the mesh index in fixHull
+	// and p[0..2] = scale, p[3] = radius
+	const MeshDesc* meshes;
+	const float4* meshVerts;  // xyz
+	const uint4* meshTris;    // mesh-local vertex indices
+	const uint4* meshWings;   // wing vertex per edge, B3G_NULL for an open edge
+	const float4* meshNodes;  // (lower, child1 bits), (upper, child2 or triangle bits)
 };
 
 // Fixture life states. A fresh fixture was written by a scene update since the
@@ -178,6 +200,17 @@ struct Buffers
 	DevManifold* touchMan;
 	uint32_t* contactOut; // 3 u32 per contact: A, B, flags
 
+	// mesh contacts (allocated when the scene has meshes)
+	float4* meshAABB[2];      // per contact: the other shape's fat AABB in mesh space (2 float4)
+	DevManifold* extraMan[2]; // per contact: manifolds 1 and 2 of a mesh contact
+	uint32_t* meshCount;      // per contact: overlapping triangles, then exclusive offsets
+	uint32_t* meshPairC;      // per (contact, triangle) work item: contact
+	uint32_t* meshPairT;      // ... triangle
+	DevManifold* meshPairMan; // ... its b3Manifold (triangleKey set)
+	float4* meshObs;          // 3 per point slot of a work item: cluster observations
+	float4* meshPoly;         // 1 per point slot: a cluster's polygon vertices
+	uint32_t meshPairCap;
+
 	// wake-ups of UpdateContacts (only when some body is asleep)
 	uint32_t* tWake;        // per body: earliest list position that woke it
 	uint32_t* wakeList;     // contacts activated this round
@@ -211,10 +244,12 @@ enum
 	CTR_WAKE_ACTIVATED,
 	CTR_LATE_DESTROYED,
 	CTR_BUCKET0 = 16,   // BK_COUNT bucket sizes
-	CTR_ASLEEP = 27,    // non-static bodies still asleep after the wake-ups
-	CTR_SCRATCH = 28,
+	CTR_ASLEEP = 28,    // non-static bodies still asleep after the wake-ups
+	CTR_SCRATCH = 29,
+	CTR_MESH_PAIRS = 30, // (contact, triangle) work items of the pass
 	CTR_COUNT = 32
 };
+static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 
 // Launch shapes of the tunable kernels (include/b3g.h, B3G_TUNE_*).
 #define B3G_CONVEX_KERNELS 9
@@ -277,6 +312,17 @@ struct b3g_ctx
 	float4* dFixTri;
 	float4* dFixWing;
 	uint32_t triSlots; // fixtures with triangle storage (all, or 1 when there are no triangles)
+
+	// triangle meshes
+	uint32_t nMeshes;
+	MeshDesc* dMeshes;
+	float4* dMeshVerts;
+	uint4* dMeshTris;
+	uint4* dMeshWings;
+	float4* dMeshNodes;
+	std::vector<MeshDesc> hMeshes;
+	uint32_t* dMeshFix;       // mesh fixtures of the scene
+	uint32_t nMeshFix;
 	uint32_t capBodies, capFixtures; // uploaded counts; nBodies / nFixtures are the processed prefixes
 	bool keysAreIndex;               // proxy keys = fixture indices (scene updates need it)
 	// staging of b3g_update_scene: a ring of pinned host / device blocks
@@ -352,6 +398,11 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s);
 void launch_narrowphase(b3g_ctx* c, cudaStream_t s);
 void launch_finalize(b3g_ctx* c, cudaStream_t s);
 uint32_t pairs_diff_launches(const b3g_ctx* c);
+void launch_mesh_fat(b3g_ctx* c, cudaStream_t s);
+void launch_mesh_prepare(b3g_ctx* c, cudaStream_t s);
+void launch_mesh_collide(b3g_ctx* c, const uint32_t* list, const uint32_t* count, cudaStream_t s);
+uint32_t mesh_launches(const b3g_ctx* c);
+void free_mesh(b3g_ctx* c);
 int resolve_wakeups(b3g_ctx* c, cudaStream_t s);
 void launch_collide_pairs(b3g_ctx* c, cudaStream_t s, uint32_t n, const uint32_t* fixA,
 	const uint32_t* fixB, const float* xfA, const float* xfB, const float* xf0A,

@@ -61,6 +61,8 @@ B3G_HD V3 cross(V3 a, V3 b)
 	return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 B3G_HD float len(V3 v) { return sqrtf((v.x * v.x + v.y * v.y) + v.z * v.z); }
+// b3Mul(vec, vec): component-wise product (scaling).
+B3G_HD V3 vmul(V3 a, V3 b) { return V3{a.x * b.x, a.y * b.y, a.z * b.z}; }
 B3G_HD float len2(V3 v) { return (v.x * v.x + v.y * v.y) + v.z * v.z; }
 B3G_HD float fminr(float a, float b) { return a < b ? a : b; } // b3Min (math.h:45-48)
 B3G_HD float fmaxr(float a, float b) { return a > b ? a : b; } // b3Max (math.h:51-54)

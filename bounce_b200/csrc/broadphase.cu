@@ -27,104 +27,6 @@ namespace {
 
 constexpr uint32_t SENT = 0xFFFFFFFFu;
 
-__device__ __forceinline__ XF load_xf(const float* s)
-{
-	XF x;
-	x.p = V3{s[0], s[1], s[2]};
-	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
-	return x;
-}
-
-// b3Shape::ComputeAABB for one transform (hull_shape.cpp:160-164,
-// sphere_shape.cpp:51-57, capsule_shape.cpp:124-131, triangle_shape.cpp:59-67).
-// Two transforms are handled in one vertex loop for hulls.
-__device__ void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb,
-	bool two, AABB& a, AABB& b)
-{
-	uint32_t type = S.fixType[fix];
-	float4 p0 = S.fixParams[3 * fix + 0];
-	float4 p1 = S.fixParams[3 * fix + 1];
-	float4 p2 = S.fixParams[3 * fix + 2];
-	if (type == B3G_SHAPE_SPHERE)
-	{
-		V3 c = V3{p0.x, p0.y, p0.z};
-		float r = p0.w;
-		V3 rv = V3{r, r, r};
-		V3 ca = xmul(xa, c);
-		a.lo = ca - rv;
-		a.hi = ca + rv;
-		if (two)
-		{
-			V3 cb = xmul(xb, c);
-			b.lo = cb - rv;
-			b.hi = cb + rv;
-		}
-	}
-	else if (type == B3G_SHAPE_CAPSULE)
-	{
-		V3 v1 = V3{p0.x, p0.y, p0.z};
-		V3 v2 = V3{p0.w, p1.x, p1.y};
-		float r = p1.z;
-		V3 rv = V3{r, r, r};
-		V3 c1 = xmul(xa, v1), c2 = xmul(xa, v2);
-		a.lo = vmin(c1, c2) - rv;
-		a.hi = vmax(c1, c2) + rv;
-		if (two)
-		{
-			c1 = xmul(xb, v1);
-			c2 = xmul(xb, v2);
-			b.lo = vmin(c1, c2) - rv;
-			b.hi = vmax(c1, c2) + rv;
-		}
-	}
-	else if (type == B3G_SHAPE_TRIANGLE)
-	{
-		// The reference ignores the transform here (triangle_shape.cpp:59-67).
-		V3 v1 = V3{p0.x, p0.y, p0.z};
-		V3 v2 = V3{p0.w, p1.x, p1.y};
-		V3 v3_ = V3{p1.z, p1.w, p2.x};
-		float r = p2.y;
-		V3 rv = V3{r, r, r};
-		a.lo = vmin(v1, vmin(v2, v3_)) - rv;
-		a.hi = vmax(v1, vmax(v2, v3_)) + rv;
-		b = a;
-	}
-	else // hull
-	{
-		const HullDesc h = S.hulls[S.fixHull[fix]];
-		const float4* hv = S.hverts + h.vOff;
-		float4 w = hv[0];
-		V3 v = V3{w.x, w.y, w.z};
-		V3 ta = xmul(xa, v);
-		a.lo = ta;
-		a.hi = ta;
-		V3 tb;
-		if (two)
-		{
-			tb = xmul(xb, v);
-			b.lo = tb;
-			b.hi = tb;
-		}
-		for (uint32_t i = 1; i < h.vCnt; ++i)
-		{
-			w = hv[i];
-			v = V3{w.x, w.y, w.z};
-			ta = xmul(xa, v);
-			a.lo = vmin(a.lo, ta);
-			a.hi = vmax(a.hi, ta);
-			if (two)
-			{
-				tb = xmul(xb, v);
-				b.lo = vmin(b.lo, tb);
-				b.hi = vmax(b.hi, tb);
-			}
-		}
-		float r = p0.x;
-		aabb_extend(a, r);
-		if (two)
-			aabb_extend(b, r);
-	}
-}
 
 __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 {
@@ -137,6 +39,13 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 		// No proxy: an empty box (lower > upper) that overlaps nothing.
 		B.fatLo[i] = make_float4(B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR, 0.0f);
 		B.fatHi[i] = make_float4(-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR, 0.0f);
+		B.moved[i] = 0;
+		return;
+	}
+	if (S.fixType[i] == B3G_SHAPE_MESH)
+	{
+		// Meshes sit on static bodies: their proxy is created once (k_mesh_fat
+		// on a creation pass) and never moves.
 		B.moved[i] = 0;
 		return;
 	}
@@ -764,6 +673,8 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 		return;
 	k_body_prep<<<(c->nBodies + 255) / 256, 256, 0, s>>>(c->scene, c->nBodies);
 	k_sync<<<(n + 127) / 128, 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
+	if (c->creationPass)
+		launch_mesh_fat(c, s);
 }
 
 // Kernels launched by launch_broadphase for the current scene (kept next to
@@ -784,7 +695,6 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	int n = (int)c->nFixtures;
-	uint32_t cur = c->cur;
 	if (n == 0)
 	{
 		cudaMemsetAsync(B.counters + CTR_RAW, 0, sizeof(uint32_t), s);

@@ -373,7 +373,9 @@ __device__ __forceinline__ void sort_polygon(CV* p, uint32_t n, V3 N)
 	}
 }
 
-// b3ReducePolygon (cluster.cpp:59-200). out holds at most 4 vertices.
+// b3ReducePolygon (cluster.cpp:59-200). out holds at most 4 vertices, so the
+// reference's per-vertex chosen flags are kept as a list of at most 4
+// indices.
 __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint32_t n, V3 N, uint32_t initialPoint)
 {
 	if (n <= 4)
@@ -383,17 +385,25 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 		sort_polygon(out, n, N);
 		return n;
 	}
-	uint64_t chosen = 0; // n <= B3G_MAX_POLY
+	uint32_t chosen[4];
+	uint32_t nChosen = 0;
+	auto isChosen = [&](uint32_t i) {
+		bool r = false;
+		for (uint32_t k = 0; k < nChosen; ++k)
+			r |= chosen[k] == i;
+		return r;
+	};
+	auto choose = [&](uint32_t i) { chosen[nChosen++] = i; };
 	uint32_t cnt = 0;
 	out[cnt++] = in[initialPoint];
-	chosen |= 1ull << initialPoint;
+	choose(initialPoint);
 	{
 		V3 A = out[0].pos;
 		uint32_t index = 0;
 		float mx = -B3G_MAX_SCALAR;
 		for (uint32_t i = 0; i < n; ++i)
 		{
-			if (chosen >> i & 1ull)
+			if (isChosen(i))
 				continue;
 			V3 d = in[i].pos - A;
 			float dd = dot(d, d);
@@ -406,7 +416,7 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 		if (mx < B3G_EPSILON * B3G_EPSILON)
 			return cnt;
 		out[cnt++] = in[index];
-		chosen |= 1ull << index;
+		choose(index);
 	}
 	{
 		V3 A = out[0].pos;
@@ -415,7 +425,7 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 		float mx = -B3G_MAX_SCALAR;
 		for (uint32_t i = 0; i < n; ++i)
 		{
-			if (chosen >> i & 1ull)
+			if (isChosen(i))
 				continue;
 			V3 C = in[i].pos;
 			V3 Nn = cross(B - A, C - A);
@@ -438,7 +448,7 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 			out[1] = t;
 		}
 		out[cnt++] = in[index];
-		chosen |= 1ull << index;
+		choose(index);
 	}
 	{
 		V3 A = out[0].pos;
@@ -447,7 +457,7 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 		float mn = B3G_MAX_SCALAR;
 		for (uint32_t i = 0; i < n; ++i)
 		{
-			if (chosen >> i & 1ull)
+			if (isChosen(i))
 				continue;
 			V3 D = in[i].pos;
 			V3 Nn = cross(B - A, D - A);
@@ -462,7 +472,7 @@ __device__ __forceinline__ uint32_t reduce_polygon(CV out[4], const CV* in, uint
 		if (fabsr(mn) < 2.0f * kAreaTol)
 			return cnt;
 		out[cnt++] = in[index];
-		chosen |= 1ull << index;
+		choose(index);
 	}
 	sort_polygon(out, cnt, N);
 	return cnt;
@@ -556,6 +566,9 @@ struct NPArgs
 	// hull-hull pairs the feature cache could not resolve
 	uint32_t* missList;
 	uint32_t* missCount;
+	// manifolds 1 and 2 of mesh contacts (null without meshes)
+	DevManifold* extraCur;
+	const DevManifold* extraPrev;
 };
 
 // ---------------------------------------------------------------------------
@@ -637,6 +650,216 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t ta, uint32_t tb)
 	}
 	return BK_COUNT; // mesh pairs: not handled by these buckets
 }
+
+// ---------------------------------------------------------------------------
+// Shape AABBs.
+
+__device__ __forceinline__ XF load_xf(const float* s)
+{
+	XF x;
+	x.p = V3{s[0], s[1], s[2]};
+	x.q = Q4{V3{s[3], s[4], s[5]}, s[6]};
+	return x;
+}
+
+// b3Shape::ComputeAABB for one transform (hull_shape.cpp:160-164,
+// sphere_shape.cpp:51-57, capsule_shape.cpp:124-131, triangle_shape.cpp:59-67).
+// Two transforms are handled in one vertex loop for hulls.
+__device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb,
+	bool two, AABB& a, AABB& b)
+{
+	uint32_t type = S.fixType[fix];
+	float4 p0 = S.fixParams[3 * fix + 0];
+	float4 p1 = S.fixParams[3 * fix + 1];
+	float4 p2 = S.fixParams[3 * fix + 2];
+	if (type == B3G_SHAPE_SPHERE)
+	{
+		V3 c = V3{p0.x, p0.y, p0.z};
+		float r = p0.w;
+		V3 rv = V3{r, r, r};
+		V3 ca = xmul(xa, c);
+		a.lo = ca - rv;
+		a.hi = ca + rv;
+		if (two)
+		{
+			V3 cb = xmul(xb, c);
+			b.lo = cb - rv;
+			b.hi = cb + rv;
+		}
+	}
+	else if (type == B3G_SHAPE_CAPSULE)
+	{
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		float r = p1.z;
+		V3 rv = V3{r, r, r};
+		V3 c1 = xmul(xa, v1), c2 = xmul(xa, v2);
+		a.lo = vmin(c1, c2) - rv;
+		a.hi = vmax(c1, c2) + rv;
+		if (two)
+		{
+			c1 = xmul(xb, v1);
+			c2 = xmul(xb, v2);
+			b.lo = vmin(c1, c2) - rv;
+			b.hi = vmax(c1, c2) + rv;
+		}
+	}
+	else if (type == B3G_SHAPE_TRIANGLE)
+	{
+		// The reference ignores the transform here (triangle_shape.cpp:59-67).
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		V3 v3_ = V3{p1.z, p1.w, p2.x};
+		float r = p2.y;
+		V3 rv = V3{r, r, r};
+		a.lo = vmin(v1, vmin(v2, v3_)) - rv;
+		a.hi = vmax(v1, vmax(v2, v3_)) + rv;
+		b = a;
+	}
+	else // hull
+	{
+		const HullDesc h = S.hulls[S.fixHull[fix]];
+		const float4* hv = S.hverts + h.vOff;
+		float4 w = hv[0];
+		V3 v = V3{w.x, w.y, w.z};
+		V3 ta = xmul(xa, v);
+		a.lo = ta;
+		a.hi = ta;
+		V3 tb;
+		if (two)
+		{
+			tb = xmul(xb, v);
+			b.lo = tb;
+			b.hi = tb;
+		}
+		for (uint32_t i = 1; i < h.vCnt; ++i)
+		{
+			w = hv[i];
+			v = V3{w.x, w.y, w.z};
+			ta = xmul(xa, v);
+			a.lo = vmin(a.lo, ta);
+			a.hi = vmax(a.hi, ta);
+			if (two)
+			{
+				tb = xmul(xb, v);
+				b.lo = vmin(b.lo, tb);
+				b.hi = vmax(b.hi, tb);
+			}
+		}
+		float r = p0.x;
+		aabb_extend(a, r);
+		if (two)
+			aabb_extend(b, r);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Meshes.
+
+// b3StaticTree::QueryAABB (static_tree.h:114-150): depth-first from the root
+// with a LIFO stack (child1 pushed, then child2, so child2 is searched
+// first), reporting each overlapping leaf's triangle in that order. False if
+// the stack overflowed (the query stops).
+template <class F>
+__device__ inline bool mesh_query(const DevScene& S, const MeshDesc& md, const AABB& box, F&& report)
+{
+	constexpr uint32_t STACK = 64;
+	uint32_t stack[STACK];
+	uint32_t sp = 0;
+	stack[sp++] = md.root;
+	while (sp > 0)
+	{
+		uint32_t id = stack[--sp];
+		if (id == B3G_NULL_NODE)
+			continue;
+		float4 lo = S.meshNodes[2 * (size_t)(md.nOff + id)], hi = S.meshNodes[2 * (size_t)(md.nOff + id) + 1];
+		bool overlap = !(hi.x < box.lo.x || lo.x > box.hi.x || hi.y < box.lo.y || lo.y > box.hi.y ||
+			hi.z < box.lo.z || lo.z > box.hi.z);
+		if (!overlap)
+			continue;
+		uint32_t child1 = __float_as_uint(lo.w), other = __float_as_uint(hi.w);
+		if (child1 == B3G_NULL_NODE)
+			report(other);
+		else
+		{
+			if (sp + 2 > STACK)
+				return false;
+			stack[sp++] = child1;
+			stack[sp++] = other;
+		}
+	}
+	return true;
+}
+
+// b3MeshShape::GetChildTriangle (mesh_shape.cpp:151-183): the scaled
+// vertices, the mesh radius and the wings of the triangle's edges, with its
+// b3TriangleHull (triangle_hull.h:36-69).
+struct MeshTri
+{
+	V3 v[3];
+	float4 wing[3]; // wing vertex, w = 1 when the edge has one
+	float radius;
+	float4 hv[3];   // hull vertices
+	float4 hp[2];   // hull planes
+	V3 centroid;
+};
+
+__device__ inline void mesh_triangle(const DevScene& S, uint32_t meshFix, uint32_t t, MeshTri& out)
+{
+	const MeshDesc md = S.meshes[S.fixHull[meshFix]];
+	float4 sp = S.fixParams[3 * meshFix];
+	V3 sc = V3{sp.x, sp.y, sp.z};
+	uint4 tri = S.meshTris[md.tOff + t];
+	uint4 w = S.meshWings[md.tOff + t];
+	auto vert = [&](uint32_t i) {
+		float4 a = S.meshVerts[md.vOff + i];
+		return vmul(sc, V3{a.x, a.y, a.z});
+	};
+	out.v[0] = vert(tri.x);
+	out.v[1] = vert(tri.y);
+	out.v[2] = vert(tri.z);
+	uint32_t wi[3] = {w.x, w.y, w.z};
+	for (int k = 0; k < 3; ++k)
+	{
+		if (wi[k] != B3G_NULL)
+		{
+			V3 e = vert(wi[k]);
+			out.wing[k] = make_float4(e.x, e.y, e.z, 1.0f);
+		}
+		else
+			out.wing[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+	}
+	out.radius = sp.w;
+	V3 A = out.v[0], B = out.v[1], C = out.v[2];
+	V3 cen = ((A + B) + C) / 3.0f;
+	V3 N = normalized(cross(B - A, C - A));
+	V3 M = -N;
+	out.hv[0] = make_float4(A.x, A.y, A.z, 0.0f);
+	out.hv[1] = make_float4(B.x, B.y, B.z, 0.0f);
+	out.hv[2] = make_float4(C.x, C.y, C.z, 0.0f);
+	out.hp[0] = make_float4(N.x, N.y, N.z, dot(N, cen));
+	out.hp[1] = make_float4(M.x, M.y, M.z, dot(M, cen));
+	out.centroid = cen;
+}
+
+__device__ __forceinline__ HullRef mesh_tri_ref(const MeshTri& t)
+{
+	HullRef r;
+	r.v = t.hv;
+	r.e = kTriEdges;
+	r.f = kTriFaces;
+	r.p = t.hp;
+	r.vCnt = 3;
+	r.eCnt = 6;
+	r.fCnt = 2;
+	r.centroid = t.centroid;
+	return r;
+}
+
+void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
+	cudaStream_t s);
+void launch_mesh_items_convex(const NPArgs& a, const Buffers& B, cudaStream_t s);
+void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s);
 
 // Narrowphase arguments of the current pass (contact arrays of c->cur).
 NPArgs make_np_args(b3g_ctx* c);

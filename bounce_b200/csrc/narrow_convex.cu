@@ -11,8 +11,6 @@
 
 namespace {
 
-__device__ __forceinline__ V3 f3(float4 a) { return V3{a.x, a.y, a.z}; }
-
 struct ShapeP
 {
 	uint32_t type;
@@ -569,9 +567,10 @@ __device__ bool feature_edge1(const GJKSimplexOut& sx, uint32_t& v1, uint32_t& v
 	return false;
 }
 
-// b3CollideTriangleAndCapsule (collide_triangle_capsule.cpp:104-278).
-__device__ void collide_triangle_capsule(DevManifold& m, const DevScene& S, uint32_t fix1, const XF& xf1,
-	const ShapeP& t1, const TriWings& wg, const XF& xf2, const ShapeP& k2)
+// b3CollideTriangleAndCapsule (collide_triangle_capsule.cpp:104-278); h1 is
+// the triangle's b3TriangleHull.
+__device__ void collide_triangle_capsule(DevManifold& m, const HullRef& h1, const XF& xf1, const ShapeP& t1,
+	const TriWings& wg, const XF& xf2, const ShapeP& k2)
 {
 	float r1 = tri_radius(t1), r2 = cap_radius(k2);
 	float totalRadius = r1 + r2;
@@ -592,7 +591,6 @@ __device__ void collide_triangle_capsule(DevManifold& m, const DevScene& S, uint
 	GJKOut q = gjk(xf1, p1, xf2, p2, false, &sx);
 	if (q.distance > totalRadius)
 		return;
-	HullRef h1 = tri_ref(S, fix1);
 	V3 v1 = cap_v1(k2), v2 = cap_v2(k2);
 	if (q.distance > 0.0f)
 	{
@@ -766,7 +764,7 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 		else if (BUCKET == BK_TRIANGLE_SPHERE)
 			collide_triangle_sphere(m, xfA, sa, load_wings(a.S, fa), xfB, sb);
 		else if (BUCKET == BK_TRIANGLE_CAPSULE)
-			collide_triangle_capsule(m, a.S, fa, xfA, sa, load_wings(a.S, fa), xfB, sb);
+			collide_triangle_capsule(m, tri_ref(a.S, fa), xfA, sa, load_wings(a.S, fa), xfB, sb);
 		finish_convex(a, c, m);
 		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
@@ -810,6 +808,11 @@ __global__ void k_inactive(NPArgs a)
 			a.cstate[c] = a.prevState[prev] & ~(1u << 16);
 			a.cache[c] = a.prevCache[prev];
 			a.man[c] = a.prevMan[prev];
+			if (a.extraCur && ((a.prevState[prev] >> 8) & 0xFFu) > 1)
+			{
+				a.extraCur[2 * (size_t)c] = a.extraPrev[2 * (size_t)prev];
+				a.extraCur[2 * (size_t)c + 1] = a.extraPrev[2 * (size_t)prev + 1];
+			}
 		}
 		else
 		{
@@ -817,6 +820,55 @@ __global__ void k_inactive(NPArgs a)
 			a.cache[c] = make_uint4(0, B3G_NULL, B3G_NULL, B3G_NULL);
 			man_clear(a.man[c]);
 		}
+	}
+}
+
+// Mesh work items whose other shape is a sphere or a capsule (the mesh is
+// fixture A, the primary order): one triangle each (b3MeshAndSphereContact /
+// b3MeshAndCapsuleContact::Evaluate, mesh_sphere_contact.cpp:42-50,
+// mesh_capsule_contact.cpp:42-50), points tagged with the triangle
+// (mesh_contact.cpp:343-356). Sensor contacts record the triangle's overlap
+// (b3TestOverlap with the child index, collision.cpp:104-113) in pointCount.
+__global__ void __launch_bounds__(128) k_mesh_items_convex(NPArgs a, Buffers B)
+{
+	uint32_t n = min(B.counters[CTR_MESH_PAIRS], B.meshPairCap);
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		uint32_t c = B.meshPairC[i], t = B.meshPairT[i];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		uint32_t tb = a.S.fixType[fb];
+		if (a.S.fixType[fa] != B3G_SHAPE_MESH || (tb != B3G_SHAPE_SPHERE && tb != B3G_SHAPE_CAPSULE))
+			continue;
+		XF xfA = body_xf(a.S, a.S.fixBody[fa]), xfB = body_xf(a.S, a.S.fixBody[fb]);
+		MeshTri tri;
+		mesh_triangle(a.S, fa, t, tri);
+		ShapeP st;
+		st.type = B3G_SHAPE_TRIANGLE;
+		st.p0 = make_float4(tri.v[0].x, tri.v[0].y, tri.v[0].z, tri.v[1].x);
+		st.p1 = make_float4(tri.v[1].y, tri.v[1].z, tri.v[2].x, tri.v[2].y);
+		st.p2 = make_float4(tri.v[2].z, tri.radius, 0.0f, 0.0f);
+		st.hull = 0;
+		ShapeP sb = load_shape(a.S, fb);
+		DevManifold& m = B.meshPairMan[i];
+		man_clear(m);
+		if ((a.S.fixFlags[fa] | a.S.fixFlags[fb]) & B3G_FIXTURE_SENSOR)
+		{
+			GJKOut q = gjk(xfA, shape_proxy(a.S, st), xfB, shape_proxy(a.S, sb), true);
+			m.pointCount = q.distance <= 10.0f * B3G_EPSILON ? 1u : 0u;
+			continue;
+		}
+		TriWings wg;
+		for (int k = 0; k < 3; ++k)
+		{
+			wg.e[k] = V3{tri.wing[k].x, tri.wing[k].y, tri.wing[k].z};
+			wg.has[k] = tri.wing[k].w != 0.0f;
+		}
+		if (tb == B3G_SHAPE_SPHERE)
+			collide_triangle_sphere(m, xfA, st, wg, xfB, sb);
+		else
+			collide_triangle_capsule(m, mesh_tri_ref(tri), xfA, st, wg, xfB, sb);
+		for (uint32_t j = 0; j < m.pointCount; ++j)
+			m.points[j].triangleKey = t;
 	}
 }
 
@@ -870,4 +922,9 @@ void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint
 {
 	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
 		launch_convex_one(k, base, lists, counts, cap, tune, s);
+}
+
+void launch_mesh_items_convex(const NPArgs& a, const Buffers& B, cudaStream_t s)
+{
+	k_mesh_items_convex<<<persistent_blocks(4), 128, 0, s>>>(a, B);
 }

@@ -43,28 +43,6 @@ __device__ __forceinline__ void warp_argmax(float& v, uint32_t& idx)
 	}
 }
 
-// b3Project(hull, plane) (sat.cpp:26-30) with the support vertex
-// (hull.h:105-119) searched over the lanes. Uniform result on all lanes.
-__device__ float warp_project(const HullRef& h, PL plane, uint32_t lane)
-{
-	V3 d = -plane.n;
-	float best = 0.0f;
-	uint32_t bi = 0xFFFFFFFFu;
-	for (uint32_t i = lane; i < h.vCnt; i += 32)
-	{
-		float proj = dot(d, hv(h, i));
-		if (bi == 0xFFFFFFFFu || proj > best)
-		{
-			best = proj;
-			bi = i;
-		}
-	}
-	if (bi == 0xFFFFFFFFu)
-		best = -INFINITY;
-	warp_argmax(best, bi);
-	return pdist(hv(h, bi), plane);
-}
-
 // b3QueryFaceSeparation(hull, hull) (sat.cpp:33-58).
 __device__ void warp_query_faces(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2,
 	uint32_t lane, uint32_t& index, float& sep)
@@ -376,16 +354,6 @@ enum
 	FT_FACE2 = 2
 };
 
-// b3FeatureCache::ReadFace (sat.cpp:209-224).
-__device__ uint32_t read_face(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2, uint32_t index1,
-	float totalRadius, uint32_t lane)
-{
-	XF xf = xmult(xf2, xf1);
-	PL plane = pmul(xf, hp(h1, index1));
-	float s = warp_project(h2, plane, lane);
-	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
-}
-
 // b3FeatureCache::ReadEdges (sat.cpp:226-281).
 __device__ uint32_t read_edges(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2, uint32_t i,
 	uint32_t j, float totalRadius)
@@ -687,12 +655,9 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 // hull-hull SAT: points on a triangle edge that has a coplanar wing take the
 // triangle's face normal (oriented from the hull to the triangle) so bodies
 // slide over mesh edges. Lane 0 only.
-__device__ void triangle_wing_normals(DevManifold& m, const DevScene& S, uint32_t fixT, const XF& xf1,
-	const HullRef& h1, const XF& xf2, const HullRef& h2)
+__device__ void triangle_wing_normals(DevManifold& m, const float4 w4[3], const XF& xf1, const HullRef& h1,
+	const XF& xf2, const HullRef& h2)
 {
-	float4 w4[3];
-	for (int k = 0; k < 3; ++k)
-		w4[k] = S.fixWing[3 * (size_t)fixT + k];
 	PL plane2 = pmul(xf2, hp(h2, 0));
 	V3 centroid1 = xmul(xf1, h1.centroid);
 	V3 centroid2 = xmul(xf2, h2.centroid);
@@ -773,9 +738,78 @@ __global__ void __launch_bounds__(W * 32) k_hull_triangle(NPArgs a, uint32_t max
 		__syncwarp();
 		if (lane == 0)
 		{
-			triangle_wing_normals(m, a.S, fb, H.xf1, H.h1, H.xf2, H.h2);
+			float4 w4[3];
+			for (int k = 0; k < 3; ++k)
+				w4[k] = a.S.fixWing[3 * (size_t)fb + k];
+			triangle_wing_normals(m, w4, H.xf1, H.h1, H.xf2, H.h2);
 			finish_convex(a, c, m);
 			a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+		}
+		__syncwarp();
+	}
+}
+
+// Mesh work items of hull-mesh contacts (hull A, mesh B): one warp per
+// triangle, b3CollideHullAndTriangle on the child triangle
+// (hull_mesh_contact.cpp:42-50), points tagged with the triangle. Sensor
+// contacts record the triangle's overlap in pointCount.
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_mesh_items_hull(NPArgs a, Buffers B, uint32_t maxUE)
+{
+	extern __shared__ float4 smem[];
+	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	uint32_t n = min(B.counters[CTR_MESH_PAIRS], B.meshPairCap);
+	for (uint32_t i = blockIdx.x * W + warp; i < n; i += gridDim.x * W)
+	{
+		uint32_t c = B.meshPairC[i], t = B.meshPairT[i];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		if (a.S.fixType[fa] != B3G_SHAPE_HULL || a.S.fixType[fb] != B3G_SHAPE_MESH)
+			continue;
+		MeshTri tri;
+		mesh_triangle(a.S, fb, t, tri);
+		HullCtx H;
+		H.xf1 = body_xf(a.S, a.S.fixBody[fa]);
+		H.xf2 = body_xf(a.S, a.S.fixBody[fb]);
+		H.h1 = hull_ref(a.S, a.S.fixHull[fa]);
+		H.h2 = mesh_tri_ref(tri);
+		H.r1 = a.S.fixParams[3 * fa].x;
+		H.r2 = tri.radius;
+		H.status = a.status;
+		H.recs = recs;
+		H.maxUE = maxUE;
+		DevManifold& m = B.meshPairMan[i];
+		if (lane == 0)
+			man_clear(m);
+		__syncwarp();
+		if ((a.S.fixFlags[fa] | a.S.fixFlags[fb]) & B3G_FIXTURE_SENSOR)
+		{
+			if (lane == 0)
+			{
+				GProxy pb;
+				pb.gv = nullptr;
+				pb.lv[0] = tri.v[0];
+				pb.lv[1] = tri.v[1];
+				pb.lv[2] = tri.v[2];
+				pb.count = 3;
+				pb.radius = tri.radius;
+				GProxy pa;
+				pa.gv = H.h1.v;
+				pa.count = H.h1.vCnt;
+				pa.radius = H.r1;
+				GJKOut q = gjk(H.xf1, pa, H.xf2, pb, true);
+				m.pointCount = q.distance <= 10.0f * B3G_EPSILON ? 1u : 0u;
+			}
+			__syncwarp();
+			continue;
+		}
+		collide_hulls_nocache(m, H, lane);
+		__syncwarp();
+		if (lane == 0)
+		{
+			triangle_wing_normals(m, tri.wing, H.xf1, H.h1, H.xf2, H.h2);
+			for (uint32_t j = 0; j < m.pointCount; ++j)
+				m.points[j].triangleKey = t;
 		}
 		__syncwarp();
 	}
@@ -873,4 +907,13 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 size_t hull_sat_smem(int warps, uint32_t maxUE)
 {
 	return (size_t)warps * 2 * maxUE * sizeof(EdgeRec);
+}
+
+void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s)
+{
+	uint32_t ue = maxUE > 3 ? maxUE : 3;
+	size_t smem = hull_sat_smem(4, ue);
+	if (smem > 48 * 1024)
+		cudaFuncSetAttribute(k_mesh_items_hull<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	k_mesh_items_hull<4><<<persistent_blocks((int)tune.v[B3G_TUNE_SAT_BLOCKS]), 128, smem, s>>>(a, B, ue);
 }

@@ -317,7 +317,11 @@ __global__ void k_wake_activate(DevScene S, Buffers B, uint32_t cur, uint32_t ca
 			}
 			continue;
 		}
-		uint32_t bk = sensor_pair(S, fa, fb) ? (uint32_t)BK_SENSOR : bucket_of(S.fixType[fa], S.fixType[fb]);
+		uint32_t bk;
+		if (S.fixType[fa] == B3G_SHAPE_MESH || S.fixType[fb] == B3G_SHAPE_MESH)
+			bk = BK_MESH;
+		else
+			bk = sensor_pair(S, fa, fb) ? (uint32_t)BK_SENSOR : bucket_of(S.fixType[fa], S.fixType[fb]);
 		if (bk >= BK_COUNT)
 			continue;
 		uint32_t slot = atomicAdd(&B.counters[CTR_BUCKET0 + bk], 1u);
@@ -401,6 +405,13 @@ __global__ void k_compact_move(Buffers B, uint32_t cur, uint32_t cap, uint32_t n
 		B.cstate[cur][pos] = B.cstate[prevBuf][old];
 		B.cache[cur][pos] = B.cache[prevBuf][old];
 		B.man[cur][pos] = B.man[prevBuf][old];
+		if (B.extraMan[cur])
+		{
+			B.extraMan[cur][2 * (size_t)pos] = B.extraMan[prevBuf][2 * (size_t)old];
+			B.extraMan[cur][2 * (size_t)pos + 1] = B.extraMan[prevBuf][2 * (size_t)old + 1];
+			B.meshAABB[cur][2 * (size_t)pos] = B.meshAABB[prevBuf][2 * (size_t)old];
+			B.meshAABB[cur][2 * (size_t)pos + 1] = B.meshAABB[prevBuf][2 * (size_t)old + 1];
+		}
 	}
 }
 
@@ -417,6 +428,17 @@ __global__ void k_set_counts(Buffers B, uint32_t pairs, uint32_t ended)
 }
 
 } // namespace
+
+// Exclusive scan of data[0, *nPtr) in place (nPtr a device count, at most
+// cap), its total written to *total.
+void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
+	cudaStream_t s)
+{
+	uint32_t blocks = (cap + SB - 1) / SB;
+	k_dscan_blocks<<<blocks, SB, 0, s>>>(data, nPtr, cap, aux);
+	k_dscan_sums<<<1, 1024, 0, s>>>(aux, blocks, total);
+	k_dscan_add<<<blocks, SB, 0, s>>>(data, nPtr, cap, aux);
+}
 
 // After the previous-contact lookup: lays out this pass's contacts in list
 // order, fills the hash table of this pass and lists the destroyed contacts.
@@ -494,6 +516,8 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 					c->maxUniqueEdges, c->tune, s);
 				launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap,
 					B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE, c->maxUniqueEdges, c->tune, s);
+				launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
+				launches += c->nMeshFix ? 3 : 0;
 				k_wake_events<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, cap, B.wakeList,
 					B.counters + CTR_WAKE_ACTIVATED, 0);
 				launches += B3G_CONVEX_KERNELS + 2 + 1 + 1;
@@ -525,6 +549,13 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 				cudaMemcpyDeviceToDevice, s);
 			cudaMemcpyAsync(B.man[prevBuf], B.man[cur] + numNew, sizeof(DevManifold) * copied,
 				cudaMemcpyDeviceToDevice, s);
+			if (B.extraMan[cur])
+			{
+				cudaMemcpyAsync(B.extraMan[prevBuf], B.extraMan[cur] + 2 * (size_t)numNew,
+					sizeof(DevManifold) * 2 * copied, cudaMemcpyDeviceToDevice, s);
+				cudaMemcpyAsync(B.meshAABB[prevBuf], B.meshAABB[cur] + 2 * (size_t)numNew,
+					sizeof(float4) * 2 * copied, cudaMemcpyDeviceToDevice, s);
+			}
 		}
 		k_compact_move<<<persistent_blocks(4), 256, 0, s>>>(B, cur, cap, np, numNew, copied, kept2, kept2Total);
 		const uint32_t total = std::min(numNew + kept2Total, cap);

@@ -65,6 +65,8 @@ __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 		uint32_t bk;
 		if (!activeA && !activeB)
 			bk = BK_INACTIVE;
+		else if (S.fixType[fa] == B3G_SHAPE_MESH || S.fixType[fb] == B3G_SHAPE_MESH)
+			bk = BK_MESH; // b3MeshContact, sensors included (its TestOverlap runs per triangle)
 		else if ((S.fixFlags[fa] | S.fixFlags[fb]) & B3G_FIXTURE_SENSOR)
 			bk = BK_SENSOR;
 		else
@@ -91,10 +93,18 @@ __global__ void k_finalize(Buffers B, uint32_t cur, uint32_t cap)
 	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
 	{
 		uint32_t st = B.cstate[cur][c];
-		uint32_t pc = ((st >> 8) & 0xFFu) ? B.man[cur][c].pointCount : 0u;
+		uint32_t mc = (st >> 8) & 0xFFu;
+		uint32_t pc = mc ? B.man[cur][c].pointCount : 0u;
 		touching += st & 1u;
 		manifolds += pc > 0 ? 1u : 0u;
 		points += pc;
+		for (uint32_t k = 1; k < mc && B.extraMan[cur]; ++k)
+		{
+			// Manifolds 1 and 2 of a mesh contact (b3MeshContact::m_stackManifolds).
+			uint32_t xp = B.extraMan[cur][2 * (size_t)c + k - 1].pointCount;
+			manifolds += xp > 0 ? 1u : 0u;
+			points += xp;
+		}
 		uint32_t flags = (st & 1u) | ((st >> 16 & 1u) << 1) | (st & 0xFF00u);
 		B.contactOut[3 * c + 0] = B.pairA[cur][c];
 		B.contactOut[3 * c + 1] = B.pairB[cur][c];
@@ -206,6 +216,8 @@ NPArgs make_np_args(b3g_ctx* c)
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
 	a.missList = B.missList;
 	a.missCount = B.counters + CTR_HULL_MISS;
+	a.extraCur = B.extraMan[cur];
+	a.extraPrev = B.extraMan[prev];
 	return a;
 }
 
@@ -213,6 +225,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	uint32_t cap = c->cfg.max_contacts;
+	launch_mesh_prepare(c, s);
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
 	NPArgs a = make_np_args(c);
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
@@ -221,6 +234,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 		c->maxUniqueEdges, c->tune, s);
 	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
 		c->maxUniqueEdges, c->tune, s);
+	launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
 	prof_mark(c, PM_HULLS, s);
 }
 

@@ -46,6 +46,11 @@ class CollisionPipeline:
                 N.ptr(ha["faces"], u32), N.ptr(ha["planes"], f32), N.ptr(ha["centroids"], f32),
             )
         )
+        meshes = getattr(scene, "mesh_arrays", None)
+        if meshes is not None:
+            self._check(self.lib.b3g_set_meshes(
+                self.ctx, len(meshes["desc"]) // 4, N.ptr(meshes["desc"], u32), N.ptr(meshes["verts"], f32),
+                N.ptr(meshes["tris"], u32), int(meshes.get("max_pairs", 0))))
         awake = np.ones(scene.n_bodies, np.uint8)
         self._check(
             self.lib.b3g_set_bodies(
@@ -118,7 +123,7 @@ class CollisionPipeline:
         return out[:m]
 
     def touching(self):
-        n = self.counts()["contacts"]
+        n = self.counts()["manifolds"]
         idx = np.zeros(max(n, 1), np.uint32)
         man = np.zeros(max(n, 1), N.MANIFOLD_DTYPE)
         m = self._check(self.lib.b3g_fetch_touching(self.ctx, N.ptr(idx, u32), ctypes.c_void_p(man.ctypes.data), n))
@@ -160,6 +165,11 @@ class CollisionPipeline:
         self._check(self.lib.b3g_get_totals(self.ctx, N.ptr(out, ctypes.c_uint64), 1 if reset else 0))
         names = ("passes", "contacts", "manifolds", "points", "begun", "ended", "launches", "graph_passes")
         return dict(zip(names, (int(x) for x in out)))
+
+    def mesh_wings(self, m, n_triangles):
+        out = np.zeros(3 * max(n_triangles, 1), np.uint32)
+        k = self._check(self.lib.b3g_mesh_wings(self.ctx, m, N.ptr(out, u32), n_triangles))
+        return out[: 3 * k].reshape(-1, 3)
 
     def autotune(self, reps=10, stream=None):
         """Times the tunable kernels on the last pass's data and keeps the

@@ -435,10 +435,9 @@ class KinematicDriver:
         return np.ascontiguousarray(out.reshape(-1))
 
 
-def terrain_triangles(nx, nz, spacing, seed, amplitude=0.5):
-    """Triangles of a height-field grid of nx x nz vertices (two per cell) and
-    the edge wings of each (the third vertex of the triangle across each
-    edge, as b3Mesh adjacency gives them): returns (params (n, 12), wings (n, 12))."""
+def grid_mesh(nx, nz, spacing, seed, amplitude=0.5):
+    """Vertices (nx * nz, 3) and triangles (2 per cell, counter-clockwise seen
+    from +y) of a height field: heights are a seeded sum of sines."""
     rng = np.random.default_rng(seed)
     xs = (np.arange(nx) - (nx - 1) / 2.0) * spacing
     zs = (np.arange(nz) - (nz - 1) / 2.0) * spacing
@@ -446,15 +445,17 @@ def terrain_triangles(nx, nz, spacing, seed, amplitude=0.5):
     X, Z = np.meshgrid(xs, zs, indexing="ij")
     Y = amplitude * (np.sin(0.7 * X + ph[0]) * np.sin(0.5 * Z + ph[1]) + 0.5 * np.sin(1.3 * X + ph[2]) * np.sin(0.9 * Z + ph[3]))
     V = np.stack([X, Y, Z], axis=-1).astype(F).reshape(-1, 3)
-    idx = lambda i, j: i * nz + j
-    tris = []
-    for i in range(nx - 1):
-        for j in range(nz - 1):
-            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
-            # counter-clockwise seen from +y
-            tris.append((a, d, c))
-            tris.append((a, c, b))
-    tris = np.array(tris, np.int64)
+    i, j = np.meshgrid(np.arange(nx - 1), np.arange(nz - 1), indexing="ij")
+    a, b, c, d = i * nz + j, (i + 1) * nz + j, (i + 1) * nz + j + 1, i * nz + j + 1
+    tris = np.stack([np.stack([a, d, c], -1), np.stack([a, c, b], -1)], axis=2).reshape(-1, 3)
+    return V, tris.astype(np.int64)
+
+
+def terrain_triangles(nx, nz, spacing, seed, amplitude=0.5):
+    """Triangles of a height-field grid of nx x nz vertices (two per cell) and
+    the edge wings of each (the third vertex of the triangle across each
+    edge, as b3Mesh adjacency gives them): returns (params (n, 12), wings (n, 12))."""
+    V, tris = grid_mesh(nx, nz, spacing, seed, amplitude)
     edge_owner = {}
     for t, (a, b, c) in enumerate(tris):
         for k, (u, v) in enumerate(((a, b), (b, c), (c, a))):
@@ -510,4 +511,44 @@ def terrain_scene(seed=3, n=800, grid=12, spacing=1.5, height=4.0, static_frac=0
             s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=hh)
     s.tri_fixtures = np.arange(first, first + len(params), dtype=np.uint32)
     s.tri_wings = wings
+    return s
+
+
+def mesh_terrain_scene(seed=5, n=800, grid=14, spacing=1.5, height=4.0, scale=(1.0, 1.0, 1.0)):
+    """Mixed moving bodies above a static triangle-mesh terrain (one mesh
+    fixture; scene.mesh_arrays holds the mesh)."""
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    V, tris = grid_mesh(grid, grid, spacing, seed)
+    s.mesh_arrays = dict(desc=np.array([0, len(V), 0, len(tris)], np.uint32),
+                         verts=np.ascontiguousarray(V.reshape(-1), F),
+                         tris=np.ascontiguousarray(tris.reshape(-1), np.uint32))
+    g = s.add_body(0, N.BODY_STATIC, (0, 0, 0), (0, 0, 0, 1))
+    s.add_fixture(g, N.SHAPE_MESH, [scale[0], scale[1], scale[2], 0.0], hull=0)
+    half = 0.5 * spacing * (grid - 1) * min(scale[0], scale[2])
+    pos = np.stack([rng.uniform(-half, half, n), rng.uniform(-0.5, height, n), rng.uniform(-half, half, n)],
+                   axis=-1).astype(F)
+    quat = random_quats(rng, n)
+    lin = rng.normal(0, 1, (n, 3)).astype(F)
+    lin[:, 1] -= 1.0
+    ang = rng.normal(0, 1, (n, 3)).astype(F)
+    for i in range(n):
+        b = s.add_body(0, N.BODY_DYNAMIC, pos[i], quat[i], lin[i], ang[i])
+        k = rng.random()
+        if k < 0.35:
+            s.add_fixture(b, N.SHAPE_SPHERE, [0, 0, 0, rng.uniform(0.2, 0.6)])
+        elif k < 0.65:
+            r = rng.uniform(0.1, 0.4)
+            h = rng.uniform(0.2, 0.7)
+            s.add_fixture(b, N.SHAPE_CAPSULE, [0, -h, 0, 0, h, 0, r])
+        else:
+            while True:
+                m = int(rng.integers(8, 20))
+                axes = rng.uniform(0.3, 0.8, 3)
+                try:
+                    hh = s.hulls.add_points(ellipsoid_points(rng, m, axes))
+                    break
+                except ValueError:
+                    continue
+            s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=hh)
     return s

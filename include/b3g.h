@@ -112,6 +112,25 @@ int b3g_set_hulls(b3g_ctx* ctx, uint32_t hull_count, const uint32_t* desc,
 	const float* verts, const uint32_t* edges, const uint32_t* faces,
 	const float* planes, const float* centroids);
 
+/* Triangle meshes (b3Mesh, mesh.h:40-60): desc 4 u32 per mesh (vertex
+ * offset, vertex count, triangle offset, triangle count into the arrays),
+ * vertices 3 floats, triangles 3 u32 (mesh-local vertex indices). The edge
+ * wings (b3Mesh::BuildAdjacency, mesh.cpp:36-119) and the static AABB tree
+ * (b3Mesh::BuildTree / b3StaticTree::Build, static_tree.cpp:22-167) are built
+ * here as the reference builds them. max_triangle_pairs bounds the
+ * (contact, triangle) work items of one pass (0: 4 x max_contacts); more are
+ * reported as B3G_E_CAPACITY. Call before b3g_set_fixtures; a mesh fixture
+ * (shape type B3G_SHAPE_MESH) names its mesh in the hull argument and has
+ * params p[0..2] = scale (b3MeshShape::m_scale, non-zero), p[3] = radius
+ * (B3_HULL_RADIUS = 0 in the reference); it must sit on a static body.
+ * Replaces b3MeshShape::m_mesh (mesh_shape.h:50). */
+int b3g_set_meshes(b3g_ctx* ctx, uint32_t mesh_count, const uint32_t* desc, const float* vertices,
+	const uint32_t* triangles, uint32_t max_triangle_pairs);
+
+/* The wing vertices of mesh m's triangles as built (3 u32 per triangle,
+ * 0xFFFFFFFF for an open edge). Returns the number of triangles written. */
+int b3g_mesh_wings(b3g_ctx* ctx, uint32_t mesh, uint32_t* out, uint32_t capacity);
+
 /* Bodies: world index, b3BodyType, awake flag (b3Body::IsAwake, body.h:585).
  * Replaces: b3World::CreateBody (world.cpp:98-126). */
 int b3g_set_bodies(b3g_ctx* ctx, uint32_t body_count, const uint32_t* world,
@@ -249,7 +268,9 @@ int b3g_fetch_contacts(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
 int b3g_fetch_manifolds(b3g_ctx* ctx, void* out, uint32_t capacity);
 
 /* Compact output: contact index (u32) and b3Manifold (320 bytes) of every
- * contact whose manifold has points, in contact order. Returns the count. */
+ * manifold with points, in contact order; a mesh contact appears once per
+ * manifold (up to B3_MAX_MANIFOLDS = 3, in manifold order). Returns the count.
+ * b3g_fetch_manifolds returns the first manifold of each contact. */
 int b3g_fetch_touching(b3g_ctx* ctx, uint32_t* index, void* manifolds, uint32_t capacity);
 
 /* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above

@@ -70,6 +70,8 @@ def lib(precision=32):
     sig = {
         "refh_create": ([ctypes.c_uint32, u32p, f32p, u32p, u32p, f32p, f32p], vp),
         "refh_destroy": ([vp], None),
+        "refh_add_meshes": ([vp, ctypes.c_uint32, u32p, f32p, u32p], None),
+        "refh_mesh_wings": ([vp, ctypes.c_uint32, u32p], None),
         "refw_create": (
             [vp, ctypes.c_uint32, u32p, f32p, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, ctypes.c_uint32],
             vp,
@@ -122,15 +124,26 @@ def _p(a, t):
 
 
 class RefHulls:
-    def __init__(self, hull_arrays, precision=32):
+    """Hulls and, when given, triangle meshes (mesh_arrays: desc, verts, tris)."""
+
+    def __init__(self, hull_arrays, precision=32, mesh_arrays=None):
         self.L = lib(precision)
         h = hull_arrays
-        self._keep = h
+        self._keep = (h, mesh_arrays)
         nh = len(h["desc"]) // 6
         self.h = self.L.refh_create(
             nh, _p(h["desc"], ctypes.c_uint32), _p(h["verts"], ctypes.c_float), _p(h["edges"], ctypes.c_uint32),
             _p(h["faces"], ctypes.c_uint32), _p(h["planes"], ctypes.c_float), _p(h["centroids"], ctypes.c_float),
         )
+        if mesh_arrays is not None:
+            m = mesh_arrays
+            self.L.refh_add_meshes(self.h, len(m["desc"]) // 4, _p(m["desc"], ctypes.c_uint32),
+                                   _p(m["verts"], ctypes.c_float), _p(m["tris"], ctypes.c_uint32))
+
+    def mesh_wings(self, m, n_triangles):
+        out = np.zeros(3 * n_triangles, np.uint32)
+        self.L.refh_mesh_wings(self.h, m, _p(out, ctypes.c_uint32))
+        return out.reshape(-1, 3)
 
     def __del__(self):
         try:
@@ -146,7 +159,7 @@ class RefWorld:
         self.L = lib(precision)
         self.precision = precision
         self.scene = scene
-        self.hulls = hulls or RefHulls(scene.hull_arrays, precision)
+        self.hulls = hulls or RefHulls(scene.hull_arrays, precision, getattr(scene, "mesh_arrays", None))
         s = scene
         self.w = self.L.refw_create(
             self.hulls.h, s.n_bodies, _p(s.body_type, ctypes.c_uint32), _p(s.body_pose, ctypes.c_float),

@@ -127,7 +127,66 @@ struct HullPool
 	std::vector<b3HalfEdge> edges;
 	std::vector<b3Face> faces;
 	std::vector<b3Plane> planes;
+	// triangle meshes (b3Mesh owns its static tree, so it is not copied)
+	std::vector<b3Mesh*> meshes;
+	std::vector<std::vector<b3Vec3>*> meshVerts;
+	std::vector<std::vector<b3MeshTriangle>*> meshTris;
+	~HullPool()
+	{
+		for (size_t i = 0; i < meshes.size(); ++i)
+		{
+			delete meshes[i];
+			delete meshVerts[i];
+			delete meshTris[i];
+		}
+	}
 };
+
+// Triangle meshes: desc 4 u32 per mesh (vertex offset, vertex count, triangle
+// offset, triangle count), vertices 3 floats, triangles 3 u32 (mesh-local
+// vertex indices). Each mesh gets its static tree and adjacency as
+// b3Mesh::BuildTree / BuildAdjacency build them.
+REF_API void refh_add_meshes(void* p, uint32_t nm, const uint32_t* desc, const float* mv, const uint32_t* mt)
+{
+	HullPool* pool = (HullPool*)p;
+	for (uint32_t m = 0; m < nm; ++m)
+	{
+		const uint32_t vOff = desc[4 * m], vCnt = desc[4 * m + 1], tOff = desc[4 * m + 2], tCnt = desc[4 * m + 3];
+		std::vector<b3Vec3>* V = new std::vector<b3Vec3>(vCnt);
+		std::vector<b3MeshTriangle>* T = new std::vector<b3MeshTriangle>(tCnt);
+		for (uint32_t i = 0; i < vCnt; ++i)
+			(*V)[i].Set(mv[3 * (vOff + i)], mv[3 * (vOff + i) + 1], mv[3 * (vOff + i) + 2]);
+		for (uint32_t i = 0; i < tCnt; ++i)
+		{
+			(*T)[i].v1 = mt[3 * (tOff + i)];
+			(*T)[i].v2 = mt[3 * (tOff + i) + 1];
+			(*T)[i].v3 = mt[3 * (tOff + i) + 2];
+		}
+		b3Mesh* mesh = new b3Mesh();
+		mesh->vertexCount = vCnt;
+		mesh->vertices = V->data();
+		mesh->triangleCount = tCnt;
+		mesh->triangles = T->data();
+		mesh->BuildTree();
+		mesh->BuildAdjacency();
+		pool->meshes.push_back(mesh);
+		pool->meshVerts.push_back(V);
+		pool->meshTris.push_back(T);
+	}
+}
+
+// Wing vertices of every triangle of mesh m (3 u32 each; B3_NULL_VERTEX for
+// an open edge), for checking the pipeline's adjacency.
+REF_API void refh_mesh_wings(void* p, uint32_t m, uint32_t* out)
+{
+	const b3Mesh* mesh = ((HullPool*)p)->meshes[m];
+	for (uint32_t i = 0; i < mesh->triangleCount; ++i)
+	{
+		out[3 * i] = mesh->triangles[i].u1;
+		out[3 * i + 1] = mesh->triangles[i].u2;
+		out[3 * i + 2] = mesh->triangles[i].u3;
+	}
+}
 
 REF_API void* refh_create(uint32_t nh, const uint32_t* desc, const float* hv, const uint32_t* he,
 	const uint32_t* hf, const float* hp, const float* hc)
@@ -188,6 +247,7 @@ struct ShapeStore
 	b3CapsuleShape capsule;
 	b3TriangleShape triangle;
 	b3HullShape hull;
+	b3MeshShape mesh;
 };
 
 // Wings of a triangle shape: 12 floats (e1, e2, e3 vertices, three flags).
@@ -222,6 +282,11 @@ static const b3Shape* MakeShape(ShapeStore& s, uint32_t type, const float* p, ui
 		s.hull.m_hull = &pool->hulls[hullIndex];
 		s.hull.m_radius = p[0];
 		return &s.hull;
+	case 4:
+		// mesh: p[0..2] scale; the radius stays B3_HULL_RADIUS
+		s.mesh.m_mesh = pool->meshes[hullIndex];
+		s.mesh.m_scale.Set(p[0], p[1], p[2]);
+		return &s.mesh;
 	default:
 		return nullptr;
 	}

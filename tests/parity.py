@@ -40,6 +40,26 @@ def compare_contacts(pipe, rw, label="", check_cache=True):
         f"{label}: point counts differ at {len(badpc)} of {len(gpc)} contacts; first "
         f"{[(int(gk[gi][i] >> 32), int(gk[gi][i] & 0xFFFFFFFF), int(gpc[i]), int(rpc[i])) for i in badpc[:5]]}"
     )
+    _compare_points(gm, rm, gpc, label)
+    if np.any(rcount > 1):
+        ref_of_gpu = np.empty(len(gi), np.int64)
+        ref_of_gpu[gi] = ri
+        compare_all_manifolds(pipe, rc, ref_of_gpu, label)
+    if check_cache:
+        gc = pipe.caches()[gi]
+        rcache = rc["cache"][ri]
+        hh = rcache[:, 0] != 0xFFFFFFFF
+        # An e_empty cache (type 0) leaves its other fields unset in the
+        # reference (sat.h:69): only the type is compared there.
+        empty = rcache[:, 0] == 0
+        same = np.where(empty[:, None], gc[:, :1] == rcache[:, :1], gc == rcache)
+        bad = np.nonzero(~np.all(same[hh], axis=1))[0]
+        assert len(bad) == 0, f"{label}: feature caches differ at {len(bad)}: {gc[hh][bad[:3]]} vs {rcache[hh][bad[:3]]}"
+    return dict(contacts=len(gs), touching=int(gt.sum()), points=int(gpc.sum()))
+
+
+def _compare_points(gm, rm, gpc, label):
+    """Points of manifolds gm (pipeline) and rm (reference), pointCount gpc each."""
     mask = np.arange(4)[None, :] < gpc[:, None]
     for f in ("n", "p1", "p2"):
         a = gm["points"][f][mask]
@@ -53,17 +73,29 @@ def compare_contacts(pipe, rw, label="", check_cache=True):
         f"{label}: persisting flags differ"
     )
     assert np.array_equal(gm["points"]["normalImpulse"][mask], rm["points"]["normalImpulse"][mask].astype(np.float32))
-    if check_cache:
-        gc = pipe.caches()[gi]
-        rcache = rc["cache"][ri]
-        hh = rcache[:, 0] != 0xFFFFFFFF
-        # An e_empty cache (type 0) leaves its other fields unset in the
-        # reference (sat.h:69): only the type is compared there.
-        empty = rcache[:, 0] == 0
-        same = np.where(empty[:, None], gc[:, :1] == rcache[:, :1], gc == rcache)
-        bad = np.nonzero(~np.all(same[hh], axis=1))[0]
-        assert len(bad) == 0, f"{label}: feature caches differ at {len(bad)}: {gc[hh][bad[:3]]} vs {rcache[hh][bad[:3]]}"
-    return dict(contacts=len(gs), touching=int(gt.sum()), points=int(gpc.sum()))
+
+
+def compare_all_manifolds(pipe, rc, ref_of_gpu, label=""):
+    """Every manifold with points (manifolds 1 and 2 of mesh contacts too), in
+    contact and manifold order, against the reference's b3Contact::m_manifolds."""
+    idx, man = pipe.touching()
+    exp_idx, exp_man = [], []
+    for c, r in enumerate(ref_of_gpu):
+        for k in range(int(rc["manifoldCount"][r])):
+            m = rc["manifolds"][r, k]
+            if m["pointCount"] > 0:
+                exp_idx.append(c)
+                exp_man.append(m)
+    exp_idx = np.asarray(exp_idx, np.uint32)
+    assert np.array_equal(idx, exp_idx), (
+        f"{label}: manifolds with points differ: gpu {len(idx)} ref {len(exp_idx)}"
+    )
+    if len(exp_man) == 0:
+        return
+    rm = np.stack(exp_man)
+    gpc = man["pointCount"]
+    assert np.array_equal(gpc, rm["pointCount"]), f"{label}: point counts of all manifolds differ"
+    _compare_points(man, rm, gpc, label + " (all manifolds)")
 
 
 def compare_fat_aabbs(pipe, rw, label=""):
