@@ -35,6 +35,13 @@ N_BODIES = 65536
 SIDE = 49.0
 SEED = 2
 WORKLOAD = "one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% hull 8-32 pts), 49 m cube, kinematic motion reflected at the cube faces"
+PILE_SEED = 9
+PILE_WORKLOAD = ("hull-heavy pile: 262,144 distinct hulls (quickhulls of 12-64 points on ellipsoids, semi-axes "
+                 "U[0.3, 1.0] m) in 512 columns of 512 with 1e-3 m vertical gaps, over a static mesh ground of "
+                 "512 x 512 vertices at 0.5 m (4 seeded sines, 2 m total amplitude); the pile settles kinematically")
+PILE_SAMPLE = ("4 of the 512 columns (2,048 hulls) over a 64 x 64-vertex patch of the same terrain: the reference's "
+               "b3Mesh::BuildAdjacency is quadratic in the triangle count, so the full 522,242-triangle ground "
+               "cannot be built on the host in the time of a run")
 
 
 def parse():
@@ -50,19 +57,24 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=30,
                     help="passes after the timed ones, with per-stage CUDA events (not part of value)")
     ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "batched", "serving"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving"])
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000",
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
     ap.add_argument("--worlds", type=int, default=1024)
     ap.add_argument("--autotune", action="store_true", default=True)
     args = ap.parse_args()
-    if args.workload == "batched":
-        # 30 steps.
+    if args.workload in ("batched", "pile"):
+        # The batched and pile workloads are quoted on 30 steps.
         if "--steps" not in sys.argv:
             args.steps = 30
         if "--warmup" not in sys.argv:
             args.warmup = 3
+    if args.workload == "pile":
+        if "--e2e-steps" not in sys.argv:
+            args.e2e_steps = 10
+        if "--profile-steps" not in sys.argv:
+            args.profile_steps = 10
     return args
 
 
@@ -147,8 +159,24 @@ def build_scene(n, seed):
     return S.mixed_scene(seed=seed, n=n, side=SIDE * (n / N_BODIES) ** (1.0 / 3.0)).finalize()
 
 
+def workload_scene(args, seed, sample=False):
+    """(scene, walls) of the single-world workload; sample: the bounded case
+    the reference's CPU pass is timed on when the full one cannot be built
+    on the host (the pile's ground mesh)."""
+    from bounce_b200 import scene as S
+
+    if args.workload == "pile":
+        sc = S.pile_scene(seed=seed, columns=4, grid=64) if sample else S.pile_scene(seed=seed)
+        return sc.finalize(), None
+    sc = build_scene(args.bodies, seed)
+    return sc, scene_half(sc)
+
+
 def config_dict(args, extra=None):
-    d = {"workload": WORKLOAD, "bodies": args.bodies, "proxies": args.bodies, "dt": 1.0 / 60.0,
+    pile = args.workload == "pile"
+    bodies = 512 * 512 if pile else args.bodies
+    d = {"workload": PILE_WORKLOAD if pile else WORKLOAD, "bodies": bodies, "proxies": bodies + (1 if pile else 0),
+         "dt": 1.0 / 60.0,
          "passes_timed": args.steps, "warmup_passes": args.warmup,
          "l2": "inputs larger than L2: per-pass contact state (two 320 B manifolds per contact) exceeds 126 MB",
          "parallelism": f"replicas x{args.gpus}"}
@@ -161,7 +189,7 @@ def config_dict(args, extra=None):
 # Reference CPU pipeline (oracle/_ref): the CPU baseline leg and --impl reference.
 
 
-def reference_run(scene, passes, seconds_cap=None, warmup=0):
+def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
     """Runs the reference's collision pass on the CPU: creation pass, `warmup`
     untimed passes, then up to `passes` timed passes (stopping early once
     seconds_cap of measured time is spent). Returns (manifolds, seconds, passes)."""
@@ -172,7 +200,7 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0):
         raise RuntimeError("oracle/_ref/libb3ref32.so not built")
     rw = O.RefWorld(scene)
     scene.set_local_centers(rw.local_centers())
-    drv = S.KinematicDriver(scene, walls=scene_half(scene))
+    drv = S.KinematicDriver(scene, walls=walls)
     rw.first_pass()
     for _ in range(warmup):
         drv.advance()
@@ -195,16 +223,19 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0):
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
         return
-    scene = build_scene(args.bodies, SEED)
-    m, t, done = reference_run(scene, args.steps, warmup=args.warmup)
+    pile = args.workload == "pile"
+    scene, walls = workload_scene(args, PILE_SEED if pile else SEED, sample=pile)
+    m, t, done = reference_run(scene, args.steps, warmup=args.warmup, walls=walls)
     v = m / t if t > 0 else 0.0
+    sample = (f"{done} passes of {PILE_SAMPLE}" if pile else
+              f"{done} passes of the full workload")
     line = {
         "metric": "manifolds/s", "value": v, "unit": "manifolds/s", "n_gpus": args.gpus, "steps": done,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t / max(done, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
         "config": config_dict(args), "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "manifolds/s", "cores": 1, "kind": "reference",
-                         "sample": f"{done} passes of the full workload on 1 host core (the reference is single-threaded)"},
+                         "sample": f"{sample} on 1 host core (the reference is single-threaded)"},
         "e2e": {"value": v, "unit": "manifolds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -234,8 +265,9 @@ def run_ours(args, rank, world, local, dist):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    scene = build_scene(args.bodies, SEED + rank)
-    drv = S.KinematicDriver(scene, walls=scene_half(scene))
+    pile = args.workload == "pile"
+    scene, walls = workload_scene(args, (PILE_SEED if pile else SEED) + rank)
+    drv = S.KinematicDriver(scene, walls=walls)
     # states: creation + warm-up, 2 passes that capture the tuned graphs, timed, profiled
     t0_k = 1 + args.warmup + 2
     n_dev = t0_k + args.steps + args.profile_steps
@@ -247,7 +279,8 @@ def run_ours(args, rank, world, local, dist):
         drv.advance()
         states[k] = drv.state17()
     d_states = torch.from_numpy(states[:n_dev]).to(dev)
-    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local, graph=not args.no_graph)
+    max_contacts = 4 * nb if pile else max(2_000_000, 40 * nb)
+    pipe = CollisionPipeline(scene, max_contacts=max_contacts, device=local, graph=not args.no_graph)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     row = 17 * nb * 4
@@ -368,10 +401,11 @@ def run_ours(args, rank, world, local, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            ref_scene = build_scene(args.bodies, SEED)
-            m, t, done = reference_run(ref_scene, 50, seconds_cap=args.cpu_seconds)
+            ref_scene, ref_walls = workload_scene(args, PILE_SEED if pile else SEED, sample=pile)
+            m, t, done = reference_run(ref_scene, 50, seconds_cap=args.cpu_seconds, walls=ref_walls)
+            what = PILE_SAMPLE if pile else "the same workload"
             cpu = {"value": m / t, "unit": "manifolds/s", "cores": 1, "kind": "reference",
-                   "sample": f"{done} passes of the same workload (creation pass excluded) on 1 host core; "
+                   "sample": f"{done} passes of {what} (creation pass excluded) on 1 host core; "
                              "the reference is single-threaded"}
         except Exception as e:  # the GPU number stands on its own
             cpu = {"value": None, "unit": "manifolds/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}

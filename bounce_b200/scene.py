@@ -18,6 +18,8 @@ operation order as the reference's inline math (include/bounce/common/math/
 quat.h:270-274, transform.h:66-69, body.h SynchronizeTransform), so transforms
 computed here equal the ones b3Body would hold, bit for bit.
 """
+import os
+
 import numpy as np
 
 from . import _native as N
@@ -134,6 +136,18 @@ class HullPool:
             N.ptr(p, N.ctypes.c_float), N.ptr(c, N.ctypes.c_float), N.ptr(counts, N.ctypes.c_uint32),
         )
         return self._add(v, e, f, p, c, counts)
+
+    def extend(self, arrays):
+        """Append packed hulls (the arrays() layout of another pool); returns
+        the index of the first."""
+        first = len(self.desc)
+        d = np.asarray(arrays["desc"], np.int64).reshape(-1, 6)
+        for k in range(len(d)):
+            v0, nv, e0, ne, f0, nf = (int(x) for x in d[k])
+            self._add(arrays["verts"][3 * v0:3 * (v0 + nv)], arrays["edges"][5 * e0:5 * (e0 + ne)],
+                      arrays["faces"][f0:f0 + nf], arrays["planes"][4 * f0:4 * (f0 + nf)],
+                      arrays["centroids"][3 * k:3 * k + 3], (nv, ne, nf))
+        return first
 
     def arrays(self):
         cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0, dt), dtype=dt)
@@ -551,4 +565,184 @@ def mesh_terrain_scene(seed=5, n=800, grid=14, spacing=1.5, height=4.0, scale=(1
                 except ValueError:
                     continue
             s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=hh)
+    return s
+
+
+# ---------------------------------------------------------------------------
+# Hull-heavy pile over a mesh ground.
+
+
+def sines_heights(X, Z, seed, amplitude=2.0):
+    """Heights of a sum of 4 seeded sines whose amplitudes add up to
+    `amplitude` (wavelengths 12-60 m, random directions and phases)."""
+    rng = np.random.default_rng(seed)
+    h = np.zeros(np.broadcast(X, Z).shape, dtype=np.float64)
+    for _ in range(4):
+        ang = rng.uniform(0, 2 * np.pi)
+        k = 2 * np.pi / rng.uniform(12.0, 60.0)
+        h += (amplitude / 4.0) * np.sin(k * (np.cos(ang) * X + np.sin(ang) * Z) + rng.uniform(0, 2 * np.pi))
+    return h
+
+
+def sines_mesh(n, spacing, seed, amplitude=2.0):
+    """An n x n vertex grid mesh (2 triangles per cell, counter-clockwise from
+    +y) with sines_heights: returns (vertices (n*n, 3), triangles)."""
+    xs = (np.arange(n) - (n - 1) / 2.0) * spacing
+    X, Z = np.meshgrid(xs, xs, indexing="ij")
+    V = np.stack([X, sines_heights(X, Z, seed, amplitude), Z], axis=-1).astype(F).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="ij")
+    a, b, c, d = i * n + j, (i + 1) * n + j, (i + 1) * n + j + 1, i * n + j + 1
+    tris = np.stack([np.stack([a, d, c], -1), np.stack([a, c, b], -1)], axis=2).reshape(-1, 3)
+    return V, tris.astype(np.int64)
+
+
+def _pile_hull_chunk(job):
+    """Worker: quickhulls of m ~ U{lo..hi} points on ellipsoids with
+    semi-axes ~ U[alo, ahi] (seeded per chunk); returns packed arrays."""
+    seed, count, pts, axes = job
+    rng = np.random.default_rng(seed)
+    pool = HullPool()
+    while len(pool) < count:
+        m = int(rng.integers(pts[0], pts[1] + 1))
+        ax = rng.uniform(axes[0], axes[1], 3)
+        try:
+            pool.add_points(ellipsoid_points(rng, m, ax))
+        except ValueError:
+            continue
+    return pool.arrays()
+
+
+def _padded_hulls(desc, verts, planes, idx, quats, vmax, fmax):
+    """Rotated vertices (m, vmax, 3) and planes (m, fmax, 4) of hulls idx
+    (float64), padding masked out: padded vertices repeat vertex 0 and padded
+    planes are (0, 0, 0, +inf), which never bind."""
+    m = len(idx)
+    W = np.empty((m, vmax, 3))
+    P = np.zeros((m, fmax, 4))
+    P[:, :, 3] = np.inf
+    for r, k in enumerate(idx):
+        v0, nv, f0, nf = int(desc[k, 0]), int(desc[k, 1]), int(desc[k, 4]), int(desc[k, 5])
+        W[r, :nv] = verts[v0:v0 + nv]
+        W[r, nv:] = verts[v0]
+        P[r, :nf] = planes[f0:f0 + nf]
+    q = quats[idx][:, None, :]
+    W = quat_rotate(np.broadcast_to(q, (m, vmax, 4)).astype(F), W.astype(F)).astype(np.float64)
+    P[:, :, :3] = quat_rotate(np.broadcast_to(q, (m, fmax, 4)).astype(F), P[:, :, :3].astype(F))
+    return W, P
+
+
+def _profile(P, dy, X, Z):
+    """Vertical lines at (X, Z) (m, k) through hulls with planes P (m, f, 4)
+    lifted by dy (m): bottom, top (m, k) and whether each line hits."""
+    n = P[:, None, :, :3]
+    off = (P[:, None, :, 3] + P[:, None, :, 1] * dy[:, None, None]) - (X[:, :, None] * n[..., 0] + Z[:, :, None] * n[..., 2])
+    ny = np.broadcast_to(n[..., 1], off.shape)
+    up, down = ny > 1e-6, ny < -1e-6
+    side = ~(up | down)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ratio = off / np.where(up | down, ny, 1.0)
+    top = np.min(np.where(up, ratio, np.inf), axis=2)
+    bot = np.max(np.where(down, ratio, -np.inf), axis=2)
+    hit = (bot <= top) & np.all(~side | (off >= -1e-9), axis=2)
+    return bot, top, hit
+
+
+def _clearances(Wl, Pl, yl, Wu, Pu, yu):
+    """Vertical clearance between lower hulls (Wl, Pl at heights yl) and the
+    upper hulls above them (Wu, Pu at yu), from each hull's vertices against
+    the other's surface; +inf where no vertex lies over the other hull."""
+    _, top, hit = _profile(Pl, yl, Wu[..., 0], Wu[..., 2])
+    c1 = np.min(np.where(hit, (Wu[..., 1] + yu[:, None]) - top, np.inf), axis=1)
+    bot, _, hit = _profile(Pu, yu, Wl[..., 0], Wl[..., 2])
+    c2 = np.min(np.where(hit, bot - (Wl[..., 1] + yl[:, None]), np.inf), axis=1)
+    return np.minimum(c1, c2)
+
+
+def _pile_columns(job):
+    """Worker: builds the hulls of a chunk of columns (seeded per chunk) and
+    stacks them level by level; returns (packed hull arrays, heights
+    (columns, per_column))."""
+    hull_seed, per_column, cx, cz, quats, gap, seed, amplitude, pts, axes = job
+    m = len(cx)
+    arrays = _pile_hull_chunk((hull_seed, m * per_column, pts, axes))
+    desc = arrays["desc"].reshape(-1, 6)
+    verts = arrays["verts"].reshape(-1, 3)
+    planes = arrays["planes"].reshape(-1, 4).astype(np.float64)
+    vmax, fmax = int(desc[:, 1].max()), int(desc[:, 5].max())
+    ys = np.empty((m, per_column))
+    below = None
+    for lv in range(per_column):
+        idx = np.arange(m) * per_column + lv
+        W, P = _padded_hulls(desc, verts, planes, idx, quats, vmax, fmax)
+        if below is None:
+            # the lowest vertex clears the terrain below it by `gap`
+            gh = sines_heights(cx[:, None] + W[..., 0], cz[:, None] + W[..., 2], seed, amplitude)
+            y = np.max(gh - W[..., 1], axis=1) + gap
+        else:
+            # first above the lower hull's highest vertex, then lowered until
+            # the hulls are `gap` apart along the vertical
+            Wl, Pl, yl = below
+            y = yl + Wl[..., 1].max(axis=1) + gap - W[..., 1].min(axis=1)
+            cl = _clearances(Wl, Pl, yl, W, P, y)
+            y = np.where(np.isfinite(cl) & (cl > gap), y - (cl - gap), y)
+        ys[:, lv] = y
+        below = (W, P, y)
+    return arrays, ys
+
+
+def pile_scene(seed=9, columns=512, per_column=512, grid=512, spacing=0.5, amplitude=2.0, gap=1e-3,
+               column_pitch=7.5, settle=0.03, jitter=0.01, spin=0.05, pts=(12, 64), axes=(0.3, 1.0),
+               chunk_columns=8, workers=None):
+    """Hull-heavy dense pile: columns x per_column distinct convex hulls
+    (quickhulls of 12-64 points on ellipsoids, semi-axes U[0.3, 1.0] m,
+    random orientation) stacked in vertical columns with `gap` m of vertical
+    clearance between neighbours, over a static mesh ground (a grid x grid
+    vertex sines terrain at `spacing` m). Hull building and stacking run in
+    spawned workers, chunk_columns columns each; the scene depends on the
+    chunk size, not on the worker count.
+
+    Motion: the pile settles. The hull at level i of its column moves down at
+    settle * i m/s (neighbours close at `settle` m/s, so the gaps close within
+    the first passes and the stack then stays in contact), plus N(0, jitter)
+    m/s and N(0, spin) rad/s."""
+    import multiprocessing as mp
+
+    rng = np.random.default_rng(seed)
+    n = columns * per_column
+    s = Scene()
+    V, T = sines_mesh(grid, spacing, seed, amplitude)
+    s.mesh_arrays = dict(desc=np.array([0, len(V), 0, len(T)], np.uint32),
+                         verts=np.ascontiguousarray(V.reshape(-1), F),
+                         tris=np.ascontiguousarray(T.reshape(-1), np.uint32))
+    g = s.add_body(0, N.BODY_STATIC, (0, 0, 0), (0, 0, 0, 1))
+    s.add_fixture(g, N.SHAPE_MESH, [1.0, 1.0, 1.0, 0.0], hull=0)
+    cols = int(np.ceil(np.sqrt(columns / 2.0)))
+    rows = (columns + cols - 1) // cols
+    quats = random_quats(rng, n)
+    lin = rng.normal(0, jitter, (n, 3))
+    lin[:, 1] -= settle * np.tile(np.arange(per_column), columns)
+    lin = lin.astype(F)
+    ang = rng.normal(0, spin, (n, 3)).astype(F)
+    ci = np.arange(columns)
+    cx = (ci % cols - (cols - 1) / 2.0) * column_pitch
+    cz = (ci // cols - (rows - 1) / 2.0) * column_pitch
+    jobs = []
+    for j, c0 in enumerate(range(0, columns, chunk_columns)):
+        c1 = min(columns, c0 + chunk_columns)
+        jobs.append((seed * 100003 + j, per_column, cx[c0:c1], cz[c0:c1],
+                     quats[c0 * per_column:c1 * per_column], gap, seed, amplitude, pts, axes))
+    workers = workers or min(len(jobs), os.cpu_count() or 1)
+    if workers <= 1:
+        parts = [_pile_columns(jb) for jb in jobs]
+    else:
+        with mp.get_context("spawn").Pool(workers) as p:
+            parts = p.map(_pile_columns, jobs)
+    ys = np.concatenate([y for _, y in parts])
+    for arrays, _ in parts:
+        s.hulls.extend(arrays)
+    for c in range(columns):
+        for lv in range(per_column):
+            k = c * per_column + lv
+            b = s.add_body(0, N.BODY_DYNAMIC, (cx[c], ys[c, lv], cz[c]), quats[k], lin[k], ang[k])
+            s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=k)
     return s

@@ -76,3 +76,28 @@ def test_mesh_terrain_passes_match_reference(oracle_mod, scale):
     assert {(4, 0), (4, 1), (3, 4)} <= kinds, kinds
     assert multi > 0
     pipe.close()
+
+
+def test_hull_pile_passes_match_reference(oracle_mod):
+    """A small hull-heavy pile (hulls of 12-64 vertices stacked in columns over
+    a sines mesh ground) settling for 10 passes."""
+    sc = S.pile_scene(seed=4, columns=4, per_column=64, grid=48).finalize()
+    rw = oracle_mod.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    touching = []
+    for k in range(10):
+        if k:
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass()
+        else:
+            rw.first_pass()
+        pipe.collide(drv.state17())
+        assert pipe.counts()["status"] == 0
+        compare_fat_aabbs(pipe, rw, f"pile pass {k}")
+        touching.append(compare_contacts(pipe, rw, f"pile pass {k}")["touching"])
+        compare_order(pipe, rw, f"pile pass {k}")
+    assert touching[-1] > 150, touching
+    pipe.close()
