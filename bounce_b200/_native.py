@@ -109,6 +109,7 @@ EXPORTED = [
     "b3g_fetch_caches",
     "b3g_fetch_fat_aabbs",
     "b3g_load_impulses",
+    "b3g_load_mesh_impulses",
     "b3g_device_results",
     "b3g_get_totals",
     "b3g_set_profiling",
@@ -169,6 +170,7 @@ def load():
         "b3g_fetch_caches": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_fat_aabbs": ([ctx, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_load_impulses": ([ctx, f32p, f32p, f32p], ctypes.c_int),
+        "b3g_load_mesh_impulses": ([ctx, f32p, f32p, f32p], ctypes.c_int),
         "b3g_device_results": ([ctx, _p(ctypes.c_void_p), _p(ctypes.c_void_p)], ctypes.c_int),
         "b3g_get_totals": ([ctx, _p(ctypes.c_uint64), ctypes.c_int], ctypes.c_int),
         "b3g_set_profiling": ([ctx, ctypes.c_int], ctypes.c_int),

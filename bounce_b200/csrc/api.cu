@@ -1615,6 +1615,53 @@ extern "C" int b3g_load_impulses(b3g_ctx* c, const float* normal, const float* t
 	return B3G_OK;
 }
 
+namespace {
+
+// Writes the host solver's impulses into manifolds 1 and 2 of each mesh
+// contact of the last pass; the next pass's warm start reads them there as
+// b3Manifold::Initialize(old) reads the old manifolds (collision.cpp:40-61).
+__global__ void k_load_extra_impulses(DevManifold* extra, const uint32_t* cstate, uint32_t n, const float* normal,
+	const float* tangent, const float* motor)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n)
+		return;
+	uint32_t mc = (cstate[c] >> 8) & 0xFFu;
+	for (uint32_t k = 0; k + 1 < mc && k < 2; ++k)
+	{
+		DevManifold& m = extra[2 * (size_t)c + k];
+		m.tangentImpulse[0] = tangent[4 * (size_t)c + 2 * k];
+		m.tangentImpulse[1] = tangent[4 * (size_t)c + 2 * k + 1];
+		m.motorImpulse = motor[2 * (size_t)c + k];
+		for (uint32_t j = 0; j < m.pointCount && j < 4; ++j)
+			m.points[j].normalImpulse = normal[8 * (size_t)c + 4 * k + j];
+	}
+}
+
+} // namespace
+
+extern "C" int b3g_load_mesh_impulses(b3g_ctx* c, const float* normal, const float* tangent, const float* motor)
+{
+	if (!c || !normal || !tangent || !motor)
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	Buffers& B = c->buf;
+	if (n == 0 || !B.extraMan[c->cur])
+		return B3G_OK;
+	float* dn = B.meshImpulses; // 14 floats per contact slot
+	float* dt = dn + 8 * (size_t)n;
+	float* dm = dt + 4 * (size_t)n;
+	CK(cudaMemcpyAsync(dn, normal, sizeof(float) * 8 * n, cudaMemcpyHostToDevice, c->stream));
+	CK(cudaMemcpyAsync(dt, tangent, sizeof(float) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+	CK(cudaMemcpyAsync(dm, motor, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, c->stream));
+	k_load_extra_impulses<<<(n + 255) / 256, 256, 0, c->stream>>>(B.extraMan[c->cur], B.cstate[c->cur], n, dn, dt, dm);
+	CK(cudaStreamSynchronize(c->stream));
+	return B3G_OK;
+}
+
 extern "C" int b3g_device_results(b3g_ctx* c, const void** contacts, const void** manifolds)
 {
 	if (!c || !contacts || !manifolds)

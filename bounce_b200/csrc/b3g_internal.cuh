@@ -209,6 +209,7 @@ struct Buffers
 	DevManifold* meshPairMan; // ... its b3Manifold (triangleKey set)
 	float4* meshObs;          // 3 per point slot of a work item: cluster observations
 	float4* meshPoly;         // 1 per point slot: a cluster's polygon vertices
+	float* meshImpulses;      // 14 per contact: host impulses of manifolds 1 and 2
 	uint32_t meshPairCap;
 
 	// wake-ups of UpdateContacts (only when some body is asleep)

@@ -190,6 +190,7 @@ void free_mesh(b3g_ctx* c)
 	mesh_free(B.meshPairMan);
 	mesh_free(B.meshObs);
 	mesh_free(B.meshPoly);
+	mesh_free(B.meshImpulses);
 	B.meshPairCap = 0;
 	c->nMeshes = 0;
 	c->hMeshes.clear();
@@ -291,7 +292,8 @@ extern "C" int b3g_set_meshes(b3g_ctx* c, uint32_t nm, const uint32_t* desc, con
 			mesh_alloc(&B.meshPairT, B.meshPairCap) == cudaSuccess &&
 			mesh_alloc(&B.meshPairMan, B.meshPairCap) == cudaSuccess &&
 			mesh_alloc(&B.meshObs, 3 * 4 * (size_t)B.meshPairCap) == cudaSuccess &&
-			mesh_alloc(&B.meshPoly, 4 * (size_t)B.meshPairCap) == cudaSuccess;
+			mesh_alloc(&B.meshPoly, 4 * (size_t)B.meshPairCap) == cudaSuccess &&
+			mesh_alloc(&B.meshImpulses, 14 * C) == cudaSuccess;
 	}
 	if (!ok)
 	{

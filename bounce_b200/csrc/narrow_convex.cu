@@ -808,6 +808,17 @@ __global__ void k_inactive(NPArgs a)
 			a.cstate[c] = a.prevState[prev] & ~(1u << 16);
 			a.cache[c] = a.prevCache[prev];
 			a.man[c] = a.prevMan[prev];
+			if (a.impN && ((a.prevState[prev] >> 8) & 0xFFu) > 0)
+			{
+				// The host solver's impulses live in the skipped contact's
+				// manifold as it does in the reference's.
+				DevManifold& m = a.man[c];
+				m.tangentImpulse[0] = a.impT[2 * prev + 0];
+				m.tangentImpulse[1] = a.impT[2 * prev + 1];
+				m.motorImpulse = a.impM[prev];
+				for (uint32_t j = 0; j < m.pointCount && j < 4; ++j)
+					m.points[j].normalImpulse = a.impN[4 * prev + j];
+			}
 			if (a.extraCur && ((a.prevState[prev] >> 8) & 0xFFu) > 1)
 			{
 				a.extraCur[2 * (size_t)c] = a.extraPrev[2 * (size_t)prev];

@@ -159,6 +159,14 @@ class CollisionPipeline:
         m = np.ascontiguousarray(motor, np.float32)
         self._check(self.lib.b3g_load_impulses(self.ctx, N.ptr(n, f32), N.ptr(t, f32), N.ptr(m, f32)))
 
+    def load_mesh_impulses(self, normal, tangent, motor):
+        """Impulses of manifolds 1 and 2 per contact: normal (n, 2, 4),
+        tangent (n, 2, 2), motor (n, 2)."""
+        n = np.ascontiguousarray(normal, np.float32)
+        t = np.ascontiguousarray(tangent, np.float32)
+        m = np.ascontiguousarray(motor, np.float32)
+        self._check(self.lib.b3g_load_mesh_impulses(self.ctx, N.ptr(n, f32), N.ptr(t, f32), N.ptr(m, f32)))
+
     def totals(self, reset=False):
         """Cumulative device counters: passes, contacts, manifolds, points, begun, ended."""
         out = np.zeros(8, np.uint64)

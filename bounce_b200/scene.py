@@ -573,14 +573,14 @@ def mesh_terrain_scene(seed=5, n=800, grid=14, spacing=1.5, height=4.0, scale=(1
 
 
 def sines_heights(X, Z, seed, amplitude=2.0):
-    """Heights of a sum of 4 seeded sines whose amplitudes add up to
-    `amplitude` (wavelengths 12-60 m, random directions and phases)."""
+    """Heights sum_k a_k sin(f_k x + p_k) sin(g_k z + q_k) over 4 seeded
+    terms whose amplitudes a_k add up to `amplitude` (wavelengths 12-60 m)."""
     rng = np.random.default_rng(seed)
     h = np.zeros(np.broadcast(X, Z).shape, dtype=np.float64)
     for _ in range(4):
-        ang = rng.uniform(0, 2 * np.pi)
-        k = 2 * np.pi / rng.uniform(12.0, 60.0)
-        h += (amplitude / 4.0) * np.sin(k * (np.cos(ang) * X + np.sin(ang) * Z) + rng.uniform(0, 2 * np.pi))
+        f, g = 2 * np.pi / rng.uniform(12.0, 60.0, 2)
+        p, q = rng.uniform(0, 2 * np.pi, 2)
+        h += (amplitude / 4.0) * np.sin(f * X + p) * np.sin(g * Z + q)
     return h
 
 

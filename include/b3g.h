@@ -300,6 +300,14 @@ int b3g_fetch_fat_aabbs(b3g_ctx* ctx, float* out, uint32_t capacity);
 int b3g_load_impulses(b3g_ctx* ctx, const float* normal_impulse, const float* tangent_impulse,
 	const float* motor_impulse);
 
+/* The same for manifolds 1 and 2 of mesh contacts (b3MeshContact keeps up to
+ * B3_MAX_MANIFOLDS = 3, mesh_contact.h:61): per contact in contact order 8
+ * normal impulses (4 per manifold), 4 tangent and 2 motor impulses; entries of
+ * manifolds a contact does not have are ignored. Call after the pass, before
+ * the next b3g_collide; manifold 0 comes from b3g_load_impulses. */
+int b3g_load_mesh_impulses(b3g_ctx* ctx, const float* normal_impulse, const float* tangent_impulse,
+	const float* motor_impulse);
+
 /* Cumulative counters since creation or the last reset: out[0] passes,
  * out[1] contacts, out[2] manifolds with points, out[3] manifold points,
  * out[4] contacts created, out[5] contacts destroyed, out[6] CUDA kernels the

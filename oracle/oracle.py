@@ -234,6 +234,16 @@ class RefWorld:
     def contact_count(self):
         return self.L.refw_contact_count(self.w)
 
+    def load_impulses(self, normal, tangent, motor):
+        """The solver's impulses for every contact in list order, per manifold
+        (B3_MAX_MANIFOLDS = 3): normal (n, 3, 4), tangent (n, 3, 2), motor (n, 3)."""
+        n = self.contact_count()
+        rec = np.zeros(max(n, 1), DCONTACT)
+        rec["manifolds"]["points"]["normalImpulse"][:n] = np.asarray(normal, np.float64)[:n]
+        rec["manifolds"]["tangentImpulse"][:n] = np.asarray(tangent, np.float64)[:n]
+        rec["manifolds"]["motorImpulse"][:n] = np.asarray(motor, np.float64)[:n]
+        self.L.refw_load_impulses(self.w, ctypes.c_void_p(rec.ctypes.data))
+
     def touching(self):
         m, p = ctypes.c_uint32(), ctypes.c_uint32()
         t = self.L.refw_touching_count(self.w, ctypes.byref(m), ctypes.byref(p))

@@ -72,7 +72,16 @@ def _compare_points(gm, rm, gpc, label):
     assert np.array_equal(gm["points"]["persisting"][mask], rm["points"]["persisting"][mask].astype(np.uint8)), (
         f"{label}: persisting flags differ"
     )
-    assert np.array_equal(gm["points"]["normalImpulse"][mask], rm["points"]["normalImpulse"][mask].astype(np.float32))
+    assert np.array_equal(gm["points"]["normalImpulse"][mask], rm["points"]["normalImpulse"][mask].astype(np.float32)), (
+        f"{label}: normal impulses differ"
+    )
+    has = gpc > 0
+    assert np.array_equal(gm["tangentImpulse"][has], rm["tangentImpulse"][has].astype(np.float32)), (
+        f"{label}: tangent impulses differ"
+    )
+    assert np.array_equal(gm["motorImpulse"][has], rm["motorImpulse"][has].astype(np.float32)), (
+        f"{label}: motor impulses differ"
+    )
 
 
 def compare_all_manifolds(pipe, rc, ref_of_gpu, label=""):

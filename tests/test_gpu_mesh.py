@@ -101,3 +101,40 @@ def test_hull_pile_passes_match_reference(oracle_mod):
         compare_order(pipe, rw, f"pile pass {k}")
     assert touching[-1] > 150, touching
     pipe.close()
+
+
+def test_warm_start_from_solver_impulses(oracle_mod):
+    """Impulses handed back after each pass (b3g_load_impulses for manifold 0,
+    b3g_load_mesh_impulses for manifolds 1 and 2) warm-start the next pass's
+    matching points exactly as in the reference, on convex, hull and mesh
+    contacts."""
+    sc = S.mesh_terrain_scene(seed=8, n=500).finalize()
+    rw = oracle_mod.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    rng = np.random.default_rng(1)
+    persisting = 0
+    for k in range(8):
+        if k:
+            n = pipe.counts()["contacts"]
+            assert n == rw.contact_count()
+            normal = rng.uniform(0, 5, (n, 3, 4)).astype(np.float32)
+            tangent = rng.uniform(-1, 1, (n, 3, 2)).astype(np.float32)
+            motor = rng.uniform(-1, 1, (n, 3)).astype(np.float32)
+            rw.load_impulses(normal, tangent, motor)
+            pipe.load_impulses(normal[:, 0], tangent[:, 0], motor[:, 0])
+            pipe.load_mesh_impulses(normal[:, 1:], tangent[:, 1:], motor[:, 1:])
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass()
+        else:
+            rw.first_pass()
+        pipe.collide(drv.state17())
+        assert pipe.counts()["status"] == 0
+        compare_contacts(pipe, rw, f"warm pass {k}")
+        compare_order(pipe, rw, f"warm pass {k}")
+        _, man = pipe.touching()
+        persisting += int(np.sum(man["points"]["persisting"]))
+    assert persisting > 100
+    pipe.close()

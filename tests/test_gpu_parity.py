@@ -100,7 +100,7 @@ def test_list_order(oracle_mod):
     pipe.close()
 
 
-def run_sleeping(O, sc, passes, label, seed, sleep_frac):
+def run_sleeping(O, sc, passes, label, seed, sleep_frac, impulses=False):
     """Sleep as the reference's solver produces it: the bodies awake after a
     pass (wake-ups included) move in the next one, a random part of them falls
     asleep right after moving (synchronised, then asleep for UpdateContacts),
@@ -115,6 +115,14 @@ def run_sleeping(O, sc, passes, label, seed, sleep_frac):
     woken_total = 0
     for k in range(passes):
         if k:
+            if impulses:
+                # the solver's impulses handed back for every contact
+                n = pipe.counts()["contacts"]
+                normal = rng.uniform(0, 5, (n, 3, 4)).astype(np.float32)
+                tangent = rng.uniform(-1, 1, (n, 3, 2)).astype(np.float32)
+                motor = rng.uniform(-1, 1, (n, 3)).astype(np.float32)
+                rw.load_impulses(normal, tangent, motor)
+                pipe.load_impulses(normal[:, 0], tangent[:, 0], motor[:, 0])
             drv.advance(moved)
             awake = moved & (rng.random(sc.n_bodies) > sleep_frac).astype(np.uint8)
             rw.set_sweeps(drv.sweeps14())
@@ -146,6 +154,13 @@ def test_mixed_sleeping(oracle_mod):
     sc = S.mixed_scene(seed=9, n=1500, side=14.0, static_frac=0.1, sensor_frac=0.05).finalize()
     woken = run_sleeping(oracle_mod, sc, 8, "sleep", seed=100, sleep_frac=0.3)
     assert woken > 0
+
+
+def test_sleeping_with_solver_impulses(oracle_mod):
+    """Impulses handed back by the host solver warm-start the contacts that
+    run and stay in the manifolds of the contacts UpdateContacts skips."""
+    sc = S.mixed_scene(seed=21, n=1500, side=14.0, static_frac=0.1, sensor_frac=0.05).finalize()
+    run_sleeping(oracle_mod, sc, 6, "sleep-impulses", seed=5, sleep_frac=0.5, impulses=True)
 
 
 def test_mostly_sleeping(oracle_mod):
