@@ -62,7 +62,9 @@ def parse():
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
     ap.add_argument("--worlds", type=int, default=1024)
-    ap.add_argument("--autotune", action="store_true", default=True)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default launch shapes instead of measuring them")
+    ap.add_argument("--max-contacts", type=int, default=0, help="contact capacity (0: sized from the workload)")
     args = ap.parse_args()
     if args.workload in ("batched", "pile"):
         # The batched and pile workloads are quoted on 30 steps.
@@ -279,7 +281,7 @@ def run_ours(args, rank, world, local, dist):
         drv.advance()
         states[k] = drv.state17()
     d_states = torch.from_numpy(states[:n_dev]).to(dev)
-    max_contacts = 4 * nb if pile else max(2_000_000, 40 * nb)
+    max_contacts = args.max_contacts or (4 * nb if pile else max(2_000_000, 40 * nb))
     pipe = CollisionPipeline(scene, max_contacts=max_contacts, device=local, graph=not args.no_graph)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream

@@ -377,7 +377,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.refitFlag, P), "alloc");
 	step(dalloc(&B.worldEnd, P), "alloc");
 	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
-	step(dalloc(&B.pairScratch, 2 * 16 * (size_t)P), "alloc"); // 16 uint2 records per leaf
+	step(dalloc(&B.pairScratch, 2 * B3G_TRAV_SLOTS * (size_t)P), "alloc"); // uint2 records per leaf
 	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
 	for (int k = 0; k < 2; ++k)
 	{
@@ -1342,7 +1342,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	// pass_begin, sync, broadphase, diff + list order, bucket + convex kernels + 2 hull + hull-triangle,
 	// finalize + pass_end + settle
 	const uint32_t passLaunches = 1 + 2 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
-		pairs_diff_launches(c) + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
+		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
 		c->havePass && !c->creationPass && s != nullptr;
 	c->lastPassImpulses = c->impulsesLoaded;

@@ -30,6 +30,7 @@ enum Bucket : uint32_t
 	BK_MESH,             // b3MeshContact subclasses (mesh-sphere, mesh-capsule, hull-mesh), sensors included
 	BK_SENSOR,           // any other pair with a sensor: b3Contact::TestOverlap path
 	BK_INACTIVE,         // both bodies asleep or static: state carried over
+	BK_APART,            // convex pairs whose bounding spheres are apart: empty manifold
 	BK_COUNT
 };
 
@@ -164,7 +165,7 @@ struct Buffers
 	uint32_t* refitFlag;
 	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
-	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (16 x n uint2)
+	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (B3G_TRAV_SLOTS x n uint2)
 	uint32_t* scanAux;
 	uint32_t* rawA;       // overlapping pairs in traversal order (this pass)
 	uint32_t* rawB;
@@ -225,6 +226,10 @@ struct Buffers
 	float* impulseMotor;
 };
 
+// Contact records a leaf's walk keeps in its scratch slots; leaves with more
+// partners walk again for the rest.
+#define B3G_TRAV_SLOTS 32u
+
 // Counter slots in Buffers::counters.
 enum
 {
@@ -245,9 +250,9 @@ enum
 	CTR_WAKE_ACTIVATED,
 	CTR_LATE_DESTROYED,
 	CTR_BUCKET0 = 16,   // BK_COUNT bucket sizes
-	CTR_ASLEEP = 28,    // non-static bodies still asleep after the wake-ups
-	CTR_SCRATCH = 29,
-	CTR_MESH_PAIRS = 30, // (contact, triangle) work items of the pass
+	CTR_ASLEEP = 29,    // non-static bodies still asleep after the wake-ups
+	CTR_SCRATCH = 30,
+	CTR_MESH_PAIRS = 31, // (contact, triangle) work items of the pass
 	CTR_COUNT = 32
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");

@@ -28,25 +28,92 @@ namespace {
 constexpr uint32_t SENT = 0xFFFFFFFFu;
 
 
+// Lanes per fixture in k_sync: a hull's vertex loop is split across them.
+constexpr uint32_t SYNC_LANES = 8;
+
+__device__ __forceinline__ V3 shfl_xor3(uint32_t mask, V3 v, int o)
+{
+	return V3{__shfl_xor_sync(mask, v.x, o), __shfl_xor_sync(mask, v.y, o), __shfl_xor_sync(mask, v.z, o)};
+}
+
+// compute_aabbs for the lanes of one group: a hull's vertices are strided
+// over the lanes and the boxes combined by min / max, which are exact, so the
+// result is the serial loop's (b3HullShape::ComputeAABB, hull_shape.cpp:160-164).
+// Every lane of the group ends with the same boxes.
+__device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb, bool two,
+	AABB& a, AABB& b, uint32_t lane, uint32_t mask)
+{
+	if (S.fixType[fix] != B3G_SHAPE_HULL)
+	{
+		compute_aabbs(S, fix, xa, xb, two, a, b);
+		return;
+	}
+	const HullDesc h = S.hulls[S.fixHull[fix]];
+	const float4* hv = S.hverts + h.vOff;
+	float4 w = hv[0];
+	V3 v0 = V3{w.x, w.y, w.z};
+	V3 ta = xmul(xa, v0), tb = two ? xmul(xb, v0) : ta;
+	a.lo = a.hi = ta;
+	b.lo = b.hi = tb;
+	for (uint32_t k = 1 + lane; k < h.vCnt; k += SYNC_LANES)
+	{
+		w = hv[k];
+		V3 v = V3{w.x, w.y, w.z};
+		ta = xmul(xa, v);
+		a.lo = vmin(a.lo, ta);
+		a.hi = vmax(a.hi, ta);
+		if (two)
+		{
+			tb = xmul(xb, v);
+			b.lo = vmin(b.lo, tb);
+			b.hi = vmax(b.hi, tb);
+		}
+	}
+	for (int o = SYNC_LANES / 2; o > 0; o >>= 1)
+	{
+		a.lo = vmin(a.lo, shfl_xor3(mask, a.lo, o));
+		a.hi = vmax(a.hi, shfl_xor3(mask, a.hi, o));
+		if (two)
+		{
+			b.lo = vmin(b.lo, shfl_xor3(mask, b.lo, o));
+			b.hi = vmax(b.hi, shfl_xor3(mask, b.hi, o));
+		}
+	}
+	float r = S.fixParams[3 * fix].x;
+	aabb_extend(a, r);
+	if (two)
+		aabb_extend(b, r);
+}
+
+// One group of SYNC_LANES lanes per fixture; lane 0 writes. All lanes of a
+// group take the same branches, so the group mask is exact for the shuffles.
 __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 {
-	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= nf)
+	const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / SYNC_LANES;
+	const uint32_t lane = threadIdx.x % SYNC_LANES;
+	const uint32_t mask = ((1u << SYNC_LANES) - 1u) << ((threadIdx.x & 31u) & ~(SYNC_LANES - 1u));
+	if (g >= nf)
 		return;
+	const uint32_t i = g;
+	const bool w0 = lane == 0;
 	const uint8_t life = S.fixLife[i];
 	if (life == FIX_DEAD)
 	{
 		// No proxy: an empty box (lower > upper) that overlaps nothing.
-		B.fatLo[i] = make_float4(B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR, 0.0f);
-		B.fatHi[i] = make_float4(-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR, 0.0f);
-		B.moved[i] = 0;
+		if (w0)
+		{
+			B.fatLo[i] = make_float4(B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR, 0.0f);
+			B.fatHi[i] = make_float4(-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR, 0.0f);
+			B.moved[i] = 0;
+		}
 		return;
 	}
 	if (S.fixType[i] == B3G_SHAPE_MESH)
 	{
 		// Meshes sit on static bodies: their proxy is created once (k_mesh_fat
 		// on a creation pass) and never moves.
-		B.moved[i] = 0;
+		if (w0)
+			B.moved[i] = 0;
 		return;
 	}
 	uint32_t body = S.fixBody[i];
@@ -56,12 +123,15 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	{
 		// b3DynamicTree::CreateProxy (dynamic_tree.cpp:108-128).
 		AABB a, unused;
-		compute_aabbs(S, i, xf1, xf1, false, a, unused);
-		V3 r = V3{B3G_AABB_EXTENSION, B3G_AABB_EXTENSION, B3G_AABB_EXTENSION};
-		V3 lo = a.lo - r, hi = a.hi + r;
-		B.fatLo[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
-		B.fatHi[i] = make_float4(hi.x, hi.y, hi.z, 0.0f);
-		B.moved[i] = 1;
+		group_aabbs(S, i, xf1, xf1, false, a, unused, lane, mask);
+		if (w0)
+		{
+			V3 r = V3{B3G_AABB_EXTENSION, B3G_AABB_EXTENSION, B3G_AABB_EXTENSION};
+			V3 lo = a.lo - r, hi = a.hi + r;
+			B.fatLo[i] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+			B.fatHi[i] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+			B.moved[i] = 1;
+		}
 		return;
 	}
 	// Every non-static body is synchronised, whatever its awake flag:
@@ -73,7 +143,8 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	uint32_t btype = S.bodyType[body];
 	if (btype == B3G_BODY_STATIC)
 	{
-		B.moved[i] = 0;
+		if (w0)
+			B.moved[i] = 0;
 		return;
 	}
 	// b3Body::SynchronizeFixtures (body.cpp:216-229): xf0 from the sweep start.
@@ -85,7 +156,9 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 
 	// b3Fixture::Synchronize (fixture.cpp:120-132).
 	AABB a1, a2;
-	compute_aabbs(S, i, xf0, xf1, true, a1, a2);
+	group_aabbs(S, i, xf0, xf1, true, a1, a2, lane, mask);
+	if (!w0)
+		return;
 	AABB aabb;
 	aabb.lo = vmin(a1.lo, a2.lo);
 	aabb.hi = vmax(a1.hi, a2.hi);
@@ -517,7 +590,7 @@ __device__ __forceinline__ uint2 canon_pair(const DevScene& S, uint32_t pa, uint
 // TRAV_SLOTS from `base` (leaves whose partners did not fit). MW: several
 // worlds share the tree, so the walk stops at the first node past the query's
 // world (worlds are contiguous in depth-first order).
-constexpr uint32_t TRAV_SLOTS = 16;
+constexpr uint32_t TRAV_SLOTS = B3G_TRAV_SLOTS;
 
 template <int MODE, bool MW>
 __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cur, uint32_t cap,
@@ -672,7 +745,7 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 	if (n == 0)
 		return;
 	k_body_prep<<<(c->nBodies + 255) / 256, 256, 0, s>>>(c->scene, c->nBodies);
-	k_sync<<<(n + 127) / 128, 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
+	k_sync<<<(uint32_t)(((size_t)n * SYNC_LANES + 127) / 128), 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
 	if (c->creationPass)
 		launch_mesh_fat(c, s);
 }

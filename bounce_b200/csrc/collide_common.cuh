@@ -753,6 +753,29 @@ __device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& 
 	}
 }
 
+// Exact cull, not in the reference: every convex routine (sphere, capsule,
+// triangle-sphere/capsule, hull-sphere/capsule) returns no point when the
+// shapes are farther apart than their radii sum (the sphere
+// and capsule routines compare closest-point distances with the radii; the
+// hull routines' face loop or GJK, whose witness points lie on the shapes,
+// then report a distance above the radii). Bounding spheres (fixture-local
+// centre, conservative radius from b3g_set_fixtures) separated by more than
+// the radii plus a margin that dominates the FP32 rounding of those
+// distances (1e-3 m + 1e-5 of the coordinate magnitude) therefore mean an
+// empty manifold, and the routine can be skipped without changing the output.
+__device__ __forceinline__ bool spheres_apart(const DevScene& S, uint32_t fa, const XF& xfA, uint32_t fb,
+	const XF& xfB)
+{
+	float4 ba = S.fixBound[fa], bb = S.fixBound[fb];
+	V3 ca = xmul(xfA, V3{ba.x, ba.y, ba.z});
+	V3 cb = xmul(xfB, V3{bb.x, bb.y, bb.z});
+	V3 d = cb - ca;
+	float mag = fmaxf(fmaxf(fmaxf(fabsf(ca.x), fabsf(ca.y)), fabsf(ca.z)),
+		fmaxf(fmaxf(fabsf(cb.x), fabsf(cb.y)), fabsf(cb.z)));
+	float reach = (ba.w + bb.w) + (1e-3f + 1e-5f * mag);
+	return dot(d, d) > reach * reach;
+}
+
 // ---------------------------------------------------------------------------
 // Meshes.
 
@@ -858,6 +881,7 @@ __device__ __forceinline__ HullRef mesh_tri_ref(const MeshTri& t)
 
 void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
 	cudaStream_t s);
+void launch_apart(const NPArgs& a, const uint32_t* list, const uint32_t* count, cudaStream_t s);
 void launch_mesh_items_convex(const NPArgs& a, const Buffers& B, cudaStream_t s);
 void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s);
 

@@ -708,29 +708,9 @@ __device__ GProxy shape_proxy(const DevScene& S, const ShapeP& s)
 	return p;
 }
 
-// Contacts listed in one bucket, one thread each.
-// Exact cull, not in the reference: every routine of this file returns no
-// point when the shapes are farther apart than their radii sum (the sphere
-// and capsule routines compare closest-point distances with the radii; the
-// hull routines' face loop or GJK, whose witness points lie on the shapes,
-// then report a distance above the radii). Bounding spheres (fixture-local
-// centre, conservative radius from b3g_set_fixtures) separated by more than
-// the radii plus a margin that dominates the FP32 rounding of those
-// distances (1e-3 m + 1e-5 of the coordinate magnitude) therefore mean an
-// empty manifold, and the routine can be skipped without changing the output.
-__device__ __forceinline__ bool spheres_apart(const DevScene& S, uint32_t fa, const XF& xfA, uint32_t fb,
-	const XF& xfB)
-{
-	float4 ba = S.fixBound[fa], bb = S.fixBound[fb];
-	V3 ca = xmul(xfA, V3{ba.x, ba.y, ba.z});
-	V3 cb = xmul(xfB, V3{bb.x, bb.y, bb.z});
-	V3 d = cb - ca;
-	float mag = fmaxf(fmaxf(fmaxf(fabsf(ca.x), fabsf(ca.y)), fabsf(ca.z)),
-		fmaxf(fmaxf(fabsf(cb.x), fabsf(cb.y)), fabsf(cb.z)));
-	float reach = (ba.w + bb.w) + (1e-3f + 1e-5f * mag);
-	return dot(d, d) > reach * reach;
-}
-
+// Contacts listed in one bucket, one thread each (spheres_apart: the exact
+// cull of collide_common.cuh, repeated here for contacts that reach these
+// kernels without k_bucket, i.e. wake-ups and b3g_collide_pairs).
 template <int BUCKET>
 __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 {
@@ -792,6 +772,21 @@ __global__ void k_sensor(NPArgs a)
 		// with: e_empty (sat.h:69), the other fields unset.
 		bool hulls = a.S.fixType[fa] == B3G_SHAPE_HULL && a.S.fixType[fb] == B3G_SHAPE_HULL;
 		a.cache[c] = make_uint4(hulls ? 0u : B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+	}
+}
+
+// Convex contacts k_bucket found apart (spheres_apart): the routine would
+// return no point, so the manifold is empty; warm start and flags as in k_convex.
+__global__ void k_apart(NPArgs a)
+{
+	uint32_t n = *a.listCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.list[t];
+		DevManifold& m = a.man[c];
+		man_clear(m);
+		finish_convex(a, c, m);
+		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
 }
 
@@ -933,6 +928,14 @@ void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint
 {
 	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
 		launch_convex_one(k, base, lists, counts, cap, tune, s);
+}
+
+void launch_apart(const NPArgs& base, const uint32_t* list, const uint32_t* count, cudaStream_t s)
+{
+	NPArgs a = base;
+	a.list = list;
+	a.listCount = count;
+	k_apart<<<persistent_blocks(4), 128, 0, s>>>(a);
 }
 
 void launch_mesh_items_convex(const NPArgs& a, const Buffers& B, cudaStream_t s)

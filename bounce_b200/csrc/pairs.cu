@@ -73,6 +73,10 @@ __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 			bk = bucket_of(S.fixType[fa], S.fixType[fb]);
 		if (bk >= BK_COUNT)
 			bk = BK_INACTIVE;
+		// Convex pairs whose bounding spheres are apart skip their routine
+		// (spheres_apart); taking them out keeps the routines' warps full.
+		if (bk <= BK_HULL_CAPSULE && spheres_apart(S, fa, body_xf(S, ba), fb, body_xf(S, bb)))
+			bk = BK_APART;
 		// Warp-aggregated append.
 		uint32_t peers = __match_any_sync(__activemask(), bk);
 		uint32_t leader = __ffs(peers) - 1;
@@ -228,6 +232,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	launch_mesh_prepare(c, s);
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
 	NPArgs a = make_np_args(c);
+	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 	prof_mark(c, PM_CONVEX, s);
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
