@@ -1339,9 +1339,9 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-	// pass_begin, sync, broadphase, diff + list order, bucket + convex kernels + 2 hull + hull-triangle,
-	// finalize + pass_end + settle
-	const uint32_t passLaunches = 1 + 2 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
+	// pass_begin, sync, broadphase, diff + list order, bucket + apart + convex kernels + 2 hull +
+	// hull-triangle, finalize + pass_end + settle
+	const uint32_t passLaunches = 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
 		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
 		c->havePass && !c->creationPass && s != nullptr;

@@ -36,19 +36,57 @@ __device__ __forceinline__ V3 shfl_xor3(uint32_t mask, V3 v, int o)
 	return V3{__shfl_xor_sync(mask, v.x, o), __shfl_xor_sync(mask, v.y, o), __shfl_xor_sync(mask, v.z, o)};
 }
 
-// compute_aabbs for the lanes of one group: a hull's vertices are strided
-// over the lanes and the boxes combined by min / max, which are exact, so the
-// result is the serial loop's (b3HullShape::ComputeAABB, hull_shape.cpp:160-164).
-// Every lane of the group ends with the same boxes.
-__device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb, bool two,
-	AABB& a, AABB& b, uint32_t lane, uint32_t mask)
+// b3Shape::ComputeAABB at two transforms for the lanes of one group, from
+// the fixture's preloaded type and params (compute_aabbs's arithmetic): a
+// hull's vertices are strided over the lanes and the boxes combined by min /
+// max, which are exact, so the result is the serial loop's
+// (b3HullShape::ComputeAABB, hull_shape.cpp:160-164). Every lane of the
+// group ends with the same boxes.
+__device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t type, float4 p0, float4 p1, float4 p2,
+	uint32_t hullIndex, const XF& xa, const XF& xb, bool two, AABB& a, AABB& b, uint32_t lane, uint32_t mask)
 {
-	if (S.fixType[fix] != B3G_SHAPE_HULL)
+	if (type == B3G_SHAPE_SPHERE)
 	{
-		compute_aabbs(S, fix, xa, xb, two, a, b);
+		V3 c = V3{p0.x, p0.y, p0.z};
+		V3 rv = V3{p0.w, p0.w, p0.w};
+		V3 ca = xmul(xa, c);
+		a.lo = ca - rv;
+		a.hi = ca + rv;
+		V3 cb = two ? xmul(xb, c) : ca;
+		b.lo = cb - rv;
+		b.hi = cb + rv;
 		return;
 	}
-	const HullDesc h = S.hulls[S.fixHull[fix]];
+	if (type == B3G_SHAPE_CAPSULE)
+	{
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		V3 rv = V3{p1.z, p1.z, p1.z};
+		V3 c1 = xmul(xa, v1), c2 = xmul(xa, v2);
+		a.lo = vmin(c1, c2) - rv;
+		a.hi = vmax(c1, c2) + rv;
+		if (two)
+		{
+			c1 = xmul(xb, v1);
+			c2 = xmul(xb, v2);
+		}
+		b.lo = vmin(c1, c2) - rv;
+		b.hi = vmax(c1, c2) + rv;
+		return;
+	}
+	if (type == B3G_SHAPE_TRIANGLE)
+	{
+		// The reference ignores the transform here (triangle_shape.cpp:59-67).
+		V3 v1 = V3{p0.x, p0.y, p0.z};
+		V3 v2 = V3{p0.w, p1.x, p1.y};
+		V3 v3_ = V3{p1.z, p1.w, p2.x};
+		V3 rv = V3{p2.y, p2.y, p2.y};
+		a.lo = vmin(v1, vmin(v2, v3_)) - rv;
+		a.hi = vmax(v1, vmax(v2, v3_)) + rv;
+		b = a;
+		return;
+	}
+	const HullDesc h = S.hulls[hullIndex];
 	const float4* hv = S.hverts + h.vOff;
 	float4 w = hv[0];
 	V3 v0 = V3{w.x, w.y, w.z};
@@ -79,7 +117,7 @@ __device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t fix, con
 			b.hi = vmax(b.hi, shfl_xor3(mask, b.hi, o));
 		}
 	}
-	float r = S.fixParams[3 * fix].x;
+	float r = p0.x;
 	aabb_extend(a, r);
 	if (two)
 		aabb_extend(b, r);
@@ -87,16 +125,36 @@ __device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t fix, con
 
 // One group of SYNC_LANES lanes per fixture; lane 0 writes. All lanes of a
 // group take the same branches, so the group mask is exact for the shuffles.
-__global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
+// The per-body transforms of the pass (m_xf and b3Sweep::GetTransform(0),
+// sweep.h:43-63, two float4 each, read by the later stages) are written by
+// lane 1 of group b for body b. The fixture's records are loaded before any
+// branch so that their loads overlap.
+__global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int creation)
 {
 	const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / SYNC_LANES;
 	const uint32_t lane = threadIdx.x % SYNC_LANES;
 	const uint32_t mask = ((1u << SYNC_LANES) - 1u) << ((threadIdx.x & 31u) & ~(SYNC_LANES - 1u));
+	if (lane == 1 && g < nb)
+	{
+		pack_xf(S.bodyXf, g, load_xf(S.bodyState + 17 * (size_t)g));
+		pack_xf(S.bodyXf0, g, sweep_xf0(S, g));
+	}
 	if (g >= nf)
 		return;
 	const uint32_t i = g;
 	const bool w0 = lane == 0;
 	const uint8_t life = S.fixLife[i];
+	const uint32_t type = S.fixType[i];
+	const uint32_t body = S.fixBody[i];
+	const uint32_t hullIndex = S.fixHull[i];
+	const float4 p0 = S.fixParams[3 * i + 0], p1 = S.fixParams[3 * i + 1], p2 = S.fixParams[3 * i + 2];
+	const float4 tl = B.fatLo[i], th = B.fatHi[i];
+	const float* st = S.bodyState + 17 * (size_t)body;
+	float sv[17];
+#pragma unroll
+	for (int k = 0; k < 17; ++k)
+		sv[k] = st[k];
+	const uint32_t btype = S.bodyType[body];
 	if (life == FIX_DEAD)
 	{
 		// No proxy: an empty box (lower > upper) that overlaps nothing.
@@ -108,7 +166,7 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 		}
 		return;
 	}
-	if (S.fixType[i] == B3G_SHAPE_MESH)
+	if (type == B3G_SHAPE_MESH)
 	{
 		// Meshes sit on static bodies: their proxy is created once (k_mesh_fat
 		// on a creation pass) and never moves.
@@ -116,14 +174,12 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 			B.moved[i] = 0;
 		return;
 	}
-	uint32_t body = S.fixBody[i];
-	const float* st = S.bodyState + 17 * (size_t)body;
-	XF xf1 = load_xf(st);
+	XF xf1 = load_xf(sv);
 	if (creation || life == FIX_FRESH)
 	{
 		// b3DynamicTree::CreateProxy (dynamic_tree.cpp:108-128).
 		AABB a, unused;
-		group_aabbs(S, i, xf1, xf1, false, a, unused, lane, mask);
+		group_aabbs(S, type, p0, p1, p2, hullIndex, xf1, xf1, false, a, unused, lane, mask);
 		if (w0)
 		{
 			V3 r = V3{B3G_AABB_EXTENSION, B3G_AABB_EXTENSION, B3G_AABB_EXTENSION};
@@ -140,7 +196,6 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	// step (island.cpp:297-305). A body asleep since its last move keeps its
 	// sweep, so synchronising it again finds its AABB inside the fat AABB it
 	// got then and moves nothing: the result is the reference's, which skips it.
-	uint32_t btype = S.bodyType[body];
 	if (btype == B3G_BODY_STATIC)
 	{
 		if (w0)
@@ -149,14 +204,14 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	}
 	// b3Body::SynchronizeFixtures (body.cpp:216-229): xf0 from the sweep start.
 	XF xf0;
-	xf0.q = Q4{V3{st[10], st[11], st[12]}, st[13]};
-	V3 c0 = V3{st[7], st[8], st[9]};
-	V3 lc = V3{st[14], st[15], st[16]};
+	xf0.q = Q4{V3{sv[10], sv[11], sv[12]}, sv[13]};
+	V3 c0 = V3{sv[7], sv[8], sv[9]};
+	V3 lc = V3{sv[14], sv[15], sv[16]};
 	xf0.p = c0 - rot(xf0.q, lc);
 
 	// b3Fixture::Synchronize (fixture.cpp:120-132).
 	AABB a1, a2;
-	group_aabbs(S, i, xf0, xf1, true, a1, a2, lane, mask);
+	group_aabbs(S, type, p0, p1, p2, hullIndex, xf0, xf1, true, a1, a2, lane, mask);
 	if (!w0)
 		return;
 	AABB aabb;
@@ -181,7 +236,6 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	else
 		fat.hi.z += d.z;
 
-	float4 tl = B.fatLo[i], th = B.fatHi[i];
 	AABB tree;
 	tree.lo = V3{tl.x, tl.y, tl.z};
 	tree.hi = V3{th.x, th.y, th.z};
@@ -198,17 +252,6 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, int creation)
 	B.fatLo[i] = make_float4(fat.lo.x, fat.lo.y, fat.lo.z, 0.0f);
 	B.fatHi[i] = make_float4(fat.hi.x, fat.hi.y, fat.hi.z, 0.0f);
 	B.moved[i] = 1;
-}
-
-// Per-body transforms used by the narrowphase, computed once per pass:
-// m_xf and b3Sweep::GetTransform(0) (sweep.h:43-63).
-__global__ void k_body_prep(DevScene S, uint32_t nb)
-{
-	uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-	if (b >= nb)
-		return;
-	pack_xf(S.bodyXf, b, load_xf(S.bodyState + 17 * (size_t)b));
-	pack_xf(S.bodyXf0, b, sweep_xf0(S, b));
 }
 
 // ---------------------------------------------------------------------------
@@ -744,8 +787,9 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 	uint32_t n = c->nFixtures;
 	if (n == 0)
 		return;
-	k_body_prep<<<(c->nBodies + 255) / 256, 256, 0, s>>>(c->scene, c->nBodies);
-	k_sync<<<(uint32_t)(((size_t)n * SYNC_LANES + 127) / 128), 128, 0, s>>>(c->scene, c->buf, n, c->creationPass ? 1 : 0);
+	const size_t groups = std::max<size_t>(n, c->nBodies);
+	k_sync<<<(uint32_t)((groups * SYNC_LANES + 127) / 128), 128, 0, s>>>(c->scene, c->buf, n, c->nBodies,
+		c->creationPass ? 1 : 0);
 	if (c->creationPass)
 		launch_mesh_fat(c, s);
 }
