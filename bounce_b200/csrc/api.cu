@@ -542,6 +542,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dFixBound);
 	dfree(c->dMeshFix);
 	free_mesh(c);
+	free_queries(c);
 	for (int i = 0; i < B3G_STAGE_RING; ++i)
 	{
 		if (c->stage[i].done)

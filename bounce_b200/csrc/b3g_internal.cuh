@@ -292,6 +292,9 @@ struct b3g_ctx
 	int device;
 	cudaStream_t stream;
 	std::string err;
+	uint32_t treeLeaves;  // leaves of the LBVH built by the last pass
+	void* qScratch;       // device scratch of the world queries
+	size_t qScratchBytes;
 
 	uint32_t nHulls, nBodies, nFixtures, nWorlds;
 	uint32_t hullVerts, hullEdges, hullFaces;
@@ -409,6 +412,7 @@ void launch_mesh_prepare(b3g_ctx* c, cudaStream_t s);
 void launch_mesh_collide(b3g_ctx* c, const uint32_t* list, const uint32_t* count, cudaStream_t s);
 uint32_t mesh_launches(const b3g_ctx* c);
 void free_mesh(b3g_ctx* c);
+void free_queries(b3g_ctx* c);
 int resolve_wakeups(b3g_ctx* c, cudaStream_t s);
 void launch_collide_pairs(b3g_ctx* c, cudaStream_t s, uint32_t n, const uint32_t* fixA,
 	const uint32_t* fixB, const float* xfA, const float* xfB, const float* xf0A,

@@ -812,6 +812,7 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	int n = (int)c->nFixtures;
+	c->treeLeaves = (uint32_t)n;
 	if (n == 0)
 	{
 		cudaMemsetAsync(B.counters + CTR_RAW, 0, sizeof(uint32_t), s);

@@ -1,0 +1,648 @@
+// World queries on the device: b3World::QueryAABB, RayCast and RayCastSingle
+// (world.cpp:452-566, :854-878) over the LBVH and fat AABBs of the last pass,
+// with each shape's own ray cast:
+//   b3SphereShape::RayCast    sphere_shape.cpp:69-122
+//   b3CapsuleShape::RayCast   capsule_shape.cpp:180-322
+//   b3HullShape::RayCast      hull_shape.cpp:189-275
+//   b3TriangleShape::RayCast  triangle_shape.cpp:95-180
+//   b3MeshShape::RayCast      mesh_shape.cpp:81-146, over b3StaticTree::RayCast
+//                             (static_tree.h:150-292)
+//
+// One thread per query walks the LBVH from the root along its ropes. The
+// reference walks its dynamic tree instead; the set of proxies a query meets
+// is the same (fat AABBs overlapping the box, or the segment), only the order
+// differs: QueryAABB and RayCast (every hit) are returned per query in LBVH
+// order, and RayCastSingle keeps the smallest fraction, the smaller fixture
+// index on an exact tie (the reference keeps the first one its tree meets).
+
+#include <vector>
+
+#include "collide_common.cuh"
+
+namespace {
+
+constexpr uint32_t SENT = 0xFFFFFFFFu;
+
+struct RayIn
+{
+	V3 p1, p2;
+	float maxFraction;
+};
+
+struct RayOut
+{
+	float fraction;
+	V3 normal;
+};
+
+__device__ __forceinline__ V3 vabs(V3 v) { return V3{fabsf(v.x), fabsf(v.y), fabsf(v.z)}; }
+
+// The segment tests of b3DynamicTree::RayCast / b3StaticTree::RayCast
+// (static_tree.h:185-262): the segment's AABB overlaps the node's, and no
+// axis of the box or of cross(e_i, r) separates them.
+struct SegTest
+{
+	V3 p1, q2, r;
+	AABB box;
+
+	__device__ void init(V3 a, V3 b, float maxFraction)
+	{
+		p1 = a;
+		r = b - a;
+		normalize_inplace(r);
+		q2 = a + maxFraction * (b - a);
+		box.lo = vmin(a, q2);
+		box.hi = vmax(a, q2);
+	}
+
+	__device__ bool pass(V3 lo, V3 hi) const
+	{
+		if (box.hi.x < lo.x || box.lo.x > hi.x || box.hi.y < lo.y || box.lo.y > hi.y || box.hi.z < lo.z ||
+			box.lo.z > hi.z)
+			return false;
+		V3 c = 0.5f * (lo + hi);
+		V3 h = 0.5f * (hi - lo);
+		V3 s = p1 - c;
+		V3 t = q2 - c;
+		if (fabsf(s.x + t.x) - (fabsf(s.x - t.x) + 2.0f * h.x) > 0.0f)
+			return false;
+		if (fabsf(s.y + t.y) - (fabsf(s.y - t.y) + 2.0f * h.y) > 0.0f)
+			return false;
+		if (fabsf(s.z + t.z) - (fabsf(s.z - t.z) + 2.0f * h.z) > 0.0f)
+			return false;
+		V3 v1 = cross(V3{1.0f, 0.0f, 0.0f}, r);
+		if (fabsf(dot(v1, s)) - dot(vabs(v1), h) > 0.0f)
+			return false;
+		V3 v2 = cross(V3{0.0f, 1.0f, 0.0f}, r);
+		if (fabsf(dot(v2, s)) - dot(vabs(v2), h) > 0.0f)
+			return false;
+		V3 v3 = cross(V3{0.0f, 0.0f, 1.0f}, r);
+		if (fabsf(dot(v3, s)) - dot(vabs(v3), h) > 0.0f)
+			return false;
+		return true;
+	}
+};
+
+// Ray against a sphere of radius `radius` around m = p1 - centre.
+__device__ __forceinline__ bool ray_sphere_at(RayOut& o, V3 m, V3 d, float a, float radius, float maxFraction)
+{
+	float b = dot(m, d);
+	float c = dot(m, m) - radius * radius;
+	float disc = b * b - a * c;
+	if (disc < 0.0f)
+		return false;
+	float t = -b - sqrtf(disc);
+	if (t > 0.0f && t <= maxFraction * a)
+	{
+		t /= a;
+		o.fraction = t;
+		o.normal = normalized(m + t * d);
+		return true;
+	}
+	return false;
+}
+
+__device__ bool ray_sphere(RayOut& o, const RayIn& in, const XF& xf, V3 center, float radius)
+{
+	V3 d = in.p2 - in.p1;
+	float a = dot(d, d);
+	if (a < B3G_EPSILON * B3G_EPSILON)
+		return false;
+	V3 m = in.p1 - xmul(xf, center);
+	return ray_sphere_at(o, m, d, a, radius, in.maxFraction);
+}
+
+__device__ bool ray_capsule(RayOut& o, const RayIn& in, const XF& xf, V3 v1, V3 v2, float radius)
+{
+	V3 A = in.p1, B = in.p2;
+	V3 n = B - A;
+	float nn = dot(n, n);
+	if (nn < B3G_EPSILON * B3G_EPSILON)
+		return false;
+	V3 P = xmul(xf, v1), Q = xmul(xf, v2);
+	V3 d = Q - P;
+	float dd = dot(d, d);
+	if (dd < B3G_EPSILON * B3G_EPSILON)
+		return ray_sphere_at(o, A - P, n, nn, radius, in.maxFraction);
+	V3 m = A - P;
+	float nd = dot(n, d);
+	float mm = dot(m, m);
+	float md = dot(m, d);
+	float mn = dot(m, n);
+	float a = dd * nn - nd * nd;
+	if (fabsf(a) < 2.0f * (B3G_EPSILON * B3G_EPSILON))
+		return false;
+	float b = dd * mn - nd * md;
+	float c = dd * (mm - radius * radius) - md * md;
+	float disc = b * b - a * c;
+	if (disc < 0.0f)
+		return false;
+	float t = -b - sqrtf(disc);
+	t /= a;
+	if (t < 0.0f || t > 1.0f)
+		return false;
+	// Which part of the capsule the cylinder hit lies on.
+	float tp = md + t * nd;
+	V3 C;
+	if (tp < 0.0f)
+		C = P;
+	else if (tp > dd)
+		C = Q;
+	else
+	{
+		V3 X = (1.0f - t) * A + t * B;
+		V3 e2 = cross(d, X - P);
+		V3 e3 = cross(e2, d);
+		normalize_inplace(e3);
+		o.fraction = t;
+		o.normal = e3;
+		return true;
+	}
+	// Hemisphere at C.
+	return ray_sphere_at(o, A - C, n, nn, radius, in.maxFraction);
+}
+
+__device__ bool ray_hull(RayOut& o, const RayIn& in, const XF& xf, const HullRef& h)
+{
+	V3 p1 = rotc(xf.q, in.p1 - xf.p);
+	V3 p2 = rotc(xf.q, in.p2 - xf.p);
+	V3 d = p2 - p1;
+	float lower = 0.0f, upper = in.maxFraction;
+	uint32_t index = B3G_NULL;
+	for (uint32_t i = 0; i < h.fCnt; ++i)
+	{
+		PL pl = hp(h, i);
+		float numerator = pl.d - dot(pl.n, p1);
+		float denominator = dot(pl.n, d);
+		if (denominator == 0.0f)
+		{
+			if (numerator < 0.0f)
+				return false;
+		}
+		else
+		{
+			if (denominator < 0.0f)
+			{
+				if (numerator < lower * denominator)
+				{
+					lower = numerator / denominator;
+					index = i;
+				}
+			}
+			else if (numerator < upper * denominator)
+				upper = numerator / denominator;
+			if (upper < lower)
+				return false;
+		}
+	}
+	if (index != B3G_NULL)
+	{
+		o.fraction = lower;
+		o.normal = rot(xf.q, hp(h, index).n);
+		return true;
+	}
+	return false;
+}
+
+__device__ bool ray_triangle(RayOut& o, const RayIn& in, const XF& xf, V3 v1, V3 v2, V3 v3)
+{
+	V3 p1 = xmult(xf, in.p1);
+	V3 p2 = xmult(xf, in.p2);
+	V3 d = p2 - p1;
+	if (dot(d, d) < B3G_EPSILON * B3G_EPSILON)
+		return false;
+	V3 n = cross(v2 - v1, v3 - v1);
+	float l = len(n);
+	if (l == 0.0f)
+		return false;
+	float inv = 1.0f / l; // b3Vec3::operator/= scales by the reciprocal
+	n = inv * n;
+	float num = dot(n, v1 - p1);
+	float den = dot(n, d);
+	if (den == 0.0f)
+		return false;
+	float fraction = num / den;
+	if (fraction < 0.0f || in.maxFraction < fraction)
+		return false;
+	V3 Q = p1 + fraction * d;
+	V3 AB = v2 - v1, AC = v3 - v1;
+	V3 QA = v1 - Q, QB = v2 - Q, QC = v3 - Q;
+	V3 QB_x_QC = cross(QB, QC);
+	V3 QC_x_QA = cross(QC, QA);
+	V3 QA_x_QB = cross(QA, QB);
+	V3 AB_x_AC = cross(AB, AC);
+	float u = dot(QB_x_QC, AB_x_AC);
+	float v = dot(QC_x_QA, AB_x_AC);
+	float w = dot(QA_x_QB, AB_x_AC);
+	if (u >= 0.0f && v >= 0.0f && w >= 0.0f)
+	{
+		o.fraction = fraction;
+		o.normal = num > 0.0f ? rot(xf.q, -n) : rot(xf.q, n);
+		return true;
+	}
+	return false;
+}
+
+// b3MeshShape::RayCast: the segment in the mesh's unscaled frame walks the
+// static tree (depth first, child2 first, as b3StaticTree::RayCast's stack);
+// each leaf's triangle (scaled) is ray cast with the original segment; the
+// first smallest fraction wins.
+__device__ bool ray_mesh(RayOut& o, const RayIn& in, const XF& xf, const DevScene& S, uint32_t fix, uint32_t* status)
+{
+	const MeshDesc md = S.meshes[S.fixHull[fix]];
+	float4 sp = S.fixParams[3 * fix];
+	V3 sc = V3{sp.x, sp.y, sp.z};
+	V3 inv = V3{1.0f / sc.x, 1.0f / sc.y, 1.0f / sc.z};
+	SegTest seg;
+	seg.init(vmul(inv, xmult(xf, in.p1)), vmul(inv, xmult(xf, in.p2)), in.maxFraction);
+	bool hit = false;
+	o.fraction = B3G_MAX_SCALAR;
+	constexpr uint32_t STACK = 64;
+	uint32_t stack[STACK];
+	uint32_t sp_ = 0;
+	stack[sp_++] = md.root;
+	while (sp_ > 0)
+	{
+		uint32_t id = stack[--sp_];
+		if (id == B3G_NULL_NODE)
+			continue;
+		float4 lo = S.meshNodes[2 * (size_t)(md.nOff + id)], hi = S.meshNodes[2 * (size_t)(md.nOff + id) + 1];
+		if (!seg.pass(V3{lo.x, lo.y, lo.z}, V3{hi.x, hi.y, hi.z}))
+			continue;
+		uint32_t child1 = __float_as_uint(lo.w), other = __float_as_uint(hi.w);
+		if (child1 == B3G_NULL_NODE)
+		{
+			uint4 t = S.meshTris[md.tOff + other];
+			auto vert = [&](uint32_t i) {
+				float4 a = S.meshVerts[md.vOff + i];
+				return vmul(sc, V3{a.x, a.y, a.z});
+			};
+			RayOut r;
+			if (ray_triangle(r, in, xf, vert(t.x), vert(t.y), vert(t.z)) && r.fraction < o.fraction)
+			{
+				hit = true;
+				o = r;
+			}
+		}
+		else
+		{
+			if (sp_ + 2 > STACK)
+			{
+				atomicOr(status, B3G_ST_POLY_OVERFLOW);
+				return hit;
+			}
+			stack[sp_++] = child1;
+			stack[sp_++] = other;
+		}
+	}
+	return hit;
+}
+
+// b3Fixture::RayCast (fixture.h) at the body's transform of the last pass.
+__device__ bool ray_fixture(RayOut& o, const RayIn& in, const DevScene& S, uint32_t f, uint32_t* status)
+{
+	XF xf = body_xf(S, S.fixBody[f]);
+	float4 p0 = S.fixParams[3 * f], p1 = S.fixParams[3 * f + 1], p2 = S.fixParams[3 * f + 2];
+	switch (S.fixType[f])
+	{
+	case B3G_SHAPE_SPHERE:
+		return ray_sphere(o, in, xf, V3{p0.x, p0.y, p0.z}, p0.w);
+	case B3G_SHAPE_CAPSULE:
+		return ray_capsule(o, in, xf, V3{p0.x, p0.y, p0.z}, V3{p0.w, p1.x, p1.y}, p1.z);
+	case B3G_SHAPE_TRIANGLE:
+		return ray_triangle(o, in, xf, V3{p0.x, p0.y, p0.z}, V3{p0.w, p1.x, p1.y}, V3{p1.z, p1.w, p2.x});
+	case B3G_SHAPE_HULL:
+		return ray_hull(o, in, xf, hull_ref(S, S.fixHull[f]));
+	case B3G_SHAPE_MESH:
+		return ray_mesh(o, in, xf, S, f, status);
+	default:
+		return false;
+	}
+}
+
+struct QueryCtx
+{
+	DevScene S;
+	const float4* nodeLo;
+	const float4* nodeHi;
+	const float4* fatLo;
+	const float4* fatHi;
+	uint32_t leaves;
+	uint32_t* status;
+};
+
+__device__ __forceinline__ bool query_takes(const QueryCtx& q, uint32_t f, uint32_t world)
+{
+	return q.S.fixLife[f] != FIX_DEAD && q.S.bodyWorld[q.S.fixBody[f]] == world;
+}
+
+// Rope walk of the LBVH from the root; visit(proxy) for every leaf `accept`
+// lets through (internal nodes are descended when `accept` passes them).
+template <class Accept, class Visit>
+__device__ __forceinline__ void lbvh_walk(const QueryCtx& q, Accept&& accept, Visit&& visit)
+{
+	const uint32_t nodes = 2u * q.leaves - 1u;
+	uint32_t node = 0;
+	uint32_t steps = 0;
+	while (node != SENT)
+	{
+		if (++steps > nodes + 1u || node >= nodes)
+		{
+			atomicOr(q.status, B3G_ST_WAIT_TIMEOUT);
+			return;
+		}
+		float4 lo = q.nodeLo[node], hi = q.nodeHi[node];
+		bool pass = accept(V3{lo.x, lo.y, lo.z}, V3{hi.x, hi.y, hi.z});
+		if (pass && node < q.leaves - 1u)
+		{
+			node = __float_as_uint(lo.w);
+			continue;
+		}
+		if (pass)
+			visit(__float_as_uint(lo.w));
+		node = __float_as_uint(hi.w);
+	}
+}
+
+// b3World::QueryAABB: fat AABBs overlapping the box (b3TestOverlap, closed).
+template <int MODE>
+__global__ void k_query_aabb(QueryCtx q, const float* boxes, const uint32_t* worlds, uint32_t n, uint32_t* counts,
+	uint2* out, uint32_t capacity)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	AABB b;
+	b.lo = V3{boxes[6 * i], boxes[6 * i + 1], boxes[6 * i + 2]};
+	b.hi = V3{boxes[6 * i + 3], boxes[6 * i + 4], boxes[6 * i + 5]};
+	uint32_t world = worlds ? worlds[i] : 0u;
+	uint32_t k = MODE == 0 ? 0u : counts[i];
+	auto overlap = [&](V3 lo, V3 hi) {
+		return !(hi.x < b.lo.x || lo.x > b.hi.x || hi.y < b.lo.y || lo.y > b.hi.y || hi.z < b.lo.z || lo.z > b.hi.z);
+	};
+	lbvh_walk(q, overlap, [&](uint32_t f) {
+		float4 lo = q.fatLo[f], hi = q.fatHi[f];
+		if (!overlap(V3{lo.x, lo.y, lo.z}, V3{hi.x, hi.y, hi.z}) || !query_takes(q, f, world))
+			return;
+		if (MODE == 1 && k < capacity)
+			out[k] = make_uint2(i, f);
+		++k;
+	});
+	if (MODE == 0)
+		counts[i] = k;
+}
+
+// b3World::RayCast with a listener that keeps every hit (MODE 0 counts,
+// MODE 1 writes fixture + (point, normal, fraction)) and b3World::RayCastSingle
+// (MODE 2: the smallest fraction).
+template <int MODE>
+__global__ void k_ray_cast(QueryCtx q, const float* rays, const uint32_t* worlds, uint32_t n, uint32_t* counts,
+	uint2* outIdx, float* outHit, uint32_t capacity)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	RayIn in;
+	in.p1 = V3{rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]};
+	in.p2 = V3{rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]};
+	in.maxFraction = 1.0f;
+	uint32_t world = worlds ? worlds[i] : 0u;
+	uint32_t k = MODE == 1 ? counts[i] : 0u;
+	uint32_t best = B3G_NULL;
+	RayOut bestOut;
+	bestOut.fraction = B3G_MAX_SCALAR;
+	bestOut.normal = V3{0.0f, 0.0f, 0.0f};
+	if (dot(in.p2 - in.p1, in.p2 - in.p1) > 0.0f)
+	{
+		SegTest seg;
+		seg.init(in.p1, in.p2, in.maxFraction);
+		lbvh_walk(q, [&](V3 lo, V3 hi) { return seg.pass(lo, hi); }, [&](uint32_t f) {
+			if (!query_takes(q, f, world))
+				return;
+			RayOut o;
+			if (!ray_fixture(o, in, q.S, f, q.status))
+				return;
+			if (MODE == 2)
+			{
+				if (o.fraction < bestOut.fraction || (o.fraction == bestOut.fraction && f < best))
+				{
+					best = f;
+					bestOut = o;
+				}
+				return;
+			}
+			if (MODE == 1 && k < capacity)
+			{
+				V3 p = (1.0f - o.fraction) * in.p1 + o.fraction * in.p2;
+				outIdx[k] = make_uint2(i, f);
+				float* h = outHit + 7 * (size_t)k;
+				h[0] = p.x, h[1] = p.y, h[2] = p.z;
+				h[3] = o.normal.x, h[4] = o.normal.y, h[5] = o.normal.z;
+				h[6] = o.fraction;
+			}
+			++k;
+		});
+	}
+	if (MODE == 0)
+		counts[i] = k;
+	if (MODE == 2)
+	{
+		outIdx[i] = make_uint2(i, best);
+		float* h = outHit + 7 * (size_t)i;
+		V3 p = best != B3G_NULL ? (1.0f - bestOut.fraction) * in.p1 + bestOut.fraction * in.p2 : V3{0.0f, 0.0f, 0.0f};
+		h[0] = p.x, h[1] = p.y, h[2] = p.z;
+		h[3] = bestOut.normal.x, h[4] = bestOut.normal.y, h[5] = bestOut.normal.z;
+		h[6] = best != B3G_NULL ? bestOut.fraction : 0.0f;
+	}
+}
+
+int qfail(b3g_ctx* c, int code, const char* msg)
+{
+	c->err = msg;
+	return code;
+}
+
+// Device scratch of the query calls, grown on demand.
+bool q_reserve(b3g_ctx* c, size_t bytes)
+{
+	if (c->qScratchBytes >= bytes)
+		return true;
+	if (c->qScratch)
+		cudaFree(c->qScratch);
+	c->qScratch = nullptr;
+	c->qScratchBytes = 0;
+	size_t want = bytes < ((size_t)1 << 20) ? ((size_t)1 << 20) : bytes;
+	if (cudaMalloc(&c->qScratch, want) != cudaSuccess)
+		return false;
+	c->qScratchBytes = want;
+	return true;
+}
+
+int q_begin(b3g_ctx* c, uint32_t n, const void* in, size_t inBytes, const uint32_t* worlds, QueryCtx& q,
+	size_t extraBytes, char*& base, const uint32_t*& dWorlds, const void*& dIn)
+{
+	if (!c->havePass || c->treeLeaves == 0)
+		return qfail(c, B3G_E_STATE, "world query: no collision pass yet");
+	if (n > std::max(c->cfg.max_proxies, c->cfg.max_contacts))
+		return qfail(c, B3G_E_CAPACITY, "world query: more queries than max(max_proxies, max_contacts) per call");
+	if (cudaSetDevice(c->device) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "world query: device");
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	size_t need = al(inBytes) + al(4 * (size_t)n) + extraBytes;
+	if (!q_reserve(c, need))
+		return qfail(c, B3G_E_CUDA, "world query: device allocation failed");
+	base = (char*)c->qScratch;
+	dIn = base;
+	if (cudaMemcpyAsync(base, in, inBytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "world query: copy");
+	base += al(inBytes);
+	dWorlds = nullptr;
+	if (worlds)
+	{
+		if (cudaMemcpyAsync(base, worlds, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+			return qfail(c, B3G_E_CUDA, "world query: copy");
+		dWorlds = (const uint32_t*)base;
+	}
+	base += al(4 * (size_t)n);
+	q.S = c->scene;
+	q.nodeLo = c->buf.nodeLo;
+	q.nodeHi = c->buf.nodeHi;
+	q.fatLo = c->buf.fatLo;
+	q.fatHi = c->buf.fatHi;
+	q.leaves = c->treeLeaves;
+	q.status = c->buf.counters + CTR_SCRATCH;
+	return B3G_OK;
+}
+
+int q_status(b3g_ctx* c)
+{
+	uint32_t st = 0;
+	if (cudaMemcpyAsync(&st, c->buf.counters + CTR_SCRATCH, 4, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+		cudaStreamSynchronize(c->stream) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "world query: kernel failed");
+	if (st)
+		return qfail(c, st & B3G_ST_WAIT_TIMEOUT ? B3G_E_TIMEOUT : B3G_E_CAPACITY,
+			"world query: tree walk stopped (stack or step limit)");
+	return B3G_OK;
+}
+
+} // namespace
+
+extern "C" int b3g_query_aabb(b3g_ctx* c, uint32_t n, const float* boxes, const uint32_t* worlds, uint32_t* out,
+	uint32_t capacity)
+{
+	if (!c || (n && (!boxes || (!out && capacity))))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_query_aabb: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return 0;
+	QueryCtx q;
+	char* base;
+	const uint32_t* dWorlds;
+	const void* dIn;
+	const size_t cntBytes = ((4 * (size_t)n + 4 + 255) & ~(size_t)255);
+	const size_t outBytes = 8 * (size_t)capacity;
+	int rc = q_begin(c, n, boxes, 24 * (size_t)n, worlds, q, cntBytes + outBytes + 256, base, dWorlds, dIn);
+	if (rc)
+		return rc;
+	uint32_t* counts = (uint32_t*)base;
+	uint2* dOut = (uint2*)(base + cntBytes);
+	cudaStream_t s = c->stream;
+	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	const uint32_t blocks = (n + 127) / 128;
+	k_query_aabb<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dOut, capacity);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	k_query_aabb<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dOut, capacity);
+	uint32_t total = 0;
+	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_query_aabb: copy");
+	rc = q_status(c);
+	if (rc)
+		return rc;
+	uint32_t m = total < capacity ? total : capacity;
+	if (m && cudaMemcpy(out, dOut, 8 * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_query_aabb: copy");
+	return (int)total;
+}
+
+extern "C" int b3g_ray_cast(b3g_ctx* c, uint32_t n, const float* rays, const uint32_t* worlds, uint32_t* index,
+	float* hits, uint32_t capacity)
+{
+	if (!c || (n && (!rays || ((!index || !hits) && capacity))))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_ray_cast: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return 0;
+	QueryCtx q;
+	char* base;
+	const uint32_t* dWorlds;
+	const void* dIn;
+	const size_t cntBytes = ((4 * (size_t)n + 4 + 255) & ~(size_t)255);
+	const size_t idxBytes = ((8 * (size_t)capacity + 255) & ~(size_t)255);
+	int rc = q_begin(c, n, rays, 24 * (size_t)n, worlds, q, cntBytes + idxBytes + 28 * (size_t)capacity + 256, base,
+		dWorlds, dIn);
+	if (rc)
+		return rc;
+	uint32_t* counts = (uint32_t*)base;
+	uint2* dIdx = (uint2*)(base + cntBytes);
+	float* dHit = (float*)(base + cntBytes + idxBytes);
+	cudaStream_t s = c->stream;
+	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	const uint32_t blocks = (n + 127) / 128;
+	k_ray_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	k_ray_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity);
+	uint32_t total = 0;
+	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_ray_cast: copy");
+	rc = q_status(c);
+	if (rc)
+		return rc;
+	uint32_t m = total < capacity ? total : capacity;
+	if (m && (cudaMemcpy(index, dIdx, 8 * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+				 cudaMemcpy(hits, dHit, 28 * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess))
+		return qfail(c, B3G_E_CUDA, "b3g_ray_cast: copy");
+	return (int)total;
+}
+
+extern "C" int b3g_ray_cast_single(b3g_ctx* c, uint32_t n, const float* rays, const uint32_t* worlds,
+	uint32_t* fixture, float* hit)
+{
+	if (!c || (n && (!rays || !fixture || !hit)))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_ray_cast_single: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return 0;
+	QueryCtx q;
+	char* base;
+	const uint32_t* dWorlds;
+	const void* dIn;
+	const size_t idxBytes = ((8 * (size_t)n + 255) & ~(size_t)255);
+	int rc = q_begin(c, n, rays, 24 * (size_t)n, worlds, q, idxBytes + 28 * (size_t)n + 256, base, dWorlds, dIn);
+	if (rc)
+		return rc;
+	uint2* dIdx = (uint2*)base;
+	float* dHit = (float*)(base + idxBytes);
+	cudaStream_t s = c->stream;
+	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	k_ray_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, nullptr, dIdx, dHit, n);
+	rc = q_status(c);
+	if (rc)
+		return rc;
+	std::vector<uint2> idx(n);
+	if (cudaMemcpy(idx.data(), dIdx, 8 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+		cudaMemcpy(hit, dHit, 28 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_ray_cast_single: copy");
+	int hits = 0;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		fixture[i] = idx[i].y;
+		hits += idx[i].y != B3G_NULL ? 1 : 0;
+	}
+	return hits;
+}
+
+void free_queries(b3g_ctx* c)
+{
+	if (c->qScratch)
+		cudaFree(c->qScratch);
+	c->qScratch = nullptr;
+	c->qScratchBytes = 0;
+}

@@ -159,6 +159,46 @@ class CollisionPipeline:
         m = np.ascontiguousarray(motor, np.float32)
         self._check(self.lib.b3g_load_impulses(self.ctx, N.ptr(n, f32), N.ptr(t, f32), N.ptr(m, f32)))
 
+    # -- world queries (after a pass) --------------------------------------
+
+    def query_aabb(self, boxes, worlds=None, capacity=None):
+        """b3World::QueryAABB for each box (6 floats): (k, 2) u32 (query, fixture)."""
+        b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+        w = None if worlds is None else np.ascontiguousarray(worlds, np.uint32)
+        cap = capacity or max(1024, 64 * len(b))
+        while True:
+            out = np.zeros((cap, 2), np.uint32)
+            k = self._check(self.lib.b3g_query_aabb(self.ctx, len(b), N.ptr(b, f32), N.ptr(w, u32), N.ptr(out, u32), cap))
+            if k <= cap:
+                return out[:k]
+            cap = k
+
+    def ray_cast(self, rays, worlds=None, capacity=None):
+        """b3World::RayCast keeping every hit, for each ray (p1, p2):
+        (k, 2) u32 (ray, fixture) and (k, 7) f32 (point, normal, fraction)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        w = None if worlds is None else np.ascontiguousarray(worlds, np.uint32)
+        cap = capacity or max(1024, 16 * len(r))
+        while True:
+            idx = np.zeros((cap, 2), np.uint32)
+            hit = np.zeros((cap, 7), np.float32)
+            k = self._check(self.lib.b3g_ray_cast(self.ctx, len(r), N.ptr(r, f32), N.ptr(w, u32), N.ptr(idx, u32),
+                                                  N.ptr(hit, f32), cap))
+            if k <= cap:
+                return idx[:k], hit[:k]
+            cap = k
+
+    def ray_cast_single(self, rays, worlds=None):
+        """b3World::RayCastSingle for each ray: fixture (0xFFFFFFFF: no hit)
+        and (n, 7) f32 (point, normal, fraction)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        w = None if worlds is None else np.ascontiguousarray(worlds, np.uint32)
+        fix = np.zeros(max(len(r), 1), np.uint32)
+        hit = np.zeros((max(len(r), 1), 7), np.float32)
+        self._check(self.lib.b3g_ray_cast_single(self.ctx, len(r), N.ptr(r, f32), N.ptr(w, u32), N.ptr(fix, u32),
+                                                 N.ptr(hit, f32)))
+        return fix[:len(r)], hit[:len(r)]
+
     def load_mesh_impulses(self, normal, tangent, motor):
         """Impulses of manifolds 1 and 2 per contact: normal (n, 2, 4),
         tangent (n, 2, 2), motor (n, 2)."""

@@ -373,6 +373,38 @@ int b3g_collide_pairs(b3g_ctx* ctx, uint32_t n, const uint32_t* fixA, const uint
 	const float* xfA, const float* xfB, const float* xf0A, const float* xf0B,
 	uint32_t* cache4, void* manifolds);
 
+/* World queries on the proxies, fat AABBs and body transforms of the last
+ * pass (after b3g_collide; a scene update takes effect at the next pass).
+ * Host buffers; at most max(max_proxies, max_contacts) queries per call;
+ * worlds (one per query) may be NULL for world 0. Filters (b3QueryFilter,
+ * b3RayCastFilter) are left to the caller: every live fixture of the query's
+ * world is considered, sensors included.
+ *
+ * b3g_query_aabb replaces b3World::QueryAABB (world.cpp:854-878) with a
+ * listener that accepts every fixture: boxes are 6 floats (lower, upper);
+ * writes (query, fixture) pairs of every fixture whose fat AABB overlaps the
+ * box (b3TestOverlap), up to capacity, and returns their number. */
+int b3g_query_aabb(b3g_ctx* ctx, uint32_t n, const float* boxes, const uint32_t* worlds, uint32_t* out,
+	uint32_t capacity);
+
+/* b3World::RayCast (world.cpp:452-500) with a listener that returns 1 for
+ * every fixture (keeps every hit): rays are 6 floats (p1, p2); writes
+ * (ray, fixture) pairs into index and 7 floats per hit into hits (point as
+ * b3World computes it, (1 - fraction) p1 + fraction p2; the shape's normal;
+ * fraction), up to capacity, and returns the number of hits. The shapes' ray
+ * casts are the reference's (sphere_shape.cpp:69-122, capsule_shape.cpp:180-322,
+ * hull_shape.cpp:189-275, triangle_shape.cpp:95-180, mesh_shape.cpp:81-146). */
+int b3g_ray_cast(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds, uint32_t* index,
+	float* hits, uint32_t capacity);
+
+/* b3World::RayCastSingle (world.cpp:502-566): per ray the hit with the
+ * smallest fraction: fixture (0xFFFFFFFF when none) and 7 floats (point,
+ * normal, fraction). Of two hits at exactly the same fraction the smaller
+ * fixture index is kept (the reference keeps the first its tree meets).
+ * Returns the number of rays that hit. */
+int b3g_ray_cast_single(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds, uint32_t* fixture,
+	float* hit);
+
 /* Pair search without device allocation ------------------------------------
  *
  * No counterpart in the reference. For callers that cannot allocate device

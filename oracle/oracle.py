@@ -93,6 +93,9 @@ def lib(precision=32):
         "refw_dump_pairs": ([vp, u32p], ctypes.c_uint32),
         "refw_dump_contacts": ([vp, ctypes.c_uint32, ctypes.c_uint32, vp], ctypes.c_uint32),
         "refw_load_impulses": ([vp, vp], None),
+        "refw_query_aabb": ([vp, f32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
+        "refw_ray_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
+        "refw_ray_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
         "ref_sizeof_dump_contact": ([], ctypes.c_uint32),
         "ref_sizeof_scalar": ([], ctypes.c_uint32),
         "ref_collide": (
@@ -233,6 +236,34 @@ class RefWorld:
 
     def contact_count(self):
         return self.L.refw_contact_count(self.w)
+
+    def query_aabb(self, box):
+        """b3World::QueryAABB: indices of the fixtures reported (report order)."""
+        b = np.ascontiguousarray(box, np.float32)
+        cap = self.scene.n_fixtures
+        out = np.zeros(max(cap, 1), np.uint32)
+        n = self.L.refw_query_aabb(self.w, _p(b, ctypes.c_float), _p(out, ctypes.c_uint32), cap)
+        return out[:n]
+
+    def ray_cast(self, ray):
+        """b3World::RayCast keeping every hit: (fixtures, hits (k, 7): point, normal, fraction)."""
+        r = np.ascontiguousarray(ray, np.float32)
+        cap = self.scene.n_fixtures
+        fix = np.zeros(max(cap, 1), np.uint32)
+        hit = np.zeros((max(cap, 1), 7), np.float64)
+        n = self.L.refw_ray_cast(self.w, _p(r, ctypes.c_float), _p(fix, ctypes.c_uint32),
+                                 hit.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)
+        return fix[:n], hit[:n]
+
+    def ray_cast_single(self, ray):
+        """b3World::RayCastSingle: (fixture, hit (7,)) or (None, None)."""
+        r = np.ascontiguousarray(ray, np.float32)
+        fix = np.zeros(1, np.uint32)
+        hit = np.zeros(7, np.float64)
+        if not self.L.refw_ray_cast_single(self.w, _p(r, ctypes.c_float), _p(fix, ctypes.c_uint32),
+                                           hit.ctypes.data_as(ctypes.POINTER(ctypes.c_double))):
+            return None, None
+        return int(fix[0]), hit
 
     def load_impulses(self, normal, tangent, motor):
         """The solver's impulses for every contact in list order, per manifold

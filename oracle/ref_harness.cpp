@@ -621,6 +621,80 @@ REF_API void refw_load_impulses(void* p, const void* in)
 	}
 }
 
+// World queries through the reference's own b3World entry points.
+struct QueryAll : b3QueryListener, b3QueryFilter
+{
+	std::vector<uint32_t> found;
+	bool ReportFixture(b3Fixture* f) override
+	{
+		found.push_back((uint32_t)(uintptr_t)f->GetUserData());
+		return true;
+	}
+	bool ShouldReport(b3Fixture*) override { return true; }
+};
+
+// b3World::QueryAABB with a listener that accepts every fixture; writes up
+// to cap fixture indices (report order) and returns their number.
+REF_API uint32_t refw_query_aabb(void* p, const float* box, uint32_t* out, uint32_t cap)
+{
+	RefWorld* w = (RefWorld*)p;
+	QueryAll q;
+	b3AABB a;
+	a.lowerBound.Set(box[0], box[1], box[2]);
+	a.upperBound.Set(box[3], box[4], box[5]);
+	w->world->QueryAABB(&q, &q, a);
+	for (uint32_t i = 0; i < q.found.size() && i < cap; ++i)
+		out[i] = q.found[i];
+	return (uint32_t)q.found.size();
+}
+
+struct RayAll : b3RayCastListener, b3RayCastFilter
+{
+	std::vector<uint32_t> fix;
+	std::vector<double> hit;
+	scalar ReportFixture(b3Fixture* f, const b3Vec3& point, const b3Vec3& normal, scalar fraction) override
+	{
+		fix.push_back((uint32_t)(uintptr_t)f->GetUserData());
+		double h[7] = {(double)point.x, (double)point.y, (double)point.z, (double)normal.x, (double)normal.y,
+			(double)normal.z, (double)fraction};
+		hit.insert(hit.end(), h, h + 7);
+		return scalar(1);
+	}
+	bool ShouldRayCast(b3Fixture*) override { return true; }
+};
+
+// b3World::RayCast with a listener that keeps every hit (returns 1): up to
+// cap hits as fixture + (point, normal, fraction); returns the hit count.
+REF_API uint32_t refw_ray_cast(void* p, const float* ray, uint32_t* fix, double* hit, uint32_t cap)
+{
+	RefWorld* w = (RefWorld*)p;
+	RayAll r;
+	w->world->RayCast(&r, &r, b3Vec3(ray[0], ray[1], ray[2]), b3Vec3(ray[3], ray[4], ray[5]));
+	for (uint32_t i = 0; i < r.fix.size() && i < cap; ++i)
+	{
+		fix[i] = r.fix[i];
+		for (int k = 0; k < 7; ++k)
+			hit[7 * i + k] = r.hit[7 * i + k];
+	}
+	return (uint32_t)r.fix.size();
+}
+
+// b3World::RayCastSingle: 1 and the closest hit, or 0.
+REF_API uint32_t refw_ray_cast_single(void* p, const float* ray, uint32_t* fix, double* hit)
+{
+	RefWorld* w = (RefWorld*)p;
+	RayAll filter;
+	b3RayCastSingleOutput o;
+	if (!w->world->RayCastSingle(&o, &filter, b3Vec3(ray[0], ray[1], ray[2]), b3Vec3(ray[3], ray[4], ray[5])))
+		return 0;
+	*fix = (uint32_t)(uintptr_t)o.fixture->GetUserData();
+	double h[7] = {(double)o.point.x, (double)o.point.y, (double)o.point.z, (double)o.normal.x, (double)o.normal.y,
+		(double)o.normal.z, (double)o.fraction};
+	for (int k = 0; k < 7; ++k)
+		hit[k] = h[k];
+	return 1;
+}
+
 // Layout of b3ManifoldPoint / b3Manifold (collision.h:97-128) for checking the
 // device records: sizes and field offsets.
 REF_API void ref_manifold_layout(uint32_t* out)
