@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=30,
                     help="passes after the timed ones, with per-stage CUDA events (not part of value)")
     ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving", "queries"])
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000",
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
@@ -224,6 +224,20 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
 
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
+        return
+    if args.workload == "queries":
+        scene, walls = workload_scene(args, SEED)
+        rays = make_rays(SEED + 100, QUERY_CPU_RAYS, scene_half(scene))
+        _, t = query_reference(scene, walls, rays)
+        v = len(rays) / t
+        print(json.dumps({
+            "metric": "rays/s", "value": v, "unit": "rays/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+            "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": QUERY_WORKLOAD, "rays_per_step": len(rays)},
+            "cpu_baseline": {"value": v, "unit": "rays/s", "cores": 1, "kind": "reference",
+                             "sample": f"{len(rays)} rays through b3World::RayCastSingle on 1 host core"},
+            "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     pile = args.workload == "pile"
     scene, walls = workload_scene(args, PILE_SEED if pile else SEED, sample=pile)
@@ -675,6 +689,167 @@ def run_serving(args, rank, world, local, dist):
     eng.close()
 
 
+# ---------------------------------------------------------------------------
+# World queries: b3World::RayCastSingle on the device LBVH of the mixed world.
+
+QUERY_RAYS = 1 << 20
+QUERY_CPU_RAYS = 1 << 16
+QUERY_WORKLOAD = ("b3World::RayCastSingle over the 65,536-body mixed world after 3 collision passes: "
+                  "1,048,576 rays per step, start uniform in the cube, direction uniform, length 10 m")
+
+
+def make_rays(seed, n, half, length=10.0):
+    rng = np.random.default_rng(seed)
+    p1 = rng.uniform(-half, half, (n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.ascontiguousarray(np.concatenate([p1, p1 + length * d], axis=1), np.float32)
+
+
+def query_reference(scene, walls, rays):
+    """The reference's RayCastSingle on the same world after the same 3 passes:
+    (fixtures, seconds) on 1 host core."""
+    from bounce_b200 import scene as S
+    from oracle import oracle as O
+
+    rw = O.RefWorld(scene)
+    scene.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(scene, walls=walls)
+    rw.first_pass()
+    for _ in range(2):
+        drv.advance()
+        rw.set_sweeps(drv.sweeps14())
+        rw.step_pass()
+    fix, t = rw.ray_cast_single_batch(rays)
+    rw.close()
+    return fix, t
+
+
+def run_queries(args, rank, world, local, dist):
+    import ctypes
+
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+    from bounce_b200 import scene as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene, walls = workload_scene(args, SEED + rank)
+    drv = S.KinematicDriver(scene, walls=walls)
+    nb = scene.n_bodies
+    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local)
+    for k in range(3):
+        if k:
+            drv.advance()
+        pipe.collide(drv.state17())
+    assert pipe.counts()["status"] == 0
+    n = QUERY_RAYS
+    rays = make_rays(SEED + 100 + rank, n, scene_half(scene))
+    d_rays = torch.from_numpy(rays).to(dev)
+    d_fix = torch.empty(n, dtype=torch.int32, device=dev)
+    d_hit = torch.empty((n, 7), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    lib = pipe.lib
+
+    def cast():
+        pipe._check(lib.b3g_ray_cast_single_device(pipe.ctx, n, ctypes.c_void_p(d_rays.data_ptr()), None,
+                                                    ctypes.c_void_p(d_fix.data_ptr()),
+                                                    ctypes.c_void_p(d_hit.data_ptr()), sptr))
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            cast()
+    stream.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flushed between steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cast()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    hits = int((d_fix != -1).sum().item())
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t[0])
+    value = world * n * args.steps / (ms_max / 1000.0)
+
+    # e2e: the host-buffer entry point (rays copied in, results copied out).
+    e2e_steps = max(1, min(args.e2e_steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fix_h, _ = pipe.ray_cast_single(rays)
+    e2e_s = time.perf_counter() - t0
+    e2e_value = n * e2e_steps / e2e_s
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world * n * e2e_steps / float(t[0])
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    algo = n * (24 + 4 + 28)
+    achieved = algo / (ms / args.steps / 1000.0) / 1e9
+    roof = {"kernel": "k_ray_cast<2> (RayCastSingle)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "algorithmic_bytes_per_launch": algo,
+            "note": "rays in (24 B) and results out (32 B) per ray; the tree walk is latency bound",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_scene, ref_walls = workload_scene(args, SEED)
+            sample = rays[:QUERY_CPU_RAYS]
+            rfix, rt = query_reference(ref_scene, ref_walls, sample)
+            agree = float(np.mean(rfix == fix_h[:QUERY_CPU_RAYS]))
+            cpu = {"value": len(sample) / rt, "unit": "rays/s", "cores": 1, "kind": "reference",
+                   "sample": f"{len(sample)} of the step's rays through b3World::RayCastSingle on 1 host core",
+                   "same_fixture_as_gpu": agree}
+        except Exception as e:
+            cpu = {"value": None, "unit": "rays/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "rays/s", "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": QUERY_WORKLOAD, "rays_per_step": n, "bodies": nb, "hit_fraction": hits / n,
+                       "l2": "flushed between steps (256 MB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 32 * n,
+                    "steps": e2e_steps},
+            "gpu_launches": args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    pipe.close()
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_init(args)
@@ -685,6 +860,8 @@ def main():
             run_batched(args, rank, world, local, dist)
         elif args.workload == "serving":
             run_serving(args, rank, world, local, dist)
+        elif args.workload == "queries":
+            run_queries(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

@@ -120,6 +120,7 @@ EXPORTED = [
     "b3g_query_aabb",
     "b3g_ray_cast",
     "b3g_ray_cast_single",
+    "b3g_ray_cast_single_device",
     "b3g_autotune",
     "b3g_update_scene",
     "b3g_update_scene_device",
@@ -188,6 +189,7 @@ def load():
         "b3g_query_aabb": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_ray_cast": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_ray_cast_single": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p], ctypes.c_int),
+        "b3g_ray_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp, vp], ctypes.c_int),
         "b3g_update_scene": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, u8p, ctypes.c_uint32, u32p, u32p, u32p, u32p,
                               f32p, u32p, ctypes.c_uint32, u32p, vp], ctypes.c_int),
         "b3g_update_scene_device": ([ctx, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp,

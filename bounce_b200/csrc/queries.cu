@@ -55,6 +55,14 @@ struct SegTest
 		box.hi = vmax(a, q2);
 	}
 
+	// Shortens the segment to [p1, p1 + f (b - p1)].
+	__device__ void clip(V3 b, float f)
+	{
+		q2 = p1 + f * (b - p1);
+		box.lo = vmin(p1, q2);
+		box.hi = vmax(p1, q2);
+	}
+
 	__device__ bool pass(V3 lo, V3 hi) const
 	{
 		if (box.hi.x < lo.x || box.lo.x > hi.x || box.hi.y < lo.y || box.lo.y > hi.y || box.hi.z < lo.z ||
@@ -282,6 +290,9 @@ __device__ bool ray_mesh(RayOut& o, const RayIn& in, const XF& xf, const DevScen
 			{
 				hit = true;
 				o = r;
+				// Triangle boxes are grown by B3_LINEAR_SLOP: a triangle hit no
+				// later than this one is met by the shortened segment too.
+				seg.clip(vmul(inv, xmult(xf, in.p2)), r.fraction);
 			}
 		}
 		else
@@ -397,7 +408,7 @@ __global__ void k_query_aabb(QueryCtx q, const float* boxes, const uint32_t* wor
 // (MODE 2: the smallest fraction).
 template <int MODE>
 __global__ void k_ray_cast(QueryCtx q, const float* rays, const uint32_t* worlds, uint32_t n, uint32_t* counts,
-	uint2* outIdx, float* outHit, uint32_t capacity)
+	uint2* outIdx, float* outHit, uint32_t capacity, uint32_t* outFix)
 {
 	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= n)
@@ -428,6 +439,11 @@ __global__ void k_ray_cast(QueryCtx q, const float* rays, const uint32_t* worlds
 				{
 					best = f;
 					bestOut = o;
+					// A fixture hit at or before this fraction has the hit point
+					// inside its shape's AABB, at least B3_AABB_EXTENSION inside its
+					// fat AABB, so the walk may stop at the hit: the shapes are
+					// still ray cast over the whole segment.
+					seg.clip(in.p2, o.fraction);
 				}
 				return;
 			}
@@ -447,7 +463,7 @@ __global__ void k_ray_cast(QueryCtx q, const float* rays, const uint32_t* worlds
 		counts[i] = k;
 	if (MODE == 2)
 	{
-		outIdx[i] = make_uint2(i, best);
+		outFix[i] = best;
 		float* h = outHit + 7 * (size_t)i;
 		V3 p = best != B3G_NULL ? (1.0f - bestOut.fraction) * in.p1 + bestOut.fraction * in.p2 : V3{0.0f, 0.0f, 0.0f};
 		h[0] = p.x, h[1] = p.y, h[2] = p.z;
@@ -587,9 +603,9 @@ extern "C" int b3g_ray_cast(b3g_ctx* c, uint32_t n, const float* rays, const uin
 	cudaStream_t s = c->stream;
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
 	const uint32_t blocks = (n + 127) / 128;
-	k_ray_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity);
+	k_ray_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity, nullptr);
 	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
-	k_ray_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity);
+	k_ray_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity, nullptr);
 	uint32_t total = 0;
 	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
 		return qfail(c, B3G_E_CUDA, "b3g_ray_cast: copy");
@@ -614,29 +630,49 @@ extern "C" int b3g_ray_cast_single(b3g_ctx* c, uint32_t n, const float* rays, co
 	char* base;
 	const uint32_t* dWorlds;
 	const void* dIn;
-	const size_t idxBytes = ((8 * (size_t)n + 255) & ~(size_t)255);
-	int rc = q_begin(c, n, rays, 24 * (size_t)n, worlds, q, idxBytes + 28 * (size_t)n + 256, base, dWorlds, dIn);
+	const size_t fixBytes = ((4 * (size_t)n + 255) & ~(size_t)255);
+	int rc = q_begin(c, n, rays, 24 * (size_t)n, worlds, q, fixBytes + 28 * (size_t)n + 256, base, dWorlds, dIn);
 	if (rc)
 		return rc;
-	uint2* dIdx = (uint2*)base;
-	float* dHit = (float*)(base + idxBytes);
+	uint32_t* dFix = (uint32_t*)base;
+	float* dHit = (float*)(base + fixBytes);
 	cudaStream_t s = c->stream;
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
-	k_ray_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, nullptr, dIdx, dHit, n);
+	k_ray_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, nullptr, nullptr, dHit, n, dFix);
 	rc = q_status(c);
 	if (rc)
 		return rc;
-	std::vector<uint2> idx(n);
-	if (cudaMemcpy(idx.data(), dIdx, 8 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+	if (cudaMemcpy(fixture, dFix, 4 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess ||
 		cudaMemcpy(hit, dHit, 28 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
 		return qfail(c, B3G_E_CUDA, "b3g_ray_cast_single: copy");
 	int hits = 0;
 	for (uint32_t i = 0; i < n; ++i)
-	{
-		fixture[i] = idx[i].y;
-		hits += idx[i].y != B3G_NULL ? 1 : 0;
-	}
+		hits += fixture[i] != B3G_NULL ? 1 : 0;
 	return hits;
+}
+
+extern "C" int b3g_ray_cast_single_device(b3g_ctx* c, uint32_t n, const float* rays, const uint32_t* worlds,
+	uint32_t* fixture, float* hit, void* stream)
+{
+	if (!c || (n && (!rays || !fixture || !hit)))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_ray_cast_single_device: null argument") : B3G_E_INVALID;
+	if (!c->havePass || c->treeLeaves == 0)
+		return qfail(c, B3G_E_STATE, "world query: no collision pass yet");
+	if (n == 0)
+		return B3G_OK;
+	QueryCtx q;
+	q.S = c->scene;
+	q.nodeLo = c->buf.nodeLo;
+	q.nodeHi = c->buf.nodeHi;
+	q.fatLo = c->buf.fatLo;
+	q.fatHi = c->buf.fatHi;
+	q.leaves = c->treeLeaves;
+	q.status = c->buf.counters + CTR_SCRATCH;
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	k_ray_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, rays, worlds, n, nullptr, nullptr, hit, n, fixture);
+	if (cudaGetLastError() != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_ray_cast_single_device: launch");
+	return B3G_OK;
 }
 
 void free_queries(b3g_ctx* c)

@@ -405,6 +405,13 @@ int b3g_ray_cast(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* wo
 int b3g_ray_cast_single(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds, uint32_t* fixture,
 	float* hit);
 
+/* b3g_ray_cast_single on device buffers (rays, worlds, fixture, hit as above,
+ * all device memory; worlds may be NULL), asynchronous on stream (NULL: the
+ * context's stream), for callers that keep their rays on the GPU. Nothing is
+ * copied or allocated; the result is ready when the stream reaches it. */
+int b3g_ray_cast_single_device(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds,
+	uint32_t* fixture, float* hit, void* stream);
+
 /* Pair search without device allocation ------------------------------------
  *
  * No counterpart in the reference. For callers that cannot allocate device

@@ -96,6 +96,7 @@ def lib(precision=32):
         "refw_query_aabb": ([vp, f32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
+        "refw_ray_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
         "ref_sizeof_dump_contact": ([], ctypes.c_uint32),
         "ref_sizeof_scalar": ([], ctypes.c_uint32),
         "ref_collide": (
@@ -264,6 +265,13 @@ class RefWorld:
                                            hit.ctypes.data_as(ctypes.POINTER(ctypes.c_double))):
             return None, None
         return int(fix[0]), hit
+
+    def ray_cast_single_batch(self, rays):
+        """RayCastSingle for each ray, timed inside the harness: (fixtures, seconds)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        fix = np.zeros(max(len(r), 1), np.uint32)
+        t = self.L.refw_ray_cast_single_batch(self.w, _p(r, ctypes.c_float), len(r), _p(fix, ctypes.c_uint32))
+        return fix[:len(r)], t
 
     def load_impulses(self, normal, tangent, motor):
         """The solver's impulses for every contact in list order, per manifold

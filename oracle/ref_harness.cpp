@@ -695,6 +695,24 @@ REF_API uint32_t refw_ray_cast_single(void* p, const float* ray, uint32_t* fix, 
 	return 1;
 }
 
+// Timed batch of b3World::RayCastSingle calls (the CPU baseline of the ray
+// cast bench): n rays (6 floats each); writes each ray's fixture (or
+// 0xFFFFFFFF) and returns the seconds spent in the calls.
+REF_API double refw_ray_cast_single_batch(void* p, const float* rays, uint32_t n, uint32_t* fix)
+{
+	RefWorld* w = (RefWorld*)p;
+	RayAll filter;
+	double t0 = Now();
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* r = rays + 6 * (size_t)i;
+		b3RayCastSingleOutput o;
+		bool hit = w->world->RayCastSingle(&o, &filter, b3Vec3(r[0], r[1], r[2]), b3Vec3(r[3], r[4], r[5]));
+		fix[i] = hit ? (uint32_t)(uintptr_t)o.fixture->GetUserData() : 0xFFFFFFFFu;
+	}
+	return Now() - t0;
+}
+
 // Layout of b3ManifoldPoint / b3Manifold (collision.h:97-128) for checking the
 // device records: sizes and field offsets.
 REF_API void ref_manifold_layout(uint32_t* out)

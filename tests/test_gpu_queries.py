@@ -89,6 +89,22 @@ def test_queries_mixed_shapes(oracle_mod):
     sc = S.mixed_scene(seed=31, n=2000, side=16.0, static_frac=0.05, sensor_frac=0.03).finalize()
     rw, pipe = run_passes(oracle_mod, sc, 4)
     check_queries(rw, pipe, np.random.default_rng(3), -8.0, 8.0, "mixed")
+    # the device-buffer entry point gives the host one's results
+    import ctypes
+
+    import torch
+
+    rays = random_rays(np.random.default_rng(8), -8.0, 8.0, 500)
+    fix, hit = pipe.ray_cast_single(rays)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_fix = torch.empty(len(rays), dtype=torch.int32, device="cuda")
+    d_hit = torch.empty((len(rays), 7), dtype=torch.float32, device="cuda")
+    pipe._check(pipe.lib.b3g_ray_cast_single_device(pipe.ctx, len(rays), ctypes.c_void_p(d_rays.data_ptr()), None,
+                                                    ctypes.c_void_p(d_fix.data_ptr()),
+                                                    ctypes.c_void_p(d_hit.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert np.array_equal(d_fix.cpu().numpy().view(np.uint32), fix)
+    assert np.array_equal(d_hit.cpu().numpy(), hit)
     pipe.close()
 
 
