@@ -350,6 +350,14 @@ __global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
 		q[k] = min((uint32_t)(t * 1024.0f), 1023u);
 	}
 	uint32_t code = (expand10(q[0]) << 2) | (expand10(q[1]) << 1) | expand10(q[2]);
+	// A proxy wider than a quarter of the scene along some axis (a ground
+	// box, a mesh) sorts after the other proxies of its world: its pairs are
+	// then found by the many short walks of the leaves before it instead of
+	// by one long walk of its own. Only the traversal order changes.
+	float e[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
+	for (int k = 0; k < 3; ++k)
+		if (hi[k] > lo[k] && e[k] > 0.25f * (hi[k] - lo[k]))
+			code = 0xFFFFFFFEu;
 	uint32_t world = S.bodyWorld[S.fixBody[i]];
 	// Dead proxies sort after every live one.
 	B.keysA[i] = S.fixLife[i] == FIX_DEAD ? ~0ull : ((unsigned long long)world << 32) | code;
