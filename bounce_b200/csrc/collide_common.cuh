@@ -776,6 +776,30 @@ __device__ __forceinline__ bool spheres_apart(const DevScene& S, uint32_t fa, co
 	return dot(d, d) > reach * reach;
 }
 
+// The same cull for a hull (bounding sphere) against a capsule's segment:
+// the hull lies inside its bounding sphere, so its distance to the segment is
+// at least the centre's distance minus the sphere radius; farther than the
+// capsule radius plus the margin means b3CollideHullAndCapsule's GJK reports
+// a distance above the radii and the manifold is empty.
+__device__ __forceinline__ bool hull_capsule_apart(const DevScene& S, uint32_t fh, const XF& xfH, uint32_t fc,
+	const XF& xfC)
+{
+	float4 bh = S.fixBound[fh];
+	float4 p0 = S.fixParams[3 * fc], p1 = S.fixParams[3 * fc + 1];
+	V3 c = xmul(xfH, V3{bh.x, bh.y, bh.z});
+	V3 a = xmul(xfC, V3{p0.x, p0.y, p0.z});
+	V3 b = xmul(xfC, V3{p0.w, p1.x, p1.y});
+	V3 d = b - a;
+	float dd = dot(d, d);
+	float t = dd > 0.0f ? dot(c - a, d) / dd : 0.0f;
+	t = fminf(fmaxf(t, 0.0f), 1.0f);
+	V3 e = c - (a + t * d);
+	float mag = fmaxf(fmaxf(fmaxf(fabsf(c.x), fabsf(c.y)), fabsf(c.z)),
+		fmaxf(fmaxf(fmaxf(fabsf(a.x), fabsf(a.y)), fabsf(a.z)), fmaxf(fmaxf(fabsf(b.x), fabsf(b.y)), fabsf(b.z))));
+	float reach = (bh.w + p1.z) + (1e-3f + 1e-5f * mag);
+	return dot(e, e) > reach * reach;
+}
+
 // ---------------------------------------------------------------------------
 // Meshes.
 

@@ -724,7 +724,8 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
 		DevManifold& m = a.man[c];
 		man_clear(m);
-		if (spheres_apart(a.S, fa, xfA, fb, xfB))
+		if (spheres_apart(a.S, fa, xfA, fb, xfB) ||
+			(BUCKET == BK_HULL_CAPSULE && hull_capsule_apart(a.S, fa, xfA, fb, xfB)))
 		{
 			finish_convex(a, c, m);
 			a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);

@@ -164,9 +164,15 @@ __device__ void warp_query_edges(const XF& xf1, const HullRef& h1, const XF& xf2
 	float best = -B3G_MAX_SCALAR;
 	uint32_t bk = 0xFFFFFFFFu;
 	uint32_t total = n1 * n2;
-	for (uint32_t k = lane; k < total; k += 32)
+	// (i, j) of k = i n2 + j, stepped without a division per pair.
+	uint32_t i = n2 ? lane / n2 : 0u, j = lane - i * n2;
+	for (uint32_t k = lane; k < total; k += 32, j += 32)
 	{
-		uint32_t i = k / n2, j = k - i * n2;
+		while (j >= n2)
+		{
+			j -= n2;
+			++i;
+		}
 		float s;
 		if (staged)
 		{

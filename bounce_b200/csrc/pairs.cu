@@ -75,8 +75,13 @@ __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 			bk = BK_INACTIVE;
 		// Convex pairs whose bounding spheres are apart skip their routine
 		// (spheres_apart); taking them out keeps the routines' warps full.
-		if (bk <= BK_HULL_CAPSULE && spheres_apart(S, fa, body_xf(S, ba), fb, body_xf(S, bb)))
-			bk = BK_APART;
+		if (bk <= BK_HULL_CAPSULE)
+		{
+			XF xfA = body_xf(S, ba), xfB = body_xf(S, bb);
+			if (spheres_apart(S, fa, xfA, fb, xfB) ||
+				(bk == BK_HULL_CAPSULE && hull_capsule_apart(S, fa, xfA, fb, xfB)))
+				bk = BK_APART;
+		}
 		// Warp-aggregated append.
 		uint32_t peers = __match_any_sync(__activemask(), bk);
 		uint32_t leader = __ffs(peers) - 1;

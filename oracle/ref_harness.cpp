@@ -621,6 +621,17 @@ REF_API void refw_load_impulses(void* p, const void* in)
 	}
 }
 
+// b3CollideHulls call and feature-cache hit counters (collide_hulls.cpp:28),
+// read and reset.
+extern uint32 b3_convexCalls, b3_convexCacheHits;
+REF_API void refw_convex_stats(uint32_t* out)
+{
+	out[0] = b3_convexCalls;
+	out[1] = b3_convexCacheHits;
+	b3_convexCalls = 0;
+	b3_convexCacheHits = 0;
+}
+
 // World queries through the reference's own b3World entry points.
 struct QueryAll : b3QueryListener, b3QueryFilter
 {
