@@ -142,18 +142,35 @@ __device__ __forceinline__ float edge_pair_sep(const EdgeRec& a, const EdgeRec& 
 	return project_edges(f3(a.P), E1, a.P.w, f3(b.P), E2, b.P.w, C1);
 }
 
-// b3QueryEdgeSeparation(hull, hull) (sat.cpp:111-174). recs holds room for
-// the unique edges of both hulls (maxUE each).
+// Hulls with fewer unique edges than this on both sides share the pairs out
+// flat over the lanes (both edge sets staged); otherwise the larger set sits
+// on the lanes and only the smaller one is staged.
+constexpr uint32_t SAT_FLAT_EDGES = 48;
+
+// Edge records of shared memory one warp needs (maxUE: the most unique
+// edges of any hull): both sets of a flat query (at most 2 maxUE, and at
+// most 2 (SAT_FLAT_EDGES - 1)), or the smaller set of a broadcast one (at
+// most maxUE).
+__host__ __device__ __forceinline__ uint32_t sat_warp_recs(uint32_t maxUE)
+{
+	if (maxUE < SAT_FLAT_EDGES)
+		return 2 * maxUE;
+	return maxUE > 2 * (SAT_FLAT_EDGES - 1) ? maxUE : 2 * (SAT_FLAT_EDGES - 1);
+}
+
+// b3QueryEdgeSeparation(hull, hull) (sat.cpp:111-174). recs holds
+// sat_warp_recs(maxUE) records.
 __device__ void warp_query_edges(const XF& xf1, const HullRef& h1, const XF& xf2, const HullRef& h2,
 	uint32_t lane, EdgeRec* recs, uint32_t maxUE, uint32_t& index1, uint32_t& index2, float& sep)
 {
 	XF xf = xmult(xf2, xf1);
 	V3 C1 = xmul(xf, h1.centroid);
 	uint32_t n1 = h1.eCnt / 2, n2 = h2.eCnt / 2;
+	const bool flat = n1 < SAT_FLAT_EDGES && n2 < SAT_FLAT_EDGES;
 	EdgeRec* r1 = recs;
-	EdgeRec* r2 = recs + maxUE;
+	EdgeRec* r2 = recs + (flat ? n1 : 0);
 	bool staged = n1 <= maxUE && n2 <= maxUE;
-	if (staged)
+	if (staged && flat)
 	{
 		for (uint32_t i = lane; i < n1; i += 32)
 			edge_rec_1(r1[i], xf, h1, 2 * i);
@@ -164,31 +181,78 @@ __device__ void warp_query_edges(const XF& xf1, const HullRef& h1, const XF& xf2
 	float best = -B3G_MAX_SCALAR;
 	uint32_t bk = 0xFFFFFFFFu;
 	uint32_t total = n1 * n2;
-	// (i, j) of k = i n2 + j, stepped without a division per pair.
-	uint32_t i = n2 ? lane / n2 : 0u, j = lane - i * n2;
-	for (uint32_t k = lane; k < total; k += 32, j += 32)
-	{
-		while (j >= n2)
-		{
-			j -= n2;
-			++i;
-		}
-		float s;
-		if (staged)
-		{
-			s = edge_pair_sep(r1[i], r2[j], C1);
-		}
-		else
-		{
-			EdgeRec a, b;
-			edge_rec_1(a, xf, h1, 2 * i);
-			edge_rec_2(b, h2, 2 * j);
-			s = edge_pair_sep(a, b, C1);
-		}
-		if (s > best)
+	// Each lane keeps the first maximum in k = i n2 + j among the pairs it
+	// tests (larger value, or equal value and smaller k; nothing at or below
+	// the start value, as the serial loop's strict test), and warp_argmax
+	// picks the first maximum over the lanes: the serial loop's answer,
+	// whatever pairs a lane is given.
+	auto keep = [&](float s, uint32_t k) {
+		if (s > best || (s == best && bk != 0xFFFFFFFFu && k < bk))
 		{
 			best = s;
 			bk = k;
+		}
+	};
+	if (staged && !flat)
+	{
+		// Larger hull's edges on the lanes, held in registers; the other
+		// hull's edges staged and read by all lanes at once (shared-memory
+		// broadcast).
+		const bool rows1 = n1 >= n2;
+		const uint32_t nl = rows1 ? n1 : n2, nb = rows1 ? n2 : n1;
+		EdgeRec* rb = recs;
+		for (uint32_t b = lane; b < nb; b += 32)
+		{
+			if (rows1)
+				edge_rec_2(rb[b], h2, 2 * b);
+			else
+				edge_rec_1(rb[b], xf, h1, 2 * b);
+		}
+		__syncwarp();
+		for (uint32_t base = 0; base < nl; base += 32)
+		{
+			const uint32_t l = base + lane;
+			const bool valid = l < nl;
+			EdgeRec mine;
+			const uint32_t le = 2 * (valid ? l : 0);
+			if (rows1)
+				edge_rec_1(mine, xf, h1, le);
+			else
+				edge_rec_2(mine, h2, le);
+			for (uint32_t b = 0; b < nb; ++b)
+			{
+				const EdgeRec other = rb[b];
+				if (!valid)
+					continue;
+				const uint32_t i = rows1 ? l : b, j = rows1 ? b : l;
+				keep(rows1 ? edge_pair_sep(mine, other, C1) : edge_pair_sep(other, mine, C1), i * n2 + j);
+			}
+		}
+	}
+	else
+	{
+		// (i, j) of k = i n2 + j, stepped without a division per pair.
+		uint32_t i = n2 ? lane / n2 : 0u, j = lane - i * n2;
+		for (uint32_t k = lane; k < total; k += 32, j += 32)
+		{
+			while (j >= n2)
+			{
+				j -= n2;
+				++i;
+			}
+			float s;
+			if (staged)
+			{
+				s = edge_pair_sep(r1[i], r2[j], C1);
+			}
+			else
+			{
+				EdgeRec a, b;
+				edge_rec_1(a, xf, h1, 2 * i);
+				edge_rec_2(b, h2, 2 * j);
+				s = edge_pair_sep(a, b, C1);
+			}
+			keep(s, k);
 		}
 	}
 	warp_argmax(best, bk);
@@ -630,7 +694,7 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
 	uint32_t n = *a.missCount;
 	uint32_t gw = blockIdx.x * W + warp;
 	uint32_t nw = gridDim.x * W;
@@ -720,7 +784,7 @@ __global__ void __launch_bounds__(W * 32) k_hull_triangle(NPArgs a, uint32_t max
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
 	uint32_t n = *a.listCount;
 	for (uint32_t t = blockIdx.x * W + warp; t < n; t += gridDim.x * W)
 	{
@@ -764,7 +828,7 @@ __global__ void __launch_bounds__(W * 32) k_mesh_items_hull(NPArgs a, Buffers B,
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * 2 * maxUE;
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
 	uint32_t n = min(B.counters[CTR_MESH_PAIRS], B.meshPairCap);
 	for (uint32_t i = blockIdx.x * W + warp; i < n; i += gridDim.x * W)
 	{
@@ -863,7 +927,7 @@ void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint3
 template <int W>
 void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
 {
-	size_t smem = (size_t)W * 2 * maxUE * sizeof(EdgeRec);
+	size_t smem = (size_t)W * sat_warp_recs(maxUE) * sizeof(EdgeRec);
 	static size_t configured = 0;
 	if (smem > 48 * 1024 && smem > configured)
 	{
@@ -912,7 +976,7 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 // Dynamic shared memory of the SAT kernel with `warps` warps per block.
 size_t hull_sat_smem(int warps, uint32_t maxUE)
 {
-	return (size_t)warps * 2 * maxUE * sizeof(EdgeRec);
+	return (size_t)warps * sat_warp_recs(maxUE) * sizeof(EdgeRec);
 }
 
 void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s)
