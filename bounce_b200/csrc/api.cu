@@ -397,6 +397,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.prevFound, C), "alloc");
 	step(dalloc(&B.rawA, C), "alloc");
 	step(dalloc(&B.rawB, C), "alloc");
+	step(dalloc(&B.travOverflow, C), "alloc");
 	step(dalloc(&B.newList, C), "alloc");
 	step(dalloc(&B.newOff, (size_t)P + 1), "alloc");
 	step(dalloc(&B.newFill, (size_t)P + 1), "alloc");
@@ -489,6 +490,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.prevFound);
 	dfree(B.rawA);
 	dfree(B.rawB);
+	dfree(B.travOverflow);
 	dfree(B.newList);
 	dfree(B.newOff);
 	dfree(B.newFill);

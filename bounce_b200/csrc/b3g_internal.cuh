@@ -169,6 +169,7 @@ struct Buffers
 	uint32_t* scanAux;
 	uint32_t* rawA;       // overlapping pairs in traversal order (this pass)
 	uint32_t* rawB;
+	uint4* travOverflow;  // records past a leaf's scratch slots: A, B, leaf, index in the leaf
 
 	// contact-list order: new contacts, then the kept previous ones
 	uint32_t* newList;    // raw indices of pairs without a previous contact
@@ -253,7 +254,8 @@ enum
 	CTR_ASLEEP = 29,    // non-static bodies still asleep after the wake-ups
 	CTR_SCRATCH = 30,
 	CTR_MESH_PAIRS = 31, // (contact, triangle) work items of the pass
-	CTR_COUNT = 32
+	CTR_TRAV_OVERFLOW = 32, // traversal records past the scratch slots
+	CTR_COUNT = 33
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 

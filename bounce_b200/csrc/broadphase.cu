@@ -635,17 +635,16 @@ __device__ __forceinline__ uint2 canon_pair(const DevScene& S, uint32_t pa, uint
 }
 
 // Rope walk from leaf j's own rope. A node is read as two float4:
-// (lower, left child | proxy) and (upper, rope). MODE 0 counts the filtered
-// overlaps and keeps the first TRAV_SLOTS contact records in the leaf's
-// scratch slots (slot-major); MODE 1 writes the records past the first
-// TRAV_SLOTS from `base` (leaves whose partners did not fit). MW: several
-// worlds share the tree, so the walk stops at the first node past the query's
-// world (worlds are contiguous in depth-first order).
+// (lower, left child | proxy) and (upper, rope). The walk counts the filtered
+// overlaps, keeps the first TRAV_SLOTS contact records in the leaf's scratch
+// slots (slot-major) and appends the others, with their leaf and index, to
+// the overflow list. MW: several worlds share the tree, so the walk stops at
+// the first node past the query's world (worlds are contiguous in
+// depth-first order).
 constexpr uint32_t TRAV_SLOTS = B3G_TRAV_SLOTS;
 
-template <int MODE, bool MW>
-__device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cur, uint32_t cap,
-	uint32_t base)
+template <bool MW>
+__device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cap)
 {
 	uint32_t leaf = n - 1 + j;
 	float4 ql = B.nodeLo[leaf], qh = B.nodeHi[leaf];
@@ -679,20 +678,14 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 			uint32_t pb = __float_as_uint(lo.w);
 			if (pair_filter(S, pa, pb))
 			{
-				if (MODE == 0)
+				uint2 p = canon_pair(S, pa, pb);
+				if (count < TRAV_SLOTS)
+					scratch[(size_t)count * n + j] = p;
+				else
 				{
-					if (count < TRAV_SLOTS)
-						scratch[(size_t)count * n + j] = canon_pair(S, pa, pb);
-				}
-				else if (count >= TRAV_SLOTS)
-				{
-					uint32_t slot = base + count;
-					if (slot < cap)
-					{
-						uint2 p = canon_pair(S, pa, pb);
-						B.rawA[slot] = p.x;
-						B.rawB[slot] = p.y;
-					}
+					uint32_t o = atomicAdd(&B.counters[CTR_TRAV_OVERFLOW], 1u);
+					if (o < cap)
+						B.travOverflow[o] = make_uint4(p.x, p.y, (uint32_t)j, count);
 				}
 				++count;
 			}
@@ -713,14 +706,12 @@ __global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uin
 		B.leafCount[j] = 0;
 		return;
 	}
-	B.leafCount[j] = walk<0, MW>(S, B, n, j, cur, cap, 0);
+	B.leafCount[j] = walk<MW>(S, B, n, j, cap);
 }
 
 // One thread per (slot, leaf), slot-major: copies the scratch records to the
 // contact arrays. After the exclusive scan leafCount holds offsets; a leaf's
 // count is the difference to the next offset (the last one to the total).
-// Slot-0 threads of leaves with more than TRAV_SLOTS partners walk again for
-// the rest.
 template <bool MW>
 __global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
 {
@@ -741,8 +732,24 @@ __global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint
 			B.rawB[slot] = p.y;
 		}
 	}
-	if (k == 0 && count > TRAV_SLOTS)
-		walk<1, MW>(S, B, n, (int)j, cur, cap, base);
+}
+
+// The overflow records: record k of leaf j goes to leafCount[j] + k. A list
+// longer than the contact capacity means more pairs than contacts fit, which
+// the status already reports.
+__global__ void k_traverse_overflow(Buffers B, uint32_t cap)
+{
+	uint32_t n = min(B.counters[CTR_TRAV_OVERFLOW], cap);
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint4 r = B.travOverflow[t];
+		uint32_t slot = B.leafCount[r.z] + r.w;
+		if (slot < cap)
+		{
+			B.rawA[slot] = r.x;
+			B.rawB[slot] = r.y;
+		}
+	}
 }
 
 // Multi-block exclusive scan of u32 (in place) with the total written to *total.
@@ -813,7 +820,7 @@ uint32_t broadphase_launches(const b3g_ctx* c)
 	while ((1u << wb) < c->nWorlds)
 		++wb;
 	uint32_t passes = 4 + (wb + 7) / 8;
-	return 3 + 3 * passes + (n > 1 ? 1 : 0) + 2 + 2 + 3;
+	return 3 + 3 * passes + (n > 1 ? 1 : 0) + 2 + 2 + 3 + 1; // + the traversal overflow copy
 }
 
 void launch_broadphase(b3g_ctx* c, cudaStream_t s)
@@ -880,6 +887,7 @@ void launch_traverse(b3g_ctx* c, cudaStream_t s)
 	if (n == 0)
 		return;
 	const int tb = (int)c->tune.v[B3G_TUNE_TRAVERSE];
+	cudaMemsetAsync(B.counters + CTR_TRAV_OVERFLOW, 0, sizeof(uint32_t), s);
 	if (c->nWorlds > 1)
 		k_traverse_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
@@ -889,4 +897,5 @@ void launch_traverse(b3g_ctx* c, cudaStream_t s)
 		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else
 		k_traverse_emit<false><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+	k_traverse_overflow<<<persistent_blocks(2), 256, 0, s>>>(B, c->cfg.max_contacts);
 }
