@@ -376,15 +376,27 @@ def run_ours(args, rank, world, local, dist):
     k0 = n_dev
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    # Each step: host state in, contact list and touching manifolds out
+    # (b3g_fetch_results_async: the copies of step k travel while step k + 1
+    # runs; the host takes step k's results before it starts step k + 2).
+    from bounce_b200 import _native as N
+
+    pending = False
     for k in range(k0, k0 + args.e2e_steps):
         h_state.numpy()[:] = states[k]
         pipe.collide(h_state.numpy())
-        nc = pipe._check(lib.b3g_fetch_contacts(pipe.ctx, ctypes.cast(h_contacts.data_ptr(), ctypes.POINTER(ctypes.c_uint32)), nmax))
-        nt = pipe._check(lib.b3g_fetch_touching(pipe.ctx, ctypes.cast(h_index.data_ptr(), ctypes.POINTER(ctypes.c_uint32)),
-                                                ctypes.c_void_p(h_man.data_ptr()), nmax))
+        if pending:
+            pipe.wait_results()
+        cnt = N.Counts()
+        pipe._check(lib.b3g_fetch_results_async(pipe.ctx, ctypes.c_void_p(h_contacts.data_ptr()), nmax,
+                                                ctypes.c_void_p(h_index.data_ptr()), ctypes.c_void_p(h_man.data_ptr()),
+                                                nmax, ctypes.byref(cnt)))
+        pending = True
+        nc, nt = cnt.contacts, cnt.manifolds
         e2e_m += nt
         e2e_h2d += 17 * 4 * nb
         e2e_d2h += nc * 12 + nt * (4 + 320)
+    pipe.wait_results()
     t1 = time.perf_counter()
     e2e_s = t1 - t0
     e2e_value = e2e_m / e2e_s

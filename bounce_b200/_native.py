@@ -105,6 +105,8 @@ EXPORTED = [
     "b3g_fetch_manifolds",
     "b3g_fetch_touching",
     "b3g_fetch_ended",
+    "b3g_fetch_results_async",
+    "b3g_wait_results",
     "b3g_fetch_awake",
     "b3g_fetch_caches",
     "b3g_fetch_fat_aabbs",
@@ -170,6 +172,8 @@ def load():
         "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_ended": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_results_async": ([ctx, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, _p(Counts)], ctypes.c_int),
+        "b3g_wait_results": ([ctx], ctypes.c_int),
         "b3g_fetch_awake": ([ctx, u8p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_caches": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_fat_aabbs": ([ctx, f32p, ctypes.c_uint32], ctypes.c_int),

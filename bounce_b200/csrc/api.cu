@@ -354,6 +354,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	};
 	step(cudaSetDevice(cfg->device), "cudaSetDevice");
 	step(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+	step(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+	step(cudaEventCreateWithFlags(&c->copyReady, cudaEventDisableTiming), "cudaEventCreate");
+	step(cudaEventCreateWithFlags(&c->copyDone, cudaEventDisableTiming), "cudaEventCreate");
 	const uint32_t P = cfg->max_proxies, C = cfg->max_contacts;
 	Buffers& B = c->buf;
 	step(dalloc(&B.fatLo, P), "alloc");
@@ -558,6 +561,15 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->dUpdateBad);
 	if (c->hCounters)
 		cudaFreeHost(c->hCounters);
+	if (c->copyStream)
+	{
+		cudaStreamSynchronize(c->copyStream);
+		cudaStreamDestroy(c->copyStream);
+	}
+	if (c->copyReady)
+		cudaEventDestroy(c->copyReady);
+	if (c->copyDone)
+		cudaEventDestroy(c->copyDone);
 	if (c->stream)
 		cudaStreamDestroy(c->stream);
 	delete c;
@@ -1332,6 +1344,14 @@ static void issue_pass(b3g_ctx* c, cudaStream_t s, const float* state, size_t by
 	launch_narrowphase(c, s);
 }
 
+// Work that rewrites the contact records or the touching output waits for
+// the copies b3g_fetch_results_async started from them.
+static void wait_copies(b3g_ctx* c, cudaStream_t s)
+{
+	if (c->copyPending)
+		cudaStreamWaitEvent(s, c->copyDone, 0);
+}
+
 extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* stream)
 {
 	if (!c || !state)
@@ -1390,6 +1410,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			g.state = state;
 			g.stream = s;
 		}
+		wait_copies(c, s);
 		CK(cudaGraphLaunch(g.exec, s));
 		++c->graphLaunches;
 	}
@@ -1410,6 +1431,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			if (rc)
 				return fail(c, rc, "b3g_collide: wake-up rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
 		}
+		wait_copies(c, s);
 		launch_finalize(c, s);
 		prof_mark(c, PM_FINAL, s);
 		if (c->profiling)
@@ -1526,6 +1548,7 @@ extern "C" int b3g_fetch_touching(b3g_ctx* c, uint32_t* index, void* manifolds, 
 		return 0;
 	uint32_t* offsets = B.leafCount; // sized max(P, C)
 	const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
+	wait_copies(c, c->stream);
 	k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, offsets);
 	scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
 	uint32_t total = 0;
@@ -1543,6 +1566,74 @@ extern "C" int b3g_fetch_touching(b3g_ctx* c, uint32_t* index, void* manifolds, 
 		CK(cudaMemcpy(manifolds, B.touchMan, sizeof(DevManifold) * m, cudaMemcpyDeviceToHost));
 	}
 	return (int)m;
+}
+
+extern "C" int b3g_fetch_results_async(b3g_ctx* c, uint32_t* contacts, uint32_t contactCapacity, uint32_t* index,
+	void* manifolds, uint32_t touchCapacity, b3g_counts* counts)
+{
+	if (!c || !counts || (contactCapacity && !contacts) || (touchCapacity && (!index || !manifolds)))
+		return fail(c, B3G_E_INVALID, "null argument");
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "no pass yet");
+	CK(cudaSetDevice(c->device));
+	// The pass's counters (sizes of the outputs); only the pass stream is
+	// waited for, so copies of earlier passes keep running.
+	CK(cudaMemcpyAsync(c->hCounters, c->buf.counters, sizeof(uint32_t) * CTR_COUNT, cudaMemcpyDeviceToHost,
+		c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	const uint32_t* h = c->hCounters;
+	const uint32_t n = std::min(h[CTR_PAIRS], c->cfg.max_contacts);
+	counts->contacts = n;
+	counts->begun = h[CTR_BEGUN];
+	counts->ended = h[CTR_ENDED];
+	counts->touching = h[CTR_TOUCHING];
+	counts->manifolds = h[CTR_MANIFOLDS];
+	counts->points = h[CTR_POINTS];
+	counts->moved = h[CTR_MOVED];
+	counts->status = status_code(h[CTR_STATUS]);
+	if (counts->status)
+		return fail(c, -(int)counts->status, "pass status 0x%x (pairs %u, capacity %u)", h[CTR_STATUS], h[CTR_PAIRS],
+			c->cfg.max_contacts);
+	const uint32_t total = h[CTR_MANIFOLDS]; // manifolds with points = the touching output
+	if (total > c->cfg.max_contacts)
+		return fail(c, B3G_E_CAPACITY, "b3g_fetch_results_async: %u manifolds exceed the output buffer", total);
+	Buffers& B = c->buf;
+	wait_copies(c, c->stream);
+	if (n && touchCapacity)
+	{
+		uint32_t* offsets = B.leafCount;
+		const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
+		k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, offsets);
+		scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
+		k_touch_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], offsets, n,
+			B.touchIndex, B.touchMan);
+	}
+	CK(cudaEventRecord(c->copyReady, c->stream));
+	CK(cudaStreamWaitEvent(c->copyStream, c->copyReady, 0));
+	const uint32_t nc = std::min(n, contactCapacity);
+	if (nc)
+		CK(cudaMemcpyAsync(contacts, B.contactOut, sizeof(uint32_t) * 3 * nc, cudaMemcpyDeviceToHost, c->copyStream));
+	const uint32_t nt = std::min(total, touchCapacity);
+	if (n && nt)
+	{
+		CK(cudaMemcpyAsync(index, B.touchIndex, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c->copyStream));
+		CK(cudaMemcpyAsync(manifolds, B.touchMan, sizeof(DevManifold) * nt, cudaMemcpyDeviceToHost, c->copyStream));
+	}
+	CK(cudaEventRecord(c->copyDone, c->copyStream));
+	c->copyPending = true;
+	return B3G_OK;
+}
+
+extern "C" int b3g_wait_results(b3g_ctx* c)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if (c->copyPending)
+	{
+		CK(cudaSetDevice(c->device));
+		CK(cudaEventSynchronize(c->copyDone));
+	}
+	return B3G_OK;
 }
 
 extern "C" int b3g_fetch_ended(b3g_ctx* c, uint32_t* out, uint32_t capacity)

@@ -295,6 +295,10 @@ struct b3g_ctx
 	cudaStream_t stream;
 	std::string err;
 	uint32_t treeLeaves;  // leaves of the LBVH built by the last pass
+	cudaStream_t copyStream;  // device-to-host copies of b3g_fetch_results_async
+	cudaEvent_t copyReady;    // results of the pass ready to copy
+	cudaEvent_t copyDone;     // those copies finished
+	bool copyPending;
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
 

@@ -129,6 +129,20 @@ class CollisionPipeline:
         m = self._check(self.lib.b3g_fetch_touching(self.ctx, N.ptr(idx, u32), ctypes.c_void_p(man.ctypes.data), n))
         return idx[:m], man[:m]
 
+    def fetch_results_async(self, contacts, index, manifolds):
+        """Starts the copies of the last pass's contact records and touching
+        output into the given host arrays ((C, 3) u32, (T,) u32, (T,)
+        MANIFOLD_DTYPE); returns the pass counts. Read the arrays after
+        wait_results()."""
+        c = N.Counts()
+        self._check(self.lib.b3g_fetch_results_async(
+            self.ctx, ctypes.c_void_p(contacts.ctypes.data), len(contacts), ctypes.c_void_p(index.ctypes.data),
+            ctypes.c_void_p(manifolds.ctypes.data), min(len(index), len(manifolds)), ctypes.byref(c)))
+        return c.as_dict()
+
+    def wait_results(self):
+        self._check(self.lib.b3g_wait_results(self.ctx))
+
     def ended(self):
         c = self.counts()
         out = np.zeros((max(c["ended"], 1), 3), np.uint32)

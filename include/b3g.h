@@ -273,6 +273,19 @@ int b3g_fetch_manifolds(b3g_ctx* ctx, void* out, uint32_t capacity);
  * b3g_fetch_manifolds returns the first manifold of each contact. */
 int b3g_fetch_touching(b3g_ctx* ctx, uint32_t* index, void* manifolds, uint32_t capacity);
 
+/* The last pass's contact records (as b3g_fetch_contacts) and touching
+ * output (as b3g_fetch_touching) copied to host buffers asynchronously, on a
+ * stream of their own, so that the next b3g_collide runs while they travel.
+ * Waits for the pass itself, fills *counts, starts the copies and returns;
+ * the buffers hold the results once b3g_wait_results returns (pinned host
+ * memory makes the copies asynchronous). The next pass waits for the copies
+ * only before rewriting the contact records, at its end. */
+int b3g_fetch_results_async(b3g_ctx* ctx, uint32_t* contacts, uint32_t contact_capacity, uint32_t* index,
+	void* manifolds, uint32_t touch_capacity, b3g_counts* counts);
+
+/* Waits for the copies of the last b3g_fetch_results_async. */
+int b3g_wait_results(b3g_ctx* ctx);
+
 /* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above
  * (flags of the destroyed contact), in the order UpdateContacts destroys them.
  * Replaces the Destroy calls of UpdateContacts (contact_manager.cpp:270-281). */

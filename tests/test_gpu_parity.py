@@ -168,3 +168,36 @@ def test_mostly_sleeping(oracle_mod):
     sc = S.mixed_scene(seed=13, n=2500, side=15.0, static_frac=0.05, sensor_frac=0.03).finalize()
     woken = run_sleeping(oracle_mod, sc, 8, "mostly-asleep", seed=7, sleep_frac=0.8)
     assert woken > 0
+
+
+def test_async_results_match_sync():
+    """b3g_fetch_results_async, with the next pass running while the copies
+    travel, returns what the synchronous fetches return for the same pass."""
+    sc = S.mixed_scene(seed=17, n=3000, side=18.0).finalize()
+    drv = S.KinematicDriver(sc)
+    sync_pipe = CollisionPipeline(sc)
+    async_pipe = CollisionPipeline(sc)
+    cap = 200000
+    bufs = [(np.zeros((cap, 3), np.uint32), np.zeros(cap, np.uint32), np.zeros(cap, S.N.MANIFOLD_DTYPE))
+            for _ in range(2)]
+    pending = None
+    expected = []
+    for k in range(6):
+        state = drv.state17()
+        sync_pipe.collide(state)
+        expected.append((sync_pipe.contacts().copy(), *[x.copy() for x in sync_pipe.touching()]))
+        async_pipe.collide(state)  # runs while the previous pass's copies travel
+        if pending is not None:
+            async_pipe.wait_results()
+            j, cnt = pending
+            c, i, m = bufs[j]
+            want_c, want_i, want_m = expected[k - 1]
+            assert np.array_equal(c[:cnt["contacts"]], want_c)
+            assert np.array_equal(i[:cnt["manifolds"]], want_i)
+            assert np.array_equal(m[:cnt["manifolds"]].view(np.uint8), want_m.view(np.uint8))
+        j = k % 2
+        pending = (j, async_pipe.fetch_results_async(*bufs[j]))
+        drv.advance()
+    async_pipe.wait_results()
+    sync_pipe.close()
+    async_pipe.close()
