@@ -106,6 +106,7 @@ EXPORTED = [
     "b3g_fetch_touching",
     "b3g_fetch_ended",
     "b3g_fetch_results_async",
+    "b3g_fetch_results_packed_async",
     "b3g_wait_results",
     "b3g_fetch_awake",
     "b3g_fetch_caches",
@@ -173,6 +174,8 @@ def load():
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_ended": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_results_async": ([ctx, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, _p(Counts)], ctypes.c_int),
+        "b3g_fetch_results_packed_async": ([ctx, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64,
+                                            _p(Counts)], ctypes.c_int),
         "b3g_wait_results": ([ctx], ctypes.c_int),
         "b3g_fetch_awake": ([ctx, u8p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_caches": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),

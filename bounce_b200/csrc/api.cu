@@ -164,6 +164,53 @@ __global__ void k_touch_scatter(const DevManifold* man, const DevManifold* extra
 	}
 }
 
+// Packed touching output: per manifold with points, its 32-byte tail
+// (pointCount, impulses, speeds: the b3Manifold fields after points) then
+// its pointCount points (72 bytes each).
+__global__ void k_pack_sizes(const DevManifold* man, const DevManifold* extra, const uint32_t* cstate, uint32_t n,
+	uint32_t* count, uint32_t* bytes)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n)
+		return;
+	uint32_t mc = (cstate[c] >> 8) & 0xFFu;
+	uint32_t k = 0, b = 0;
+	for (uint32_t j = 0; j < mc && j < 3; ++j)
+	{
+		const DevManifold& m = j == 0 ? man[c] : extra[2 * (size_t)c + j - 1];
+		uint32_t pc = m.pointCount;
+		k += pc > 0 ? 1u : 0u;
+		b += pc > 0 ? 32u + 72u * pc : 0u;
+	}
+	count[c] = k;
+	bytes[c] = b;
+}
+
+__global__ void k_pack_scatter(const DevManifold* man, const DevManifold* extra, const uint32_t* cstate, uint32_t n,
+	const uint32_t* countOff, const uint32_t* byteOff, uint32_t* index, unsigned long long* out)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n)
+		return;
+	uint32_t mc = (cstate[c] >> 8) & 0xFFu;
+	uint32_t o = countOff[c];
+	size_t w = byteOff[c] / 8; // every record is a multiple of 8 bytes
+	for (uint32_t j = 0; j < mc && j < 3; ++j)
+	{
+		const DevManifold& m = j == 0 ? man[c] : extra[2 * (size_t)c + j - 1];
+		uint32_t pc = m.pointCount;
+		if (pc == 0)
+			continue;
+		index[o++] = c;
+		const unsigned long long* tail = reinterpret_cast<const unsigned long long*>(&m.pointCount);
+		for (int q = 0; q < 4; ++q)
+			out[w++] = tail[q];
+		const unsigned long long* pts = reinterpret_cast<const unsigned long long*>(m.points);
+		for (uint32_t q = 0; q < 9 * pc; ++q)
+			out[w++] = pts[q];
+	}
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -568,6 +615,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	}
 	if (c->copyReady)
 		cudaEventDestroy(c->copyReady);
+	if (c->touchBytes)
+		cudaFree(c->touchBytes);
 	if (c->copyDone)
 		cudaEventDestroy(c->copyDone);
 	if (c->stream)
@@ -1618,6 +1667,66 @@ extern "C" int b3g_fetch_results_async(b3g_ctx* c, uint32_t* contacts, uint32_t 
 	{
 		CK(cudaMemcpyAsync(index, B.touchIndex, sizeof(uint32_t) * nt, cudaMemcpyDeviceToHost, c->copyStream));
 		CK(cudaMemcpyAsync(manifolds, B.touchMan, sizeof(DevManifold) * nt, cudaMemcpyDeviceToHost, c->copyStream));
+	}
+	CK(cudaEventRecord(c->copyDone, c->copyStream));
+	c->copyPending = true;
+	return B3G_OK;
+}
+
+extern "C" int b3g_fetch_results_packed_async(b3g_ctx* c, uint32_t* contacts, uint32_t contactCapacity,
+	uint32_t* index, void* packed, uint32_t touchCapacity, uint64_t packedCapacity, b3g_counts* counts)
+{
+	if (!c || !counts || (contactCapacity && !contacts) || (touchCapacity && (!index || !packed)))
+		return fail(c, B3G_E_INVALID, "null argument");
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "no pass yet");
+	CK(cudaSetDevice(c->device));
+	CK(cudaMemcpyAsync(c->hCounters, c->buf.counters, sizeof(uint32_t) * CTR_COUNT, cudaMemcpyDeviceToHost,
+		c->stream));
+	CK(cudaStreamSynchronize(c->stream));
+	const uint32_t* h = c->hCounters;
+	const uint32_t n = std::min(h[CTR_PAIRS], c->cfg.max_contacts);
+	counts->contacts = n;
+	counts->begun = h[CTR_BEGUN];
+	counts->ended = h[CTR_ENDED];
+	counts->touching = h[CTR_TOUCHING];
+	counts->manifolds = h[CTR_MANIFOLDS];
+	counts->points = h[CTR_POINTS];
+	counts->moved = h[CTR_MOVED];
+	counts->status = status_code(h[CTR_STATUS]);
+	if (counts->status)
+		return fail(c, -(int)counts->status, "pass status 0x%x (pairs %u, capacity %u)", h[CTR_STATUS], h[CTR_PAIRS],
+			c->cfg.max_contacts);
+	const uint32_t total = h[CTR_MANIFOLDS];
+	const uint64_t bytes = 32ull * total + 72ull * h[CTR_POINTS];
+	if (total > c->cfg.max_contacts)
+		return fail(c, B3G_E_CAPACITY, "b3g_fetch_results_packed_async: %u manifolds exceed the output buffer", total);
+	if (touchCapacity && (total > touchCapacity || bytes > packedCapacity))
+		return fail(c, B3G_E_CAPACITY, "b3g_fetch_results_packed_async: %u manifolds, %llu bytes do not fit", total,
+			(unsigned long long)bytes);
+	Buffers& B = c->buf;
+	if (!c->touchBytes)
+		CK(cudaMalloc((void**)&c->touchBytes, sizeof(uint32_t) * std::max<size_t>(c->cfg.max_contacts, 1)));
+	wait_copies(c, c->stream);
+	if (n && touchCapacity)
+	{
+		const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
+		k_pack_sizes<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, B.leafCount,
+			c->touchBytes);
+		scan_exclusive(B.leafCount, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
+		scan_exclusive(c->touchBytes, n, B.scanAux, B.counters + CTR_SCRATCH, c->stream);
+		k_pack_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, B.leafCount,
+			c->touchBytes, B.touchIndex, reinterpret_cast<unsigned long long*>(B.touchMan));
+	}
+	CK(cudaEventRecord(c->copyReady, c->stream));
+	CK(cudaStreamWaitEvent(c->copyStream, c->copyReady, 0));
+	const uint32_t nc = std::min(n, contactCapacity);
+	if (nc)
+		CK(cudaMemcpyAsync(contacts, B.contactOut, sizeof(uint32_t) * 3 * nc, cudaMemcpyDeviceToHost, c->copyStream));
+	if (n && touchCapacity && total)
+	{
+		CK(cudaMemcpyAsync(index, B.touchIndex, sizeof(uint32_t) * total, cudaMemcpyDeviceToHost, c->copyStream));
+		CK(cudaMemcpyAsync(packed, B.touchMan, (size_t)bytes, cudaMemcpyDeviceToHost, c->copyStream));
 	}
 	CK(cudaEventRecord(c->copyDone, c->copyStream));
 	c->copyPending = true;

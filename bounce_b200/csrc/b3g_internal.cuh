@@ -299,6 +299,7 @@ struct b3g_ctx
 	cudaEvent_t copyReady;    // results of the pass ready to copy
 	cudaEvent_t copyDone;     // those copies finished
 	bool copyPending;
+	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds (allocated on first use)
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
 

@@ -140,6 +140,30 @@ class CollisionPipeline:
             ctypes.c_void_p(manifolds.ctypes.data), min(len(index), len(manifolds)), ctypes.byref(c)))
         return c.as_dict()
 
+    def fetch_results_packed_async(self, contacts, index, packed):
+        """As fetch_results_async with the touching output packed into the
+        byte array `packed` (see unpack_manifolds)."""
+        c = N.Counts()
+        self._check(self.lib.b3g_fetch_results_packed_async(
+            self.ctx, ctypes.c_void_p(contacts.ctypes.data), len(contacts), ctypes.c_void_p(index.ctypes.data),
+            ctypes.c_void_p(packed.ctypes.data), len(index), packed.nbytes, ctypes.byref(c)))
+        return c.as_dict()
+
+    @staticmethod
+    def unpack_manifolds(packed, count):
+        """b3Manifold records (MANIFOLD_DTYPE) from `count` packed records;
+        point slots past pointCount are zero."""
+        out = np.zeros(count, N.MANIFOLD_DTYPE)
+        raw = out.view(np.uint8).reshape(count, 320)
+        src = np.asarray(packed).view(np.uint8).reshape(-1)
+        off = 0
+        for k in range(count):
+            raw[k, 288:320] = src[off:off + 32]
+            pc = int(src[off:off + 4].view(np.uint32)[0])
+            raw[k, 0:72 * pc] = src[off + 32:off + 32 + 72 * pc]
+            off += 32 + 72 * pc
+        return out
+
     def wait_results(self):
         self._check(self.lib.b3g_wait_results(self.ctx))
 

@@ -283,7 +283,19 @@ int b3g_fetch_touching(b3g_ctx* ctx, uint32_t* index, void* manifolds, uint32_t 
 int b3g_fetch_results_async(b3g_ctx* ctx, uint32_t* contacts, uint32_t contact_capacity, uint32_t* index,
 	void* manifolds, uint32_t touch_capacity, b3g_counts* counts);
 
-/* Waits for the copies of the last b3g_fetch_results_async. */
+/* b3g_fetch_results_async with the touching output packed: per manifold
+ * with points, the 32 bytes of b3Manifold that follow its points array
+ * (pointCount, tangentImpulse, motorImpulse, motorSpeed, tangentSpeed1,
+ * tangentSpeed2, padding) and then its pointCount points (72 bytes each,
+ * b3ManifoldPoint), back to back; index holds the contact of each record as
+ * in b3g_fetch_touching. The packed size is 32 * counts->manifolds +
+ * 72 * counts->points bytes (a full b3Manifold is 320 bytes), so less data
+ * crosses the host link; the host copies the records into b3Manifold. */
+int b3g_fetch_results_packed_async(b3g_ctx* ctx, uint32_t* contacts, uint32_t contact_capacity, uint32_t* index,
+	void* packed, uint32_t touch_capacity, uint64_t packed_capacity, b3g_counts* counts);
+
+/* Waits for the copies of the last b3g_fetch_results_async or
+ * b3g_fetch_results_packed_async. */
 int b3g_wait_results(b3g_ctx* ctx);
 
 /* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above

@@ -170,6 +170,33 @@ def test_mostly_sleeping(oracle_mod):
     assert woken > 0
 
 
+def test_packed_results_match_touching():
+    """The packed touching output unpacks to b3g_fetch_touching's records
+    (point slots past pointCount aside)."""
+    sc = S.mixed_scene(seed=19, n=3000, side=18.0).finalize()
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    for k in range(4):
+        pipe.collide(drv.state17())
+        drv.advance()
+        idx, man = pipe.touching()
+        contacts = np.zeros((200000, 3), np.uint32)
+        index = np.zeros(200000, np.uint32)
+        packed = np.zeros(200000 * 320, np.uint8)
+        cnt = pipe.fetch_results_packed_async(contacts, index, packed)
+        pipe.wait_results()
+        assert cnt["manifolds"] == len(idx)
+        assert np.array_equal(index[:len(idx)], idx)
+        assert np.array_equal(contacts[:cnt["contacts"]], pipe.contacts())
+        got = pipe.unpack_manifolds(packed, len(idx))
+        assert np.array_equal(got["pointCount"], man["pointCount"])
+        for f in ("tangentImpulse", "motorImpulse", "motorSpeed", "tangentSpeed1", "tangentSpeed2"):
+            assert np.array_equal(got[f], man[f]), f
+        mask = np.arange(4)[None, :] < man["pointCount"][:, None]
+        assert np.array_equal(got["points"][mask].view(np.uint8), man["points"][mask].view(np.uint8))
+    pipe.close()
+
+
 def test_async_results_match_sync():
     """b3g_fetch_results_async, with the next pass running while the copies
     travel, returns what the synchronous fetches return for the same pass."""
