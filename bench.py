@@ -385,15 +385,23 @@ def run_ours(args, rank, world, local, dist):
     from bounce_b200 import _native as N
 
     pending = False
+    host_s = [0.0, 0.0, 0.0]  # host seconds in collide, waiting for copies, fetch (waits for the pass)
     for k in range(k0, k0 + args.e2e_steps):
+        ta = time.perf_counter()
         pipe.collide(h_states[k - k0].numpy())
+        tb = time.perf_counter()
         if pending:
             pipe.wait_results()
+        tc = time.perf_counter()
         cnt = N.Counts()
         pipe._check(lib.b3g_fetch_results_packed_async(pipe.ctx, ctypes.c_void_p(h_contacts.data_ptr()), nmax,
                                                        ctypes.c_void_p(h_index.data_ptr()),
                                                        ctypes.c_void_p(h_man.data_ptr()), nmax, 320 * nmax,
                                                        ctypes.byref(cnt)))
+        td = time.perf_counter()
+        host_s[0] += tb - ta
+        host_s[1] += tc - tb
+        host_s[2] += td - tc
         pending = True
         nc, nt = cnt.contacts, cnt.manifolds
         e2e_m += nt
@@ -449,7 +457,10 @@ def run_ours(args, rank, world, local, dist):
             "config": config_dict(args, {"contacts_last_pass": c["contacts"], "touching_last_pass": c["touching"],
                                           "points_last_pass": c["points"]}),
             "e2e": {"value": e2e_value, "unit": "manifolds/s", "h2d_bytes_per_step": e2e_h2d // max(args.e2e_steps, 1),
-                    "d2h_bytes_per_step": e2e_d2h // max(args.e2e_steps, 1), "steps": args.e2e_steps},
+                    "d2h_bytes_per_step": e2e_d2h // max(args.e2e_steps, 1), "steps": args.e2e_steps,
+                    "host_ms_per_step": {"collide": 1e3 * host_s[0] / args.e2e_steps,
+                                         "wait_copies": 1e3 * host_s[1] / args.e2e_steps,
+                                         "fetch": 1e3 * host_s[2] / args.e2e_steps}},
             "gpu_launches": tot["launches"],
             "graph_passes": tot["graph_passes"],
             "launch_shapes": tuning,

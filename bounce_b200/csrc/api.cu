@@ -1415,14 +1415,25 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	// hull-triangle, finalize + pass_end + settle
 	const uint32_t passLaunches = 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
 		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
-	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && onDevice && !c->profiling && c->asleep == 0 &&
-		c->havePass && !c->creationPass && s != nullptr;
+	// Host state takes the graph path when it is pinned (a graph copies it
+	// asynchronously; pageable memory would need the synchronous copy).
+	bool pinnedHost = false;
+	if (!onDevice)
+	{
+		cudaPointerAttributes attr;
+		if (cudaPointerGetAttributes(&attr, state) == cudaSuccess)
+			pinnedHost = attr.type == cudaMemoryTypeHost;
+		else
+			cudaGetLastError();
+	}
+	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && (onDevice || pinnedHost) && !c->profiling &&
+		c->asleep == 0 && c->havePass && !c->creationPass && s != nullptr;
 	c->lastPassImpulses = c->impulsesLoaded;
 	if (graph)
 	{
 		c->cur ^= 1u;
 		PassGraph& g = c->graphs[c->cur][c->impulsesLoaded ? 1 : 0];
-		if (g.exec && g.stream == s && g.state != state)
+		if (g.exec && g.stream == s && g.kind == kind && g.state != state)
 		{
 			// Same pass, state at another address: re-point the copy node.
 			if (g.copyNode && cudaGraphExecMemcpyNodeSetParams1D(g.exec, g.copyNode, c->dBodyState, state, bytes,
@@ -1431,17 +1442,20 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			else
 				cudaGetLastError();
 		}
-		if (!g.exec || g.state != state || g.stream != s)
+		if (!g.exec || g.state != state || g.stream != s || g.kind != kind)
 		{
 			if (g.exec)
 				cudaGraphExecDestroy(g.exec);
 			if (g.graph)
 				cudaGraphDestroy(g.graph);
-			g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+			g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr, cudaMemcpyDefault};
 			// The captured kernels use the contact buffers of this parity and
 			// the host-side pass state every later pass of this parity has.
 			CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
 			issue_pass(c, s, state, bytes, kind, &g.copyNode);
+			// Copies of the previous results (b3g_fetch_results_async) finish
+			// before finalize rewrites the contact records.
+			cudaStreamWaitEvent(s, c->copyDone, cudaEventWaitExternal);
 			launch_finalize(c, s);
 			cudaError_t e = cudaStreamEndCapture(s, &g.graph);
 			if (e != cudaSuccess)
@@ -1453,13 +1467,13 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			if (e != cudaSuccess)
 			{
 				cudaGraphDestroy(g.graph);
-				g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+				g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr, cudaMemcpyDefault};
 				return fail(c, B3G_E_CUDA, "b3g_collide: graph instantiation failed: %s", cudaGetErrorString(e));
 			}
 			g.state = state;
 			g.stream = s;
+			g.kind = kind;
 		}
-		wait_copies(c, s);
 		CK(cudaGraphLaunch(g.exec, s));
 		++c->graphLaunches;
 	}

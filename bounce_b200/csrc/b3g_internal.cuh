@@ -276,6 +276,7 @@ struct PassGraph
 	cudaGraphNode_t copyNode;
 	const float* state;
 	cudaStream_t stream;
+	cudaMemcpyKind kind; // of the state copy node
 };
 
 // One staging block of b3g_update_scene.

@@ -199,11 +199,16 @@ def test_packed_results_match_touching():
 
 def test_async_results_match_sync():
     """b3g_fetch_results_async, with the next pass running while the copies
-    travel, returns what the synchronous fetches return for the same pass."""
+    travel, returns what the synchronous fetches return for the same pass;
+    the asynchronous context replays its passes from CUDA graphs fed with
+    pinned host state."""
+    import torch
+
     sc = S.mixed_scene(seed=17, n=3000, side=18.0).finalize()
     drv = S.KinematicDriver(sc)
     sync_pipe = CollisionPipeline(sc)
-    async_pipe = CollisionPipeline(sc)
+    async_pipe = CollisionPipeline(sc, graph=True)
+    pinned = [torch.empty(17 * sc.n_bodies, dtype=torch.float32).pin_memory() for _ in range(2)]
     cap = 200000
     bufs = [(np.zeros((cap, 3), np.uint32), np.zeros(cap, np.uint32), np.zeros(cap, S.N.MANIFOLD_DTYPE))
             for _ in range(2)]
@@ -213,7 +218,9 @@ def test_async_results_match_sync():
         state = drv.state17()
         sync_pipe.collide(state)
         expected.append((sync_pipe.contacts().copy(), *[x.copy() for x in sync_pipe.touching()]))
-        async_pipe.collide(state)  # runs while the previous pass's copies travel
+        host = pinned[k % 2].numpy()
+        host[:] = state
+        async_pipe.collide(host)  # runs while the previous pass's copies travel
         if pending is not None:
             async_pipe.wait_results()
             j, cnt = pending
@@ -226,5 +233,6 @@ def test_async_results_match_sync():
         pending = (j, async_pipe.fetch_results_async(*bufs[j]))
         drv.advance()
     async_pipe.wait_results()
+    assert async_pipe.totals()["graph_passes"] >= 3
     sync_pipe.close()
     async_pipe.close()
