@@ -273,6 +273,21 @@ def algorithmic_bytes(scene, counts):
     return int(scene.n_fixtures * (68 + 60 + 64 + 1) + hv)
 
 
+def committed_traffic(kernel, args):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/roofline_traffic.md), for the workload it was captured on."""
+    if args.workload != "mixed" or args.bodies != N_BODIES:
+        return None
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "roofline_traffic.md")):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) == 3 and cells[0] == kernel and cells[1] == "mixed 65,536":
+                return int(cells[2])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def run_ours(args, rank, world, local, dist):
     import torch
 
@@ -433,7 +448,7 @@ def run_ours(args, rank, world, local, dist):
         sb = algorithmic_bytes(scene, c)
         achieved = sb / (sync_ms / 1000.0) / 1e9 if sync_ms > 0 else 0.0
         roof = {"kernel": "k_sync (fat-AABB update)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": committed_traffic("k_sync", args),
                 "algorithmic_bytes_per_launch": sb,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
 
