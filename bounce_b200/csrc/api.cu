@@ -404,6 +404,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
 	step(cudaEventCreateWithFlags(&c->copyReady, cudaEventDisableTiming), "cudaEventCreate");
 	step(cudaEventCreateWithFlags(&c->copyDone, cudaEventDisableTiming), "cudaEventCreate");
+	step(cudaStreamCreateWithFlags(&c->sideStream, cudaStreamNonBlocking), "cudaStreamCreate");
+	step(cudaEventCreateWithFlags(&c->forkEvent, cudaEventDisableTiming), "cudaEventCreate");
+	step(cudaEventCreateWithFlags(&c->joinEvent, cudaEventDisableTiming), "cudaEventCreate");
 	const uint32_t P = cfg->max_proxies, C = cfg->max_contacts;
 	Buffers& B = c->buf;
 	step(dalloc(&B.fatLo, P), "alloc");
@@ -617,6 +620,15 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 		cudaEventDestroy(c->copyReady);
 	if (c->touchBytes)
 		cudaFree(c->touchBytes);
+	if (c->sideStream)
+	{
+		cudaStreamSynchronize(c->sideStream);
+		cudaStreamDestroy(c->sideStream);
+	}
+	if (c->forkEvent)
+		cudaEventDestroy(c->forkEvent);
+	if (c->joinEvent)
+		cudaEventDestroy(c->joinEvent);
 	if (c->copyDone)
 		cudaEventDestroy(c->copyDone);
 	if (c->stream)

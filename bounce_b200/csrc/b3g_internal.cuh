@@ -301,6 +301,8 @@ struct b3g_ctx
 	cudaEvent_t copyDone;     // those copies finished
 	bool copyPending;
 	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds (allocated on first use)
+	cudaStream_t sideStream;  // hull-hull / hull-triangle narrowphase, beside the convex buckets
+	cudaEvent_t forkEvent, joinEvent;
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
 

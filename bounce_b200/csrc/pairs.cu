@@ -237,13 +237,28 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	launch_mesh_prepare(c, s);
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
 	NPArgs a = make_np_args(c);
+	// The buckets are disjoint sets of contacts: the hull-hull and
+	// hull-triangle kernels run on a second stream beside the convex ones
+	// (joined before the mesh work; a stream capture takes both branches).
+	// Under profiling they stay on one stream so the stage marks hold.
+	cudaStream_t side = c->profiling ? s : c->sideStream;
+	if (side != s)
+	{
+		cudaEventRecord(c->forkEvent, s);
+		cudaStreamWaitEvent(side, c->forkEvent, 0);
+	}
+	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
+		c->maxUniqueEdges, c->tune, side);
+	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
+		c->maxUniqueEdges, c->tune, side);
 	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
 	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 	prof_mark(c, PM_CONVEX, s);
-	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
-		c->maxUniqueEdges, c->tune, s);
-	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
-		c->maxUniqueEdges, c->tune, s);
+	if (side != s)
+	{
+		cudaEventRecord(c->joinEvent, side);
+		cudaStreamWaitEvent(s, c->joinEvent, 0);
+	}
 	launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
 	prof_mark(c, PM_HULLS, s);
 }
