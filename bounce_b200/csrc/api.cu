@@ -407,6 +407,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(cudaStreamCreateWithFlags(&c->sideStream, cudaStreamNonBlocking), "cudaStreamCreate");
 	step(cudaEventCreateWithFlags(&c->forkEvent, cudaEventDisableTiming), "cudaEventCreate");
 	step(cudaEventCreateWithFlags(&c->joinEvent, cudaEventDisableTiming), "cudaEventCreate");
+	step(cudaStreamCreateWithFlags(&c->meshStream, cudaStreamNonBlocking), "cudaStreamCreate");
+	step(cudaEventCreateWithFlags(&c->meshFork, cudaEventDisableTiming), "cudaEventCreate");
+	step(cudaEventCreateWithFlags(&c->meshJoin, cudaEventDisableTiming), "cudaEventCreate");
 	const uint32_t P = cfg->max_proxies, C = cfg->max_contacts;
 	Buffers& B = c->buf;
 	step(dalloc(&B.fatLo, P), "alloc");
@@ -625,6 +628,15 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 		cudaStreamSynchronize(c->sideStream);
 		cudaStreamDestroy(c->sideStream);
 	}
+	if (c->meshStream)
+	{
+		cudaStreamSynchronize(c->meshStream);
+		cudaStreamDestroy(c->meshStream);
+	}
+	if (c->meshFork)
+		cudaEventDestroy(c->meshFork);
+	if (c->meshJoin)
+		cudaEventDestroy(c->meshJoin);
 	if (c->forkEvent)
 		cudaEventDestroy(c->forkEvent);
 	if (c->joinEvent)

@@ -302,7 +302,8 @@ struct b3g_ctx
 	bool copyPending;
 	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds (allocated on first use)
 	cudaStream_t sideStream;  // hull-hull / hull-triangle narrowphase, beside the convex buckets
-	cudaEvent_t forkEvent, joinEvent;
+	cudaStream_t meshStream;  // mesh midphase (tree queries, work items), beside both
+	cudaEvent_t forkEvent, joinEvent, meshFork, meshJoin;
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
 

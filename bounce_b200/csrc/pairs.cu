@@ -234,7 +234,18 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	uint32_t cap = c->cfg.max_contacts;
-	launch_mesh_prepare(c, s);
+	// Mesh midphase on its own stream beside the bucketing and the convex
+	// and hull kernels (joined before the mesh work items).
+	const bool meshSide = !c->profiling && c->nMeshFix;
+	cudaStream_t ms = meshSide ? c->meshStream : s;
+	if (meshSide)
+	{
+		cudaEventRecord(c->meshFork, s);
+		cudaStreamWaitEvent(ms, c->meshFork, 0);
+	}
+	launch_mesh_prepare(c, ms);
+	if (meshSide)
+		cudaEventRecord(c->meshJoin, ms);
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
 	NPArgs a = make_np_args(c);
 	// The buckets are disjoint sets of contacts: the hull-hull and
@@ -259,6 +270,8 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 		cudaEventRecord(c->joinEvent, side);
 		cudaStreamWaitEvent(s, c->joinEvent, 0);
 	}
+	if (meshSide)
+		cudaStreamWaitEvent(s, c->meshJoin, 0);
 	launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
 	prof_mark(c, PM_HULLS, s);
 }
