@@ -93,6 +93,21 @@ def dist_init(args):
     return rank, world, local, dist
 
 
+def replica_totals(dist, device, seconds, work):
+    """Replicas: the slowest rank's time and the work of all ranks
+    (max / sum all-reduce; device is "cuda:i" under NCCL, "cpu" under gloo)."""
+    if dist is None:
+        return seconds, work
+    import torch
+
+    t = torch.tensor([seconds, float(work)], device=device, dtype=torch.float64)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return float(tmax[0]), float(tsum[1])
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
@@ -366,16 +381,7 @@ def run_ours(args, rank, world, local, dist):
         pipe.set_profiling(False)
         assert pipe.counts()["status"] == 0
 
-    ms_max = ms
-    manifolds_all = tot["manifolds"]
-    if dist is not None:
-        t = torch.tensor([ms, float(tot["manifolds"])], device=dev, dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        ms_max = float(tmax[0])
-        manifolds_all = float(tsum[1])
+    ms_max, manifolds_all = replica_totals(dist, dev, ms, tot["manifolds"])
     value = manifolds_all / (ms_max / 1000.0)
 
     # e2e through the C ABI with host buffers (pinned), continuing the motion.
@@ -427,12 +433,8 @@ def run_ours(args, rank, world, local, dist):
     e2e_s = t1 - t0
     e2e_value = e2e_m / e2e_s
     if dist is not None:
-        t = torch.tensor([e2e_s, float(e2e_m)], device=dev, dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        e2e_value = float(tsum[1]) / float(tmax[0])
+        e2e_max, e2e_all = replica_totals(dist, dev, e2e_s, e2e_m)
+        e2e_value = e2e_all / e2e_max
 
     # Roofline of the dominant stage.
     roof = None
