@@ -419,7 +419,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.keysB, P), "alloc");
 	step(dalloc(&B.valsA, P), "alloc");
 	step(dalloc(&B.valsB, P), "alloc");
-	step(dalloc(&B.sortHist, 256 * ((P + 4095) / 4096 + 1)), "alloc");
+	step(dalloc(&B.sortHist, 256 * (9 + 8 * ((size_t)(P + 1023) / 1024 + 1))), "alloc"); // digit counts, tile status
 	step(dalloc(&B.sceneBounds, 8), "alloc");
 	step(dalloc(&B.nodeLo, 2 * P), "alloc");
 	step(dalloc(&B.nodeHi, 2 * P), "alloc");

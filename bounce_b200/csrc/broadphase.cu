@@ -365,32 +365,7 @@ __global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
 }
 
 // ---------------------------------------------------------------------------
-// LSD radix sort of (u64 key, u32 value), 8-bit digits, stable.
-// Tiles of 4096 elements (256 threads x 16). Per pass: per-tile digit
-// histograms, one exclusive scan in digit-major order, and a stable scatter
-// that ranks equal digits within a warp with __match_any_sync and across the
-// warps of a round through shared-memory prefix sums.
-
-constexpr int RS_THREADS = 256;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
-
-__global__ void k_rs_hist(const unsigned long long* keys, uint32_t n, int shift, uint32_t* hist,
-	uint32_t numTiles)
-{
-	__shared__ uint32_t h[256];
-	h[threadIdx.x] = 0;
-	__syncthreads();
-	uint32_t base = blockIdx.x * RS_TILE;
-	for (int k = 0; k < RS_ITEMS; ++k)
-	{
-		uint32_t idx = base + k * RS_THREADS + threadIdx.x;
-		if (idx < n)
-			atomicAdd(&h[(uint32_t)(keys[idx] >> shift) & 0xFFu], 1u);
-	}
-	__syncthreads();
-	hist[threadIdx.x * numTiles + blockIdx.x] = h[threadIdx.x];
-}
+// Scans.
 
 // Single-block exclusive scan of m entries (m <= 1024 * per-thread chunk).
 __global__ void k_scan_single(uint32_t* data, uint32_t m, uint32_t* total)
@@ -422,54 +397,160 @@ __global__ void k_scan_single(uint32_t* data, uint32_t m, uint32_t* total)
 		*total = s[threadIdx.x];
 }
 
-__global__ void k_rs_scatter(const unsigned long long* kin, const uint32_t* vin,
-	unsigned long long* kout, uint32_t* vout, uint32_t n, int shift, const uint32_t* hist,
-	uint32_t numTiles)
+// One-sweep LSD radix sort (Merrill & Garland's decoupled look-back): one
+// histogram kernel for every digit pass up front, then one kernel per pass.
+// A block ranks its tile's keys per digit in shared memory (stable: element
+// order within the tile), publishes the tile's digit counts, adds up the
+// counts of the tiles before it (walking back until a tile that already
+// published an inclusive prefix) and scatters. Tiles are taken in launch
+// order through a counter, so a tile only waits for tiles of blocks that
+// started before it; the waits are bounded all the same.
+constexpr int OS_THREADS = 256;
+constexpr int OS_ITEMS = 4;
+constexpr uint32_t OS_TILE = OS_THREADS * OS_ITEMS;
+constexpr uint32_t OS_AGG = 1u << 30;     // the tile's own count is published
+constexpr uint32_t OS_INC = 2u << 30;     // the count through this tile is published
+constexpr uint32_t OS_MASK = OS_AGG - 1u; // counts below 2^30
+constexpr uint32_t OS_SPIN = 1u << 22;
+
+struct SortShifts
 {
-	__shared__ uint32_t base[256];
+	int s[8];
+	int n;
+};
+
+__global__ void k_os_hist(const unsigned long long* keys, uint32_t n, SortShifts sh, uint32_t* ghist)
+{
+	__shared__ uint32_t h[8][256];
+	for (int p = 0; p < sh.n; ++p)
+		h[p][threadIdx.x] = 0;
+	__syncthreads();
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+	{
+		unsigned long long k = keys[i];
+		for (int p = 0; p < sh.n; ++p)
+			atomicAdd(&h[p][(uint32_t)(k >> sh.s[p]) & 0xFFu], 1u);
+	}
+	__syncthreads();
+	for (int p = 0; p < sh.n; ++p)
+		if (h[p][threadIdx.x])
+			atomicAdd(&ghist[p * 256 + threadIdx.x], h[p][threadIdx.x]);
+}
+
+// Exclusive scan of each pass's 256 digit counts (one block of 256 per pass).
+__global__ void k_os_scan(uint32_t* ghist)
+{
+	__shared__ uint32_t v[256];
+	uint32_t* g = ghist + blockIdx.x * 256;
+	uint32_t x = g[threadIdx.x];
+	v[threadIdx.x] = x;
+	__syncthreads();
+	for (uint32_t off = 1; off < 256; off <<= 1)
+	{
+		uint32_t y = threadIdx.x >= off ? v[threadIdx.x - off] : 0u;
+		__syncthreads();
+		v[threadIdx.x] += y;
+		__syncthreads();
+	}
+	g[threadIdx.x] = v[threadIdx.x] - x;
+}
+
+__global__ void __launch_bounds__(OS_THREADS) k_onesweep(const unsigned long long* kin, const uint32_t* vin,
+	unsigned long long* kout, uint32_t* vout, uint32_t n, int shift, const uint32_t* gOffset, uint32_t* status,
+	uint32_t* tileCounter, uint32_t* err)
+{
+	__shared__ uint32_t sTile;
 	__shared__ uint32_t run[256];
-	__shared__ uint32_t wc[RS_THREADS / 32][256];
+	__shared__ uint32_t wc[OS_THREADS / 32][256];
+	__shared__ uint32_t base[256];
 	const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-	base[t] = hist[t * numTiles + blockIdx.x];
+	if (t == 0)
+		sTile = atomicAdd(tileCounter, 1u);
 	run[t] = 0;
-	for (int w = 0; w < RS_THREADS / 32; ++w)
+	for (int w = 0; w < OS_THREADS / 32; ++w)
 		wc[w][t] = 0;
 	__syncthreads();
+	const uint32_t tile = sTile;
 	const uint32_t lt = (1u << lane) - 1u;
-	uint32_t tile = blockIdx.x * RS_TILE;
-	for (int r = 0; r < RS_ITEMS; ++r)
+	unsigned long long key[OS_ITEMS];
+	uint32_t val[OS_ITEMS], dig[OS_ITEMS], rank[OS_ITEMS];
+	for (int r = 0; r < OS_ITEMS; ++r)
 	{
-		uint32_t idx = tile + r * RS_THREADS + t;
+		uint32_t idx = tile * OS_TILE + r * OS_THREADS + t;
 		bool valid = idx < n;
-		unsigned long long key = valid ? kin[idx] : 0ull;
-		uint32_t val = valid ? vin[idx] : 0u;
-		uint32_t d = valid ? ((uint32_t)(key >> shift) & 0xFFu) : 0x100u;
+		key[r] = valid ? kin[idx] : 0ull;
+		val[r] = valid ? vin[idx] : 0u;
+		uint32_t d = valid ? ((uint32_t)(key[r] >> shift) & 0xFFu) : 0x100u;
+		dig[r] = d;
 		uint32_t peers = __match_any_sync(0xffffffffu, d);
-		uint32_t rank = __popc(peers & lt);
-		if (valid && rank == 0)
+		uint32_t pr = __popc(peers & lt);
+		if (valid && pr == 0)
 			wc[warp][d] = __popc(peers);
 		__syncthreads();
 		{
 			uint32_t sum = run[t];
-			for (int w = 0; w < RS_THREADS / 32; ++w)
+			for (int w = 0; w < OS_THREADS / 32; ++w)
 			{
-				uint32_t c = wc[w][t];
+				uint32_t cnt = wc[w][t];
 				wc[w][t] = sum;
-				sum += c;
+				sum += cnt;
 			}
 			run[t] = sum;
 		}
 		__syncthreads();
-		if (valid)
-		{
-			uint32_t pos = base[d] + wc[warp][d] + rank;
-			kout[pos] = key;
-			vout[pos] = val;
-		}
+		rank[r] = valid ? wc[warp][d] + pr : 0u;
 		__syncthreads();
-		for (int w = 0; w < RS_THREADS / 32; ++w)
+		for (int w = 0; w < OS_THREADS / 32; ++w)
 			wc[w][t] = 0;
 		__syncthreads();
+	}
+	// Thread t owns digit t: publish, look back, publish the inclusive prefix.
+	{
+		const uint32_t mine = run[t];
+		volatile uint32_t* st = status;
+		if (tile == 0)
+			st[t] = OS_INC | mine;
+		else
+		{
+			st[(size_t)tile * 256 + t] = OS_AGG | mine;
+			uint32_t prefix = 0;
+			int32_t look = (int32_t)tile - 1;
+			uint32_t spins = 0;
+			while (look >= 0)
+			{
+				uint32_t v = st[(size_t)look * 256 + t];
+				if ((v & ~OS_MASK) == 0u)
+				{
+					if (++spins > OS_SPIN)
+					{
+						atomicOr(err, B3G_ST_WAIT_TIMEOUT);
+						break;
+					}
+					continue;
+				}
+				prefix += v & OS_MASK;
+				if (v & OS_INC)
+					break;
+				--look;
+			}
+			__threadfence();
+			st[(size_t)tile * 256 + t] = OS_INC | (prefix + mine);
+			base[t] = gOffset[t] + prefix;
+		}
+		if (tile == 0)
+			base[t] = gOffset[t];
+	}
+	__syncthreads();
+	for (int r = 0; r < OS_ITEMS; ++r)
+	{
+		if (dig[r] > 0xFFu)
+			continue;
+		uint32_t pos = base[dig[r]] + rank[r];
+		if (pos < n)
+		{
+			kout[pos] = key[r];
+			vout[pos] = val[r];
+		}
 	}
 }
 
@@ -820,7 +901,7 @@ uint32_t broadphase_launches(const b3g_ctx* c)
 	while ((1u << wb) < c->nWorlds)
 		++wb;
 	uint32_t passes = 4 + (wb + 7) / 8;
-	return 3 + 3 * passes + (n > 1 ? 1 : 0) + 2 + 2 + 3 + 1; // + the traversal overflow copy
+	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 2 + 3 + 1; // sort: histogram, scan, one kernel per pass
 }
 
 void launch_broadphase(b3g_ctx* c, cudaStream_t s)
@@ -839,23 +920,29 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	k_morton<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
 
 	// Radix sort over the Morton bits and, for several worlds, the world bits.
-	uint32_t numTiles = (n + RS_TILE - 1) / RS_TILE;
-	int shifts[8];
-	int ns = 0;
+	SortShifts sh;
+	sh.n = 0;
 	for (int sft = 0; sft < 32; sft += 8)
-		shifts[ns++] = sft;
+		sh.s[sh.n++] = sft;
 	uint32_t wb = 0;
 	while ((1u << wb) < c->nWorlds)
 		++wb;
 	for (uint32_t sft = 0; sft < wb; sft += 8)
-		shifts[ns++] = 32 + (int)sft;
+		sh.s[sh.n++] = 32 + (int)sft;
+	const uint32_t numTiles = ((uint32_t)n + OS_TILE - 1) / OS_TILE;
+	// sortHist: digit counts (8 x 256), tile counters (256), tile status (8 x tiles x 256)
+	uint32_t* ghist = B.sortHist;
+	uint32_t* tileCounters = B.sortHist + 8 * 256;
+	uint32_t* status = B.sortHist + 9 * 256;
+	cudaMemsetAsync(B.sortHist, 0, sizeof(uint32_t) * (9 * 256 + (size_t)sh.n * numTiles * 256), s);
+	k_os_hist<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(B.keysA, (uint32_t)n, sh, ghist);
+	k_os_scan<<<sh.n, 256, 0, s>>>(ghist);
 	unsigned long long *kin = B.keysA, *kout = B.keysB;
 	uint32_t *vin = B.valsA, *vout = B.valsB;
-	for (int p = 0; p < ns; ++p)
+	for (int p = 0; p < sh.n; ++p)
 	{
-		k_rs_hist<<<numTiles, RS_THREADS, 0, s>>>(kin, n, shifts[p], B.sortHist, numTiles);
-		k_scan_single<<<1, 1024, 0, s>>>(B.sortHist, 256 * numTiles, nullptr);
-		k_rs_scatter<<<numTiles, RS_THREADS, 0, s>>>(kin, vin, kout, vout, n, shifts[p], B.sortHist, numTiles);
+		k_onesweep<<<numTiles, OS_THREADS, 0, s>>>(kin, vin, kout, vout, (uint32_t)n, sh.s[p], ghist + 256 * p,
+			status + (size_t)p * numTiles * 256, tileCounters + p, B.counters + CTR_STATUS);
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}
