@@ -317,7 +317,8 @@ def run_ours(args, rank, world, local, dist):
     # states: creation + warm-up, 2 passes that capture the tuned graphs, timed, profiled
     t0_k = 1 + args.warmup + 2
     n_dev = t0_k + args.steps + args.profile_steps
-    total = n_dev + args.e2e_steps
+    e2e_warm = 2  # untimed host-state passes: they capture the pinned-state graphs
+    total = n_dev + e2e_warm + args.e2e_steps
     nb = scene.n_bodies
     states = np.empty((total, 17 * nb), np.float32)
     states[0] = drv.state17()
@@ -391,12 +392,15 @@ def run_ours(args, rank, world, local, dist):
     h_man = torch.empty((nmax, 80), dtype=torch.int32, pin_memory=True)  # packed records fit in nmax * 320 bytes
     # The e2e steps' inputs sit in pinned host memory before the timed region
     # (the solver would write them there); each step copies its own.
-    h_states = torch.from_numpy(states[n_dev:n_dev + args.e2e_steps]).pin_memory()
+    h_states = torch.from_numpy(states[n_dev:n_dev + e2e_warm + args.e2e_steps]).pin_memory()
     import ctypes
 
     lib = pipe.lib
     e2e_m, e2e_h2d, e2e_d2h = 0, 0, 0
-    k0 = n_dev
+    for k in range(e2e_warm):
+        pipe.collide(h_states[k].numpy())
+    pipe.counts()
+    k0 = n_dev + e2e_warm
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     # Each step: host state in, contact list and touching manifolds out
@@ -409,7 +413,7 @@ def run_ours(args, rank, world, local, dist):
     host_s = [0.0, 0.0, 0.0]  # host seconds in collide, waiting for copies, fetch (waits for the pass)
     for k in range(k0, k0 + args.e2e_steps):
         ta = time.perf_counter()
-        pipe.collide(h_states[k - k0].numpy())
+        pipe.collide(h_states[k - n_dev].numpy())
         tb = time.perf_counter()
         if pending:
             pipe.wait_results()
