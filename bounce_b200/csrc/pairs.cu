@@ -263,7 +263,11 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
 		c->maxUniqueEdges, c->tune, side);
 	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
-	launch_convex_buckets(a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
+	// The hull-sphere kernel follows the hull kernels on the second stream,
+	// which evens the two branches out (the hull-capsule kernel is the
+	// longest of the convex ones).
+	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
+		launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, k == 5 ? side : s);
 	prof_mark(c, PM_CONVEX, s);
 	if (side != s)
 	{
