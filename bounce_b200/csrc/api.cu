@@ -432,6 +432,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.splitRight, P), "alloc");
 	step(dalloc(&B.refitFlag, P), "alloc");
 	step(dalloc(&B.worldEnd, P), "alloc");
+	step(dalloc(&B.proxyInfo, P), "alloc");
 	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
 	step(dalloc(&B.pairScratch, 2 * B3G_TRAV_SLOTS * (size_t)P), "alloc"); // uint2 records per leaf
 	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
@@ -529,6 +530,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.splitRight);
 	dfree(B.refitFlag);
 	dfree(B.worldEnd);
+	dfree(B.proxyInfo);
 	dfree(B.leafCount);
 	dfree(B.pairScratch);
 	dfree(B.scanAux);

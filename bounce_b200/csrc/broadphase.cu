@@ -155,6 +155,9 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int crea
 	for (int k = 0; k < 17; ++k)
 		sv[k] = st[k];
 	const uint32_t btype = S.bodyType[body];
+	// The walk's filter reads one word per proxy (pair_filter).
+	if (w0)
+		B.proxyInfo[i] = (body & 0x0FFFFFFFu) | (btype == B3G_BODY_DYNAMIC ? 1u << 28 : 0u) | (type << 29);
 	if (life == FIX_DEAD)
 	{
 		// No proxy: an empty box (lower > upper) that overlaps nothing.
@@ -691,14 +694,13 @@ __device__ __forceinline__ bool primary(uint32_t a, uint32_t b)
 // AddPair filters: same body (contact_manager.cpp:104-108), b3Body::ShouldCollide
 // (at least one dynamic body, body.cpp:240-246) and a registered shape pair
 // (b3Contact::Create returns nullptr otherwise, contact.cpp:318-321).
-__device__ __forceinline__ bool pair_filter(const DevScene& S, uint32_t pa, uint32_t pb)
+__device__ __forceinline__ bool pair_filter(uint32_t infoA, uint32_t infoB)
 {
-	uint32_t ba = S.fixBody[pa], bb = S.fixBody[pb];
-	if (ba == bb)
+	if (((infoA ^ infoB) & 0x0FFFFFFFu) == 0u)
 		return false;
-	if (S.bodyType[ba] != B3G_BODY_DYNAMIC && S.bodyType[bb] != B3G_BODY_DYNAMIC)
+	if (((infoA | infoB) & (1u << 28)) == 0u)
 		return false;
-	return registered(S.fixType[pa], S.fixType[pb]);
+	return registered(infoA >> 29, infoB >> 29);
 }
 
 // The contact record of overlapping proxies pa, pb: the broadphase order
@@ -728,8 +730,9 @@ template <bool MW>
 __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cap)
 {
 	uint32_t leaf = n - 1 + j;
-	float4 ql = B.nodeLo[leaf], qh = B.nodeHi[leaf];
+	float4 ql = __ldg(B.nodeLo + leaf), qh = __ldg(B.nodeHi + leaf);
 	uint32_t pa = __float_as_uint(ql.w);
+	const uint32_t infoA = __ldg(B.proxyInfo + pa);
 	uint32_t wend = MW ? B.worldEnd[S.bodyWorld[S.fixBody[pa]]] : 0xFFFFFFFFu;
 	uint32_t count = 0;
 	uint32_t node = __float_as_uint(qh.w);
@@ -747,7 +750,8 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 		}
 		if (MW && B.nodeFirst[node] > wend)
 			break;
-		float4 lo = B.nodeLo[node], hi = B.nodeHi[node];
+		// The tree is read-only here: the read-only data path caches it in L1.
+		float4 lo = __ldg(B.nodeLo + node), hi = __ldg(B.nodeHi + node);
 		bool overlap = !(hi.x < ql.x || lo.x > qh.x || hi.y < ql.y || lo.y > qh.y || hi.z < ql.z || lo.z > qh.z);
 		if (overlap && node < (uint32_t)(n - 1))
 		{
@@ -757,7 +761,7 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 		if (overlap)
 		{
 			uint32_t pb = __float_as_uint(lo.w);
-			if (pair_filter(S, pa, pb))
+			if (pair_filter(infoA, __ldg(B.proxyInfo + pb)))
 			{
 				uint2 p = canon_pair(S, pa, pb);
 				if (count < TRAV_SLOTS)
