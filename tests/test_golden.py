@@ -105,3 +105,60 @@ def test_reference_reproduces_triangle_poses(oracle_mod):
         for f in ("n", "p1", "p2"):
             assert np.array_equal(m["points"][f][:pc].astype(np.float32), d[f][i][:pc]), (i, f)
         assert np.array_equal(m["points"]["key"][:pc], d["key"][i][:pc]), i
+
+
+def test_fp64_error_statement_triangles_and_meshes(oracle_mod):
+    """The reference's FP32 results (which the GPU reproduces bit for bit)
+    against its FP64 rerun on a triangle terrain and a mesh terrain: the same
+    contacts; where both pick the same features, points within 1e-4 m and
+    normals within 1e-3 rad (near-degenerate sphere and capsule contacts turn
+    FP32 rounding into a few 1e-4 rad of normal); feature choices that differ
+    (ties) stay rare."""
+    O = oracle_mod
+    from bounce_b200 import scene as S
+
+    def keys(a, b):
+        return (np.asarray(a, np.uint64) << np.uint64(32)) | np.asarray(b, np.uint64)
+
+    for name, sc in (("mesh", S.mesh_terrain_scene(seed=5, n=400).finalize()),
+                     ("triangles", S.terrain_scene(seed=3, n=400).finalize())):
+        r32 = O.RefWorld(sc, precision=32)
+        sc.set_local_centers(r32.local_centers())
+        r64 = O.RefWorld(sc, precision=64)
+        drv = S.KinematicDriver(sc)
+        for k in range(3):
+            if k:
+                drv.advance()
+                sw = drv.sweeps14()
+                for rw in (r32, r64):
+                    rw.set_sweeps(sw)
+                    rw.step_pass()
+            else:
+                r32.first_pass()
+                r64.first_pass()
+            a, b = r32.contacts(), r64.contacts()
+            ka, kb = keys(a["fixtureA"], a["fixtureB"]), keys(b["fixtureA"], b["fixtureB"])
+            assert np.array_equal(np.sort(ka), np.sort(kb)), (name, k)
+            _, ia, ib = np.intersect1d(ka, kb, return_indices=True)
+            worst_p = worst_n = 0.0
+            ties = points = 0
+            for i, j in zip(ia, ib):
+                for m in range(min(a["manifoldCount"][i], b["manifoldCount"][j])):
+                    ma, mb = a["manifolds"][i, m], b["manifolds"][j, m]
+                    if ma["pointCount"] != mb["pointCount"]:
+                        ties += 1
+                        continue
+                    for q in range(ma["pointCount"]):
+                        pa, pb = ma["points"][q], mb["points"][q]
+                        if not (np.array_equal(pa["key"], pb["key"]) and pa["triangleKey"] == pb["triangleKey"]):
+                            ties += 1
+                            continue
+                        points += 1
+                        worst_p = max(worst_p, float(np.abs(pa["p1"] - pb["p1"]).max()),
+                                      float(np.abs(pa["p2"] - pb["p2"]).max()))
+                        c = np.dot(pa["n"], pb["n"]) / (np.linalg.norm(pa["n"]) * np.linalg.norm(pb["n"]))
+                        worst_n = max(worst_n, float(np.arccos(np.clip(c, -1.0, 1.0))))
+            assert points > 100
+            assert worst_p <= 1e-4, (name, k, worst_p)
+            assert worst_n <= 1e-3, (name, k, worst_n)
+            assert ties <= 0.05 * points, (name, k, ties)
