@@ -10,8 +10,11 @@ fat-AABB update, broadphase, contact begin/end, narrowphase manifolds (the
 
 Metric: manifolds/s = manifolds with at least one point produced per second.
 `value` times passes with the body state already in HBM; `e2e` times the same
-through the C ABI with host buffers (host->device state copy, device->host
-contact list and touching manifolds every step). The reference arm
+through the C ABI with host buffers (host->device copy of the pinned state,
+device->host contact list and packed touching manifolds every step, the
+copies of one step overlapping the next step's pass). Other workloads:
+--workload pile (hull pile over a mesh), batched (1,024 worlds), serving
+(request stream) and queries (ray casts). The reference arm
 (--impl reference) runs the reference's own CPU pipeline (oracle/_ref, the
 unmodified Bounce sources) on the same scene and body motion.
 
