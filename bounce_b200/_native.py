@@ -105,6 +105,7 @@ EXPORTED = [
     "b3g_fetch_manifolds",
     "b3g_fetch_touching",
     "b3g_fetch_ended",
+    "b3g_fetch_fixture_contacts",
     "b3g_fetch_results_async",
     "b3g_fetch_results_packed_async",
     "b3g_wait_results",
@@ -173,6 +174,7 @@ def load():
         "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_ended": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_fetch_fixture_contacts": ([ctx, u32p, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_results_async": ([ctx, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, _p(Counts)], ctypes.c_int),
         "b3g_fetch_results_packed_async": ([ctx, vp, ctypes.c_uint32, vp, vp, ctypes.c_uint32, ctypes.c_uint64,
                                             _p(Counts)], ctypes.c_int),

@@ -211,6 +211,23 @@ __global__ void k_pack_scatter(const DevManifold* man, const DevManifold* extra,
 	}
 }
 
+// Contact edges of the fixtures: record 2c is (fixture A of contact c, c),
+// 2c + 1 is (fixture B, c); counts per fixture.
+__global__ void k_edge_records(const uint32_t* pairA, const uint32_t* pairB, uint32_t n, unsigned long long* keys,
+	uint32_t* vals, uint32_t* counts)
+{
+	uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+	if (c >= n)
+		return;
+	uint32_t a = pairA[c], b = pairB[c];
+	keys[2 * (size_t)c] = a;
+	vals[2 * (size_t)c] = c;
+	keys[2 * (size_t)c + 1] = b;
+	vals[2 * (size_t)c + 1] = c;
+	atomicAdd(&counts[a], 1u);
+	atomicAdd(&counts[b], 1u);
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -625,6 +642,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 		cudaEventDestroy(c->copyReady);
 	if (c->touchBytes)
 		cudaFree(c->touchBytes);
+	if (c->edgeBuf)
+		cudaFree(c->edgeBuf);
 	if (c->sideStream)
 	{
 		cudaStreamSynchronize(c->sideStream);
@@ -1783,6 +1802,64 @@ extern "C" int b3g_wait_results(b3g_ctx* c)
 		CK(cudaEventSynchronize(c->copyDone));
 	}
 	return B3G_OK;
+}
+
+extern "C" int b3g_fetch_fixture_contacts(b3g_ctx* c, uint32_t* offsets, uint32_t* contacts, uint32_t capacity)
+{
+	if (!c || !offsets || (capacity && !contacts))
+		return fail(c, B3G_E_INVALID, "null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	const uint32_t nf = c->nFixtures;
+	const uint32_t m = 2 * n;
+	int bits = 1;
+	while (bits < 32 && (1u << bits) < nf)
+		++bits;
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	const size_t need = 2 * al(8 * (size_t)m) + 2 * al(4 * (size_t)m) + al(4 * ((size_t)nf + 1)) +
+		al(4 * (size_t)radix_sort_scratch_words(std::max(m, 1u), bits));
+	if (c->edgeBytes < need)
+	{
+		if (c->edgeBuf)
+			CK(cudaFree(c->edgeBuf));
+		c->edgeBuf = nullptr;
+		c->edgeBytes = 0;
+		CK(cudaMalloc(&c->edgeBuf, need));
+		c->edgeBytes = need;
+	}
+	char* p = (char*)c->edgeBuf;
+	unsigned long long* keys = (unsigned long long*)p;
+	p += al(8 * (size_t)m);
+	unsigned long long* keysTmp = (unsigned long long*)p;
+	p += al(8 * (size_t)m);
+	uint32_t* vals = (uint32_t*)p;
+	p += al(4 * (size_t)m);
+	uint32_t* valsTmp = (uint32_t*)p;
+	p += al(4 * (size_t)m);
+	uint32_t* counts = (uint32_t*)p;
+	p += al(4 * ((size_t)nf + 1));
+	uint32_t* scratch = (uint32_t*)p;
+	Buffers& B = c->buf;
+	cudaStream_t s = c->stream;
+	CK(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * ((size_t)nf + 1), s));
+	if (n)
+		k_edge_records<<<(n + 255) / 256, 256, 0, s>>>(B.pairA[c->cur], B.pairB[c->cur], n, keys, vals, counts);
+	// Fixture f's edges are the contact list filtered to f, in list order:
+	// AddPair prepends a contact to the list and to both fixtures' edge lists
+	// (contact_manager.cpp:105-137), Destroy unlinks it from all three. A
+	// stable sort by fixture of the records, taken in contact order, gives
+	// every fixture's edges in its own list's order.
+	bool swapped = m ? radix_sort_pairs(keys, vals, keysTmp, valsTmp, m, bits, scratch, B.counters + CTR_STATUS, s)
+					 : false;
+	scan_exclusive(counts, nf, B.scanAux, counts + nf, s);
+	CK(cudaStreamSynchronize(s));
+	CK(cudaMemcpy(offsets, counts, sizeof(uint32_t) * ((size_t)nf + 1), cudaMemcpyDeviceToHost));
+	const uint32_t k = std::min(m, capacity);
+	if (k)
+		CK(cudaMemcpy(contacts, swapped ? valsTmp : vals, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost));
+	return (int)m;
 }
 
 extern "C" int b3g_fetch_ended(b3g_ctx* c, uint32_t* out, uint32_t capacity)

@@ -302,6 +302,8 @@ struct b3g_ctx
 	cudaEvent_t copyDone;     // those copies finished
 	bool copyPending;
 	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds (allocated on first use)
+	void* edgeBuf;            // b3g_fetch_fixture_contacts scratch (allocated on first use)
+	size_t edgeBytes;
 	cudaStream_t sideStream;  // hull-hull / hull-triangle narrowphase, beside the convex buckets
 	cudaStream_t meshStream;  // mesh midphase (tree queries, work items), beside both
 	cudaEvent_t forkEvent, joinEvent, meshFork, meshJoin;

@@ -885,6 +885,41 @@ void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, 
 	k_scan_add<<<blocks, SCAN_BLOCK, 0, s>>>(data, n, aux);
 }
 
+// Stable sort of n (key, value) records by the low `bits` bits of the keys
+// (the one-sweep passes of the broadphase sort). scratch holds
+// radix_sort_scratch_words(n, bits) words. Returns the buffer pair holding
+// the result: (keys, vals) or (keysTmp, valsTmp).
+uint32_t radix_sort_scratch_words(uint32_t n, int bits)
+{
+	uint32_t passes = (uint32_t)(bits + 7) / 8;
+	return 256u * (9u + passes * ((n + OS_TILE - 1) / OS_TILE));
+}
+
+bool radix_sort_pairs(unsigned long long* keys, uint32_t* vals, unsigned long long* keysTmp, uint32_t* valsTmp,
+	uint32_t n, int bits, uint32_t* scratch, uint32_t* err, cudaStream_t s)
+{
+	SortShifts sh;
+	sh.n = 0;
+	for (int sft = 0; sft < bits && sh.n < 8; sft += 8)
+		sh.s[sh.n++] = sft;
+	if (n == 0 || sh.n == 0)
+		return false;
+	const uint32_t numTiles = (n + OS_TILE - 1) / OS_TILE;
+	cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * (9 * 256 + (size_t)sh.n * numTiles * 256), s);
+	k_os_hist<<<min((n + 255) / 256, 148u * 4u), 256, 0, s>>>(keys, n, sh, scratch);
+	k_os_scan<<<sh.n, 256, 0, s>>>(scratch);
+	unsigned long long *kin = keys, *kout = keysTmp;
+	uint32_t *vin = vals, *vout = valsTmp;
+	for (int p = 0; p < sh.n; ++p)
+	{
+		k_onesweep<<<numTiles, OS_THREADS, 0, s>>>(kin, vin, kout, vout, n, sh.s[p], scratch + 256 * p,
+			scratch + 9 * 256 + (size_t)p * numTiles * 256, scratch + 8 * 256 + p, err);
+		std::swap(kin, kout);
+		std::swap(vin, vout);
+	}
+	return kin != keys;
+}
+
 void launch_sync(b3g_ctx* c, cudaStream_t s)
 {
 	uint32_t n = c->nFixtures;

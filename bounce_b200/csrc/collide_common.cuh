@@ -923,6 +923,9 @@ void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStr
 void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE,
 	const Tune& tune, cudaStream_t s);
 void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
+uint32_t radix_sort_scratch_words(uint32_t n, int bits);
+bool radix_sort_pairs(unsigned long long* keys, uint32_t* vals, unsigned long long* keysTmp, uint32_t* valsTmp,
+	uint32_t n, int bits, uint32_t* scratch, uint32_t* err, cudaStream_t s);
 
 __device__ __forceinline__ XF load_xf7(const float* s)
 {

@@ -167,6 +167,15 @@ class CollisionPipeline:
     def wait_results(self):
         self._check(self.lib.b3g_wait_results(self.ctx))
 
+    def fixture_contacts(self):
+        """Island-graph edges: (offsets (nFixtures + 1,), contact indices) with
+        fixture f's contacts in its edge-list order at offsets[f]:offsets[f + 1]."""
+        n = self.counts()["contacts"]
+        offsets = np.zeros(self.scene.n_fixtures + 1, np.uint32)
+        out = np.zeros(max(2 * n, 1), np.uint32)
+        m = self._check(self.lib.b3g_fetch_fixture_contacts(self.ctx, N.ptr(offsets, u32), N.ptr(out, u32), len(out)))
+        return offsets, out[:m]
+
     def ended(self):
         c = self.counts()
         out = np.zeros((max(c["ended"], 1), 3), np.uint32)

@@ -298,6 +298,15 @@ int b3g_fetch_results_packed_async(b3g_ctx* ctx, uint32_t* contacts, uint32_t co
  * b3g_fetch_results_packed_async. */
 int b3g_wait_results(b3g_ctx* ctx);
 
+/* The island graph's edges: for every fixture, its contacts in the order of
+ * its edge list b3Fixture::m_contactList (which b3World::Solve walks to build
+ * islands, world.cpp:324-370; AddPair prepends an edge, Destroy unlinks it,
+ * contact_manager.cpp:115-137). offsets receives nFixtures + 1 entries
+ * (fixture f's edges are contacts[offsets[f] .. offsets[f + 1])), contacts
+ * the contact indices (positions in the contact list of the last pass), up
+ * to capacity. Returns the number of edges, 2 per contact. */
+int b3g_fetch_fixture_contacts(b3g_ctx* ctx, uint32_t* offsets, uint32_t* contacts, uint32_t capacity);
+
 /* Contacts destroyed by the last pass: fixtureA, fixtureB, flags as above
  * (flags of the destroyed contact), in the order UpdateContacts destroys them.
  * Replaces the Destroy calls of UpdateContacts (contact_manager.cpp:270-281). */

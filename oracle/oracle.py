@@ -94,6 +94,7 @@ def lib(precision=32):
         "refw_dump_contacts": ([vp, ctypes.c_uint32, ctypes.c_uint32, vp], ctypes.c_uint32),
         "refw_load_impulses": ([vp, vp], None),
         "refw_query_aabb": ([vp, f32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
+        "refw_fixture_edges": ([vp, u32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
         "refw_ray_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
@@ -237,6 +238,16 @@ class RefWorld:
 
     def contact_count(self):
         return self.L.refw_contact_count(self.w)
+
+    def fixture_edges(self):
+        """Each fixture's contact edge list: (offsets (fixtures + 1,), (edges, 2)
+        fixtureA, fixtureB of the edge's contact)."""
+        nf = self.scene.n_fixtures
+        offsets = np.zeros(nf + 1, np.uint32)
+        cap = 2 * self.contact_count()
+        pairs = np.zeros((max(cap, 1), 2), np.uint32)
+        k = self.L.refw_fixture_edges(self.w, _p(offsets, ctypes.c_uint32), _p(pairs, ctypes.c_uint32), cap)
+        return offsets, pairs[:k]
 
     def query_aabb(self, box):
         """b3World::QueryAABB: indices of the fixtures reported (report order)."""

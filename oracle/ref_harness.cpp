@@ -632,6 +632,29 @@ REF_API void refw_convex_stats(uint32_t* out)
 	b3_convexCacheHits = 0;
 }
 
+// Each fixture's contact edges (b3Fixture::m_contactList) in list order:
+// offsets (fixture count + 1) and the (fixtureA, fixtureB) of every edge's
+// contact; returns the number of edges.
+REF_API uint32_t refw_fixture_edges(void* p, uint32_t* offsets, uint32_t* pairs, uint32_t cap)
+{
+	RefWorld* w = (RefWorld*)p;
+	uint32_t k = 0;
+	for (size_t i = 0; i < w->fixtures.size(); ++i)
+	{
+		offsets[i] = k;
+		for (b3ContactEdge* ce = w->fixtures[i]->m_contactList; ce; ce = ce->next, ++k)
+		{
+			if (k < cap)
+			{
+				pairs[2 * k] = (uint32_t)(uintptr_t)ce->contact->m_fixtureA->m_userData;
+				pairs[2 * k + 1] = (uint32_t)(uintptr_t)ce->contact->m_fixtureB->m_userData;
+			}
+		}
+	}
+	offsets[w->fixtures.size()] = k;
+	return k;
+}
+
 // World queries through the reference's own b3World entry points.
 struct QueryAll : b3QueryListener, b3QueryFilter
 {

@@ -236,3 +236,29 @@ def test_async_results_match_sync():
     assert async_pipe.totals()["graph_passes"] >= 3
     sync_pipe.close()
     async_pipe.close()
+
+
+def test_fixture_edge_lists(oracle_mod):
+    """The island graph's edges: every fixture's contacts in the order of its
+    b3Fixture::m_contactList, pass after pass (contacts created, kept and
+    destroyed), against the reference's own edge lists."""
+    sc = S.mixed_scene(seed=23, n=2000, side=15.0, static_frac=0.05).finalize()
+    rw = oracle_mod.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    for k in range(6):
+        if k:
+            drv.advance()
+            rw.set_sweeps(drv.sweeps14())
+            rw.step_pass()
+        else:
+            rw.first_pass()
+        pipe.collide(drv.state17())
+        assert pipe.counts()["status"] == 0
+        offsets, edges = pipe.fixture_contacts()
+        want_off, want_pairs = rw.fixture_edges()
+        assert np.array_equal(offsets, want_off), f"pass {k}: edge counts differ"
+        got_pairs = pipe.contacts()[edges, :2]
+        assert np.array_equal(got_pairs, want_pairs), f"pass {k}: edge order differs"
+    pipe.close()
