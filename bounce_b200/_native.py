@@ -88,6 +88,76 @@ MANIFOLD_DTYPE = np.dtype(
 )
 assert POINT_DTYPE.itemsize == 72 and MANIFOLD_DTYPE.itemsize == 320
 
+# Solver input records (include/b3g.h): b3g_solver_body (b3Position /
+# b3Velocity entries and body fields, island.cpp:130-134), b3g_contact_constraint
+# (b3ContactVelocityConstraint, contact_solver.h:93-105) and
+# b3g_manifold_constraint (b3VelocityConstraintManifold with its points and the
+# b3PositionConstraintPoints, contact_solver.h:31-91).
+SOLVER_BODY_DTYPE = np.dtype(
+    [
+        ("x", "<f4", 3),
+        ("q", "<f4", 4),
+        ("v", "<f4", 3),
+        ("w", "<f4", 3),
+        ("invMass", "<f4"),
+        ("localCenter", "<f4", 3),
+        ("invI", "<f4", 9),
+        ("pad", "<f4", 2),
+    ]
+)
+CONTACT_CONSTRAINT_DTYPE = np.dtype(
+    [
+        ("indexA", "<u4"),
+        ("indexB", "<u4"),
+        ("manifoldStart", "<u4"),
+        ("manifoldCount", "<u4"),
+        ("invMassA", "<f4"),
+        ("invMassB", "<f4"),
+        ("friction", "<f4"),
+        ("restitution", "<f4"),
+        ("invIA", "<f4", 9),
+        ("invIB", "<f4", 9),
+        ("radiusA", "<f4"),
+        ("radiusB", "<f4"),
+        ("contact", "<u4"),
+        ("pad", "<u4", 3),
+    ]
+)
+VELOCITY_POINT_DTYPE = np.dtype(
+    [
+        ("rA", "<f4", 3),
+        ("rB", "<f4", 3),
+        ("normal", "<f4", 3),
+        ("normalMass", "<f4"),
+        ("normalImpulse", "<f4"),
+        ("velocityBias", "<f4"),
+    ]
+)
+POSITION_POINT_DTYPE = np.dtype([("localNormalA", "<f4", 3), ("localPointA", "<f4", 3), ("localPointB", "<f4", 3)])
+MANIFOLD_CONSTRAINT_DTYPE = np.dtype(
+    [
+        ("rA", "<f4", 3),
+        ("rB", "<f4", 3),
+        ("normal", "<f4", 3),
+        ("tangent1", "<f4", 3),
+        ("tangent2", "<f4", 3),
+        ("tangentSpeed1", "<f4"),
+        ("tangentSpeed2", "<f4"),
+        ("tangentMass", "<f4", 4),
+        ("tangentImpulse", "<f4", 2),
+        ("motorImpulse", "<f4"),
+        ("motorMass", "<f4"),
+        ("motorSpeed", "<f4"),
+        ("pointCount", "<u4"),
+        ("constraint", "<u4"),
+        ("pad", "<u4", 4),
+        ("points", VELOCITY_POINT_DTYPE, 4),
+        ("positionPoints", POSITION_POINT_DTYPE, 4),
+    ]
+)
+assert SOLVER_BODY_DTYPE.itemsize == 112 and CONTACT_CONSTRAINT_DTYPE.itemsize == 128
+assert MANIFOLD_CONSTRAINT_DTYPE.itemsize == 464
+
 EXPORTED = [
     "b3g_create",
     "b3g_destroy",
@@ -125,6 +195,9 @@ EXPORTED = [
     "b3g_ray_cast",
     "b3g_ray_cast_single",
     "b3g_ray_cast_single_device",
+    "b3g_set_materials",
+    "b3g_contact_constraints",
+    "b3g_contact_constraints_device",
     "b3g_autotune",
     "b3g_update_scene",
     "b3g_update_scene_device",
@@ -199,6 +272,11 @@ def load():
         "b3g_ray_cast": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_ray_cast_single": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p], ctypes.c_int),
         "b3g_ray_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp, vp], ctypes.c_int),
+        "b3g_set_materials": ([ctx, f32p, f32p], ctypes.c_int),
+        "b3g_contact_constraints": ([ctx, ctypes.c_uint32, u32p, vp, ctypes.c_float, ctypes.c_int, vp,
+                                     ctypes.c_uint32, vp, ctypes.c_uint32, u32p], ctypes.c_int),
+        "b3g_contact_constraints_device": ([ctx, ctypes.c_uint32, vp, vp, ctypes.c_float, ctypes.c_int, vp,
+                                            ctypes.c_uint32, vp, ctypes.c_uint32, vp, vp], ctypes.c_int),
         "b3g_update_scene": ([ctx, ctypes.c_uint32, u32p, u32p, u32p, u8p, ctypes.c_uint32, u32p, u32p, u32p, u32p,
                               f32p, u32p, ctypes.c_uint32, u32p, vp], ctypes.c_int),
         "b3g_update_scene_device": ([ctx, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp,

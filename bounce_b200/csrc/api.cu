@@ -644,6 +644,10 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 		cudaFree(c->touchBytes);
 	if (c->edgeBuf)
 		cudaFree(c->edgeBuf);
+	dfree(c->dFixMaterial);
+	dfree(c->ciTiles);
+	if (c->ciHost)
+		cudaFree(c->ciHost);
 	if (c->sideStream)
 	{
 		cudaStreamSynchronize(c->sideStream);
@@ -950,6 +954,13 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 	CK(dalloc(&c->dFixLife, nf));
 	CK(cudaMemset(c->dFixLife, FIX_LIVE, nf ? nf : 1));
 	CK(dalloc(&c->dFixParams, 3 * (size_t)nf));
+	{
+		// b3FixtureDef's friction and restitution (fixture.h:46-47) until b3g_set_materials.
+		dfree(c->dFixMaterial);
+		CK(dalloc(&c->dFixMaterial, nf));
+		std::vector<float2> mat(std::max(nf, 1u), make_float2(0.3f, 0.0f));
+		CK(cudaMemcpy(c->dFixMaterial, mat.data(), sizeof(float2) * mat.size(), cudaMemcpyHostToDevice));
+	}
 	if (nf)
 	{
 		CK(cudaMemcpy(c->dFixBody, body, sizeof(uint32_t) * nf, cudaMemcpyHostToDevice));
@@ -1860,6 +1871,132 @@ extern "C" int b3g_fetch_fixture_contacts(b3g_ctx* c, uint32_t* offsets, uint32_
 	if (k)
 		CK(cudaMemcpy(contacts, swapped ? valsTmp : vals, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost));
 	return (int)m;
+}
+
+extern "C" int b3g_set_materials(b3g_ctx* c, const float* friction, const float* restitution)
+{
+	if (!c || !friction || !restitution)
+		return fail(c, B3G_E_INVALID, "b3g_set_materials: null argument");
+	if (!c->dFixMaterial)
+		return fail(c, B3G_E_STATE, "b3g_set_materials: no fixtures yet");
+	const uint32_t nf = c->nFixtures;
+	std::vector<float2> mat(std::max(nf, 1u), make_float2(0.3f, 0.0f));
+	for (uint32_t i = 0; i < nf; ++i)
+		mat[i] = make_float2(friction[i], restitution[i]);
+	CK(cudaSetDevice(c->device));
+	CK(cudaStreamSynchronize(c->stream));
+	CK(cudaMemcpy(c->dFixMaterial, mat.data(), sizeof(float2) * nf, cudaMemcpyHostToDevice));
+	return B3G_OK;
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+extern "C" int b3g_contact_constraints_device(b3g_ctx* c, uint32_t count, const uint32_t* contacts,
+	const b3g_solver_body* bodies, float dtRatio, int warm, b3g_contact_constraint* constraints, uint32_t cCap,
+	b3g_manifold_constraint* manifolds, uint32_t mCap, uint32_t* counts, void* stream)
+{
+	if (!c || !bodies || !counts)
+		return fail(c, B3G_E_INVALID, "b3g_contact_constraints_device: null argument");
+	if (!aligned16(bodies) || !aligned16(constraints) || !aligned16(manifolds))
+		return fail(c, B3G_E_INVALID, "b3g_contact_constraints_device: buffers must be 16-byte aligned");
+	if (!c->havePass)
+		return fail(c, B3G_E_STATE, "b3g_contact_constraints_device: no pass yet");
+	if (contacts && count > c->cfg.max_contacts)
+		return fail(c, B3G_E_CAPACITY, "b3g_contact_constraints_device: %u contacts exceed max_contacts %u", count,
+			c->cfg.max_contacts);
+	CK(cudaSetDevice(c->device));
+	const uint32_t tiles = std::max(contact_constraint_tiles(c->cfg.max_contacts), 1u);
+	if (c->ciTileCap < tiles)
+	{
+		dfree(c->ciTiles);
+		c->ciTileCap = 0;
+		CK(dalloc(&c->ciTiles, tiles));
+		c->ciTileCap = tiles;
+	}
+	ConstraintCall q;
+	q.list = contacts;
+	q.listCount = contacts ? count : 0;
+	q.material = c->dFixMaterial;
+	q.bodies = bodies;
+	q.dtRatio = dtRatio;
+	q.warm = warm ? 1 : 0;
+	q.tiles = c->ciTiles;
+	q.counts = counts;
+	q.constraints = constraints;
+	q.constraintCap = constraints ? cCap : 0;
+	q.manifolds = manifolds;
+	q.manifoldCap = manifolds ? mCap : 0;
+	launch_contact_constraints(c, q, stream ? (cudaStream_t)stream : c->stream);
+	CK(cudaGetLastError());
+	return B3G_OK;
+}
+
+extern "C" int b3g_contact_constraints(b3g_ctx* c, uint32_t count, const uint32_t* contacts,
+	const b3g_solver_body* bodies, float dtRatio, int warm, b3g_contact_constraint* constraints, uint32_t cCap,
+	b3g_manifold_constraint* manifolds, uint32_t mCap, uint32_t* counts)
+{
+	if (!c || !bodies || !counts || (cCap && !constraints) || (mCap && !manifolds))
+		return fail(c, B3G_E_INVALID, "b3g_contact_constraints: null argument");
+	uint32_t n;
+	int rc = contacts_now(c, n);
+	if (rc)
+		return rc;
+	if (contacts)
+	{
+		if (count > c->cfg.max_contacts)
+			return fail(c, B3G_E_CAPACITY, "b3g_contact_constraints: %u contacts exceed max_contacts %u", count,
+				c->cfg.max_contacts);
+		for (uint32_t i = 0; i < count; ++i)
+			if (contacts[i] >= n)
+				return fail(c, B3G_E_INVALID, "b3g_contact_constraints: contact %u of %u past the list", contacts[i],
+					n);
+	}
+	// Device copies: bodies, the list, counts, then the records (sized for
+	// every selected contact: at most max_contacts constraints, 3 manifolds
+	// each, bounded by the capacities asked for).
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	const uint32_t nb = c->nBodies;
+	const uint32_t cMax = std::min(cCap, contacts ? count : n);
+	const uint32_t mMax = std::min<uint64_t>(mCap, 3ull * (contacts ? count : n));
+	const size_t need = al(sizeof(b3g_solver_body) * std::max(nb, 1u)) + al(4 * (size_t)std::max(count, 1u)) +
+		al(8) + al(sizeof(b3g_contact_constraint) * std::max(cMax, 1u)) +
+		al(sizeof(b3g_manifold_constraint) * std::max(mMax, 1u));
+	if (c->ciHostBytes < need)
+	{
+		if (c->ciHost)
+			CK(cudaFree(c->ciHost));
+		c->ciHost = nullptr;
+		c->ciHostBytes = 0;
+		CK(cudaMalloc(&c->ciHost, need));
+		c->ciHostBytes = need;
+	}
+	char* p = (char*)c->ciHost;
+	b3g_solver_body* dBodies = (b3g_solver_body*)p;
+	p += al(sizeof(b3g_solver_body) * std::max(nb, 1u));
+	uint32_t* dList = (uint32_t*)p;
+	p += al(4 * (size_t)std::max(count, 1u));
+	uint32_t* dCounts = (uint32_t*)p;
+	p += al(8);
+	b3g_contact_constraint* dCon = (b3g_contact_constraint*)p;
+	p += al(sizeof(b3g_contact_constraint) * std::max(cMax, 1u));
+	b3g_manifold_constraint* dMan = (b3g_manifold_constraint*)p;
+	cudaStream_t s = c->stream;
+	if (nb)
+		CK(cudaMemcpyAsync(dBodies, bodies, sizeof(b3g_solver_body) * nb, cudaMemcpyHostToDevice, s));
+	if (contacts && count)
+		CK(cudaMemcpyAsync(dList, contacts, 4 * (size_t)count, cudaMemcpyHostToDevice, s));
+	rc = b3g_contact_constraints_device(c, count, contacts ? dList : nullptr, dBodies, dtRatio, warm, dCon, cMax,
+		dMan, mMax, dCounts, s);
+	if (rc)
+		return rc;
+	CK(cudaMemcpyAsync(counts, dCounts, 8, cudaMemcpyDeviceToHost, s));
+	CK(cudaStreamSynchronize(s));
+	const uint32_t kc = std::min(counts[0], cMax), km = std::min(counts[1], mMax);
+	if (kc)
+		CK(cudaMemcpy(constraints, dCon, sizeof(b3g_contact_constraint) * kc, cudaMemcpyDeviceToHost));
+	if (km)
+		CK(cudaMemcpy(manifolds, dMan, sizeof(b3g_manifold_constraint) * km, cudaMemcpyDeviceToHost));
+	return (int)counts[0];
 }
 
 extern "C" int b3g_fetch_ended(b3g_ctx* c, uint32_t* out, uint32_t capacity)

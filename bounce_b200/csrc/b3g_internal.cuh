@@ -309,6 +309,11 @@ struct b3g_ctx
 	cudaEvent_t forkEvent, joinEvent, meshFork, meshJoin;
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
+	float2* dFixMaterial;         // per fixture: friction, restitution (b3g_set_materials)
+	unsigned long long* ciTiles;  // b3g_contact_constraints_device: tile sums (allocated on first use)
+	uint32_t ciTileCap;
+	void* ciHost;                 // b3g_contact_constraints: device copies of its host buffers
+	size_t ciHostBytes;
 
 	uint32_t nHulls, nBodies, nFixtures, nWorlds;
 	uint32_t hullVerts, hullEdges, hullFaces;
@@ -431,6 +436,25 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s);
 void launch_collide_pairs(b3g_ctx* c, cudaStream_t s, uint32_t n, const uint32_t* fixA,
 	const uint32_t* fixB, const float* xfA, const float* xfB, const float* xf0A,
 	const float* xf0B, uint4* cache, DevManifold* out);
+
+// One b3g_contact_constraints_device call (solver_input.cu).
+struct ConstraintCall
+{
+	const uint32_t* list; // contacts to solve, or null for every touching non-sensor contact
+	uint32_t listCount;
+	const float2* material;
+	const b3g_solver_body* bodies;
+	float dtRatio;
+	int warm;
+	unsigned long long* tiles;
+	uint32_t* counts;
+	b3g_contact_constraint* constraints;
+	uint32_t constraintCap;
+	b3g_manifold_constraint* manifolds;
+	uint32_t manifoldCap;
+};
+uint32_t contact_constraint_tiles(uint32_t items);
+void launch_contact_constraints(b3g_ctx* c, const ConstraintCall& q, cudaStream_t s);
 
 // Grid size for grid-stride loops over device-side counts.
 inline int persistent_blocks(int perSM = 8) { return 148 * perSM; }

@@ -176,6 +176,32 @@ class CollisionPipeline:
         m = self._check(self.lib.b3g_fetch_fixture_contacts(self.ctx, N.ptr(offsets, u32), N.ptr(out, u32), len(out)))
         return offsets, out[:m]
 
+    def set_materials(self, friction, restitution):
+        """Friction and restitution per fixture (b3Fixture::m_friction, m_restitution)."""
+        fr = np.ascontiguousarray(friction, np.float32)
+        re = np.ascontiguousarray(restitution, np.float32)
+        assert len(fr) == len(re) == self.scene.n_fixtures
+        self._check(self.lib.b3g_set_materials(self.ctx, N.ptr(fr, ctypes.c_float), N.ptr(re, ctypes.c_float)))
+
+    def contact_constraints(self, bodies, dt_ratio=1.0, warm=True, contacts=None):
+        """b3ContactSolver's constructor + InitializeVelocityConstraints on the
+        last pass: bodies is a SOLVER_BODY_DTYPE array (one per body);
+        contacts the contact-list positions to solve, in order (None: every
+        touching non-sensor contact in list order). Returns (constraints,
+        manifolds) as CONTACT_CONSTRAINT_DTYPE / MANIFOLD_CONSTRAINT_DTYPE arrays."""
+        b = np.ascontiguousarray(bodies, N.SOLVER_BODY_DTYPE)
+        assert len(b) == self.n_bodies
+        lst = None if contacts is None else np.ascontiguousarray(contacts, np.uint32)
+        k = self.counts()["contacts"] if lst is None else len(lst)
+        con = np.zeros(max(k, 1), N.CONTACT_CONSTRAINT_DTYPE)
+        man = np.zeros(max(3 * k, 1), N.MANIFOLD_CONSTRAINT_DTYPE)
+        counts = np.zeros(2, np.uint32)
+        m = self._check(self.lib.b3g_contact_constraints(
+            self.ctx, 0 if lst is None else len(lst), None if lst is None else N.ptr(lst, u32),
+            ctypes.c_void_p(b.ctypes.data), float(dt_ratio), 1 if warm else 0, ctypes.c_void_p(con.ctypes.data),
+            len(con), ctypes.c_void_p(man.ctypes.data), len(man), N.ptr(counts, u32)))
+        return con[:m], man[:counts[1]]
+
     def ended(self):
         c = self.counts()
         out = np.zeros((max(c["ended"], 1), 3), np.uint32)

@@ -446,6 +446,111 @@ int b3g_ray_cast_single(b3g_ctx* ctx, uint32_t n, const float* rays, const uint3
 int b3g_ray_cast_single_device(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds,
 	uint32_t* fixture, float* hit, void* stream);
 
+/* Solver input -------------------------------------------------------------
+ *
+ * b3ContactSolver's constructor and InitializeVelocityConstraints
+ * (src/bounce/dynamics/contacts/contact_solver.cpp:28-149, :177-305) on the
+ * manifolds of the last pass, bit for bit. The reference fills them island
+ * by island from b3Position / b3Velocity arrays indexed by the bodies'
+ * island indices (island.cpp:130-152); here the caller gives one
+ * b3g_solver_body per body (body index of b3g_set_bodies) and, optionally,
+ * the contacts to solve in its own order (an island's m_contacts). Body-level
+ * fields of b3ContactPositionConstraint (invMass, localInvI, localCenter) stay
+ * in the caller's body arrays; the records name the bodies by index. */
+
+/* Friction and restitution per fixture (b3Fixture::m_friction, m_restitution;
+ * b3FixtureDef's defaults 0.3 and 0 until this call, fixture.h:46-47). Host
+ * arrays of the fixture count. */
+int b3g_set_materials(b3g_ctx* ctx, const float* friction, const float* restitution);
+
+/* One body: its b3Position and b3Velocity entries (island.cpp:130-134) and
+ * the fields the constraints read from b3Body. 112 bytes, 16-byte aligned. */
+typedef struct b3g_solver_body
+{
+	float x[3];           /* b3Position::x, centre of mass (b3Sweep::worldCenter) */
+	float q[4];           /* b3Position::q, xyzw */
+	float v[3];           /* b3Velocity::v */
+	float w[3];           /* b3Velocity::w */
+	float inv_mass;       /* b3Body::m_invMass */
+	float local_center[3]; /* b3Body::m_sweep.localCenter */
+	float inv_i[9];       /* b3Position::I, world inverse inertia, columns x, y, z */
+	float pad[2];
+} b3g_solver_body;
+
+/* b3ContactVelocityConstraint (contact_solver.h:93-105) with the radii of
+ * b3ContactPositionConstraint; its manifolds are records manifold_start ..
+ * manifold_start + manifold_count - 1. 128 bytes. */
+typedef struct b3g_contact_constraint
+{
+	uint32_t index_a, index_b;    /* bodies (0xFFFFFFFF: listed index past the contact list) */
+	uint32_t manifold_start, manifold_count;
+	float inv_mass_a, inv_mass_b;
+	float friction;               /* b3MixFriction: sqrt(fA * fB) */
+	float restitution;            /* b3MixRestitution: max(eA, eB) */
+	float inv_i_a[9], inv_i_b[9]; /* b3Position::I of the bodies */
+	float radius_a, radius_b;     /* b3Shape::m_radius */
+	uint32_t contact;             /* position in the contact list */
+	uint32_t pad[3];
+} b3g_contact_constraint;
+
+/* b3VelocityConstraintPoint (contact_solver.h:60-69). */
+typedef struct b3g_velocity_point
+{
+	float r_a[3], r_b[3], normal[3];
+	float normal_mass, normal_impulse, velocity_bias;
+} b3g_velocity_point;
+
+/* b3PositionConstraintPoint (contact_solver.h:31-36). */
+typedef struct b3g_position_point
+{
+	float local_normal_a[3], local_point_a[3], local_point_b[3];
+} b3g_position_point;
+
+/* b3VelocityConstraintManifold (contact_solver.h:71-91) and the points of
+ * the matching b3PositionConstraintManifold; points past point_count are
+ * zero. Fields the reference leaves unset when a manifold has no points
+ * (tangents) are zero. 464 bytes. */
+typedef struct b3g_manifold_constraint
+{
+	float r_a[3], r_b[3];
+	float normal[3], tangent1[3], tangent2[3];
+	float tangent_speed1, tangent_speed2;
+	float tangent_mass[4];        /* b3Mat22 columns x, y */
+	float tangent_impulse[2];
+	float motor_impulse, motor_mass, motor_speed;
+	uint32_t point_count;
+	uint32_t constraint;          /* its b3g_contact_constraint */
+	uint32_t pad[4];
+	b3g_velocity_point points[4];
+	b3g_position_point position_points[4];
+} b3g_manifold_constraint;
+
+/* Builds the constraints on device buffers, asynchronously on stream (NULL:
+ * the context's stream), without host synchronisation; the first call
+ * allocates a small scratch array (tile sums), later calls allocate nothing.
+ * contacts: count contact indices (device memory) in the order to solve
+ * them; NULL selects every touching contact whose fixtures are not sensors,
+ * in contact-list order (the contacts b3World::Solve puts on islands,
+ * world.cpp:336-348), and count is ignored (count <= max_contacts).
+ * bodies: one b3g_solver_body per body. dt_ratio, warm_starting: the
+ * b3TimeStep fields (impulses are dt_ratio times the manifolds' warm-start
+ * impulses, or zero). Writes up to constraint_capacity and
+ * manifold_capacity records and, into counts (device memory, 2 u32), the
+ * numbers of constraints and manifolds (which may exceed the capacities).
+ * All device pointers 16-byte aligned. */
+int b3g_contact_constraints_device(b3g_ctx* ctx, uint32_t count, const uint32_t* contacts,
+	const b3g_solver_body* bodies, float dt_ratio, int warm_starting, b3g_contact_constraint* constraints,
+	uint32_t constraint_capacity, b3g_manifold_constraint* manifolds, uint32_t manifold_capacity,
+	uint32_t* counts, void* stream);
+
+/* The same on host buffers (copied in and out on the context's stream;
+ * synchronous). counts (host, 2 u32) receives the totals; returns the number
+ * of constraints, or B3G_E_INVALID for a listed index past the contact list. */
+int b3g_contact_constraints(b3g_ctx* ctx, uint32_t count, const uint32_t* contacts,
+	const b3g_solver_body* bodies, float dt_ratio, int warm_starting, b3g_contact_constraint* constraints,
+	uint32_t constraint_capacity, b3g_manifold_constraint* manifolds, uint32_t manifold_capacity,
+	uint32_t* counts);
+
 /* Pair search without device allocation ------------------------------------
  *
  * No counterpart in the reference. For callers that cannot allocate device

@@ -95,6 +95,11 @@ def lib(precision=32):
         "refw_load_impulses": ([vp, vp], None),
         "refw_query_aabb": ([vp, f32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_fixture_edges": ([vp, u32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
+        "refw_contact_solver": (
+            [vp, ctypes.c_uint32, u32p, f32p, f32p, f32p, ctypes.c_float, ctypes.c_uint32, u32p, u32p, u32p],
+            ctypes.c_uint32,
+        ),
+        "refw_mass_data": ([vp, f32p], None),
         "refw_ray_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
         "refw_ray_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
@@ -248,6 +253,35 @@ class RefWorld:
         pairs = np.zeros((max(cap, 1), 2), np.uint32)
         k = self.L.refw_fixture_edges(self.w, _p(offsets, ctypes.c_uint32), _p(pairs, ctypes.c_uint32), cap)
         return offsets, pairs[:k]
+
+    def mass_data(self):
+        """Per body as the reference computed it from the fixtures: m_invMass
+        (n,), m_invI (n, 9) and m_worldInvI (n, 9), matrices by columns."""
+        nb = self.scene.n_bodies
+        out = np.zeros((max(nb, 1), 19), np.float32)
+        self.L.refw_mass_data(self.w, _p(out, ctypes.c_float))
+        return out[:nb, 0].copy(), out[:nb, 1:10].copy(), out[:nb, 10:19].copy()
+
+    def contact_solver(self, bodies, friction, restitution, dt_ratio=1.0, warm=True, contacts=None):
+        """The reference's b3ContactSolver constructor and
+        InitializeVelocityConstraints on this world's contacts (the listed
+        contact-list positions, or every touching non-sensor contact in list
+        order). bodies: (n, 28) float32 in the b3g_solver_body layout;
+        friction, restitution per fixture. Returns the raw records:
+        constraints (k, 32) and manifolds (m, 116) as uint32 words."""
+        b = np.ascontiguousarray(bodies, np.float32).reshape(-1, 28)
+        fr = np.ascontiguousarray(friction, np.float32)
+        re = np.ascontiguousarray(restitution, np.float32)
+        lst = None if contacts is None else np.ascontiguousarray(contacts, np.uint32)
+        count = self.contact_count() if lst is None else len(lst)
+        con = np.zeros((max(count, 1), 32), np.uint32)
+        man = np.zeros((max(3 * count, 1), 116), np.uint32)
+        mc = ctypes.c_uint32()
+        k = self.L.refw_contact_solver(self.w, 0 if lst is None else len(lst), _p(lst, ctypes.c_uint32),
+                                       _p(b, ctypes.c_float), _p(fr, ctypes.c_float), _p(re, ctypes.c_float),
+                                       float(dt_ratio), 1 if warm else 0, _p(con, ctypes.c_uint32),
+                                       _p(man, ctypes.c_uint32), ctypes.byref(mc))
+        return con[:k], man[:mc.value]
 
     def query_aabb(self, box):
         """b3World::QueryAABB: indices of the fixtures reported (report order)."""

@@ -43,6 +43,8 @@
 #include <bounce/dynamics/contacts/hull_contact.h>
 #include <bounce/dynamics/contacts/mesh_contact.h>
 #include <bounce/collision/sat/sat.h>
+#include <bounce/dynamics/contacts/contact_solver.h>
+#include <bounce/dynamics/time_step.h>
 #undef private
 #undef protected
 
@@ -653,6 +655,210 @@ REF_API uint32_t refw_fixture_edges(void* p, uint32_t* offsets, uint32_t* pairs,
 	}
 	offsets[w->fixtures.size()] = k;
 	return k;
+}
+
+static inline void PutF(uint32_t* o, scalar x)
+{
+	float f = (float)x;
+	memcpy(o, &f, 4);
+}
+
+static inline void PutV(uint32_t* o, const b3Vec3& v)
+{
+	PutF(o, v.x);
+	PutF(o + 1, v.y);
+	PutF(o + 2, v.z);
+}
+
+static inline void PutM(uint32_t* o, const b3Mat33& m)
+{
+	PutV(o, m.x);
+	PutV(o + 3, m.y);
+	PutV(o + 6, m.z);
+}
+
+// The reference's b3ContactSolver constructor and InitializeVelocityConstraints
+// (contact_solver.cpp:28-149, :177-305) on this world's contacts: the listed
+// contact-list positions (count of them) or, with list null, every touching
+// contact without a sensor fixture, in list order (the filter of
+// b3World::Solve, world.cpp:336-348). bodies: 28 floats per body (x, q, v, w,
+// invMass, localCenter, I columns, pad) becoming b3Position / b3Velocity
+// entries at island index = body index and the body's m_invMass and
+// m_sweep.localCenter (restored afterwards); friction and restitution per
+// fixture are set on the fixtures. Writes 32 words per constraint and 116
+// per manifold (the records of include/b3g.h); tangents of manifolds without
+// points, which the reference leaves unset, are written as zero. Returns the
+// constraint count; *manifoldCount receives the manifold count.
+REF_API uint32_t refw_contact_solver(void* p, uint32_t count, const uint32_t* list, const float* bodies,
+	const float* friction, const float* restitution, float dtRatio, uint32_t warm, uint32_t* conOut,
+	uint32_t* manOut, uint32_t* manifoldCount)
+{
+	RefWorld* w = (RefWorld*)p;
+	std::vector<b3Contact*> all;
+	for (b3Contact* c = w->world->m_contactManager.m_contactList; c; c = c->m_next)
+		all.push_back(c);
+	std::vector<b3Contact*> sel;
+	std::vector<uint32_t> selIndex;
+	if (list)
+	{
+		for (uint32_t i = 0; i < count; ++i)
+		{
+			sel.push_back(all[list[i]]);
+			selIndex.push_back(list[i]);
+		}
+	}
+	else
+	{
+		for (size_t i = 0; i < all.size(); ++i)
+		{
+			b3Contact* c = all[i];
+			if (!c->IsTouching() || c->m_fixtureA->m_isSensor || c->m_fixtureB->m_isSensor)
+				continue;
+			sel.push_back(c);
+			selIndex.push_back((uint32_t)i);
+		}
+	}
+	for (size_t i = 0; i < w->fixtures.size(); ++i)
+	{
+		w->fixtures[i]->m_friction = friction[i];
+		w->fixtures[i]->m_restitution = restitution[i];
+	}
+	const size_t nb = w->bodies.size();
+	std::vector<b3Position> pos(nb);
+	std::vector<b3Velocity> vel(nb);
+	std::vector<scalar> savedMass(nb);
+	std::vector<b3Vec3> savedCenter(nb);
+	for (size_t i = 0; i < nb; ++i)
+	{
+		b3Body* b = w->bodies[i];
+		const float* r = bodies + 28 * i;
+		savedMass[i] = b->m_invMass;
+		savedCenter[i] = b->m_sweep.localCenter;
+		b->m_islandIndex = (uint32)i;
+		b->m_invMass = r[13];
+		b->m_sweep.localCenter.Set(r[14], r[15], r[16]);
+		pos[i].x.Set(r[0], r[1], r[2]);
+		pos[i].q.v.Set(r[3], r[4], r[5]);
+		pos[i].q.s = r[6];
+		pos[i].I = b3Mat33(b3Vec3(r[17], r[18], r[19]), b3Vec3(r[20], r[21], r[22]), b3Vec3(r[23], r[24], r[25]));
+		vel[i].v.Set(r[7], r[8], r[9]);
+		vel[i].w.Set(r[10], r[11], r[12]);
+	}
+	b3TimeStep step;
+	step.dt = scalar(1) / scalar(60);
+	step.inv_dt = scalar(60);
+	step.dtRatio = dtRatio;
+	step.velocityIterations = 8;
+	step.positionIterations = 2;
+	step.warmStarting = warm != 0;
+	b3ContactSolverDef def;
+	def.step = step;
+	def.contacts = sel.data();
+	def.count = (uint32)sel.size();
+	def.positions = pos.data();
+	def.velocities = vel.data();
+	def.allocator = &w->world->m_stackAllocator;
+	uint32_t mk = 0;
+	{
+		b3ContactSolver solver(&def);
+		solver.InitializeVelocityConstraints();
+		for (uint32_t i = 0; i < def.count; ++i)
+		{
+			const b3ContactVelocityConstraint& vc = solver.m_velocityConstraints[i];
+			const b3ContactPositionConstraint& pc = solver.m_positionConstraints[i];
+			uint32_t* o = conOut + 32 * (size_t)i;
+			memset(o, 0, 128);
+			o[0] = vc.indexA;
+			o[1] = vc.indexB;
+			o[2] = mk;
+			o[3] = vc.manifoldCount;
+			PutF(o + 4, vc.invMassA);
+			PutF(o + 5, vc.invMassB);
+			PutF(o + 6, vc.friction);
+			PutF(o + 7, vc.restitution);
+			PutM(o + 8, vc.invIA);
+			PutM(o + 17, vc.invIB);
+			PutF(o + 26, pc.radiusA);
+			PutF(o + 27, pc.radiusB);
+			o[28] = selIndex[i];
+			for (uint32_t j = 0; j < vc.manifoldCount; ++j, ++mk)
+			{
+				const b3VelocityConstraintManifold& vm = vc.manifolds[j];
+				const b3PositionConstraintManifold& pm = pc.manifolds[j];
+				uint32_t* m = manOut + 116 * (size_t)mk;
+				memset(m, 0, 464);
+				PutV(m, vm.rA);
+				PutV(m + 3, vm.rB);
+				PutV(m + 6, vm.normal);
+				if (vm.pointCount > 0)
+				{
+					PutV(m + 9, vm.tangent1);
+					PutV(m + 12, vm.tangent2);
+				}
+				PutF(m + 15, vm.tangentSpeed1);
+				PutF(m + 16, vm.tangentSpeed2);
+				PutF(m + 17, vm.tangentMass.x.x);
+				PutF(m + 18, vm.tangentMass.x.y);
+				PutF(m + 19, vm.tangentMass.y.x);
+				PutF(m + 20, vm.tangentMass.y.y);
+				PutF(m + 21, vm.tangentImpulse.x);
+				PutF(m + 22, vm.tangentImpulse.y);
+				PutF(m + 23, vm.motorImpulse);
+				PutF(m + 24, vm.motorMass);
+				PutF(m + 25, vm.motorSpeed);
+				m[26] = vm.pointCount;
+				m[27] = i;
+				for (uint32_t k = 0; k < vm.pointCount && k < 4; ++k)
+				{
+					const b3VelocityConstraintPoint& vp = vm.points[k];
+					uint32_t* q = m + 32 + 12 * k;
+					PutV(q, vp.rA);
+					PutV(q + 3, vp.rB);
+					PutV(q + 6, vp.normal);
+					PutF(q + 9, vp.normalMass);
+					PutF(q + 10, vp.normalImpulse);
+					PutF(q + 11, vp.velocityBias);
+					const b3PositionConstraintPoint& pp = pm.points[k];
+					uint32_t* r = m + 80 + 9 * k;
+					PutV(r, pp.localNormalA);
+					PutV(r + 3, pp.localPointA);
+					PutV(r + 6, pp.localPointB);
+				}
+			}
+		}
+	}
+	for (size_t i = 0; i < nb; ++i)
+	{
+		w->bodies[i]->m_invMass = savedMass[i];
+		w->bodies[i]->m_sweep.localCenter = savedCenter[i];
+	}
+	*manifoldCount = mk;
+	return (uint32_t)sel.size();
+}
+
+// Mass data of every body as the reference computed it from its fixtures
+// (b3Body::ResetMassData): 1 + 9 + 9 floats per body, m_invMass, m_invI and
+// m_worldInvI (columns x, y, z).
+REF_API void refw_mass_data(void* p, float* out)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		const b3Body* b = w->bodies[i];
+		float* o = out + 19 * i;
+		o[0] = (float)b->m_invMass;
+		const b3Mat33* m[2] = {&b->m_invI, &b->m_worldInvI};
+		for (int k = 0; k < 2; ++k)
+		{
+			const b3Vec3* col[3] = {&m[k]->x, &m[k]->y, &m[k]->z};
+			for (int c = 0; c < 3; ++c)
+			{
+				o[1 + 9 * k + 3 * c] = (float)col[c]->x;
+				o[2 + 9 * k + 3 * c] = (float)col[c]->y;
+				o[3 + 9 * k + 3 * c] = (float)col[c]->z;
+			}
+		}
+	}
 }
 
 // World queries through the reference's own b3World entry points.
