@@ -14,7 +14,8 @@ through the C ABI with host buffers (host->device copy of the pinned state,
 device->host contact list and packed touching manifolds every step, the
 copies of one step overlapping the next step's pass). Other workloads:
 --workload pile (hull pile over a mesh), batched (1,024 worlds), serving
-(request stream) and queries (ray casts). The reference arm
+(request stream), queries (ray casts) and constraints (the solver's contact
+constraints built from the pass's manifolds). The reference arm
 (--impl reference) runs the reference's own CPU pipeline (oracle/_ref, the
 unmodified Bounce sources) on the same scene and body motion.
 
@@ -60,7 +61,8 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=30,
                     help="passes after the timed ones, with per-stage CUDA events (not part of value)")
     ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
-    ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving", "queries"])
+    ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving", "queries",
+                                                             "constraints"])
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000",
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
@@ -243,6 +245,20 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
         return
+    if args.workload == "constraints":
+        scene, walls = workload_scene(args, SEED)
+        rc, rm, t = constraint_reference(scene, walls, SEED + 200)
+        v = rc / t
+        print(json.dumps({
+            "metric": "contact constraints/s", "value": v, "unit": "constraints/s", "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": CONSTRAINT_WORKLOAD, "constraints_per_step": rc, "manifolds_per_step": rm},
+            "cpu_baseline": {"value": v, "unit": "constraints/s", "cores": 1, "kind": "reference",
+                             "sample": f"the whole step ({rc} constraints) through b3ContactSolver's constructor "
+                                       "and InitializeVelocityConstraints on 1 host core"},
+            "e2e": {"value": v, "unit": "constraints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
     if args.workload == "queries":
         scene, walls = workload_scene(args, SEED)
         rays = make_rays(SEED + 100, QUERY_CPU_RAYS, scene_half(scene))
@@ -291,15 +307,15 @@ def algorithmic_bytes(scene, counts):
     return int(scene.n_fixtures * (68 + 60 + 64 + 1) + hv)
 
 
-def committed_traffic(kernel, args):
+def committed_traffic(kernel, args, label="mixed 65,536"):
     """DRAM bytes per launch of `kernel` from the committed ncu summary
     (profiles/roofline_traffic.md), for the workload it was captured on."""
-    if args.workload != "mixed" or args.bodies != N_BODIES:
+    if args.workload not in ("mixed", "constraints") or args.bodies != N_BODIES:
         return None
     try:
         for line in open(os.path.join(ROOT, "profiles", "roofline_traffic.md")):
             cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if len(cells) == 3 and cells[0] == kernel and cells[1] == "mixed 65,536":
+            if len(cells) == 3 and cells[0] == kernel and cells[1] == label:
                 return int(cells[2])
     except (OSError, ValueError):
         pass
@@ -900,6 +916,192 @@ def run_queries(args, rank, world, local, dist):
     pipe.close()
 
 
+CONSTRAINT_WORKLOAD = ("b3ContactSolver constructor + InitializeVelocityConstraints over the 65,536-body mixed "
+                       "world after 3 collision passes: every touching non-sensor contact, seeded body velocities "
+                       "N(0, 1), inverse masses 1/U(0.5, 5) kg, world inverse inertias R diag(1/U(0.05, 2)) R^T, "
+                       "friction U(0.2, 0.8) and restitution U(0, 0.5) per fixture")
+
+
+def constraint_inputs(scene, drv, seed):
+    """Seeded solver inputs: one b3g_solver_body per body (the pass's centre
+    of mass and orientation, synthetic velocities and mass data) and the
+    fixtures' friction and restitution."""
+    from bounce_b200 import _native as N
+
+    rng = np.random.default_rng(seed)
+    sw = drv.sweeps14().reshape(-1, 14)
+    n = len(sw)
+    b = np.zeros(n, N.SOLVER_BODY_DTYPE)
+    b["x"], b["q"] = sw[:, 7:10], sw[:, 10:14]
+    b["v"] = rng.normal(0.0, 1.0, (n, 3))
+    b["w"] = rng.normal(0.0, 1.0, (n, 3))
+    b["localCenter"] = np.asarray(scene.local_center, np.float32).reshape(-1, 3)
+    dyn = scene.body_type == 2
+    b["invMass"] = np.where(dyn, 1.0 / rng.uniform(0.5, 5.0, n), 0.0)
+    q = sw[:, 10:14].astype(np.float64)
+    x, y, z, s = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    R = np.stack([np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - s * z), 2 * (x * z + s * y)], -1),
+                  np.stack([2 * (x * y + s * z), 1 - 2 * (x * x + z * z), 2 * (y * z - s * x)], -1),
+                  np.stack([2 * (x * z - s * y), 2 * (y * z + s * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+    d = 1.0 / rng.uniform(0.05, 2.0, (n, 3))
+    inv_i = np.einsum("nij,nj,nkj->nik", R, d, R) * dyn[:, None, None]
+    b["invI"] = inv_i.transpose(0, 2, 1).reshape(n, 9)  # columns x, y, z
+    nf = scene.n_fixtures
+    fr = rng.uniform(0.2, 0.8, nf).astype(np.float32)
+    re = rng.uniform(0.0, 0.5, nf).astype(np.float32)
+    return b, fr, re
+
+
+def constraint_reference(scene, walls, seed):
+    """The reference's b3ContactSolver constructor and
+    InitializeVelocityConstraints on the same world after the same 3 passes,
+    on 1 host core: (constraints, manifolds, seconds)."""
+    from bounce_b200 import scene as S
+    from oracle import oracle as O
+
+    rw = O.RefWorld(scene)
+    drv = S.KinematicDriver(scene, walls=walls)
+    rw.first_pass()
+    for _ in range(2):
+        drv.advance()
+        rw.set_sweeps(drv.sweeps14())
+        rw.step_pass()
+    b, fr, re = constraint_inputs(scene, drv, seed)
+    con, man, t = rw.contact_solver(b.view(np.float32).reshape(-1, 28), fr, re, timed=True)
+    rw.close()
+    return len(con), len(man), t
+
+
+def run_constraints(args, rank, world, local, dist):
+    import ctypes
+
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+    from bounce_b200 import scene as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene, walls = workload_scene(args, SEED + rank)
+    drv = S.KinematicDriver(scene, walls=walls)
+    nb, nf = scene.n_bodies, scene.n_fixtures
+    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local)
+    for k in range(3):
+        if k:
+            drv.advance()
+        pipe.collide(drv.state17())
+    counts = pipe.counts()
+    assert counts["status"] == 0
+    bodies, fr, re = constraint_inputs(scene, drv, SEED + 200 + rank)
+    pipe.set_materials(fr, re)
+    con_h, man_h = pipe.contact_constraints(bodies)
+    nc, nm = len(con_h), len(man_h)
+    d_bodies = torch.from_numpy(bodies.view(np.uint8).copy()).to(dev)
+    d_con = torch.empty(max(nc, 1) * 128, dtype=torch.uint8, device=dev)
+    d_man = torch.empty(max(nm, 1) * 464, dtype=torch.uint8, device=dev)
+    d_counts = torch.zeros(2, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    lib = pipe.lib
+
+    def build():
+        pipe._check(lib.b3g_contact_constraints_device(
+            pipe.ctx, 0, None, ctypes.c_void_p(d_bodies.data_ptr()), 1.0, 1, ctypes.c_void_p(d_con.data_ptr()), nc,
+            ctypes.c_void_p(d_man.data_ptr()), nm, ctypes.c_void_p(d_counts.data_ptr()), sptr))
+
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            build()
+    stream.synchronize()
+    assert d_counts.cpu().numpy().tolist() == [nc, nm]
+    same = bool(np.array_equal(d_man.cpu().numpy().view(np.uint32), man_h.view(np.uint32).reshape(-1)))
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flushed between steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            build()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    secs, work = replica_totals(dist, dev, ms / 1000.0, nc * args.steps)
+    value = work / secs
+
+    # e2e: the host-buffer entry point (bodies copied in, records copied out).
+    e2e_steps = max(1, min(args.e2e_steps, 10))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        pipe.contact_constraints(bodies)
+    e2e_s, e2e_work = replica_totals(dist, dev, time.perf_counter() - t0, nc * e2e_steps)
+    e2e_value = e2e_work / e2e_s
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # Algorithmic bytes of one launch, each byte once: per contact its state
+    # and fixtures (12 B); per fixture flags, body, type, radius and material
+    # (24 B); per body its b3g_solver_body (112 B); per manifold its header
+    # and points as read (24 + 40 per point); the records written.
+    points = int(man_h["pointCount"].sum())
+    algo = (12 * counts["contacts"] + 24 * nf + 112 * nb + 24 * nm + 40 * points + 128 * nc + 464 * nm)
+    achieved = algo / (ms / args.steps / 1000.0) / 1e9
+    roof = {"kernel": "k_ci_tiles + k_ci_scan_tiles + k_ci_build (b3g_contact_constraints_device)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+            "traffic": committed_traffic("k_ci_build", args, "constraints 65,536"), "algorithmic_bytes_per_launch": algo,
+            "note": "three launches per step; achieved over the whole call",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_scene, ref_walls = workload_scene(args, SEED)
+            rc, rm, rt = constraint_reference(ref_scene, ref_walls, SEED + 200)
+            cpu = {"value": rc / rt, "unit": "constraints/s", "cores": 1, "kind": "reference",
+                   "sample": f"the whole step ({rc} constraints, {rm} manifolds) through the reference's "
+                             "b3ContactSolver constructor and InitializeVelocityConstraints on 1 host core"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "constraints/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "contact constraints/s", "value": value, "unit": "constraints/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": CONSTRAINT_WORKLOAD, "bodies": nb, "contacts": counts["contacts"],
+                       "constraints_per_step": nc, "manifolds_per_step": nm, "points_per_step": points,
+                       "device_records_equal_host_entry": same,
+                       "l2": "flushed between steps (256 MB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "constraints/s", "h2d_bytes_per_step": 112 * nb,
+                    "d2h_bytes_per_step": 128 * nc + 464 * nm + 8, "steps": e2e_steps},
+            "gpu_launches": 3 * args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    pipe.close()
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_init(args)
@@ -912,6 +1114,8 @@ def main():
             run_serving(args, rank, world, local, dist)
         elif args.workload == "queries":
             run_queries(args, rank, world, local, dist)
+        elif args.workload == "constraints":
+            run_constraints(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

@@ -1905,13 +1905,14 @@ extern "C" int b3g_contact_constraints_device(b3g_ctx* c, uint32_t count, const 
 		return fail(c, B3G_E_CAPACITY, "b3g_contact_constraints_device: %u contacts exceed max_contacts %u", count,
 			c->cfg.max_contacts);
 	CK(cudaSetDevice(c->device));
-	const uint32_t tiles = std::max(contact_constraint_tiles(c->cfg.max_contacts), 1u);
-	if (c->ciTileCap < tiles)
+	// Tile counter and one status word per tile of the largest call.
+	const uint32_t words = contact_constraint_tiles(c->cfg.max_contacts) + 1;
+	if (c->ciTileCap < words)
 	{
 		dfree(c->ciTiles);
 		c->ciTileCap = 0;
-		CK(dalloc(&c->ciTiles, tiles));
-		c->ciTileCap = tiles;
+		CK(dalloc(&c->ciTiles, words));
+		c->ciTileCap = words;
 	}
 	ConstraintCall q;
 	q.list = contacts;

@@ -310,7 +310,7 @@ struct b3g_ctx
 	void* qScratch;       // device scratch of the world queries
 	size_t qScratchBytes;
 	float2* dFixMaterial;         // per fixture: friction, restitution (b3g_set_materials)
-	unsigned long long* ciTiles;  // b3g_contact_constraints_device: tile sums (allocated on first use)
+	unsigned long long* ciTiles;  // b3g_contact_constraints_device: tile counter and states (allocated on first use)
 	uint32_t ciTileCap;
 	void* ciHost;                 // b3g_contact_constraints: device copies of its host buffers
 	size_t ciHostBytes;

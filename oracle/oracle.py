@@ -96,7 +96,7 @@ def lib(precision=32):
         "refw_query_aabb": ([vp, f32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_fixture_edges": ([vp, u32p, u32p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_contact_solver": (
-            [vp, ctypes.c_uint32, u32p, f32p, f32p, f32p, ctypes.c_float, ctypes.c_uint32, u32p, u32p, u32p],
+            [vp, ctypes.c_uint32, u32p, f32p, f32p, f32p, ctypes.c_float, ctypes.c_uint32, u32p, u32p, u32p, f64p],
             ctypes.c_uint32,
         ),
         "refw_mass_data": ([vp, f32p], None),
@@ -262,13 +262,14 @@ class RefWorld:
         self.L.refw_mass_data(self.w, _p(out, ctypes.c_float))
         return out[:nb, 0].copy(), out[:nb, 1:10].copy(), out[:nb, 10:19].copy()
 
-    def contact_solver(self, bodies, friction, restitution, dt_ratio=1.0, warm=True, contacts=None):
+    def contact_solver(self, bodies, friction, restitution, dt_ratio=1.0, warm=True, contacts=None, timed=False):
         """The reference's b3ContactSolver constructor and
         InitializeVelocityConstraints on this world's contacts (the listed
         contact-list positions, or every touching non-sensor contact in list
         order). bodies: (n, 28) float32 in the b3g_solver_body layout;
         friction, restitution per fixture. Returns the raw records:
-        constraints (k, 32) and manifolds (m, 116) as uint32 words."""
+        constraints (k, 32) and manifolds (m, 116) as uint32 words (and, with
+        timed, the seconds of the constructor and InitializeVelocityConstraints)."""
         b = np.ascontiguousarray(bodies, np.float32).reshape(-1, 28)
         fr = np.ascontiguousarray(friction, np.float32)
         re = np.ascontiguousarray(restitution, np.float32)
@@ -277,10 +278,13 @@ class RefWorld:
         con = np.zeros((max(count, 1), 32), np.uint32)
         man = np.zeros((max(3 * count, 1), 116), np.uint32)
         mc = ctypes.c_uint32()
+        secs = ctypes.c_double()
         k = self.L.refw_contact_solver(self.w, 0 if lst is None else len(lst), _p(lst, ctypes.c_uint32),
                                        _p(b, ctypes.c_float), _p(fr, ctypes.c_float), _p(re, ctypes.c_float),
                                        float(dt_ratio), 1 if warm else 0, _p(con, ctypes.c_uint32),
-                                       _p(man, ctypes.c_uint32), ctypes.byref(mc))
+                                       _p(man, ctypes.c_uint32), ctypes.byref(mc), ctypes.byref(secs))
+        if timed:
+            return con[:k], man[:mc.value], secs.value
         return con[:k], man[:mc.value]
 
     def query_aabb(self, box):

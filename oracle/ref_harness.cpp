@@ -688,10 +688,12 @@ static inline void PutM(uint32_t* o, const b3Mat33& m)
 // fixture are set on the fixtures. Writes 32 words per constraint and 116
 // per manifold (the records of include/b3g.h); tangents of manifolds without
 // points, which the reference leaves unset, are written as zero. Returns the
-// constraint count; *manifoldCount receives the manifold count.
+// constraint count; *manifoldCount receives the manifold count and, when
+// seconds is not null, *seconds the time of the constructor and
+// InitializeVelocityConstraints alone.
 REF_API uint32_t refw_contact_solver(void* p, uint32_t count, const uint32_t* list, const float* bodies,
 	const float* friction, const float* restitution, float dtRatio, uint32_t warm, uint32_t* conOut,
-	uint32_t* manOut, uint32_t* manifoldCount)
+	uint32_t* manOut, uint32_t* manifoldCount, double* seconds)
 {
 	RefWorld* w = (RefWorld*)p;
 	std::vector<b3Contact*> all;
@@ -760,8 +762,11 @@ REF_API uint32_t refw_contact_solver(void* p, uint32_t count, const uint32_t* li
 	def.allocator = &w->world->m_stackAllocator;
 	uint32_t mk = 0;
 	{
+		double t0 = Now();
 		b3ContactSolver solver(&def);
 		solver.InitializeVelocityConstraints();
+		if (seconds)
+			*seconds = Now() - t0;
 		for (uint32_t i = 0; i < def.count; ++i)
 		{
 			const b3ContactVelocityConstraint& vc = solver.m_velocityConstraints[i];
