@@ -155,6 +155,22 @@ MANIFOLD_CONSTRAINT_DTYPE = np.dtype(
         ("positionPoints", POSITION_POINT_DTYPE, 4),
     ]
 )
+# b3g_shape_cast_input: a convex shape at a transform swept along a
+# displacement (b3World::ShapeCast's arguments, world.cpp:752-753).
+SHAPE_CAST_DTYPE = np.dtype(
+    [
+        ("type", "<u4"),
+        ("hull", "<u4"),
+        ("world", "<u4"),
+        ("pad", "<u4"),
+        ("params", "<f4", 12),
+        ("position", "<f4", 3),
+        ("rotation", "<f4", 4),
+        ("displacement", "<f4", 3),
+        ("pad2", "<f4", 2),
+    ]
+)
+assert SHAPE_CAST_DTYPE.itemsize == 112
 assert SOLVER_BODY_DTYPE.itemsize == 112 and CONTACT_CONSTRAINT_DTYPE.itemsize == 128
 assert MANIFOLD_CONSTRAINT_DTYPE.itemsize == 464
 
@@ -195,6 +211,8 @@ EXPORTED = [
     "b3g_ray_cast",
     "b3g_ray_cast_single",
     "b3g_ray_cast_single_device",
+    "b3g_shape_cast",
+    "b3g_shape_cast_single",
     "b3g_set_materials",
     "b3g_contact_constraints",
     "b3g_contact_constraints_device",
@@ -272,6 +290,8 @@ def load():
         "b3g_ray_cast": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_ray_cast_single": ([ctx, ctypes.c_uint32, f32p, u32p, u32p, f32p], ctypes.c_int),
         "b3g_ray_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp, vp], ctypes.c_int),
+        "b3g_shape_cast": ([ctx, ctypes.c_uint32, vp, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
+        "b3g_shape_cast_single": ([ctx, ctypes.c_uint32, vp, u32p, f32p], ctypes.c_int),
         "b3g_set_materials": ([ctx, f32p, f32p], ctypes.c_int),
         "b3g_contact_constraints": ([ctx, ctypes.c_uint32, u32p, vp, ctypes.c_float, ctypes.c_int, vp,
                                      ctypes.c_uint32, vp, ctypes.c_uint32, u32p], ctypes.c_int),

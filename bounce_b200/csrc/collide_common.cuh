@@ -663,15 +663,12 @@ __device__ __forceinline__ XF load_xf(const float* s)
 }
 
 // b3Shape::ComputeAABB for one transform (hull_shape.cpp:160-164,
-// sphere_shape.cpp:51-57, capsule_shape.cpp:124-131, triangle_shape.cpp:59-67).
+// sphere_shape.cpp:51-57, capsule_shape.cpp:124-131, triangle_shape.cpp:59-67)
+// of a shape given by its type, parameters (the fixture layout) and hull.
 // Two transforms are handled in one vertex loop for hulls.
-__device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb,
-	bool two, AABB& a, AABB& b)
+__device__ inline void compute_shape_aabbs(const DevScene& S, uint32_t type, float4 p0, float4 p1, float4 p2,
+	uint32_t hull, const XF& xa, const XF& xb, bool two, AABB& a, AABB& b)
 {
-	uint32_t type = S.fixType[fix];
-	float4 p0 = S.fixParams[3 * fix + 0];
-	float4 p1 = S.fixParams[3 * fix + 1];
-	float4 p2 = S.fixParams[3 * fix + 2];
 	if (type == B3G_SHAPE_SPHERE)
 	{
 		V3 c = V3{p0.x, p0.y, p0.z};
@@ -718,7 +715,7 @@ __device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& 
 	}
 	else // hull
 	{
-		const HullDesc h = S.hulls[S.fixHull[fix]];
+		const HullDesc h = S.hulls[hull];
 		const float4* hv = S.hverts + h.vOff;
 		float4 w = hv[0];
 		V3 v = V3{w.x, w.y, w.z};
@@ -751,6 +748,24 @@ __device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& 
 		if (two)
 			aabb_extend(b, r);
 	}
+}
+
+// b3AABB::Scale (aabb.h:287-294).
+__device__ __forceinline__ AABB aabb_scaled(const AABB& a, V3 s)
+{
+	V3 l = vmul(s, a.lo), u = vmul(s, a.hi);
+	AABB r;
+	r.lo = vmin(l, u);
+	r.hi = vmax(l, u);
+	return r;
+}
+
+// The same for fixture fix.
+__device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb, bool two, AABB& a,
+	AABB& b)
+{
+	compute_shape_aabbs(S, S.fixType[fix], S.fixParams[3 * fix + 0], S.fixParams[3 * fix + 1],
+		S.fixParams[3 * fix + 2], S.fixHull[fix], xa, xb, two, a, b);
 }
 
 // Exact cull, not in the reference: every convex routine (sphere, capsule,

@@ -395,26 +395,11 @@ struct Simplex
 	}
 };
 
-// b3GJK with an empty simplex cache (gjk.cpp:654-812 via :1104-1110).
-__device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, bool applyRadius,
-	GJKSimplexOut* simplexOut = nullptr)
+// The main loop of b3GJK (gjk.cpp:683-768) on an initialised simplex;
+// returns the support iterations.
+__device__ __forceinline__ uint32_t gjk_loop(Simplex& sx, const XF& xf1, const GProxy& p1, const XF& xf2,
+	const GProxy& p2)
 {
-	Simplex sx;
-	{
-		// Arbitrary first vertex (gjk.cpp:850-863).
-		SVert& v = sx.v[0];
-		v.point1 = xmul(xf1, gp_vertex(p1, 0));
-		v.point2 = xmul(xf2, gp_vertex(p2, 0));
-		v.point = v.point2 - v.point1;
-		v.weight = 1.0f;
-		v.index1 = 0;
-		v.index2 = 0;
-		sx.count = 1;
-	}
-	// The simplex is indexed with constants only (unrolled loops, explicit
-	// slot selection) so it stays in registers.
-	for (int i = 1; i < 4; ++i)
-		sx.v[i] = sx.v[0];
 	uint32_t save1[4], save2[4];
 	uint32_t saveCount = 0;
 	const uint32_t kMaxIters = 20;
@@ -462,6 +447,34 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 			sx.v[3] = vx;
 		++sx.count;
 	}
+	return iter;
+}
+
+// b3Simplex's arbitrary first vertex (gjk.cpp:855-867).
+__device__ __forceinline__ void simplex_first(Simplex& sx, const XF& xf1, const GProxy& p1, const XF& xf2,
+	const GProxy& p2)
+{
+	SVert& v = sx.v[0];
+	v.point1 = xmul(xf1, gp_vertex(p1, 0));
+	v.point2 = xmul(xf2, gp_vertex(p2, 0));
+	v.point = v.point2 - v.point1;
+	v.weight = 1.0f;
+	v.index1 = 0;
+	v.index2 = 0;
+	sx.count = 1;
+	// The simplex is indexed with constants only (unrolled loops, explicit
+	// slot selection) so it stays in registers.
+	for (int i = 1; i < 4; ++i)
+		sx.v[i] = sx.v[0];
+}
+
+// b3GJK with an empty simplex cache (gjk.cpp:654-812 via :1104-1110).
+__device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, bool applyRadius,
+	GJKSimplexOut* simplexOut = nullptr)
+{
+	Simplex sx;
+	simplex_first(sx, xf1, p1, xf2, p2);
+	uint32_t iter = gjk_loop(sx, xf1, p1, xf2, p2);
 	if (simplexOut)
 	{
 		simplexOut->count = sx.count;
@@ -494,6 +507,86 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 			out.point2 = p;
 			out.distance = 0.0f;
 		}
+	}
+	return out;
+}
+
+// b3SimplexCache (gjk.h): the support indices of the last simplex and its
+// metric.
+struct GJKCache
+{
+	uint32_t count;
+	uint32_t index1[4], index2[4];
+	float metric;
+};
+
+// b3Simplex::GetMetric (gjk.cpp:881-912).
+__device__ __forceinline__ float simplex_metric(const Simplex& sx)
+{
+	if (sx.count == 2)
+		return len(sx.v[0].point - sx.v[1].point);
+	if (sx.count == 3)
+		return len(cross(sx.v[1].point - sx.v[0].point, sx.v[2].point - sx.v[0].point));
+	if (sx.count == 4)
+	{
+		V3 E1 = sx.v[1].point - sx.v[0].point;
+		V3 E2 = sx.v[2].point - sx.v[0].point;
+		V3 E3 = sx.v[3].point - sx.v[0].point;
+		float det = det3(E1, E2, E3);
+		return signf_(det) * det;
+	}
+	return 0.0f;
+}
+
+// b3GJK(xf1, proxy1, xf2, proxy2, false, &cache) (gjk.cpp:654-812): the
+// simplex starts from the cache (b3Simplex::ReadCache, gjk.cpp:820-868: the
+// cached support points with zero weights, flushed to the arbitrary vertex
+// when their metric changed by more than a factor of two or vanished) and is
+// written back to it (WriteCache, gjk.cpp:870-879). No radius is applied.
+__device__ inline GJKOut gjk_cached(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, GJKCache& cache)
+{
+	Simplex sx;
+	sx.count = cache.count;
+	// Only the cached entries are read (their indices are support indices of
+	// these proxies); the slots past them repeat slot 0.
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+	{
+		SVert& v = sx.v[i];
+		if ((uint32_t)i < cache.count)
+		{
+			v.index1 = cache.index1[i];
+			v.index2 = cache.index2[i];
+			v.point1 = xmul(xf1, gp_vertex(p1, v.index1));
+			v.point2 = xmul(xf2, gp_vertex(p2, v.index2));
+			v.point = v.point2 - v.point1;
+			v.weight = 0.0f;
+		}
+		else if (i > 0)
+		{
+			v = sx.v[0];
+		}
+	}
+	if (sx.count > 1)
+	{
+		const float metric1 = cache.metric;
+		const float metric2 = simplex_metric(sx);
+		if (metric2 < 0.5f * metric1 || 2.0f * metric1 < metric2 || metric2 < B3G_EPSILON)
+			sx.count = 0;
+	}
+	if (sx.count == 0)
+		simplex_first(sx, xf1, p1, xf2, p2);
+	GJKOut out;
+	out.iterations = gjk_loop(sx, xf1, p1, xf2, p2);
+	sx.closest_points(out.point1, out.point2);
+	out.distance = len(out.point1 - out.point2);
+	cache.metric = simplex_metric(sx);
+	cache.count = sx.count;
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+	{
+		cache.index1[i] = sx.v[i].index1;
+		cache.index2[i] = sx.v[i].index2;
 	}
 	return out;
 }

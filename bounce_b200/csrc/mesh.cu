@@ -345,16 +345,6 @@ __device__ __forceinline__ V3 mesh_scale(const DevScene& S, uint32_t f)
 	return V3{p.x, p.y, p.z};
 }
 
-// b3AABB::Scale (aabb.h:287-294).
-__device__ __forceinline__ AABB aabb_scaled(const AABB& a, V3 s)
-{
-	V3 l = vmul(s, a.lo), u = vmul(s, a.hi);
-	AABB r;
-	r.lo = vmin(l, u);
-	r.hi = vmax(l, u);
-	return r;
-}
-
 // b3MeshContact::MoveAABB (mesh_contact.cpp:175-231): false when the box
 // stays inside the old fat box.
 __device__ __forceinline__ bool move_aabb(AABB& fat, const AABB& aabb, V3 d)

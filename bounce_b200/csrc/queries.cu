@@ -1,6 +1,6 @@
-// World queries on the device: b3World::QueryAABB, RayCast and RayCastSingle
-// (world.cpp:452-566, :854-878) over the LBVH and fat AABBs of the last pass,
-// with each shape's own ray cast:
+// World queries on the device: b3World::QueryAABB, RayCast, RayCastSingle,
+// ShapeCast and ShapeCastSingle (world.cpp:452-878) over the LBVH and fat
+// AABBs of the last pass, with each shape's own ray cast:
 //   b3SphereShape::RayCast    sphere_shape.cpp:69-122
 //   b3CapsuleShape::RayCast   capsule_shape.cpp:180-322
 //   b3HullShape::RayCast      hull_shape.cpp:189-275
@@ -472,6 +472,314 @@ __global__ void k_ray_cast(QueryCtx q, const float* rays, const uint32_t* worlds
 	}
 }
 
+// ---------------------------------------------------------------------------
+// Shape casts: b3World::ShapeCast / ShapeCastSingle (world.cpp:568-851), each
+// candidate fixture (fat AABB overlapping the swept AABB of the cast shape)
+// tested with the translational b3TimeOfImpact (time_of_impact.cpp:666-776)
+// and the touching ones evaluated with b3GJK at the time of impact.
+
+// b3TOIOutput::State (time_of_impact.h:40-47).
+enum : uint32_t
+{
+	TOI_UNKNOWN = 0,
+	TOI_FAILED,
+	TOI_OVERLAPPED,
+	TOI_TOUCHING,
+	TOI_SEPARATED
+};
+
+struct TOIOut
+{
+	uint32_t state;
+	float t;
+};
+
+// b3TimeOfImpact(xf1, proxy1, d1, xf2, proxy2, d2) (time_of_impact.cpp:666-776):
+// Mirtich's conservative advancement along the translations, the GJK simplex
+// carried from one iteration to the next, at most 20 iterations.
+__device__ TOIOut toi_translate(const XF& xf1, const GProxy& p1, V3 d1, const XF& xf2, const GProxy& p2, V3 d2)
+{
+	const float totalRadius = p1.radius + p2.radius;
+	const float target = fmaxr(B3G_LINEAR_SLOP, totalRadius - 3.0f * B3G_LINEAR_SLOP);
+	const float tolerance = 0.25f * B3G_LINEAR_SLOP;
+	GJKCache cache;
+	cache.count = 0;
+	cache.metric = 0.0f;
+	for (int i = 0; i < 4; ++i)
+		cache.index1[i] = cache.index2[i] = 0u;
+	float t = 0.0f;
+	XF xf1t = xf1, xf2t = xf2;
+	for (uint32_t iteration = 0; iteration < 20u; ++iteration)
+	{
+		GJKOut q = gjk_cached(xf1t, p1, xf2t, p2, cache);
+		if (q.distance == 0.0f)
+			return TOIOut{TOI_OVERLAPPED, 0.0f};
+		if (q.distance < target + tolerance)
+			return TOIOut{TOI_TOUCHING, t};
+		V3 n = (q.point2 - q.point1) / q.distance;
+		float denominator = dot(d2 - d1, n);
+		if (denominator >= 0.0f)
+			return TOIOut{TOI_SEPARATED, 1.0f};
+		float dt = (target - q.distance) / denominator;
+		t += dt;
+		if (t >= 1.0f)
+			return TOIOut{TOI_SEPARATED, 1.0f};
+		xf1t.p = xf1.p + t * d1;
+		xf2t.p = xf2.p + t * d2;
+	}
+	return TOIOut{TOI_UNKNOWN, t};
+}
+
+// b3GJKProxy::Set (gjk.cpp:37-95) for a convex shape given by type,
+// parameters (the fixture layout) and hull.
+__device__ GProxy cast_proxy(const DevScene& S, uint32_t type, float4 p0, float4 p1, float4 p2, uint32_t hull)
+{
+	GProxy g;
+	g.gv = nullptr;
+	g.lv[0] = g.lv[1] = g.lv[2] = V3{0.0f, 0.0f, 0.0f};
+	switch (type)
+	{
+	case B3G_SHAPE_SPHERE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.count = 1;
+		g.radius = p0.w;
+		break;
+	case B3G_SHAPE_CAPSULE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.lv[1] = V3{p0.w, p1.x, p1.y};
+		g.count = 2;
+		g.radius = p1.z;
+		break;
+	case B3G_SHAPE_TRIANGLE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.lv[1] = V3{p0.w, p1.x, p1.y};
+		g.lv[2] = V3{p1.z, p1.w, p2.x};
+		g.count = 3;
+		g.radius = p2.y;
+		break;
+	default:
+	{
+		const HullDesc h = S.hulls[hull];
+		g.gv = S.hverts + h.vOff;
+		g.count = h.vCnt;
+		g.radius = p0.x;
+		break;
+	}
+	}
+	return g;
+}
+
+// The proxy of a mesh fixture's triangle (gjk.cpp:75-89): its vertices
+// scaled by the mesh scale, the mesh radius.
+__device__ GProxy mesh_triangle_proxy(const DevScene& S, uint32_t fix, uint32_t tri)
+{
+	const MeshDesc md = S.meshes[S.fixHull[fix]];
+	const float4 sp = S.fixParams[3 * fix];
+	const V3 sc = V3{sp.x, sp.y, sp.z};
+	const uint4 t = S.meshTris[md.tOff + tri];
+	auto vert = [&](uint32_t i) {
+		float4 a = S.meshVerts[md.vOff + i];
+		return vmul(sc, V3{a.x, a.y, a.z});
+	};
+	GProxy g;
+	g.gv = nullptr;
+	g.lv[0] = vert(t.x);
+	g.lv[1] = vert(t.y);
+	g.lv[2] = vert(t.z);
+	g.count = 3;
+	g.radius = sp.w;
+	return g;
+}
+
+// b3WorldShapeCastQueryWrapper::Evaluate (world.cpp:719-731).
+__device__ void cast_evaluate(V3& point, V3& normal, const XF& xA, const GProxy& pA, const XF& xB, const GProxy& pB)
+{
+	GJKOut q = gjk(xA, pA, xB, pB, false);
+	normal = normalized(q.point1 - q.point2);
+	point = q.point2 + pB.radius * normal;
+}
+
+struct CastIn
+{
+	uint32_t type, hull, world;
+	float4 p0, p1, p2;
+	XF xf;
+	V3 d;
+};
+
+// b3g_shape_cast_input: type, hull, world, pad, params[12], position[3],
+// rotation[4], displacement[3], pad[2].
+__device__ __forceinline__ CastIn load_cast(const float* in, uint32_t i)
+{
+	const float* r = in + 28 * (size_t)i;
+	CastIn c;
+	c.type = __float_as_uint(r[0]);
+	c.hull = __float_as_uint(r[1]);
+	c.world = __float_as_uint(r[2]);
+	c.p0 = make_float4(r[4], r[5], r[6], r[7]);
+	c.p1 = make_float4(r[8], r[9], r[10], r[11]);
+	c.p2 = make_float4(r[12], r[13], r[14], r[15]);
+	c.xf.p = V3{r[16], r[17], r[18]};
+	c.xf.q = Q4{V3{r[19], r[20], r[21]}, r[22]};
+	c.d = V3{r[23], r[24], r[25]};
+	return c;
+}
+
+// b3World::ShapeCast with a listener that returns 1 for every fixture
+// (MODE 0 counts, MODE 1 writes (cast, fixture, triangle) + (point, normal,
+// fraction)) and b3World::ShapeCastSingle (MODE 2: the smallest fraction,
+// then the smaller fixture and triangle on an exact tie). Mesh fixtures are
+// tested triangle by triangle over their static tree, with the swept box in
+// the unscaled mesh frame (world.cpp:638-664).
+template <int MODE>
+__global__ void k_shape_cast(QueryCtx q, const float* casts, uint32_t n, uint32_t* counts, uint32_t* outIdx,
+	float* outHit, uint32_t capacity, uint32_t* outSingle)
+{
+	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const CastIn in = load_cast(casts, i);
+	const DevScene& S = q.S;
+	uint32_t k = MODE == 1 ? counts[i] : 0u;
+	uint32_t bestF = B3G_NULL, bestChild = B3G_NULL;
+	float bestT = B3G_MAX_SCALAR;
+	const V3 zero = V3{0.0f, 0.0f, 0.0f};
+	if (in.type != B3G_SHAPE_MESH)
+	{
+		const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
+		XF xf2 = in.xf;
+		xf2.p = in.xf.p + in.d;
+		AABB a1, a2;
+		compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, in.xf, xf2, true, a1, a2);
+		AABB sw;
+		sw.lo = vmin(a1.lo, a2.lo);
+		sw.hi = vmax(a1.hi, a2.hi);
+		auto overlap = [&](V3 lo, V3 hi) {
+			return !(hi.x < sw.lo.x || lo.x > sw.hi.x || hi.y < sw.lo.y || lo.y > sw.hi.y || hi.z < sw.lo.z ||
+				lo.z > sw.hi.z);
+		};
+		auto report = [&](uint32_t f, uint32_t child, float t, const XF& xfB, const GProxy& pB) {
+			if (MODE == 2)
+			{
+				if (t < bestT || (t == bestT && (f < bestF || (f == bestF && child < bestChild))))
+				{
+					bestT = t;
+					bestF = f;
+					bestChild = child;
+				}
+				return;
+			}
+			if (MODE == 1 && k < capacity)
+			{
+				XF xt;
+				xt.q = in.xf.q;
+				xt.p = in.xf.p + t * in.d;
+				V3 point, normal;
+				cast_evaluate(point, normal, xt, pA, xfB, pB);
+				uint32_t* o = outIdx + 3 * (size_t)k;
+				o[0] = i;
+				o[1] = f;
+				o[2] = child;
+				float* h = outHit + 7 * (size_t)k;
+				h[0] = point.x, h[1] = point.y, h[2] = point.z;
+				h[3] = normal.x, h[4] = normal.y, h[5] = normal.z;
+				h[6] = t;
+			}
+			++k;
+		};
+		lbvh_walk(q, overlap, [&](uint32_t f) {
+			float4 lo = q.fatLo[f], hi = q.fatHi[f];
+			if (!overlap(V3{lo.x, lo.y, lo.z}, V3{hi.x, hi.y, hi.z}) || !query_takes(q, f, in.world))
+				return;
+			const XF xfB = body_xf(S, S.fixBody[f]);
+			if (S.fixType[f] != B3G_SHAPE_MESH)
+			{
+				const GProxy pB = cast_proxy(S, S.fixType[f], S.fixParams[3 * f], S.fixParams[3 * f + 1],
+					S.fixParams[3 * f + 2], S.fixHull[f]);
+				TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, zero);
+				if (r.state == TOI_TOUCHING)
+					report(f, 0u, r.t, xfB, pB);
+				return;
+			}
+			// The swept box in the unscaled tree's frame.
+			const MeshDesc md = S.meshes[S.fixHull[f]];
+			const float4 sp = S.fixParams[3 * f];
+			const V3 inv = V3{1.0f / sp.x, 1.0f / sp.y, 1.0f / sp.z};
+			AABB m1, m2;
+			compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, xmult(xfB, in.xf), xmult(xfB, xf2), true,
+				m1, m2);
+			m1 = aabb_scaled(m1, inv);
+			m2 = aabb_scaled(m2, inv);
+			AABB box;
+			box.lo = vmin(m1.lo, m2.lo);
+			box.hi = vmax(m1.hi, m2.hi);
+			constexpr uint32_t STACK = 64;
+			uint32_t stack[STACK];
+			uint32_t sp_ = 0;
+			stack[sp_++] = md.root;
+			while (sp_ > 0)
+			{
+				uint32_t id = stack[--sp_];
+				if (id == B3G_NULL_NODE)
+					continue;
+				float4 nlo = S.meshNodes[2 * (size_t)(md.nOff + id)], nhi = S.meshNodes[2 * (size_t)(md.nOff + id) + 1];
+				if (nhi.x < box.lo.x || nlo.x > box.hi.x || nhi.y < box.lo.y || nlo.y > box.hi.y ||
+					nhi.z < box.lo.z || nlo.z > box.hi.z)
+					continue;
+				uint32_t child1 = __float_as_uint(nlo.w), other = __float_as_uint(nhi.w);
+				if (child1 == B3G_NULL_NODE)
+				{
+					const GProxy pB = mesh_triangle_proxy(S, f, other);
+					TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, zero);
+					if (r.state == TOI_TOUCHING)
+						report(f, other, r.t, xfB, pB);
+				}
+				else
+				{
+					if (sp_ + 2 > STACK)
+					{
+						atomicOr(q.status, B3G_ST_POLY_OVERFLOW);
+						return;
+					}
+					stack[sp_++] = child1;
+					stack[sp_++] = other;
+				}
+			}
+		});
+		if (MODE == 2 && bestF != B3G_NULL)
+		{
+			// b3World::ShapeCastSingle (world.cpp:828-848): evaluate the winner.
+			const XF xfB = body_xf(S, S.fixBody[bestF]);
+			const GProxy pB = S.fixType[bestF] == B3G_SHAPE_MESH
+				? mesh_triangle_proxy(S, bestF, bestChild)
+				: cast_proxy(S, S.fixType[bestF], S.fixParams[3 * bestF], S.fixParams[3 * bestF + 1],
+					  S.fixParams[3 * bestF + 2], S.fixHull[bestF]);
+			XF xt;
+			xt.q = in.xf.q;
+			xt.p = in.xf.p + bestT * in.d;
+			V3 point, normal;
+			cast_evaluate(point, normal, xt, pA, xfB, pB);
+			float* h = outHit + 7 * (size_t)i;
+			h[0] = point.x, h[1] = point.y, h[2] = point.z;
+			h[3] = normal.x, h[4] = normal.y, h[5] = normal.z;
+			h[6] = bestT;
+		}
+	}
+	if (MODE == 0)
+		counts[i] = k;
+	if (MODE == 2)
+	{
+		outSingle[2 * (size_t)i] = bestF;
+		outSingle[2 * (size_t)i + 1] = bestF != B3G_NULL ? bestChild : B3G_NULL;
+		if (bestF == B3G_NULL)
+		{
+			float* h = outHit + 7 * (size_t)i;
+			for (int e = 0; e < 7; ++e)
+				h[e] = 0.0f;
+		}
+	}
+}
+
 int qfail(b3g_ctx* c, int code, const char* msg)
 {
 	c->err = msg;
@@ -673,6 +981,100 @@ extern "C" int b3g_ray_cast_single_device(b3g_ctx* c, uint32_t n, const float* r
 	if (cudaGetLastError() != cudaSuccess)
 		return qfail(c, B3G_E_CUDA, "b3g_ray_cast_single_device: launch");
 	return B3G_OK;
+}
+
+// Host check of the casts: the shape types a cast may have and their hulls.
+static_assert(sizeof(b3g_shape_cast_input) == 112, "b3g_shape_cast_input: 28 words");
+
+static int cast_check(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input* casts)
+{
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const uint32_t t = casts[i].shape_type;
+		if (t > B3G_SHAPE_MESH)
+			return qfail(c, B3G_E_INVALID, "shape cast: unknown shape type");
+		if (t == B3G_SHAPE_HULL && casts[i].hull >= c->nHulls)
+			return qfail(c, B3G_E_INVALID, "shape cast: hull out of range");
+	}
+	return B3G_OK;
+}
+
+extern "C" int b3g_shape_cast(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* index,
+	float* hits, uint32_t capacity)
+{
+	if (!c || (n && (!casts || ((!index || !hits) && capacity))))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_shape_cast: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return 0;
+	int rc = cast_check(c, n, casts);
+	if (rc)
+		return rc;
+	QueryCtx q;
+	char* base;
+	const uint32_t* dWorlds;
+	const void* dIn;
+	const size_t cntBytes = ((4 * (size_t)n + 4 + 255) & ~(size_t)255);
+	const size_t idxBytes = ((12 * (size_t)capacity + 255) & ~(size_t)255);
+	rc = q_begin(c, n, casts, sizeof(b3g_shape_cast_input) * (size_t)n, nullptr, q,
+		cntBytes + idxBytes + 28 * (size_t)capacity + 256, base, dWorlds, dIn);
+	if (rc)
+		return rc;
+	uint32_t* counts = (uint32_t*)base;
+	uint32_t* dIdx = (uint32_t*)(base + cntBytes);
+	float* dHit = (float*)(base + cntBytes + idxBytes);
+	cudaStream_t s = c->stream;
+	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	const uint32_t blocks = (n + 127) / 128;
+	k_shape_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, n, counts, dIdx, dHit, capacity, nullptr);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	k_shape_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, n, counts, dIdx, dHit, capacity, nullptr);
+	uint32_t total = 0;
+	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_shape_cast: copy");
+	rc = q_status(c);
+	if (rc)
+		return rc;
+	uint32_t m = total < capacity ? total : capacity;
+	if (m && (cudaMemcpy(index, dIdx, 12 * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+				 cudaMemcpy(hits, dHit, 28 * (size_t)m, cudaMemcpyDeviceToHost) != cudaSuccess))
+		return qfail(c, B3G_E_CUDA, "b3g_shape_cast: copy");
+	return (int)total;
+}
+
+extern "C" int b3g_shape_cast_single(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* fixture,
+	float* hit)
+{
+	if (!c || (n && (!casts || !fixture || !hit)))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_shape_cast_single: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return 0;
+	int rc = cast_check(c, n, casts);
+	if (rc)
+		return rc;
+	QueryCtx q;
+	char* base;
+	const uint32_t* dWorlds;
+	const void* dIn;
+	const size_t fixBytes = ((8 * (size_t)n + 255) & ~(size_t)255);
+	rc = q_begin(c, n, casts, sizeof(b3g_shape_cast_input) * (size_t)n, nullptr, q, fixBytes + 28 * (size_t)n + 256,
+		base, dWorlds, dIn);
+	if (rc)
+		return rc;
+	uint32_t* dFix = (uint32_t*)base;
+	float* dHit = (float*)(base + fixBytes);
+	cudaStream_t s = c->stream;
+	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	k_shape_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, n, nullptr, nullptr, dHit, n, dFix);
+	rc = q_status(c);
+	if (rc)
+		return rc;
+	if (cudaMemcpy(fixture, dFix, 8 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+		cudaMemcpy(hit, dHit, 28 * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_shape_cast_single: copy");
+	int hits = 0;
+	for (uint32_t i = 0; i < n; ++i)
+		hits += fixture[2 * i] != B3G_NULL ? 1 : 0;
+	return hits;
 }
 
 void free_queries(b3g_ctx* c)

@@ -176,6 +176,30 @@ class CollisionPipeline:
         m = self._check(self.lib.b3g_fetch_fixture_contacts(self.ctx, N.ptr(offsets, u32), N.ptr(out, u32), len(out)))
         return offsets, out[:m]
 
+    def shape_cast(self, casts):
+        """b3World::ShapeCast keeping every hit, per cast (SHAPE_CAST_DTYPE):
+        (index (k, 3): cast, fixture, triangle; hits (k, 7): point, normal, fraction)."""
+        c = np.ascontiguousarray(casts, N.SHAPE_CAST_DTYPE)
+        cap = 64 * len(c) + 1024
+        while True:
+            idx = np.zeros((cap, 3), np.uint32)
+            hits = np.zeros((cap, 7), np.float32)
+            m = self._check(self.lib.b3g_shape_cast(self.ctx, len(c), ctypes.c_void_p(c.ctypes.data),
+                                                    N.ptr(idx, u32), N.ptr(hits, ctypes.c_float), cap))
+            if m <= cap:
+                return idx[:m], hits[:m]
+            cap = m
+
+    def shape_cast_single(self, casts):
+        """b3World::ShapeCastSingle per cast: (fixture and triangle (n, 2),
+        0xFFFFFFFF when none; hit (n, 7): point, normal, fraction)."""
+        c = np.ascontiguousarray(casts, N.SHAPE_CAST_DTYPE)
+        fix = np.zeros((max(len(c), 1), 2), np.uint32)
+        hit = np.zeros((max(len(c), 1), 7), np.float32)
+        self._check(self.lib.b3g_shape_cast_single(self.ctx, len(c), ctypes.c_void_p(c.ctypes.data),
+                                                   N.ptr(fix, u32), N.ptr(hit, ctypes.c_float)))
+        return fix[:len(c)], hit[:len(c)]
+
     def set_materials(self, friction, restitution):
         """Friction and restitution per fixture (b3Fixture::m_friction, m_restitution)."""
         fr = np.ascontiguousarray(friction, np.float32)

@@ -446,6 +446,41 @@ int b3g_ray_cast_single(b3g_ctx* ctx, uint32_t n, const float* rays, const uint3
 int b3g_ray_cast_single_device(b3g_ctx* ctx, uint32_t n, const float* rays, const uint32_t* worlds,
 	uint32_t* fixture, float* hit, void* stream);
 
+/* One shape cast: a convex shape (sphere, capsule, triangle or hull; params
+ * and hull as in b3g_set_fixtures) at a transform, swept along a
+ * displacement, in a world. A mesh cannot be cast (the reference returns
+ * without a hit, world.cpp:755-760); such casts report nothing. 112 bytes. */
+typedef struct b3g_shape_cast_input
+{
+	uint32_t shape_type;
+	uint32_t hull;
+	uint32_t world;
+	uint32_t pad;
+	float params[12];
+	float position[3]; /* b3Transform::translation */
+	float rotation[4]; /* b3Transform::rotation, xyzw */
+	float displacement[3];
+	float pad2[2];
+} b3g_shape_cast_input;
+
+/* b3World::ShapeCast (world.cpp:752-786) with a listener that returns 1 for
+ * every fixture: each fixture (each triangle of a mesh fixture) whose
+ * translational time of impact (b3TimeOfImpact, time_of_impact.cpp:666-776)
+ * reports touching. Writes (cast, fixture, triangle or 0) into index (3 u32
+ * per hit) and 7 floats per hit (point on the fixture and normal from b3GJK
+ * at the time of impact, world.cpp:719-731; fraction) up to capacity, and
+ * returns the number of hits. */
+int b3g_shape_cast(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* index, float* hits,
+	uint32_t capacity);
+
+/* b3World::ShapeCastSingle (world.cpp:788-851): per cast the hit with the
+ * smallest fraction: fixture and triangle (2 u32; 0xFFFFFFFF when none) and 7
+ * floats (point, normal, fraction). Of two hits at exactly the same fraction
+ * the smaller fixture, then triangle, is kept (the reference keeps the first
+ * its tree meets). Returns the number of casts that hit. */
+int b3g_shape_cast_single(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* fixture,
+	float* hit);
+
 /* Solver input -------------------------------------------------------------
  *
  * b3ContactSolver's constructor and InitializeVelocityConstraints

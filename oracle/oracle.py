@@ -103,6 +103,9 @@ def lib(precision=32):
         "refw_ray_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_ray_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
         "refw_ray_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
+        "refw_shape_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
+        "refw_shape_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
+        "refw_shape_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
         "ref_sizeof_dump_contact": ([], ctypes.c_uint32),
         "ref_sizeof_scalar": ([], ctypes.c_uint32),
         "ref_collide": (
@@ -321,6 +324,36 @@ class RefWorld:
         fix = np.zeros(max(len(r), 1), np.uint32)
         t = self.L.refw_ray_cast_single_batch(self.w, _p(r, ctypes.c_float), len(r), _p(fix, ctypes.c_uint32))
         return fix[:len(r)], t
+
+    def shape_cast(self, cast):
+        """b3World::ShapeCast keeping every hit; cast is 28 float32 words in
+        the b3g_shape_cast_input layout: (fixtures, hits (k, 7): point, normal,
+        fraction)."""
+        c = np.ascontiguousarray(cast, np.float32).reshape(28)
+        cap = 4 * self.scene.n_fixtures + 64
+        fix = np.zeros(cap, np.uint32)
+        hit = np.zeros((cap, 7), np.float64)
+        n = self.L.refw_shape_cast(self.w, _p(c, ctypes.c_float), _p(fix, ctypes.c_uint32),
+                                   hit.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap)
+        assert n <= cap
+        return fix[:n], hit[:n]
+
+    def shape_cast_single(self, cast):
+        """b3World::ShapeCastSingle: (fixture, hit (7,)) or (None, None)."""
+        c = np.ascontiguousarray(cast, np.float32).reshape(28)
+        fix = np.zeros(1, np.uint32)
+        hit = np.zeros(7, np.float64)
+        if not self.L.refw_shape_cast_single(self.w, _p(c, ctypes.c_float), _p(fix, ctypes.c_uint32),
+                                             hit.ctypes.data_as(ctypes.POINTER(ctypes.c_double))):
+            return None, None
+        return int(fix[0]), hit
+
+    def shape_cast_single_batch(self, casts):
+        """ShapeCastSingle for each cast, timed inside the harness: (fixtures, seconds)."""
+        c = np.ascontiguousarray(casts, np.float32).reshape(-1, 28)
+        fix = np.zeros(max(len(c), 1), np.uint32)
+        t = self.L.refw_shape_cast_single_batch(self.w, _p(c, ctypes.c_float), len(c), _p(fix, ctypes.c_uint32))
+        return fix[:len(c)], t
 
     def load_impulses(self, normal, tangent, motor):
         """The solver's impulses for every contact in list order, per manifold

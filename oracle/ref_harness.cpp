@@ -958,6 +958,101 @@ REF_API double refw_ray_cast_single_batch(void* p, const float* rays, uint32_t n
 	return Now() - t0;
 }
 
+// Shape casts through b3World::ShapeCast / ShapeCastSingle. A cast is 28
+// words in the b3g_shape_cast_input layout: type, hull, world, pad,
+// params[12], position[3], rotation[4], displacement[3], pad[2].
+struct CastAll : b3ShapeCastListener, b3ShapeCastFilter
+{
+	std::vector<uint32_t> fix;
+	std::vector<double> hit;
+	scalar ReportFixture(b3Fixture* f, const b3Vec3& point, const b3Vec3& normal, scalar fraction) override
+	{
+		fix.push_back((uint32_t)(uintptr_t)f->GetUserData());
+		double h[7] = {(double)point.x, (double)point.y, (double)point.z, (double)normal.x, (double)normal.y,
+			(double)normal.z, (double)fraction};
+		hit.insert(hit.end(), h, h + 7);
+		return scalar(1);
+	}
+	bool ShouldShapeCast(b3Fixture*) override { return true; }
+};
+
+static const b3Shape* CastShape(ShapeStore& store, const RefWorld* w, const float* cast)
+{
+	uint32_t type, hull;
+	memcpy(&type, cast, 4);
+	memcpy(&hull, cast + 1, 4);
+	return MakeShape(store, type, cast + 4, hull, w->pool);
+}
+
+static b3Transform CastXf(const float* cast)
+{
+	b3Transform xf;
+	xf.translation.Set(cast[16], cast[17], cast[18]);
+	xf.rotation.v.Set(cast[19], cast[20], cast[21]);
+	xf.rotation.s = cast[22];
+	return xf;
+}
+
+// b3World::ShapeCast with a listener that returns 1 (keeps every hit): up to
+// cap hits as fixture + (point, normal, fraction); returns the hit count.
+REF_API uint32_t refw_shape_cast(void* p, const float* cast, uint32_t* fix, double* hit, uint32_t cap)
+{
+	RefWorld* w = (RefWorld*)p;
+	ShapeStore store;
+	const b3Shape* shape = CastShape(store, w, cast);
+	CastAll all;
+	w->world->ShapeCast(&all, &all, shape, CastXf(cast), b3Vec3(cast[23], cast[24], cast[25]));
+	uint32_t n = (uint32_t)all.fix.size();
+	for (uint32_t i = 0; i < n && i < cap; ++i)
+	{
+		fix[i] = all.fix[i];
+		for (int k = 0; k < 7; ++k)
+			hit[7 * i + k] = all.hit[7 * i + k];
+	}
+	return n;
+}
+
+// b3World::ShapeCastSingle: 1 and the closest hit, or 0.
+REF_API uint32_t refw_shape_cast_single(void* p, const float* cast, uint32_t* fix, double* hit)
+{
+	RefWorld* w = (RefWorld*)p;
+	ShapeStore store;
+	const b3Shape* shape = CastShape(store, w, cast);
+	CastAll filter;
+	b3ShapeCastSingleOutput o;
+	if (!w->world->ShapeCastSingle(&o, &filter, shape, CastXf(cast), b3Vec3(cast[23], cast[24], cast[25])))
+		return 0;
+	*fix = (uint32_t)(uintptr_t)o.fixture->GetUserData();
+	double h[7] = {(double)o.point.x, (double)o.point.y, (double)o.point.z, (double)o.normal.x, (double)o.normal.y,
+		(double)o.normal.z, (double)o.fraction};
+	for (int k = 0; k < 7; ++k)
+		hit[k] = h[k];
+	return 1;
+}
+
+// Timed batch of b3World::ShapeCastSingle calls (the CPU baseline of the
+// shape cast bench): writes each cast's fixture (or 0xFFFFFFFF) and returns
+// the seconds spent in the calls.
+REF_API double refw_shape_cast_single_batch(void* p, const float* casts, uint32_t n, uint32_t* fix)
+{
+	RefWorld* w = (RefWorld*)p;
+	std::vector<ShapeStore> stores(n);
+	std::vector<const b3Shape*> shapes(n);
+	for (uint32_t i = 0; i < n; ++i)
+		shapes[i] = CastShape(stores[i], w, casts + 28 * (size_t)i);
+	CastAll filter;
+	double t0 = Now();
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* c = casts + 28 * (size_t)i;
+		b3ShapeCastSingleOutput o;
+		fix[i] = w->world->ShapeCastSingle(&o, &filter, shapes[i], CastXf(c), b3Vec3(c[23], c[24], c[25]))
+			? (uint32_t)(uintptr_t)o.fixture->GetUserData()
+			: 0xFFFFFFFFu;
+	}
+	return Now() - t0;
+}
+
 // Layout of b3ManifoldPoint / b3Manifold (collision.h:97-128) for checking the
 // device records: sizes and field offsets.
 REF_API void ref_manifold_layout(uint32_t* out)
