@@ -14,8 +14,9 @@ through the C ABI with host buffers (host->device copy of the pinned state,
 device->host contact list and packed touching manifolds every step, the
 copies of one step overlapping the next step's pass). Other workloads:
 --workload pile (hull pile over a mesh), batched (1,024 worlds), serving
-(request stream), queries (ray casts) and constraints (the solver's contact
-constraints built from the pass's manifolds). The reference arm
+(request stream), queries (ray casts), shapecast (shape casts) and
+constraints (the solver's contact constraints built from the pass's
+manifolds). The reference arm
 (--impl reference) runs the reference's own CPU pipeline (oracle/_ref, the
 unmodified Bounce sources) on the same scene and body motion.
 
@@ -62,7 +63,7 @@ def parse():
                     help="passes after the timed ones, with per-stage CUDA events (not part of value)")
     ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
     ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving", "queries",
-                                                             "constraints"])
+                                                             "constraints", "shapecast"])
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000",
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
@@ -244,6 +245,20 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
 
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
+        return
+    if args.workload == "shapecast":
+        scene, walls = workload_scene(args, SEED)
+        casts = make_casts(scene, SEED + 300, CAST_CPU_COUNT, scene_half(scene))
+        _, _, t = cast_reference(scene, walls, casts)
+        v = len(casts) / t
+        print(json.dumps({
+            "metric": "shape casts/s", "value": v, "unit": "casts/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+            "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": CAST_WORKLOAD, "casts_per_step": len(casts)},
+            "cpu_baseline": {"value": v, "unit": "casts/s", "cores": 1, "kind": "reference",
+                             "sample": f"{len(casts)} casts through b3World::ShapeCastSingle on 1 host core"},
+            "e2e": {"value": v, "unit": "casts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     if args.workload == "constraints":
         scene, walls = workload_scene(args, SEED)
@@ -916,6 +931,175 @@ def run_queries(args, rank, world, local, dist):
     pipe.close()
 
 
+CAST_COUNT = 1 << 17
+CAST_CPU_COUNT = 1 << 13
+CAST_WORKLOAD = ("b3World::ShapeCastSingle over the 65,536-body mixed world after 3 collision passes: the world's "
+                 "own sphere, capsule and hull shapes at uniform positions in the body cube and uniform rotations, "
+                 "swept 1-4 m in uniform directions")
+
+
+def make_casts(scene, seed, n, half):
+    """Seeded shape casts of the scene's own convex shapes (b3g_shape_cast_input records)."""
+    from bounce_b200 import _native as N
+
+    rng = np.random.default_rng(seed)
+    params = scene.fix_params.reshape(-1, 12)
+    pool = np.nonzero(np.isin(scene.fix_type, [0, 1, 3]))[0]
+    pick = rng.choice(pool, n)
+    c = np.zeros(n, N.SHAPE_CAST_DTYPE)
+    c["type"] = scene.fix_type[pick]
+    c["hull"] = np.where(scene.fix_type[pick] == 3, scene.fix_hull[pick], 0)
+    c["params"] = params[pick]
+    c["position"] = rng.uniform(-half, half, (n, 3))
+    q = rng.normal(size=(n, 4))
+    c["rotation"] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    c["displacement"] = d * rng.uniform(1.0, 4.0, (n, 1))
+    return c
+
+
+def cast_reference(scene, walls, casts):
+    """The reference's ShapeCastSingle on the same world after the same 3
+    passes: (fixtures, seconds) on 1 host core."""
+    from bounce_b200 import scene as S
+    from oracle import oracle as O
+
+    rw = O.RefWorld(scene)
+    scene.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(scene, walls=walls)
+    rw.first_pass()
+    for _ in range(2):
+        drv.advance()
+        rw.set_sweeps(drv.sweeps14())
+        rw.step_pass()
+    fix, frac, t = rw.shape_cast_single_batch(casts.view(np.float32).reshape(-1, 28))
+    rw.close()
+    return fix, frac, t
+
+
+def run_shapecast(args, rank, world, local, dist):
+    import ctypes
+
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+    from bounce_b200 import scene as S
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    scene, walls = workload_scene(args, SEED + rank)
+    drv = S.KinematicDriver(scene, walls=walls)
+    nb = scene.n_bodies
+    pipe = CollisionPipeline(scene, max_contacts=max(2_000_000, 40 * nb), device=local)
+    for k in range(3):
+        if k:
+            drv.advance()
+        pipe.collide(drv.state17())
+    assert pipe.counts()["status"] == 0
+    n = CAST_COUNT
+    casts = make_casts(scene, SEED + 300 + rank, n, scene_half(scene))
+    d_casts = torch.from_numpy(casts.view(np.uint8).copy()).to(dev)
+    d_fix = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    d_hit = torch.empty((n, 7), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    lib = pipe.lib
+
+    def cast():
+        pipe._check(lib.b3g_shape_cast_single_device(pipe.ctx, n, ctypes.c_void_p(d_casts.data_ptr()),
+                                                      ctypes.c_void_p(d_fix.data_ptr()),
+                                                      ctypes.c_void_p(d_hit.data_ptr()), sptr))
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            cast()
+    stream.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flushed between steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cast()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    hits = int((d_fix[:, 0] != -1).sum().item())
+    secs, work = replica_totals(dist, dev, ms / 1000.0, n * args.steps)
+    value = work / secs
+
+    # e2e: the host-buffer entry point (casts copied in, results copied out).
+    e2e_steps = max(1, min(args.e2e_steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fix_h, hit_h = pipe.shape_cast_single(casts)
+    e2e_s, e2e_work = replica_totals(dist, dev, time.perf_counter() - t0, n * e2e_steps)
+    e2e_value = e2e_work / e2e_s
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    algo = n * (112 + 8 + 28)
+    achieved = algo / (ms / args.steps / 1000.0) / 1e9
+    roof = {"kernel": "k_shape_cast<2> (ShapeCastSingle)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "algorithmic_bytes_per_launch": algo,
+            "note": "casts in (112 B) and results out (36 B) per cast; the tree walk and the GJK iterations of "
+                    "each candidate's time of impact are latency and compute bound",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref_scene, ref_walls = workload_scene(args, SEED)
+            sample = casts[:CAST_CPU_COUNT]
+            rfix, rfrac, rt = cast_reference(ref_scene, ref_walls, sample)
+            k = CAST_CPU_COUNT
+            cpu = {"value": len(sample) / rt, "unit": "casts/s", "cores": 1, "kind": "reference",
+                   "sample": f"{len(sample)} of the step's casts through b3World::ShapeCastSingle on 1 host core",
+                   "same_fraction_as_gpu": float(np.mean(rfrac == hit_h[:k, 6])),
+                   "same_fixture_as_gpu": float(np.mean(rfix == fix_h[:k, 0])),
+                   "note": "fixtures differ where several hits share the smallest fraction exactly (most often "
+                           "0, casts that start touching several bodies): the reference keeps the first its "
+                           "tree meets, the device the smallest fixture index"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "casts/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "shape casts/s", "value": value, "unit": "casts/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": CAST_WORKLOAD, "casts_per_step": n, "bodies": nb, "hit_fraction": hits / n,
+                       "l2": "flushed between steps (256 MB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "casts/s", "h2d_bytes_per_step": 112 * n,
+                    "d2h_bytes_per_step": 36 * n, "steps": e2e_steps},
+            "gpu_launches": args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    pipe.close()
+
+
 CONSTRAINT_WORKLOAD = ("b3ContactSolver constructor + InitializeVelocityConstraints over the 65,536-body mixed "
                        "world after 3 collision passes: every touching non-sensor contact, seeded body velocities "
                        "N(0, 1), inverse masses 1/U(0.5, 5) kg, world inverse inertias R diag(1/U(0.05, 2)) R^T, "
@@ -1117,6 +1301,8 @@ def main():
             run_queries(args, rank, world, local, dist)
         elif args.workload == "constraints":
             run_constraints(args, rank, world, local, dist)
+        elif args.workload == "shapecast":
+            run_shapecast(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

@@ -213,6 +213,7 @@ EXPORTED = [
     "b3g_ray_cast_single_device",
     "b3g_shape_cast",
     "b3g_shape_cast_single",
+    "b3g_shape_cast_single_device",
     "b3g_set_materials",
     "b3g_contact_constraints",
     "b3g_contact_constraints_device",
@@ -292,6 +293,7 @@ def load():
         "b3g_ray_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp, vp], ctypes.c_int),
         "b3g_shape_cast": ([ctx, ctypes.c_uint32, vp, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_shape_cast_single": ([ctx, ctypes.c_uint32, vp, u32p, f32p], ctypes.c_int),
+        "b3g_shape_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp], ctypes.c_int),
         "b3g_set_materials": ([ctx, f32p, f32p], ctypes.c_int),
         "b3g_contact_constraints": ([ctx, ctypes.c_uint32, u32p, vp, ctypes.c_float, ctypes.c_int, vp,
                                      ctypes.c_uint32, vp, ctypes.c_uint32, u32p], ctypes.c_int),

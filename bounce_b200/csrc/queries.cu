@@ -497,7 +497,8 @@ struct TOIOut
 // b3TimeOfImpact(xf1, proxy1, d1, xf2, proxy2, d2) (time_of_impact.cpp:666-776):
 // Mirtich's conservative advancement along the translations, the GJK simplex
 // carried from one iteration to the next, at most 20 iterations.
-__device__ TOIOut toi_translate(const XF& xf1, const GProxy& p1, V3 d1, const XF& xf2, const GProxy& p2, V3 d2)
+__device__ __noinline__ TOIOut toi_translate(const XF& xf1, const GProxy& p1, V3 d1, const XF& xf2, const GProxy& p2,
+	V3 d2)
 {
 	const float totalRadius = p1.radius + p2.radius;
 	const float target = fmaxr(B3G_LINEAR_SLOP, totalRadius - 3.0f * B3G_LINEAR_SLOP);
@@ -592,7 +593,8 @@ __device__ GProxy mesh_triangle_proxy(const DevScene& S, uint32_t fix, uint32_t 
 }
 
 // b3WorldShapeCastQueryWrapper::Evaluate (world.cpp:719-731).
-__device__ void cast_evaluate(V3& point, V3& normal, const XF& xA, const GProxy& pA, const XF& xB, const GProxy& pB)
+__device__ __noinline__ void cast_evaluate(V3& point, V3& normal, const XF& xA, const GProxy& pA, const XF& xB,
+	const GProxy& pB)
 {
 	GJKOut q = gjk(xA, pA, xB, pB, false);
 	normal = normalized(q.point1 - q.point2);
@@ -625,159 +627,326 @@ __device__ __forceinline__ CastIn load_cast(const float* in, uint32_t i)
 	return c;
 }
 
+// The cast's end transform and swept AABB (world.cpp:759-768).
+__device__ __forceinline__ AABB cast_sweep(const DevScene& S, const CastIn& in, XF& xf2)
+{
+	xf2 = in.xf;
+	xf2.p = in.xf.p + in.d;
+	AABB a1, a2;
+	compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, in.xf, xf2, true, a1, a2);
+	AABB sw;
+	sw.lo = vmin(a1.lo, a2.lo);
+	sw.hi = vmax(a1.hi, a2.hi);
+	return sw;
+}
+
+__device__ __forceinline__ bool box_overlap(const AABB& b, float4 lo, float4 hi)
+{
+	return !(hi.x < b.lo.x || lo.x > b.hi.x || hi.y < b.lo.y || lo.y > b.hi.y || hi.z < b.lo.z || lo.z > b.hi.z);
+}
+
+// Mesh fixture f against cast `in`: the triangles under the swept box in the
+// unscaled mesh frame (world.cpp:638-664), in the static tree's depth-first
+// order; visit(triangle, toi, proxy) for each touching one.
+template <class Visit>
+__device__ __forceinline__ void cast_mesh(const QueryCtx& q, const CastIn& in, const GProxy& pA, const XF& xf2,
+	uint32_t f, const XF& xfB, Visit&& visit)
+{
+	const DevScene& S = q.S;
+	const MeshDesc md = S.meshes[S.fixHull[f]];
+	const float4 sp = S.fixParams[3 * f];
+	const V3 inv = V3{1.0f / sp.x, 1.0f / sp.y, 1.0f / sp.z};
+	AABB m1, m2;
+	compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, xmult(xfB, in.xf), xmult(xfB, xf2), true, m1, m2);
+	m1 = aabb_scaled(m1, inv);
+	m2 = aabb_scaled(m2, inv);
+	AABB box;
+	box.lo = vmin(m1.lo, m2.lo);
+	box.hi = vmax(m1.hi, m2.hi);
+	const V3 zero = V3{0.0f, 0.0f, 0.0f};
+	constexpr uint32_t STACK = 64;
+	uint32_t stack[STACK];
+	uint32_t sp_ = 0;
+	stack[sp_++] = md.root;
+	while (sp_ > 0)
+	{
+		uint32_t id = stack[--sp_];
+		if (id == B3G_NULL_NODE)
+			continue;
+		float4 nlo = S.meshNodes[2 * (size_t)(md.nOff + id)], nhi = S.meshNodes[2 * (size_t)(md.nOff + id) + 1];
+		if (!box_overlap(box, nlo, nhi))
+			continue;
+		uint32_t child1 = __float_as_uint(nlo.w), other = __float_as_uint(nhi.w);
+		if (child1 == B3G_NULL_NODE)
+		{
+			const GProxy pB = mesh_triangle_proxy(S, f, other);
+			TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, zero);
+			if (r.state == TOI_TOUCHING)
+				visit(other, r.t, pB);
+		}
+		else
+		{
+			if (sp_ + 2 > STACK)
+			{
+				atomicOr(q.status, B3G_ST_POLY_OVERFLOW);
+				return;
+			}
+			stack[sp_++] = child1;
+			stack[sp_++] = other;
+		}
+	}
+}
+
+// One (cast, fixture) candidate on one lane: the time of impact against a
+// convex fixture, or against each triangle of a mesh fixture. MODE 0 counts
+// the touching results in *count, MODE 1 writes them (slot base + a count
+// taken from *count), MODE 2 lowers *best to (fraction bits, fixture).
+template <int MODE>
+__device__ __noinline__ void cast_candidate(const QueryCtx& q, const float* casts, uint32_t i, uint32_t f,
+	uint32_t* count, uint32_t base, uint32_t* outIdx, float* outHit, uint32_t capacity, unsigned long long* best)
+{
+	const DevScene& S = q.S;
+	const CastIn in = load_cast(casts, i);
+	const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
+	const XF xfB = body_xf(S, S.fixBody[f]);
+	auto act = [&](uint32_t child, float t, const GProxy& pB) {
+		if (MODE == 2)
+		{
+			atomicMin(best, ((unsigned long long)__float_as_uint(t) << 32) | f);
+			return;
+		}
+		const uint32_t slot = atomicAdd(count, 1u);
+		if (MODE == 1 && base + slot < capacity)
+		{
+			XF xt;
+			xt.q = in.xf.q;
+			xt.p = in.xf.p + t * in.d;
+			V3 point, normal;
+			cast_evaluate(point, normal, xt, pA, xfB, pB);
+			uint32_t* o = outIdx + 3 * (size_t)(base + slot);
+			o[0] = i;
+			o[1] = f;
+			o[2] = child;
+			float* h = outHit + 7 * (size_t)(base + slot);
+			h[0] = point.x, h[1] = point.y, h[2] = point.z;
+			h[3] = normal.x, h[4] = normal.y, h[5] = normal.z;
+			h[6] = t;
+		}
+	};
+	if (S.fixType[f] != B3G_SHAPE_MESH)
+	{
+		const GProxy pB =
+			cast_proxy(S, S.fixType[f], S.fixParams[3 * f], S.fixParams[3 * f + 1], S.fixParams[3 * f + 2], S.fixHull[f]);
+		TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, V3{0.0f, 0.0f, 0.0f});
+		if (r.state == TOI_TOUCHING)
+			act(0u, r.t, pB);
+		return;
+	}
+	XF xf2;
+	cast_sweep(S, in, xf2);
+	cast_mesh(q, in, pA, xf2, f, xfB, act);
+}
+
 // b3World::ShapeCast with a listener that returns 1 for every fixture
 // (MODE 0 counts, MODE 1 writes (cast, fixture, triangle) + (point, normal,
-// fraction)) and b3World::ShapeCastSingle (MODE 2: the smallest fraction,
-// then the smaller fixture and triangle on an exact tie). Mesh fixtures are
-// tested triangle by triangle over their static tree, with the swept box in
-// the unscaled mesh frame (world.cpp:638-664).
+// fraction), in no particular order within a cast) and
+// b3World::ShapeCastSingle (MODE 2: the smallest fraction, then the smaller
+// fixture and triangle on an exact tie).
+//
+// A warp holds 32 casts. Its lanes walk their casts' LBVH paths only until
+// each finds its next candidate fixture (fat AABB overlapping the swept box)
+// and push it into the warp's queue in shared memory; whenever 32 candidates
+// are queued (or the walks are over) every lane takes one and runs its time
+// of impact, so the lanes run the same GJK code on different candidates
+// instead of each walking and testing its own cast alone. Per-cast results
+// meet in shared memory (counts, or the smallest (fraction, fixture) key).
 template <int MODE>
-__global__ void k_shape_cast(QueryCtx q, const float* casts, uint32_t n, uint32_t* counts, uint32_t* outIdx,
-	float* outHit, uint32_t capacity, uint32_t* outSingle)
+__global__ void __launch_bounds__(128) k_shape_cast(QueryCtx q, const float* casts, const uint32_t* order, uint32_t n,
+	uint32_t* counts, uint32_t* outIdx, float* outHit, uint32_t capacity, uint32_t* outSingle)
 {
-	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n)
-		return;
-	const CastIn in = load_cast(casts, i);
+	constexpr int WARPS = 4;
+	__shared__ uint32_t qLane[WARPS][64], qFix[WARPS][64];
+	__shared__ uint32_t sCount[WARPS][32];
+	__shared__ unsigned long long sBest[WARPS][32];
+	const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+	const uint32_t warpBase = blockIdx.x * blockDim.x + w * 32u;
+	const uint32_t t = warpBase + lane;
+	const bool active = t < n;
+	// Casts are taken in the order of their Morton keys, so the lanes of a
+	// warp walk neighbouring parts of the tree; results go to their own slots.
+	const uint32_t i = active ? (order ? order[t] : t) : 0u;
+	sCount[w][lane] = 0;
+	sBest[w][lane] = ~0ull;
+	__syncwarp();
 	const DevScene& S = q.S;
-	uint32_t k = MODE == 1 ? counts[i] : 0u;
-	uint32_t bestF = B3G_NULL, bestChild = B3G_NULL;
-	float bestT = B3G_MAX_SCALAR;
-	const V3 zero = V3{0.0f, 0.0f, 0.0f};
-	if (in.type != B3G_SHAPE_MESH)
+	bool walking = false;
+	uint32_t world = 0;
+	AABB sw;
+	sw.lo = sw.hi = V3{0.0f, 0.0f, 0.0f};
+	if (active)
 	{
-		const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
-		XF xf2 = in.xf;
-		xf2.p = in.xf.p + in.d;
-		AABB a1, a2;
-		compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, in.xf, xf2, true, a1, a2);
-		AABB sw;
-		sw.lo = vmin(a1.lo, a2.lo);
-		sw.hi = vmax(a1.hi, a2.hi);
-		auto overlap = [&](V3 lo, V3 hi) {
-			return !(hi.x < sw.lo.x || lo.x > sw.hi.x || hi.y < sw.lo.y || lo.y > sw.hi.y || hi.z < sw.lo.z ||
-				lo.z > sw.hi.z);
-		};
-		auto report = [&](uint32_t f, uint32_t child, float t, const XF& xfB, const GProxy& pB) {
-			if (MODE == 2)
-			{
-				if (t < bestT || (t == bestT && (f < bestF || (f == bestF && child < bestChild))))
-				{
-					bestT = t;
-					bestF = f;
-					bestChild = child;
-				}
-				return;
-			}
-			if (MODE == 1 && k < capacity)
-			{
-				XF xt;
-				xt.q = in.xf.q;
-				xt.p = in.xf.p + t * in.d;
-				V3 point, normal;
-				cast_evaluate(point, normal, xt, pA, xfB, pB);
-				uint32_t* o = outIdx + 3 * (size_t)k;
-				o[0] = i;
-				o[1] = f;
-				o[2] = child;
-				float* h = outHit + 7 * (size_t)k;
-				h[0] = point.x, h[1] = point.y, h[2] = point.z;
-				h[3] = normal.x, h[4] = normal.y, h[5] = normal.z;
-				h[6] = t;
-			}
-			++k;
-		};
-		lbvh_walk(q, overlap, [&](uint32_t f) {
-			float4 lo = q.fatLo[f], hi = q.fatHi[f];
-			if (!overlap(V3{lo.x, lo.y, lo.z}, V3{hi.x, hi.y, hi.z}) || !query_takes(q, f, in.world))
-				return;
-			const XF xfB = body_xf(S, S.fixBody[f]);
-			if (S.fixType[f] != B3G_SHAPE_MESH)
-			{
-				const GProxy pB = cast_proxy(S, S.fixType[f], S.fixParams[3 * f], S.fixParams[3 * f + 1],
-					S.fixParams[3 * f + 2], S.fixHull[f]);
-				TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, zero);
-				if (r.state == TOI_TOUCHING)
-					report(f, 0u, r.t, xfB, pB);
-				return;
-			}
-			// The swept box in the unscaled tree's frame.
-			const MeshDesc md = S.meshes[S.fixHull[f]];
-			const float4 sp = S.fixParams[3 * f];
-			const V3 inv = V3{1.0f / sp.x, 1.0f / sp.y, 1.0f / sp.z};
-			AABB m1, m2;
-			compute_shape_aabbs(S, in.type, in.p0, in.p1, in.p2, in.hull, xmult(xfB, in.xf), xmult(xfB, xf2), true,
-				m1, m2);
-			m1 = aabb_scaled(m1, inv);
-			m2 = aabb_scaled(m2, inv);
-			AABB box;
-			box.lo = vmin(m1.lo, m2.lo);
-			box.hi = vmax(m1.hi, m2.hi);
-			constexpr uint32_t STACK = 64;
-			uint32_t stack[STACK];
-			uint32_t sp_ = 0;
-			stack[sp_++] = md.root;
-			while (sp_ > 0)
-			{
-				uint32_t id = stack[--sp_];
-				if (id == B3G_NULL_NODE)
-					continue;
-				float4 nlo = S.meshNodes[2 * (size_t)(md.nOff + id)], nhi = S.meshNodes[2 * (size_t)(md.nOff + id) + 1];
-				if (nhi.x < box.lo.x || nlo.x > box.hi.x || nhi.y < box.lo.y || nlo.y > box.hi.y ||
-					nhi.z < box.lo.z || nlo.z > box.hi.z)
-					continue;
-				uint32_t child1 = __float_as_uint(nlo.w), other = __float_as_uint(nhi.w);
-				if (child1 == B3G_NULL_NODE)
-				{
-					const GProxy pB = mesh_triangle_proxy(S, f, other);
-					TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, zero);
-					if (r.state == TOI_TOUCHING)
-						report(f, other, r.t, xfB, pB);
-				}
-				else
-				{
-					if (sp_ + 2 > STACK)
-					{
-						atomicOr(q.status, B3G_ST_POLY_OVERFLOW);
-						return;
-					}
-					stack[sp_++] = child1;
-					stack[sp_++] = other;
-				}
-			}
-		});
-		if (MODE == 2 && bestF != B3G_NULL)
+		const CastIn in = load_cast(casts, i);
+		// A mesh cannot be cast (world.cpp:755-760).
+		walking = in.type != B3G_SHAPE_MESH;
+		world = in.world;
+		XF xf2;
+		sw = cast_sweep(S, in, xf2);
+	}
+	const uint32_t nodes = 2u * q.leaves - 1u;
+	uint32_t node = 0, steps = 0, qn = 0;
+	for (;;)
+	{
+		uint32_t f = 0;
+		bool got = false;
+		while (walking && node != SENT)
 		{
-			// b3World::ShapeCastSingle (world.cpp:828-848): evaluate the winner.
+			if (++steps > nodes + 1u || node >= nodes)
+			{
+				atomicOr(q.status, B3G_ST_WAIT_TIMEOUT);
+				node = SENT;
+				break;
+			}
+			const float4 lo = q.nodeLo[node], hi = q.nodeHi[node];
+			const bool pass = box_overlap(sw, lo, hi);
+			if (pass && node < q.leaves - 1u)
+			{
+				node = __float_as_uint(lo.w);
+				continue;
+			}
+			node = __float_as_uint(hi.w);
+			if (pass)
+			{
+				const uint32_t proxy = __float_as_uint(lo.w);
+				if (box_overlap(sw, q.fatLo[proxy], q.fatHi[proxy]) && query_takes(q, proxy, world))
+				{
+					f = proxy;
+					got = true;
+					break;
+				}
+			}
+		}
+		if (!got)
+			walking = false;
+		const uint32_t m = __ballot_sync(0xFFFFFFFFu, got);
+		if (got)
+		{
+			const uint32_t pos = qn + __popc(m & ((1u << lane) - 1u));
+			qLane[w][pos] = lane;
+			qFix[w][pos] = f;
+		}
+		qn += __popc(m);
+		const bool more = __any_sync(0xFFFFFFFFu, walking);
+		if (qn >= 32u || (!more && qn > 0u))
+		{
+			__syncwarp();
+			const uint32_t take = min(qn, 32u);
+			if (lane < take)
+			{
+				const uint32_t e = qn - take + lane;
+				const uint32_t cl = qLane[w][e];
+				const uint32_t ci = order ? order[warpBase + cl] : warpBase + cl;
+				cast_candidate<MODE>(q, casts, ci, qFix[w][e], &sCount[w][cl], MODE == 1 ? counts[ci] : 0u, outIdx,
+					outHit, capacity, &sBest[w][cl]);
+			}
+			qn -= take;
+			__syncwarp();
+		}
+		if (!more && qn == 0u)
+			break;
+	}
+	__syncwarp();
+	if (!active)
+		return;
+	if (MODE == 0)
+		counts[i] = sCount[w][lane];
+	if (MODE == 2)
+	{
+		const unsigned long long key = sBest[w][lane];
+		uint32_t bestF = B3G_NULL, bestChild = B3G_NULL;
+		float* h = outHit + 7 * (size_t)i;
+		if (key != ~0ull)
+		{
+			bestF = (uint32_t)(key & 0xFFFFFFFFull);
+			const float bestT = __uint_as_float((uint32_t)(key >> 32));
+			const CastIn in = load_cast(casts, i);
+			const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
 			const XF xfB = body_xf(S, S.fixBody[bestF]);
-			const GProxy pB = S.fixType[bestF] == B3G_SHAPE_MESH
-				? mesh_triangle_proxy(S, bestF, bestChild)
-				: cast_proxy(S, S.fixType[bestF], S.fixParams[3 * bestF], S.fixParams[3 * bestF + 1],
-					  S.fixParams[3 * bestF + 2], S.fixHull[bestF]);
+			GProxy pB;
+			pB.gv = nullptr;
+			pB.lv[0] = pB.lv[1] = pB.lv[2] = V3{0.0f, 0.0f, 0.0f};
+			pB.count = 1;
+			pB.radius = 0.0f;
+			if (S.fixType[bestF] == B3G_SHAPE_MESH)
+			{
+				// The winning mesh's smallest triangle at that fraction.
+				XF xf2;
+				cast_sweep(S, in, xf2);
+				cast_mesh(q, in, pA, xf2, bestF, xfB, [&](uint32_t tri, float tt, const GProxy& pt) {
+					if (tt == bestT && tri < bestChild)
+					{
+						bestChild = tri;
+						pB = pt;
+					}
+				});
+			}
+			else
+			{
+				bestChild = 0;
+				pB = cast_proxy(S, S.fixType[bestF], S.fixParams[3 * bestF], S.fixParams[3 * bestF + 1],
+					S.fixParams[3 * bestF + 2], S.fixHull[bestF]);
+			}
+			// b3World::ShapeCastSingle (world.cpp:828-848): evaluate the winner.
 			XF xt;
 			xt.q = in.xf.q;
 			xt.p = in.xf.p + bestT * in.d;
 			V3 point, normal;
 			cast_evaluate(point, normal, xt, pA, xfB, pB);
-			float* h = outHit + 7 * (size_t)i;
 			h[0] = point.x, h[1] = point.y, h[2] = point.z;
 			h[3] = normal.x, h[4] = normal.y, h[5] = normal.z;
 			h[6] = bestT;
 		}
-	}
-	if (MODE == 0)
-		counts[i] = k;
-	if (MODE == 2)
-	{
-		outSingle[2 * (size_t)i] = bestF;
-		outSingle[2 * (size_t)i + 1] = bestF != B3G_NULL ? bestChild : B3G_NULL;
-		if (bestF == B3G_NULL)
+		else
 		{
-			float* h = outHit + 7 * (size_t)i;
 			for (int e = 0; e < 7; ++e)
 				h[e] = 0.0f;
 		}
+		outSingle[2 * (size_t)i] = bestF;
+		outSingle[2 * (size_t)i + 1] = bestChild;
 	}
+}
+
+__device__ __forceinline__ uint32_t cast_expand10(uint32_t v)
+{
+	v = (v * 0x00010001u) & 0xFF0000FFu;
+	v = (v * 0x00000101u) & 0x0F00F00Fu;
+	v = (v * 0x00000011u) & 0xC30C30C3u;
+	v = (v * 0x00000005u) & 0x49249249u;
+	return v;
+}
+
+// Sort keys of the casts: world, then the 30-bit Morton code of the middle of
+// the sweep within the tree's root box.
+__global__ void k_cast_keys(const float* casts, uint32_t n, const float4* nodeLo, const float4* nodeHi,
+	unsigned long long* keys, uint32_t* vals)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n)
+		return;
+	const float* r = casts + 28 * (size_t)i;
+	const float4 lo = nodeLo[0], hi = nodeHi[0];
+	const float c[3] = {r[16] + 0.5f * r[23], r[17] + 0.5f * r[24], r[18] + 0.5f * r[25]};
+	const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+	uint32_t qv[3];
+	for (int k = 0; k < 3; ++k)
+	{
+		float ext = h[k] - l[k];
+		float t = ext > 0.0f ? (c[k] - l[k]) / ext : 0.0f;
+		t = fminf(fmaxf(t, 0.0f), 1.0f);
+		qv[k] = min((uint32_t)(t * 1024.0f), 1023u);
+	}
+	const uint32_t code = (cast_expand10(qv[0]) << 2) | (cast_expand10(qv[1]) << 1) | cast_expand10(qv[2]);
+	keys[i] = ((unsigned long long)__float_as_uint(r[2]) << 30) | code;
+	vals[i] = i;
 }
 
 int qfail(b3g_ctx* c, int code, const char* msg)
@@ -986,6 +1155,42 @@ extern "C" int b3g_ray_cast_single_device(b3g_ctx* c, uint32_t n, const float* r
 // Host check of the casts: the shape types a cast may have and their hulls.
 static_assert(sizeof(b3g_shape_cast_input) == 112, "b3g_shape_cast_input: 28 words");
 
+// Scratch bytes of cast_order for n casts.
+static size_t cast_order_bytes(uint32_t n)
+{
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	return 2 * al(8 * (size_t)n) + 2 * al(4 * (size_t)n) + al(4 * (size_t)radix_sort_scratch_words(n, 48));
+}
+
+// The casts' processing order (sorted by world and Morton key) in scratch
+// at p; returns the order array.
+static const uint32_t* cast_order(b3g_ctx* c, const float* dCasts, uint32_t n, char* p, uint32_t worldBits,
+	cudaStream_t s)
+{
+	auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+	unsigned long long* keys = (unsigned long long*)p;
+	p += al(8 * (size_t)n);
+	unsigned long long* keysTmp = (unsigned long long*)p;
+	p += al(8 * (size_t)n);
+	uint32_t* vals = (uint32_t*)p;
+	p += al(4 * (size_t)n);
+	uint32_t* valsTmp = (uint32_t*)p;
+	p += al(4 * (size_t)n);
+	uint32_t* scratch = (uint32_t*)p;
+	k_cast_keys<<<(n + 255) / 256, 256, 0, s>>>(dCasts, n, c->buf.nodeLo, c->buf.nodeHi, keys, vals);
+	bool swapped = radix_sort_pairs(keys, vals, keysTmp, valsTmp, n, 30 + (int)worldBits, scratch,
+		c->buf.counters + CTR_SCRATCH, s);
+	return swapped ? valsTmp : vals;
+}
+
+static uint32_t world_bits(const b3g_ctx* c)
+{
+	uint32_t b = 0;
+	while (b < 18 && (1u << b) < c->nWorlds)
+		++b;
+	return b;
+}
+
 static int cast_check(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input* casts)
 {
 	for (uint32_t i = 0; i < n; ++i)
@@ -1015,8 +1220,9 @@ extern "C" int b3g_shape_cast(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input
 	const void* dIn;
 	const size_t cntBytes = ((4 * (size_t)n + 4 + 255) & ~(size_t)255);
 	const size_t idxBytes = ((12 * (size_t)capacity + 255) & ~(size_t)255);
+	const size_t hitBytes = ((28 * (size_t)capacity + 255) & ~(size_t)255);
 	rc = q_begin(c, n, casts, sizeof(b3g_shape_cast_input) * (size_t)n, nullptr, q,
-		cntBytes + idxBytes + 28 * (size_t)capacity + 256, base, dWorlds, dIn);
+		cntBytes + idxBytes + hitBytes + cast_order_bytes(n) + 256, base, dWorlds, dIn);
 	if (rc)
 		return rc;
 	uint32_t* counts = (uint32_t*)base;
@@ -1024,10 +1230,12 @@ extern "C" int b3g_shape_cast(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input
 	float* dHit = (float*)(base + cntBytes + idxBytes);
 	cudaStream_t s = c->stream;
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
+	const uint32_t* order =
+		cast_order(c, (const float*)dIn, n, base + cntBytes + idxBytes + hitBytes, world_bits(c), s);
 	const uint32_t blocks = (n + 127) / 128;
-	k_shape_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, n, counts, dIdx, dHit, capacity, nullptr);
+	k_shape_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, order, n, counts, dIdx, dHit, capacity, nullptr);
 	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
-	k_shape_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, n, counts, dIdx, dHit, capacity, nullptr);
+	k_shape_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, order, n, counts, dIdx, dHit, capacity, nullptr);
 	uint32_t total = 0;
 	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
 		return qfail(c, B3G_E_CUDA, "b3g_shape_cast: copy");
@@ -1056,15 +1264,17 @@ extern "C" int b3g_shape_cast_single(b3g_ctx* c, uint32_t n, const b3g_shape_cas
 	const uint32_t* dWorlds;
 	const void* dIn;
 	const size_t fixBytes = ((8 * (size_t)n + 255) & ~(size_t)255);
-	rc = q_begin(c, n, casts, sizeof(b3g_shape_cast_input) * (size_t)n, nullptr, q, fixBytes + 28 * (size_t)n + 256,
-		base, dWorlds, dIn);
+	const size_t hitBytes = ((28 * (size_t)n + 255) & ~(size_t)255);
+	rc = q_begin(c, n, casts, sizeof(b3g_shape_cast_input) * (size_t)n, nullptr, q,
+		fixBytes + hitBytes + cast_order_bytes(n) + 256, base, dWorlds, dIn);
 	if (rc)
 		return rc;
 	uint32_t* dFix = (uint32_t*)base;
 	float* dHit = (float*)(base + fixBytes);
 	cudaStream_t s = c->stream;
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
-	k_shape_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, n, nullptr, nullptr, dHit, n, dFix);
+	const uint32_t* order = cast_order(c, (const float*)dIn, n, base + fixBytes + hitBytes, world_bits(c), s);
+	k_shape_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)dIn, order, n, nullptr, nullptr, dHit, n, dFix);
 	rc = q_status(c);
 	if (rc)
 		return rc;
@@ -1075,6 +1285,36 @@ extern "C" int b3g_shape_cast_single(b3g_ctx* c, uint32_t n, const b3g_shape_cas
 	for (uint32_t i = 0; i < n; ++i)
 		hits += fixture[2 * i] != B3G_NULL ? 1 : 0;
 	return hits;
+}
+
+extern "C" int b3g_shape_cast_single_device(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input* casts,
+	uint32_t* fixture, float* hit, void* stream)
+{
+	if (!c || (n && (!casts || !fixture || !hit)))
+		return c ? qfail(c, B3G_E_INVALID, "b3g_shape_cast_single_device: null argument") : B3G_E_INVALID;
+	if (!c->havePass || c->treeLeaves == 0)
+		return qfail(c, B3G_E_STATE, "world query: no collision pass yet");
+	if (n == 0)
+		return B3G_OK;
+	QueryCtx q;
+	q.S = c->scene;
+	q.nodeLo = c->buf.nodeLo;
+	q.nodeHi = c->buf.nodeHi;
+	q.fatLo = c->buf.fatLo;
+	q.fatHi = c->buf.fatHi;
+	q.leaves = c->treeLeaves;
+	q.status = c->buf.counters + CTR_SCRATCH;
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	if (n > std::max(c->cfg.max_proxies, c->cfg.max_contacts))
+		return qfail(c, B3G_E_CAPACITY, "world query: more queries than max(max_proxies, max_contacts) per call");
+	if (!q_reserve(c, cast_order_bytes(n)))
+		return qfail(c, B3G_E_CUDA, "world query: device allocation failed");
+	const uint32_t* order = cast_order(c, (const float*)casts, n, (char*)c->qScratch, world_bits(c), s);
+	k_shape_cast<2><<<(n + 127) / 128, 128, 0, s>>>(q, (const float*)casts, order, n, nullptr, nullptr, hit, n,
+		fixture);
+	if (cudaGetLastError() != cudaSuccess)
+		return qfail(c, B3G_E_CUDA, "b3g_shape_cast_single_device: launch");
+	return B3G_OK;
 }
 
 void free_queries(b3g_ctx* c)

@@ -7,9 +7,12 @@
  * contact creation of b3ContactManager::FindNewContacts / AddPair
  * (src/bounce/dynamics/contact_manager.cpp:98-223) and the narrowphase of
  * b3ContactManager::UpdateContacts (contact_manager.cpp:225-287), all on the
- * GPU. The reference's solver, islands, sleep and TOI stay host code and
- * consume the manifolds this library writes in the reference's own
- * b3Manifold layout (include/bounce/collision/collision.h:110-128, 320 bytes).
+ * GPU. The reference's solver iterations, island search and sleep decisions
+ * stay host code and consume the manifolds this library writes in the
+ * reference's own b3Manifold layout (include/bounce/collision/collision.h:110-128,
+ * 320 bytes). Around the pass, the world queries (AABB, ray and shape casts),
+ * the fixtures' contact edge lists and the contact solver's constraints are
+ * built here too.
  *
  * Conventions
  *  - Every entry point returns B3G_OK (0) or a negative status; the message of
@@ -469,7 +472,7 @@ typedef struct b3g_shape_cast_input
  * reports touching. Writes (cast, fixture, triangle or 0) into index (3 u32
  * per hit) and 7 floats per hit (point on the fixture and normal from b3GJK
  * at the time of impact, world.cpp:719-731; fraction) up to capacity, and
- * returns the number of hits. */
+ * returns the number of hits. A cast's hits come in no particular order. */
 int b3g_shape_cast(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* index, float* hits,
 	uint32_t capacity);
 
@@ -480,6 +483,14 @@ int b3g_shape_cast(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, 
  * its tree meets). Returns the number of casts that hit. */
 int b3g_shape_cast_single(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* fixture,
 	float* hit);
+
+/* b3g_shape_cast_single on device buffers (casts, fixture, hit as above, all
+ * device memory), asynchronous on stream (NULL: the context's stream), for
+ * callers that keep their casts on the GPU. The casts are not checked: every
+ * hull index must be below the hull count. Nothing is copied; the scratch of
+ * the cast ordering is the context's query scratch (grown on first use). */
+int b3g_shape_cast_single_device(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* fixture,
+	float* hit, void* stream);
 
 /* Solver input -------------------------------------------------------------
  *

@@ -105,7 +105,7 @@ def lib(precision=32):
         "refw_ray_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
         "refw_shape_cast": ([vp, f32p, u32p, f64p, ctypes.c_uint32], ctypes.c_uint32),
         "refw_shape_cast_single": ([vp, f32p, u32p, f64p], ctypes.c_uint32),
-        "refw_shape_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p], ctypes.c_double),
+        "refw_shape_cast_single_batch": ([vp, f32p, ctypes.c_uint32, u32p, f32p], ctypes.c_double),
         "ref_sizeof_dump_contact": ([], ctypes.c_uint32),
         "ref_sizeof_scalar": ([], ctypes.c_uint32),
         "ref_collide": (
@@ -349,11 +349,14 @@ class RefWorld:
         return int(fix[0]), hit
 
     def shape_cast_single_batch(self, casts):
-        """ShapeCastSingle for each cast, timed inside the harness: (fixtures, seconds)."""
+        """ShapeCastSingle for each cast, timed inside the harness:
+        (fixtures, fractions, seconds)."""
         c = np.ascontiguousarray(casts, np.float32).reshape(-1, 28)
         fix = np.zeros(max(len(c), 1), np.uint32)
-        t = self.L.refw_shape_cast_single_batch(self.w, _p(c, ctypes.c_float), len(c), _p(fix, ctypes.c_uint32))
-        return fix[:len(c)], t
+        frac = np.zeros(max(len(c), 1), np.float32)
+        t = self.L.refw_shape_cast_single_batch(self.w, _p(c, ctypes.c_float), len(c), _p(fix, ctypes.c_uint32),
+                                                _p(frac, ctypes.c_float))
+        return fix[:len(c)], frac[:len(c)], t
 
     def load_impulses(self, normal, tangent, motor):
         """The solver's impulses for every contact in list order, per manifold

@@ -1032,8 +1032,9 @@ REF_API uint32_t refw_shape_cast_single(void* p, const float* cast, uint32_t* fi
 
 // Timed batch of b3World::ShapeCastSingle calls (the CPU baseline of the
 // shape cast bench): writes each cast's fixture (or 0xFFFFFFFF) and returns
-// the seconds spent in the calls.
-REF_API double refw_shape_cast_single_batch(void* p, const float* casts, uint32_t n, uint32_t* fix)
+// the seconds spent in the calls; frac (may be null) receives each hit's
+// fraction (0 without a hit).
+REF_API double refw_shape_cast_single_batch(void* p, const float* casts, uint32_t n, uint32_t* fix, float* frac)
 {
 	RefWorld* w = (RefWorld*)p;
 	std::vector<ShapeStore> stores(n);
@@ -1046,9 +1047,10 @@ REF_API double refw_shape_cast_single_batch(void* p, const float* casts, uint32_
 	{
 		const float* c = casts + 28 * (size_t)i;
 		b3ShapeCastSingleOutput o;
-		fix[i] = w->world->ShapeCastSingle(&o, &filter, shapes[i], CastXf(c), b3Vec3(c[23], c[24], c[25]))
-			? (uint32_t)(uintptr_t)o.fixture->GetUserData()
-			: 0xFFFFFFFFu;
+		bool hit = w->world->ShapeCastSingle(&o, &filter, shapes[i], CastXf(c), b3Vec3(c[23], c[24], c[25]));
+		fix[i] = hit ? (uint32_t)(uintptr_t)o.fixture->GetUserData() : 0xFFFFFFFFu;
+		if (frac)
+			frac[i] = hit ? (float)o.fraction : 0.0f;
 	}
 	return Now() - t0;
 }
