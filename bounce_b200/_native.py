@@ -171,6 +171,25 @@ SHAPE_CAST_DTYPE = np.dtype(
     ]
 )
 assert SHAPE_CAST_DTYPE.itemsize == 112
+
+# b3g_toi_input (b3TOIInput) and b3g_gjk_cast_input (b3ShapeCast's arguments).
+SWEEP_FIELDS = 18  # localCenter, orientation0, worldCenter0, t0, orientation, worldCenter
+TOI_INPUT_DTYPE = np.dtype(
+    [
+        ("type_a", "<u4"), ("hull_a", "<u4"), ("type_b", "<u4"), ("hull_b", "<u4"),
+        ("params_a", "<f4", 12), ("params_b", "<f4", 12),
+        ("sweep_a", "<f4", SWEEP_FIELDS), ("sweep_b", "<f4", SWEEP_FIELDS),
+        ("t_max", "<f4"), ("pad", "<f4", 3),
+    ]
+)
+GJK_CAST_DTYPE = np.dtype(
+    [
+        ("type_a", "<u4"), ("hull_a", "<u4"), ("type_b", "<u4"), ("hull_b", "<u4"),
+        ("params_a", "<f4", 12), ("params_b", "<f4", 12),
+        ("xf_a", "<f4", 7), ("xf_b", "<f4", 7), ("translation_b", "<f4", 3), ("pad", "<f4", 3),
+    ]
+)
+assert TOI_INPUT_DTYPE.itemsize == 272 and GJK_CAST_DTYPE.itemsize == 192
 assert SOLVER_BODY_DTYPE.itemsize == 112 and CONTACT_CONSTRAINT_DTYPE.itemsize == 128
 assert MANIFOLD_CONSTRAINT_DTYPE.itemsize == 464
 
@@ -214,6 +233,9 @@ EXPORTED = [
     "b3g_shape_cast",
     "b3g_shape_cast_single",
     "b3g_shape_cast_single_device",
+    "b3g_time_of_impact",
+    "b3g_time_of_impact_aabb",
+    "b3g_gjk_shape_cast",
     "b3g_set_materials",
     "b3g_contact_constraints",
     "b3g_contact_constraints_device",
@@ -294,6 +316,9 @@ def load():
         "b3g_shape_cast": ([ctx, ctypes.c_uint32, vp, u32p, f32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_shape_cast_single": ([ctx, ctypes.c_uint32, vp, u32p, f32p], ctypes.c_int),
         "b3g_shape_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp], ctypes.c_int),
+        "b3g_time_of_impact": ([ctx, ctypes.c_uint32, vp, u32p], ctypes.c_int),
+        "b3g_time_of_impact_aabb": ([ctx, ctypes.c_uint32, f32p, u32p], ctypes.c_int),
+        "b3g_gjk_shape_cast": ([ctx, ctypes.c_uint32, vp, f32p], ctypes.c_int),
         "b3g_set_materials": ([ctx, f32p, f32p], ctypes.c_int),
         "b3g_contact_constraints": ([ctx, ctypes.c_uint32, u32p, vp, ctypes.c_float, ctypes.c_int, vp,
                                      ctypes.c_uint32, vp, ctypes.c_uint32, u32p], ctypes.c_int),

@@ -760,6 +760,45 @@ __device__ __forceinline__ AABB aabb_scaled(const AABB& a, V3 s)
 	return r;
 }
 
+// b3GJKProxy::Set (gjk.cpp:37-95) for a convex shape given by type,
+// parameters (the fixture layout) and hull.
+__device__ inline GProxy convex_proxy(const DevScene& S, uint32_t type, float4 p0, float4 p1, float4 p2, uint32_t hull)
+{
+	GProxy g;
+	g.gv = nullptr;
+	g.lv[0] = g.lv[1] = g.lv[2] = V3{0.0f, 0.0f, 0.0f};
+	switch (type)
+	{
+	case B3G_SHAPE_SPHERE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.count = 1;
+		g.radius = p0.w;
+		break;
+	case B3G_SHAPE_CAPSULE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.lv[1] = V3{p0.w, p1.x, p1.y};
+		g.count = 2;
+		g.radius = p1.z;
+		break;
+	case B3G_SHAPE_TRIANGLE:
+		g.lv[0] = V3{p0.x, p0.y, p0.z};
+		g.lv[1] = V3{p0.w, p1.x, p1.y};
+		g.lv[2] = V3{p1.z, p1.w, p2.x};
+		g.count = 3;
+		g.radius = p2.y;
+		break;
+	default:
+	{
+		const HullDesc h = S.hulls[hull];
+		g.gv = S.hverts + h.vOff;
+		g.count = h.vCnt;
+		g.radius = p0.x;
+		break;
+	}
+	}
+	return g;
+}
+
 // The same for fixture fix.
 __device__ inline void compute_aabbs(const DevScene& S, uint32_t fix, const XF& xa, const XF& xb, bool two, AABB& a,
 	AABB& b)

@@ -531,45 +531,6 @@ __device__ __noinline__ TOIOut toi_translate(const XF& xf1, const GProxy& p1, V3
 	return TOIOut{TOI_UNKNOWN, t};
 }
 
-// b3GJKProxy::Set (gjk.cpp:37-95) for a convex shape given by type,
-// parameters (the fixture layout) and hull.
-__device__ GProxy cast_proxy(const DevScene& S, uint32_t type, float4 p0, float4 p1, float4 p2, uint32_t hull)
-{
-	GProxy g;
-	g.gv = nullptr;
-	g.lv[0] = g.lv[1] = g.lv[2] = V3{0.0f, 0.0f, 0.0f};
-	switch (type)
-	{
-	case B3G_SHAPE_SPHERE:
-		g.lv[0] = V3{p0.x, p0.y, p0.z};
-		g.count = 1;
-		g.radius = p0.w;
-		break;
-	case B3G_SHAPE_CAPSULE:
-		g.lv[0] = V3{p0.x, p0.y, p0.z};
-		g.lv[1] = V3{p0.w, p1.x, p1.y};
-		g.count = 2;
-		g.radius = p1.z;
-		break;
-	case B3G_SHAPE_TRIANGLE:
-		g.lv[0] = V3{p0.x, p0.y, p0.z};
-		g.lv[1] = V3{p0.w, p1.x, p1.y};
-		g.lv[2] = V3{p1.z, p1.w, p2.x};
-		g.count = 3;
-		g.radius = p2.y;
-		break;
-	default:
-	{
-		const HullDesc h = S.hulls[hull];
-		g.gv = S.hverts + h.vOff;
-		g.count = h.vCnt;
-		g.radius = p0.x;
-		break;
-	}
-	}
-	return g;
-}
-
 // The proxy of a mesh fixture's triangle (gjk.cpp:75-89): its vertices
 // scaled by the mesh scale, the mesh radius.
 __device__ GProxy mesh_triangle_proxy(const DevScene& S, uint32_t fix, uint32_t tri)
@@ -707,7 +668,7 @@ __device__ __noinline__ void cast_candidate(const QueryCtx& q, const float* cast
 {
 	const DevScene& S = q.S;
 	const CastIn in = load_cast(casts, i);
-	const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
+	const GProxy pA = convex_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
 	const XF xfB = body_xf(S, S.fixBody[f]);
 	auto act = [&](uint32_t child, float t, const GProxy& pB) {
 		if (MODE == 2)
@@ -736,7 +697,7 @@ __device__ __noinline__ void cast_candidate(const QueryCtx& q, const float* cast
 	if (S.fixType[f] != B3G_SHAPE_MESH)
 	{
 		const GProxy pB =
-			cast_proxy(S, S.fixType[f], S.fixParams[3 * f], S.fixParams[3 * f + 1], S.fixParams[3 * f + 2], S.fixHull[f]);
+			convex_proxy(S, S.fixType[f], S.fixParams[3 * f], S.fixParams[3 * f + 1], S.fixParams[3 * f + 2], S.fixHull[f]);
 		TOIOut r = toi_translate(in.xf, pA, in.d, xfB, pB, V3{0.0f, 0.0f, 0.0f});
 		if (r.state == TOI_TOUCHING)
 			act(0u, r.t, pB);
@@ -869,7 +830,7 @@ __global__ void __launch_bounds__(128) k_shape_cast(QueryCtx q, const float* cas
 			bestF = (uint32_t)(key & 0xFFFFFFFFull);
 			const float bestT = __uint_as_float((uint32_t)(key >> 32));
 			const CastIn in = load_cast(casts, i);
-			const GProxy pA = cast_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
+			const GProxy pA = convex_proxy(S, in.type, in.p0, in.p1, in.p2, in.hull);
 			const XF xfB = body_xf(S, S.fixBody[bestF]);
 			GProxy pB;
 			pB.gv = nullptr;
@@ -892,7 +853,7 @@ __global__ void __launch_bounds__(128) k_shape_cast(QueryCtx q, const float* cas
 			else
 			{
 				bestChild = 0;
-				pB = cast_proxy(S, S.fixType[bestF], S.fixParams[3 * bestF], S.fixParams[3 * bestF + 1],
+				pB = convex_proxy(S, S.fixType[bestF], S.fixParams[3 * bestF], S.fixParams[3 * bestF + 1],
 					S.fixParams[3 * bestF + 2], S.fixHull[bestF]);
 			}
 			// b3World::ShapeCastSingle (world.cpp:828-848): evaluate the winner.

@@ -200,6 +200,30 @@ class CollisionPipeline:
                                                    N.ptr(fix, u32), N.ptr(hit, ctypes.c_float)))
         return fix[:len(c)], hit[:len(c)]
 
+    def time_of_impact(self, queries):
+        """b3TimeOfImpact(b3TOIInput) per TOI_INPUT_DTYPE query: (n, 4) u32
+        state, t bits, iterations, 0."""
+        q = np.ascontiguousarray(queries, N.TOI_INPUT_DTYPE)
+        out = np.zeros((max(len(q), 1), 4), np.uint32)
+        self._check(self.lib.b3g_time_of_impact(self.ctx, len(q), ctypes.c_void_p(q.ctypes.data), N.ptr(out, u32)))
+        return out[:len(q)]
+
+    def time_of_impact_aabb(self, queries):
+        """b3TimeOfImpact(aabb1, d1, aabb2, d2) per (18,) float query: (n, 4) u32."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 18)
+        out = np.zeros((max(len(q), 1), 4), np.uint32)
+        self._check(self.lib.b3g_time_of_impact_aabb(self.ctx, len(q), N.ptr(q, ctypes.c_float), N.ptr(out, u32)))
+        return out[:len(q)]
+
+    def gjk_shape_cast(self, queries):
+        """b3ShapeCast per GJK_CAST_DTYPE query: (n, 9) float32 words hit,
+        t, point, normal, iterations."""
+        q = np.ascontiguousarray(queries, N.GJK_CAST_DTYPE)
+        out = np.zeros((max(len(q), 1), 9), np.float32)
+        self._check(self.lib.b3g_gjk_shape_cast(self.ctx, len(q), ctypes.c_void_p(q.ctypes.data),
+                                                N.ptr(out, ctypes.c_float)))
+        return out[:len(q)]
+
     def set_materials(self, friction, restitution):
         """Friction and restitution per fixture (b3Fixture::m_friction, m_restitution)."""
         fr = np.ascontiguousarray(friction, np.float32)

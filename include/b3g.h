@@ -492,6 +492,52 @@ int b3g_shape_cast_single(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* 
 int b3g_shape_cast_single_device(b3g_ctx* ctx, uint32_t n, const b3g_shape_cast_input* casts, uint32_t* fixture,
 	float* hit, void* stream);
 
+/* Time of impact and GJK shape cast ---------------------------------------
+ *
+ * Batched forms of the reference's free functions (no world needed; hull
+ * shapes refer to the hulls of b3g_set_hulls). Host buffers, synchronous.
+ * Shapes are convex (sphere, capsule, triangle, hull) with params as in
+ * b3g_set_fixtures. Results per query: 4 u32 = b3TOIOutput state
+ * (0 unknown, 1 failed, 2 overlapped, 3 touching, 4 separated), t (float
+ * bits), iterations, 0. Each returns the query count. */
+
+/* b3TOIInput (time_of_impact.h:27-34): two shapes, their b3Sweeps (18 floats
+ * each in member order: localCenter, orientation0 xyzw, worldCenter0, t0,
+ * orientation xyzw, worldCenter) and tMax. 272 bytes. */
+typedef struct b3g_toi_input
+{
+	uint32_t type_a, hull_a, type_b, hull_b;
+	float params_a[12], params_b[12];
+	float sweep_a[18], sweep_b[18];
+	float t_max;
+	float pad[3];
+} b3g_toi_input;
+
+/* b3TimeOfImpact(const b3TOIInput&) (time_of_impact.cpp:465-660): the local
+ * separating axis method over the two sweeps. Where the reference reaches a
+ * simplex feature combination it asserts never happens, the query ends as
+ * failed at the current time. */
+int b3g_time_of_impact(b3g_ctx* ctx, uint32_t n, const b3g_toi_input* queries, uint32_t* out);
+
+/* b3TimeOfImpact(aabb1, d1, aabb2, d2) (time_of_impact.cpp:782-902): 18
+ * floats per query (aabb1 lower, upper, d1, aabb2 lower, upper, d2). */
+int b3g_time_of_impact_aabb(b3g_ctx* ctx, uint32_t n, const float* queries, uint32_t* out);
+
+/* b3ShapeCast (gjk.cpp:938-1102): proxy B moved by translation_b from its
+ * transform against proxy A. 192 bytes. */
+typedef struct b3g_gjk_cast_input
+{
+	uint32_t type_a, hull_a, type_b, hull_b;
+	float params_a[12], params_b[12];
+	float xf_a[7], xf_b[7]; /* translation, rotation xyzw */
+	float translation_b[3];
+	float pad[3];
+} b3g_gjk_cast_input;
+
+/* Writes 9 words per query: hit (u32 0 or 1), t, point (on A, radius
+ * included), normal, iterations (u32); zeros where there is no hit. */
+int b3g_gjk_shape_cast(b3g_ctx* ctx, uint32_t n, const b3g_gjk_cast_input* queries, float* out);
+
 /* Solver input -------------------------------------------------------------
  *
  * b3ContactSolver's constructor and InitializeVelocityConstraints

@@ -119,6 +119,9 @@ def lib(precision=32):
             ctypes.c_int,
         ),
         "ref_sweep_xf0": ([f32p, f32p, f32p, f32p, f32p], None),
+        "refh_toi": ([vp, ctypes.c_uint32, f32p, u32p], None),
+        "refh_toi_aabb": ([ctypes.c_uint32, f32p, u32p], None),
+        "refh_gjk_cast": ([vp, ctypes.c_uint32, f32p, f32p], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -152,6 +155,22 @@ class RefHulls:
             m = mesh_arrays
             self.L.refh_add_meshes(self.h, len(m["desc"]) // 4, _p(m["desc"], ctypes.c_uint32),
                                    _p(m["verts"], ctypes.c_float), _p(m["tris"], ctypes.c_uint32))
+
+    def time_of_impact(self, queries):
+        """b3TimeOfImpact(b3TOIInput) per query ((n, 68) float32 words in the
+        b3g_toi_input layout): (n, 4) u32 state, t bits, iterations, 0."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 68)
+        out = np.zeros((max(len(q), 1), 4), np.uint32)
+        self.L.refh_toi(self.h, len(q), _p(q, ctypes.c_float), _p(out, ctypes.c_uint32))
+        return out[:len(q)]
+
+    def gjk_shape_cast(self, queries):
+        """b3ShapeCast per query ((n, 48) words, b3g_gjk_cast_input layout):
+        (n, 9) float32 words hit, t, point, normal, iterations."""
+        q = np.ascontiguousarray(queries, np.float32).reshape(-1, 48)
+        out = np.zeros((max(len(q), 1), 9), np.float32)
+        self.L.refh_gjk_cast(self.h, len(q), _p(q, ctypes.c_float), _p(out, ctypes.c_float))
+        return out[:len(q)]
 
     def mesh_wings(self, m, n_triangles):
         out = np.zeros(3 * n_triangles, np.uint32)
@@ -399,6 +418,16 @@ class RefWorld:
 
 
 _restate = None
+
+
+def time_of_impact_aabb(queries, precision=32):
+    """b3TimeOfImpact(aabb1, d1, aabb2, d2) per query ((n, 18) float32):
+    (n, 4) u32 state, t bits, iterations, 0."""
+    L = lib(precision)
+    q = np.ascontiguousarray(queries, np.float32).reshape(-1, 18)
+    out = np.zeros((max(len(q), 1), 4), np.uint32)
+    L.refh_toi_aabb(len(q), _p(q, ctypes.c_float), _p(out, ctypes.c_uint32))
+    return out[:len(q)]
 
 
 def restate():

@@ -45,6 +45,8 @@
 #include <bounce/collision/sat/sat.h>
 #include <bounce/dynamics/contacts/contact_solver.h>
 #include <bounce/dynamics/time_step.h>
+#include <bounce/collision/gjk/gjk_proxy.h>
+#include <bounce/collision/time_of_impact.h>
 #undef private
 #undef protected
 
@@ -291,6 +293,119 @@ static const b3Shape* MakeShape(ShapeStore& s, uint32_t type, const float* p, ui
 		return &s.mesh;
 	default:
 		return nullptr;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Time of impact and GJK shape cast, the reference's free functions on
+// shapes built from fixture parameters (hulls from the pool).
+
+// b3ShapeCast and its output are defined in gjk.cpp (gjk.cpp:930-942) without
+// a header; declared here as they are defined there.
+struct b3ShapeCastOutput
+{
+	scalar t;
+	b3Vec3 point;
+	b3Vec3 normal;
+	uint32 iterations;
+};
+bool b3ShapeCast(b3ShapeCastOutput* output, const b3Transform& xf1, const b3GJKProxy& proxy1,
+	const b3Transform& xf2, const b3GJKProxy& proxy2, const b3Vec3& translation2);
+
+static void SetSweep(b3Sweep& w, const float* s)
+{
+	w.localCenter.Set(s[0], s[1], s[2]);
+	w.orientation0.v.Set(s[3], s[4], s[5]);
+	w.orientation0.s = s[6];
+	w.worldCenter0.Set(s[7], s[8], s[9]);
+	w.t0 = s[10];
+	w.orientation.v.Set(s[11], s[12], s[13]);
+	w.orientation.s = s[14];
+	w.worldCenter.Set(s[15], s[16], s[17]);
+}
+
+static void PutTOI(uint32_t* o, const b3TOIOutput& r)
+{
+	float t = (float)r.t;
+	o[0] = (uint32_t)r.state;
+	memcpy(o + 1, &t, 4);
+	o[2] = r.iterations;
+	o[3] = 0;
+}
+
+// b3TimeOfImpact(const b3TOIInput&) per query (68 words, the b3g_toi_input
+// layout); 4 words out each: state, t bits, iterations, 0.
+REF_API void refh_toi(void* hullPool, uint32_t n, const float* q, uint32_t* out)
+{
+	const HullPool* pool = (const HullPool*)hullPool;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* r = q + 68 * (size_t)i;
+		uint32_t w[4];
+		memcpy(w, r, 16);
+		ShapeStore sa, sb;
+		const b3Shape* a = MakeShape(sa, w[0], r + 4, w[1], pool);
+		const b3Shape* b = MakeShape(sb, w[2], r + 16, w[3], pool);
+		b3TOIInput in;
+		in.proxy1.Set(a, 0);
+		in.proxy2.Set(b, 0);
+		SetSweep(in.sweep1, r + 28);
+		SetSweep(in.sweep2, r + 46);
+		in.tMax = r[64];
+		PutTOI(out + 4 * (size_t)i, b3TimeOfImpact(in));
+	}
+}
+
+// b3TimeOfImpact(aabb1, d1, aabb2, d2) per query (18 floats).
+REF_API void refh_toi_aabb(uint32_t n, const float* q, uint32_t* out)
+{
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* r = q + 18 * (size_t)i;
+		b3AABB a, b;
+		a.lowerBound.Set(r[0], r[1], r[2]);
+		a.upperBound.Set(r[3], r[4], r[5]);
+		b.lowerBound.Set(r[9], r[10], r[11]);
+		b.upperBound.Set(r[12], r[13], r[14]);
+		PutTOI(out + 4 * (size_t)i,
+			b3TimeOfImpact(a, b3Vec3(r[6], r[7], r[8]), b, b3Vec3(r[15], r[16], r[17])));
+	}
+}
+
+// b3ShapeCast per query (48 words, the b3g_gjk_cast_input layout); 9 words
+// out each: hit, t, point, normal, iterations (zeros without a hit).
+REF_API void refh_gjk_cast(void* hullPool, uint32_t n, const float* q, float* out)
+{
+	const HullPool* pool = (const HullPool*)hullPool;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		const float* r = q + 48 * (size_t)i;
+		uint32_t w[4];
+		memcpy(w, r, 16);
+		ShapeStore sa, sb;
+		const b3Shape* a = MakeShape(sa, w[0], r + 4, w[1], pool);
+		const b3Shape* b = MakeShape(sb, w[2], r + 16, w[3], pool);
+		b3GJKProxy pa(a, 0), pb(b, 0);
+		b3Transform xa, xb;
+		xa.translation.Set(r[28], r[29], r[30]);
+		xa.rotation.v.Set(r[31], r[32], r[33]);
+		xa.rotation.s = r[34];
+		xb.translation.Set(r[35], r[36], r[37]);
+		xb.rotation.v.Set(r[38], r[39], r[40]);
+		xb.rotation.s = r[41];
+		b3ShapeCastOutput o;
+		bool hit = b3ShapeCast(&o, xa, pa, xb, pb, b3Vec3(r[42], r[43], r[44]));
+		float* d = out + 9 * (size_t)i;
+		uint32_t h = hit ? 1u : 0u, it = o.iterations;
+		memcpy(d, &h, 4);
+		d[1] = hit ? (float)o.t : 0.0f;
+		d[2] = hit ? (float)o.point.x : 0.0f;
+		d[3] = hit ? (float)o.point.y : 0.0f;
+		d[4] = hit ? (float)o.point.z : 0.0f;
+		d[5] = hit ? (float)o.normal.x : 0.0f;
+		d[6] = hit ? (float)o.normal.y : 0.0f;
+		d[7] = hit ? (float)o.normal.z : 0.0f;
+		memcpy(d + 8, &it, 4);
 	}
 }
 
