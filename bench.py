@@ -14,9 +14,9 @@ through the C ABI with host buffers (host->device copy of the pinned state,
 device->host contact list and packed touching manifolds every step, the
 copies of one step overlapping the next step's pass). Other workloads:
 --workload pile (hull pile over a mesh), batched (1,024 worlds), serving
-(request stream), queries (ray casts), shapecast (shape casts) and
-constraints (the solver's contact constraints built from the pass's
-manifolds). The reference arm
+(request stream), queries (ray casts), shapecast (shape casts), toi (time
+of impact of sweep pairs) and constraints (the solver's contact constraints
+built from the pass's manifolds). The reference arm
 (--impl reference) runs the reference's own CPU pipeline (oracle/_ref, the
 unmodified Bounce sources) on the same scene and body motion.
 
@@ -63,7 +63,7 @@ def parse():
                     help="passes after the timed ones, with per-stage CUDA events (not part of value)")
     ap.add_argument("--no-graph", action="store_true", help="launch each pass kernel by kernel")
     ap.add_argument("--workload", default="mixed", choices=["mixed", "pile", "batched", "serving", "queries",
-                                                             "constraints", "shapecast"])
+                                                             "constraints", "shapecast", "toi"])
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000",
                     help="serving: arrival rates (worlds/s) of the sweep")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serving: arrival window per rate")
@@ -245,6 +245,19 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
 
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
+        return
+    if args.workload == "toi":
+        sc, q = toi_setup(SEED)
+        _, t = toi_reference(sc, q[:TOI_CPU_COUNT])
+        v = TOI_CPU_COUNT / t
+        print(json.dumps({
+            "metric": "time-of-impact queries/s", "value": v, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": TOI_WORKLOAD, "queries_per_step": TOI_CPU_COUNT},
+            "cpu_baseline": {"value": v, "unit": "queries/s", "cores": 1, "kind": "reference",
+                             "sample": f"{TOI_CPU_COUNT} queries through b3TimeOfImpact on 1 host core"},
+            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     if args.workload == "shapecast":
         scene, walls = workload_scene(args, SEED)
@@ -1100,6 +1113,134 @@ def run_shapecast(args, rank, world, local, dist):
     pipe.close()
 
 
+TOI_COUNT = 1 << 20
+TOI_CPU_COUNT = 1 << 16
+TOI_WORKLOAD = ("b3TimeOfImpact(b3TOIInput) on 1,048,576 seeded sweep pairs of spheres, capsules, triangles and "
+                "hulls (the hull pool of a 4,096-body mixed world): shape A sweeps toward the middle while "
+                "rotating, shape B drifts near it, tMax = 1")
+
+
+def toi_setup(seed):
+    from bounce_b200 import scene as S
+
+    sc = S.mixed_scene(seed=seed, n=4096, side=SIDE * (4096 / N_BODIES) ** (1.0 / 3.0)).finalize()
+    q = S.toi_queries(np.random.default_rng(seed + 400), TOI_COUNT, len(sc.hull_arrays["desc"]) // 6)
+    return sc, q
+
+
+def toi_reference(sc, q):
+    """The reference's b3TimeOfImpact over the queries on 1 host core: (states, seconds)."""
+    from oracle import oracle as O
+
+    hulls = O.RefHulls(sc.hull_arrays)
+    raw = q.view(np.float32).reshape(-1, 68)
+    t0 = time.perf_counter()
+    out = hulls.time_of_impact(raw)
+    return out, time.perf_counter() - t0
+
+
+def run_toi(args, rank, world, local, dist):
+    import ctypes
+
+    import torch
+
+    from bounce_b200.pipeline import CollisionPipeline
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sc, q = toi_setup(SEED + rank)
+    pipe = CollisionPipeline(sc, device=local)
+    n = len(q)
+    d_q = torch.from_numpy(q.view(np.uint8).copy()).to(dev)
+    d_out = torch.empty((n, 4), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    lib = pipe.lib
+
+    def run():
+        pipe._check(lib.b3g_time_of_impact_device(pipe.ctx, n, ctypes.c_void_p(d_q.data_ptr()),
+                                                   ctypes.c_void_p(d_out.data_ptr()), sptr))
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            run()
+    stream.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.2)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flushed between steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    states = np.bincount(d_out[:, 0].cpu().numpy(), minlength=5).tolist()
+    secs, work = replica_totals(dist, dev, ms / 1000.0, n * args.steps)
+    value = work / secs
+
+    # e2e: the host-buffer entry point (queries copied in, results copied out).
+    e2e_steps = max(1, min(args.e2e_steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        out_h = pipe.time_of_impact(q)
+    e2e_s, e2e_work = replica_totals(dist, dev, time.perf_counter() - t0, n * e2e_steps)
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    algo = n * (272 + 16)
+    achieved = algo / (ms / args.steps / 1000.0) / 1e9
+    roof = {"kernel": "k_toi_sweeps (b3TimeOfImpact)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+            "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "algorithmic_bytes_per_launch": algo,
+            "note": "queries in (272 B) and results out (16 B) per query; the conservative advancement and GJK "
+                    "iterations are compute and divergence bound",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            k = TOI_CPU_COUNT
+            ref, rt = toi_reference(sc, q[:k])
+            cpu = {"value": k / rt, "unit": "queries/s", "cores": 1, "kind": "reference",
+                   "sample": f"{k} of the step's queries through b3TimeOfImpact on 1 host core",
+                   "identical_to_gpu": float(np.mean(np.all(ref == out_h[:k], axis=1)))}
+        except Exception as e:
+            cpu = {"value": None, "unit": "queries/s", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "time-of-impact queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": TOI_WORKLOAD, "queries_per_step": n,
+                       "states_unknown_failed_overlapped_touching_separated": states,
+                       "l2": "flushed between steps (256 MB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_work / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": 272 * n,
+                    "d2h_bytes_per_step": 16 * n, "steps": e2e_steps},
+            "gpu_launches": args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }))
+    pipe.close()
+
+
 CONSTRAINT_WORKLOAD = ("b3ContactSolver constructor + InitializeVelocityConstraints over the 65,536-body mixed "
                        "world after 3 collision passes: every touching non-sensor contact, seeded body velocities "
                        "N(0, 1), inverse masses 1/U(0.5, 5) kg, world inverse inertias R diag(1/U(0.05, 2)) R^T, "
@@ -1303,6 +1444,8 @@ def main():
             run_constraints(args, rank, world, local, dist)
         elif args.workload == "shapecast":
             run_shapecast(args, rank, world, local, dist)
+        elif args.workload == "toi":
+            run_toi(args, rank, world, local, dist)
         else:
             run_ours(args, rank, world, local, dist)
     finally:

@@ -234,6 +234,7 @@ EXPORTED = [
     "b3g_shape_cast_single",
     "b3g_shape_cast_single_device",
     "b3g_time_of_impact",
+    "b3g_time_of_impact_device",
     "b3g_time_of_impact_aabb",
     "b3g_gjk_shape_cast",
     "b3g_set_materials",
@@ -317,6 +318,7 @@ def load():
         "b3g_shape_cast_single": ([ctx, ctypes.c_uint32, vp, u32p, f32p], ctypes.c_int),
         "b3g_shape_cast_single_device": ([ctx, ctypes.c_uint32, vp, vp, vp, vp], ctypes.c_int),
         "b3g_time_of_impact": ([ctx, ctypes.c_uint32, vp, u32p], ctypes.c_int),
+        "b3g_time_of_impact_device": ([ctx, ctypes.c_uint32, vp, vp, vp], ctypes.c_int),
         "b3g_time_of_impact_aabb": ([ctx, ctypes.c_uint32, f32p, u32p], ctypes.c_int),
         "b3g_gjk_shape_cast": ([ctx, ctypes.c_uint32, vp, f32p], ctypes.c_int),
         "b3g_set_materials": ([ctx, f32p, f32p], ctypes.c_int),

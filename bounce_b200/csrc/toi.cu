@@ -859,6 +859,22 @@ extern "C" int b3g_time_of_impact(b3g_ctx* c, uint32_t n, const b3g_toi_input* i
 	});
 }
 
+extern "C" int b3g_time_of_impact_device(b3g_ctx* c, uint32_t n, const b3g_toi_input* in, uint32_t* out,
+	void* stream)
+{
+	if (!c || (n && (!in || !out)))
+		return c ? tfail(c, B3G_E_INVALID, "b3g_time_of_impact_device: null argument") : B3G_E_INVALID;
+	if (n == 0)
+		return B3G_OK;
+	if (cudaSetDevice(c->device) != cudaSuccess)
+		return tfail(c, B3G_E_CUDA, "time of impact: device");
+	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+	k_toi_sweeps<<<(n + 127) / 128, 128, 0, s>>>(c->scene, (const float*)in, n, out);
+	if (cudaGetLastError() != cudaSuccess)
+		return tfail(c, B3G_E_CUDA, "b3g_time_of_impact_device: launch");
+	return B3G_OK;
+}
+
 extern "C" int b3g_time_of_impact_aabb(b3g_ctx* c, uint32_t n, const float* in, uint32_t* out)
 {
 	if (!c || (n && (!in || !out)))

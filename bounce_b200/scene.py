@@ -746,3 +746,74 @@ def pile_scene(seed=9, columns=512, per_column=512, grid=512, spacing=0.5, ampli
             b = s.add_body(0, N.BODY_DYNAMIC, (cx[c], ys[c, lv], cz[c]), quats[k], lin[k], ang[k])
             s.add_fixture(b, N.SHAPE_HULL, [0.0], hull=k)
     return s
+
+
+# ---------------------------------------------------------------------------
+# Queries of the time-of-impact entry points.
+
+
+def unit_quats(rng, n):
+    """n uniform random unit quaternions (xyzw)."""
+    q = rng.normal(size=(n, 4))
+    return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+def qmul(a, b):
+    """Quaternion products of (n, 4) xyzw arrays."""
+    av, aw = a[:, :3], a[:, 3:]
+    bv, bw = b[:, :3], b[:, 3:]
+    v = np.cross(av, bv) + aw * bv + bw * av
+    w = aw * bw - np.sum(av * bv, axis=1, keepdims=True)
+    return np.concatenate([v, w], axis=1)
+
+
+def random_convex_shapes(rng, n, n_hulls):
+    """Types and params of random convex shapes (hull indices into the pool)."""
+    types = rng.choice([N.SHAPE_SPHERE, N.SHAPE_CAPSULE, N.SHAPE_TRIANGLE, N.SHAPE_HULL], n, p=[0.25, 0.25, 0.15, 0.35])
+    params = np.zeros((n, 12), np.float32)
+    hulls = np.zeros(n, np.uint32)
+    for i, t in enumerate(types):
+        if t == N.SHAPE_SPHERE:
+            params[i, :4] = [*rng.uniform(-0.1, 0.1, 3), rng.uniform(0.2, 0.8)]
+        elif t == N.SHAPE_CAPSULE:
+            h = rng.uniform(0.2, 0.8)
+            params[i, :7] = [0, -h, 0, 0, h, 0, rng.uniform(0.1, 0.4)]
+        elif t == N.SHAPE_TRIANGLE:
+            params[i, :9] = rng.uniform(-0.8, 0.8, 9)
+            params[i, 9] = 0.0
+        else:
+            hulls[i] = rng.integers(0, n_hulls)
+    return types.astype(np.uint32), params, hulls
+
+
+def toi_queries(rng, n, n_hulls):
+    """Seeded b3TOIInput queries (TOI_INPUT_DTYPE): shape A sweeps from a
+    random point toward the middle while rotating a little, shape B drifts
+    near the middle; quaternion pairs of both signs; tMax = 1."""
+    q = np.zeros(n, N.TOI_INPUT_DTYPE)
+    q["type_a"], q["params_a"], q["hull_a"] = random_convex_shapes(rng, n, n_hulls)
+    q["type_b"], q["params_b"], q["hull_b"] = random_convex_shapes(rng, n, n_hulls)
+    for side, move in (("sweep_a", 1.0), ("sweep_b", 0.3)):
+        sw = np.zeros((n, 18), np.float32)
+        sw[:, 0:3] = rng.uniform(-0.1, 0.1, (n, 3))
+        q0 = unit_quats(rng, n)
+        small = np.concatenate([rng.normal(0, 0.3, (n, 3)), np.ones((n, 1))], axis=1)
+        small /= np.linalg.norm(small, axis=1, keepdims=True)
+        q1 = qmul(q0, small)
+        flip = rng.random(n) < 0.3
+        q1[flip] = -q1[flip]
+        sw[:, 3:7] = q0
+        sw[:, 11:15] = q1
+        if side == "sweep_a":
+            c0 = rng.uniform(-3, 3, (n, 3))
+            target = rng.uniform(-1, 1, (n, 3))
+            d = target - c0
+            sw[:, 7:10] = c0
+            sw[:, 15:18] = c0 + d * rng.uniform(0.5, 2.5, (n, 1)) * move
+        else:
+            c0 = rng.uniform(-0.5, 0.5, (n, 3))
+            sw[:, 7:10] = c0
+            sw[:, 15:18] = c0 + rng.normal(0, move, (n, 3))
+        q[side] = sw
+    q["t_max"] = 1.0
+    return q

@@ -519,6 +519,12 @@ typedef struct b3g_toi_input
  * failed at the current time. */
 int b3g_time_of_impact(b3g_ctx* ctx, uint32_t n, const b3g_toi_input* queries, uint32_t* out);
 
+/* The same on device buffers, asynchronous on stream (NULL: the context's
+ * stream); the queries are not checked (hull indices below the hull count,
+ * convex types only). Nothing is copied or allocated. */
+int b3g_time_of_impact_device(b3g_ctx* ctx, uint32_t n, const b3g_toi_input* queries, uint32_t* out,
+	void* stream);
+
 /* b3TimeOfImpact(aabb1, d1, aabb2, d2) (time_of_impact.cpp:782-902): 18
  * floats per query (aabb1 lower, upper, d1, aabb2 lower, upper, d2). */
 int b3g_time_of_impact_aabb(b3g_ctx* ctx, uint32_t n, const float* queries, uint32_t* out);
