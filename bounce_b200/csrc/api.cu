@@ -648,6 +648,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(c->ciTiles);
 	if (c->ciHost)
 		cudaFree(c->ciHost);
+	if (c->toiScratch)
+		cudaFree(c->toiScratch);
 	if (c->sideStream)
 	{
 		cudaStreamSynchronize(c->sideStream);

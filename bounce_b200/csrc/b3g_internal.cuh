@@ -314,6 +314,8 @@ struct b3g_ctx
 	uint32_t ciTileCap;
 	void* ciHost;                 // b3g_contact_constraints: device copies of its host buffers
 	size_t ciHostBytes;
+	void* toiScratch;             // time-of-impact batches: device copies of their host buffers
+	size_t toiScratchBytes;
 
 	uint32_t nHulls, nBodies, nFixtures, nWorlds;
 	uint32_t hullVerts, hullEdges, hullFaces;

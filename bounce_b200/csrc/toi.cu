@@ -806,7 +806,8 @@ int tfail(b3g_ctx* c, int code, const char* msg)
 }
 
 // Copies n records of `bytes` each in, runs the launch, copies `outBytes`
-// per record out (synchronous, on the context's stream).
+// per record out (synchronous, on the context's stream). The device copies
+// live in the context's scratch, grown on demand.
 template <class Launch>
 int run_batch(b3g_ctx* c, uint32_t n, const void* in, size_t bytes, void* out, size_t outBytes, Launch&& launch)
 {
@@ -814,27 +815,28 @@ int run_batch(b3g_ctx* c, uint32_t n, const void* in, size_t bytes, void* out, s
 		return 0;
 	if (cudaSetDevice(c->device) != cudaSuccess)
 		return tfail(c, B3G_E_CUDA, "time of impact: device");
-	void* dIn = nullptr;
-	void* dOut = nullptr;
-	if (cudaMalloc(&dIn, bytes * n) != cudaSuccess || cudaMalloc(&dOut, outBytes * n) != cudaSuccess)
+	const size_t inBytes = (bytes * n + 255) & ~(size_t)255;
+	const size_t need = inBytes + outBytes * n;
+	if (c->toiScratchBytes < need)
 	{
-		cudaFree(dIn);
-		return tfail(c, B3G_E_CUDA, "time of impact: device allocation failed");
+		if (c->toiScratch && cudaFree(c->toiScratch) != cudaSuccess)
+			return tfail(c, B3G_E_CUDA, "time of impact: device free failed");
+		c->toiScratch = nullptr;
+		c->toiScratchBytes = 0;
+		if (cudaMalloc(&c->toiScratch, need) != cudaSuccess)
+			return tfail(c, B3G_E_CUDA, "time of impact: device allocation failed");
+		c->toiScratchBytes = need;
 	}
-	int rc = n;
+	void* dIn = c->toiScratch;
+	void* dOut = (char*)c->toiScratch + inBytes;
 	if (cudaMemcpyAsync(dIn, in, bytes * n, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
-		rc = tfail(c, B3G_E_CUDA, "time of impact: copy");
-	if (rc >= 0)
-	{
-		launch((const float*)dIn, dOut, c->stream);
-		if (cudaGetLastError() != cudaSuccess ||
-			cudaMemcpyAsync(out, dOut, outBytes * n, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
-			cudaStreamSynchronize(c->stream) != cudaSuccess)
-			rc = tfail(c, B3G_E_CUDA, "time of impact: kernel or copy failed");
-	}
-	cudaFree(dIn);
-	cudaFree(dOut);
-	return rc;
+		return tfail(c, B3G_E_CUDA, "time of impact: copy");
+	launch((const float*)dIn, dOut, c->stream);
+	if (cudaGetLastError() != cudaSuccess ||
+		cudaMemcpyAsync(out, dOut, outBytes * n, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+		cudaStreamSynchronize(c->stream) != cudaSuccess)
+		return tfail(c, B3G_E_CUDA, "time of impact: kernel or copy failed");
+	return (int)n;
 }
 
 // Shape types and hulls of a query's two proxies: convex types only.
