@@ -36,8 +36,10 @@ __device__ __forceinline__ Sweep load_sweep(const float* s)
 	return w;
 }
 
-// b3Sweep::GetTransform (sweep.h:43-63).
-__device__ __forceinline__ XF sweep_at(const Sweep& w, float t)
+// b3Sweep::GetTransform (sweep.h:43-63). Kept out of line (as are the
+// separation function's methods): the time of impact calls them from many
+// places, and inlined copies overflow the instruction cache.
+__device__ __noinline__ XF sweep_at(const Sweep& w, float t)
 {
 	const V3 c = (1.0f - t) * w.c0 + t * w.c;
 	Q4 q1 = w.q0;
@@ -196,7 +198,7 @@ struct Separation
 	V3 localPoint, axis;
 	bool parallel;
 
-	__device__ void init(const GJKCache& cache, float t1)
+	__device__ __noinline__ void init(const GJKCache& cache, float t1)
 	{
 		const XF xfA = sweep_at(*sA, t1), xfB = sweep_at(*sB, t1);
 		const FeaturePair fp = feature_pair(cache);
@@ -296,7 +298,7 @@ struct Separation
 		}
 	}
 
-	__device__ float find_min(uint32_t& indexA, uint32_t& indexB, float t) const
+	__device__ __noinline__ float find_min(uint32_t& indexA, uint32_t& indexB, float t) const
 	{
 		const XF xfA = sweep_at(*sA, t), xfB = sweep_at(*sB, t);
 		switch (type)
@@ -359,7 +361,7 @@ struct Separation
 		}
 	}
 
-	__device__ float evaluate(uint32_t indexA, uint32_t indexB, float t) const
+	__device__ __noinline__ float evaluate(uint32_t indexA, uint32_t indexB, float t) const
 	{
 		const XF xfA = sweep_at(*sA, t), xfB = sweep_at(*sB, t);
 		switch (type)
