@@ -1413,6 +1413,15 @@ def run_constraints(args, rank, world, local, dist):
     e2e_value = e2e_work / e2e_s
     e2e_same = bool(np.array_equal(h_man.numpy().view(np.uint32), man_h.view(np.uint32).reshape(-1)))
 
+    # The island graph's edges of the same pass (b3g_fetch_fixture_contacts:
+    # every fixture's contact list, device sort and copy to the host), timed
+    # by wall clock through the host entry point.
+    pipe.fixture_contacts()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        offsets, edges = pipe.fixture_contacts()
+    edge_ms = (time.perf_counter() - t0) / 5 * 1000.0
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -1453,6 +1462,7 @@ def run_constraints(args, rank, world, local, dist):
             "config": {"workload": CONSTRAINT_WORKLOAD, "bodies": nb, "contacts": counts["contacts"],
                        "constraints_per_step": nc, "manifolds_per_step": nm, "points_per_step": points,
                        "device_records_equal_host_entry": same and e2e_same,
+                       "fixture_edges": {"edges": int(len(edges)), "ms_host_entry": edge_ms},
                        "l2": "flushed between steps (256 MB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "constraints/s", "h2d_bytes_per_step": 112 * nb,
