@@ -39,8 +39,13 @@ sys.path.insert(0, ROOT)
 N_BODIES = 65536
 SIDE = 49.0
 SEED = 2
-WORKLOAD = "one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% hull 8-32 pts), 49 m cube, kinematic motion reflected at the cube faces"
+WORKLOAD = ("one world, 65,536 mixed bodies (40% sphere, 30% capsule, 30% convex hull of 8-32 points on ellipsoids, "
+            "built by this project's incremental hull builder, not the reference's quickhull), 49 m cube, "
+            "kinematic motion reflected at the cube faces")
 PILE_SEED = 9
+# Untimed passes after the warm-up in which the device arm captures its CUDA
+# graphs (one per contact-buffer parity); both arms skip them.
+GRAPH_PASSES = 2
 PILE_WORKLOAD = ("hull-heavy pile: 262,144 distinct hulls (quickhulls of 12-64 points on ellipsoids, semi-axes "
                  "U[0.3, 1.0] m) in 512 columns of 512 with 1e-3 m vertical gaps, over a static mesh ground of "
                  "512 x 512 vertices at 0.5 m (4 seeded sines, 2 m total amplitude); the pile settles kinematically")
@@ -222,7 +227,9 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
     if not O.available(32):
         raise RuntimeError("oracle/_ref/libb3ref32.so not built")
     rw = O.RefWorld(scene)
-    scene.set_local_centers(rw.local_centers())
+    # Both arms move the bodies with the scene's own centres of mass, so the
+    # reference sees the transforms the device pass sees.
+    rw.set_local_centers(scene.local_center)
     drv = S.KinematicDriver(scene, walls=walls)
     rw.first_pass()
     for _ in range(warmup):
@@ -246,6 +253,11 @@ def reference_run(scene, passes, seconds_cap=None, warmup=0, walls=None):
 def run_reference_arm(args, rank, world, dist):
     if rank != 0:
         return
+    # Scenes are built with the pure-Python hull builder here, so this process
+    # maps no library of this project: only the reference build in oracle/_ref.
+    from bounce_b200 import scene as S
+
+    S.NATIVE_HULLS = False
     if args.workload == "toi":
         sc, q = toi_setup(SEED)
         _, t = toi_reference(sc, q[:TOI_CPU_COUNT])
@@ -303,7 +315,9 @@ def run_reference_arm(args, rank, world, dist):
         return
     pile = args.workload == "pile"
     scene, walls = workload_scene(args, PILE_SEED if pile else SEED, sample=pile)
-    m, t, done = reference_run(scene, args.steps, warmup=args.warmup, walls=walls)
+    # The same pass window as the device arm: creation pass, W warm-up passes
+    # and the 2 passes that capture its graphs untimed, then K timed passes.
+    m, t, done = reference_run(scene, args.steps, warmup=args.warmup + GRAPH_PASSES, walls=walls)
     v = m / t if t > 0 else 0.0
     sample = (f"{done} passes of {PILE_SAMPLE}" if pile else
               f"{done} passes of the full workload")
@@ -362,7 +376,7 @@ def run_ours(args, rank, world, local, dist):
     scene, walls = workload_scene(args, (PILE_SEED if pile else SEED) + rank)
     drv = S.KinematicDriver(scene, walls=walls)
     # states: creation + warm-up, 2 passes that capture the tuned graphs, timed, profiled
-    t0_k = 1 + args.warmup + 2
+    t0_k = 1 + args.warmup + GRAPH_PASSES
     n_dev = t0_k + args.steps + args.profile_steps
     e2e_warm = 2  # untimed host-state passes: they capture the pinned-state graphs
     total = n_dev + e2e_warm + args.e2e_steps
@@ -509,7 +523,8 @@ def run_ours(args, rank, world, local, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             ref_scene, ref_walls = workload_scene(args, PILE_SEED if pile else SEED, sample=pile)
-            m, t, done = reference_run(ref_scene, 50, seconds_cap=args.cpu_seconds, walls=ref_walls)
+            m, t, done = reference_run(ref_scene, 50, seconds_cap=args.cpu_seconds,
+                                       warmup=args.warmup + GRAPH_PASSES, walls=ref_walls)
             what = PILE_SAMPLE if pile else "the same workload"
             cpu = {"value": m / t, "unit": "manifolds/s", "cores": 1, "kind": "reference",
                    "sample": f"{done} passes of {what} (creation pass excluded) on 1 host core; "
@@ -522,8 +537,8 @@ def run_ours(args, rank, world, local, dist):
             "metric": "manifolds/s", "value": value, "unit": "manifolds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": config_dict(args, {"contacts_last_pass": c["contacts"], "touching_last_pass": c["touching"],
-                                          "points_last_pass": c["points"]}),
+            "config": config_dict(args),
+            "counts_last_pass": {"contacts": c["contacts"], "touching": c["touching"], "points": c["points"]},
             "e2e": {"value": e2e_value, "unit": "manifolds/s", "h2d_bytes_per_step": e2e_h2d // max(args.e2e_steps, 1),
                     "d2h_bytes_per_step": e2e_d2h // max(args.e2e_steps, 1), "steps": args.e2e_steps,
                     "host_ms_per_step": {"collide": 1e3 * host_s[0] / args.e2e_steps,

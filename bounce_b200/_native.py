@@ -206,6 +206,7 @@ EXPORTED = [
     "b3g_mesh_wings",
     "b3g_collide",
     "b3g_get_counts",
+    "b3g_get_pass_stats",
     "b3g_fetch_contacts",
     "b3g_fetch_manifolds",
     "b3g_fetch_touching",
@@ -285,6 +286,7 @@ def load():
         "b3g_mesh_wings": ([ctx, ctypes.c_uint32, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_collide": ([ctx, vp, ctypes.c_int, vp], ctypes.c_int),
         "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
+        "b3g_get_pass_stats": ([ctx, _p(ctypes.c_uint32), ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_contacts": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),

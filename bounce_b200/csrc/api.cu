@@ -1617,6 +1617,32 @@ extern "C" int b3g_get_counts(b3g_ctx* c, b3g_counts* out)
 	return B3G_OK;
 }
 
+extern "C" int b3g_get_pass_stats(b3g_ctx* c, uint32_t* out, uint32_t capacity)
+{
+	if (!c || !out)
+		return fail(c, B3G_E_INVALID, "b3g_get_pass_stats: null argument");
+	int rc = sync_counts(c);
+	if (rc)
+		return rc;
+	const uint32_t* h = c->hCounters;
+	uint32_t s[B3G_STAT_COUNT];
+	s[B3G_STAT_RAW_PAIRS] = h[CTR_RAW];
+	s[B3G_STAT_KEPT] = h[CTR_KEPT];
+	s[B3G_STAT_HULL_MISS] = h[CTR_HULL_MISS];
+	s[B3G_STAT_TRAV_OVERFLOW] = h[CTR_TRAV_OVERFLOW];
+	s[B3G_STAT_MESH_ITEMS] = h[CTR_MESH_PAIRS];
+	s[B3G_STAT_WAKE_EVENTS] = h[CTR_WAKE_EVENTS];
+	s[B3G_STAT_WAKE_ACTIVATED] = h[CTR_WAKE_ACTIVATED];
+	s[B3G_STAT_LATE_DESTROYED] = h[CTR_LATE_DESTROYED];
+	s[B3G_STAT_ASLEEP] = h[CTR_ASLEEP];
+	static_assert(B3G_STAT_BUCKET0 + BK_COUNT == B3G_STAT_COUNT, "one statistic per bucket");
+	for (uint32_t b = 0; b < BK_COUNT; ++b)
+		s[B3G_STAT_BUCKET0 + b] = h[CTR_BUCKET0 + b];
+	uint32_t n = std::min<uint32_t>(capacity, B3G_STAT_COUNT);
+	std::memcpy(out, s, sizeof(uint32_t) * n);
+	return (int)n;
+}
+
 static int contacts_now(b3g_ctx* c, uint32_t& n)
 {
 	if (!c->havePass)

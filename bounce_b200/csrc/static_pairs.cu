@@ -166,6 +166,11 @@ extern "C" int b3g_find_pairs_static(const float* aabbs, uint32_t n, uint32_t* p
 		return B3G_E_CAPACITY;
 	if (!count || (n && (!aabbs || (capacity && !pairs))))
 		return B3G_E_INVALID;
+	// An error left pending by earlier work on this thread is not this call's:
+	// leave it for its owner to read and run nothing. Past this check, a
+	// launch error belongs to the launch just made.
+	if (cudaPeekAtLastError() != cudaSuccess)
+		return B3G_E_CUDA;
 	int dev = 0;
 	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
 		return B3G_E_CUDA;
@@ -196,8 +201,14 @@ extern "C" int b3g_find_pairs_static(const float* aabbs, uint32_t n, uint32_t* p
 		cudaFuncSetAttribute(k_sp_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
 		return B3G_E_CUDA;
 	k_sp_sort<<<1, SP_SORT_THREADS, smem, s>>>(aabbs, n, sc);
+	if (cudaGetLastError() != cudaSuccess)
+		return B3G_E_CUDA;
 	k_sp_sweep<false><<<(n + 127) / 128, 128, 0, s>>>(aabbs, n, sc, pairs, capacity);
+	if (cudaGetLastError() != cudaSuccess)
+		return B3G_E_CUDA;
 	k_sp_scan<<<1, 1024, 0, s>>>(n, sc, count);
+	if (cudaGetLastError() != cudaSuccess)
+		return B3G_E_CUDA;
 	k_sp_sweep<true><<<(n + 127) / 128, 128, 0, s>>>(aabbs, n, sc, pairs, capacity);
 	if (cudaGetLastError() != cudaSuccess)
 		return B3G_E_CUDA;

@@ -108,6 +108,22 @@ class CollisionPipeline:
         self._check(self.lib.b3g_get_counts(self.ctx, ctypes.byref(c)))
         return c.as_dict()
 
+    STAT_NAMES = ("raw_pairs", "kept", "hull_miss", "trav_overflow", "mesh_items", "wake_events", "wake_activated",
+                  "late_destroyed", "asleep")
+    BUCKET_NAMES = ("spheres", "capsule_sphere", "capsules", "triangle_sphere", "triangle_capsule", "hull_sphere",
+                    "hull_capsule", "hull_triangle", "hulls", "mesh", "sensor", "inactive", "apart")
+
+    def pass_stats(self):
+        """Inner counters of the last pass (b3g_get_pass_stats): named
+        statistics plus a 'buckets' dict of narrowphase bucket sizes."""
+        n = len(self.STAT_NAMES) + len(self.BUCKET_NAMES)
+        out = np.zeros(n, np.uint32)
+        k = self._check(self.lib.b3g_get_pass_stats(self.ctx, N.ptr(out, ctypes.c_uint32), n))
+        assert k == n, k
+        d = {name: int(out[i]) for i, name in enumerate(self.STAT_NAMES)}
+        d["buckets"] = {name: int(out[len(self.STAT_NAMES) + i]) for i, name in enumerate(self.BUCKET_NAMES)}
+        return d
+
     # -- results ----------------------------------------------------------
 
     def contacts(self):

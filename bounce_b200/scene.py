@@ -23,8 +23,14 @@ import os
 import numpy as np
 
 from . import _native as N
+from . import hull as H
 
 F = np.float32
+
+# Hull construction for scene input: the native builder in the CUDA library
+# (fast) or its pure-Python restatement in hull.py (the same arrays bit for
+# bit), for processes that must not map the CUDA library.
+NATIVE_HULLS = True
 
 # ---------------------------------------------------------------------------
 # float32 vector helpers with the reference's operation order.
@@ -105,6 +111,12 @@ class HullPool:
         return len(self.desc) - 1
 
     def add_points(self, pts):
+        if not NATIVE_HULLS:
+            try:
+                v, e, f, p, c, counts = H.hull_from_points(pts)
+            except ValueError:
+                raise ValueError("degenerate hull point set") from None
+            return self._add(v, e, f, p, c, counts)
         lib = N.load()
         pts = np.ascontiguousarray(pts, dtype=F)
         n = len(pts)
@@ -124,6 +136,8 @@ class HullPool:
         return self._add(v, e, f, p, c, counts)
 
     def add_box(self, ex, ey, ez):
+        if not NATIVE_HULLS:
+            return self._add(*H.hull_box(ex, ey, ez))
         lib = N.load()
         v = np.zeros(24, F)
         e = np.zeros(5 * 24, np.uint32)
@@ -662,7 +676,9 @@ def _pile_columns(job):
     """Worker: builds the hulls of a chunk of columns (seeded per chunk) and
     stacks them level by level; returns (packed hull arrays, heights
     (columns, per_column))."""
-    hull_seed, per_column, cx, cz, quats, gap, seed, amplitude, pts, axes = job
+    global NATIVE_HULLS
+    hull_seed, per_column, cx, cz, quats, gap, seed, amplitude, pts, axes, native = job
+    NATIVE_HULLS = native
     m = len(cx)
     arrays = _pile_hull_chunk((hull_seed, m * per_column, pts, axes))
     desc = arrays["desc"].reshape(-1, 6)
@@ -730,7 +746,7 @@ def pile_scene(seed=9, columns=512, per_column=512, grid=512, spacing=0.5, ampli
     for j, c0 in enumerate(range(0, columns, chunk_columns)):
         c1 = min(columns, c0 + chunk_columns)
         jobs.append((seed * 100003 + j, per_column, cx[c0:c1], cz[c0:c1],
-                     quats[c0 * per_column:c1 * per_column], gap, seed, amplitude, pts, axes))
+                     quats[c0 * per_column:c1 * per_column], gap, seed, amplitude, pts, axes, NATIVE_HULLS))
     workers = workers or min(len(jobs), os.cpu_count() or 1)
     if workers <= 1:
         parts = [_pile_columns(jb) for jb in jobs]

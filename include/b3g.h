@@ -250,6 +250,36 @@ int b3g_collide(b3g_ctx* ctx, const float* body_state, int state_on_device, void
 /* Waits for the last pass and returns its counters. */
 int b3g_get_counts(b3g_ctx* ctx, b3g_counts* out);
 
+/* Inner counters of the last pass, for diagnostics and work accounting: the
+ * overlapping pairs the broadphase found, previous contacts kept, hull-hull
+ * contacts the feature cache did not resolve (full SAT), traversal records
+ * past a leaf's scratch slots, mesh (contact, triangle) work items, wake-up
+ * events and the contacts they activated or destroyed, bodies asleep after
+ * the pass, and the size of each narrowphase bucket (one per b3Contact
+ * subclass of contact.cpp:256-267, then sensor, inactive and apart pairs).
+ * Writes min(capacity, B3G_STAT_COUNT) values; returns that number or a
+ * negative status. Waits for the pass. Counterpart of the reference's
+ * per-step collision statistics (b3_convexCalls, b3_gjkCalls and the like,
+ * world.cpp:191-199). */
+enum
+{
+	B3G_STAT_RAW_PAIRS = 0,
+	B3G_STAT_KEPT,
+	B3G_STAT_HULL_MISS,
+	B3G_STAT_TRAV_OVERFLOW,
+	B3G_STAT_MESH_ITEMS,
+	B3G_STAT_WAKE_EVENTS,
+	B3G_STAT_WAKE_ACTIVATED,
+	B3G_STAT_LATE_DESTROYED,
+	B3G_STAT_ASLEEP,
+	B3G_STAT_BUCKET0, /* 13 bucket sizes: spheres, capsule-sphere, capsules,
+	                     triangle-sphere, triangle-capsule, hull-sphere,
+	                     hull-capsule, hull-triangle, hulls, mesh, sensor,
+	                     inactive, apart */
+	B3G_STAT_COUNT = B3G_STAT_BUCKET0 + 13
+};
+int b3g_get_pass_stats(b3g_ctx* ctx, uint32_t* out, uint32_t capacity);
+
 /* Results ---------------------------------------------------------------- */
 
 /* Contacts of the last pass, 3 u32 each: fixtureA, fixtureB (after the
@@ -665,7 +695,10 @@ int b3g_contact_constraints(b3g_ctx* ctx, uint32_t count, const uint32_t* contac
  * 2 u32 each, up to capacity pairs, unspecified order) and the number of
  * overlapping pairs into *count (device memory; may exceed capacity).
  * Asynchronous on stream (a cudaStream_t, NULL for the legacy stream), on
- * the current device. Returns B3G_E_CAPACITY when n > B3G_STATIC_MAX_PROXIES.
+ * the current device. Returns B3G_E_CAPACITY when n > B3G_STATIC_MAX_PROXIES,
+ * and B3G_E_CUDA without running anything when a CUDA error of earlier work
+ * is pending on the calling thread (cudaPeekAtLastError; that error is left
+ * in place for its owner).
  *
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make that first call before any stream capture.

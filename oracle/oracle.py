@@ -12,7 +12,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_SRC = "/root/reference"
+# The reference checkout (Bounce sources) the oracle is compiled from: the
+# BOUNCE_REF_SRC environment variable, else the checkout's usual location.
+REFERENCE_SRC = os.environ.get("BOUNCE_REF_SRC", "/root/reference")
 
 # Harness dump records (ref_harness.cpp DumpPoint / DumpManifold / DumpContact).
 DPOINT = np.dtype(
@@ -44,7 +46,7 @@ DCONTACT = np.dtype(
 
 
 def build(quiet=True):
-    """Compile oracle/_ref from the reference sources (needs /root/reference)."""
+    """Compile oracle/_ref from the reference sources at REFERENCE_SRC."""
     if not os.path.isdir(REFERENCE_SRC):
         return False
     cmd = ["make", "-C", HERE, "-j8", f"REF={REFERENCE_SRC}"]
@@ -79,6 +81,7 @@ def lib(precision=32):
         "refw_destroy": ([vp], None),
         "refw_get_bodies": ([vp, f32p], None),
         "refw_set_sweeps": ([vp, f32p], None),
+        "refw_set_local_centers": ([vp, f32p], None),
         "refw_set_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
         "refw_get_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
         "refw_set_triangle_wings": ([vp, ctypes.c_uint32, u32p, f32p], None),
@@ -222,6 +225,13 @@ class RefWorld:
 
     def local_centers(self):
         return self.bodies17().reshape(-1, 17)[:, 14:17].copy()
+
+    def set_local_centers(self, lc):
+        """Use the caller's centres of mass (n x 3, body frame) for the
+        dynamic bodies instead of the ones the reference computed."""
+        a = np.ascontiguousarray(lc, np.float32).reshape(-1)
+        assert len(a) == 3 * self.scene.n_bodies
+        self.L.refw_set_local_centers(self.w, _p(a, ctypes.c_float))
 
     def set_sweeps(self, sweeps14):
         a = np.ascontiguousarray(sweeps14, np.float32)

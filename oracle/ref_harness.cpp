@@ -492,6 +492,26 @@ REF_API void refw_get_bodies(void* p, float* out)
 	}
 }
 
+// 3 floats per body: the centre of mass in body frame. Sets each dynamic
+// body's m_sweep.localCenter and its world centres from the current
+// transform, as b3Body::ResetMass ends (body.cpp:370-372), so that a caller
+// whose scene computed the centres itself drives the reference's sweeps with
+// the same transforms. Mass and inertia stay as the reference computed them
+// (the collision pass reads neither).
+REF_API void refw_set_local_centers(void* p, const float* lc)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (size_t i = 0; i < w->bodies.size(); ++i)
+	{
+		b3Body* b = w->bodies[i];
+		if (b->m_type != e_dynamicBody)
+			continue;
+		b->m_sweep.localCenter.Set(lc[3 * i + 0], lc[3 * i + 1], lc[3 * i + 2]);
+		b->m_sweep.worldCenter = b3Mul(b->m_xf, b->m_sweep.localCenter);
+		b->m_sweep.worldCenter0 = b->m_sweep.worldCenter;
+	}
+}
+
 // 14 floats per body: worldCenter0(3), orientation0(4), worldCenter(3), orientation(4).
 // Static bodies are skipped (their sweep never changes in the reference).
 REF_API void refw_set_sweeps(void* p, const float* in)

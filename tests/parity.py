@@ -112,3 +112,77 @@ def compare_fat_aabbs(pipe, rw, label=""):
     b = rw.fat_aabbs()
     bad = np.nonzero(~np.all(a == b, axis=1))[0]
     assert len(bad) == 0, f"{label}: fat AABBs differ at {len(bad)} proxies, e.g. {a[bad[:2]]} vs {b[bad[:2]]}"
+
+
+class BatchedPass:
+    """One pass's results of a many-world pipeline, fetched once, from which
+    WorldView gives each world's part in the shape of a one-world pipeline."""
+
+    def __init__(self, pipe, scene):
+        self.c = pipe.contacts()
+        self.m = pipe.manifolds()
+        self.cache = pipe.caches()
+        self.fat = pipe.fat_aabbs()
+        self.end = pipe.ended()
+        self.fix_world = scene.body_world[scene.fix_body]
+        self.n_fixtures = scene.n_fixtures
+
+
+class WorldView:
+    """World w of a BatchedPass with fixture indices local to the world (the
+    indices of world_subset(w)), in the world's own list order."""
+
+    def __init__(self, bp, w, fixtures):
+        local = np.full(bp.n_fixtures, -1, np.int64)
+        local[fixtures] = np.arange(len(fixtures))
+        sel = bp.fix_world[bp.c[:, 0]] == w
+        c = bp.c[sel].astype(np.int64)
+        c[:, 0] = local[c[:, 0]]
+        c[:, 1] = local[c[:, 1]]
+        self._c = c.astype(np.uint32)
+        self._m = bp.m[sel]
+        self._cache = bp.cache[sel]
+        self._fat = bp.fat[fixtures]
+        if len(bp.end):
+            e = bp.end[bp.fix_world[bp.end[:, 0]] == w].astype(np.int64)
+            e[:, 0] = local[e[:, 0]]
+            e[:, 1] = local[e[:, 1]]
+        else:
+            e = np.zeros((0, 3), np.int64)
+        self._e = e.astype(np.uint32)
+
+    def contacts(self):
+        return self._c
+
+    def manifolds(self):
+        return self._m
+
+    def caches(self):
+        return self._cache
+
+    def fat_aabbs(self):
+        return self._fat
+
+    def ended(self):
+        return self._e
+
+
+def compare_order(pipe, rw, label):
+    """The contact arrays follow the reference's contact list exactly:
+    fixtures, touching flag and manifold count per position."""
+    g = pipe.contacts()
+    r = rw.pairs()
+    assert len(g) == len(r), f"{label}: {len(g)} contacts vs {len(r)}"
+    bad = np.nonzero(np.any(g[:, :2] != r[:, :2], axis=1))[0]
+    assert len(bad) == 0, f"{label}: list order differs at {len(bad)} positions, first {bad[:5]}: {g[bad[:3]]} vs {r[bad[:3]]}"
+    assert np.array_equal(g[:, 2] & 0xFF01, r[:, 2] & 0xFF01), f"{label}: flags differ in list order"
+
+
+def compare_ended(pipe, prev, cur, label):
+    """The contacts destroyed by the pass, in the previous list's order, with
+    their touching flags (prev, cur: the reference's lists before and after)."""
+    ck = set(map(tuple, cur[:, :2].tolist()))
+    want = np.array([r for r in prev.tolist() if (r[0], r[1]) not in ck], np.uint32).reshape(-1, 3)
+    got = pipe.ended()
+    assert np.array_equal(got[:, :2], want[:, :2]), f"{label}: ended list"
+    assert np.array_equal(got[:, 2] & 1, want[:, 2] & 1), f"{label}: ended touching flags"

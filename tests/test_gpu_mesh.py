@@ -13,7 +13,7 @@ import pytest
 from bounce_b200 import scene as S
 from bounce_b200.pipeline import CollisionPipeline
 from tests.parity import compare_contacts, compare_fat_aabbs
-from tests.test_gpu_parity import compare_order
+from tests.parity import compare_order
 
 pytestmark = pytest.mark.gpu
 

@@ -6,7 +6,7 @@ import pytest
 
 from bounce_b200 import scene as S
 from bounce_b200.pipeline import CollisionPipeline
-from tests.parity import compare_contacts, compare_fat_aabbs
+from tests.parity import compare_contacts, compare_fat_aabbs, compare_order
 
 pytestmark = pytest.mark.gpu
 
@@ -56,17 +56,6 @@ def test_mixed_passes(oracle_mod):
     sc = S.mixed_scene(seed=7, n=3000, side=18.0).finalize()
     st = run_parity(oracle_mod, sc, 8, "mixed")
     assert st[-1]["touching"] > 100
-
-
-def compare_order(pipe, rw, label):
-    """The contact arrays follow the reference's contact list exactly:
-    fixtures, touching flag and manifold count per position."""
-    g = pipe.contacts()
-    r = rw.pairs()
-    assert len(g) == len(r), f"{label}: {len(g)} contacts vs {len(r)}"
-    bad = np.nonzero(np.any(g[:, :2] != r[:, :2], axis=1))[0]
-    assert len(bad) == 0, f"{label}: list order differs at {len(bad)} positions, first {bad[:5]}: {g[bad[:3]]} vs {r[bad[:3]]}"
-    assert np.array_equal(g[:, 2] & 0xFF01, r[:, 2] & 0xFF01), f"{label}: flags differ in list order"
 
 
 def test_list_order(oracle_mod):
