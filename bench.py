@@ -349,6 +349,42 @@ def algorithmic_bytes(scene, counts):
     return int(scene.n_fixtures * (68 + 60 + 64 + 1) + hv)
 
 
+def broadphase_bytes(scene, counts):
+    """Algorithmic HBM bytes of one pass's broadphase (sync, sort, build,
+    traversal, contact begin/end), by the formula
+        N (2 x 28 [xf0, xf1] + 24 [old fat AABB] + 24 [new fat AABB] + 1 [moved])
+      + 12 per hull vertex of the hull fixtures (read once)
+      + 2 N 12 [sort keys and ids, one read and one write]
+      + (2N - 1) 32 [tree nodes written: box 24 + two child ids]
+      + 8 P [contacts out] + 8 P_prev [previous contacts looked up]
+      + 8 (P_begin + P_end) [begun and ended lists]
+    with N proxies and P the contacts of the pass (P_prev = P - begun + ended)."""
+    n = scene.n_fixtures
+    ha = scene.hull_arrays
+    desc = ha["desc"].reshape(-1, 6)
+    hull_fix = scene.fix_type == 3
+    hv = int(desc[scene.fix_hull[hull_fix], 1].sum())
+    p = counts["contacts"]
+    p_prev = p - counts["begun"] + counts["ended"]
+    return int(n * (2 * 28 + 24 + 24 + 1) + 12 * hv + 2 * n * 12 + (2 * n - 1) * 32 + 8 * p + 8 * p_prev
+               + 8 * (counts["begun"] + counts["ended"]))
+
+
+def committed_flops(args):
+    """Mean algorithmic narrowphase flops per pass of the timed window, as
+    counted in the reference's FP64 build on this workload (written by
+    oracle/count_flops.py to profiles/narrowphase_flops_mixed65536.md)."""
+    if args.workload != "mixed" or args.bodies != N_BODIES:
+        return None
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "narrowphase_flops_mixed65536.md")):
+            if line.startswith("flops_per_pass_mean |"):
+                return float(line.split("|")[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def committed_traffic(kernel, args, label="mixed 65,536"):
     """DRAM bytes per launch of `kernel` from the committed ncu summary
     (profiles/roofline_traffic.md), for the workload it was captured on."""
@@ -443,6 +479,7 @@ def run_ours(args, rank, world, local, dist):
         pipe.set_profiling(False)
         assert pipe.counts()["status"] == 0
 
+    pass_stats = pipe.pass_stats()
     ms_max, manifolds_all = replica_totals(dist, dev, ms, tot["manifolds"])
     value = manifolds_all / (ms_max / 1000.0)
 
@@ -501,23 +538,52 @@ def run_ours(args, rank, world, local, dist):
         e2e_max, e2e_all = replica_totals(dist, dev, e2e_s, e2e_m)
         e2e_value = e2e_all / e2e_max
 
-    # Roofline of the dominant stage.
-    roof = None
+    # Rooflines. The narrowphase (its kernels are most of a pass) is bound by
+    # the FP32 pipe: algorithmic flops of the pass (counted in the reference's
+    # FP64 build on this workload) over the narrowphase stages' time, against
+    # one FP32 operation per lane per clock (multiplies and adds are separate
+    # instructions here: -fmad=false keeps the reference's rounding), at the
+    # SM clock sampled during the timed region. The broadphase is bound by HBM:
+    # its algorithmic bytes over the time of its stages.
+    roof = roof_bp = roof_sync = None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     stage_ms = {k: v[0] / max(v[1], 1) for k, v in prof.items()}
     if stage_ms:
+        props = torch.cuda.get_device_properties(dev)
+        mhz = float(clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0) if isinstance(clocks, dict) else 1965.0
+        fp32_peak = props.multi_processor_count * 128 * mhz * 1e6 / 1e12
+        narrow_ms = sum(stage_ms.get(k, 0.0) for k in ("bucket", "narrow_hulls", "narrow_convex", "narrow_mesh"))
+        fl = committed_flops(args)
+        if fl and narrow_ms > 0:
+            ach = fl / (narrow_ms / 1000.0) / 1e12
+            roof = {"kernel": "narrowphase: k_bucket, k_hulls_probe, k_hulls_sat, k_hull_triangle, k_apart, k_convex<0-6>, "
+                              "sensor/inactive (profiled passes, one stream)",
+                    "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                    "traffic": None, "flops_per_pass": fl, "narrow_ms_per_pass": narrow_ms,
+                    "peak_source": f"{props.multi_processor_count} SMs x 128 FP32 lanes x {mhz:.0f} MHz (sampled SM clock); "
+                                   "an FMA-counted peak is twice this",
+                    "flops_source": "profiles/narrowphase_flops_mixed65536.md (oracle/count_flops.py)"}
+        bp_ms = sum(stage_ms.get(k, 0.0) for k in ("sync", "sort", "build", "traverse", "diff"))
+        bb = broadphase_bytes(scene, c)
+        if bp_ms > 0:
+            ach = bb / (bp_ms / 1000.0) / 1e9
+            roof_bp = {"kernel": "broadphase: k_sync, bounds/Morton/one-sweep sort, k_build/k_leaves/k_refit, "
+                                 "k_traverse_count/emit/overflow, hash diff and list-order layout",
+                       "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                       "traffic": None, "algorithmic_bytes_per_pass": bb, "ms_per_pass": bp_ms, "peak_source": hbm_src}
         sync_ms = stage_ms.get("sync", 0.0)
         sb = algorithmic_bytes(scene, c)
-        achieved = sb / (sync_ms / 1000.0) / 1e9 if sync_ms > 0 else 0.0
-        roof = {"kernel": "k_sync (fat-AABB update)", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": committed_traffic("k_sync", args),
-                "algorithmic_bytes_per_launch": sb,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650 GB/s"}
+        if sync_ms > 0:
+            ach = sb / (sync_ms / 1000.0) / 1e9
+            roof_sync = {"kernel": "k_sync (fat-AABB update)", "bound": "hbm", "achieved": ach, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": ach / hbm_peak, "traffic": committed_traffic("k_sync", args),
+                         "algorithmic_bytes_per_launch": sb, "peak_source": hbm_src}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -550,7 +616,10 @@ def run_ours(args, rank, world, local, dist):
             "pairs_per_s": tot["contacts"] / (ms / 1000.0),
             "points_per_s": tot["points"] / (ms / 1000.0),
             "stage_ms": stage_ms,
+            "pass_stats": pass_stats,
             "roofline": roof,
+            "roofline_broadphase": roof_bp,
+            "roofline_sync": roof_sync,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

@@ -23,6 +23,7 @@ BODY_STATIC, BODY_KINEMATIC, BODY_DYNAMIC = 0, 1, 2
 FLAG_WARM_STARTING = 1
 FLAG_CONVEX_CACHE = 2
 FLAG_GRAPH = 4
+FLAG_CONTACT_FILTER = 8
 TUNE_CONVEX, TUNE_PROBE, TUNE_SAT_WARPS, TUNE_SAT_BLOCKS, TUNE_TRAVERSE, TUNE_COUNT = 0, 9, 10, 11, 12, 13
 FIXTURE_SENSOR = 1
 
@@ -207,6 +208,10 @@ EXPORTED = [
     "b3g_collide",
     "b3g_get_counts",
     "b3g_get_pass_stats",
+    "b3g_set_joint_pairs",
+    "b3g_set_contact_veto",
+    "b3g_fetch_new_pairs",
+    "b3g_finish_pass",
     "b3g_fetch_contacts",
     "b3g_fetch_manifolds",
     "b3g_fetch_touching",
@@ -287,6 +292,10 @@ def load():
         "b3g_collide": ([ctx, vp, ctypes.c_int, vp], ctypes.c_int),
         "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
         "b3g_get_pass_stats": ([ctx, _p(ctypes.c_uint32), ctypes.c_uint32], ctypes.c_int),
+        "b3g_set_joint_pairs": ([ctx, ctypes.c_uint32, _p(ctypes.c_uint32)], ctypes.c_int),
+        "b3g_set_contact_veto": ([ctx, ctypes.c_uint32, _p(ctypes.c_uint8)], ctypes.c_int),
+        "b3g_fetch_new_pairs": ([ctx, _p(ctypes.c_uint32), ctypes.c_uint32], ctypes.c_int),
+        "b3g_finish_pass": ([ctx, _p(ctypes.c_uint8), ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_contacts": ([ctx, u32p, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_manifolds": ([ctx, vp, ctypes.c_uint32], ctypes.c_int),
         "b3g_fetch_touching": ([ctx, u32p, vp, ctypes.c_uint32], ctypes.c_int),

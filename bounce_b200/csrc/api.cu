@@ -240,10 +240,16 @@ static const char* kStageNames[PROF_STAGES] = {
 	"build",         // Karras tree, leaves, ropes, refit
 	"traverse",      // pair count, scan, pair write
 	"diff",          // persistent-pair hash, ended contacts
-	"narrow_convex", // buckets + sphere/capsule/hull-sphere/hull-capsule/sensor
-	"narrow_hulls",  // hull-hull SAT
+	"bucket",        // narrowphase buckets (and the mesh midphase)
+	"narrow_hulls",  // hull-hull and hull-triangle kernels
+	"narrow_convex", // apart, sphere/capsule/hull-sphere/hull-capsule/sensor/inactive kernels
+	"narrow_mesh",   // mesh work items and clustering
 	"finalize",      // counters, contact records
 };
+// Under profiling every kernel of a pass runs on the pass's stream, one after
+// the other, so that each stage's events enclose its own kernels; without
+// profiling the hull and mesh stages overlap the convex stage on their own
+// streams, and a pass takes less than the sum of the stages.
 
 void prof_mark(b3g_ctx* c, int mark, cudaStream_t s)
 {
@@ -406,6 +412,19 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->launches = 0;
 	c->profPass = c->profHarvest = 0;
 	c->profEvents = nullptr;
+	c->dJointKeys = nullptr;
+	c->nJoints = c->jointCap = 0;
+	c->dBodyJoint = nullptr;
+	c->bodyJointCap = 0;
+	c->dVetoPrev = nullptr;
+	c->nVeto = 0;
+	c->dRawDrop = nullptr;
+	c->dCand = nullptr;
+	c->dCandPairs = nullptr;
+	c->nCand = 0;
+	c->candFetched = false;
+	c->passOpen = false;
+	c->filterMode = 0;
 	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
 	{
 		delete c;
@@ -631,6 +650,12 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	}
 	dfree(c->dWorldCounts);
 	dfree(c->dUpdateBad);
+	dfree(c->dJointKeys);
+	dfree(c->dBodyJoint);
+	dfree(c->dVetoPrev);
+	dfree(c->dRawDrop);
+	dfree(c->dCand);
+	dfree(c->dCandPairs);
 	if (c->hCounters)
 		cudaFreeHost(c->hCounters);
 	if (c->copyStream)
@@ -819,6 +844,9 @@ extern "C" int b3g_set_bodies(b3g_ctx* c, uint32_t nb, const uint32_t* world, co
 	c->scene.bodyState = c->dBodyState;
 	c->creationPass = true;
 	c->havePass = false;
+	// Joints and a contact veto name bodies and contacts of the old scene.
+	c->nJoints = 0;
+	c->nVeto = 0;
 	return B3G_OK;
 }
 
@@ -1425,6 +1453,14 @@ extern "C" int b3g_fetch_awake(b3g_ctx* c, uint8_t* out, uint32_t capacity)
 	return (int)c->nBodies;
 }
 
+// The contact list and the narrowphase of a pass whose broadphase has run.
+static void issue_pass_rest(b3g_ctx* c, cudaStream_t s)
+{
+	launch_pairs_diff(c, s);
+	prof_mark(c, PM_DIFFED, s);
+	launch_narrowphase(c, s);
+}
+
 // Kernels of one pass up to the narrowphase, on s (profiling marks when on).
 // While s is being captured, *copyNode receives the state copy's graph node.
 static void issue_pass(b3g_ctx* c, cudaStream_t s, const float* state, size_t bytes, cudaMemcpyKind kind,
@@ -1446,9 +1482,14 @@ static void issue_pass(b3g_ctx* c, cudaStream_t s, const float* state, size_t by
 	launch_sync(c, s);
 	prof_mark(c, PM_SYNCED, s);
 	launch_broadphase(c, s);
-	launch_pairs_diff(c, s);
-	prof_mark(c, PM_DIFFED, s);
-	launch_narrowphase(c, s);
+	if (c->filterMode == 2)
+	{
+		// The caller's contact filter decides the new pairs before the
+		// contact list is built: the pass stops here (b3g_finish_pass).
+		launch_candidates(c, s);
+		return;
+	}
+	issue_pass_rest(c, s);
 }
 
 // Work that rewrites the contact records or the touching output waits for
@@ -1484,8 +1525,19 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 		else
 			cudaGetLastError();
 	}
+	if (c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_collide: the last pass waits for b3g_finish_pass");
+	// Filters of this pass: the caller's contact filter (a host round trip in
+	// the middle of the pass), else joints or a contact veto (inside the pass).
+	c->filterMode = (c->cfg.flags & B3G_FLAG_CONTACT_FILTER) ? 2 : ((c->nJoints || c->nVeto) ? 1 : 0);
+	if (c->filterMode == 2 && (!c->dRawDrop || !c->dCand || !c->dCandPairs))
+	{
+		CK(dalloc(&c->dRawDrop, c->cfg.max_contacts));
+		CK(dalloc(&c->dCand, c->cfg.max_contacts));
+		CK(dalloc(&c->dCandPairs, c->cfg.max_contacts));
+	}
 	const bool graph = (c->cfg.flags & B3G_FLAG_GRAPH) && (onDevice || pinnedHost) && !c->profiling &&
-		c->asleep == 0 && c->havePass && !c->creationPass && s != nullptr;
+		c->asleep == 0 && c->havePass && !c->creationPass && s != nullptr && c->filterMode == 0;
 	c->lastPassImpulses = c->impulsesLoaded;
 	if (graph)
 	{
@@ -1546,6 +1598,16 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 		if (c->havePass)
 			c->cur ^= 1u;
 		issue_pass(c, s, state, bytes, kind);
+		if (c->filterMode == 2)
+		{
+			c->passOpen = true;
+			c->candFetched = false;
+			c->passStream = s;
+			// pass begin, sync, broadphase, candidates; the rest in b3g_finish_pass
+			c->launches += 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) + 2;
+			CK(cudaGetLastError());
+			return B3G_OK;
+		}
 		if (c->asleep > 0)
 		{
 			int rc = resolve_wakeups(c, s);
@@ -1563,6 +1625,168 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	c->creationPass = false;
 	c->havePass = true;
 	c->impulsesLoaded = false;
+	c->nVeto = 0;
+	return B3G_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Collision filters.
+
+static int sync_counts(b3g_ctx* c);
+
+extern "C" int b3g_set_joint_pairs(b3g_ctx* c, uint32_t count, const uint32_t* bodyPairs)
+{
+	if (!c || (count && !bodyPairs))
+		return fail(c, B3G_E_INVALID, "b3g_set_joint_pairs: null argument");
+	if (c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_set_joint_pairs: the last pass waits for b3g_finish_pass");
+	if (c->nBodies == 0)
+		return fail(c, B3G_E_STATE, "b3g_set_joint_pairs: no bodies");
+	CK(cudaSetDevice(c->device));
+	std::vector<unsigned long long> keys;
+	keys.reserve(count);
+	std::vector<uint8_t> flag(c->nBodies, 0);
+	for (uint32_t i = 0; i < count; ++i)
+	{
+		uint32_t a = bodyPairs[2 * i], b = bodyPairs[2 * i + 1];
+		if (a >= c->nBodies || b >= c->nBodies || a == b)
+			return fail(c, B3G_E_INVALID, "b3g_set_joint_pairs: pair %u (%u, %u) is not two bodies of the scene", i,
+				a, b);
+		keys.push_back(a < b ? ((unsigned long long)a << 32) | b : ((unsigned long long)b << 32) | a);
+		flag[a] = flag[b] = 1;
+	}
+	std::sort(keys.begin(), keys.end());
+	keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+	CK(cudaStreamSynchronize(c->stream));
+	if (keys.size() > c->jointCap)
+	{
+		dfree(c->dJointKeys);
+		CK(dalloc(&c->dJointKeys, keys.size()));
+		c->jointCap = (uint32_t)keys.size();
+	}
+	const uint32_t nb = std::max(c->capBodies, c->nBodies);
+	if (c->bodyJointCap < nb)
+	{
+		dfree(c->dBodyJoint);
+		CK(dalloc(&c->dBodyJoint, nb));
+		c->bodyJointCap = nb;
+	}
+	flag.resize(nb, 0);
+	if (!keys.empty())
+		CK(cudaMemcpy(c->dJointKeys, keys.data(), sizeof(unsigned long long) * keys.size(), cudaMemcpyHostToDevice));
+	CK(cudaMemcpy(c->dBodyJoint, flag.data(), flag.size(), cudaMemcpyHostToDevice));
+	c->nJoints = (uint32_t)keys.size();
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_contact_veto(b3g_ctx* c, uint32_t count, const uint8_t* veto)
+{
+	if (!c || (count && !veto))
+		return fail(c, B3G_E_INVALID, "b3g_set_contact_veto: null argument");
+	if (c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_set_contact_veto: the last pass waits for b3g_finish_pass");
+	int rc = sync_counts(c);
+	if (rc)
+		return rc;
+	uint32_t n = std::min(c->hCounters[CTR_PAIRS], c->cfg.max_contacts);
+	if (!c->havePass || count != n)
+		return fail(c, B3G_E_INVALID, "b3g_set_contact_veto: %u flags for %u contacts of the last pass", count, n);
+	if (!c->dVetoPrev)
+		CK(dalloc(&c->dVetoPrev, c->cfg.max_contacts));
+	if (count)
+		CK(cudaMemcpy(c->dVetoPrev, veto, count, cudaMemcpyHostToDevice));
+	c->nVeto = count;
+	return B3G_OK;
+}
+
+extern "C" int b3g_fetch_new_pairs(b3g_ctx* c, uint32_t* out, uint32_t capacity)
+{
+	if (!c || (capacity && !out))
+		return fail(c, B3G_E_INVALID, "b3g_fetch_new_pairs: null argument");
+	if (!c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_fetch_new_pairs: no pass waits for the contact filter");
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = c->passStream;
+	uint32_t n = 0;
+	CK(cudaMemcpyAsync(&n, c->buf.counters + CTR_CANDIDATES, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+	CK(cudaStreamSynchronize(s));
+	n = std::min(n, c->cfg.max_contacts);
+	std::vector<uint4> rec(n);
+	std::vector<uint32_t> raw(n);
+	if (n)
+	{
+		launch_candidate_pairs(c, n, s);
+		++c->launches;
+		CK(cudaMemcpyAsync(rec.data(), c->dCandPairs, sizeof(uint4) * n, cudaMemcpyDeviceToHost, s));
+		CK(cudaMemcpyAsync(raw.data(), c->dCand, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+		CK(cudaStreamSynchronize(s));
+	}
+	// AddPair order: the pairs FindPairs reports, ascending by (smaller proxy
+	// key, larger proxy key) (broad_phase.h:181-206).
+	std::vector<uint32_t> order(n);
+	for (uint32_t i = 0; i < n; ++i)
+		order[i] = i;
+	std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+		return rec[x].z != rec[y].z ? rec[x].z < rec[y].z : rec[x].w < rec[y].w;
+	});
+	c->hCandOrder.resize(n);
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		c->hCandOrder[i] = raw[order[i]];
+		if (i < capacity)
+		{
+			out[2 * i + 0] = rec[order[i]].x;
+			out[2 * i + 1] = rec[order[i]].y;
+		}
+	}
+	c->nCand = n;
+	c->candFetched = true;
+	return (int)n;
+}
+
+extern "C" int b3g_finish_pass(b3g_ctx* c, const uint8_t* keep, uint32_t count)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if (!c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_finish_pass: no pass waits for the contact filter");
+	if (keep && (!c->candFetched || count != c->nCand))
+		return fail(c, B3G_E_INVALID, "b3g_finish_pass: %u flags for %u new pairs (b3g_fetch_new_pairs first)", count,
+			c->candFetched ? c->nCand : 0u);
+	CK(cudaSetDevice(c->device));
+	cudaStream_t s = c->passStream;
+	std::vector<uint32_t> rejected;
+	if (keep)
+		for (uint32_t i = 0; i < count; ++i)
+			if (!keep[i])
+				rejected.push_back(c->hCandOrder[i]);
+	uint32_t* dRejected = reinterpret_cast<uint32_t*>(c->dCandPairs);
+	if (!rejected.empty())
+	{
+		// From pageable memory: the call returns once the host buffer is read.
+		CK(cudaMemcpyAsync(dRejected, rejected.data(), sizeof(uint32_t) * rejected.size(), cudaMemcpyHostToDevice, s));
+		launch_apply_veto(c, dRejected, (uint32_t)rejected.size(), s);
+	}
+	c->passOpen = false;
+	issue_pass_rest(c, s);
+	if (c->asleep > 0)
+	{
+		int rc = resolve_wakeups(c, s);
+		if (rc)
+			return fail(c, rc, "b3g_finish_pass: wake-up rounds failed: %s", cudaGetErrorString(cudaGetLastError()));
+	}
+	wait_copies(c, s);
+	launch_finalize(c, s);
+	prof_mark(c, PM_FINAL, s);
+	if (c->profiling)
+		++c->profPass;
+	c->launches += pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3 +
+		(rejected.empty() ? 0 : 1);
+	CK(cudaGetLastError());
+	c->creationPass = false;
+	c->havePass = true;
+	c->impulsesLoaded = false;
+	c->nVeto = 0;
 	return B3G_OK;
 }
 
@@ -1589,6 +1813,8 @@ extern "C" int b3g_get_counts(b3g_ctx* c, b3g_counts* out)
 {
 	if (!c || !out)
 		return fail(c, B3G_E_INVALID, "b3g_get_counts: null argument");
+	if (c->passOpen)
+		return fail(c, B3G_E_INVALID, "b3g_get_counts: the last pass waits for b3g_finish_pass");
 	int rc = sync_counts(c);
 	if (rc)
 		return rc;

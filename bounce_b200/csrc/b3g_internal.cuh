@@ -228,6 +228,46 @@ struct Buffers
 	float* impulseMotor;
 };
 
+// Collision filters beyond the shape-type rules, decided pass by pass: joints
+// that keep their bodies from colliding (b3Body::ShouldCollide, body.cpp:240-263)
+// and the caller's contact filter (b3ContactFilter::ShouldCollide, called by
+// AddPair, contact_manager.cpp:86-92, and for every contact by UpdateContacts,
+// :189-199). mode 0: none (the default pass); 1: joints and the per-contact
+// veto applied inside k_diff / k_kept; 2: as 1, plus new pairs the caller's
+// filter rejected, precomputed per overlapping pair in rawDrop.
+// With a filter in use a new contact also needs a proxy that moved this pass
+// (was re-inserted or created): FindPairs reports only pairs of moved proxies
+// (broad_phase.h:158-207), so a pair that a filter once refused stays no
+// contact until one of its proxies moves. Without filters every such pair is
+// already a contact, and the rule changes nothing.
+struct FilterArgs
+{
+	int mode;
+	const unsigned long long* jointKeys; // sorted (smaller body << 32 | larger body)
+	uint32_t nJoints;
+	const uint8_t* bodyJoint;            // per body: in some joint pair
+	const uint8_t* vetoPrev;             // per contact of the previous pass: destroy it
+	uint32_t nVeto;
+	uint8_t* rawDrop;                    // per overlapping pair of the pass: no contact (mode 2)
+};
+
+__device__ __forceinline__ bool joint_excluded(const FilterArgs& F, uint32_t ba, uint32_t bb)
+{
+	if (F.nJoints == 0 || !F.bodyJoint[ba] || !F.bodyJoint[bb])
+		return false;
+	unsigned long long k = ba < bb ? ((unsigned long long)ba << 32) | bb : ((unsigned long long)bb << 32) | ba;
+	uint32_t lo = 0, hi = F.nJoints;
+	while (lo < hi)
+	{
+		uint32_t mid = (lo + hi) >> 1;
+		if (F.jointKeys[mid] < k)
+			lo = mid + 1;
+		else
+			hi = mid;
+	}
+	return lo < F.nJoints && F.jointKeys[lo] == k;
+}
+
 // Contact records a leaf's walk keeps in its scratch slots; leaves with more
 // partners walk again for the rest.
 #define B3G_TRAV_SLOTS 32u
@@ -256,7 +296,8 @@ enum
 	CTR_SCRATCH = 30,
 	CTR_MESH_PAIRS = 31, // (contact, triangle) work items of the pass
 	CTR_TRAV_OVERFLOW = 32, // traversal records past the scratch slots
-	CTR_COUNT = 33
+	CTR_CANDIDATES = 33,    // new pairs handed to the caller's contact filter
+	CTR_COUNT = 34
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 
@@ -389,6 +430,25 @@ struct b3g_ctx
 	uint64_t graphLaunches;
 	bool lastPassImpulses;  // the last pass warm-started from host impulses
 
+	// collision filters (b3g_set_joint_pairs, b3g_set_contact_veto,
+	// B3G_FLAG_CONTACT_FILTER); device arrays allocated on first use
+	unsigned long long* dJointKeys;
+	uint32_t nJoints, jointCap;
+	uint8_t* dBodyJoint;
+	uint32_t bodyJointCap;
+	uint8_t* dVetoPrev;  // max_contacts bytes
+	uint32_t nVeto;      // contacts of the last pass the veto covers (0: none)
+	uint8_t* dRawDrop;   // max_contacts bytes
+	uint32_t* dCand;     // candidates: raw index of each (max_contacts)
+	uint4* dCandPairs;   // per candidate: fixtures as AddPair gets them and their keys; then
+	                     // the raw indices the caller's filter rejected (max_contacts uint4)
+	std::vector<uint32_t> hCandOrder; // raw indices of the candidates in AddPair order
+	uint32_t nCand;
+	bool candFetched;
+	bool passOpen;       // b3g_collide stopped before the contact list for the filter
+	cudaStream_t passStream; // the stream of the open pass
+	int filterMode;      // FilterArgs::mode of the pass under way
+
 	// stage profiling: a ring of per-pass event sets
 	bool profiling;
 	uint64_t profPass;     // passes recorded since enabling
@@ -408,8 +468,10 @@ enum
 	PM_BUILT,
 	PM_TRAVERSED,
 	PM_DIFFED,
-	PM_CONVEX,
+	PM_BUCKETED,
 	PM_HULLS,
+	PM_CONVEX,
+	PM_MESH,
 	PM_FINAL,
 	PROF_MARKS
 };
@@ -425,6 +487,9 @@ void launch_sync(b3g_ctx* c, cudaStream_t s);
 void launch_broadphase(b3g_ctx* c, cudaStream_t s);
 void launch_traverse(b3g_ctx* c, cudaStream_t s);
 void launch_pairs_diff(b3g_ctx* c, cudaStream_t s);
+void launch_candidates(b3g_ctx* c, cudaStream_t s);
+void launch_candidate_pairs(b3g_ctx* c, uint32_t n, cudaStream_t s);
+void launch_apply_veto(b3g_ctx* c, const uint32_t* rejected, uint32_t n, cudaStream_t s);
 void launch_narrowphase(b3g_ctx* c, cudaStream_t s);
 void launch_finalize(b3g_ctx* c, cudaStream_t s);
 uint32_t pairs_diff_launches(const b3g_ctx* c);

@@ -152,7 +152,11 @@ __device__ __forceinline__ bool body_active(const DevScene& S, uint32_t b)
 
 // Previous contacts: kept when their pair overlaps again, or when neither body
 // is active (UpdateContacts skips the contact without testing the overlap).
-__global__ void k_kept(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
+// With filters (FilterArgs), a contact whose bodies a joint keeps apart or
+// that the caller's filter rejects is destroyed whatever its bodies' state:
+// UpdateContacts tests both before the inactive skip
+// (contact_manager.cpp:176-199).
+__global__ void k_kept(DevScene S, Buffers B, FilterArgs F, uint32_t cur, uint32_t cap)
 {
 	uint32_t prevBuf = cur ^ 1u;
 	uint32_t n = min(B.counters[CTR_PREV_PAIRS], cap);
@@ -162,6 +166,9 @@ __global__ void k_kept(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 		uint32_t fa = B.pairA[prevBuf][p], fb = B.pairB[prevBuf][p];
 		if (S.fixLife[fa] != FIX_LIVE || S.fixLife[fb] != FIX_LIVE)
 			kept = 0; // a fixture was replaced or removed by a scene update
+		else if (F.mode != 0 && ((F.vetoPrev && p < F.nVeto && F.vetoPrev[p]) ||
+									joint_excluded(F, S.fixBody[fa], S.fixBody[fb])))
+			kept = 0;
 		else if (!B.prevFound[p])
 		{
 			uint32_t ba = S.fixBody[fa], bb = S.fixBody[fb];
@@ -442,6 +449,8 @@ void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, u
 
 // After the previous-contact lookup: lays out this pass's contacts in list
 // order, fills the hash table of this pass and lists the destroyed contacts.
+FilterArgs make_filter_args(const b3g_ctx* c);
+
 void launch_order(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
@@ -453,7 +462,7 @@ void launch_order(b3g_ctx* c, cudaStream_t s)
 	if (havePrev)
 	{
 		uint32_t blocks = (cap + SB - 1) / SB;
-		k_kept<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, cur, cap);
+		k_kept<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap);
 		k_dscan_blocks<<<blocks, SB, 0, s>>>(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux);
 		k_dscan_sums<<<1, 1024, 0, s>>>(B.scanAux, blocks, B.counters + CTR_KEPT);
 		k_dscan_add<<<blocks, SB, 0, s>>>(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux);

@@ -17,7 +17,30 @@ uint32_t order_launches(const b3g_ctx* c);
 
 namespace {
 
-__global__ void k_diff(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32_t nf, int havePrev)
+// The previous contact of overlapping pair (a, b), or -1.
+__device__ __forceinline__ int32_t previous_contact(const DevScene& S, const Buffers& B, uint32_t prevBuf, int havePrev,
+	uint32_t a, uint32_t b)
+{
+	// A fresh fixture continues no contact of its slot's previous holder.
+	bool fresh = S.fixLife[a] == FIX_FRESH || S.fixLife[b] == FIX_FRESH;
+	return havePrev && !fresh ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf], B.hashCap, pair_key(a, b))
+							  : -1;
+}
+
+// Whether overlapping pair (a, b), whose previous contact is prev (or -1), is
+// no contact this pass under the joints, the per-contact veto and the moved
+// rule (FilterArgs).
+__device__ __forceinline__ bool filter_drop(const DevScene& S, const Buffers& B, const FilterArgs& F, uint32_t a,
+	uint32_t b, int32_t prev)
+{
+	if (joint_excluded(F, S.fixBody[a], S.fixBody[b]))
+		return true;
+	if (prev >= 0)
+		return F.vetoPrev && (uint32_t)prev < F.nVeto && F.vetoPrev[prev] != 0;
+	return B.moved[a] == 0 && B.moved[b] == 0;
+}
+
+__global__ void k_diff(DevScene S, Buffers B, FilterArgs F, uint32_t cur, uint32_t cap, uint32_t nf, int havePrev)
 {
 	uint32_t n = min(B.counters[CTR_RAW], cap);
 	uint32_t prevBuf = cur ^ 1u;
@@ -29,12 +52,17 @@ __global__ void k_diff(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32
 		if (c < n)
 		{
 			uint32_t a = B.rawA[c], b = B.rawB[c];
-			// A fresh fixture continues no contact of its slot's previous holder.
-			bool fresh = S.fixLife[a] == FIX_FRESH || S.fixLife[b] == FIX_FRESH;
-			int32_t prev = havePrev && !fresh ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf],
-													B.hashCap, pair_key(a, b))
-											  : -1;
-			if (prev >= 0)
+			int32_t prev = previous_contact(S, B, prevBuf, havePrev, a, b);
+			bool drop = false;
+			if (F.mode == 2)
+				drop = F.rawDrop[c] != 0;
+			else if (F.mode == 1)
+				drop = filter_drop(S, B, F, a, b, prev);
+			if (drop)
+			{
+				// No contact: a previous one is destroyed (k_kept), none is created.
+			}
+			else if (prev >= 0)
 				B.prevFound[prev] = 1;
 			else
 			{
@@ -51,6 +79,49 @@ __global__ void k_diff(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32
 		if (isNew)
 			B.newList[slot + __popc(ballot & ((1u << lane) - 1u))] = c;
 	}
+}
+
+// Contact filter (mode 2), before the contact list: the drop flag of every
+// overlapping pair, and the pairs that would be new contacts (the AddPair
+// calls the caller's filter decides) listed for the host.
+__global__ void k_candidates(DevScene S, Buffers B, FilterArgs F, uint32_t* cand, uint32_t cur, uint32_t cap,
+	int havePrev)
+{
+	uint32_t n = min(B.counters[CTR_RAW], cap);
+	uint32_t prevBuf = cur ^ 1u;
+	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+	{
+		uint32_t a = B.rawA[c], b = B.rawB[c];
+		int32_t prev = previous_contact(S, B, prevBuf, havePrev, a, b);
+		bool drop = filter_drop(S, B, F, a, b, prev);
+		F.rawDrop[c] = drop ? 1 : 0;
+		if (!drop && prev < 0)
+		{
+			uint32_t slot = atomicAdd(&B.counters[CTR_CANDIDATES], 1u);
+			if (slot < cap)
+				cand[slot] = c;
+		}
+	}
+}
+
+// Per candidate: the two fixtures as AddPair receives them (the fixture of
+// the smaller proxy key first, broad_phase.cpp:341-342) and their keys.
+__global__ void k_candidate_pairs(DevScene S, Buffers B, const uint32_t* cand, uint32_t n, uint4* out)
+{
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = cand[t];
+		uint32_t a = B.rawA[c], b = B.rawB[c];
+		uint32_t ka = S.fixKey[a], kb = S.fixKey[b];
+		out[t] = ka < kb ? make_uint4(a, b, ka, kb) : make_uint4(b, a, kb, ka);
+	}
+}
+
+// The caller's filter rejected these candidates (raw indices).
+__global__ void k_apply_veto(FilterArgs F, const uint32_t* rejected, uint32_t n)
+{
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+		F.rawDrop[rejected[t]] = 1;
 }
 
 __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
@@ -178,6 +249,40 @@ __global__ void k_overflow_check(Buffers B, uint32_t cap)
 
 } // namespace
 
+FilterArgs make_filter_args(const b3g_ctx* c)
+{
+	FilterArgs F;
+	F.mode = c->filterMode;
+	F.jointKeys = c->dJointKeys;
+	F.nJoints = c->nJoints;
+	F.bodyJoint = c->dBodyJoint;
+	F.vetoPrev = c->nVeto ? c->dVetoPrev : nullptr;
+	F.nVeto = c->nVeto;
+	F.rawDrop = c->dRawDrop;
+	return F;
+}
+
+void launch_candidates(b3g_ctx* c, cudaStream_t s)
+{
+	Buffers& B = c->buf;
+	uint32_t cap = c->cfg.max_contacts;
+	k_overflow_check<<<1, 1, 0, s>>>(B, cap);
+	k_candidates<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), c->dCand, c->cur, cap,
+		c->havePass ? 1 : 0);
+}
+
+void launch_candidate_pairs(b3g_ctx* c, uint32_t n, cudaStream_t s)
+{
+	if (n)
+		k_candidate_pairs<<<persistent_blocks(2), 256, 0, s>>>(c->scene, c->buf, c->dCand, n, c->dCandPairs);
+}
+
+void launch_apply_veto(b3g_ctx* c, const uint32_t* rejected, uint32_t n, cudaStream_t s)
+{
+	if (n)
+		k_apply_veto<<<persistent_blocks(2), 256, 0, s>>>(make_filter_args(c), rejected, n);
+}
+
 void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
@@ -189,7 +294,8 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 	cudaMemsetAsync(B.newOff, 0, sizeof(uint32_t) * (nf + 1), s);
 	cudaMemsetAsync(B.newFill, 0, sizeof(uint32_t) * (nf + 1), s);
 	k_overflow_check<<<1, 1, 0, s>>>(B, cap);
-	k_diff<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, cur, cap, nf, c->havePass ? 1 : 0);
+	k_diff<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap, nf,
+		c->havePass ? 1 : 0);
 	launch_order(c, s);
 	k_count_moved<<<persistent_blocks(2), 256, 0, s>>>(B, c->nFixtures);
 }
@@ -247,6 +353,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	if (meshSide)
 		cudaEventRecord(c->meshJoin, ms);
 	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
+	prof_mark(c, PM_BUCKETED, s);
 	NPArgs a = make_np_args(c);
 	// The buckets are disjoint sets of contacts: the hull-hull and
 	// hull-triangle kernels run on a second stream beside the convex ones
@@ -262,6 +369,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 		c->maxUniqueEdges, c->tune, side);
 	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
 		c->maxUniqueEdges, c->tune, side);
+	prof_mark(c, PM_HULLS, s);
 	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
 	// The hull-sphere kernel follows the hull kernels on the second stream,
 	// which evens the two branches out (the hull-capsule kernel is the
@@ -277,7 +385,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	if (meshSide)
 		cudaStreamWaitEvent(s, c->meshJoin, 0);
 	launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
-	prof_mark(c, PM_HULLS, s);
+	prof_mark(c, PM_MESH, s);
 }
 
 void launch_finalize(b3g_ctx* c, cudaStream_t s)

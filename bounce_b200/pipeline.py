@@ -17,7 +17,8 @@ u32, f32 = ctypes.c_uint32, ctypes.c_float
 
 
 class CollisionPipeline:
-    def __init__(self, scene, max_contacts=None, warm_starting=True, convex_cache=True, device=0, graph=False):
+    def __init__(self, scene, max_contacts=None, warm_starting=True, convex_cache=True, device=0, graph=False,
+                 contact_filter=False):
         self.lib = N.load()
         self.scene = scene
         nf = scene.n_fixtures
@@ -29,7 +30,7 @@ class CollisionPipeline:
             max_contacts=int(max_contacts),
             max_hull_data=0,
             flags=(N.FLAG_WARM_STARTING if warm_starting else 0) | (N.FLAG_CONVEX_CACHE if convex_cache else 0)
-            | (N.FLAG_GRAPH if graph else 0),
+            | (N.FLAG_GRAPH if graph else 0) | (N.FLAG_CONTACT_FILTER if contact_filter else 0),
             device=device,
         )
         h = ctypes.c_void_p()
@@ -102,6 +103,34 @@ class CollisionPipeline:
             assert state17.dtype == np.float32 and state17.flags["C_CONTIGUOUS"]
             p = ctypes.c_void_p(state17.ctypes.data)
         self._check(self.lib.b3g_collide(self.ctx, p, 1 if on_device else 0, ctypes.c_void_p(stream or 0)))
+
+    # -- collision filters (b3g_set_joint_pairs and the contact filter) ------
+
+    def set_joint_pairs(self, body_pairs):
+        """Body pairs of the joints with collideConnected = false."""
+        a = np.ascontiguousarray(body_pairs, np.uint32).reshape(-1)
+        self._check(self.lib.b3g_set_joint_pairs(self.ctx, len(a) // 2, N.ptr(a, u32) if len(a) else None))
+
+    def set_contact_veto(self, veto):
+        """The contact filter's rejections of the last pass's contacts, in list order."""
+        v = np.ascontiguousarray(veto, np.uint8)
+        self._check(self.lib.b3g_set_contact_veto(self.ctx, len(v), N.ptr(v, ctypes.c_uint8) if len(v) else None))
+
+    def new_pairs(self):
+        """The new pairs the contact filter decides this pass (after collide
+        with contact_filter=True), in AddPair order: (n, 2) fixtures."""
+        n = self._check(self.lib.b3g_fetch_new_pairs(self.ctx, None, 0))
+        out = np.zeros((max(n, 1), 2), np.uint32)
+        n = self._check(self.lib.b3g_fetch_new_pairs(self.ctx, N.ptr(out, u32), n))
+        return out[:n]
+
+    def finish_pass(self, keep=None):
+        """Rest of the pass with the filter's answers (None keeps every new pair)."""
+        if keep is None:
+            self._check(self.lib.b3g_finish_pass(self.ctx, None, 0))
+        else:
+            k = np.ascontiguousarray(keep, np.uint8)
+            self._check(self.lib.b3g_finish_pass(self.ctx, N.ptr(k, ctypes.c_uint8) if len(k) else None, len(k)))
 
     def counts(self):
         c = N.Counts()

@@ -66,6 +66,10 @@ extern "C" {
 #define B3G_FLAG_CONVEX_CACHE 2u  /* b3_convexCache (collide_hulls.cpp:27, forced on by b3World()) */
 /* Replay each steady-state pass from a captured CUDA graph (see b3g_collide). */
 #define B3G_FLAG_GRAPH 4u
+/* The caller has a contact filter (b3World::SetContactFilter, world.h:77):
+ * each b3g_collide stops after the broadphase until b3g_finish_pass hands in
+ * the filter's answers for the new pairs (see "Collision filters"). */
+#define B3G_FLAG_CONTACT_FILTER 8u
 
 /* Fixture flags. */
 #define B3G_FIXTURE_SENSOR 1u     /* b3FixtureDef::isSensor (fixture.h:60) */
@@ -250,6 +254,47 @@ int b3g_collide(b3g_ctx* ctx, const float* body_state, int state_on_device, void
 /* Waits for the last pass and returns its counters. */
 int b3g_get_counts(b3g_ctx* ctx, b3g_counts* out);
 
+/* Collision filters ------------------------------------------------------
+ *
+ * Beyond the shape-type rules, the reference asks two questions about every
+ * pair: b3Body::ShouldCollide (body.cpp:240-263: at least one dynamic body,
+ * and no joint between the two bodies with collideConnected == false) and the
+ * world's b3ContactFilter::ShouldCollide (world_callbacks.h:131-138). Both are
+ * asked by AddPair before a contact is created (contact_manager.cpp:78-92)
+ * and again for every contact by UpdateContacts, before it skips inactive
+ * contacts (contact_manager.cpp:176-199); a contact that fails is destroyed
+ * at its place in the contact list. While any filter is in use, a new contact
+ * also needs one of its proxies to have moved this pass, as FindPairs only
+ * reports pairs of moved proxies (broad_phase.h:158-207): a pair a filter once
+ * refused stays no contact until one of its proxies moves, as in the
+ * reference. Passes with a filter in use run kernel by kernel (no graph).
+ *
+ * b3g_set_joint_pairs: the body pairs of every joint whose collideConnected
+ * is false (2 u32 each, any order; repeats allowed; count 0 clears). Replaces
+ * the joint-list walk of b3Body::ShouldCollide; holds for the following
+ * passes until set again, and is cleared by b3g_set_bodies.
+ *
+ * b3g_set_contact_veto: the contact filter's answers for the contacts of the
+ * last pass, in contact-list order (count = b3g_counts.contacts; veto[i] != 0
+ * when ShouldCollide(fixtureA, fixtureB) of contact i is false). The next pass
+ * destroys those contacts; it holds for that pass only.
+ *
+ * With B3G_FLAG_CONTACT_FILTER, b3g_collide runs the pass up to the
+ * broadphase and returns. b3g_fetch_new_pairs then waits for it and returns
+ * the number of overlapping pairs that would become new contacts, writing up
+ * to capacity of them (2 u32 each: the fixture of the smaller proxy key, then
+ * the other, as AddPair receives them) in the order AddPair meets them
+ * (ascending proxy keys). b3g_finish_pass takes the filter's answer for each
+ * (keep[i] != 0: create the contact; keep = NULL keeps them all, count
+ * ignored) and runs the rest of the pass. Until b3g_finish_pass, other calls
+ * on the context fail with B3G_E_INVALID. The filter is not asked about pairs
+ * whose shape types have no collide routine (b3Contact::Create returns none,
+ * contact.cpp:318-321): such pairs never become contacts either way. */
+int b3g_set_joint_pairs(b3g_ctx* ctx, uint32_t count, const uint32_t* body_pairs);
+int b3g_set_contact_veto(b3g_ctx* ctx, uint32_t count, const uint8_t* veto);
+int b3g_fetch_new_pairs(b3g_ctx* ctx, uint32_t* pairs, uint32_t capacity);
+int b3g_finish_pass(b3g_ctx* ctx, const uint8_t* keep, uint32_t count);
+
 /* Inner counters of the last pass, for diagnostics and work accounting: the
  * overlapping pairs the broadphase found, previous contacts kept, hull-hull
  * contacts the feature cache did not resolve (full SAT), traversal records
@@ -388,7 +433,11 @@ int b3g_get_totals(b3g_ctx* ctx, uint64_t* out, int reset);
  * counterpart of b3Profiler scopes (include/bounce/common/profiler.h:96-161).
  * enable != 0 starts (and clears) accumulation. b3g_get_profile waits for the
  * recorded passes and returns per stage the summed milliseconds and the
- * number of passes, in the order of b3g_stage_name(0 .. count-1). */
+ * number of passes, in the order of b3g_stage_name(0 .. count-1): upload,
+ * sync, sort, build, traverse, diff, bucket, narrow_hulls, narrow_convex,
+ * narrow_mesh, finalize. A profiled pass runs all its kernels on one stream
+ * so that each stage's events enclose its own kernels (an unprofiled pass
+ * runs the hull and mesh stages beside the convex one). */
 int b3g_set_profiling(b3g_ctx* ctx, int enable);
 int b3g_get_profile(b3g_ctx* ctx, double* ms, uint32_t* passes, uint32_t capacity);
 const char* b3g_stage_name(uint32_t stage);

@@ -82,6 +82,11 @@ def lib(precision=32):
         "refw_get_bodies": ([vp, f32p], None),
         "refw_set_sweeps": ([vp, f32p], None),
         "refw_set_local_centers": ([vp, f32p], None),
+        "refw_add_joints": ([vp, ctypes.c_uint32, u32p], None),
+        "refw_clear_joints": ([vp], None),
+        "refw_set_filter": ([vp, ctypes.c_uint32, ctypes.c_uint32], None),
+        "refw_filter_calls": ([vp, u32p, ctypes.c_uint32], ctypes.c_uint32),
+        "ref_filter_rejects": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32], ctypes.c_uint32),
         "refw_set_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
         "refw_get_awake": ([vp, ctypes.POINTER(ctypes.c_uint8)], None),
         "refw_set_triangle_wings": ([vp, ctypes.c_uint32, u32p, f32p], None),
@@ -126,6 +131,9 @@ def lib(precision=32):
         "refh_toi_aabb": ([ctypes.c_uint32, f32p, u32p], None),
         "refh_gjk_cast": ([vp, ctypes.c_uint32, f32p, f32p], None),
     }
+    if precision == 64:
+        sig["refc_reset"] = ([], None)
+        sig["refc_read"] = ([f64p, ctypes.c_uint32], ctypes.c_uint32)
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
@@ -133,6 +141,37 @@ def lib(precision=32):
     assert L.ref_sizeof_dump_contact() == DCONTACT.itemsize, "dump layout mismatch"
     _libs[precision] = L
     return L
+
+
+# Counters of flop_count.cpp (FP64 build), in its RC_* order.
+FLOP_COUNTERS = ("flops", "spheres", "capsule_sphere", "capsules", "hull_sphere", "hull_capsule", "hulls",
+                 "face_queries", "face_trips", "edge_queries", "edge_pairs", "edge_qualified", "gjk_calls",
+                 "gjk_iters", "clip_planes", "clip_vertices", "cache_reads", "hull_sphere_planes", "flops_sat",
+                 "flops_gjk", "flops_clip")
+
+
+def filter_rejects(ia, ib, modulus, salt):
+    """The seeded contact filter's rule (vectorised): reject when a hash of
+    (smaller, larger fixture index, salt) is 0 modulo `modulus`."""
+    ia = np.asarray(ia, np.uint64)
+    ib = np.asarray(ib, np.uint64)
+    lo, hi = np.minimum(ia, ib), np.maximum(ia, ib)
+    h = (lo * np.uint64(2654435761) + hi * np.uint64(40503) + np.uint64(salt) * np.uint64(97)) & np.uint64(0xFFFFFFFF)
+    if modulus == 0:
+        return np.zeros(h.shape, bool)
+    return ((h >> np.uint64(8)) % np.uint64(modulus)) == 0
+
+
+def flop_counts(reset=False):
+    """The narrowphase trip and flop counters of the FP64 reference build
+    since the last reset (oracle/flop_count.cpp, constants in flops.h)."""
+    L = lib(64)
+    out = np.zeros(len(FLOP_COUNTERS), np.float64)
+    n = L.refc_read(out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(out))
+    assert n == len(out), n
+    if reset:
+        L.refc_reset()
+    return dict(zip(FLOP_COUNTERS, out.tolist()))
 
 
 def _p(a, t):
@@ -232,6 +271,25 @@ class RefWorld:
         a = np.ascontiguousarray(lc, np.float32).reshape(-1)
         assert len(a) == 3 * self.scene.n_bodies
         self.L.refw_set_local_centers(self.w, _p(a, ctypes.c_float))
+
+    def add_joints(self, body_pairs):
+        """A joint with collideConnected = false between each body pair."""
+        a = np.ascontiguousarray(body_pairs, np.uint32).reshape(-1)
+        self.L.refw_add_joints(self.w, len(a) // 2, _p(a, ctypes.c_uint32))
+
+    def clear_joints(self):
+        self.L.refw_clear_joints(self.w)
+
+    def set_filter(self, modulus, salt=0):
+        """The seeded contact filter (filter_rejects); modulus 0 removes it."""
+        self.L.refw_set_filter(self.w, modulus, salt)
+
+    def filter_calls(self):
+        """Fixture pairs the filter was asked about by AddPair in the last
+        pass, in call order."""
+        out = np.zeros(2 * 4_000_000, np.uint32)
+        n = self.L.refw_filter_calls(self.w, _p(out, ctypes.c_uint32), len(out) // 2)
+        return out[:2 * n].reshape(-1, 2).copy()
 
     def set_sweeps(self, sweeps14):
         a = np.ascontiguousarray(sweeps14, np.float32)

@@ -412,6 +412,36 @@ REF_API void refh_gjk_cast(void* hullPool, uint32_t n, const float* q, float* ou
 // ---------------------------------------------------------------------------
 // World.
 
+// A seeded contact filter (b3ContactFilter, world_callbacks.h:131-138) for
+// the filter tests: it rejects a fixture pair when a hash of (smaller index,
+// larger index, salt) is 0 modulo `modulus` (0: accept every pair). While
+// `log` is on it records the pairs it is asked about, in call order.
+static bool filter_rejects(uint32_t ia, uint32_t ib, uint32_t modulus, uint32_t salt)
+{
+	if (modulus == 0)
+		return false;
+	uint32_t lo = ia < ib ? ia : ib, hi = ia < ib ? ib : ia;
+	uint32_t h = lo * 2654435761u + hi * 40503u + salt * 97u;
+	return ((h >> 8) % modulus) == 0;
+}
+
+struct HarnessFilter : b3ContactFilter
+{
+	uint32_t modulus = 0, salt = 0;
+	bool log = false;
+	std::vector<uint32_t> calls;
+	bool ShouldCollide(b3Fixture* a, b3Fixture* b) override
+	{
+		uint32_t ia = (uint32_t)(uintptr_t)a->GetUserData(), ib = (uint32_t)(uintptr_t)b->GetUserData();
+		if (log)
+		{
+			calls.push_back(ia);
+			calls.push_back(ib);
+		}
+		return !filter_rejects(ia, ib, modulus, salt);
+	}
+};
+
 struct RefWorld
 {
 	b3World* world;
@@ -420,7 +450,21 @@ struct RefWorld
 	const HullPool* pool;
 	double tFind;
 	double tUpdate;
+	HarnessFilter* filter = nullptr;
 };
+
+// FindNewContacts with the filter's AddPair calls logged.
+static void find_new_contacts(RefWorld* w)
+{
+	if (w->filter)
+	{
+		w->filter->calls.clear();
+		w->filter->log = true;
+	}
+	w->world->m_contactManager.FindNewContacts();
+	if (w->filter)
+		w->filter->log = false;
+}
 
 static inline double Now()
 {
@@ -470,7 +514,65 @@ REF_API void refw_destroy(void* p)
 {
 	RefWorld* w = (RefWorld*)p;
 	delete w->world;
+	delete w->filter;
 	delete w;
+}
+
+// Joints with collideConnected = false between body pairs (2 u32 each): a
+// b3SphereJoint per pair, which b3Body::ShouldCollide finds in the bodies'
+// joint lists (body.cpp:248-260). The collision pass never solves joints.
+REF_API void refw_add_joints(void* p, uint32_t n, const uint32_t* pairs)
+{
+	RefWorld* w = (RefWorld*)p;
+	for (uint32_t i = 0; i < n; ++i)
+	{
+		b3SphereJointDef jd;
+		jd.bodyA = w->bodies[pairs[2 * i]];
+		jd.bodyB = w->bodies[pairs[2 * i + 1]];
+		jd.collideConnected = false;
+		w->world->CreateJoint(jd);
+	}
+}
+
+// Destroys every joint of the world.
+REF_API void refw_clear_joints(void* p)
+{
+	RefWorld* w = (RefWorld*)p;
+	while (w->world->GetJointList())
+		w->world->DestroyJoint(w->world->GetJointList());
+}
+
+// Installs (modulus != 0) or removes the seeded contact filter.
+REF_API void refw_set_filter(void* p, uint32_t modulus, uint32_t salt)
+{
+	RefWorld* w = (RefWorld*)p;
+	if (!w->filter)
+		w->filter = new HarnessFilter;
+	w->filter->modulus = modulus;
+	w->filter->salt = salt;
+	w->world->SetContactFilter(modulus ? w->filter : nullptr);
+}
+
+// The pairs the filter was asked about by AddPair in the last pass, in call
+// order (2 u32 each, fixture indices). Returns the number of pairs.
+REF_API uint32_t refw_filter_calls(void* p, uint32_t* out, uint32_t capacity)
+{
+	RefWorld* w = (RefWorld*)p;
+	if (!w->filter)
+		return 0;
+	uint32_t n = (uint32_t)(w->filter->calls.size() / 2);
+	for (uint32_t i = 0; i < n && i < capacity; ++i)
+	{
+		out[2 * i] = w->filter->calls[2 * i];
+		out[2 * i + 1] = w->filter->calls[2 * i + 1];
+	}
+	return n;
+}
+
+// The filter's rule, for callers that apply the same filter elsewhere.
+REF_API uint32_t ref_filter_rejects(uint32_t ia, uint32_t ib, uint32_t modulus, uint32_t salt)
+{
+	return filter_rejects(ia, ib, modulus, salt) ? 1u : 0u;
 }
 
 // 17 floats per body: xf.translation(3), xf.rotation(xyzw 4), sweep.worldCenter0(3),
@@ -560,7 +662,7 @@ REF_API void refw_first_pass(void* p, double* times)
 	double t0 = Now();
 	if (w->world->m_newContacts)
 	{
-		w->world->m_contactManager.FindNewContacts();
+		find_new_contacts(w);
 		w->world->m_newContacts = false;
 	}
 	double t1 = Now();
@@ -586,7 +688,7 @@ REF_API void refw_pass(void* p, double* times)
 		b->SynchronizeFixtures();
 	}
 	world->m_contactManager.SynchronizeFixtures();
-	world->m_contactManager.FindNewContacts();
+	find_new_contacts(w);
 	double t1 = Now();
 	world->m_contactManager.UpdateContacts();
 	double t2 = Now();
@@ -612,7 +714,7 @@ REF_API void refw_pass_sleep(void* p, const uint8_t* moved, const uint8_t* awake
 			b->SynchronizeFixtures();
 	}
 	world->m_contactManager.SynchronizeFixtures();
-	world->m_contactManager.FindNewContacts();
+	find_new_contacts(w);
 	refw_set_awake(p, awake);
 	double t1 = Now();
 	world->m_contactManager.UpdateContacts();
