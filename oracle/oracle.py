@@ -62,9 +62,13 @@ _libs = {}
 
 
 def lib(precision=32):
+    """The reference build: 32 (FP32), 64 (the FP64 rerun) or "shim" (FP32
+    with the GPU contact manager of bounce_b200/shim in place of the
+    reference's, linked to the library)."""
     if precision in _libs:
         return _libs[precision]
-    path = os.path.join(REF_DIR, f"libb3ref{precision}.so")
+    name = "libb3shim.so" if precision == "shim" else f"libb3ref{precision}.so"
+    path = os.path.join(REF_DIR, name)
     if not os.path.exists(path):
         raise RuntimeError(f"{path} missing: build the oracle with make -C oracle")
     L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
@@ -131,6 +135,11 @@ def lib(precision=32):
         "refh_toi_aabb": ([ctypes.c_uint32, f32p, u32p], None),
         "refh_gjk_cast": ([vp, ctypes.c_uint32, f32p, f32p], None),
     }
+    sig["stepw_create"] = ([vp, ctypes.c_uint32, u32p, f32p, f32p, ctypes.c_uint32, u32p, u32p, u32p, f32p, u32p, f32p],
+                           vp)
+    sig["stepw_step"] = ([vp, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32], None)
+    if precision == "shim":
+        sig["b3g_shim_failures"] = ([], ctypes.c_uint32)
     if precision == 64:
         sig["refc_reset"] = ([], None)
         sig["refc_read"] = ([f64p, ctypes.c_uint32], ctypes.c_uint32)
@@ -250,6 +259,32 @@ class RefWorld:
         if self.w:
             self.L.refw_destroy(self.w)
             self.w = None
+
+    @classmethod
+    def stepping(cls, scene, build=32, gravity=(0.0, -9.8, 0.0)):
+        """A world for whole b3World::Step calls (solver, islands, sleep): the
+        scene's bodies with their velocities, gravity and sleeping on. build:
+        32 (the reference) or "shim" (the reference with the GPU contact
+        manager)."""
+        self = cls.__new__(cls)
+        self.L = lib(build)
+        self.precision = 32
+        self.scene = scene
+        self.hulls = RefHulls(scene.hull_arrays, build, getattr(scene, "mesh_arrays", None))
+        s = scene
+        vel = np.ascontiguousarray(np.concatenate([s.body_lin, s.body_ang], axis=1), np.float32)
+        g = np.asarray(gravity, np.float32)
+        self._keep = (vel, g)
+        self.w = self.L.stepw_create(
+            self.hulls.h, s.n_bodies, _p(s.body_type, ctypes.c_uint32), _p(s.body_pose, ctypes.c_float),
+            _p(vel, ctypes.c_float), s.n_fixtures, _p(s.fix_body, ctypes.c_uint32), _p(s.fix_type, ctypes.c_uint32),
+            _p(s.fix_hull, ctypes.c_uint32), _p(s.fix_params, ctypes.c_float), _p(s.fix_flags, ctypes.c_uint32),
+            _p(g, ctypes.c_float))
+        self.times = np.zeros(2)
+        return self
+
+    def step(self, dt=1.0 / 60.0, velocity_iterations=8, position_iterations=2):
+        self.L.stepw_step(self.w, dt, velocity_iterations, position_iterations)
 
     def __del__(self):
         try:

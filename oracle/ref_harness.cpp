@@ -510,12 +510,68 @@ REF_API void* refw_create(void* hullPool, uint32_t nb, const uint32_t* bodyType,
 	return w;
 }
 
+// The device state a GPU contact manager keeps beside the world, in a build
+// whose b3ContactManager is the shim of bounce_b200/shim (absent otherwise).
+extern "C" void b3g_shim_release(b3ContactManager* cm) __attribute__((weak));
+
 REF_API void refw_destroy(void* p)
 {
 	RefWorld* w = (RefWorld*)p;
+	if (b3g_shim_release)
+		b3g_shim_release(&w->world->m_contactManager);
 	delete w->world;
 	delete w->filter;
 	delete w;
+}
+
+// A world for whole steps of b3World::Step (the solver, islands and sleep
+// included): as refw_create, with gravity, sleeping allowed, and each body's
+// linear and angular velocity (6 floats per body).
+REF_API void* stepw_create(void* hullPool, uint32_t nb, const uint32_t* bodyType, const float* bodyPose,
+	const float* bodyVel, uint32_t nf, const uint32_t* fixBody, const uint32_t* fixType, const uint32_t* fixHull,
+	const float* fixParams, const uint32_t* fixFlags, const float* gravity)
+{
+	RefWorld* w = new RefWorld;
+	w->pool = (const HullPool*)hullPool;
+	w->world = new b3World();
+	w->world->SetGravity(b3Vec3(gravity[0], gravity[1], gravity[2]));
+	w->world->SetSleeping(true);
+	w->world->SetWarmStarting(true);
+	w->tFind = 0;
+	w->tUpdate = 0;
+	for (uint32_t i = 0; i < nb; ++i)
+	{
+		b3BodyDef bd;
+		bd.type = (b3BodyType)bodyType[i];
+		bd.position.Set(bodyPose[7 * i + 0], bodyPose[7 * i + 1], bodyPose[7 * i + 2]);
+		bd.orientation.v.Set(bodyPose[7 * i + 3], bodyPose[7 * i + 4], bodyPose[7 * i + 5]);
+		bd.orientation.s = bodyPose[7 * i + 6];
+		if (bd.type != e_staticBody)
+		{
+			bd.linearVelocity.Set(bodyVel[6 * i + 0], bodyVel[6 * i + 1], bodyVel[6 * i + 2]);
+			bd.angularVelocity.Set(bodyVel[6 * i + 3], bodyVel[6 * i + 4], bodyVel[6 * i + 5]);
+		}
+		w->bodies.push_back(w->world->CreateBody(bd));
+	}
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		ShapeStore store;
+		const b3Shape* shape = MakeShape(store, fixType[i], fixParams + 12 * i, fixHull[i], w->pool);
+		b3FixtureDef fd;
+		fd.shape = shape;
+		fd.density = bodyType[fixBody[i]] == e_dynamicBody ? scalar(1) : scalar(0);
+		fd.isSensor = (fixFlags[i] & 1) != 0;
+		fd.userData = (void*)(uintptr_t)i;
+		w->fixtures.push_back(w->bodies[fixBody[i]]->CreateFixture(fd));
+	}
+	return w;
+}
+
+// One b3World::Step.
+REF_API void stepw_step(void* p, float dt, uint32_t velocityIterations, uint32_t positionIterations)
+{
+	RefWorld* w = (RefWorld*)p;
+	w->world->Step(dt, velocityIterations, positionIterations);
 }
 
 // Joints with collideConnected = false between body pairs (2 u32 each): a
