@@ -296,57 +296,3 @@ B3G_HD V3 perp(V3 v)
 	normalize_inplace(u);
 	return u;
 }
-
-// First maximum of dot(d, v[i].xyz) over 0 <= i < n (n >= 1), the loop of
-// b3Hull::GetSupportVertex / GetSupportFace and b3GJKProxy::GetSupportIndex
-// (the larger value wins; on equal values the earlier index stays). The
-// loads are issued four at a time, so four are in flight where the plain loop
-// waits for each; the comparisons run in index order as in the plain loop, so
-// the index is the same. v may point to global or local memory (a mesh
-// triangle's hull is built in registers / local memory): plain loads only.
-__device__ __forceinline__ uint32_t argmax_dot4(const float4* v, uint32_t n, V3 d)
-{
-	float4 w = v[0];
-	uint32_t maxIndex = 0;
-	float maxProj = dot(d, V3{w.x, w.y, w.z});
-	uint32_t i = 1;
-	for (; i + 4 <= n; i += 4)
-	{
-		float4 a = v[i], b = v[i + 1], c = v[i + 2], e = v[i + 3];
-		float pa = dot(d, V3{a.x, a.y, a.z});
-		float pb = dot(d, V3{b.x, b.y, b.z});
-		float pc = dot(d, V3{c.x, c.y, c.z});
-		float pe = dot(d, V3{e.x, e.y, e.z});
-		if (pa > maxProj)
-		{
-			maxIndex = i;
-			maxProj = pa;
-		}
-		if (pb > maxProj)
-		{
-			maxIndex = i + 1;
-			maxProj = pb;
-		}
-		if (pc > maxProj)
-		{
-			maxIndex = i + 2;
-			maxProj = pc;
-		}
-		if (pe > maxProj)
-		{
-			maxIndex = i + 3;
-			maxProj = pe;
-		}
-	}
-	for (; i < n; ++i)
-	{
-		float4 a = v[i];
-		float pa = dot(d, V3{a.x, a.y, a.z});
-		if (pa > maxProj)
-		{
-			maxIndex = i;
-			maxProj = pa;
-		}
-	}
-	return maxIndex;
-}

@@ -76,13 +76,35 @@ __device__ __forceinline__ uint32_t he_next(const HullRef& h, uint32_t i) { retu
 // b3Hull::GetSupportVertex (hull.h:105-119): first maximum.
 __device__ __forceinline__ uint32_t hull_support_vertex(const HullRef& h, V3 d)
 {
-	return argmax_dot4(h.v, h.vCnt, d);
+	uint32_t maxIndex = 0;
+	float maxProj = dot(d, hv(h, 0));
+	for (uint32_t i = 1; i < h.vCnt; ++i)
+	{
+		float proj = dot(d, hv(h, i));
+		if (proj > maxProj)
+		{
+			maxIndex = i;
+			maxProj = proj;
+		}
+	}
+	return maxIndex;
 }
 
 // b3Hull::GetSupportFace (hull.h:121-135).
 __device__ __forceinline__ uint32_t hull_support_face(const HullRef& h, V3 d)
 {
-	return argmax_dot4(h.p, h.fCnt, d);
+	uint32_t maxIndex = 0;
+	float maxProj = dot(d, hp(h, 0).n);
+	for (uint32_t i = 1; i < h.fCnt; ++i)
+	{
+		float proj = dot(d, hp(h, i).n);
+		if (proj > maxProj)
+		{
+			maxIndex = i;
+			maxProj = proj;
+		}
+	}
+	return maxIndex;
 }
 
 // b3Hull::GetEdgeSidePlane (hull.h:137-152).
@@ -544,14 +566,6 @@ struct NPArgs
 	// hull-hull pairs the feature cache could not resolve
 	uint32_t* missList;
 	uint32_t* missCount;
-	// hull-hull pairs whose cached face contact is rebuilt by its own kernel
-	// (null: the probe rebuilds it)
-	uint32_t* faceList;
-	uint32_t* faceCount;
-	// SAT queries of contacts whose face contact is built by k_hulls_sat_face
-	// (2 uint4 per contact), and their count in faceList
-	uint4* satRec;
-	uint32_t* satFaceCount;
 	// manifolds 1 and 2 of mesh contacts (null without meshes)
 	DevManifold* extraCur;
 	const DevManifold* extraPrev;

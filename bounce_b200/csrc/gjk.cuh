@@ -30,8 +30,6 @@ __device__ __forceinline__ V3 gp_vertex(const GProxy& p, uint32_t i)
 // b3GJKProxy::GetSupportIndex (gjk_proxy.h:72-86): first maximum.
 __device__ __forceinline__ uint32_t gp_support(const GProxy& p, V3 d)
 {
-	if (p.gv)
-		return argmax_dot4(p.gv, p.count, d);
 	uint32_t maxIndex = 0;
 	float maxProj = dot(d, gp_vertex(p, 0));
 	for (uint32_t i = 1; i < p.count; ++i)

@@ -176,30 +176,16 @@ __device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF&
 	V3 cLocal = xmult(xf1, xmul(xf2, sph_center(s2)));
 	uint32_t faceIndex = 0;
 	float separation = -B3G_MAX_SCALAR;
-	// Planes loaded four at a time; the tests run in face order, so the
-	// early exit and the first maximum are the reference's.
-	for (uint32_t i = 0; i < h1.fCnt; i += 4)
+	for (uint32_t i = 0; i < h1.fCnt; ++i)
 	{
-		float s[4];
-		const uint32_t m4 = min(4u, h1.fCnt - i);
-#pragma unroll
-		for (uint32_t k = 0; k < 4; ++k)
+		PL plane = hp(h1, i);
+		float s = pdist(cLocal, plane);
+		if (s > radius)
+			return;
+		if (s > separation)
 		{
-			float4 w = h1.p[i + (k < m4 ? k : 0)];
-			s[k] = pdist(cLocal, PL{V3{w.x, w.y, w.z}, w.w});
-		}
-#pragma unroll
-		for (uint32_t k = 0; k < 4; ++k)
-		{
-			if (k >= m4)
-				break;
-			if (s[k] > radius)
-				return;
-			if (s[k] > separation)
-			{
-				faceIndex = i + k;
-				separation = s[k];
-			}
+			faceIndex = i;
+			separation = s;
 		}
 	}
 	if (separation < 0.0f)

@@ -54,7 +54,17 @@ __device__ void warp_query_faces(const XF& xf1, const HullRef& h1, const XF& xf2
 	{
 		PL plane = pmul(xf, hp(h1, i));
 		V3 d = -plane.n;
-		uint32_t si = argmax_dot4(h2.v, h2.vCnt, d);
+		uint32_t si = 0;
+		float sp = dot(d, hv(h2, 0));
+		for (uint32_t k = 1; k < h2.vCnt; ++k)
+		{
+			float proj = dot(d, hv(h2, k));
+			if (proj > sp)
+			{
+				si = k;
+				sp = proj;
+			}
+		}
 		float s = pdist(hv(h2, si), plane);
 		if (s > best)
 		{
@@ -509,22 +519,13 @@ __device__ uint32_t read_face_thread(const XF& xf1, const HullRef& h1, const XF&
 	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
 }
 
-enum : uint32_t
-{
-	PR_DONE = 0, // the cache decided the contact
-	PR_MISS,     // the cache is flushed: the contact needs the SAT
-	PR_FACE      // an overlap hit whose face contact is rebuilt later (k_hulls_face)
-};
-
 // The cache half of b3CollideHullsCache (collide_hulls.cpp:367-415), one
 // thread per contact: b3FeatureCache::ReadState (sat.cpp:178-207), then the
 // separation hit, or the overlap hit that rebuilds the cached edge or face
-// contact. On a miss the cache is flushed (cacheType = empty, the feature
-// fields as ReadState left them) and the contact needs the SAT. With
-// deferFace an overlap hit on a face returns PR_FACE with the cache as read:
-// the clipping of the face contact runs in k_hulls_face, where every thread
-// of a warp clips, instead of a few threads here while the others wait.
-__device__ uint32_t probe_cache(DevManifold& m, const HullCtx& H, uint4& cache, bool deferFace)
+// contact. Returns true when the contact is finished; otherwise the cache is
+// flushed (cacheType = empty, the feature fields as ReadState left them) and
+// the contact needs the SAT.
+__device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 {
 	float totalRadius = H.r1 + H.r2;
 	uint32_t state0 = cache.x;
@@ -545,35 +546,20 @@ __device__ uint32_t probe_cache(DevManifold& m, const HullCtx& H, uint4& cache, 
 	else
 		state1 = CT_EMPTY;
 	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
-		return PR_DONE; // separation cache hit
+		return true; // separation cache hit
 	if (state0 == CT_OVERLAP && state1 == CT_OVERLAP)
 	{
 		if (cache.y == FT_EDGES)
 			rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
-		else if (deferFace && (cache.y == FT_FACE1 || cache.y == FT_FACE2))
-			return PR_FACE;
 		else if (cache.y == FT_FACE1)
 			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
 		else if (cache.y == FT_FACE2)
 			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
 		if (m.pointCount > 0)
-			return PR_DONE; // overlap cache hit
+			return true; // overlap cache hit
 	}
 	cache.x = CT_EMPTY;
-	return PR_MISS;
-}
-
-// Warp-aggregated append of c to a list (the calling lanes of the warp).
-__device__ __forceinline__ void warp_append(uint32_t* list, uint32_t* count, uint32_t c)
-{
-	uint32_t mask = __activemask();
-	uint32_t lane = threadIdx.x & 31;
-	uint32_t leader = __ffs(mask) - 1;
-	uint32_t base = 0;
-	if (lane == leader)
-		base = atomicAdd(count, (uint32_t)__popc(mask));
-	base = __shfl_sync(mask, base, leader);
-	list[base + __popc(mask & ((1u << lane) - 1u))] = c;
+	return false;
 }
 
 // The SAT half of b3CollideHullsCache (collide_hulls.cpp:417-515), one warp
@@ -647,101 +633,6 @@ __device__ void sat_after_miss(DevManifold& m, const HullCtx& H, uint4& cache, u
 	}
 }
 
-// The SAT queries of a contact whose face contact is built by
-// k_hulls_sat_face: face indices and separations of both face queries and the
-// edge query's result.
-struct SatRec
-{
-	uint32_t fi1, fi2, ei1, ei2;
-	float fs1, fs2, es;
-};
-
-// The SAT half of b3CollideHullsCache up to the face contacts (collide_hulls.cpp:
-// 417-447), one warp per contact: separations and edge contacts finish here;
-// otherwise rec holds the queries, the function returns true and the rest of
-// the decision (face contacts, their fallbacks, :449-515) runs in
-// sat_face_tail. cache is uniform across the warp; m is written by lane 0.
-__device__ bool sat_queries(DevManifold& m, const HullCtx& H, uint4& cache, uint32_t lane, SatRec& rec)
-{
-	float totalRadius = H.r1 + H.r2;
-	uint32_t fi1, fi2, ei1, ei2;
-	float fs1, fs2, es;
-	warp_query_faces(H.xf1, H.h1, H.xf2, H.h2, lane, fi1, fs1);
-	if (fs1 > totalRadius)
-	{
-		cache = make_uint4(CT_SEPARATION, FT_FACE1, fi1, fi1);
-		return false;
-	}
-	warp_query_faces(H.xf2, H.h2, H.xf1, H.h1, lane, fi2, fs2);
-	if (fs2 > totalRadius)
-	{
-		cache = make_uint4(CT_SEPARATION, FT_FACE2, fi2, fi2);
-		return false;
-	}
-	warp_query_edges(H.xf1, H.h1, H.xf2, H.h2, lane, H.recs, H.maxUE, ei1, ei2, es);
-	if (es > totalRadius)
-	{
-		cache = make_uint4(CT_SEPARATION, FT_EDGES, ei1, ei2);
-		return false;
-	}
-	const float kRelEdgeTol = 0.90f;
-	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
-	if (es > kRelEdgeTol * fmaxr(fs1, fs2) + kAbsTol)
-	{
-		if (lane == 0)
-			build_edge_contact(m, H.xf1, ei1, H.h1, H.xf2, ei2, H.h2);
-		cache = make_uint4(CT_OVERLAP, FT_EDGES, ei1, ei2);
-		return false;
-	}
-	rec = SatRec{fi1, fi2, ei1, ei2, fs1, fs2, es};
-	return true;
-}
-
-// The face-contact rest of sat_after_miss (collide_hulls.cpp:449-515), one
-// thread: the same builds in the same order on the same manifold.
-__device__ void sat_face_tail(DevManifold& m, const HullCtx& H, uint4& cache, const SatRec& r)
-{
-	const float kRelFaceTol = 0.98f;
-	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
-	if (r.fs2 > kRelFaceTol * r.fs1 + kAbsTol)
-	{
-		build_face_contact(m, H.xf2, r.fi2, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status);
-		if (m.pointCount > 0)
-		{
-			cache = make_uint4(CT_OVERLAP, FT_FACE2, r.fi2, r.fi2);
-			return;
-		}
-	}
-	else
-	{
-		build_face_contact(m, H.xf1, r.fi1, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status);
-		if (m.pointCount > 0)
-		{
-			cache = make_uint4(CT_OVERLAP, FT_FACE1, r.fi1, r.fi1);
-			return;
-		}
-	}
-	// Heuristic failed. Fallback.
-	if (r.es > fmaxr(r.fs1, r.fs2))
-	{
-		build_edge_contact(m, H.xf1, r.ei1, H.h1, H.xf2, r.ei2, H.h2);
-		cache = make_uint4(CT_OVERLAP, FT_EDGES, r.ei1, r.ei2);
-		return;
-	}
-	if (r.fs2 > r.fs1)
-	{
-		build_face_contact(m, H.xf2, r.fi2, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status);
-		if (m.pointCount > 0)
-			cache = make_uint4(CT_OVERLAP, FT_FACE2, r.fi2, r.fi2);
-	}
-	else
-	{
-		build_face_contact(m, H.xf1, r.fi1, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status);
-		if (m.pointCount > 0)
-			cache = make_uint4(CT_OVERLAP, FT_FACE1, r.fi1, r.fi1);
-	}
-}
-
 __device__ __forceinline__ void load_hull_ctx(const NPArgs& a, uint32_t c, HullCtx& H)
 {
 	uint32_t fa = a.pairA[c], fb = a.pairB[c];
@@ -760,7 +651,6 @@ __device__ __forceinline__ void load_hull_ctx(const NPArgs& a, uint32_t c, HullC
 }
 
 // Pass 1: one thread per hull-hull contact reads its feature cache.
-template <bool DEFER_FACE>
 __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 {
 	uint32_t n = *a.listCount;
@@ -771,60 +661,35 @@ __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
 		DevManifold& m = a.man[c];
 		man_clear(m);
-		uint32_t r = PR_MISS;
+		bool done = false;
 		if (a.convexCache)
 		{
 			HullCtx H;
 			load_hull_ctx(a, c, H);
-			r = probe_cache(m, H, cache, DEFER_FACE);
+			done = probe_cache(m, H, cache);
 		}
 		a.cache[c] = cache;
-		if (r == PR_DONE)
-			finish_convex(a, c, m);
-		else if (DEFER_FACE && r == PR_FACE)
-			warp_append(a.faceList, a.faceCount, c);
-		else
-			warp_append(a.missList, a.missCount, c);
-	}
-}
-
-// Pass 1b: one thread per overlap hit on a cached face (b3RebuildFaceContact,
-// collide_hulls.cpp:323-353, from b3CollideHullsCache :395-414): the face
-// contact is rebuilt; a rebuild without points flushes the cache and sends
-// the contact to the SAT, as the probe would have.
-__global__ void __launch_bounds__(128) k_hulls_face(NPArgs a)
-{
-	uint32_t n = *a.faceCount;
-	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-	{
-		uint32_t c = a.faceList[t];
-		HullCtx H;
-		load_hull_ctx(a, c, H);
-		uint4 cache = a.cache[c];
-		DevManifold& m = a.man[c];
-		if (cache.y == FT_FACE1)
-			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
-		else
-			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
-		if (m.pointCount > 0)
+		if (done)
 		{
 			finish_convex(a, c, m);
 		}
 		else
 		{
-			cache.x = CT_EMPTY;
-			a.cache[c] = cache;
-			warp_append(a.missList, a.missCount, c);
+			// Warp-aggregated append to the SAT list.
+			uint32_t mask = __activemask();
+			uint32_t lane = threadIdx.x & 31;
+			uint32_t leader = __ffs(mask) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(a.missCount, (uint32_t)__popc(mask));
+			base = __shfl_sync(mask, base, leader);
+			a.missList[base + __popc(mask & ((1u << lane) - 1u))] = c;
 		}
 	}
 }
 
 // Pass 2: one warp per contact the cache did not resolve (W warps per block).
-// With DEFER_FACE (the feature cache on and a.faceList set), contacts that
-// end in a face contact leave it to k_hulls_sat_face: their queries go to
-// a.satRec and the contact to the face list (reused: k_hulls_face is done
-// with it), so no lane of the warp clips polygons while the others wait.
-template <int W, bool DEFER_FACE>
+template <int W>
 __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
@@ -842,53 +707,17 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 		H.maxUE = maxUE;
 		uint4 cache = a.cache[c];
 		DevManifold& m = a.man[c];
-		bool deferred = false;
-		if constexpr (DEFER_FACE)
-		{
-			SatRec rec{};
-			deferred = sat_queries(m, H, cache, lane, rec);
-			if (deferred && lane == 0)
-			{
-				a.satRec[2 * (size_t)c + 0] = make_uint4(rec.fi1, rec.fi2, rec.ei1, rec.ei2);
-				a.satRec[2 * (size_t)c + 1] =
-					make_uint4(__float_as_uint(rec.fs1), __float_as_uint(rec.fs2), __float_as_uint(rec.es), 0u);
-				uint32_t slot = atomicAdd(a.satFaceCount, 1u);
-				a.faceList[slot] = c;
-			}
-		}
+		if (a.convexCache)
+			sat_after_miss(m, H, cache, lane);
 		else
-		{
-			if (a.convexCache)
-				sat_after_miss(m, H, cache, lane);
-			else
-				collide_hulls_nocache(m, H, lane);
-		}
+			collide_hulls_nocache(m, H, lane);
 		__syncwarp();
-		if (lane == 0 && !deferred)
+		if (lane == 0)
 		{
 			finish_convex(a, c, m);
 			a.cache[c] = cache;
 		}
 		__syncwarp();
-	}
-}
-
-// Pass 3: one thread per contact whose SAT ended in a face contact.
-__global__ void __launch_bounds__(128) k_hulls_sat_face(NPArgs a)
-{
-	uint32_t n = *a.satFaceCount;
-	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-	{
-		uint32_t c = a.faceList[t];
-		HullCtx H;
-		load_hull_ctx(a, c, H);
-		uint4 r0 = a.satRec[2 * (size_t)c + 0], r1 = a.satRec[2 * (size_t)c + 1];
-		SatRec rec{r0.x, r0.y, r0.z, r0.w, __uint_as_float(r1.x), __uint_as_float(r1.y), __uint_as_float(r1.z)};
-		uint4 cache = a.cache[c];
-		DevManifold& m = a.man[c];
-		sat_face_tail(m, H, cache, rec);
-		finish_convex(a, c, m);
-		a.cache[c] = cache;
 	}
 }
 
@@ -1095,29 +924,17 @@ void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint3
 	}
 }
 
-template <int W, bool DEFER_FACE>
-void launch_sat_kernel(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
+template <int W>
+void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
 {
 	size_t smem = (size_t)W * sat_warp_recs(maxUE) * sizeof(EdgeRec);
 	static size_t configured = 0;
 	if (smem > 48 * 1024 && smem > configured)
 	{
-		cudaFuncSetAttribute(k_hulls_sat<W, DEFER_FACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		cudaFuncSetAttribute(k_hulls_sat<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 		configured = smem;
 	}
-	k_hulls_sat<W, DEFER_FACE><<<persistent_blocks(blocksPerSM), W * 32, smem, s>>>(a, maxUE);
-}
-
-template <int W>
-void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
-{
-	if (a.faceList && a.convexCache)
-	{
-		launch_sat_kernel<W, true>(a, maxUE, blocksPerSM, s);
-		k_hulls_sat_face<<<persistent_blocks(blocksPerSM), 128, 0, s>>>(a);
-	}
-	else
-		launch_sat_kernel<W, false>(a, maxUE, blocksPerSM, s);
+	k_hulls_sat<W><<<persistent_blocks(blocksPerSM), W * 32, smem, s>>>(a, maxUE);
 }
 
 void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, const Tune& tune,
@@ -1126,14 +943,7 @@ void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* coun
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	const int bps = (int)tune.v[B3G_TUNE_PROBE];
-	if (a.faceList)
-	{
-		k_hulls_probe<true><<<persistent_blocks(bps), 128, 0, s>>>(a);
-		k_hulls_face<<<persistent_blocks(bps), 128, 0, s>>>(a);
-	}
-	else
-		k_hulls_probe<false><<<persistent_blocks(bps), 128, 0, s>>>(a);
+	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
 	launch_hulls_sat(a, maxUE, tune, s);
 }
 
@@ -1160,14 +970,7 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	const int bps = (int)tune.v[B3G_TUNE_PROBE];
-	if (a.faceList)
-	{
-		k_hulls_probe<true><<<persistent_blocks(bps), 128, 0, s>>>(a);
-		k_hulls_face<<<persistent_blocks(bps), 128, 0, s>>>(a);
-	}
-	else
-		k_hulls_probe<false><<<persistent_blocks(bps), 128, 0, s>>>(a);
+	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
 }
 
 // Dynamic shared memory of the SAT kernel with `warps` warps per block.
