@@ -365,6 +365,247 @@ __device__ void build_face_contact(DevManifold& m, const XF& xf1, uint32_t index
 	m.pointCount = cnt;
 }
 
+// Shared-memory buffers of one warp for warp_build_face_contact: two clip
+// polygons (ping-pong) and the kept points of the reference face.
+struct WarpClip
+{
+	ClipV a[B3G_MAX_POLY];
+	ClipV b[B3G_MAX_POLY];
+	CV kept[B3G_MAX_POLY];
+};
+
+// Shared memory of one warp in the hull kernels: the edge records of the edge
+// query, then (the query done) the clip buffers of the face contact.
+__host__ __device__ __forceinline__ size_t sat_warp_bytes(uint32_t maxUE)
+{
+	size_t recs = (size_t)sat_warp_recs(maxUE) * sizeof(EdgeRec);
+	return recs > sizeof(WarpClip) ? recs : sizeof(WarpClip);
+}
+
+// Exclusive prefix sum of v over the warp; *total receives the sum.
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t lane, uint32_t& total)
+{
+	uint32_t x = v;
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+		if (lane >= (uint32_t)o)
+			x += y;
+	}
+	total = __shfl_sync(0xffffffffu, x, 31);
+	return x - v;
+}
+
+// b3ClipPolygonToPlane (clip.cpp:101-150) on the warp: vertex i (lanes take i
+// and i + 32) emits what the sequential loop emits at step i — v2, the
+// intersection, or both — at the place a prefix sum of the emit counts gives,
+// so out holds the sequential loop's polygon, same values, same order. d1 of
+// step i is the distance of vertex i - 1 (n - 1 for step 0), the value the
+// loop carries over. Returns the new vertex count, or B3G_MAX_POLY + 1 when
+// the polygon would outgrow the buffer (the loop fails there too).
+__device__ uint32_t warp_clip_polygon_to_plane(ClipV* out, const ClipV* in, uint32_t n, PL plane, uint32_t edge,
+	uint32_t lane)
+{
+	uint32_t base = 0;
+	for (uint32_t i0 = 0; i0 < n; i0 += 32)
+	{
+		const uint32_t i = i0 + lane;
+		uint32_t cnt = 0;
+		ClipV v1, v2;
+		float d1 = 0.0f, d2 = 0.0f;
+		if (i < n)
+		{
+			v2 = in[i];
+			v1 = in[i == 0 ? n - 1 : i - 1];
+			d2 = pdist(v2.pos, plane);
+			d1 = pdist(v1.pos, plane);
+			if (d1 <= 0.0f && d2 <= 0.0f)
+				cnt = 1;
+			else if (d1 <= 0.0f && d2 > 0.0f)
+				cnt = 1;
+			else if (d1 > 0.0f && d2 <= 0.0f)
+				cnt = 2;
+		}
+		uint32_t total;
+		const uint32_t o = base + warp_excl_scan(cnt, lane, total);
+		base += total;
+		// Writes past the buffer are skipped; the count reports the overflow.
+		if (cnt != 0 && o + cnt <= B3G_MAX_POLY)
+		{
+			if (d1 <= 0.0f && d2 <= 0.0f)
+				out[o] = v2;
+			else if (d1 <= 0.0f && d2 > 0.0f)
+			{
+				float fraction = d1 / (d1 - d2);
+				out[o].pos = v1.pos + fraction * (v2.pos - v1.pos);
+				out[o].pair = mkpair(edge, B3G_NULL_EDGE, v1.pair.outEdge2, B3G_NULL_EDGE);
+			}
+			else
+			{
+				float fraction = d1 / (d1 - d2);
+				out[o].pos = v1.pos + fraction * (v2.pos - v1.pos);
+				out[o].pair = mkpair(B3G_NULL_EDGE, edge, B3G_NULL_EDGE, v2.pair.inEdge2);
+				out[o + 1] = v2;
+			}
+		}
+	}
+	__syncwarp();
+	return base > B3G_MAX_POLY ? B3G_MAX_POLY + 1 : base;
+}
+
+// b3BuildFaceContact (collide_hulls.cpp:75-187) on the warp, with W in
+// shared memory: the incident polygon (lane 0 walks the face loop), the
+// clipping against the reference face's side planes (warp_clip_polygon_to_
+// plane), the kept points and the deepest of them (first minimum: smaller
+// separation, on ties the earlier point), then the reduction to four points
+// and the manifold on lane 0. Same operations and order as build_face_contact;
+// returns the point count on every lane.
+__device__ __noinline__ uint32_t warp_build_face_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1,
+	float r1, const XF& xf2, const HullRef& h2, float r2, bool flipNormal, uint32_t* status, uint32_t lane,
+	WarpClip& W)
+{
+	float totalRadius = r1 + r2;
+	PL localPlane1 = hp(h1, index1);
+	PL plane1 = pmul(xf1, localPlane1);
+	V3 normal1 = rotc(xf2.q, plane1.n);
+	uint32_t index2 = hull_support_face(h2, -normal1);
+	uint32_t n = 0;
+	if (lane == 0)
+	{
+		uint32_t begin = h2.f[index2];
+		uint32_t edge = begin;
+		do
+		{
+			if (n >= B3G_MAX_POLY)
+			{
+				n = B3G_MAX_POLY + 1;
+				break;
+			}
+			ClipV& cv = W.a[n++];
+			cv.pos = xmul(xf2, hv(h2, he_origin(h2, edge)));
+			cv.pair = mkpair(B3G_NULL_EDGE, B3G_NULL_EDGE, he_prev(h2, edge), edge);
+			edge = he_next(h2, edge);
+		} while (edge != begin);
+	}
+	n = __shfl_sync(0xffffffffu, n, 0);
+	__syncwarp();
+	bool ok = n <= B3G_MAX_POLY;
+	ClipV* in = W.a;
+	ClipV* out = W.b;
+	if (ok)
+	{
+		uint32_t begin = h1.f[index1];
+		uint32_t edge = begin;
+		uint32_t guard = 0;
+		do
+		{
+			if (++guard > h1.eCnt)
+			{
+				ok = false;
+				break;
+			}
+			PL plane = hull_edge_side_plane(h1, edge);
+			plane.d += totalRadius;
+			PL cp = pmul(xf1, plane);
+			uint32_t nn = warp_clip_polygon_to_plane(out, in, n, cp, edge, lane);
+			if (nn > B3G_MAX_POLY)
+			{
+				ok = false;
+				break;
+			}
+			ClipV* t = in;
+			in = out;
+			out = t;
+			n = nn;
+			if (n == 0)
+				break;
+			edge = he_next(h1, edge);
+		} while (edge != begin);
+	}
+	if (!ok)
+	{
+		if (lane == 0)
+			atomicOr(status, B3G_ST_POLY_OVERFLOW);
+		return 0;
+	}
+	if (n == 0)
+		return 0;
+	// Kept points (separation within the radius), projected on the reference
+	// plane, in order; the first of the smallest separation.
+	uint32_t base = 0;
+	float bestS = B3G_MAX_SCALAR;
+	uint32_t bestK = 0xFFFFFFFFu;
+	for (uint32_t i0 = 0; i0 < n; i0 += 32)
+	{
+		const uint32_t i = i0 + lane;
+		bool keep = false;
+		V3 p{0.0f, 0.0f, 0.0f};
+		float sep = 0.0f;
+		if (i < n)
+		{
+			p = in[i].pos;
+			sep = pdist(p, plane1);
+			keep = sep <= totalRadius;
+		}
+		uint32_t total;
+		const uint32_t k = base + warp_excl_scan(keep ? 1u : 0u, lane, total);
+		if (keep)
+		{
+			W.kept[k].pos = pclosest(p, plane1);
+			W.kept[k].clipIndex = i;
+			if (sep < bestS || (sep == bestS && k < bestK))
+			{
+				bestS = sep;
+				bestK = k;
+			}
+		}
+		base += total;
+	}
+	const uint32_t n1 = base;
+	if (n1 == 0)
+		return 0;
+	for (int o = 16; o > 0; o >>= 1)
+	{
+		float os = __shfl_xor_sync(0xffffffffu, bestS, o);
+		uint32_t ok2 = __shfl_xor_sync(0xffffffffu, bestK, o);
+		if (os < bestS || (os == bestS && ok2 < bestK))
+		{
+			bestS = os;
+			bestK = ok2;
+		}
+	}
+	__syncwarp();
+	uint32_t cnt = 0;
+	if (lane == 0)
+	{
+		V3 normal = plane1.n;
+		V3 oriented = flipNormal ? -normal : normal;
+		CV red[4];
+		cnt = reduce_polygon(red, W.kept, n1, oriented, bestK);
+		for (uint32_t i = 0; i < cnt; ++i)
+		{
+			const ClipV& v2 = in[red[i].clipIndex];
+			V3 v1 = pclosest(v2.pos, plane1);
+			DevPoint& mp = m.points[i];
+			if (flipNormal)
+			{
+				set_point(mp, rotc(xf2.q, oriented), xmult(xf2, v2.pos), xmult(xf1, v1));
+				set_id(mp, mkpair(v2.pair.inEdge2, v2.pair.outEdge2, v2.pair.inEdge1, v2.pair.outEdge1));
+			}
+			else
+			{
+				set_point(mp, rotc(xf1.q, oriented), xmult(xf1, v1), xmult(xf2, v2.pos));
+				set_id(mp, v2.pair);
+			}
+			mp.edgeContact = 0;
+		}
+		m.pointCount = cnt;
+	}
+	cnt = __shfl_sync(0xffffffffu, cnt, 0);
+	__syncwarp();
+	return cnt;
+}
+
 // b3RebuildEdgeContact (collide_hulls.cpp:266-321).
 __device__ void rebuild_edge_contact(DevManifold& m, const XF& xf1, uint32_t index1, const HullRef& h1,
 	const XF& xf2, uint32_t index2, const HullRef& h2)
@@ -451,19 +692,17 @@ struct HullCtx
 	EdgeRec* recs;
 	uint32_t maxUE;
 	uint32_t* status;
+	WarpClip* clip; // the warp's shared clip buffers
 };
 
 // Lane 0 builds, the warp learns the point count.
+// Face contact on the warp (H.clip: the warp's shared clip buffers); every
+// lane learns the point count.
 __device__ uint32_t face_contact_all(DevManifold& m, const HullCtx& H, bool flip, uint32_t index, uint32_t lane)
 {
-	if (lane == 0)
-	{
-		if (flip)
-			build_face_contact(m, H.xf2, index, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status);
-		else
-			build_face_contact(m, H.xf1, index, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status);
-	}
-	return __shfl_sync(0xffffffffu, m.pointCount, 0);
+	if (flip)
+		return warp_build_face_contact(m, H.xf2, index, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status, lane, *H.clip);
+	return warp_build_face_contact(m, H.xf1, index, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status, lane, *H.clip);
 }
 
 // b3CollideHulls without cache (collide_hulls.cpp:189-264).
@@ -519,13 +758,22 @@ __device__ uint32_t read_face_thread(const XF& xf1, const HullRef& h1, const XF&
 	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
 }
 
+enum : uint32_t
+{
+	PR_DONE = 0, // the cache decided the contact
+	PR_MISS,     // the cache is flushed: the contact needs the SAT
+	PR_FACE      // an overlap hit whose face contact k_hulls_face rebuilds
+};
+
 // The cache half of b3CollideHullsCache (collide_hulls.cpp:367-415), one
 // thread per contact: b3FeatureCache::ReadState (sat.cpp:178-207), then the
 // separation hit, or the overlap hit that rebuilds the cached edge or face
-// contact. Returns true when the contact is finished; otherwise the cache is
-// flushed (cacheType = empty, the feature fields as ReadState left them) and
-// the contact needs the SAT.
-__device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
+// contact. On a miss the cache is flushed (cacheType = empty, the feature
+// fields as ReadState left them) and the contact needs the SAT. With
+// DEFER_FACE an overlap hit on a face returns PR_FACE with the cache as read:
+// its clipping runs on a whole warp in k_hulls_face.
+template <bool DEFER_FACE>
+__device__ uint32_t probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 {
 	float totalRadius = H.r1 + H.r2;
 	uint32_t state0 = cache.x;
@@ -546,20 +794,35 @@ __device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 	else
 		state1 = CT_EMPTY;
 	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
-		return true; // separation cache hit
+		return PR_DONE; // separation cache hit
 	if (state0 == CT_OVERLAP && state1 == CT_OVERLAP)
 	{
 		if (cache.y == FT_EDGES)
 			rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
-		else if (cache.y == FT_FACE1)
+		else if (DEFER_FACE && (cache.y == FT_FACE1 || cache.y == FT_FACE2))
+			return PR_FACE;
+		else if (!DEFER_FACE && cache.y == FT_FACE1)
 			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
-		else if (cache.y == FT_FACE2)
+		else if (!DEFER_FACE && cache.y == FT_FACE2)
 			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
 		if (m.pointCount > 0)
-			return true; // overlap cache hit
+			return PR_DONE; // overlap cache hit
 	}
 	cache.x = CT_EMPTY;
-	return false;
+	return PR_MISS;
+}
+
+// Warp-aggregated append of c to a list (the calling lanes of the warp).
+__device__ __forceinline__ void warp_append(uint32_t* list, uint32_t* count, uint32_t c)
+{
+	uint32_t mask = __activemask();
+	uint32_t lane = threadIdx.x & 31;
+	uint32_t leader = __ffs(mask) - 1;
+	uint32_t base = 0;
+	if (lane == leader)
+		base = atomicAdd(count, (uint32_t)__popc(mask));
+	base = __shfl_sync(mask, base, leader);
+	list[base + __popc(mask & ((1u << lane) - 1u))] = c;
 }
 
 // The SAT half of b3CollideHullsCache (collide_hulls.cpp:417-515), one warp
@@ -648,9 +911,11 @@ __device__ __forceinline__ void load_hull_ctx(const NPArgs& a, uint32_t c, HullC
 	H.status = a.status;
 	H.recs = nullptr;
 	H.maxUE = 0;
+	H.clip = nullptr;
 }
 
 // Pass 1: one thread per hull-hull contact reads its feature cache.
+template <bool DEFER_FACE>
 __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 {
 	uint32_t n = *a.listCount;
@@ -661,30 +926,74 @@ __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
 		DevManifold& m = a.man[c];
 		man_clear(m);
-		bool done = false;
+		uint32_t r = PR_MISS;
 		if (a.convexCache)
 		{
 			HullCtx H;
 			load_hull_ctx(a, c, H);
-			done = probe_cache(m, H, cache);
+			r = probe_cache<DEFER_FACE>(m, H, cache);
 		}
 		a.cache[c] = cache;
-		if (done)
-		{
+		if (r == PR_DONE)
 			finish_convex(a, c, m);
-		}
+		else if (DEFER_FACE && r == PR_FACE)
+			warp_append(a.faceList, a.faceCount, c);
 		else
+			warp_append(a.missList, a.missCount, c);
+	}
+}
+
+// Pass 1b: one warp per overlap hit on a cached face (b3RebuildFaceContact,
+// collide_hulls.cpp:323-353, from b3CollideHullsCache :395-414), the clipping
+// on the warp in shared memory: the face contact is rebuilt when the relative
+// rotation stayed within the tolerance; a rebuild without points flushes the
+// cache and sends the contact to the SAT, as the probe would have.
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_hulls_face(NPArgs a)
+{
+	__shared__ WarpClip clipBuf[W];
+	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const uint32_t n = *a.faceCount;
+	for (uint32_t t = blockIdx.x * W + warp; t < n; t += gridDim.x * W)
+	{
+		const uint32_t c = a.faceList[t];
+		HullCtx H;
+		load_hull_ctx(a, c, H);
+		uint4 cache = a.cache[c];
+		DevManifold& m = a.man[c];
+		const bool flip = cache.y == FT_FACE2;
+		const XF& xfA = flip ? H.xf2 : H.xf1;
+		const XF& xfB = flip ? H.xf1 : H.xf2;
+		const XF& xf0A = flip ? H.xf02 : H.xf01;
+		const XF& xf0B = flip ? H.xf01 : H.xf02;
+		// b3RebuildFaceContact's rotation test (collide_hulls.cpp:330-341).
+		Q4 dq0 = qmul(conj(xf0A.q), xf0B.q);
+		Q4 dq = qmul(conj(xfA.q), xfB.q);
+		Q4 q = qmul(conj(dq0), dq);
+		const float kCosTol = 0.995f;
+		uint32_t pc = 0;
+		if (fabsr(q.s) > kCosTol)
 		{
-			// Warp-aggregated append to the SAT list.
-			uint32_t mask = __activemask();
-			uint32_t lane = threadIdx.x & 31;
-			uint32_t leader = __ffs(mask) - 1;
-			uint32_t base = 0;
-			if (lane == leader)
-				base = atomicAdd(a.missCount, (uint32_t)__popc(mask));
-			base = __shfl_sync(mask, base, leader);
-			a.missList[base + __popc(mask & ((1u << lane) - 1u))] = c;
+			if (flip)
+				pc = warp_build_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status, lane,
+					clipBuf[warp]);
+			else
+				pc = warp_build_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status, lane,
+					clipBuf[warp]);
 		}
+		if (lane == 0)
+		{
+			if (pc > 0)
+				finish_convex(a, c, m);
+			else
+			{
+				cache.x = CT_EMPTY;
+				a.cache[c] = cache;
+				uint32_t slot = atomicAdd(a.missCount, 1u);
+				a.missList[slot] = c;
+			}
+		}
+		__syncwarp();
 	}
 }
 
@@ -694,7 +1003,8 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
+	char* wsm = reinterpret_cast<char*>(smem) + (size_t)warp * sat_warp_bytes(maxUE);
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(wsm);
 	uint32_t n = *a.missCount;
 	uint32_t gw = blockIdx.x * W + warp;
 	uint32_t nw = gridDim.x * W;
@@ -704,6 +1014,7 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 		HullCtx H;
 		load_hull_ctx(a, c, H);
 		H.recs = recs;
+		H.clip = reinterpret_cast<WarpClip*>(wsm);
 		H.maxUE = maxUE;
 		uint4 cache = a.cache[c];
 		DevManifold& m = a.man[c];
@@ -784,7 +1095,8 @@ __global__ void __launch_bounds__(W * 32) k_hull_triangle(NPArgs a, uint32_t max
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
+	char* wsm = reinterpret_cast<char*>(smem) + (size_t)warp * sat_warp_bytes(maxUE);
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(wsm);
 	uint32_t n = *a.listCount;
 	for (uint32_t t = blockIdx.x * W + warp; t < n; t += gridDim.x * W)
 	{
@@ -799,6 +1111,7 @@ __global__ void __launch_bounds__(W * 32) k_hull_triangle(NPArgs a, uint32_t max
 		H.r2 = a.S.fixParams[3 * fb + 2].y;
 		H.status = a.status;
 		H.recs = recs;
+		H.clip = reinterpret_cast<WarpClip*>(wsm);
 		H.maxUE = maxUE;
 		DevManifold& m = a.man[c];
 		if (lane == 0)
@@ -828,7 +1141,8 @@ __global__ void __launch_bounds__(W * 32) k_mesh_items_hull(NPArgs a, Buffers B,
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	EdgeRec* recs = reinterpret_cast<EdgeRec*>(smem) + (size_t)warp * sat_warp_recs(maxUE);
+	char* wsm = reinterpret_cast<char*>(smem) + (size_t)warp * sat_warp_bytes(maxUE);
+	EdgeRec* recs = reinterpret_cast<EdgeRec*>(wsm);
 	uint32_t n = min(B.counters[CTR_MESH_PAIRS], B.meshPairCap);
 	for (uint32_t i = blockIdx.x * W + warp; i < n; i += gridDim.x * W)
 	{
@@ -847,6 +1161,7 @@ __global__ void __launch_bounds__(W * 32) k_mesh_items_hull(NPArgs a, Buffers B,
 		H.r2 = tri.radius;
 		H.status = a.status;
 		H.recs = recs;
+		H.clip = reinterpret_cast<WarpClip*>(wsm);
 		H.maxUE = maxUE;
 		DevManifold& m = B.meshPairMan[i];
 		if (lane == 0)
@@ -927,7 +1242,7 @@ void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint3
 template <int W>
 void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
 {
-	size_t smem = (size_t)W * sat_warp_recs(maxUE) * sizeof(EdgeRec);
+	size_t smem = (size_t)W * sat_warp_bytes(maxUE);
 	static size_t configured = 0;
 	if (smem > 48 * 1024 && smem > configured)
 	{
@@ -943,7 +1258,7 @@ void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* coun
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
+	launch_hulls_probe(a, a.list, a.listCount, tune, s);
 	launch_hulls_sat(a, maxUE, tune, s);
 }
 
@@ -970,13 +1285,20 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
+	const int bps = (int)tune.v[B3G_TUNE_PROBE];
+	if (a.faceList && a.convexCache)
+	{
+		k_hulls_probe<true><<<persistent_blocks(bps), 128, 0, s>>>(a);
+		k_hulls_face<4><<<persistent_blocks(bps), 128, 0, s>>>(a);
+	}
+	else
+		k_hulls_probe<false><<<persistent_blocks(bps), 128, 0, s>>>(a);
 }
 
 // Dynamic shared memory of the SAT kernel with `warps` warps per block.
 size_t hull_sat_smem(int warps, uint32_t maxUE)
 {
-	return (size_t)warps * sat_warp_recs(maxUE) * sizeof(EdgeRec);
+	return (size_t)warps * sat_warp_bytes(maxUE);
 }
 
 void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s)
