@@ -504,7 +504,6 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.lateDestroyed, C), "alloc");
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
 	step(dalloc(&B.missList, C), "alloc");
-	step(dalloc(&B.faceList, C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
 	step(dalloc(&c->dUpdateBad, 1), "alloc");
 	step(dalloc(&B.totals, 8), "alloc");
@@ -600,7 +599,6 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.tWake);
 	dfree(B.bucketList);
 	dfree(B.missList);
-	dfree(B.faceList);
 	dfree(B.counters);
 	dfree(B.totals);
 	if (c->profEvents)
@@ -1512,10 +1510,10 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-	// pass_begin, sync, broadphase, diff + list order, bucket + apart + convex kernels + 3 hull +
+	// pass_begin, sync, broadphase, diff + list order, bucket + apart + convex kernels + 2 hull +
 	// hull-triangle, finalize + pass_end + settle
 	const uint32_t passLaunches = 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
-		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 3 + 1 + mesh_launches(c) + 3;
+		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
 	// Host state takes the graph path when it is pinned (a graph copies it
 	// asynchronously; pageable memory would need the synchronous copy).
 	bool pinnedHost = false;
@@ -1782,7 +1780,7 @@ extern "C" int b3g_finish_pass(b3g_ctx* c, const uint8_t* keep, uint32_t count)
 	prof_mark(c, PM_FINAL, s);
 	if (c->profiling)
 		++c->profPass;
-	c->launches += pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 3 + 1 + mesh_launches(c) + 3 +
+	c->launches += pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3 +
 		(rejected.empty() ? 0 : 1);
 	CK(cudaGetLastError());
 	c->creationPass = false;
@@ -2504,8 +2502,6 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 		a.ex0B = dX0B;
 		a.missList = dMiss;
 		a.missCount = dMissCount;
-		a.faceList = nullptr;
-		a.faceCount = nullptr;
 		std::vector<uint32_t> flat(n), counts(BK_COUNT, 0);
 		std::vector<uint32_t> offs(BK_COUNT, 0);
 		uint32_t o = 0;
@@ -2717,7 +2713,6 @@ extern "C" int b3g_autotune(b3g_ctx* c, uint32_t reps, void* stream, uint32_t* o
 	const uint32_t* hullCount = B.counters + CTR_BUCKET0 + BK_HULLS;
 	auto probe = [&] {
 		cudaMemsetAsync(B.counters + CTR_HULL_MISS, 0, sizeof(uint32_t), s);
-		cudaMemsetAsync(B.counters + CTR_HULL_FACE, 0, sizeof(uint32_t), s);
 		launch_hulls_probe(a, hullList, hullCount, c->tune, s);
 	};
 	if (h[CTR_BUCKET0 + BK_HULLS] && rc == B3G_OK)

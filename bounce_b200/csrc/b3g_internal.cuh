@@ -196,7 +196,6 @@ struct Buffers
 	// narrowphase work lists
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
 	uint32_t* missList;   // hull-hull contacts for the SAT kernel
-	uint32_t* faceList;   // hull-hull contacts whose cached face contact is rebuilt
 	uint32_t* counters;   // device counters (see CTR_*)
 	unsigned long long* totals; // cumulative: passes, contacts, manifolds, points, begun, ended
 	uint32_t* endedList;  // 3 u32 per ended contact
@@ -298,8 +297,7 @@ enum
 	CTR_MESH_PAIRS = 31, // (contact, triangle) work items of the pass
 	CTR_TRAV_OVERFLOW = 32, // traversal records past the scratch slots
 	CTR_CANDIDATES = 33,    // new pairs handed to the caller's contact filter
-	CTR_HULL_FACE = 34,     // hull-hull contacts whose cached face contact is rebuilt
-	CTR_COUNT = 35
+	CTR_COUNT = 34
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 

@@ -566,10 +566,6 @@ struct NPArgs
 	// hull-hull pairs the feature cache could not resolve
 	uint32_t* missList;
 	uint32_t* missCount;
-	// hull-hull pairs whose cached face contact is rebuilt by its own kernel
-	// (null: the probe rebuilds it)
-	uint32_t* faceList;
-	uint32_t* faceCount;
 	// manifolds 1 and 2 of mesh contacts (null without meshes)
 	DevManifold* extraCur;
 	const DevManifold* extraPrev;

@@ -758,22 +758,15 @@ __device__ uint32_t read_face_thread(const XF& xf1, const HullRef& h1, const XF&
 	return s > totalRadius ? CT_SEPARATION : CT_OVERLAP;
 }
 
-enum : uint32_t
-{
-	PR_DONE = 0, // the cache decided the contact
-	PR_MISS,     // the cache is flushed: the contact needs the SAT
-	PR_FACE      // an overlap hit whose face contact k_hulls_face rebuilds
-};
-
 // The cache half of b3CollideHullsCache (collide_hulls.cpp:367-415), one
 // thread per contact: b3FeatureCache::ReadState (sat.cpp:178-207), then the
 // separation hit, or the overlap hit that rebuilds the cached edge or face
-// contact. On a miss the cache is flushed (cacheType = empty, the feature
-// fields as ReadState left them) and the contact needs the SAT. With
-// DEFER_FACE an overlap hit on a face returns PR_FACE with the cache as read:
-// its clipping runs on a whole warp in k_hulls_face.
-template <bool DEFER_FACE>
-__device__ uint32_t probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
+// contact. Returns true when the contact is finished; otherwise the cache is
+// flushed (cacheType = empty, the feature fields as ReadState left them) and
+// the contact needs the SAT. The face rebuild clips on this thread: the
+// polygons are small (3 or 4 vertices on these hulls), and a warp per rebuild
+// measured slower than the threads that do it here.
+__device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 {
 	float totalRadius = H.r1 + H.r2;
 	uint32_t state0 = cache.x;
@@ -794,22 +787,20 @@ __device__ uint32_t probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 	else
 		state1 = CT_EMPTY;
 	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
-		return PR_DONE; // separation cache hit
+		return true; // separation cache hit
 	if (state0 == CT_OVERLAP && state1 == CT_OVERLAP)
 	{
 		if (cache.y == FT_EDGES)
 			rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
-		else if (DEFER_FACE && (cache.y == FT_FACE1 || cache.y == FT_FACE2))
-			return PR_FACE;
-		else if (!DEFER_FACE && cache.y == FT_FACE1)
+		else if (cache.y == FT_FACE1)
 			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
-		else if (!DEFER_FACE && cache.y == FT_FACE2)
+		else if (cache.y == FT_FACE2)
 			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
 		if (m.pointCount > 0)
-			return PR_DONE; // overlap cache hit
+			return true; // overlap cache hit
 	}
 	cache.x = CT_EMPTY;
-	return PR_MISS;
+	return false;
 }
 
 // Warp-aggregated append of c to a list (the calling lanes of the warp).
@@ -915,7 +906,6 @@ __device__ __forceinline__ void load_hull_ctx(const NPArgs& a, uint32_t c, HullC
 }
 
 // Pass 1: one thread per hull-hull contact reads its feature cache.
-template <bool DEFER_FACE>
 __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 {
 	uint32_t n = *a.listCount;
@@ -926,74 +916,18 @@ __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 		uint4 cache = prev >= 0 ? a.prevCache[prev] : make_uint4(CT_EMPTY, FT_FACE1, 0, 0);
 		DevManifold& m = a.man[c];
 		man_clear(m);
-		uint32_t r = PR_MISS;
+		bool done = false;
 		if (a.convexCache)
 		{
 			HullCtx H;
 			load_hull_ctx(a, c, H);
-			r = probe_cache<DEFER_FACE>(m, H, cache);
+			done = probe_cache(m, H, cache);
 		}
 		a.cache[c] = cache;
-		if (r == PR_DONE)
+		if (done)
 			finish_convex(a, c, m);
-		else if (DEFER_FACE && r == PR_FACE)
-			warp_append(a.faceList, a.faceCount, c);
 		else
 			warp_append(a.missList, a.missCount, c);
-	}
-}
-
-// Pass 1b: one warp per overlap hit on a cached face (b3RebuildFaceContact,
-// collide_hulls.cpp:323-353, from b3CollideHullsCache :395-414), the clipping
-// on the warp in shared memory: the face contact is rebuilt when the relative
-// rotation stayed within the tolerance; a rebuild without points flushes the
-// cache and sends the contact to the SAT, as the probe would have.
-template <int W>
-__global__ void __launch_bounds__(W * 32) k_hulls_face(NPArgs a)
-{
-	__shared__ WarpClip clipBuf[W];
-	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const uint32_t n = *a.faceCount;
-	for (uint32_t t = blockIdx.x * W + warp; t < n; t += gridDim.x * W)
-	{
-		const uint32_t c = a.faceList[t];
-		HullCtx H;
-		load_hull_ctx(a, c, H);
-		uint4 cache = a.cache[c];
-		DevManifold& m = a.man[c];
-		const bool flip = cache.y == FT_FACE2;
-		const XF& xfA = flip ? H.xf2 : H.xf1;
-		const XF& xfB = flip ? H.xf1 : H.xf2;
-		const XF& xf0A = flip ? H.xf02 : H.xf01;
-		const XF& xf0B = flip ? H.xf01 : H.xf02;
-		// b3RebuildFaceContact's rotation test (collide_hulls.cpp:330-341).
-		Q4 dq0 = qmul(conj(xf0A.q), xf0B.q);
-		Q4 dq = qmul(conj(xfA.q), xfB.q);
-		Q4 q = qmul(conj(dq0), dq);
-		const float kCosTol = 0.995f;
-		uint32_t pc = 0;
-		if (fabsr(q.s) > kCosTol)
-		{
-			if (flip)
-				pc = warp_build_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.status, lane,
-					clipBuf[warp]);
-			else
-				pc = warp_build_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.status, lane,
-					clipBuf[warp]);
-		}
-		if (lane == 0)
-		{
-			if (pc > 0)
-				finish_convex(a, c, m);
-			else
-			{
-				cache.x = CT_EMPTY;
-				a.cache[c] = cache;
-				uint32_t slot = atomicAdd(a.missCount, 1u);
-				a.missList[slot] = c;
-			}
-		}
-		__syncwarp();
 	}
 }
 
@@ -1285,14 +1219,7 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 	NPArgs a = base;
 	a.list = list;
 	a.listCount = count;
-	const int bps = (int)tune.v[B3G_TUNE_PROBE];
-	if (a.faceList && a.convexCache)
-	{
-		k_hulls_probe<true><<<persistent_blocks(bps), 128, 0, s>>>(a);
-		k_hulls_face<4><<<persistent_blocks(bps), 128, 0, s>>>(a);
-	}
-	else
-		k_hulls_probe<false><<<persistent_blocks(bps), 128, 0, s>>>(a);
+	k_hulls_probe<<<persistent_blocks((int)tune.v[B3G_TUNE_PROBE]), 128, 0, s>>>(a);
 }
 
 // Dynamic shared memory of the SAT kernel with `warps` warps per block.

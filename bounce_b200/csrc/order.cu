@@ -509,7 +509,6 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 			cudaMemsetAsync(B.counters + CTR_BUCKET0, 0, sizeof(uint32_t) * BK_COUNT, s);
 			cudaMemsetAsync(B.counters + CTR_WAKE_ACTIVATED, 0, sizeof(uint32_t), s);
 			cudaMemsetAsync(B.counters + CTR_HULL_MISS, 0, sizeof(uint32_t), s);
-			cudaMemsetAsync(B.counters + CTR_HULL_FACE, 0, sizeof(uint32_t), s);
 			k_wake_activate<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, cap, nInactive);
 			++launches;
 			if (!fetch())

@@ -331,8 +331,6 @@ NPArgs make_np_args(b3g_ctx* c)
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
 	a.missList = B.missList;
 	a.missCount = B.counters + CTR_HULL_MISS;
-	a.faceList = B.faceList;
-	a.faceCount = B.counters + CTR_HULL_FACE;
 	a.extraCur = B.extraMan[cur];
 	a.extraPrev = B.extraMan[prev];
 	return a;
