@@ -425,6 +425,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->candFetched = false;
 	c->passOpen = false;
 	c->filterMode = 0;
+	c->walkLimit = 0;
 	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
 	{
 		delete c;
@@ -2632,6 +2633,17 @@ extern "C" int b3g_set_tuning(b3g_ctx* c, const uint32_t* t)
 	destroy_graphs(c);
 	for (int k = 0; k < B3G_TUNE_COUNT; ++k)
 		c->tune.v[k] = t[k];
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_walk_limit(b3g_ctx* c, uint32_t maxNodes)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	CK(cudaSetDevice(c->device));
+	CK(cudaDeviceSynchronize());
+	destroy_graphs(c); // captured passes hold the old limit
+	c->walkLimit = maxNodes;
 	return B3G_OK;
 }
 

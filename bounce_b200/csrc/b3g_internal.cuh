@@ -448,6 +448,7 @@ struct b3g_ctx
 	bool passOpen;       // b3g_collide stopped before the contact list for the filter
 	cudaStream_t passStream; // the stream of the open pass
 	int filterMode;      // FilterArgs::mode of the pass under way
+	uint32_t walkLimit;  // node visits per broadphase walk (0: the depth-first bound), b3g_set_walk_limit
 
 	// stage profiling: a ring of per-pass event sets
 	bool profiling;

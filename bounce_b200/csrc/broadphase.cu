@@ -730,7 +730,7 @@ __device__ __forceinline__ uint2 canon_pair(const DevScene& S, uint32_t pa, uint
 constexpr uint32_t TRAV_SLOTS = B3G_TRAV_SLOTS;
 
 template <bool MW>
-__device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cap)
+__device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, int j, uint32_t cap, uint32_t limit)
 {
 	uint32_t leaf = n - 1 + j;
 	float4 ql = __ldg(B.nodeLo + leaf), qh = __ldg(B.nodeHi + leaf);
@@ -742,7 +742,7 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 	uint2* scratch = reinterpret_cast<uint2*>(B.pairScratch);
 	// A depth-first walk visits each of the 2n - 1 nodes at most once.
 	uint32_t steps = 0;
-	const uint32_t maxSteps = 2u * (uint32_t)n + 1u;
+	const uint32_t maxSteps = limit ? limit : 2u * (uint32_t)n + 1u;
 	const uint32_t nodes = 2u * (uint32_t)n - 1u;
 	while (node != SENT)
 	{
@@ -783,8 +783,10 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 	return count;
 }
 
+// limit: node visits allowed per walk (0: 2n + 1, more than a depth-first
+// walk makes), see b3g_set_walk_limit.
 template <bool MW>
-__global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
+__global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap, uint32_t limit)
 {
 	int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= n)
@@ -794,7 +796,7 @@ __global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uin
 		B.leafCount[j] = 0;
 		return;
 	}
-	B.leafCount[j] = walk<MW>(S, B, n, j, cap);
+	B.leafCount[j] = walk<MW>(S, B, n, j, cap, limit);
 }
 
 // One thread per (slot, leaf), slot-major: copies the scratch records to the
@@ -1018,9 +1020,11 @@ void launch_traverse(b3g_ctx* c, cudaStream_t s)
 	const int tb = (int)c->tune.v[B3G_TUNE_TRAVERSE];
 	cudaMemsetAsync(B.counters + CTR_TRAV_OVERFLOW, 0, sizeof(uint32_t), s);
 	if (c->nWorlds > 1)
-		k_traverse_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts,
+			c->walkLimit);
 	else
-		k_traverse_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
+		k_traverse_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts,
+			c->walkLimit);
 	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, s);
 	if (c->nWorlds > 1)
 		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);

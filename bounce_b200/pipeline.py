@@ -132,6 +132,10 @@ class CollisionPipeline:
             k = np.ascontiguousarray(keep, np.uint8)
             self._check(self.lib.b3g_finish_pass(self.ctx, N.ptr(k, ctypes.c_uint8) if len(k) else None, len(k)))
 
+    def set_walk_limit(self, max_nodes):
+        """Node visits allowed per broadphase walk (0: the depth-first bound)."""
+        self._check(self.lib.b3g_set_walk_limit(self.ctx, int(max_nodes)))
+
     def counts(self):
         c = N.Counts()
         self._check(self.lib.b3g_get_counts(self.ctx, ctypes.byref(c)))

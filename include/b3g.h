@@ -471,6 +471,19 @@ const char* b3g_stage_name(uint32_t stage);
 #define B3G_TUNE_COUNT 13
 int b3g_autotune(b3g_ctx* ctx, uint32_t reps, void* stream, uint32_t* out);
 int b3g_set_tuning(b3g_ctx* ctx, const uint32_t* table);
+
+/* Bounded waits. The device work never waits without a bound: the radix
+ * sort's and the solver input's look-backs spin at most 2^22 times, and every
+ * tree walk (broadphase pair search, queries) visits at most the nodes of a
+ * depth-first walk; a wait that runs out sets the pass status, and the call
+ * that reads it (b3g_get_counts) returns B3G_E_TIMEOUT with the context still
+ * usable; the next pass starts clean. b3g_set_walk_limit lowers the bound of
+ * the broadphase walks to max_nodes node visits (0 restores the depth-first
+ * bound), so that a test can make a wait run out on purpose: the walks stop
+ * early, leave fewer pairs than exist, and report the timeout. The captured
+ * passes are dropped so the new bound takes effect. The reference has no
+ * counterpart (its walks and sorts run on the host without bounds). */
+int b3g_set_walk_limit(b3g_ctx* ctx, uint32_t max_nodes);
 int b3g_get_tuning(b3g_ctx* ctx, uint32_t* table);
 
 /* Device pointers of the last pass's results for zero-copy consumers:

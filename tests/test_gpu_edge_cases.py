@@ -104,3 +104,45 @@ def test_coincident_shapes(oracle_mod):
     assert pipe.counts()["contacts"] == len(specs)
     assert pipe.counts()["touching"] >= len(specs) - 2
     pipe.close()
+
+
+def test_walk_limit_reports_timeout_and_recovers(oracle_mod):
+    """A device wait that runs out is reported, not hidden, and leaves the
+    context usable: with the broadphase walks capped at 3 node visits the pass
+    reports B3G_E_TIMEOUT (b3g_get_counts) and finds fewer pairs; with the
+    bound restored the next passes match the reference again."""
+    sc = S.mixed_scene(seed=61, n=1500, side=14.0).finalize()
+    rw = oracle_mod.RefWorld(sc)
+    sc.set_local_centers(rw.local_centers())
+    drv = S.KinematicDriver(sc)
+    pipe = CollisionPipeline(sc)
+    rw.first_pass()
+    pipe.collide(drv.state17())
+    full = pipe.counts()["contacts"]
+    compare_contacts(pipe, rw, "before the limit")
+    pipe.set_walk_limit(3)
+    drv.advance()
+    pipe.collide(drv.state17())
+    with pytest.raises(N.B3GError) as err:
+        pipe.counts()
+    assert err.value.code == N.B3G_E_TIMEOUT
+    assert pipe.pass_stats()["raw_pairs"] < full
+    pipe.set_walk_limit(0)
+    # The next pass starts clean; its new contacts (all pairs again) then
+    # match a reference world driven through the same motion.
+    rw2 = oracle_mod.RefWorld(sc)
+    rw2.set_local_centers(sc.local_center)
+    rw2.first_pass()
+    drv2 = S.KinematicDriver(sc)
+    for _ in range(2):
+        drv2.advance()
+        rw2.set_sweeps(drv2.sweeps14())
+        rw2.step_pass()
+    drv.advance()
+    pipe.collide(drv.state17())
+    assert pipe.counts()["status"] == 0
+    g = pipe.contacts()
+    r = rw2.pairs()
+    key = lambda a: np.sort((a[:, 0].astype(np.uint64) << np.uint64(32)) | a[:, 1])
+    assert np.array_equal(key(g), key(r))
+    pipe.close()
