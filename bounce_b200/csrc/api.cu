@@ -714,7 +714,7 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 	CK(cudaSetDevice(c->device));
 	CK(cudaStreamSynchronize(c->stream));
 	destroy_graphs(c);
-	uint32_t nv = 0, ne = 0, nf = 0, maxUE = 0;
+	uint32_t nv = 0, ne = 0, nf = 0, maxUE = 0, maxV = 0, maxE = 0, maxF = 0;
 	std::vector<HullDesc> hd(nh);
 	for (uint32_t h = 0; h < nh; ++h)
 	{
@@ -751,6 +751,9 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 		ne = std::max(ne, d[2] + d[3]);
 		nf = std::max(nf, d[4] + d[5]);
 		maxUE = std::max(maxUE, d[3] / 2);
+		maxV = std::max(maxV, d[1]);
+		maxE = std::max(maxE, d[3]);
+		maxF = std::max(maxF, d[5]);
 	}
 	if (c->cfg.max_hull_data && (size_t)nv + ne + nf > c->cfg.max_hull_data)
 		return fail(c, B3G_E_CAPACITY, "hull data %zu exceeds max_hull_data %u", (size_t)nv + ne + nf,
@@ -788,6 +791,9 @@ extern "C" int b3g_set_hulls(b3g_ctx* c, uint32_t nh, const uint32_t* desc, cons
 	c->hullEdges = ne;
 	c->hullFaces = nf;
 	c->maxUniqueEdges = maxUE;
+	c->scene.hullMaxV = maxV;
+	c->scene.hullMaxE = maxE;
+	c->scene.hullMaxF = maxF;
 	c->scene.hulls = c->dHulls;
 	c->scene.hverts = c->dHverts;
 	c->scene.hedges = c->dHedges;

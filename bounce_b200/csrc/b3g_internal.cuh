@@ -94,6 +94,7 @@ struct DevScene
 	const uint4* hedges;   // origin, face, prev, next (twin = i ^ 1)
 	const uint32_t* hfaces;
 	const float4* hplanes; // normal, offset
+	uint32_t hullMaxV, hullMaxE, hullMaxF; // the largest hull's counts (shared-memory staging)
 
 	// bodies
 	const uint32_t* bodyWorld;

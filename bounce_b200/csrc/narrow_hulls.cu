@@ -931,14 +931,89 @@ __global__ void __launch_bounds__(128) k_hulls_probe(NPArgs a)
 	}
 }
 
+// Bulk copies from global into shared memory (the TMA engine without a
+// tensor map: cp.async.bulk, 16-byte aligned addresses, sizes multiples of 16
+// bytes) that complete on a shared-memory barrier. Sources are this GPU's
+// own memory; no multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+	return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t arrivals)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(arrivals) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+				 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t phase)
+{
+	uint32_t done;
+	asm volatile("{\n\t.reg .pred p;\n\t"
+				 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+				 "selp.u32 %0, 1, 0, p;\n\t}"
+				 : "=r"(done)
+				 : "r"(smem_addr(bar)), "r"(phase)
+				 : "memory");
+	return done != 0;
+}
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, uint32_t bytes, unsigned long long* bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+					 smem_addr(dst)),
+				 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+				 : "memory");
+}
+
+// Bytes of one warp's staging area: vertices, planes and half-edges of two
+// hulls of the scene's largest sizes.
+__host__ __device__ __forceinline__ size_t sat_stage_bytes(uint32_t maxV, uint32_t maxF, uint32_t maxE)
+{
+	return 2 * 16 * ((size_t)maxV + maxF + maxE);
+}
+
+// Waits at most STAGE_SPIN polls for the barrier's phase; every lane polls.
+constexpr uint32_t STAGE_SPIN = 1u << 22;
+__device__ __forceinline__ bool stage_wait(unsigned long long* bar, uint32_t phase)
+{
+	for (uint32_t k = 0; k < STAGE_SPIN; ++k)
+		if (mbar_try_wait(bar, phase))
+			return true;
+	return false;
+}
+
 // Pass 2: one warp per contact the cache did not resolve (W warps per block).
-template <int W>
+// With STAGE, each pair's hull vertices, planes and half-edges are brought
+// into the warp's shared memory by bulk copies (lane 0 issues six, the warp
+// waits on its barrier), and the face and edge queries and the face contact
+// read them there instead of from global memory, where every lane's loop
+// over the other hull's vertices waited on each load. Shared memory per block:
+// W barriers (16-byte rounded), then per warp its query / clip area
+// (sat_warp_bytes), then per warp its staging area (sat_stage_bytes).
+template <int W, bool STAGE>
 __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 {
 	extern __shared__ float4 smem[];
 	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	char* wsm = reinterpret_cast<char*>(smem) + (size_t)warp * sat_warp_bytes(maxUE);
+	const size_t barBytes = STAGE ? ((W * 8 + 15) & ~15) : 0;
+	char* base = reinterpret_cast<char*>(smem) + barBytes;
+	char* wsm = base + (size_t)warp * sat_warp_bytes(maxUE);
 	EdgeRec* recs = reinterpret_cast<EdgeRec*>(wsm);
+	unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem) + warp;
+	const size_t stageBytes = sat_stage_bytes(a.S.hullMaxV, a.S.hullMaxF, a.S.hullMaxE);
+	char* stage = base + (size_t)W * sat_warp_bytes(maxUE) + (size_t)warp * stageBytes;
+	uint32_t phase = 0;
+	if (STAGE)
+	{
+		if (lane == 0)
+		{
+			mbar_init(bar, 1);
+			asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+		}
+		__syncwarp();
+	}
 	uint32_t n = *a.missCount;
 	uint32_t gw = blockIdx.x * W + warp;
 	uint32_t nw = gridDim.x * W;
@@ -950,6 +1025,46 @@ __global__ void __launch_bounds__(W * 32) k_hulls_sat(NPArgs a, uint32_t maxUE)
 		H.recs = recs;
 		H.clip = reinterpret_cast<WarpClip*>(wsm);
 		H.maxUE = maxUE;
+		if (STAGE)
+		{
+			float4* v1 = reinterpret_cast<float4*>(stage);
+			float4* p1 = v1 + H.h1.vCnt;
+			uint4* e1 = reinterpret_cast<uint4*>(p1 + H.h1.fCnt);
+			float4* v2 = reinterpret_cast<float4*>(e1 + H.h1.eCnt);
+			float4* p2 = v2 + H.h2.vCnt;
+			uint4* e2 = reinterpret_cast<uint4*>(p2 + H.h2.fCnt);
+			if (lane == 0)
+			{
+				// The warp's reads of the previous pair (generic proxy) come
+				// before these writes (async proxy).
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				const uint32_t bytes = 16u * (H.h1.vCnt + H.h1.fCnt + H.h1.eCnt + H.h2.vCnt + H.h2.fCnt + H.h2.eCnt);
+				mbar_arrive_expect_tx(bar, bytes);
+				bulk_to_shared(v1, H.h1.v, 16u * H.h1.vCnt, bar);
+				bulk_to_shared(p1, H.h1.p, 16u * H.h1.fCnt, bar);
+				bulk_to_shared(e1, H.h1.e, 16u * H.h1.eCnt, bar);
+				bulk_to_shared(v2, H.h2.v, 16u * H.h2.vCnt, bar);
+				bulk_to_shared(p2, H.h2.p, 16u * H.h2.fCnt, bar);
+				bulk_to_shared(e2, H.h2.e, 16u * H.h2.eCnt, bar);
+			}
+			const bool ok = stage_wait(bar, phase);
+			if (!__all_sync(0xffffffffu, ok))
+			{
+				// The copies did not land in time: report it, wait (bounded)
+				// for them before the shared memory goes away, and stop.
+				if (lane == 0)
+					atomicOr(a.status, B3G_ST_WAIT_TIMEOUT);
+				stage_wait(bar, phase);
+				return;
+			}
+			phase ^= 1u;
+			H.h1.v = v1;
+			H.h1.p = p1;
+			H.h1.e = e1;
+			H.h2.v = v2;
+			H.h2.p = p2;
+			H.h2.e = e2;
+		}
 		uint4 cache = a.cache[c];
 		DevManifold& m = a.man[c];
 		if (a.convexCache)
@@ -1173,17 +1288,38 @@ void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint3
 	}
 }
 
-template <int W>
-void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
+template <int W, bool STAGE>
+void launch_sat_kernel(const NPArgs& a, uint32_t maxUE, int blocksPerSM, size_t smem, cudaStream_t s)
 {
-	size_t smem = (size_t)W * sat_warp_bytes(maxUE);
 	static size_t configured = 0;
 	if (smem > 48 * 1024 && smem > configured)
 	{
-		cudaFuncSetAttribute(k_hulls_sat<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		cudaFuncSetAttribute(k_hulls_sat<W, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 		configured = smem;
 	}
-	k_hulls_sat<W><<<persistent_blocks(blocksPerSM), W * 32, smem, s>>>(a, maxUE);
+	k_hulls_sat<W, STAGE><<<persistent_blocks(blocksPerSM), W * 32, smem, s>>>(a, maxUE);
+}
+
+// The staged kernel when its shared memory fits a block, else the kernel
+// that reads the hulls from global memory.
+template <int W>
+void launch_sat(const NPArgs& a, uint32_t maxUE, int blocksPerSM, cudaStream_t s)
+{
+	const size_t plain = (size_t)W * sat_warp_bytes(maxUE);
+	const size_t staged = ((W * 8 + 15) & ~(size_t)15) + plain +
+		(size_t)W * sat_stage_bytes(a.S.hullMaxV, a.S.hullMaxF, a.S.hullMaxE);
+	static int optin = -1;
+	if (optin < 0)
+	{
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+			optin = 48 * 1024;
+	}
+	if (staged <= (size_t)optin && a.S.hullMaxV > 0)
+		launch_sat_kernel<W, true>(a, maxUE, blocksPerSM, staged, s);
+	else
+		launch_sat_kernel<W, false>(a, maxUE, blocksPerSM, plain, s);
 }
 
 void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, const Tune& tune,
