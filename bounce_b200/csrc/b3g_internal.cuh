@@ -197,6 +197,7 @@ struct Buffers
 	// narrowphase work lists
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
 	uint32_t* missList;   // hull-hull contacts for the SAT kernel
+	float4* hcPost;       // hull-capsule contacts past their GJK: 2 float4 each
 	uint32_t* counters;   // device counters (see CTR_*)
 	unsigned long long* totals; // cumulative: passes, contacts, manifolds, points, begun, ended
 	uint32_t* endedList;  // 3 u32 per ended contact
@@ -298,7 +299,9 @@ enum
 	CTR_MESH_PAIRS = 31, // (contact, triangle) work items of the pass
 	CTR_TRAV_OVERFLOW = 32, // traversal records past the scratch slots
 	CTR_CANDIDATES = 33,    // new pairs handed to the caller's contact filter
-	CTR_COUNT = 34
+	CTR_HC_POST = 34,       // hull-capsule contacts past their GJK (k_hull_capsule_post): at a distance
+	CTR_HC_DEEP = 35,       // ... and overlapping
+	CTR_COUNT = 36
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 

@@ -569,6 +569,13 @@ struct NPArgs
 	// manifolds 1 and 2 of mesh contacts (null without meshes)
 	DevManifold* extraCur;
 	const DevManifold* extraPrev;
+	// hull-capsule contacts whose GJK distance is within the radii: two
+	// float4 per entry (point1, distance; point2, contact index); those with a
+	// positive distance fill the entries from the front, the overlapping ones
+	// from the back (hcPostCap entries), counted in hcPostCount[0] and [1]
+	float4* hcPost;
+	uint32_t* hcPostCount;
+	uint32_t hcPostCap;
 };
 
 // ---------------------------------------------------------------------------

@@ -215,12 +215,59 @@ __device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF&
 	}
 }
 
-// b3QueryFaceSeparation(hull, capsule) (sat_hull_edge.cpp:29-59).
-__device__ void query_face_hull_capsule(const HullRef& h1, V3 lv1, V3 lv2, uint32_t& index, float& sep)
+// First maximum of (v, idx) over the G lanes of a lane group (lanes
+// [k*G, k*G + G) of the warp, gmask): the largest value, and among equal
+// values the lowest index, which is what the reference's serial scans keep
+// with their strict "greater" test. Every lane of the group ends with it.
+template <int G>
+__device__ __forceinline__ void group_argmax(float& v, uint32_t& idx, uint32_t gmask)
+{
+#pragma unroll
+	for (int o = G / 2; o > 0; o >>= 1)
+	{
+		float ov = __shfl_xor_sync(gmask, v, o, G);
+		uint32_t oi = __shfl_xor_sync(gmask, idx, o, G);
+		if (ov > v || (ov == v && oi < idx))
+		{
+			v = ov;
+			idx = oi;
+		}
+	}
+}
+
+// b3Hull::GetSupportFace (hull.h:121-135) with the faces spread over the
+// group's lanes (lane gl takes faces gl, gl + G, ...).
+template <int G>
+__device__ __forceinline__ uint32_t group_support_face(const HullRef& h, V3 d, uint32_t gl, uint32_t gmask)
+{
+	if (G == 1)
+		return hull_support_face(h, d);
+	float best = -INFINITY;
+	uint32_t bi = 0xFFFFFFFFu;
+	for (uint32_t i = gl; i < h.fCnt; i += G)
+	{
+		float proj = dot(d, hp(h, i).n);
+		if (bi == 0xFFFFFFFFu || proj > best)
+		{
+			best = proj;
+			bi = i;
+		}
+	}
+	group_argmax<G>(best, bi, gmask);
+	return bi;
+}
+
+// b3QueryFaceSeparation(hull, capsule) (sat_hull_edge.cpp:29-59), faces
+// spread over the group's lanes. A lane that finds no separation above the
+// start value keeps (-max, 0), so the group's answer is (-max, 0) exactly
+// when the serial scan's is.
+template <int G>
+__device__ void query_face_hull_capsule(const HullRef& h1, V3 lv1, V3 lv2, uint32_t& index, float& sep,
+	uint32_t gl, uint32_t gmask)
 {
 	uint32_t maxIndex = 0;
 	float maxSep = -B3G_MAX_SCALAR;
-	for (uint32_t i = 0; i < h1.fCnt; ++i)
+	for (uint32_t i = gl; i < h1.fCnt; i += G)
 	{
 		PL plane = hp(h1, i);
 		V3 d = -plane.n;
@@ -232,6 +279,7 @@ __device__ void query_face_hull_capsule(const HullRef& h1, V3 lv1, V3 lv2, uint3
 			maxSep = s;
 		}
 	}
+	group_argmax<G>(maxSep, maxIndex, gmask);
 	index = maxIndex;
 	sep = maxSep;
 }
@@ -256,14 +304,17 @@ __device__ __forceinline__ float project_edge_capsule(V3 P1, V3 E1, V3 C1, V3 P2
 	return dot(N, P2 - P1);
 }
 
-// b3QueryEdgeSeparation(hull, capsule) (sat_hull_edge.cpp:102-146).
-__device__ void query_edge_hull_capsule(const HullRef& h1, V3 P2, V3 Q2, uint32_t& index, float& sep)
+// b3QueryEdgeSeparation(hull, capsule) (sat_hull_edge.cpp:102-146), the
+// hull's edges (half-edge pairs i, i + 1) spread over the group's lanes.
+template <int G>
+__device__ void query_edge_hull_capsule(const HullRef& h1, V3 P2, V3 Q2, uint32_t& index, float& sep,
+	uint32_t gl, uint32_t gmask)
 {
 	uint32_t maxIndex = 0;
 	float maxSep = -B3G_MAX_SCALAR;
 	V3 C1 = h1.centroid;
 	V3 E2 = Q2 - P2;
-	for (uint32_t i = 0; i < h1.eCnt; i += 2)
+	for (uint32_t i = 2 * gl; i < h1.eCnt; i += 2 * G)
 	{
 		uint4 e1 = h1.e[i], t1 = h1.e[i + 1];
 		V3 P1 = hv(h1, e1.x);
@@ -282,6 +333,7 @@ __device__ void query_edge_hull_capsule(const HullRef& h1, V3 P2, V3 Q2, uint32_
 			}
 		}
 	}
+	group_argmax<G>(maxSep, maxIndex, gmask);
 	index = maxIndex;
 	sep = maxSep;
 }
@@ -335,8 +387,12 @@ __device__ void hull_capsule_face_contact(DevManifold& m, const XF& xf1, const H
 	m.pointCount = pointCount;
 }
 
-__device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
-	const XF& xf2, const ShapeP& k2)
+// b3CollideHullAndCapsule (collide_hull_capsule.cpp:29-190), first part:
+// the GJK distance between the hull and the capsule's segment. False when it
+// is above the radii (an empty manifold); else the rest of the routine
+// (hull_capsule_after_gjk) builds the manifold from q.
+__device__ __forceinline__ bool hull_capsule_gjk(const DevScene& S, const XF& xf1, const ShapeP& hs, const XF& xf2,
+	const ShapeP& k2, GJKOut& q)
 {
 	float r1 = hull_radius(hs), r2 = cap_radius(k2);
 	float totalRadius = r1 + r2;
@@ -348,9 +404,21 @@ __device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF
 	p2.lv[1] = cap_v2(k2);
 	p2.count = 2;
 	p2.radius = r2;
-	GJKOut q = gjk(xf1, p1, xf2, p2, false);
-	if (q.distance > totalRadius)
-		return;
+	q = gjk(xf1, p1, xf2, p2, false);
+	return !(q.distance > totalRadius);
+}
+
+// The rest of b3CollideHullAndCapsule after its GJK, run by a group of G
+// lanes (gl the lane in the group): the support face or the SAT queries
+// spread over the lanes, the contact points built by lane 0, which alone
+// writes m.
+template <int G>
+__device__ void hull_capsule_after_gjk(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
+	const XF& xf2, const ShapeP& k2, const GJKOut& q, uint32_t gl, uint32_t gmask)
+{
+	float r1 = hull_radius(hs), r2 = cap_radius(k2);
+	float totalRadius = r1 + r2;
+	HullRef h1 = hull_ref(S, hs.hull);
 	V3 v1 = cap_v1(k2), v2 = cap_v2(k2);
 	if (q.distance > 0.0f)
 	{
@@ -358,7 +426,9 @@ __device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF
 		float d = q.distance;
 		V3 N1 = (c2 - c1) / d;
 		V3 localN1 = rotc(xf1.q, N1);
-		uint32_t index1 = hull_support_face(h1, localN1);
+		uint32_t index1 = group_support_face<G>(h1, localN1, gl, gmask);
+		if (gl != 0)
+			return;
 		V3 localFaceN1 = hp(h1, index1).n;
 		const float kTol = 0.005f;
 		V3 N = cross(localN1, localFaceN1);
@@ -379,13 +449,13 @@ __device__ void collide_hull_capsule(DevManifold& m, const DevScene& S, const XF
 	V3 lv1 = xmul(xf, v1), lv2 = xmul(xf, v2);
 	uint32_t faceIndex;
 	float faceSep;
-	query_face_hull_capsule(h1, lv1, lv2, faceIndex, faceSep);
+	query_face_hull_capsule<G>(h1, lv1, lv2, faceIndex, faceSep, gl, gmask);
 	if (faceSep > totalRadius)
 		return;
 	uint32_t edgeIndex;
 	float edgeSep;
-	query_edge_hull_capsule(h1, lv1, lv2, edgeIndex, edgeSep);
-	if (edgeSep > totalRadius)
+	query_edge_hull_capsule<G>(h1, lv1, lv2, edgeIndex, edgeSep, gl, gmask);
+	if (edgeSep > totalRadius || gl != 0)
 		return;
 	const float kRelEdgeTol = 0.90f;
 	const float kAbsTol = 0.5f * B3G_LINEAR_SLOP;
@@ -658,12 +728,12 @@ __device__ void collide_triangle_capsule(DevManifold& m, const HullRef& h1, cons
 	V3 lv1 = xmul(xf, v1), lv2 = xmul(xf, v2);
 	uint32_t faceIndex;
 	float faceSep;
-	query_face_hull_capsule(h1, lv1, lv2, faceIndex, faceSep);
+	query_face_hull_capsule<1>(h1, lv1, lv2, faceIndex, faceSep, 0, 1u);
 	if (faceSep > totalRadius)
 		return;
 	uint32_t edgeIndex;
 	float edgeSep;
-	query_edge_hull_capsule(h1, lv1, lv2, edgeIndex, edgeSep);
+	query_edge_hull_capsule<1>(h1, lv1, lv2, edgeIndex, edgeSep, 0, 1u);
 	if (edgeSep > totalRadius)
 		return;
 	const float kRelEdgeTol = 0.90f;
@@ -741,13 +811,79 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 		else if (BUCKET == BK_HULL_SPHERE)
 			collide_hull_sphere(m, a.S, xfA, sa, xfB, sb);
 		else if (BUCKET == BK_HULL_CAPSULE)
-			collide_hull_capsule(m, a.S, xfA, sa, xfB, sb);
+		{
+			GJKOut q;
+			if (hull_capsule_gjk(a.S, xfA, sa, xfB, sb, q))
+			{
+				// Within the radii: k_hull_capsule_post builds the manifold
+				// and finishes the contact.
+				const uint32_t act = __activemask();
+				const uint32_t lane = threadIdx.x & 31u;
+				const bool deep = !(q.distance > 0.0f);
+				const uint32_t deepMask = __ballot_sync(act, deep);
+				const uint32_t mine = deep ? deepMask : act & ~deepMask;
+				const uint32_t leader = __ffs(mine) - 1;
+				uint32_t base = 0;
+				if (lane == leader)
+					base = atomicAdd(a.hcPostCount + (deep ? 1 : 0), __popc(mine));
+				base = __shfl_sync(mine, base, leader);
+				const uint32_t k = base + __popc(mine & ((1u << lane) - 1u));
+				const uint32_t j = deep ? a.hcPostCap - 1u - k : k;
+				a.hcPost[2 * (size_t)j] = make_float4(q.point1.x, q.point1.y, q.point1.z, q.distance);
+				a.hcPost[2 * (size_t)j + 1] = make_float4(q.point2.x, q.point2.y, q.point2.z, __uint_as_float(c));
+				continue;
+			}
+		}
 		else if (BUCKET == BK_TRIANGLE_SPHERE)
 			collide_triangle_sphere(m, xfA, sa, load_wings(a.S, fa), xfB, sb);
 		else if (BUCKET == BK_TRIANGLE_CAPSULE)
 			collide_triangle_capsule(m, tri_ref(a.S, fa), xfA, sa, load_wings(a.S, fa), xfB, sb);
 		finish_convex(a, c, m);
 		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+	}
+}
+
+// Lanes per contact and blocks per SM of k_hull_capsule_post.
+constexpr int HC_POST_LANES = 8;
+constexpr int HC_POST_BLOCKS = 6;
+
+// Hull-capsule contacts past their GJK (k_convex<BK_HULL_CAPSULE> lists them),
+// G lanes per contact: the support-face and SAT scans run on the group's
+// lanes, so a warp no longer walks, one lane at a time, the faces and edges
+// of every hull in it that needs them.
+template <int G>
+__global__ void __launch_bounds__(128, HC_POST_BLOCKS) k_hull_capsule_post(NPArgs a)
+{
+	// The contacts at a distance first, then the overlapping ones, so the
+	// groups of a warp mostly take the same branch.
+	const uint32_t nSep = a.hcPostCount[0];
+	const uint32_t n = nSep + a.hcPostCount[1];
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t gl = lane % G;
+	const uint32_t gmask = G == 32 ? 0xFFFFFFFFu : (((1u << G) - 1u) << (lane - gl));
+	const uint32_t groups = gridDim.x * (blockDim.x / G);
+	for (uint32_t t = blockIdx.x * (blockDim.x / G) + threadIdx.x / G; t < n; t += groups)
+	{
+		const uint32_t j = t < nSep ? t : a.hcPostCap - 1u - (t - nSep);
+		float4 q0 = a.hcPost[2 * (size_t)j], q1 = a.hcPost[2 * (size_t)j + 1];
+		uint32_t c = __float_as_uint(q1.w);
+		GJKOut q;
+		q.point1 = V3{q0.x, q0.y, q0.z};
+		q.point2 = V3{q1.x, q1.y, q1.z};
+		q.distance = q0.w;
+		q.iterations = 0;
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+		XF xfA = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
+		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
+		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
+		DevManifold& m = a.man[c];
+		hull_capsule_after_gjk<G>(m, a.S, xfA, sa, xfB, sb, q, gl, gmask);
+		if (gl == 0)
+		{
+			finish_convex(a, c, m);
+			a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+		}
 	}
 }
 
@@ -913,7 +1049,9 @@ void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const u
 		k_convex<BK_HULL_SPHERE><<<blocks, 128, 0, s>>>(a);
 		break;
 	case 6:
+		cudaMemsetAsync(a.hcPostCount, 0, 2 * sizeof(uint32_t), s);
 		k_convex<BK_HULL_CAPSULE><<<blocks, 128, 0, s>>>(a);
+		k_hull_capsule_post<HC_POST_LANES><<<persistent_blocks(HC_POST_BLOCKS), 128, 0, s>>>(a);
 		break;
 	case 7:
 		k_sensor<<<blocks, 128, 0, s>>>(a);

@@ -331,6 +331,9 @@ NPArgs make_np_args(b3g_ctx* c)
 	a.exA = a.exB = a.ex0A = a.ex0B = nullptr;
 	a.missList = B.missList;
 	a.missCount = B.counters + CTR_HULL_MISS;
+	a.hcPost = B.hcPost;
+	a.hcPostCount = B.counters + CTR_HC_POST;
+	a.hcPostCap = c->cfg.max_contacts;
 	a.extraCur = B.extraMan[cur];
 	a.extraPrev = B.extraMan[prev];
 	return a;
