@@ -506,6 +506,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.bucketList, (size_t)BK_COUNT * C), "alloc");
 	step(dalloc(&B.missList, C), "alloc");
 	step(dalloc(&B.hcPost, 2 * (size_t)C), "alloc");
+	step(dalloc(&B.hsPost, C), "alloc");
 	step(dalloc(&B.counters, CTR_COUNT), "alloc");
 	step(dalloc(&c->dUpdateBad, 1), "alloc");
 	step(dalloc(&B.totals, 8), "alloc");
@@ -602,6 +603,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.bucketList);
 	dfree(B.missList);
 	dfree(B.hcPost);
+	dfree(B.hsPost);
 	dfree(B.counters);
 	dfree(B.totals);
 	if (c->profEvents)
@@ -2440,6 +2442,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	uint32_t* dStatus = nullptr;
 	uint32_t *dMiss = nullptr, *dMissCount = nullptr;
 	float4* dPost = nullptr;
+	uint32_t* dHsPost = nullptr;
 	int32_t* dPrev = nullptr;
 	uint4 *dCache = nullptr, *dCacheIn = nullptr;
 	float *dXA = nullptr, *dXB = nullptr, *dX0A = nullptr, *dX0B = nullptr;
@@ -2466,8 +2469,9 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	step(dalloc(&dMan, n));
 	step(dalloc(&dPrevMan, 1));
 	step(dalloc(&dMiss, n));
-	step(dalloc(&dMissCount, 3));
+	step(dalloc(&dMissCount, 4));
 	step(dalloc(&dPost, 2 * (size_t)n));
+	step(dalloc(&dHsPost, n));
 	if (rc == B3G_OK)
 	{
 		std::vector<int32_t> prev(n);
@@ -2488,7 +2492,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 		step(cudaMemcpy(dCacheIn, cin.data(), 16 * (size_t)n, cudaMemcpyHostToDevice));
 		step(cudaMemset(dPrevState, 0, 4 * n));
 		step(cudaMemset(dStatus, 0, 4));
-		step(cudaMemset(dMissCount, 0, 12));
+		step(cudaMemset(dMissCount, 0, 16));
 	}
 	if (rc == B3G_OK)
 	{
@@ -2516,6 +2520,8 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 		a.hcPost = dPost;
 		a.hcPostCount = dMissCount + 1;
 		a.hcPostCap = n;
+		a.hsPost = dHsPost;
+		a.hsPostCount = dMissCount + 3;
 		a.extraCur = nullptr;
 		a.extraPrev = nullptr;
 		std::vector<uint32_t> flat(n), counts(BK_COUNT, 0);
@@ -2598,6 +2604,7 @@ extern "C" int b3g_collide_pairs(b3g_ctx* c, uint32_t n, const uint32_t* fixA, c
 	dfree(dMiss);
 	dfree(dMissCount);
 	dfree(dPost);
+	dfree(dHsPost);
 	return rc;
 }
 

@@ -198,6 +198,7 @@ struct Buffers
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries
 	uint32_t* missList;   // hull-hull contacts for the SAT kernel
 	float4* hcPost;       // hull-capsule contacts past their GJK: 2 float4 each
+	uint32_t* hsPost;     // hull-sphere contacts past their face scan
 	uint32_t* counters;   // device counters (see CTR_*)
 	unsigned long long* totals; // cumulative: passes, contacts, manifolds, points, begun, ended
 	uint32_t* endedList;  // 3 u32 per ended contact
@@ -301,7 +302,8 @@ enum
 	CTR_CANDIDATES = 33,    // new pairs handed to the caller's contact filter
 	CTR_HC_POST = 34,       // hull-capsule contacts past their GJK (k_hull_capsule_post): at a distance
 	CTR_HC_DEEP = 35,       // ... and overlapping
-	CTR_COUNT = 36
+	CTR_HS_POST = 36,       // hull-sphere contacts past their face scan (k_hull_sphere_gjk)
+	CTR_COUNT = 37
 };
 static_assert(CTR_BUCKET0 + BK_COUNT <= CTR_ASLEEP, "bucket counters overlap");
 

@@ -576,6 +576,9 @@ struct NPArgs
 	float4* hcPost;
 	uint32_t* hcPostCount;
 	uint32_t hcPostCap;
+	// hull-sphere contacts whose face scan leaves the GJK to run, and their count
+	uint32_t* hsPost;
+	uint32_t* hsPostCount;
 };
 
 // ---------------------------------------------------------------------------

@@ -168,8 +168,13 @@ __device__ __forceinline__ GProxy hull_proxy(const HullRef& h, float r)
 	return p;
 }
 
-__device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
-	const XF& xf2, const ShapeP& s2)
+// b3CollideHullAndSphere (collide_hull_sphere.cpp:26-97), first part: the
+// scan of the hull's faces for the sphere centre. False when that settles
+// the manifold (empty: a face farther than the radii; one point: the centre
+// inside the hull); true when the routine goes on to its GJK
+// (hull_sphere_gjk).
+__device__ __forceinline__ bool hull_sphere_faces(DevManifold& m, const DevScene& S, const XF& xf1,
+	const ShapeP& hs, const XF& xf2, const ShapeP& s2)
 {
 	float radius = hull_radius(hs) + sph_radius(s2);
 	HullRef h1 = hull_ref(S, hs.hull);
@@ -181,7 +186,7 @@ __device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF&
 		PL plane = hp(h1, i);
 		float s = pdist(cLocal, plane);
 		if (s > radius)
-			return;
+			return false;
 		if (s > separation)
 		{
 			faceIndex = i;
@@ -195,8 +200,17 @@ __device__ void collide_hull_sphere(DevManifold& m, const DevScene& S, const XF&
 		m.pointCount = 1;
 		set_point(m.points[0], lp.n, c1, sph_center(s2));
 		set_id0(m.points[0]);
-		return;
+		return false;
 	}
+	return true;
+}
+
+// The rest of b3CollideHullAndSphere: GJK between the hull and the centre.
+__device__ __forceinline__ void hull_sphere_gjk(DevManifold& m, const DevScene& S, const XF& xf1, const ShapeP& hs,
+	const XF& xf2, const ShapeP& s2)
+{
+	float radius = hull_radius(hs) + sph_radius(s2);
+	HullRef h1 = hull_ref(S, hs.hull);
 	GProxy p1 = hull_proxy(h1, hull_radius(hs));
 	GProxy p2;
 	p2.gv = nullptr;
@@ -809,7 +823,21 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 		else if (BUCKET == BK_CAPSULES)
 			collide_capsules(m, xfA, sa, xfB, sb);
 		else if (BUCKET == BK_HULL_SPHERE)
-			collide_hull_sphere(m, a.S, xfA, sa, xfB, sb);
+		{
+			if (hull_sphere_faces(m, a.S, xfA, sa, xfB, sb))
+			{
+				// The GJK runs in k_hull_sphere_gjk, which finishes the contact.
+				const uint32_t act = __activemask();
+				const uint32_t lane = threadIdx.x & 31u;
+				const uint32_t leader = __ffs(act) - 1;
+				uint32_t base = 0;
+				if (lane == leader)
+					base = atomicAdd(a.hsPostCount, __popc(act));
+				base = __shfl_sync(act, base, leader);
+				a.hsPost[base + __popc(act & ((1u << lane) - 1u))] = c;
+				continue;
+			}
+		}
 		else if (BUCKET == BK_HULL_CAPSULE)
 		{
 			GJKOut q;
@@ -838,6 +866,27 @@ __global__ void __launch_bounds__(128, 4) k_convex(NPArgs a)
 			collide_triangle_sphere(m, xfA, sa, load_wings(a.S, fa), xfB, sb);
 		else if (BUCKET == BK_TRIANGLE_CAPSULE)
 			collide_triangle_capsule(m, tri_ref(a.S, fa), xfA, sa, load_wings(a.S, fa), xfB, sb);
+		finish_convex(a, c, m);
+		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
+	}
+}
+
+// Hull-sphere contacts whose face scan left the GJK to run
+// (k_convex<BK_HULL_SPHERE> lists them), one thread each: the warps that run
+// a GJK no longer wait on the face scans of the others.
+__global__ void __launch_bounds__(128, 4) k_hull_sphere_gjk(NPArgs a)
+{
+	const uint32_t n = *a.hsPostCount;
+	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+	{
+		uint32_t c = a.hsPost[t];
+		uint32_t fa = a.pairA[c], fb = a.pairB[c];
+		uint32_t ba = a.S.fixBody[fa], bb = a.S.fixBody[fb];
+		XF xfA = a.exA ? load_xf7(a.exA + 7 * (size_t)c) : body_xf(a.S, ba);
+		XF xfB = a.exB ? load_xf7(a.exB + 7 * (size_t)c) : body_xf(a.S, bb);
+		ShapeP sa = load_shape(a.S, fa), sb = load_shape(a.S, fb);
+		DevManifold& m = a.man[c];
+		hull_sphere_gjk(m, a.S, xfA, sa, xfB, sb);
 		finish_convex(a, c, m);
 		a.cache[c] = make_uint4(B3G_NULL, B3G_NULL, B3G_NULL, B3G_NULL);
 	}
@@ -1046,7 +1095,9 @@ void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const u
 		k_convex<BK_TRIANGLE_CAPSULE><<<blocks, 128, 0, s>>>(a);
 		break;
 	case 5:
+		cudaMemsetAsync(a.hsPostCount, 0, sizeof(uint32_t), s);
 		k_convex<BK_HULL_SPHERE><<<blocks, 128, 0, s>>>(a);
+		k_hull_sphere_gjk<<<persistent_blocks(4), 128, 0, s>>>(a);
 		break;
 	case 6:
 		cudaMemsetAsync(a.hcPostCount, 0, 2 * sizeof(uint32_t), s);

@@ -334,6 +334,8 @@ NPArgs make_np_args(b3g_ctx* c)
 	a.hcPost = B.hcPost;
 	a.hcPostCount = B.counters + CTR_HC_POST;
 	a.hcPostCap = c->cfg.max_contacts;
+	a.hsPost = B.hsPost;
+	a.hsPostCount = B.counters + CTR_HS_POST;
 	a.extraCur = B.extraMan[cur];
 	a.extraPrev = B.extraMan[prev];
 	return a;
@@ -374,11 +376,11 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 		c->maxUniqueEdges, c->tune, side);
 	prof_mark(c, PM_HULLS, s);
 	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
-	// The hull-sphere kernel follows the hull kernels on the second stream,
-	// which evens the two branches out (the hull-capsule kernel is the
-	// longest of the convex ones).
+	// The convex kernels (hull-sphere and hull-capsule each a scan kernel and
+	// a follow-up kernel on the contacts the scan hands on) run beside the
+	// hull-hull probe and SAT: the two branches take about as long.
 	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
-		launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, k == 5 ? side : s);
+		launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 	prof_mark(c, PM_CONVEX, s);
 	if (side != s)
 	{
