@@ -626,6 +626,9 @@ __global__ void k_leaves(DevScene S, Buffers B, int n)
 	B.nodeLo[node] = make_float4(lo.x, lo.y, lo.z, __uint_as_float(proxy));
 	B.nodeHi[node] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(rope));
 	B.nodeRope[node] = rope;
+	// What the walk's filter and contact order need of the proxy, addressed
+	// by the leaf's position so it loads beside the node.
+	B.leafData[j] = make_uint2(B.proxyInfo[proxy], S.fixKey[proxy]);
 	if (j < n - 1)
 	{
 		B.nodeRope[j] = (B.nodeEnd[j] == (uint32_t)(n - 1)) ? SENT : B.splitRight[B.nodeEnd[j]];
@@ -706,22 +709,26 @@ __device__ __forceinline__ bool pair_filter(uint32_t infoA, uint32_t infoB)
 	return registered(infoA >> 29, infoB >> 29);
 }
 
-// The contact record of overlapping proxies pa, pb: the broadphase order
-// (min, max) of proxy ids (b3BroadPhase::Report, broad_phase.cpp:341-342)
-// followed by the factory's primary-type swap (b3Contact::Create,
-// contact.cpp:306-317). x = fixture A, y = fixture B.
-__device__ __forceinline__ uint2 canon_pair(const DevScene& S, uint32_t pa, uint32_t pb)
+// The contact record of overlapping proxies pa, pb (keys keyA, keyB, shape
+// types typeA, typeB): the broadphase order (min, max) of proxy ids
+// (b3BroadPhase::Report, broad_phase.cpp:341-342) followed by the factory's
+// primary-type swap (b3Contact::Create, contact.cpp:306-317). x = fixture A,
+// y = fixture B.
+__device__ __forceinline__ uint2 canon_pair_keys(uint32_t pa, uint32_t keyA, uint32_t typeA, uint32_t pb,
+	uint32_t keyB, uint32_t typeB)
 {
-	uint32_t keyA = S.fixKey[pa], keyB = S.fixKey[pb];
-	uint32_t f1 = keyA < keyB ? pa : pb;
-	uint32_t f2 = keyA < keyB ? pb : pa;
-	if (!primary(S.fixType[f1], S.fixType[f2]))
+	const bool aFirst = keyA < keyB;
+	uint32_t f1 = aFirst ? pa : pb, f2 = aFirst ? pb : pa;
+	uint32_t t1 = aFirst ? typeA : typeB, t2 = aFirst ? typeB : typeA;
+	if (!primary(t1, t2))
 		return make_uint2(f2, f1);
 	return make_uint2(f1, f2);
 }
 
 // Rope walk from leaf j's own rope. A node is read as two float4:
-// (lower, left child | proxy) and (upper, rope). The walk counts the filtered
+// (lower, left child | proxy) and (upper, rope); a leaf's proxy word and key
+// (leafData) load beside it, so a found pair costs no further dependent
+// load. The walk counts the filtered
 // overlaps, keeps the first TRAV_SLOTS contact records in the leaf's scratch
 // slots (slot-major) and appends the others, with their leaf and index, to
 // the overflow list. MW: several worlds share the tree, so the walk stops at
@@ -735,7 +742,8 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 	uint32_t leaf = n - 1 + j;
 	float4 ql = __ldg(B.nodeLo + leaf), qh = __ldg(B.nodeHi + leaf);
 	uint32_t pa = __float_as_uint(ql.w);
-	const uint32_t infoA = __ldg(B.proxyInfo + pa);
+	const uint2 da = __ldg(B.leafData + j);
+	const uint32_t infoA = da.x, keyA = da.y;
 	uint32_t wend = MW ? B.worldEnd[S.bodyWorld[S.fixBody[pa]]] : 0xFFFFFFFFu;
 	uint32_t count = 0;
 	uint32_t node = __float_as_uint(qh.w);
@@ -755,8 +763,10 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 			break;
 		// The tree is read-only here: the read-only data path caches it in L1.
 		float4 lo = __ldg(B.nodeLo + node), hi = __ldg(B.nodeHi + node);
+		const bool leafNode = node >= (uint32_t)(n - 1);
+		const uint2 db = leafNode ? __ldg(B.leafData + (node - (uint32_t)(n - 1))) : make_uint2(0u, 0u);
 		bool overlap = !(hi.x < ql.x || lo.x > qh.x || hi.y < ql.y || lo.y > qh.y || hi.z < ql.z || lo.z > qh.z);
-		if (overlap && node < (uint32_t)(n - 1))
+		if (overlap && !leafNode)
 		{
 			node = __float_as_uint(lo.w); // descend
 			continue;
@@ -764,9 +774,9 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 		if (overlap)
 		{
 			uint32_t pb = __float_as_uint(lo.w);
-			if (pair_filter(infoA, __ldg(B.proxyInfo + pb)))
+			if (pair_filter(infoA, db.x))
 			{
-				uint2 p = canon_pair(S, pa, pb);
+				uint2 p = canon_pair_keys(pa, keyA, infoA >> 29, pb, db.y, db.x >> 29);
 				if (count < TRAV_SLOTS)
 					scratch[(size_t)count * n + j] = p;
 				else

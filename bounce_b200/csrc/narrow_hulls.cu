@@ -777,13 +777,18 @@ __device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 		cache.z = 0;
 		cache.w = 0;
 	}
+	// A face of either hull is read by one call with the hulls in the face's
+	// order, so the lanes of a warp with face caches of hull 1 and of hull 2
+	// run it together rather than one group after the other.
+	const bool face = cache.y == FT_FACE1 || cache.y == FT_FACE2;
+	const bool f2 = cache.y == FT_FACE2;
+	const XF xa = f2 ? H.xf2 : H.xf1, xb = f2 ? H.xf1 : H.xf2;
+	const HullRef ha = f2 ? H.h2 : H.h1, hb = f2 ? H.h1 : H.h2;
 	uint32_t state1;
 	if (cache.y == FT_EDGES)
 		state1 = read_edges(H.xf1, H.h1, H.xf2, H.h2, cache.z, cache.w, totalRadius);
-	else if (cache.y == FT_FACE1)
-		state1 = read_face_thread(H.xf1, H.h1, H.xf2, H.h2, cache.z, totalRadius);
-	else if (cache.y == FT_FACE2)
-		state1 = read_face_thread(H.xf2, H.h2, H.xf1, H.h1, cache.z, totalRadius);
+	else if (face)
+		state1 = read_face_thread(xa, ha, xb, hb, cache.z, totalRadius);
 	else
 		state1 = CT_EMPTY;
 	if (state0 == CT_SEPARATION && state1 == CT_SEPARATION)
@@ -792,10 +797,9 @@ __device__ bool probe_cache(DevManifold& m, const HullCtx& H, uint4& cache)
 	{
 		if (cache.y == FT_EDGES)
 			rebuild_edge_contact(m, H.xf1, cache.z, H.h1, H.xf2, cache.w, H.h2);
-		else if (cache.y == FT_FACE1)
-			rebuild_face_contact(m, H.xf1, cache.z, H.h1, H.r1, H.xf2, H.h2, H.r2, false, H.xf01, H.xf02, H.status);
-		else if (cache.y == FT_FACE2)
-			rebuild_face_contact(m, H.xf2, cache.z, H.h2, H.r2, H.xf1, H.h1, H.r1, true, H.xf02, H.xf01, H.status);
+		else if (face)
+			rebuild_face_contact(m, xa, cache.z, ha, f2 ? H.r2 : H.r1, xb, hb, f2 ? H.r1 : H.r2, f2,
+				f2 ? H.xf02 : H.xf01, f2 ? H.xf01 : H.xf02, H.status);
 		if (m.pointCount > 0)
 			return true; // overlap cache hit
 	}
