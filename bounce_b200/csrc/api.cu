@@ -473,7 +473,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.proxyInfo, P), "alloc");
 	step(dalloc(&B.leafCount, std::max(P, C)), "alloc");
 	step(dalloc(&B.pairScratch, 2 * B3G_TRAV_SLOTS * (size_t)P), "alloc"); // uint2 records per leaf
-	step(dalloc(&B.scanAux, (std::max(P, C) + 1023) / 1024 + 1), "alloc");
+	step(dalloc(&B.scanAux, scan_aux_words(std::max(P, C) + 1)), "alloc");
 	for (int k = 0; k < 2; ++k)
 	{
 		step(dalloc(&B.pairA[k], C), "alloc");
@@ -1936,7 +1936,7 @@ extern "C" int b3g_fetch_touching(b3g_ctx* c, uint32_t* index, void* manifolds, 
 	const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
 	wait_copies(c, c->stream);
 	k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, offsets);
-	scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
+	scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, B.counters + CTR_STATUS, c->stream);
 	uint32_t total = 0;
 	CK(cudaMemcpyAsync(&total, B.counters + CTR_TOUCH_OUT, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
 	CK(cudaStreamSynchronize(c->stream));
@@ -1990,7 +1990,7 @@ extern "C" int b3g_fetch_results_async(b3g_ctx* c, uint32_t* contacts, uint32_t 
 		uint32_t* offsets = B.leafCount;
 		const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
 		k_touch_flags<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, offsets);
-		scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
+		scan_exclusive(offsets, n, B.scanAux, B.counters + CTR_TOUCH_OUT, B.counters + CTR_STATUS, c->stream);
 		k_touch_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], offsets, n,
 			B.touchIndex, B.touchMan);
 	}
@@ -2050,8 +2050,8 @@ extern "C" int b3g_fetch_results_packed_async(b3g_ctx* c, uint32_t* contacts, ui
 		const DevManifold* extra = B.extraMan[c->cur] ? B.extraMan[c->cur] : B.man[c->cur];
 		k_pack_sizes<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, B.leafCount,
 			c->touchBytes);
-		scan_exclusive(B.leafCount, n, B.scanAux, B.counters + CTR_TOUCH_OUT, c->stream);
-		scan_exclusive(c->touchBytes, n, B.scanAux, B.counters + CTR_SCRATCH, c->stream);
+		scan_exclusive(B.leafCount, n, B.scanAux, B.counters + CTR_TOUCH_OUT, B.counters + CTR_STATUS, c->stream);
+		scan_exclusive(c->touchBytes, n, B.scanAux, B.counters + CTR_SCRATCH, B.counters + CTR_STATUS, c->stream);
 		k_pack_scatter<<<(n + 255) / 256, 256, 0, c->stream>>>(B.man[c->cur], extra, B.cstate[c->cur], n, B.leafCount,
 			c->touchBytes, B.touchIndex, reinterpret_cast<unsigned long long*>(B.touchMan));
 	}
@@ -2131,7 +2131,7 @@ extern "C" int b3g_fetch_fixture_contacts(b3g_ctx* c, uint32_t* offsets, uint32_
 	// every fixture's edges in its own list's order.
 	bool swapped = m ? radix_sort_pairs(keys, vals, keysTmp, valsTmp, m, bits, scratch, B.counters + CTR_STATUS, s)
 					 : false;
-	scan_exclusive(counts, nf, B.scanAux, counts + nf, s);
+	scan_exclusive(counts, nf, B.scanAux, counts + nf, B.counters + CTR_STATUS, s);
 	CK(cudaStreamSynchronize(s));
 	CK(cudaMemcpy(offsets, counts, sizeof(uint32_t) * ((size_t)nf + 1), cudaMemcpyDeviceToHost));
 	const uint32_t k = std::min(m, capacity);

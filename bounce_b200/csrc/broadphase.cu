@@ -852,49 +852,144 @@ __global__ void k_traverse_overflow(Buffers B, uint32_t cap)
 	}
 }
 
-// Multi-block exclusive scan of u32 (in place) with the total written to *total.
-constexpr int SCAN_BLOCK = 1024;
+// One-pass exclusive scan of u32 in place (decoupled look-back, as the
+// one-sweep sort): a block takes the next tile through a counter, reduces its
+// SC_TILE entries, publishes the tile's sum, adds up the sums of the tiles
+// before it (walking back until a tile that already published its inclusive
+// prefix; bounded wait) and writes its entries' offsets. n: *nPtr (at most
+// cap) when nPtr is set, else nHost. state: the tile counter, then one word
+// per tile (flag in bits 62-63, sum in bits 0-31), zeroed before the launch.
+// The tile holding the last entry writes the total (0 for an empty scan).
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 8;
+constexpr uint32_t SC_TILE = SC_THREADS * SC_ITEMS;
+constexpr unsigned long long SC_AGG = 1ull << 62;
+constexpr unsigned long long SC_INC = 2ull << 62;
+constexpr uint32_t SC_SPIN = 1u << 22;
 
-__global__ void k_scan_blocks(uint32_t* data, uint32_t n, uint32_t* blockSums)
+__global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(uint32_t* data, const uint32_t* nPtr, uint32_t nHost,
+	uint32_t cap, unsigned long long* state, uint32_t* total, uint32_t* err)
 {
-	__shared__ uint32_t s[SCAN_BLOCK];
-	uint32_t i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
-	uint32_t v = i < n ? data[i] : 0;
-	s[threadIdx.x] = v;
+	__shared__ uint32_t sTile, sPrefix;
+	__shared__ uint32_t warpSums[SC_THREADS / 32];
+	const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+	const uint32_t n = nPtr ? min(*nPtr, cap) : nHost;
+	if (t == 0)
+		sTile = atomicAdd(reinterpret_cast<unsigned int*>(state), 1u);
 	__syncthreads();
-	for (uint32_t off = 1; off < SCAN_BLOCK; off <<= 1)
+	const uint32_t tile = sTile;
+	const uint32_t numTiles = (n + SC_TILE - 1) / SC_TILE;
+	if (tile >= numTiles)
 	{
-		uint32_t a = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-		__syncthreads();
-		s[threadIdx.x] += a;
-		__syncthreads();
+		if (tile == 0 && t == 0 && total)
+			*total = 0u;
+		return;
 	}
-	if (i < n)
-		data[i] = s[threadIdx.x] - v;
-	if (threadIdx.x == SCAN_BLOCK - 1)
-		blockSums[blockIdx.x] = s[threadIdx.x];
-}
-
-__global__ void k_scan_add(uint32_t* data, uint32_t n, const uint32_t* blockSums)
-{
-	uint32_t i = blockIdx.x * SCAN_BLOCK + threadIdx.x;
-	if (i < n)
-		data[i] += blockSums[blockIdx.x];
+	// Thread t owns entries [t * SC_ITEMS, t * SC_ITEMS + SC_ITEMS) of the tile.
+	const uint32_t first = tile * SC_TILE + t * SC_ITEMS;
+	uint32_t v[SC_ITEMS];
+	uint32_t sum = 0;
+#pragma unroll
+	for (int r = 0; r < SC_ITEMS; ++r)
+	{
+		v[r] = first + r < n ? data[first + r] : 0u;
+		sum += v[r];
+	}
+	uint32_t incl = sum;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1)
+	{
+		uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+		if (lane >= (uint32_t)o)
+			incl += y;
+	}
+	if (lane == 31)
+		warpSums[warp] = incl;
+	__syncthreads();
+	if (warp == 0)
+	{
+		uint32_t w = lane < SC_THREADS / 32 ? warpSums[lane] : 0u;
+		uint32_t wi = w;
+#pragma unroll
+		for (int o = 1; o < SC_THREADS / 32; o <<= 1)
+		{
+			uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+			if (lane >= (uint32_t)o)
+				wi += y;
+		}
+		const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, SC_THREADS / 32 - 1);
+		if (lane < SC_THREADS / 32)
+			warpSums[lane] = wi - w;
+		if (lane == 0)
+		{
+			volatile unsigned long long* st = state + 1;
+			uint32_t prefix = 0;
+			if (tile == 0)
+				st[0] = SC_INC | agg;
+			else
+			{
+				st[tile] = SC_AGG | agg;
+				int32_t look = (int32_t)tile - 1;
+				uint32_t spins = 0;
+				while (look >= 0)
+				{
+					const unsigned long long w8 = st[look];
+					if ((w8 >> 62) == 0ull)
+					{
+						if (++spins > SC_SPIN)
+						{
+							atomicOr(err, B3G_ST_WAIT_TIMEOUT);
+							break;
+						}
+						continue;
+					}
+					prefix += (uint32_t)w8;
+					if (w8 & SC_INC)
+						break;
+					--look;
+				}
+				__threadfence();
+				st[tile] = SC_INC | (uint32_t)(prefix + agg);
+			}
+			sPrefix = prefix;
+			if (tile == numTiles - 1 && total)
+				*total = prefix + agg;
+		}
+	}
+	__syncthreads();
+	uint32_t run = sPrefix + warpSums[warp] + incl - sum;
+#pragma unroll
+	for (int r = 0; r < SC_ITEMS; ++r)
+	{
+		if (first + r < n)
+			data[first + r] = run;
+		run += v[r];
+	}
 }
 
 } // namespace
 
-void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s)
+// Words of scan state (u32) a scan of up to n entries needs in aux.
+uint32_t scan_aux_words(uint32_t n)
 {
-	uint32_t blocks = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
-	if (blocks == 0)
-	{
-		cudaMemsetAsync(total, 0, sizeof(uint32_t), s);
-		return;
-	}
-	k_scan_blocks<<<blocks, SCAN_BLOCK, 0, s>>>(data, n, aux);
-	k_scan_single<<<1, 1024, 0, s>>>(aux, blocks, total);
-	k_scan_add<<<blocks, SCAN_BLOCK, 0, s>>>(data, n, aux);
+	return 2u * ((n + SC_TILE - 1) / SC_TILE + 1u);
+}
+
+void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, uint32_t* err, cudaStream_t s)
+{
+	const uint32_t tiles = (n + SC_TILE - 1) / SC_TILE;
+	cudaMemsetAsync(aux, 0, sizeof(unsigned long long) * (tiles + 1u), s);
+	k_scan_tiles<<<tiles ? tiles : 1u, SC_THREADS, 0, s>>>(data, nullptr, n, n,
+		reinterpret_cast<unsigned long long*>(aux), total, err);
+}
+
+void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
+	uint32_t* err, cudaStream_t s)
+{
+	const uint32_t tiles = (cap + SC_TILE - 1) / SC_TILE;
+	cudaMemsetAsync(aux, 0, sizeof(unsigned long long) * (tiles + 1u), s);
+	k_scan_tiles<<<tiles ? tiles : 1u, SC_THREADS, 0, s>>>(data, nPtr, 0u, cap,
+		reinterpret_cast<unsigned long long*>(aux), total, err);
 }
 
 // Stable sort of n (key, value) records by the low `bits` bits of the keys
@@ -1035,7 +1130,7 @@ void launch_traverse(b3g_ctx* c, cudaStream_t s)
 	else
 		k_traverse_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts,
 			c->walkLimit);
-	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, s);
+	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, B.counters + CTR_STATUS, s);
 	if (c->nWorlds > 1)
 		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	else

@@ -968,7 +968,7 @@ __device__ __forceinline__ HullRef mesh_tri_ref(const MeshTri& t)
 }
 
 void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
-	cudaStream_t s);
+	uint32_t* err, cudaStream_t s);
 void launch_apart(const NPArgs& a, const uint32_t* list, const uint32_t* count, cudaStream_t s);
 void launch_mesh_items_convex(const NPArgs& a, const Buffers& B, cudaStream_t s);
 void launch_mesh_items_hull(const NPArgs& a, const Buffers& B, uint32_t maxUE, const Tune& tune, cudaStream_t s);
@@ -986,7 +986,8 @@ void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t
 void launch_hulls_sat(const NPArgs& a, uint32_t maxUE, const Tune& tune, cudaStream_t s);
 void launch_hull_triangles(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE,
 	const Tune& tune, cudaStream_t s);
-void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, cudaStream_t s);
+void scan_exclusive(uint32_t* data, uint32_t n, uint32_t* aux, uint32_t* total, uint32_t* err, cudaStream_t s);
+uint32_t scan_aux_words(uint32_t n);
 uint32_t radix_sort_scratch_words(uint32_t n, int bits);
 bool radix_sort_pairs(unsigned long long* keys, uint32_t* vals, unsigned long long* keysTmp, uint32_t* valsTmp,
 	uint32_t n, int bits, uint32_t* scratch, uint32_t* err, cudaStream_t s);

@@ -855,7 +855,8 @@ void launch_mesh_prepare(b3g_ctx* c, cudaStream_t s)
 	Buffers& B = c->buf;
 	const uint32_t cap = c->cfg.max_contacts, cur = c->cur;
 	k_mesh_sync<<<persistent_blocks(4), 128, 0, s>>>(c->scene, B, cur, cap);
-	scan_exclusive_device(B.meshCount, B.counters + CTR_PAIRS, cap, B.scanAux, B.counters + CTR_MESH_PAIRS, s);
+	scan_exclusive_device(B.meshCount, B.counters + CTR_PAIRS, cap, B.scanAux, B.counters + CTR_MESH_PAIRS,
+		B.counters + CTR_STATUS, s);
 	k_mesh_overflow<<<1, 1, 0, s>>>(B);
 	k_mesh_emit<<<persistent_blocks(4), 128, 0, s>>>(c->scene, B, cur, cap);
 }

@@ -31,73 +31,6 @@
 
 namespace {
 
-constexpr int SB = 1024;
-
-// Exclusive scan of data[0, *nPtr) in place; the grid covers the capacity and
-// blocks past the device-side count only write a zero block sum.
-__global__ void k_dscan_blocks(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* sums)
-{
-	__shared__ uint32_t s[SB];
-	uint32_t n = min(*nPtr, cap);
-	if (blockIdx.x * SB >= n)
-	{
-		if (threadIdx.x == 0)
-			sums[blockIdx.x] = 0;
-		return;
-	}
-	uint32_t i = blockIdx.x * SB + threadIdx.x;
-	uint32_t v = i < n ? data[i] : 0;
-	s[threadIdx.x] = v;
-	__syncthreads();
-	for (uint32_t off = 1; off < SB; off <<= 1)
-	{
-		uint32_t a = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-		__syncthreads();
-		s[threadIdx.x] += a;
-		__syncthreads();
-	}
-	if (i < n)
-		data[i] = s[threadIdx.x] - v;
-	if (threadIdx.x == SB - 1)
-		sums[blockIdx.x] = s[threadIdx.x];
-}
-
-__global__ void k_dscan_sums(uint32_t* sums, uint32_t m, uint32_t* total)
-{
-	__shared__ uint32_t s[1024];
-	uint32_t per = (m + blockDim.x - 1) / blockDim.x;
-	uint32_t beg = threadIdx.x * per, end = min(beg + per, m);
-	uint32_t sum = 0;
-	for (uint32_t i = beg; i < end; ++i)
-		sum += sums[i];
-	s[threadIdx.x] = sum;
-	__syncthreads();
-	for (uint32_t off = 1; off < blockDim.x; off <<= 1)
-	{
-		uint32_t v = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-		__syncthreads();
-		s[threadIdx.x] += v;
-		__syncthreads();
-	}
-	uint32_t run = s[threadIdx.x] - sum;
-	for (uint32_t i = beg; i < end; ++i)
-	{
-		uint32_t v = sums[i];
-		sums[i] = run;
-		run += v;
-	}
-	if (threadIdx.x == blockDim.x - 1)
-		*total = s[threadIdx.x];
-}
-
-__global__ void k_dscan_add(uint32_t* data, const uint32_t* nPtr, uint32_t cap, const uint32_t* sums)
-{
-	uint32_t n = min(*nPtr, cap);
-	uint32_t i = blockIdx.x * SB + threadIdx.x;
-	if (i < n)
-		data[i] += sums[blockIdx.x];
-}
-
 __device__ __forceinline__ void insert_contact(Buffers& B, uint32_t cur, uint32_t a, uint32_t b, uint32_t index)
 {
 	if (!pair_hash_insert(B.hashKeys[cur], B.hashVals[cur], B.hashCap, pair_key(a, b), index))
@@ -436,17 +369,6 @@ __global__ void k_set_counts(Buffers B, uint32_t pairs, uint32_t ended)
 
 } // namespace
 
-// Exclusive scan of data[0, *nPtr) in place (nPtr a device count, at most
-// cap), its total written to *total.
-void scan_exclusive_device(uint32_t* data, const uint32_t* nPtr, uint32_t cap, uint32_t* aux, uint32_t* total,
-	cudaStream_t s)
-{
-	uint32_t blocks = (cap + SB - 1) / SB;
-	k_dscan_blocks<<<blocks, SB, 0, s>>>(data, nPtr, cap, aux);
-	k_dscan_sums<<<1, 1024, 0, s>>>(aux, blocks, total);
-	k_dscan_add<<<blocks, SB, 0, s>>>(data, nPtr, cap, aux);
-}
-
 // After the previous-contact lookup: lays out this pass's contacts in list
 // order, fills the hash table of this pass and lists the destroyed contacts.
 FilterArgs make_filter_args(const b3g_ctx* c);
@@ -456,16 +378,14 @@ void launch_order(b3g_ctx* c, cudaStream_t s)
 	Buffers& B = c->buf;
 	const uint32_t cap = c->cfg.max_contacts, cur = c->cur, nf = c->nFixtures;
 	const int havePrev = c->havePass ? 1 : 0;
-	scan_exclusive(B.newOff, nf + 1, B.scanAux, B.counters + CTR_SCRATCH, s);
+	scan_exclusive(B.newOff, nf + 1, B.scanAux, B.counters + CTR_SCRATCH, B.counters + CTR_STATUS, s);
 	k_new_scatter<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, nf);
 	k_new_place<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, nf, havePrev);
 	if (havePrev)
 	{
-		uint32_t blocks = (cap + SB - 1) / SB;
 		k_kept<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap);
-		k_dscan_blocks<<<blocks, SB, 0, s>>>(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux);
-		k_dscan_sums<<<1, 1024, 0, s>>>(B.scanAux, blocks, B.counters + CTR_KEPT);
-		k_dscan_add<<<blocks, SB, 0, s>>>(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux);
+		scan_exclusive_device(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux, B.counters + CTR_KEPT,
+			B.counters + CTR_STATUS, s);
 		k_layout_prev<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap);
 	}
 }
@@ -545,7 +465,7 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 		const uint32_t copied = std::min(keptTotal, cap - std::min(numNew, cap));
 		uint32_t* kept2 = B.newTmp;
 		k_compact_flags<<<persistent_blocks(4), 256, 0, s>>>(B, np, numNew, keptTotal, kept2);
-		scan_exclusive(kept2, np, B.scanAux, B.counters + CTR_SCRATCH, s);
+		scan_exclusive(kept2, np, B.scanAux, B.counters + CTR_SCRATCH, B.counters + CTR_STATUS, s);
 		if (!fetch())
 			return B3G_E_CUDA;
 		const uint32_t kept2Total = h[CTR_SCRATCH];

@@ -166,29 +166,57 @@ __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 	}
 }
 
+// Counters of the pass and the contact records (A, B, flags). A thread takes
+// FIN_BATCH contacts a grid stride apart and loads all of their words before
+// it uses any (the manifold's point count too, whether or not the contact
+// has a manifold), so the loads of a contact do not wait on one another.
+constexpr int FIN_BATCH = 4;
+
 __global__ void k_finalize(Buffers B, uint32_t cur, uint32_t cap)
 {
 	uint32_t n = min(B.counters[CTR_PAIRS], cap);
 	uint32_t touching = 0, manifolds = 0, points = 0;
-	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+	const uint32_t* __restrict__ cst = B.cstate[cur];
+	const uint32_t* __restrict__ pA = B.pairA[cur];
+	const uint32_t* __restrict__ pB = B.pairB[cur];
+	const DevManifold* __restrict__ man = B.man[cur];
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for (uint32_t c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < n; c0 += FIN_BATCH * stride)
 	{
-		uint32_t st = B.cstate[cur][c];
-		uint32_t mc = (st >> 8) & 0xFFu;
-		uint32_t pc = mc ? B.man[cur][c].pointCount : 0u;
-		touching += st & 1u;
-		manifolds += pc > 0 ? 1u : 0u;
-		points += pc;
-		for (uint32_t k = 1; k < mc && B.extraMan[cur]; ++k)
+		uint32_t st[FIN_BATCH], pc0[FIN_BATCH], a[FIN_BATCH], b[FIN_BATCH];
+#pragma unroll
+		for (int k = 0; k < FIN_BATCH; ++k)
 		{
-			// Manifolds 1 and 2 of a mesh contact (b3MeshContact::m_stackManifolds).
-			uint32_t xp = B.extraMan[cur][2 * (size_t)c + k - 1].pointCount;
-			manifolds += xp > 0 ? 1u : 0u;
-			points += xp;
+			const uint32_t c = c0 + k * stride;
+			const bool in = c < n;
+			st[k] = in ? __ldg(cst + c) : 0u;
+			pc0[k] = in ? __ldg(&man[c].pointCount) : 0u;
+			a[k] = in ? __ldg(pA + c) : 0u;
+			b[k] = in ? __ldg(pB + c) : 0u;
 		}
-		uint32_t flags = (st & 1u) | ((st >> 16 & 1u) << 1) | (st & 0xFF00u);
-		B.contactOut[3 * c + 0] = B.pairA[cur][c];
-		B.contactOut[3 * c + 1] = B.pairB[cur][c];
-		B.contactOut[3 * c + 2] = flags;
+#pragma unroll
+		for (int k = 0; k < FIN_BATCH; ++k)
+		{
+			const uint32_t c = c0 + k * stride;
+			if (c >= n)
+				break;
+			uint32_t mc = (st[k] >> 8) & 0xFFu;
+			uint32_t pc = mc ? pc0[k] : 0u;
+			touching += st[k] & 1u;
+			manifolds += pc > 0 ? 1u : 0u;
+			points += pc;
+			for (uint32_t j = 1; j < mc && B.extraMan[cur]; ++j)
+			{
+				// Manifolds 1 and 2 of a mesh contact (b3MeshContact::m_stackManifolds).
+				uint32_t xp = B.extraMan[cur][2 * (size_t)c + j - 1].pointCount;
+				manifolds += xp > 0 ? 1u : 0u;
+				points += xp;
+			}
+			uint32_t flags = (st[k] & 1u) | ((st[k] >> 16 & 1u) << 1) | (st[k] & 0xFF00u);
+			B.contactOut[3 * c + 0] = a[k];
+			B.contactOut[3 * c + 1] = b[k];
+			B.contactOut[3 * c + 2] = flags;
+		}
 	}
 	for (int o = 16; o > 0; o >>= 1)
 	{

@@ -1004,7 +1004,7 @@ extern "C" int b3g_query_aabb(b3g_ctx* c, uint32_t n, const float* boxes, const 
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
 	const uint32_t blocks = (n + 127) / 128;
 	k_query_aabb<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dOut, capacity);
-	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, c->buf.counters + CTR_STATUS, s);
 	k_query_aabb<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dOut, capacity);
 	uint32_t total = 0;
 	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -1042,7 +1042,7 @@ extern "C" int b3g_ray_cast(b3g_ctx* c, uint32_t n, const float* rays, const uin
 	cudaMemsetAsync(c->buf.counters + CTR_SCRATCH, 0, 4, s);
 	const uint32_t blocks = (n + 127) / 128;
 	k_ray_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity, nullptr);
-	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, c->buf.counters + CTR_STATUS, s);
 	k_ray_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, dWorlds, n, counts, dIdx, dHit, capacity, nullptr);
 	uint32_t total = 0;
 	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -1195,7 +1195,7 @@ extern "C" int b3g_shape_cast(b3g_ctx* c, uint32_t n, const b3g_shape_cast_input
 		cast_order(c, (const float*)dIn, n, base + cntBytes + idxBytes + hitBytes, world_bits(c), s);
 	const uint32_t blocks = (n + 127) / 128;
 	k_shape_cast<0><<<blocks, 128, 0, s>>>(q, (const float*)dIn, order, n, counts, dIdx, dHit, capacity, nullptr);
-	scan_exclusive(counts, n, c->buf.scanAux, counts + n, s);
+	scan_exclusive(counts, n, c->buf.scanAux, counts + n, c->buf.counters + CTR_STATUS, s);
 	k_shape_cast<1><<<blocks, 128, 0, s>>>(q, (const float*)dIn, order, n, counts, dIdx, dHit, capacity, nullptr);
 	uint32_t total = 0;
 	if (cudaMemcpyAsync(&total, counts + n, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess)
