@@ -209,6 +209,7 @@ EXPORTED = [
     "b3g_get_counts",
     "b3g_get_pass_stats",
     "b3g_set_walk_limit",
+    "b3g_set_tree_rebuild_interval",
     "b3g_set_joint_pairs",
     "b3g_set_contact_veto",
     "b3g_fetch_new_pairs",
@@ -294,6 +295,7 @@ def load():
         "b3g_get_counts": ([ctx, _p(Counts)], ctypes.c_int),
         "b3g_get_pass_stats": ([ctx, _p(ctypes.c_uint32), ctypes.c_uint32], ctypes.c_int),
         "b3g_set_walk_limit": ([ctx, ctypes.c_uint32], ctypes.c_int),
+        "b3g_set_tree_rebuild_interval": ([ctx, ctypes.c_uint32], ctypes.c_int),
         "b3g_set_joint_pairs": ([ctx, ctypes.c_uint32, _p(ctypes.c_uint32)], ctypes.c_int),
         "b3g_set_contact_veto": ([ctx, ctypes.c_uint32, _p(ctypes.c_uint8)], ctypes.c_int),
         "b3g_fetch_new_pairs": ([ctx, _p(ctypes.c_uint32), ctypes.c_uint32], ctypes.c_int),

@@ -62,6 +62,9 @@ void dfree(T*& p)
 // Captured passes become invalid when the scene or a launch shape changes.
 void destroy_graphs(b3g_ctx* c)
 {
+	// Whatever made the captured passes stale may have changed the proxy set:
+	// the next pass rebuilds the LBVH.
+	c->treeForce = true;
 	for (int i = 0; i < 2; ++i)
 		for (int j = 0; j < 2; ++j)
 		{
@@ -426,6 +429,10 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->passOpen = false;
 	c->filterMode = 0;
 	c->walkLimit = 0;
+	c->treeLeaves = 0;
+	c->treeWorlds = 0;
+	c->treeInterval = B3G_TREE_REBUILD_INTERVAL;
+	c->treeForce = true;
 	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
 	{
 		delete c;
@@ -465,6 +472,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.nodeRope, 2 * P), "alloc");
 	step(dalloc(&B.nodeFirst, 2 * P), "alloc");
 	step(dalloc(&B.leafData, P), "alloc");
+	step(dalloc(&B.treeState, 4), "alloc");
+	step(dalloc(&B.lifeSeen, P), "alloc");
 	step(dalloc(&B.nodeParent, 2 * P), "alloc");
 	step(dalloc(&B.nodeEnd, P), "alloc");
 	step(dalloc(&B.splitRight, P), "alloc");
@@ -524,6 +533,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 		step(cudaMemsetAsync(B.counters, 0, sizeof(uint32_t) * CTR_COUNT, c->stream), "memset");
 		step(cudaMemsetAsync(c->dUpdateBad, 0, sizeof(uint32_t), c->stream), "memset");
 		step(cudaMemsetAsync(B.totals, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
+		step(cudaMemsetAsync(B.treeState, 0, sizeof(uint32_t) * 4, c->stream), "memset");
+		step(cudaMemsetAsync(B.lifeSeen, 0xFF, P, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[0], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.hashKeys[0], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
@@ -566,6 +577,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.nodeRope);
 	dfree(B.nodeFirst);
 	dfree(B.leafData);
+	dfree(B.treeState);
+	dfree(B.lifeSeen);
 	dfree(B.nodeParent);
 	dfree(B.nodeEnd);
 	dfree(B.splitRight);
@@ -2669,6 +2682,20 @@ extern "C" int b3g_set_walk_limit(b3g_ctx* c, uint32_t maxNodes)
 	CK(cudaDeviceSynchronize());
 	destroy_graphs(c); // captured passes hold the old limit
 	c->walkLimit = maxNodes;
+	return B3G_OK;
+}
+
+extern "C" int b3g_set_tree_rebuild_interval(b3g_ctx* c, uint32_t passes)
+{
+	if (!c)
+		return B3G_E_INVALID;
+	if (passes == 0)
+		return fail(c, B3G_E_INVALID, "b3g_set_tree_rebuild_interval: the interval is at least 1 pass");
+	CK(cudaSetDevice(c->device));
+	CK(cudaDeviceSynchronize());
+	destroy_graphs(c); // captured passes hold the old interval
+	c->treeInterval = passes;
+	c->treeForce = true;
 	return B3G_OK;
 }
 

@@ -136,6 +136,11 @@ class CollisionPipeline:
         """Node visits allowed per broadphase walk (0: the depth-first bound)."""
         self._check(self.lib.b3g_set_walk_limit(self.ctx, int(max_nodes)))
 
+    def set_tree_rebuild_interval(self, passes):
+        """Passes between LBVH rebuilds (the tree is refit in between; 1
+        rebuilds every pass). Results do not depend on it."""
+        self._check(self.lib.b3g_set_tree_rebuild_interval(self.ctx, int(passes)))
+
     def counts(self):
         c = N.Counts()
         self._check(self.lib.b3g_get_counts(self.ctx, ctypes.byref(c)))

@@ -484,6 +484,19 @@ int b3g_set_tuning(b3g_ctx* ctx, const uint32_t* table);
  * passes are dropped so the new bound takes effect. The reference has no
  * counterpart (its walks and sorts run on the host without bounds). */
 int b3g_set_walk_limit(b3g_ctx* ctx, uint32_t max_nodes);
+
+/* LBVH reuse. A pass rebuilds the broadphase tree (Morton keys, sort, build)
+ * only every `passes` passes, and whenever the set of proxies changed (a
+ * fixture created, destroyed or replaced, another fixture or world count, a
+ * new scene); the passes in between put the new fat AABBs in the leaves and
+ * refit the internal boxes, as the reference's b3DynamicTree keeps its tree
+ * across steps (dynamic_tree.cpp:108-207). The pairs found, their order and
+ * every result are the same for any interval; only the walk lengths change.
+ * 1 rebuilds every pass. Default B3G_TREE_REBUILD_INTERVAL. The captured
+ * passes are dropped. The reference has no counterpart (its tree is
+ * incremental by construction). */
+#define B3G_TREE_REBUILD_INTERVAL 8u
+int b3g_set_tree_rebuild_interval(b3g_ctx* ctx, uint32_t passes);
 int b3g_get_tuning(b3g_ctx* ctx, uint32_t* table);
 
 /* Device pointers of the last pass's results for zero-copy consumers:
