@@ -524,6 +524,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.touchIndex, C), "alloc");
 	step(dalloc(&B.touchMan, C), "alloc");
 	step(dalloc(&B.contactOut, 3 * (size_t)C), "alloc");
+	// The packed result copies' per-contact byte counts, allocated here so no
+	// fetch pays for an allocation.
+	step(dalloc(&c->touchBytes, C), "alloc");
 	step(dalloc(&B.impulseNormal, 4 * (size_t)C), "alloc");
 	step(dalloc(&B.impulseTangent, 2 * (size_t)C), "alloc");
 	step(dalloc(&B.impulseMotor, C), "alloc");

@@ -356,7 +356,7 @@ struct b3g_ctx
 	cudaEvent_t copyReady;    // results of the pass ready to copy
 	cudaEvent_t copyDone;     // those copies finished
 	bool copyPending;
-	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds (allocated on first use)
+	uint32_t* touchBytes;     // per contact: packed bytes of its manifolds
 	void* edgeBuf;            // b3g_fetch_fixture_contacts scratch (allocated on first use)
 	size_t edgeBytes;
 	cudaStream_t sideStream;  // hull-hull / hull-triangle narrowphase, beside the convex buckets

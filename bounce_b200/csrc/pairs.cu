@@ -124,45 +124,64 @@ __global__ void k_apply_veto(FilterArgs F, const uint32_t* rejected, uint32_t n)
 		F.rawDrop[rejected[t]] = 1;
 }
 
-__global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
+// Contacts to their narrowphase lists. The lists' counters are a dozen
+// addresses that every contact of the pass adds to, so a block takes a tile of
+// BUCKET_THREADS contacts, counts them per list in shared memory, reserves each
+// list's range with one atomic, and then writes its contacts there.
+constexpr int BUCKET_THREADS = 256;
+
+__global__ void __launch_bounds__(BUCKET_THREADS) k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 {
-	uint32_t n = min(B.counters[CTR_PAIRS], cap);
-	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+	__shared__ uint32_t sCount[BK_COUNT], sBase[BK_COUNT];
+	const uint32_t n = min(B.counters[CTR_PAIRS], cap);
+	const uint32_t lane = threadIdx.x & 31;
+	for (uint32_t tile = blockIdx.x * BUCKET_THREADS; tile < n; tile += gridDim.x * BUCKET_THREADS)
 	{
-		uint32_t fa = B.pairA[cur][c], fb = B.pairB[cur][c];
-		uint32_t ba = S.fixBody[fa], bb = S.fixBody[fb];
-		bool activeA = S.bodyAwake[ba] && S.bodyType[ba] != B3G_BODY_STATIC;
-		bool activeB = S.bodyAwake[bb] && S.bodyType[bb] != B3G_BODY_STATIC;
-		uint32_t bk;
-		if (!activeA && !activeB)
-			bk = BK_INACTIVE;
-		else if (S.fixType[fa] == B3G_SHAPE_MESH || S.fixType[fb] == B3G_SHAPE_MESH)
-			bk = BK_MESH; // b3MeshContact, sensors included (its TestOverlap runs per triangle)
-		else if ((S.fixFlags[fa] | S.fixFlags[fb]) & B3G_FIXTURE_SENSOR)
-			bk = BK_SENSOR;
-		else
-			bk = bucket_of(S.fixType[fa], S.fixType[fb]);
-		if (bk >= BK_COUNT)
-			bk = BK_INACTIVE;
-		// Convex pairs whose bounding spheres are apart skip their routine
-		// (spheres_apart); taking them out keeps the routines' warps full.
-		if (bk <= BK_HULL_CAPSULE)
+		if (threadIdx.x < BK_COUNT)
+			sCount[threadIdx.x] = 0;
+		__syncthreads();
+		const uint32_t c = tile + threadIdx.x;
+		uint32_t bk = BK_COUNT, off = 0;
+		if (c < n)
 		{
-			XF xfA = body_xf(S, ba), xfB = body_xf(S, bb);
-			if (spheres_apart(S, fa, xfA, fb, xfB) ||
-				(bk == BK_HULL_CAPSULE && hull_capsule_apart(S, fa, xfA, fb, xfB)))
-				bk = BK_APART;
+			uint32_t fa = B.pairA[cur][c], fb = B.pairB[cur][c];
+			uint32_t ba = S.fixBody[fa], bb = S.fixBody[fb];
+			bool activeA = S.bodyAwake[ba] && S.bodyType[ba] != B3G_BODY_STATIC;
+			bool activeB = S.bodyAwake[bb] && S.bodyType[bb] != B3G_BODY_STATIC;
+			if (!activeA && !activeB)
+				bk = BK_INACTIVE;
+			else if (S.fixType[fa] == B3G_SHAPE_MESH || S.fixType[fb] == B3G_SHAPE_MESH)
+				bk = BK_MESH; // b3MeshContact, sensors included (its TestOverlap runs per triangle)
+			else if ((S.fixFlags[fa] | S.fixFlags[fb]) & B3G_FIXTURE_SENSOR)
+				bk = BK_SENSOR;
+			else
+				bk = bucket_of(S.fixType[fa], S.fixType[fb]);
+			if (bk >= BK_COUNT)
+				bk = BK_INACTIVE;
+			// Convex pairs whose bounding spheres are apart skip their routine
+			// (spheres_apart); taking them out keeps the routines' warps full.
+			if (bk <= BK_HULL_CAPSULE)
+			{
+				XF xfA = body_xf(S, ba), xfB = body_xf(S, bb);
+				if (spheres_apart(S, fa, xfA, fb, xfB) ||
+					(bk == BK_HULL_CAPSULE && hull_capsule_apart(S, fa, xfA, fb, xfB)))
+					bk = BK_APART;
+			}
+			// The warp's contacts of one list take one shared-memory atomic.
+			uint32_t peers = __match_any_sync(__activemask(), bk);
+			uint32_t leader = __ffs(peers) - 1;
+			uint32_t base = 0;
+			if (lane == leader)
+				base = atomicAdd(&sCount[bk], (uint32_t)__popc(peers));
+			off = __shfl_sync(peers, base, leader) + __popc(peers & ((1u << lane) - 1u));
 		}
-		// Warp-aggregated append.
-		uint32_t peers = __match_any_sync(__activemask(), bk);
-		uint32_t leader = __ffs(peers) - 1;
-		uint32_t lane = threadIdx.x & 31;
-		uint32_t base = 0;
-		if (lane == leader)
-			base = atomicAdd(&B.counters[CTR_BUCKET0 + bk], (uint32_t)__popc(peers));
-		base = __shfl_sync(peers, base, leader);
-		uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-		B.bucketList[(size_t)bk * cap + base + rank] = c;
+		__syncthreads();
+		if (threadIdx.x < BK_COUNT && sCount[threadIdx.x])
+			sBase[threadIdx.x] = atomicAdd(&B.counters[CTR_BUCKET0 + threadIdx.x], sCount[threadIdx.x]);
+		__syncthreads();
+		if (bk < BK_COUNT)
+			B.bucketList[(size_t)bk * cap + sBase[bk] + off] = c;
+		__syncthreads();
 	}
 }
 
@@ -171,8 +190,9 @@ __global__ void k_bucket(DevScene S, Buffers B, uint32_t cur, uint32_t cap)
 // it uses any (the manifold's point count too, whether or not the contact
 // has a manifold), so the loads of a contact do not wait on one another.
 constexpr int FIN_BATCH = 4;
+constexpr int FIN_THREADS = 256;
 
-__global__ void k_finalize(Buffers B, uint32_t cur, uint32_t cap)
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize(Buffers B, uint32_t cur, uint32_t cap)
 {
 	uint32_t n = min(B.counters[CTR_PAIRS], cap);
 	uint32_t touching = 0, manifolds = 0, points = 0;
@@ -224,8 +244,26 @@ __global__ void k_finalize(Buffers B, uint32_t cur, uint32_t cap)
 		manifolds += __shfl_xor_sync(0xffffffffu, manifolds, o);
 		points += __shfl_xor_sync(0xffffffffu, points, o);
 	}
-	if ((threadIdx.x & 31) == 0)
+	// One atomic per counter and block: the counters are a handful of
+	// addresses that every block adds to.
+	__shared__ uint32_t sSum[3][FIN_THREADS / 32];
+	const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (lane == 0)
 	{
+		sSum[0][warp] = touching;
+		sSum[1][warp] = manifolds;
+		sSum[2][warp] = points;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		touching = manifolds = points = 0;
+		for (uint32_t w = 0; w < FIN_THREADS / 32; ++w)
+		{
+			touching += sSum[0][w];
+			manifolds += sSum[1][w];
+			points += sSum[2][w];
+		}
 		if (touching)
 			atomicAdd(&B.counters[CTR_TOUCHING], touching);
 		if (manifolds)
@@ -385,7 +423,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	launch_mesh_prepare(c, ms);
 	if (meshSide)
 		cudaEventRecord(c->meshJoin, ms);
-	k_bucket<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, c->cur, cap);
+	k_bucket<<<persistent_blocks(8), BUCKET_THREADS, 0, s>>>(c->scene, B, c->cur, cap);
 	prof_mark(c, PM_BUCKETED, s);
 	NPArgs a = make_np_args(c);
 	// The buckets are disjoint sets of contacts: the hull-hull and
@@ -423,7 +461,7 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 
 void launch_finalize(b3g_ctx* c, cudaStream_t s)
 {
-	k_finalize<<<persistent_blocks(4), 256, 0, s>>>(c->buf, c->cur, c->cfg.max_contacts);
+	k_finalize<<<persistent_blocks(4), FIN_THREADS, 0, s>>>(c->buf, c->cur, c->cfg.max_contacts);
 	k_pass_end<<<1, 32, 0, s>>>(c->buf, c->cfg.max_contacts);
 	k_settle<<<(c->nFixtures + 255) / 256, 256, 0, s>>>(c->scene, c->nFixtures);
 }
