@@ -955,34 +955,47 @@ __global__ void __launch_bounds__(SC_THREADS) k_scan_tiles(uint32_t* data, const
 		const uint32_t agg = __shfl_sync(0xFFFFFFFFu, wi, SC_THREADS / 32 - 1);
 		if (lane < SC_THREADS / 32)
 			warpSums[lane] = wi - w;
+		// Look-back by the whole warp: lane k reads the tile k + 1 places
+		// back, so a round trip covers 32 tiles. A window is taken once every
+		// tile in it has published; the nearest inclusive prefix in it ends
+		// the walk (tiles before the first one count as an inclusive 0).
+		volatile unsigned long long* st = state + 1;
+		if (lane == 0)
+			st[tile] = (tile == 0 ? SC_INC : SC_AGG) | agg;
+		uint32_t prefix = 0;
+		int32_t look = (int32_t)tile - 1;
+		uint32_t spins = 0;
+		while (tile > 0)
+		{
+			const int32_t idx = look - (int32_t)lane;
+			unsigned long long w8 = 2ull << 62; // before tile 0: an inclusive 0
+			if (idx >= 0)
+				w8 = st[idx];
+			if (!__all_sync(0xFFFFFFFFu, (w8 >> 62) != 0ull))
+			{
+				if (++spins > SC_SPIN)
+				{
+					if (lane == 0)
+						atomicOr(err, B3G_ST_WAIT_TIMEOUT);
+					break;
+				}
+				continue;
+			}
+			const uint32_t inc = __ballot_sync(0xFFFFFFFFu, (w8 & SC_INC) != 0ull);
+			const uint32_t last = inc ? (uint32_t)(__ffs(inc) - 1) : 31u;
+			uint32_t v = lane <= last ? (uint32_t)w8 : 0u;
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1)
+				v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+			prefix += v;
+			if (inc)
+				break;
+			look -= 32;
+		}
 		if (lane == 0)
 		{
-			volatile unsigned long long* st = state + 1;
-			uint32_t prefix = 0;
-			if (tile == 0)
-				st[0] = SC_INC | agg;
-			else
+			if (tile > 0)
 			{
-				st[tile] = SC_AGG | agg;
-				int32_t look = (int32_t)tile - 1;
-				uint32_t spins = 0;
-				while (look >= 0)
-				{
-					const unsigned long long w8 = st[look];
-					if ((w8 >> 62) == 0ull)
-					{
-						if (++spins > SC_SPIN)
-						{
-							atomicOr(err, B3G_ST_WAIT_TIMEOUT);
-							break;
-						}
-						continue;
-					}
-					prefix += (uint32_t)w8;
-					if (w8 & SC_INC)
-						break;
-					--look;
-				}
 				__threadfence();
 				st[tile] = SC_INC | (uint32_t)(prefix + agg);
 			}
