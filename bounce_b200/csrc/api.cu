@@ -81,6 +81,8 @@ void default_tuning(Tune& t)
 {
 	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
 		t.v[B3G_TUNE_CONVEX + k] = 4;
+	// The hull-sphere face scan holds few registers: twice the blocks fit.
+	t.v[B3G_TUNE_CONVEX + 5] = 8;
 	t.v[B3G_TUNE_PROBE] = 4;
 	t.v[B3G_TUNE_SAT_WARPS] = 4;
 	t.v[B3G_TUNE_SAT_BLOCKS] = 2;

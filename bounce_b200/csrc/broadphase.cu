@@ -400,36 +400,6 @@ __global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
 // ---------------------------------------------------------------------------
 // Scans.
 
-// Single-block exclusive scan of m entries (m <= 1024 * per-thread chunk).
-__global__ void k_scan_single(uint32_t* data, uint32_t m, uint32_t* total)
-{
-	__shared__ uint32_t s[1024];
-	uint32_t per = (m + blockDim.x - 1) / blockDim.x;
-	uint32_t beg = threadIdx.x * per;
-	uint32_t end = min(beg + per, m);
-	uint32_t sum = 0;
-	for (uint32_t i = beg; i < end; ++i)
-		sum += data[i];
-	s[threadIdx.x] = sum;
-	__syncthreads();
-	for (uint32_t off = 1; off < blockDim.x; off <<= 1)
-	{
-		uint32_t v = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-		__syncthreads();
-		s[threadIdx.x] += v;
-		__syncthreads();
-	}
-	uint32_t run = s[threadIdx.x] - sum;
-	for (uint32_t i = beg; i < end; ++i)
-	{
-		uint32_t v = data[i];
-		data[i] = run;
-		run += v;
-	}
-	if (total && threadIdx.x == blockDim.x - 1)
-		*total = s[threadIdx.x];
-}
-
 // One-sweep LSD radix sort (Merrill & Garland's decoupled look-back): one
 // histogram kernel for every digit pass up front, then one kernel per pass.
 // A block ranks its tile's keys per digit in shared memory (stable: element

@@ -457,6 +457,9 @@ const char* b3g_stage_name(uint32_t stage);
  *                          SAT kernels (2, 4, 8)
  *   [B3G_TUNE_SAT_BLOCKS]  blocks per SM of those kernels
  *   [B3G_TUNE_TRAVERSE]    threads per block of the LBVH traversal (64, 128, 256)
+ * Defaults: 4 blocks per SM everywhere but the hull-sphere kernel (8: its
+ * face scan holds few registers), 4 SAT warps per block, 2 SAT blocks per SM,
+ * 128 traversal threads.
  * b3g_autotune picks each entry by timing the kernel it drives on the last
  * pass's data (the kernels re-run on the same inputs write the same outputs,
  * so the pass's results are unchanged), reps launches per candidate; it

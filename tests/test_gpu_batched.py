@@ -71,7 +71,7 @@ def test_launch_shapes_do_not_change_results():
     high = CollisionPipeline(sc)
     tuned = CollisionPipeline(sc)
     t = base.tuning()
-    assert list(t) == [4] * 9 + [4, 4, 2, 128]
+    assert list(t) == [4] * 5 + [8] + [4] * 3 + [4, 4, 2, 128]
     lo = np.array([1] * 9 + [1, 2, 1, 64], np.uint32)
     hi = np.array([16] * 9 + [16, 8, 8, 256], np.uint32)
     low.set_tuning(lo)
