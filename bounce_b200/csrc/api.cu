@@ -67,13 +67,15 @@ void destroy_graphs(b3g_ctx* c)
 	c->treeForce = true;
 	for (int i = 0; i < 2; ++i)
 		for (int j = 0; j < 2; ++j)
-		{
-			if (c->graphs[i][j].exec)
-				cudaGraphExecDestroy(c->graphs[i][j].exec);
-			if (c->graphs[i][j].graph)
-				cudaGraphDestroy(c->graphs[i][j].graph);
-			c->graphs[i][j] = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
-		}
+			for (int r = 0; r < 2; ++r)
+			{
+				PassGraph& g = c->graphs[i][j][r];
+				if (g.exec)
+					cudaGraphExecDestroy(g.exec);
+				if (g.graph)
+					cudaGraphDestroy(g.graph);
+				g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+			}
 }
 
 // Launch shapes before any tuning.
@@ -408,7 +410,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->lastPassImpulses = false;
 	for (int i = 0; i < 2; ++i)
 		for (int j = 0; j < 2; ++j)
-			c->graphs[i][j] = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
+			for (int r = 0; r < 2; ++r)
+				c->graphs[i][j][r] = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr};
 	default_tuning(c->tune);
 	c->dFixParams = nullptr;
 	c->dFixBound = nullptr;
@@ -434,7 +437,9 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	c->treeLeaves = 0;
 	c->treeWorlds = 0;
 	c->treeInterval = B3G_TREE_REBUILD_INTERVAL;
+	c->treeSince = 0;
 	c->treeForce = true;
+	c->treeRebuild = true;
 	if (cfg->max_proxies == 0 || cfg->max_contacts == 0)
 	{
 		delete c;
@@ -474,8 +479,6 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.nodeRope, 2 * P), "alloc");
 	step(dalloc(&B.nodeFirst, 2 * P), "alloc");
 	step(dalloc(&B.leafData, P), "alloc");
-	step(dalloc(&B.treeState, 4), "alloc");
-	step(dalloc(&B.lifeSeen, P), "alloc");
 	step(dalloc(&B.nodeParent, 2 * P), "alloc");
 	step(dalloc(&B.nodeEnd, P), "alloc");
 	step(dalloc(&B.splitRight, P), "alloc");
@@ -538,8 +541,6 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 		step(cudaMemsetAsync(B.counters, 0, sizeof(uint32_t) * CTR_COUNT, c->stream), "memset");
 		step(cudaMemsetAsync(c->dUpdateBad, 0, sizeof(uint32_t), c->stream), "memset");
 		step(cudaMemsetAsync(B.totals, 0, sizeof(unsigned long long) * 8, c->stream), "memset");
-		step(cudaMemsetAsync(B.treeState, 0, sizeof(uint32_t) * 4, c->stream), "memset");
-		step(cudaMemsetAsync(B.lifeSeen, 0xFF, P, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[0], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.hashKeys[0], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
@@ -582,8 +583,6 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.nodeRope);
 	dfree(B.nodeFirst);
 	dfree(B.leafData);
-	dfree(B.treeState);
-	dfree(B.lifeSeen);
 	dfree(B.nodeParent);
 	dfree(B.nodeEnd);
 	dfree(B.splitRight);
@@ -1292,6 +1291,7 @@ extern "C" int b3g_update_scene_device(b3g_ctx* c, uint32_t nb, const uint32_t* 
 	u.rIdx = retireIndex;
 	launch_update(c, u, s);
 	CK(cudaGetLastError());
+	c->treeForce = true; // fixtures created, replaced or retired: new leaves
 	// The host copy of fixture types is refreshed when the stand-alone
 	// narrowphase next needs it; written bodies are awake, so the sleep count
 	// can only have dropped (it stays an upper bound until the next wake-up
@@ -1385,6 +1385,7 @@ extern "C" int b3g_update_scene(b3g_ctx* c, uint32_t nb, const uint32_t* bodyInd
 	CK(cudaEventRecord(slot.done, s));
 	launch_update(c, u, s);
 	CK(cudaGetLastError());
+	c->treeForce = true; // fixtures created, replaced or retired: new leaves
 	// Host shadows: fixture types (stand-alone narrowphase) and sleep count.
 	for (uint32_t i = 0; i < nf; ++i)
 		c->hFixType[fixIndex[i]] = shapeType[i];
@@ -1531,6 +1532,27 @@ static void wait_copies(b3g_ctx* c, cudaStream_t s)
 		cudaStreamWaitEvent(s, c->copyDone, 0);
 }
 
+// Kernels of a pass's narrowphase: bucketing, the apart pairs, the convex
+// buckets (with the hull-sphere and hull-capsule follow-up kernels), the hull
+// probe and SAT, hull-triangle, and the mesh work.
+static uint32_t narrow_launches(const b3g_ctx* c)
+{
+	return 1 + 1 + B3G_CONVEX_KERNELS + 2 + 2 + 1 + mesh_launches(c);
+}
+
+// The LBVH bookkeeping once a pass's broadphase is issued.
+static void tree_pass_issued(b3g_ctx* c)
+{
+	if (c->treeRebuild)
+	{
+		c->treeSince = 0;
+		c->treeForce = false;
+		c->treeWorlds = c->nWorlds;
+	}
+	else
+		++c->treeSince;
+}
+
 extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* stream)
 {
 	if (!c || !state)
@@ -1541,10 +1563,14 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
 	size_t bytes = sizeof(float) * 17 * (size_t)c->nBodies;
 	const cudaMemcpyKind kind = onDevice ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+	// LBVH plan of this pass (broadphase.cu): rebuild every treeInterval
+	// passes and whenever the proxy set may have changed, else refit.
+	c->treeRebuild = c->treeForce || c->treeLeaves != c->nFixtures || c->treeWorlds != c->nWorlds ||
+		c->treeSince + 1 >= c->treeInterval;
 	// pass_begin, sync, broadphase, diff + list order, bucket + apart + convex kernels + 2 hull +
 	// hull-triangle, finalize + pass_end + settle
 	const uint32_t passLaunches = 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
-		pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3;
+		pairs_diff_launches(c) + narrow_launches(c) + 3;
 	// Host state takes the graph path when it is pinned (a graph copies it
 	// asynchronously; pageable memory would need the synchronous copy).
 	bool pinnedHost = false;
@@ -1573,18 +1599,25 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	if (graph)
 	{
 		c->cur ^= 1u;
-		PassGraph& g = c->graphs[c->cur][c->impulsesLoaded ? 1 : 0];
-		if (g.exec && g.stream == s && g.kind == kind && g.state != state)
+		// A pass of this parity is captured in both forms (tree rebuilt,
+		// tree refit) the first time either is needed, so a later pass never
+		// pays for a capture.
+		const bool rebuild = c->treeRebuild;
+		for (int variant = 0; variant < 2; ++variant)
 		{
-			// Same pass, state at another address: re-point the copy node.
-			if (g.copyNode && cudaGraphExecMemcpyNodeSetParams1D(g.exec, g.copyNode, c->dBodyState, state, bytes,
-								   kind) == cudaSuccess)
-				g.state = state;
-			else
-				cudaGetLastError();
-		}
-		if (!g.exec || g.state != state || g.stream != s || g.kind != kind)
-		{
+			c->treeRebuild = variant == 0 ? rebuild : !rebuild;
+			PassGraph& g = c->graphs[c->cur][c->impulsesLoaded ? 1 : 0][c->treeRebuild ? 1 : 0];
+			if (g.exec && g.stream == s && g.kind == kind && g.state != state)
+			{
+				// Same pass, state at another address: re-point the copy node.
+				if (g.copyNode && cudaGraphExecMemcpyNodeSetParams1D(g.exec, g.copyNode, c->dBodyState, state,
+									   bytes, kind) == cudaSuccess)
+					g.state = state;
+				else
+					cudaGetLastError();
+			}
+			if (g.exec && g.state == state && g.stream == s && g.kind == kind)
+				continue;
 			if (g.exec)
 				cudaGraphExecDestroy(g.exec);
 			if (g.graph)
@@ -1602,6 +1635,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			if (e != cudaSuccess)
 			{
 				g.graph = nullptr;
+				c->treeRebuild = rebuild;
 				return fail(c, B3G_E_CUDA, "b3g_collide: pass capture failed: %s", cudaGetErrorString(e));
 			}
 			e = cudaGraphInstantiate(&g.exec, g.graph, 0);
@@ -1609,13 +1643,15 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			{
 				cudaGraphDestroy(g.graph);
 				g = PassGraph{nullptr, nullptr, nullptr, nullptr, nullptr, cudaMemcpyDefault};
+				c->treeRebuild = rebuild;
 				return fail(c, B3G_E_CUDA, "b3g_collide: graph instantiation failed: %s", cudaGetErrorString(e));
 			}
 			g.state = state;
 			g.stream = s;
 			g.kind = kind;
 		}
-		CK(cudaGraphLaunch(g.exec, s));
+		c->treeRebuild = rebuild;
+		CK(cudaGraphLaunch(c->graphs[c->cur][c->impulsesLoaded ? 1 : 0][rebuild ? 1 : 0].exec, s));
 		++c->graphLaunches;
 	}
 	else
@@ -1637,6 +1673,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 			// pass begin, sync, broadphase, candidates; the rest in b3g_finish_pass
 			c->launches += 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) + 2;
 			CK(cudaGetLastError());
+			tree_pass_issued(c);
 			return B3G_OK;
 		}
 		if (c->asleep > 0)
@@ -1653,6 +1690,7 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	}
 	c->launches += passLaunches;
 	CK(cudaGetLastError());
+	tree_pass_issued(c);
 	c->creationPass = false;
 	c->havePass = true;
 	c->impulsesLoaded = false;
@@ -1811,7 +1849,7 @@ extern "C" int b3g_finish_pass(b3g_ctx* c, const uint8_t* keep, uint32_t count)
 	prof_mark(c, PM_FINAL, s);
 	if (c->profiling)
 		++c->profPass;
-	c->launches += pairs_diff_launches(c) + 1 + 1 + B3G_CONVEX_KERNELS + 2 + 1 + mesh_launches(c) + 3 +
+	c->launches += pairs_diff_launches(c) + narrow_launches(c) + 3 +
 		(rejected.empty() ? 0 : 1);
 	CK(cudaGetLastError());
 	c->creationPass = false;

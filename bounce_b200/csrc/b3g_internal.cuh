@@ -167,10 +167,6 @@ struct Buffers
 	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
 	uint32_t* proxyInfo;  // per proxy: body (bits 0-27), dynamic body (bit 28), shape type (bits 29-31)
 	uint2* leafData;      // per sorted leaf: its proxy's proxyInfo word and fixture key
-	// LBVH reuse: [0] rebuild in this pass, [1] passes since the last
-	// rebuild, [2] a rebuild is due (a fixture's life changed, or the host asked)
-	uint32_t* treeState;
-	uint8_t* lifeSeen;    // per fixture: its life state when the pass last synced it
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
 	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (B3G_TRAV_SLOTS x n uint2)
 	uint32_t* scanAux;
@@ -351,7 +347,9 @@ struct b3g_ctx
 	uint32_t treeLeaves;  // leaves of the LBVH built by the last pass
 	uint32_t treeWorlds;  // worlds of the scene the LBVH was last asked to rebuild for
 	uint32_t treeInterval; // passes between LBVH rebuilds (refit in between), b3g_set_tree_rebuild_interval
-	bool treeForce;       // the next pass rebuilds the LBVH (scene or launch-shape change)
+	uint32_t treeSince;   // passes since the LBVH was last rebuilt
+	bool treeForce;       // the next pass rebuilds the LBVH (the proxy set may have changed)
+	bool treeRebuild;     // the pass being issued rebuilds the LBVH
 	cudaStream_t copyStream;  // device-to-host copies of b3g_fetch_results_async
 	cudaEvent_t copyReady;    // results of the pass ready to copy
 	cudaEvent_t copyDone;     // those copies finished
@@ -440,7 +438,7 @@ struct b3g_ctx
 
 	// launch shapes and captured passes
 	Tune tune;
-	PassGraph graphs[2][2]; // [contact buffer][warm start from host impulses]
+	PassGraph graphs[2][2][2]; // [contact buffer][warm start from host impulses][LBVH rebuilt]
 	uint64_t graphLaunches;
 	bool lastPassImpulses;  // the last pass warm-started from host impulses
 

@@ -159,16 +159,7 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int crea
 	const uint32_t btype = S.bodyType[body];
 	// The walk's filter reads one word per proxy (pair_filter).
 	if (w0)
-	{
 		B.proxyInfo[i] = (body & 0x0FFFFFFFu) | (btype == B3G_BODY_DYNAMIC ? 1u << 28 : 0u) | (type << 29);
-		// A proxy created, destroyed or replaced since the last pass changes
-		// the set of leaves: the LBVH is rebuilt this pass.
-		if (B.lifeSeen[i] != life)
-		{
-			B.lifeSeen[i] = life;
-			atomicOr(&B.treeState[2], 1u);
-		}
-	}
 	if (life == FIX_DEAD)
 	{
 		// No proxy: an empty box (lower > upper) that overlaps nothing.
@@ -281,25 +272,8 @@ __device__ __forceinline__ float o2f(int i)
 	return __int_as_float(i >= 0 ? i : i ^ 0x7FFFFFFF);
 }
 
-// LBVH reuse. The set of pairs a walk finds does not depend on the tree's
-// shape, only on its boxes, and the contact order does not depend on the
-// order they are found in (it follows the proxy keys). So the tree is rebuilt
-// (Morton keys, sort, Karras build) every `interval` passes, or when the set
-// of leaves changed (a fixture's life changed, k_sync; or the host asked:
-// another leaf count, world count, or scene); in the passes between, the
-// leaves take the new fat AABBs and the internal boxes are refit, as
-// b3DynamicTree keeps its tree across steps. treeState[0] tells the sort and
-// build kernels of the pass whether to run.
-__global__ void k_tree_plan(int* bnd, uint32_t* ts, uint32_t interval)
+__global__ void k_bounds_init(int* bnd)
 {
-	if (threadIdx.x == 0)
-	{
-		const uint32_t since = ts[1] + 1u;
-		const bool rebuild = ts[2] != 0u || since >= interval;
-		ts[0] = rebuild ? 1u : 0u;
-		ts[1] = rebuild ? 0u : since;
-		ts[2] = 0u;
-	}
 	if (threadIdx.x < 3)
 		bnd[threadIdx.x] = 0x7FFFFFFF;
 	else if (threadIdx.x < 6)
@@ -308,8 +282,6 @@ __global__ void k_tree_plan(int* bnd, uint32_t* ts, uint32_t interval)
 
 __global__ void k_bounds(DevScene S, Buffers B, uint32_t n, int* bnd)
 {
-	if (B.treeState[0] == 0u)
-		return;
 	__shared__ int s[6][8];
 	float mn[3] = {B3G_MAX_SCALAR, B3G_MAX_SCALAR, B3G_MAX_SCALAR};
 	float mx[3] = {-B3G_MAX_SCALAR, -B3G_MAX_SCALAR, -B3G_MAX_SCALAR};
@@ -368,7 +340,7 @@ __device__ __forceinline__ uint32_t expand10(uint32_t v)
 __global__ void k_morton(DevScene S, Buffers B, uint32_t n, const int* bnd)
 {
 	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n || B.treeState[0] == 0u)
+	if (i >= n)
 		return;
 	float lo[3] = {o2f(bnd[0]), o2f(bnd[1]), o2f(bnd[2])};
 	float hi[3] = {o2f(bnd[3]), o2f(bnd[4]), o2f(bnd[5])};
@@ -422,12 +394,9 @@ struct SortShifts
 	int n;
 };
 
-__global__ void k_os_hist(const unsigned long long* keys, uint32_t n, SortShifts sh, uint32_t* ghist,
-	const uint32_t* run)
+__global__ void k_os_hist(const unsigned long long* keys, uint32_t n, SortShifts sh, uint32_t* ghist)
 {
 	__shared__ uint32_t h[8][256];
-	if (run && *run == 0u)
-		return;
 	for (int p = 0; p < sh.n; ++p)
 		h[p][threadIdx.x] = 0;
 	__syncthreads();
@@ -444,11 +413,9 @@ __global__ void k_os_hist(const unsigned long long* keys, uint32_t n, SortShifts
 }
 
 // Exclusive scan of each pass's 256 digit counts (one block of 256 per pass).
-__global__ void k_os_scan(uint32_t* ghist, const uint32_t* run)
+__global__ void k_os_scan(uint32_t* ghist)
 {
 	__shared__ uint32_t v[256];
-	if (run && *run == 0u)
-		return;
 	uint32_t* g = ghist + blockIdx.x * 256;
 	uint32_t x = g[threadIdx.x];
 	v[threadIdx.x] = x;
@@ -465,10 +432,8 @@ __global__ void k_os_scan(uint32_t* ghist, const uint32_t* run)
 
 __global__ void __launch_bounds__(OS_THREADS) k_onesweep(const unsigned long long* kin, const uint32_t* vin,
 	unsigned long long* kout, uint32_t* vout, uint32_t n, int shift, const uint32_t* gOffset, uint32_t* status,
-	uint32_t* tileCounter, uint32_t* err, const uint32_t* plan)
+	uint32_t* tileCounter, uint32_t* err)
 {
-	if (plan && *plan == 0u)
-		return;
 	__shared__ uint32_t sTile;
 	__shared__ uint32_t run[256];
 	__shared__ uint32_t wc[OS_THREADS / 32][256];
@@ -580,7 +545,7 @@ __device__ __forceinline__ int delta(const unsigned long long* k, int n, int i, 
 __global__ void k_build(Buffers B, int n)
 {
 	int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n - 1 || B.treeState[0] == 0u)
+	if (i >= n - 1)
 		return;
 	const unsigned long long* k = B.keysA;
 	int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
@@ -1031,14 +996,14 @@ bool radix_sort_pairs(unsigned long long* keys, uint32_t* vals, unsigned long lo
 		return false;
 	const uint32_t numTiles = (n + OS_TILE - 1) / OS_TILE;
 	cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * (9 * 256 + (size_t)sh.n * numTiles * 256), s);
-	k_os_hist<<<min((n + 255) / 256, 148u * 4u), 256, 0, s>>>(keys, n, sh, scratch, nullptr);
-	k_os_scan<<<sh.n, 256, 0, s>>>(scratch, nullptr);
+	k_os_hist<<<min((n + 255) / 256, 148u * 4u), 256, 0, s>>>(keys, n, sh, scratch);
+	k_os_scan<<<sh.n, 256, 0, s>>>(scratch);
 	unsigned long long *kin = keys, *kout = keysTmp;
 	uint32_t *vin = vals, *vout = valsTmp;
 	for (int p = 0; p < sh.n; ++p)
 	{
 		k_onesweep<<<numTiles, OS_THREADS, 0, s>>>(kin, vin, kout, vout, n, sh.s[p], scratch + 256 * p,
-			scratch + 9 * 256 + (size_t)p * numTiles * 256, scratch + 8 * 256 + p, err, nullptr);
+			scratch + 9 * 256 + (size_t)p * numTiles * 256, scratch + 8 * 256 + p, err);
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}
@@ -1068,27 +1033,37 @@ uint32_t broadphase_launches(const b3g_ctx* c)
 	while ((1u << wb) < c->nWorlds)
 		++wb;
 	uint32_t passes = 4 + (wb + 7) / 8;
-	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 2 + 3 + 1; // sort: histogram, scan, one kernel per pass
+	// traversal: walk, scan, emit, overflow
+	if (!c->treeRebuild)
+		return 2 + 4; // leaves, refit
+	// bounds init, bounds, Morton; sort: histogram, scan, one kernel per
+	// pass; build; leaves, refit
+	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 4;
 }
 
 void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	int n = (int)c->nFixtures;
-	if (c->treeForce || c->treeLeaves != (uint32_t)n || c->treeWorlds != c->nWorlds)
-	{
-		cudaMemsetAsync(B.treeState + 2, 0xFF, sizeof(uint32_t), s);
-		c->treeForce = false;
-		c->treeWorlds = c->nWorlds;
-	}
 	c->treeLeaves = (uint32_t)n;
 	if (n == 0)
 	{
 		cudaMemsetAsync(B.counters + CTR_RAW, 0, sizeof(uint32_t), s);
 		return;
 	}
+	if (!c->treeRebuild)
+	{
+		// Same tree as the last pass: new leaf boxes, refit, walk.
+		prof_mark(c, PM_SORTED, s);
+		k_leaves<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, n);
+		k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
+		prof_mark(c, PM_BUILT, s);
+		launch_traverse(c, s);
+		prof_mark(c, PM_TRAVERSED, s);
+		return;
+	}
 	int* bnd = (int*)B.sceneBounds;
-	k_tree_plan<<<1, 32, 0, s>>>(bnd, B.treeState, c->treeInterval);
+	k_bounds_init<<<1, 32, 0, s>>>(bnd);
 	k_bounds<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
 	k_morton<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, (uint32_t)n, bnd);
 
@@ -1108,14 +1083,14 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	uint32_t* tileCounters = B.sortHist + 8 * 256;
 	uint32_t* status = B.sortHist + 9 * 256;
 	cudaMemsetAsync(B.sortHist, 0, sizeof(uint32_t) * (9 * 256 + (size_t)sh.n * numTiles * 256), s);
-	k_os_hist<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(B.keysA, (uint32_t)n, sh, ghist, B.treeState);
-	k_os_scan<<<sh.n, 256, 0, s>>>(ghist, B.treeState);
+	k_os_hist<<<min((n + 255) / 256, 148 * 4), 256, 0, s>>>(B.keysA, (uint32_t)n, sh, ghist);
+	k_os_scan<<<sh.n, 256, 0, s>>>(ghist);
 	unsigned long long *kin = B.keysA, *kout = B.keysB;
 	uint32_t *vin = B.valsA, *vout = B.valsB;
 	for (int p = 0; p < sh.n; ++p)
 	{
 		k_onesweep<<<numTiles, OS_THREADS, 0, s>>>(kin, vin, kout, vout, (uint32_t)n, sh.s[p], ghist + 256 * p,
-			status + (size_t)p * numTiles * 256, tileCounters + p, B.counters + CTR_STATUS, B.treeState);
+			status + (size_t)p * numTiles * 256, tileCounters + p, B.counters + CTR_STATUS);
 		std::swap(kin, kout);
 		std::swap(vin, vout);
 	}

@@ -879,6 +879,6 @@ uint32_t mesh_launches(const b3g_ctx* c)
 {
 	if (!c->nMeshFix)
 		return 0;
-	// sync, scan (3), overflow, emit; two evaluation kernels, cluster
-	return 1 + 3 + 1 + 1 + 2 + 1;
+	// sync, scan, overflow, emit; two evaluation kernels, cluster
+	return 1 + 1 + 1 + 1 + 2 + 1;
 }

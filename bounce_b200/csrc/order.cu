@@ -392,7 +392,8 @@ void launch_order(b3g_ctx* c, cudaStream_t s)
 
 uint32_t order_launches(const b3g_ctx* c)
 {
-	return 3 + 2 + (c->havePass ? 5 : 0);
+	// scan, scatter, place; kept, scan, layout of the previous contacts
+	return 3 + (c->havePass ? 3 : 0);
 }
 
 // Host-driven replay of the wake-ups; runs only when some non-static body is
