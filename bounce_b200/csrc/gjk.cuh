@@ -186,6 +186,14 @@ struct Simplex
 		}
 	}
 
+	// closest_points with the witness points recomputed from the support
+	// indices, by the same expressions that made them when each vertex
+	// joined the simplex (the same bits): the simplex then carries no
+	// witness points through the loop, and the registers they would hold
+	// stay free.
+	__device__ void closest_points_from(const XF& xf1, const GProxy& p1, const XF& xf2, const GProxy& p2, V3& P1,
+		V3& P2) const;
+
 	__device__ void set1(const SVert& a)
 	{
 		count = 1;
@@ -395,6 +403,46 @@ struct Simplex
 	}
 };
 
+__device__ __forceinline__ void Simplex::closest_points_from(const XF& xf1, const GProxy& p1, const XF& xf2,
+	const GProxy& p2, V3& P1, V3& P2) const
+{
+	V3 a1[4], a2[4];
+#pragma unroll
+	for (int i = 0; i < 4; ++i)
+	{
+		if ((uint32_t)i < count)
+		{
+			a1[i] = xmul(xf1, gp_vertex(p1, v[i].index1));
+			a2[i] = xmul(xf2, gp_vertex(p2, v[i].index2));
+		}
+		else
+		{
+			a1[i] = V3{0.0f, 0.0f, 0.0f};
+			a2[i] = V3{0.0f, 0.0f, 0.0f};
+		}
+	}
+	if (count == 1)
+	{
+		P1 = a1[0];
+		P2 = a2[0];
+	}
+	else if (count == 2)
+	{
+		P1 = v[0].weight * a1[0] + v[1].weight * a1[1];
+		P2 = v[0].weight * a2[0] + v[1].weight * a2[1];
+	}
+	else if (count == 3)
+	{
+		P1 = (v[0].weight * a1[0] + v[1].weight * a1[1]) + v[2].weight * a1[2];
+		P2 = (v[0].weight * a2[0] + v[1].weight * a2[1]) + v[2].weight * a2[2];
+	}
+	else if (count == 4)
+	{
+		P1 = ((v[0].weight * a1[0] + v[1].weight * a1[1]) + v[2].weight * a1[2]) + v[3].weight * a1[3];
+		P2 = P1;
+	}
+}
+
 // The main loop of b3GJK (gjk.cpp:683-768) on an initialised simplex;
 // returns the support iterations.
 __device__ __forceinline__ uint32_t gjk_loop(Simplex& sx, const XF& xf1, const GProxy& p1, const XF& xf2,
@@ -486,7 +534,7 @@ __device__ inline GJKOut gjk(const XF& xf1, const GProxy& p1, const XF& xf2, con
 		}
 	}
 	GJKOut out;
-	sx.closest_points(out.point1, out.point2);
+	sx.closest_points_from(xf1, p1, xf2, p2, out.point1, out.point2);
 	out.distance = len(out.point1 - out.point2);
 	out.iterations = iter;
 	if (applyRadius)
@@ -578,7 +626,7 @@ __device__ inline GJKOut gjk_cached(const XF& xf1, const GProxy& p1, const XF& x
 		simplex_first(sx, xf1, p1, xf2, p2);
 	GJKOut out;
 	out.iterations = gjk_loop(sx, xf1, p1, xf2, p2);
-	sx.closest_points(out.point1, out.point2);
+	sx.closest_points_from(xf1, p1, xf2, p2, out.point1, out.point2);
 	out.distance = len(out.point1 - out.point2);
 	cache.metric = simplex_metric(sx);
 	cache.count = sx.count;

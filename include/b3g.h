@@ -476,7 +476,8 @@ int b3g_autotune(b3g_ctx* ctx, uint32_t reps, void* stream, uint32_t* out);
 int b3g_set_tuning(b3g_ctx* ctx, const uint32_t* table);
 
 /* Bounded waits. The device work never waits without a bound: the radix
- * sort's and the solver input's look-backs spin at most 2^22 times, and every
+ * sort's, the scans' and the solver input's look-backs and the hull SAT
+ * kernel's wait for its shared-memory copies spin at most 2^22 times, and every
  * tree walk (broadphase pair search, queries) visits at most the nodes of a
  * depth-first walk; a wait that runs out sets the pass status, and the call
  * that reads it (b3g_get_counts) returns B3G_E_TIMEOUT with the context still
