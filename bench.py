@@ -83,8 +83,9 @@ def parse():
         # The autotuner times each kernel alone; in a single world's pass the
         # convex and hull-hull branches run at the same time, and the shapes
         # it picks there measured slower than the default table (0.80 against
-        # 0.77 ms per pass), so only the batched pass uses it by default.
-        args.autotune = args.workload == "batched"
+        # 0.77 ms per pass), so only the batched pass and the hull pile (its
+        # narrowphase is the hull-hull branch alone) use it by default.
+        args.autotune = args.workload in ("batched", "pile")
     if args.workload in ("batched", "pile"):
         # The batched and pile workloads are quoted on 30 steps.
         if "--steps" not in sys.argv:
