@@ -497,6 +497,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 		step(dalloc(&B.man[k], C), "alloc");
 	}
 	B.hashCap = pow2_at_least(2 * C);
+	step(dalloc(&B.hashMask, 2), "alloc");
 	for (int k = 0; k < 2; ++k)
 	{
 		step(dalloc(&B.hashKeys[k], B.hashCap), "alloc");
@@ -545,6 +546,8 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 		step(cudaMemsetAsync(B.cstate[1], 0, sizeof(uint32_t) * C, c->stream), "memset");
 		step(cudaMemsetAsync(B.hashKeys[0], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
 		step(cudaMemsetAsync(B.hashKeys[1], 0xFF, sizeof(unsigned long long) * B.hashCap, c->stream), "memset");
+		const uint32_t fullMask[2] = {B.hashCap - 1u, B.hashCap - 1u};
+		step(cudaMemcpyAsync(B.hashMask, fullMask, sizeof(fullMask), cudaMemcpyHostToDevice, c->stream), "memcpy");
 		step(cudaStreamSynchronize(c->stream), "sync");
 	}
 	if (rc != B3G_OK)
@@ -600,6 +603,8 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 		dfree(B.cache[k]);
 		dfree(B.man[k]);
 		dfree(B.hashKeys[k]);
+		if (k == 0)
+			dfree(B.hashMask);
 		dfree(B.hashVals[k]);
 	}
 	dfree(B.prevIndex);

@@ -193,7 +193,8 @@ struct Buffers
 	uint32_t* prevFound; // per previous contact: its pair overlaps again this pass
 	unsigned long long* hashKeys[2];
 	uint32_t* hashVals[2];
-	uint32_t hashCap;
+	uint32_t hashCap;     // slots allocated per table (for the contact capacity)
+	uint32_t* hashMask;   // per table: slots in use - 1 (a power of two - 1), sized to its pass's contacts
 
 	// narrowphase work lists
 	uint32_t* bucketList; // BK_COUNT lists of max_contacts entries

@@ -31,10 +31,35 @@
 
 namespace {
 
-__device__ __forceinline__ void insert_contact(Buffers& B, uint32_t cur, uint32_t a, uint32_t b, uint32_t index)
+__device__ __forceinline__ void insert_contact(Buffers& B, uint32_t cur, uint32_t mask, uint32_t a, uint32_t b,
+	uint32_t index)
 {
-	if (!pair_hash_insert(B.hashKeys[cur], B.hashVals[cur], B.hashCap, pair_key(a, b), index))
+	if (!pair_hash_insert(B.hashKeys[cur], B.hashVals[cur], mask + 1u, pair_key(a, b), index))
 		atomicOr(&B.counters[CTR_STATUS], B3G_ST_HASH_OVERFLOW);
+}
+
+// The pass's table of (fixture pair -> contact), read by the next pass's
+// lookup: sized to twice this pass's contacts (rounded up to a power of two,
+// at most the allocation), so the table the lookups and inserts touch stays
+// small enough for L2 rather than spanning the capacity's allocation.
+__device__ __forceinline__ uint32_t hash_mask_for(const Buffers& B, uint32_t contacts)
+{
+	uint32_t slots = 1024u;
+	while (slots < 2u * contacts && slots < B.hashCap)
+		slots <<= 1;
+	return min(slots, B.hashCap) - 1u;
+}
+
+// Clears the slots the table of this pass will use (total contacts, or the
+// pass's count when total is ~0u) and records its size.
+__global__ void k_hash_clear(Buffers B, uint32_t cur, uint32_t cap, uint32_t total)
+{
+	const uint32_t n = total == ~0u ? min(B.counters[CTR_PAIRS], cap) : total;
+	const uint32_t mask = hash_mask_for(B, n);
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		B.hashMask[cur] = mask;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= mask; i += gridDim.x * blockDim.x)
+		B.hashKeys[cur][i] = B3G_EMPTY_KEY;
 }
 
 // New contacts grouped by the smaller key rank, reversed (descending order).
@@ -72,7 +97,6 @@ __global__ void k_new_place(DevScene S, Buffers B, uint32_t cur, uint32_t nf, in
 		B.pairB[cur][pos] = b;
 		B.prevIndex[pos] = -1;
 		B.posKey[pos] = pos;
-		insert_contact(B, cur, a, b, pos);
 	}
 	if (!havePrev && blockIdx.x == 0 && threadIdx.x == 0)
 		B.counters[CTR_PAIRS] = n;
@@ -133,7 +157,6 @@ __global__ void k_layout_prev(Buffers B, uint32_t cur, uint32_t cap)
 				B.pairB[cur][pos] = b;
 				B.prevIndex[pos] = (int32_t)p;
 				B.posKey[pos] = numNew + p;
-				insert_contact(B, cur, a, b, pos);
 			}
 		}
 		else
@@ -355,10 +378,14 @@ __global__ void k_compact_move(Buffers B, uint32_t cur, uint32_t cap, uint32_t n
 	}
 }
 
-__global__ void k_rehash(Buffers B, uint32_t cur, uint32_t n)
+// Fills the pass's table with its contacts (total, or the pass's count when
+// total is ~0u), after k_hash_clear.
+__global__ void k_rehash(Buffers B, uint32_t cur, uint32_t cap, uint32_t total)
 {
+	const uint32_t n = total == ~0u ? min(B.counters[CTR_PAIRS], cap) : total;
+	const uint32_t mask = B.hashMask[cur];
 	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
-		insert_contact(B, cur, B.pairA[cur][c], B.pairB[cur][c], c);
+		insert_contact(B, cur, mask, B.pairA[cur][c], B.pairB[cur][c], c);
 }
 
 __global__ void k_set_counts(Buffers B, uint32_t pairs, uint32_t ended)
@@ -388,12 +415,16 @@ void launch_order(b3g_ctx* c, cudaStream_t s)
 			B.counters + CTR_STATUS, s);
 		k_layout_prev<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap);
 	}
+	// The contacts in their final places: the pass's table.
+	k_hash_clear<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, ~0u);
+	k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, ~0u);
 }
 
 uint32_t order_launches(const b3g_ctx* c)
 {
-	// scan, scatter, place; kept, scan, layout of the previous contacts
-	return 3 + (c->havePass ? 3 : 0);
+	// scan, scatter, place; kept, scan, layout of the previous contacts;
+	// the table's clear and fill
+	return 3 + (c->havePass ? 3 : 0) + 2;
 }
 
 // Host-driven replay of the wake-ups; runs only when some non-static body is
@@ -489,8 +520,8 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 		}
 		k_compact_move<<<persistent_blocks(4), 256, 0, s>>>(B, cur, cap, np, numNew, copied, kept2, kept2Total);
 		const uint32_t total = std::min(numNew + kept2Total, cap);
-		cudaMemsetAsync(B.hashKeys[cur], 0xFF, sizeof(unsigned long long) * B.hashCap, s);
-		k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, total);
+		k_hash_clear<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, total);
+		k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, total);
 		k_set_counts<<<1, 1, 0, s>>>(B, total, np - kept2Total);
 		launches += 1 + 3 + 1 + 1 + 1 + 1;
 	}

@@ -23,8 +23,9 @@ __device__ __forceinline__ int32_t previous_contact(const DevScene& S, const Buf
 {
 	// A fresh fixture continues no contact of its slot's previous holder.
 	bool fresh = S.fixLife[a] == FIX_FRESH || S.fixLife[b] == FIX_FRESH;
-	return havePrev && !fresh ? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf], B.hashCap, pair_key(a, b))
-							  : -1;
+	return havePrev && !fresh
+		? pair_hash_find(B.hashKeys[prevBuf], B.hashVals[prevBuf], B.hashMask[prevBuf] + 1u, pair_key(a, b))
+		: -1;
 }
 
 // Whether overlapping pair (a, b), whose previous contact is prev (or -1), is
@@ -355,7 +356,6 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 	uint32_t cap = c->cfg.max_contacts;
 	uint32_t cur = c->cur;
 	uint32_t nf = c->nFixtures;
-	cudaMemsetAsync(B.hashKeys[cur], 0xFF, sizeof(unsigned long long) * B.hashCap, s);
 	cudaMemsetAsync(B.prevFound, 0, sizeof(uint32_t) * cap, s);
 	cudaMemsetAsync(B.newOff, 0, sizeof(uint32_t) * (nf + 1), s);
 	cudaMemsetAsync(B.newFill, 0, sizeof(uint32_t) * (nf + 1), s);
