@@ -51,10 +51,10 @@ __device__ __forceinline__ uint32_t hash_mask_for(const Buffers& B, uint32_t con
 }
 
 // Clears the slots the table of this pass will use (total contacts, or the
-// pass's count when total is ~0u) and records its size.
+// pass's new plus kept contacts when total is ~0u) and records its size.
 __global__ void k_hash_clear(Buffers B, uint32_t cur, uint32_t cap, uint32_t total)
 {
-	const uint32_t n = total == ~0u ? min(B.counters[CTR_PAIRS], cap) : total;
+	const uint32_t n = total == ~0u ? min(B.counters[CTR_BEGUN] + B.counters[CTR_KEPT], cap) : total;
 	const uint32_t mask = hash_mask_for(B, n);
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		B.hashMask[cur] = mask;
@@ -82,6 +82,7 @@ __global__ void k_new_scatter(DevScene S, Buffers B, uint32_t nf)
 __global__ void k_new_place(DevScene S, Buffers B, uint32_t cur, uint32_t nf, int havePrev)
 {
 	uint32_t n = B.counters[CTR_BEGUN];
+	const uint32_t mask = B.hashMask[cur];
 	for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
 	{
 		uint32_t c = B.newTmp[t];
@@ -97,6 +98,7 @@ __global__ void k_new_place(DevScene S, Buffers B, uint32_t cur, uint32_t nf, in
 		B.pairB[cur][pos] = b;
 		B.prevIndex[pos] = -1;
 		B.posKey[pos] = pos;
+		insert_contact(B, cur, mask, a, b, pos);
 	}
 	if (!havePrev && blockIdx.x == 0 && threadIdx.x == 0)
 		B.counters[CTR_PAIRS] = n;
@@ -139,6 +141,7 @@ __global__ void k_kept(DevScene S, Buffers B, FilterArgs F, uint32_t cur, uint32
 // others are destroyed, listed in list order.
 __global__ void k_layout_prev(Buffers B, uint32_t cur, uint32_t cap)
 {
+	const uint32_t mask = B.hashMask[cur];
 	uint32_t prevBuf = cur ^ 1u;
 	uint32_t n = min(B.counters[CTR_PREV_PAIRS], cap);
 	uint32_t numNew = B.counters[CTR_BEGUN];
@@ -157,6 +160,7 @@ __global__ void k_layout_prev(Buffers B, uint32_t cur, uint32_t cap)
 				B.pairB[cur][pos] = b;
 				B.prevIndex[pos] = (int32_t)p;
 				B.posKey[pos] = numNew + p;
+				insert_contact(B, cur, mask, a, b, pos);
 			}
 		}
 		else
@@ -378,11 +382,11 @@ __global__ void k_compact_move(Buffers B, uint32_t cur, uint32_t cap, uint32_t n
 	}
 }
 
-// Fills the pass's table with its contacts (total, or the pass's count when
-// total is ~0u), after k_hash_clear.
-__global__ void k_rehash(Buffers B, uint32_t cur, uint32_t cap, uint32_t total)
+// Refills the pass's table with its first total contacts (after the
+// wake-up rounds moved them), after k_hash_clear.
+__global__ void k_rehash(Buffers B, uint32_t cur, uint32_t total)
 {
-	const uint32_t n = total == ~0u ? min(B.counters[CTR_PAIRS], cap) : total;
+	const uint32_t n = total;
 	const uint32_t mask = B.hashMask[cur];
 	for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
 		insert_contact(B, cur, mask, B.pairA[cur][c], B.pairB[cur][c], c);
@@ -406,25 +410,26 @@ void launch_order(b3g_ctx* c, cudaStream_t s)
 	const uint32_t cap = c->cfg.max_contacts, cur = c->cur, nf = c->nFixtures;
 	const int havePrev = c->havePass ? 1 : 0;
 	scan_exclusive(B.newOff, nf + 1, B.scanAux, B.counters + CTR_SCRATCH, B.counters + CTR_STATUS, s);
-	k_new_scatter<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, nf);
-	k_new_place<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, nf, havePrev);
 	if (havePrev)
 	{
 		k_kept<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap);
 		scan_exclusive_device(B.keptScan, B.counters + CTR_PREV_PAIRS, cap, B.scanAux, B.counters + CTR_KEPT,
 			B.counters + CTR_STATUS, s);
-		k_layout_prev<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap);
 	}
-	// The contacts in their final places: the pass's table.
+	// New and kept counts known: the pass's table, filled as the contacts
+	// take their places.
 	k_hash_clear<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, ~0u);
-	k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, ~0u);
+	k_new_scatter<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, nf);
+	k_new_place<<<persistent_blocks(4), 256, 0, s>>>(c->scene, B, cur, nf, havePrev);
+	if (havePrev)
+		k_layout_prev<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap);
 }
 
 uint32_t order_launches(const b3g_ctx* c)
 {
 	// scan, scatter, place; kept, scan, layout of the previous contacts;
-	// the table's clear and fill
-	return 3 + (c->havePass ? 3 : 0) + 2;
+	// the table's clear
+	return 3 + (c->havePass ? 3 : 0) + 1;
 }
 
 // Host-driven replay of the wake-ups; runs only when some non-static body is
@@ -521,7 +526,7 @@ int resolve_wakeups(b3g_ctx* c, cudaStream_t s)
 		k_compact_move<<<persistent_blocks(4), 256, 0, s>>>(B, cur, cap, np, numNew, copied, kept2, kept2Total);
 		const uint32_t total = std::min(numNew + kept2Total, cap);
 		k_hash_clear<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, total);
-		k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, cap, total);
+		k_rehash<<<persistent_blocks(8), 256, 0, s>>>(B, cur, total);
 		k_set_counts<<<1, 1, 0, s>>>(B, total, np - kept2Total);
 		launches += 1 + 3 + 1 + 1 + 1 + 1;
 	}

@@ -308,10 +308,18 @@ __global__ void k_settle(DevScene S, uint32_t nf)
 		S.fixLife[i] = FIX_LIVE;
 }
 
-__global__ void k_overflow_check(Buffers B, uint32_t cap)
+// The pair-overflow status; with clearFound, also clears the previous
+// contacts' found flags (k_diff sets them), only as many as the previous pass
+// had.
+__global__ void k_overflow_check(Buffers B, uint32_t cap, int clearFound)
 {
-	if (B.counters[CTR_RAW] > cap)
+	if (blockIdx.x == 0 && threadIdx.x == 0 && B.counters[CTR_RAW] > cap)
 		atomicOr(&B.counters[CTR_STATUS], B3G_ST_PAIR_OVERFLOW);
+	if (!clearFound)
+		return;
+	const uint32_t n = min(B.counters[CTR_PREV_PAIRS], cap);
+	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+		B.prevFound[p] = 0;
 }
 
 } // namespace
@@ -333,7 +341,7 @@ void launch_candidates(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	uint32_t cap = c->cfg.max_contacts;
-	k_overflow_check<<<1, 1, 0, s>>>(B, cap);
+	k_overflow_check<<<1, 1, 0, s>>>(B, cap, 0);
 	k_candidates<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), c->dCand, c->cur, cap,
 		c->havePass ? 1 : 0);
 }
@@ -356,10 +364,9 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 	uint32_t cap = c->cfg.max_contacts;
 	uint32_t cur = c->cur;
 	uint32_t nf = c->nFixtures;
-	cudaMemsetAsync(B.prevFound, 0, sizeof(uint32_t) * cap, s);
 	cudaMemsetAsync(B.newOff, 0, sizeof(uint32_t) * (nf + 1), s);
 	cudaMemsetAsync(B.newFill, 0, sizeof(uint32_t) * (nf + 1), s);
-	k_overflow_check<<<1, 1, 0, s>>>(B, cap);
+	k_overflow_check<<<persistent_blocks(2), 256, 0, s>>>(B, cap, 1);
 	k_diff<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap, nf,
 		c->havePass ? 1 : 0);
 	launch_order(c, s);
