@@ -764,40 +764,43 @@ __device__ __forceinline__ uint32_t walk(const DevScene& S, Buffers& B, int n, i
 }
 
 // limit: node visits allowed per walk (0: 2n + 1, more than a depth-first
-// walk makes), see b3g_set_walk_limit.
+// walk makes), see b3g_set_walk_limit. Each leaf's pairs then take a range of
+// the pass's pair list (rawA, rawB): one atomic per warp reserves the warp's
+// ranges (the order of the pairs is free: the contact order follows the proxy
+// keys), leafCount[j] keeps the range's start for the overflow records, and
+// the thread copies its scratch slots there.
 template <bool MW>
 __global__ void k_traverse_count(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap, uint32_t limit)
 {
-	int j = blockIdx.x * blockDim.x + threadIdx.x;
+	const int j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= n)
 		return;
-	if (S.fixLife[B.valsA[j]] == FIX_DEAD)
+	const uint32_t count = S.fixLife[B.valsA[j]] == FIX_DEAD ? 0u : walk<MW>(S, B, n, j, cap, limit);
+	// The warp's lanes with a leaf: a prefix of the warp.
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t live = min(32u, (uint32_t)n - ((uint32_t)j - lane));
+	const uint32_t mask = live == 32u ? 0xFFFFFFFFu : (1u << live) - 1u;
+	__syncwarp(mask);
+	uint32_t incl = count;
+	for (uint32_t o = 1; o < 32u; o <<= 1)
 	{
-		B.leafCount[j] = 0;
-		return;
+		const uint32_t y = __shfl_up_sync(mask, incl, o);
+		if (lane >= o)
+			incl += y;
 	}
-	B.leafCount[j] = walk<MW>(S, B, n, j, cap, limit);
-}
-
-// One thread per (slot, leaf), slot-major: copies the scratch records to the
-// contact arrays. After the exclusive scan leafCount holds offsets; a leaf's
-// count is the difference to the next offset (the last one to the total).
-template <bool MW>
-__global__ void k_traverse_emit(DevScene S, Buffers B, int n, uint32_t cur, uint32_t cap)
-{
-	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= (uint32_t)n * TRAV_SLOTS)
-		return;
-	uint32_t k = t / (uint32_t)n, j = t - k * (uint32_t)n;
-	uint32_t base = B.leafCount[j];
-	uint32_t end = (j == (uint32_t)n - 1) ? B.counters[CTR_RAW] : B.leafCount[j + 1];
-	uint32_t count = end - base;
-	if (k < count && k < TRAV_SLOTS)
+	uint32_t base = 0;
+	if (lane == live - 1u)
+		base = atomicAdd(&B.counters[CTR_RAW], incl);
+	base = __shfl_sync(mask, base, live - 1u) + incl - count;
+	B.leafCount[j] = base;
+	const uint2* scratch = reinterpret_cast<const uint2*>(B.pairScratch);
+	const uint32_t kept = min(count, TRAV_SLOTS);
+	for (uint32_t k = 0; k < kept; ++k)
 	{
-		uint32_t slot = base + k;
+		const uint32_t slot = base + k;
 		if (slot < cap)
 		{
-			uint2 p = reinterpret_cast<const uint2*>(B.pairScratch)[(size_t)k * n + j];
+			const uint2 p = scratch[(size_t)k * n + j];
 			B.rawA[slot] = p.x;
 			B.rawB[slot] = p.y;
 		}
@@ -1033,12 +1036,12 @@ uint32_t broadphase_launches(const b3g_ctx* c)
 	while ((1u << wb) < c->nWorlds)
 		++wb;
 	uint32_t passes = 4 + (wb + 7) / 8;
-	// traversal: walk, scan, emit, overflow
+	// traversal: walk (with the pair list's ranges), overflow records
 	if (!c->treeRebuild)
-		return 2 + 4; // leaves, refit
+		return 2 + 2; // leaves, refit
 	// bounds init, bounds, Morton; sort: histogram, scan, one kernel per
 	// pass; build; leaves, refit
-	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 4;
+	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 2;
 }
 
 void launch_broadphase(b3g_ctx* c, cudaStream_t s)
@@ -1123,16 +1126,12 @@ void launch_traverse(b3g_ctx* c, cudaStream_t s)
 		return;
 	const int tb = (int)c->tune.v[B3G_TUNE_TRAVERSE];
 	cudaMemsetAsync(B.counters + CTR_TRAV_OVERFLOW, 0, sizeof(uint32_t), s);
+	cudaMemsetAsync(B.counters + CTR_RAW, 0, sizeof(uint32_t), s);
 	if (c->nWorlds > 1)
 		k_traverse_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts,
 			c->walkLimit);
 	else
 		k_traverse_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts,
 			c->walkLimit);
-	scan_exclusive(B.leafCount, (uint32_t)n, B.scanAux, B.counters + CTR_RAW, B.counters + CTR_STATUS, s);
-	if (c->nWorlds > 1)
-		k_traverse_emit<true><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
-	else
-		k_traverse_emit<false><<<(n * TRAV_SLOTS + 255) / 256, 256, 0, s>>>(c->scene, B, n, cur, c->cfg.max_contacts);
 	k_traverse_overflow<<<persistent_blocks(2), 256, 0, s>>>(B, c->cfg.max_contacts);
 }
