@@ -1573,9 +1573,9 @@ extern "C" int b3g_collide(b3g_ctx* c, const float* state, int onDevice, void* s
 	c->treeRebuild = c->treeForce || c->treeLeaves != c->nFixtures || c->treeWorlds != c->nWorlds ||
 		c->treeSince + 1 >= c->treeInterval;
 	// pass_begin, sync, broadphase, diff + list order, bucket + apart + convex kernels + 2 hull +
-	// hull-triangle, finalize + pass_end + settle
+	// hull-triangle, finalize
 	const uint32_t passLaunches = 1 + 1 + (c->creationPass && c->nMeshFix ? 1 : 0) + broadphase_launches(c) +
-		pairs_diff_launches(c) + narrow_launches(c) + 3;
+		pairs_diff_launches(c) + narrow_launches(c) + 1;
 	// Host state takes the graph path when it is pinned (a graph copies it
 	// asynchronously; pageable memory would need the synchronous copy).
 	bool pinnedHost = false;
@@ -1854,7 +1854,7 @@ extern "C" int b3g_finish_pass(b3g_ctx* c, const uint8_t* keep, uint32_t count)
 	prof_mark(c, PM_FINAL, s);
 	if (c->profiling)
 		++c->profPass;
-	c->launches += pairs_diff_launches(c) + narrow_launches(c) + 3 +
+	c->launches += pairs_diff_launches(c) + narrow_launches(c) + 1 +
 		(rejected.empty() ? 0 : 1);
 	CK(cudaGetLastError());
 	c->creationPass = false;

@@ -193,8 +193,20 @@ __global__ void __launch_bounds__(BUCKET_THREADS) k_bucket(DevScene S, Buffers B
 constexpr int FIN_BATCH = 4;
 constexpr int FIN_THREADS = 256;
 
-__global__ void __launch_bounds__(FIN_THREADS) k_finalize(Buffers B, uint32_t cur, uint32_t cap)
+__global__ void __launch_bounds__(FIN_THREADS) k_finalize(DevScene S, Buffers B, uint32_t cur, uint32_t cap, uint32_t nf)
 {
+	// The pass's totals (counts the kernel does not change), and the fresh
+	// fixtures become ordinary live ones.
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+	{
+		B.totals[0] += 1;
+		B.totals[1] += min(B.counters[CTR_PAIRS], cap);
+		B.totals[4] += B.counters[CTR_BEGUN];
+		B.totals[5] += B.counters[CTR_ENDED];
+	}
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x)
+		if (S.fixLife[i] == FIX_FRESH)
+			S.fixLife[i] = FIX_LIVE;
 	uint32_t n = min(B.counters[CTR_PAIRS], cap);
 	uint32_t touching = 0, manifolds = 0, points = 0;
 	const uint32_t* __restrict__ cst = B.cstate[cur];
@@ -278,40 +290,10 @@ __global__ void __launch_bounds__(FIN_THREADS) k_finalize(Buffers B, uint32_t cu
 	}
 }
 
-__global__ void k_pass_end(Buffers B, uint32_t cap)
-{
-	if (threadIdx.x == 0)
-	{
-		B.totals[0] += 1;
-		B.totals[1] += min(B.counters[CTR_PAIRS], cap);
-		B.totals[4] += B.counters[CTR_BEGUN];
-		B.totals[5] += B.counters[CTR_ENDED];
-	}
-}
-
-__global__ void k_count_moved(Buffers B, uint32_t n)
-{
-	uint32_t m = 0;
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-		m += B.moved[i];
-	for (int o = 16; o > 0; o >>= 1)
-		m += __shfl_xor_sync(0xffffffffu, m, o);
-	if ((threadIdx.x & 31) == 0 && m)
-		atomicAdd(&B.counters[CTR_MOVED], m);
-}
-
-// After the pass, fresh fixtures are ordinary live ones.
-__global__ void k_settle(DevScene S, uint32_t nf)
-{
-	uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < nf && S.fixLife[i] == FIX_FRESH)
-		S.fixLife[i] = FIX_LIVE;
-}
-
 // The pair-overflow status; with clearFound, also clears the previous
 // contacts' found flags (k_diff sets them), only as many as the previous pass
 // had.
-__global__ void k_overflow_check(Buffers B, uint32_t cap, int clearFound)
+__global__ void k_overflow_check(Buffers B, uint32_t cap, int clearFound, uint32_t nf)
 {
 	if (blockIdx.x == 0 && threadIdx.x == 0 && B.counters[CTR_RAW] > cap)
 		atomicOr(&B.counters[CTR_STATUS], B3G_ST_PAIR_OVERFLOW);
@@ -320,6 +302,24 @@ __global__ void k_overflow_check(Buffers B, uint32_t cap, int clearFound)
 	const uint32_t n = min(B.counters[CTR_PREV_PAIRS], cap);
 	for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
 		B.prevFound[p] = 0;
+	// The proxies the broadphase re-inserted, one atomic per block.
+	__shared__ uint32_t sMoved[32];
+	uint32_t m = 0;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += gridDim.x * blockDim.x)
+		m += B.moved[i];
+	for (int o = 16; o > 0; o >>= 1)
+		m += __shfl_xor_sync(0xffffffffu, m, o);
+	if ((threadIdx.x & 31) == 0)
+		sMoved[threadIdx.x >> 5] = m;
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		m = 0;
+		for (uint32_t w = 0; w < blockDim.x / 32; ++w)
+			m += sMoved[w];
+		if (m)
+			atomicAdd(&B.counters[CTR_MOVED], m);
+	}
 }
 
 } // namespace
@@ -341,7 +341,7 @@ void launch_candidates(b3g_ctx* c, cudaStream_t s)
 {
 	Buffers& B = c->buf;
 	uint32_t cap = c->cfg.max_contacts;
-	k_overflow_check<<<1, 1, 0, s>>>(B, cap, 0);
+	k_overflow_check<<<1, 1, 0, s>>>(B, cap, 0, 0);
 	k_candidates<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), c->dCand, c->cur, cap,
 		c->havePass ? 1 : 0);
 }
@@ -366,16 +366,16 @@ void launch_pairs_diff(b3g_ctx* c, cudaStream_t s)
 	uint32_t nf = c->nFixtures;
 	cudaMemsetAsync(B.newOff, 0, sizeof(uint32_t) * (nf + 1), s);
 	cudaMemsetAsync(B.newFill, 0, sizeof(uint32_t) * (nf + 1), s);
-	k_overflow_check<<<persistent_blocks(2), 256, 0, s>>>(B, cap, 1);
+	k_overflow_check<<<persistent_blocks(2), 256, 0, s>>>(B, cap, 1, nf);
 	k_diff<<<persistent_blocks(8), 256, 0, s>>>(c->scene, B, make_filter_args(c), cur, cap, nf,
 		c->havePass ? 1 : 0);
 	launch_order(c, s);
-	k_count_moved<<<persistent_blocks(2), 256, 0, s>>>(B, c->nFixtures);
 }
 
 uint32_t pairs_diff_launches(const b3g_ctx* c)
 {
-	return 2 + order_launches(c) + 1;
+	// overflow check (with the found flags and the moved count), diff, order
+	return 2 + order_launches(c);
 }
 
 NPArgs make_np_args(b3g_ctx* c)
@@ -468,7 +468,6 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 
 void launch_finalize(b3g_ctx* c, cudaStream_t s)
 {
-	k_finalize<<<persistent_blocks(4), FIN_THREADS, 0, s>>>(c->buf, c->cur, c->cfg.max_contacts);
-	k_pass_end<<<1, 32, 0, s>>>(c->buf, c->cfg.max_contacts);
-	k_settle<<<(c->nFixtures + 255) / 256, 256, 0, s>>>(c->scene, c->nFixtures);
+	k_finalize<<<persistent_blocks(4), FIN_THREADS, 0, s>>>(c->scene, c->buf, c->cur, c->cfg.max_contacts,
+		c->nFixtures);
 }
