@@ -641,6 +641,57 @@ __global__ void k_refit(Buffers B, int n)
 	}
 }
 
+// Atomic min / max of IEEE floats (no NaN): non-negative floats order like
+// their bits as signed integers, negative ones in reverse as unsigned.
+__device__ __forceinline__ void atomic_min_float(float* a, float v)
+{
+	if (v >= 0.0f)
+		atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
+	else
+		atomicMax(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_float(float* a, float v)
+{
+	if (v >= 0.0f)
+		atomicMax(reinterpret_cast<int*>(a), __float_as_int(v));
+	else
+		atomicMin(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+
+// Refit of a reused tree (the passes between rebuilds): only the leaves whose
+// fat AABB was re-inserted (moved) changed, and a walk needs every node to
+// contain its leaves, not to be tight. A moved leaf's thread grows its
+// ancestors' boxes by its new box (atomic min / max per coordinate) and stops
+// at the first that already contains it (every node above contains that
+// one). Nodes only grow until the next rebuild makes them tight again; a dead
+// proxy's empty box and an unmoved leaf's box are contained already.
+__global__ void k_refit_grow(Buffers B, int n)
+{
+	const int j = blockIdx.x * blockDim.x + threadIdx.x;
+	if (j >= n || n < 2 || !B.moved[B.valsA[j]])
+		return;
+	const uint32_t leaf = n - 1 + j;
+	const float4 lo = B.nodeLo[leaf], hi = B.nodeHi[leaf];
+	uint32_t p = B.nodeParent[leaf];
+	while (true)
+	{
+		const float4 cl = __ldcg(&B.nodeLo[p]), ch = __ldcg(&B.nodeHi[p]);
+		if (cl.x <= lo.x && cl.y <= lo.y && cl.z <= lo.z && ch.x >= hi.x && ch.y >= hi.y && ch.z >= hi.z)
+			return;
+		float* plo = reinterpret_cast<float*>(&B.nodeLo[p]);
+		float* phi = reinterpret_cast<float*>(&B.nodeHi[p]);
+		atomic_min_float(plo + 0, lo.x);
+		atomic_min_float(plo + 1, lo.y);
+		atomic_min_float(plo + 2, lo.z);
+		atomic_max_float(phi + 0, hi.x);
+		atomic_max_float(phi + 1, hi.y);
+		atomic_max_float(phi + 2, hi.z);
+		if (p == 0)
+			return;
+		p = B.nodeParent[p];
+	}
+}
+
 // ---------------------------------------------------------------------------
 // Pair search.
 
@@ -1056,10 +1107,11 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	}
 	if (!c->treeRebuild)
 	{
-		// Same tree as the last pass: new leaf boxes, refit, walk.
+		// Same tree as the last pass: new leaf boxes, the moved leaves'
+		// ancestors grown to hold them, walk.
 		prof_mark(c, PM_SORTED, s);
 		k_leaves<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, n);
-		k_refit<<<(n + 255) / 256, 256, 0, s>>>(B, n);
+		k_refit_grow<<<(n + 255) / 256, 256, 0, s>>>(B, n);
 		prof_mark(c, PM_BUILT, s);
 		launch_traverse(c, s);
 		prof_mark(c, PM_TRAVERSED, s);
