@@ -479,6 +479,7 @@ extern "C" int b3g_create(const b3g_config* cfg, b3g_ctx** out)
 	step(dalloc(&B.nodeRope, 2 * P), "alloc");
 	step(dalloc(&B.nodeFirst, 2 * P), "alloc");
 	step(dalloc(&B.leafData, P), "alloc");
+	step(dalloc(&B.leafOf, P), "alloc");
 	step(dalloc(&B.nodeParent, 2 * P), "alloc");
 	step(dalloc(&B.nodeEnd, P), "alloc");
 	step(dalloc(&B.splitRight, P), "alloc");
@@ -586,6 +587,7 @@ extern "C" void b3g_destroy(b3g_ctx* c)
 	dfree(B.nodeRope);
 	dfree(B.nodeFirst);
 	dfree(B.leafData);
+	dfree(B.leafOf);
 	dfree(B.nodeParent);
 	dfree(B.nodeEnd);
 	dfree(B.splitRight);

@@ -167,6 +167,7 @@ struct Buffers
 	uint32_t* worldEnd;   // per sorted leaf: last sorted leaf of its world
 	uint32_t* proxyInfo;  // per proxy: body (bits 0-27), dynamic body (bit 28), shape type (bits 29-31)
 	uint2* leafData;      // per sorted leaf: its proxy's proxyInfo word and fixture key
+	uint32_t* leafOf;     // per proxy: its sorted leaf (set when the LBVH is built)
 	uint32_t* leafCount;  // pair count per sorted leaf (then exclusive offsets)
 	uint32_t* pairScratch; // first contact records (A, B) found per leaf, slot-major (B3G_TRAV_SLOTS x n uint2)
 	uint32_t* scanAux;

@@ -125,13 +125,70 @@ __device__ __forceinline__ void group_aabbs(const DevScene& S, uint32_t type, fl
 		aabb_extend(b, r);
 }
 
+// Atomic min / max of IEEE floats (no NaN): non-negative floats order like
+// their bits as signed integers, negative ones in reverse as unsigned.
+__device__ __forceinline__ void atomic_min_float(float* a, float v)
+{
+	if (v >= 0.0f)
+		atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
+	else
+		atomicMax(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_float(float* a, float v)
+{
+	if (v >= 0.0f)
+		atomicMax(reinterpret_cast<int*>(a), __float_as_int(v));
+	else
+		atomicMin(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
+}
+
+// Refit of a reused tree (the passes between rebuilds): only the proxies
+// whose fat AABB was re-inserted (moved) changed, and a walk needs every
+// node to contain its leaves, not to be tight. k_sync writes a moved proxy's
+// new box into its leaf and grows the leaf's ancestors by it (atomic min /
+// max per coordinate), stopping at the first that already contains it (every
+// node above contains that one). Nodes only grow until the next rebuild makes
+// them tight again; an unmoved leaf's box is contained already.
+__device__ __forceinline__ void grow_leaf(Buffers& B, uint32_t nLeaves, uint32_t proxy, V3 lo, V3 hi)
+{
+	const uint32_t leaf = nLeaves - 1u + B.leafOf[proxy];
+	float* llo = reinterpret_cast<float*>(&B.nodeLo[leaf]);
+	float* lhi = reinterpret_cast<float*>(&B.nodeHi[leaf]);
+	llo[0] = lo.x;
+	llo[1] = lo.y;
+	llo[2] = lo.z;
+	lhi[0] = hi.x;
+	lhi[1] = hi.y;
+	lhi[2] = hi.z;
+	if (nLeaves < 2)
+		return;
+	uint32_t p = B.nodeParent[leaf];
+	while (true)
+	{
+		const float4 cl = __ldcg(&B.nodeLo[p]), ch = __ldcg(&B.nodeHi[p]);
+		if (cl.x <= lo.x && cl.y <= lo.y && cl.z <= lo.z && ch.x >= hi.x && ch.y >= hi.y && ch.z >= hi.z)
+			return;
+		float* plo = reinterpret_cast<float*>(&B.nodeLo[p]);
+		float* phi = reinterpret_cast<float*>(&B.nodeHi[p]);
+		atomic_min_float(plo + 0, lo.x);
+		atomic_min_float(plo + 1, lo.y);
+		atomic_min_float(plo + 2, lo.z);
+		atomic_max_float(phi + 0, hi.x);
+		atomic_max_float(phi + 1, hi.y);
+		atomic_max_float(phi + 2, hi.z);
+		if (p == 0)
+			return;
+		p = B.nodeParent[p];
+	}
+}
+
 // One group of SYNC_LANES lanes per fixture; lane 0 writes. All lanes of a
 // group take the same branches, so the group mask is exact for the shuffles.
 // The per-body transforms of the pass (m_xf and b3Sweep::GetTransform(0),
 // sweep.h:43-63, two float4 each, read by the later stages) are written by
 // lane 1 of group b for body b. The fixture's records are loaded before any
 // branch so that their loads overlap.
-__global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int creation)
+__global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int creation, int grow)
 {
 	const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) / SYNC_LANES;
 	const uint32_t lane = threadIdx.x % SYNC_LANES;
@@ -257,6 +314,8 @@ __global__ void k_sync(DevScene S, Buffers B, uint32_t nf, uint32_t nb, int crea
 	B.fatLo[i] = make_float4(fat.lo.x, fat.lo.y, fat.lo.z, 0.0f);
 	B.fatHi[i] = make_float4(fat.hi.x, fat.hi.y, fat.hi.z, 0.0f);
 	B.moved[i] = 1;
+	if (grow)
+		grow_leaf(B, nf, i, fat.lo, fat.hi);
 }
 
 // ---------------------------------------------------------------------------
@@ -590,6 +649,7 @@ __global__ void k_leaves(DevScene S, Buffers B, int n)
 	uint32_t rope = (j == n - 1) ? SENT : B.splitRight[j];
 	B.nodeLeft[node] = proxy;
 	B.nodeFirst[node] = j;
+	B.leafOf[proxy] = j;
 	// Traversal reads a node as two float4: (lower, left child or proxy) and
 	// (upper, rope).
 	float4 lo = B.fatLo[proxy], hi = B.fatHi[proxy];
@@ -635,57 +695,6 @@ __global__ void k_refit(Buffers B, int n)
 		B.nodeLo[p] = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), __uint_as_float(l));
 		B.nodeHi[p] = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z),
 			__uint_as_float(B.nodeRope[p]));
-		if (p == 0)
-			return;
-		p = B.nodeParent[p];
-	}
-}
-
-// Atomic min / max of IEEE floats (no NaN): non-negative floats order like
-// their bits as signed integers, negative ones in reverse as unsigned.
-__device__ __forceinline__ void atomic_min_float(float* a, float v)
-{
-	if (v >= 0.0f)
-		atomicMin(reinterpret_cast<int*>(a), __float_as_int(v));
-	else
-		atomicMax(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
-}
-__device__ __forceinline__ void atomic_max_float(float* a, float v)
-{
-	if (v >= 0.0f)
-		atomicMax(reinterpret_cast<int*>(a), __float_as_int(v));
-	else
-		atomicMin(reinterpret_cast<unsigned int*>(a), __float_as_uint(v));
-}
-
-// Refit of a reused tree (the passes between rebuilds): only the leaves whose
-// fat AABB was re-inserted (moved) changed, and a walk needs every node to
-// contain its leaves, not to be tight. A moved leaf's thread grows its
-// ancestors' boxes by its new box (atomic min / max per coordinate) and stops
-// at the first that already contains it (every node above contains that
-// one). Nodes only grow until the next rebuild makes them tight again; a dead
-// proxy's empty box and an unmoved leaf's box are contained already.
-__global__ void k_refit_grow(Buffers B, int n)
-{
-	const int j = blockIdx.x * blockDim.x + threadIdx.x;
-	if (j >= n || n < 2 || !B.moved[B.valsA[j]])
-		return;
-	const uint32_t leaf = n - 1 + j;
-	const float4 lo = B.nodeLo[leaf], hi = B.nodeHi[leaf];
-	uint32_t p = B.nodeParent[leaf];
-	while (true)
-	{
-		const float4 cl = __ldcg(&B.nodeLo[p]), ch = __ldcg(&B.nodeHi[p]);
-		if (cl.x <= lo.x && cl.y <= lo.y && cl.z <= lo.z && ch.x >= hi.x && ch.y >= hi.y && ch.z >= hi.z)
-			return;
-		float* plo = reinterpret_cast<float*>(&B.nodeLo[p]);
-		float* phi = reinterpret_cast<float*>(&B.nodeHi[p]);
-		atomic_min_float(plo + 0, lo.x);
-		atomic_min_float(plo + 1, lo.y);
-		atomic_min_float(plo + 2, lo.z);
-		atomic_max_float(phi + 0, hi.x);
-		atomic_max_float(phi + 1, hi.y);
-		atomic_max_float(phi + 2, hi.z);
 		if (p == 0)
 			return;
 		p = B.nodeParent[p];
@@ -1070,8 +1079,10 @@ void launch_sync(b3g_ctx* c, cudaStream_t s)
 	if (n == 0)
 		return;
 	const size_t groups = std::max<size_t>(n, c->nBodies);
+	// A pass that reuses the LBVH refits it from here (grow_leaf).
+	const int grow = !c->treeRebuild && c->treeLeaves == n ? 1 : 0;
 	k_sync<<<(uint32_t)((groups * SYNC_LANES + 127) / 128), 128, 0, s>>>(c->scene, c->buf, n, c->nBodies,
-		c->creationPass ? 1 : 0);
+		c->creationPass ? 1 : 0, grow);
 	if (c->creationPass)
 		launch_mesh_fat(c, s);
 }
@@ -1089,7 +1100,7 @@ uint32_t broadphase_launches(const b3g_ctx* c)
 	uint32_t passes = 4 + (wb + 7) / 8;
 	// traversal: walk (with the pair list's ranges), overflow records
 	if (!c->treeRebuild)
-		return 2 + 2; // leaves, refit
+		return 2; // the tree refit by the sync kernel
 	// bounds init, bounds, Morton; sort: histogram, scan, one kernel per
 	// pass; build; leaves, refit
 	return 3 + (passes + 2) + (n > 1 ? 1 : 0) + 2 + 2;
@@ -1107,11 +1118,8 @@ void launch_broadphase(b3g_ctx* c, cudaStream_t s)
 	}
 	if (!c->treeRebuild)
 	{
-		// Same tree as the last pass: new leaf boxes, the moved leaves'
-		// ancestors grown to hold them, walk.
+		// Same tree as the last pass, refit by k_sync (grow_leaf): walk.
 		prof_mark(c, PM_SORTED, s);
-		k_leaves<<<(n + 255) / 256, 256, 0, s>>>(c->scene, B, n);
-		k_refit_grow<<<(n + 255) / 256, 256, 0, s>>>(B, n);
 		prof_mark(c, PM_BUILT, s);
 		launch_traverse(c, s);
 		prof_mark(c, PM_TRAVERSED, s);
