@@ -1039,6 +1039,12 @@ extern "C" int b3g_set_fixtures(b3g_ctx* c, uint32_t nf, const uint32_t* body, c
 		CK(cudaMemcpy(c->dFixParams, p4.data(), sizeof(float4) * 3 * nf, cudaMemcpyHostToDevice));
 	}
 	c->hFixType.assign(shapeType, shapeType + nf);
+	c->anyTriangle = c->anySensor = false;
+	for (uint32_t i = 0; i < nf; ++i)
+	{
+		c->anyTriangle |= shapeType[i] == B3G_SHAPE_TRIANGLE;
+		c->anySensor |= (flags[i] & B3G_FIXTURE_SENSOR) != 0;
+	}
 	c->nFixtures = nf;
 	c->capFixtures = nf;
 	c->keysAreIndex = true;
@@ -1299,6 +1305,8 @@ extern "C" int b3g_update_scene_device(b3g_ctx* c, uint32_t nb, const uint32_t* 
 	launch_update(c, u, s);
 	CK(cudaGetLastError());
 	c->treeForce = true; // fixtures created, replaced or retired: new leaves
+	// The written fixtures' types and flags stay on the device.
+	c->anyTriangle = c->anySensor = true;
 	// The host copy of fixture types is refreshed when the stand-alone
 	// narrowphase next needs it; written bodies are awake, so the sleep count
 	// can only have dropped (it stays an upper bound until the next wake-up
@@ -1395,7 +1403,11 @@ extern "C" int b3g_update_scene(b3g_ctx* c, uint32_t nb, const uint32_t* bodyInd
 	c->treeForce = true; // fixtures created, replaced or retired: new leaves
 	// Host shadows: fixture types (stand-alone narrowphase) and sleep count.
 	for (uint32_t i = 0; i < nf; ++i)
+	{
 		c->hFixType[fixIndex[i]] = shapeType[i];
+		c->anyTriangle |= shapeType[i] == B3G_SHAPE_TRIANGLE;
+		c->anySensor |= (flags[i] & B3G_FIXTURE_SENSOR) != 0;
+	}
 	for (uint32_t i = 0; i < nb; ++i)
 	{
 		uint32_t b = bodyIndex[i];
@@ -1544,7 +1556,10 @@ static void wait_copies(b3g_ctx* c, cudaStream_t s)
 // probe and SAT, hull-triangle, and the mesh work.
 static uint32_t narrow_launches(const b3g_ctx* c)
 {
-	return 1 + 1 + B3G_CONVEX_KERNELS + 2 + 2 + 1 + mesh_launches(c);
+	uint32_t k = 0;
+	for (int b = 0; b < B3G_CONVEX_KERNELS; ++b)
+		k += convex_bucket_possible(c, b) ? 1u : 0u;
+	return 1 + 1 + k + 2 + 2 + (c->anyTriangle ? 1u : 0u) + mesh_launches(c);
 }
 
 // The LBVH bookkeeping once a pass's broadphase is issued.

@@ -434,6 +434,8 @@ struct b3g_ctx
 	// next pass
 	std::vector<uint32_t> hBodyType;
 	uint32_t asleep;
+	bool anyTriangle;     // some fixture may be a triangle (the triangle buckets can be non-empty)
+	bool anySensor;       // some fixture may be a sensor
 
 	// kernels launched by passes (host count)
 	uint64_t launches;

@@ -979,6 +979,10 @@ void launch_convex_buckets(const NPArgs& base, const uint32_t* lists, const uint
 	const Tune& tune, cudaStream_t s);
 void launch_convex_one(int k, const NPArgs& base, const uint32_t* lists, const uint32_t* counts, uint32_t cap,
 	const Tune& tune, cudaStream_t s);
+// Whether convex bucket kernel k (the order of B3G_TUNE_CONVEX) can have
+// contacts in this context's pass: the triangle buckets need triangle
+// fixtures, the sensor bucket sensors, the inactive bucket a sleeping body.
+bool convex_bucket_possible(const b3g_ctx* c, int k);
 void launch_hulls(const NPArgs& base, const uint32_t* list, const uint32_t* count, uint32_t maxUE, const Tune& tune,
 	cudaStream_t s);
 void launch_hulls_probe(const NPArgs& base, const uint32_t* list, const uint32_t* count, const Tune& tune,

@@ -445,15 +445,17 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 	}
 	launch_hulls(a, B.bucketList + (size_t)BK_HULLS * cap, B.counters + CTR_BUCKET0 + BK_HULLS,
 		c->maxUniqueEdges, c->tune, side);
-	launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap, B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE,
-		c->maxUniqueEdges, c->tune, side);
+	if (c->anyTriangle)
+		launch_hull_triangles(a, B.bucketList + (size_t)BK_HULL_TRIANGLE * cap,
+			B.counters + CTR_BUCKET0 + BK_HULL_TRIANGLE, c->maxUniqueEdges, c->tune, side);
 	prof_mark(c, PM_HULLS, s);
 	launch_apart(a, B.bucketList + (size_t)BK_APART * cap, B.counters + CTR_BUCKET0 + BK_APART, s);
 	// The convex kernels (hull-sphere and hull-capsule each a scan kernel and
 	// a follow-up kernel on the contacts the scan hands on) run beside the
 	// hull-hull probe and SAT: the two branches take about as long.
 	for (int k = 0; k < B3G_CONVEX_KERNELS; ++k)
-		launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
+		if (convex_bucket_possible(c, k))
+			launch_convex_one(k, a, B.bucketList, B.counters + CTR_BUCKET0, cap, c->tune, s);
 	prof_mark(c, PM_CONVEX, s);
 	if (side != s)
 	{
@@ -464,6 +466,22 @@ void launch_narrowphase(b3g_ctx* c, cudaStream_t s)
 		cudaStreamWaitEvent(s, c->meshJoin, 0);
 	launch_mesh_collide(c, B.bucketList + (size_t)BK_MESH * cap, B.counters + CTR_BUCKET0 + BK_MESH, s);
 	prof_mark(c, PM_MESH, s);
+}
+
+bool convex_bucket_possible(const b3g_ctx* c, int k)
+{
+	switch (k)
+	{
+	case 3:
+	case 4:
+		return c->anyTriangle;
+	case 7:
+		return c->anySensor;
+	case 8:
+		return c->asleep > 0;
+	default:
+		return true;
+	}
 }
 
 void launch_finalize(b3g_ctx* c, cudaStream_t s)
